@@ -1,0 +1,145 @@
+/*
+ * mflab200: C ABI of the B200 (sm_100a) multi-double dense linear-algebra
+ * backend for Float64x2 / Float64x3 / Float64x4.
+ *
+ * Every entry point replaces a Julia generic function of
+ * MultiFloatLinearAlgebra.jl on the dense hot path; the citation on each
+ * declaration is the reference function (path:line inside that project) whose
+ * arguments, results and failure behaviour it keeps.
+ *
+ * Conventions
+ *   - A Float64xN matrix lives in device memory as N column-major binary64
+ *     planes ("limb planes"): limb l of element (r, c) (0-based) of matrix X
+ *     is X[l*lsx + c*ldx + r].  ldx is the column stride, lsx the plane
+ *     stride, both in doubles.  Sub-matrix views are plain pointer offsets.
+ *   - `limbs` is N in {2, 3, 4}.  Scalars (alpha, beta) are HOST arrays of
+ *     `limbs` doubles.
+ *   - `stream` is a cudaStream_t (NULL = the legacy default stream).  All
+ *     work is stream-ordered; nothing synchronises unless stated.
+ *   - Return value: MFLAB_OK (0) or a negative MFLAB_ERR_* code for bad
+ *     arguments (the reference's DimensionMismatch / ArgumentError), CUDA
+ *     failures or bounded-wait timeouts.  Numerical status of a
+ *     factorization (0, -1 non-finite input, k > 0 failing pivot) is written
+ *     to a DEVICE int, exactly the reference's `info` field.
+ *   - Pivot vectors are 1-based int64 on the device, as in the reference.
+ *   - No entry point falls back to the CPU: without a usable device it
+ *     returns an error.
+ */
+#ifndef MFLAB200_H
+#define MFLAB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MFLAB_OK 0
+#define MFLAB_ERR_ARG (-1)         /* shape / argument error (DimensionMismatch, ArgumentError) */
+#define MFLAB_ERR_CUDA (-2)        /* a CUDA runtime call failed */
+#define MFLAB_ERR_UNSUPPORTED (-3) /* limb count or option not supported */
+#define MFLAB_ERR_TIMEOUT (-4)     /* a bounded device wait ran out */
+#define MFLAB_ERR_ALLOC (-5)       /* device memory could not be reserved */
+#define MFLAB_ERR_ALIAS (-6)       /* output aliases an input (types.jl:261-267) */
+
+/* GEMM routes (gemm.jl:44-136 gemm_plan strategies) */
+#define MFLAB_GEMM_AUTO 0   /* reference :auto: fused mulacc for x3, direct otherwise */
+#define MFLAB_GEMM_DIRECT 1 /* reference :direct: acc + a*b for every limb count */
+#define MFLAB_GEMM_OZAKI 2  /* INT8-slice tensor-core route (no reference counterpart) */
+
+typedef struct mflab_handle mflab_handle;
+
+/* ------------------------------------------------------------ library --- */
+/* library version as 10000*major + 100*minor + patch */
+int mflab_version(void);
+/* short description of an MFLAB_* code */
+const char *mflab_status_string(int code);
+/* message of the last error raised on the calling host thread ("" if none) */
+const char *mflab_last_error(void);
+
+/* A handle owns per-caller device scratch, like the reference's MFWorkspace
+   (types.jl:71-123): one handle per concurrent caller. */
+int mflab_create(mflab_handle **out, int device);
+int mflab_destroy(mflab_handle *h);
+
+/* ---------------------------------------------------------- BLAS-like --- */
+/* C = alpha*A*B + beta*C; A m x k, B k x n, C m x n.  With beta == 0 C is not
+   read.  route: MFLAB_GEMM_*.
+   Replaces gemm!(C, A, B, alpha, beta; config) — src/kernels/gemm.jl:747-774. */
+int mflab_gemm(mflab_handle *h, void *stream, int limbs, int route, int64_t m, int64_t n,
+               int64_t k, const double *A, int64_t lda, int64_t lsa, const double *B, int64_t ldb,
+               int64_t lsb, double *C, int64_t ldc, int64_t lsc, const double *alpha,
+               const double *beta);
+
+/* lower(C) = alpha * P^T * P + beta * lower(C); P is k x n, C n x n.  The
+   strict upper triangle of C is neither read nor written.
+   Replaces syrk!(C, P, alpha, beta; uplo=:lower) — src/kernels/syrk.jl:67-108. */
+int mflab_syrk_lower(mflab_handle *h, void *stream, int limbs, int64_t n, int64_t k,
+                     const double *P, int64_t ldp, int64_t lsp, double *C, int64_t ldc,
+                     int64_t lsc, const double *alpha, const double *beta);
+
+/* lower(C) = alpha * A * B^T + beta * lower(C); A, B are n x k.
+   Replaces gemmt!(C, A, B, alpha, beta) — src/kernels/gemmt.jl:69-108. */
+int mflab_gemmt_lower(mflab_handle *h, void *stream, int limbs, int64_t n, int64_t k,
+                      const double *A, int64_t lda, int64_t lsa, const double *B, int64_t ldb,
+                      int64_t lsb, double *C, int64_t ldc, int64_t lsc, const double *alpha,
+                      const double *beta);
+
+/* side: 0 = left (op(A) X = alpha B, A m x m), 1 = right (X op(A) = alpha B,
+   A n x n); uplo: 0 lower, 1 upper; trans: 0 N, 1 T; diag: 0 nonunit, 1 unit.
+   B (m x n) is overwritten with X.
+   Replaces trsm!(B, A, alpha; side, uplo, trans, diag) — src/kernels/trsm.jl:224-302,
+   and for n == 1, side == 0 also trsv! — src/kernels/trsv.jl:19-73. */
+int mflab_trsm(mflab_handle *h, void *stream, int limbs, int side, int uplo, int trans, int diag,
+               int64_t m, int64_t n, const double *A, int64_t lda, int64_t lsa, double *B,
+               int64_t ldb, int64_t lsb, const double *alpha);
+
+/* ----------------------------------------------------- factorizations --- */
+/* Blocked lower Cholesky in place (block <= 32 columns; the reference default
+   is 16).  Only the lower triangle is read or written.  *info (device int):
+   0 success, -1 non-finite lower triangle, k > 0 the first column whose
+   Schur-complement diagonal is not positive.
+   Replaces cholesky!(A; check=false, config) — src/factorizations/cholesky.jl:68-107. */
+int mflab_potrf(mflab_handle *h, void *stream, int limbs, int64_t n, double *A, int64_t lda,
+                int64_t lsa, int64_t block, int *info);
+
+/* B <- S^{-1} B with a successful Cholesky factor L (n x n), B n x nrhs.
+   Replaces ldiv!(B, F::MFCholesky) — src/solve.jl:54-83 (vector form :23-50). */
+int mflab_potrs(mflab_handle *h, void *stream, int limbs, int64_t n, int64_t nrhs,
+                const double *L, int64_t ldl, int64_t lsl, double *B, int64_t ldb, int64_t lsb);
+
+/* Blocked partial-pivoting LU in place; ipiv (device, min(m,n) int64,
+   1-based) records the row swapped with row k at step k.  *info: 0, -1
+   non-finite input, k > 0 exactly zero pivot at column k.
+   Replaces lu!(A; check=false, config) — src/factorizations/lu.jl:128-195. */
+int mflab_getrf(mflab_handle *h, void *stream, int limbs, int64_t m, int64_t n, double *A,
+                int64_t lda, int64_t lsa, int64_t *ipiv, int64_t block, int *info);
+
+/* B <- A^{-1} B with a successful LU factor: row interchanges, unit-lower
+   then upper triangular solves.
+   Replaces ldiv!(B, F::MFLU) — src/solve.jl:147-181 (vector form :115-145). */
+int mflab_getrs(mflab_handle *h, void *stream, int limbs, int64_t n, int64_t nrhs,
+                const double *LU, int64_t ldl, int64_t lsl, const int64_t *ipiv, double *B,
+                int64_t ldb, int64_t lsb);
+
+/* ------------------------------------------------------- diagnostics --- */
+/* out (device, limbs+1 doubles) = [max |A(r,c)| over the region, finite flag]
+   with region 0 all entries, 1 lower (r >= c), 2 upper (r <= c).
+   Serves _maximum_abs / _lower_maximum_abs / _all_finite /
+   _lower_triangle_finite (src/types.jl:306-331) and _lu_maximum_u
+   (src/diagnostics.jl:74-81). */
+int mflab_max_abs(mflab_handle *h, void *stream, int limbs, int64_t m, int64_t n, const double *A,
+                  int64_t lda, int64_t lsa, int region, double *out);
+
+/* O(n) tail of factor_diagnostics (src/diagnostics.jl:21-107): out (device,
+   4*limbs+2 doubles) = [min |A(i,i)|, max |A(i,i)|, max/min (Inf if min is
+   zero), num/den (0 if den is zero), count, count > 0] over i < count.
+   num/den (device, limbs doubles each) may be NULL. */
+int mflab_diag_summary(mflab_handle *h, void *stream, int limbs, const double *A, int64_t lda,
+                       int64_t lsa, int64_t count, const double *num, const double *den,
+                       double *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MFLAB200_H */

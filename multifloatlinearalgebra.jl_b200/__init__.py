@@ -1,0 +1,686 @@
+"""B200 multi-double dense linear algebra with MultiFloatLinearAlgebra.jl's API.
+
+Host-side mirror of the reference's public surface
+(src/MultiFloatLinearAlgebra.jl:34-49) over the mflab200 C ABI.  Julia's
+mutating `name!` functions are spelled `name_` here (gemm_, cholesky_, ldiv_,
+...); argument meaning, defaults and failure behaviour follow the reference:
+
+* DimensionMismatch / ArgumentError for bad shapes, options and aliasing;
+* cholesky_/lu_/ldlt_ with check=True raise PosDefException /
+  SingularException / DomainError, with check=False return a factor whose
+  factor_status is the reference's info code (0, -1, k);
+* beta == 0 never reads the destination; only the authoritative triangle is
+  read or written by syrk_/gemmt_/cholesky_/ldlt_.
+
+Matrices live on the GPU as MFMatrix: N column-major float64 limb planes in a
+torch tensor (PyTorch provides device memory and the current stream only).
+Every numerical operation runs in the CUDA library; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+import threading
+from typing import Optional, Sequence, Union
+
+import numpy as np
+import torch
+
+from . import _native
+
+__all__ = [
+    "MFMatrix", "KernelConfig", "DimensionMismatch", "ArgumentError", "DomainError",
+    "PosDefException", "SingularException", "MFLABError",
+    "gemm_", "syrk_", "gemmt_", "trsm_", "trsv_", "gemm_plan",
+    "cholesky_", "lu_", "ldiv_", "solve", "issuccess",
+    "factor_status", "factor_state", "factor_kind", "factor_matrix", "factor_precision",
+    "factor_provider", "factor_pivots", "factor_diagnostics",
+    "MFCholesky", "MFLU", "capabilities", "limb_type_name",
+]
+
+
+# ------------------------------------------------------------- errors ----
+class DimensionMismatch(ValueError):
+    """Julia's DimensionMismatch."""
+
+
+class ArgumentError(ValueError):
+    """Julia's ArgumentError."""
+
+
+class DomainError(ValueError):
+    """Julia's DomainError (non-finite factorization input with check=true)."""
+
+
+class PosDefException(Exception):
+    """LinearAlgebra.PosDefException(info)."""
+
+    def __init__(self, info: int):
+        super().__init__(f"matrix is not positive definite; factorization failed at {info}")
+        self.info = info
+
+
+class SingularException(Exception):
+    """LinearAlgebra.SingularException(info)."""
+
+    def __init__(self, info: int):
+        super().__init__(f"matrix is singular; factorization failed at {info}")
+        self.info = info
+
+
+class MFLABError(RuntimeError):
+    """A CUDA failure, timeout or resource error reported by the library."""
+
+
+def _check(rc: int, what: str) -> None:
+    if rc == _native.MFLAB_OK:
+        return
+    lib = _native.load()
+    msg = f"{what}: {lib.mflab_status_string(rc).decode()}"
+    detail = lib.mflab_last_error().decode()
+    if detail:
+        msg += f" ({detail})"
+    if rc == _native.MFLAB_ERR_ARG:
+        raise DimensionMismatch(msg)
+    if rc == _native.MFLAB_ERR_ALIAS:
+        raise ArgumentError(f"{what} does not support output/input aliasing")
+    if rc == _native.MFLAB_ERR_UNSUPPORTED:
+        raise ArgumentError(msg)
+    raise MFLABError(msg)
+
+
+# ------------------------------------------------------------ handles ----
+_handles: dict = {}
+_handles_lock = threading.Lock()
+
+
+def _handle(device: int):
+    key = (device, threading.get_ident())
+    with _handles_lock:
+        h = _handles.get(key)
+        if h is None:
+            lib = _native.load()
+            out = C.c_void_p()
+            _check(lib.mflab_create(C.byref(out), device), "mflab_create")
+            h = out
+            _handles[key] = h
+        return h
+
+
+def _stream(device: int) -> int:
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+def limb_type_name(N: int) -> str:
+    return f"Float64x{N}"
+
+
+# ------------------------------------------------------------- config ----
+@dataclasses.dataclass(frozen=True)
+class KernelConfig:
+    """Route and block configuration (src/types.jl:13-27).  Fields without a
+    GPU meaning (thread_count, reduction_tile, column_tile, packed-GEMM
+    tuning) are kept for signature compatibility and ignored."""
+
+    reduction_tile: int = 64
+    column_tile: int = 16
+    cholesky_block: int = 16
+    lu_block: int = 16
+    ldlt_block: int = 0
+    ldlt_strategy: str = "auto"
+    ldlt_blocked_crossover: int = 512
+    thread_count: int = 1
+    gemm_strategy: str = "auto"
+    gemm_packed_crossover: int = 2**63 - 1
+    gemm_panel_columns: int = 0
+    gemm_micro_columns: int = 0
+    ozaki_slices: int = 0
+
+
+_DEFAULT = KernelConfig()
+_ROUTES = {"auto": 0, "direct": 1, "fused": 0, "ozaki": 2}
+
+
+def gemm_plan(N: int, m: int, k: int, n: int, config: KernelConfig = _DEFAULT) -> dict:
+    """Resolve the GEMM route (src/kernels/gemm.jl:44-136) for the device."""
+    if not 1 <= N <= 4:
+        raise ArgumentError("only 1-4 limb MultiFloats are supported")
+    s = config.gemm_strategy
+    if s not in ("auto", "direct", "packed", "fused", "ozaki"):
+        raise ArgumentError("gemm_strategy must be :auto, :direct, :packed, :fused or :ozaki")
+    if s == "fused" and N != 3:
+        raise ArgumentError("gemm_strategy=:fused is only available for Float64x3")
+    if s == "packed":
+        s = "direct"  # packing is a CPU cache device; the device mainloop stages tiles itself
+    if s == "auto":
+        strategy, reason = ("fused", "auto_fused_direct") if N == 3 else ("direct", "auto_direct")
+    else:
+        strategy, reason = s, f"forced_{s}"
+    return {"strategy": strategy, "reason": reason}
+
+
+# ------------------------------------------------------------- matrix ----
+class MFMatrix:
+    """A Float64xN matrix (or vector) as N column-major limb planes on a GPU.
+
+    storage: torch.float64 CUDA tensor of shape (N, ncols, ld); limb l of
+    element (r, c) of this view is storage[l, c0 + c, r0 + r]."""
+
+    __slots__ = ("storage", "r0", "c0", "m", "n", "is_vector")
+
+    def __init__(self, storage: torch.Tensor, r0: int = 0, c0: int = 0, m: Optional[int] = None,
+                 n: Optional[int] = None, is_vector: bool = False):
+        if storage.dtype != torch.float64 or storage.dim() != 3:
+            raise ArgumentError("MFMatrix storage must be a (N, ncols, ld) float64 tensor")
+        if not storage.is_cuda:
+            raise ArgumentError("MFMatrix storage must live on a CUDA device")
+        if storage.stride(2) != 1:
+            raise ArgumentError("limb planes must be column-major (unit row stride)")
+        self.storage = storage
+        self.r0, self.c0 = r0, c0
+        self.m = storage.shape[2] - r0 if m is None else m
+        self.n = storage.shape[1] - c0 if n is None else n
+        self.is_vector = is_vector
+
+    # geometry
+    @property
+    def N(self) -> int:
+        return self.storage.shape[0]
+
+    @property
+    def shape(self):
+        return (self.m,) if self.is_vector else (self.m, self.n)
+
+    @property
+    def ld(self) -> int:
+        return self.storage.stride(1)
+
+    @property
+    def ls(self) -> int:
+        return self.storage.stride(0)
+
+    @property
+    def device(self) -> int:
+        return self.storage.device.index
+
+    def ptr(self) -> int:
+        return self.storage.data_ptr() + 8 * (self.c0 * self.ld + self.r0)
+
+    def __len__(self):
+        return self.m
+
+    def __repr__(self):
+        kind = "vector" if self.is_vector else "matrix"
+        return f"MFMatrix({limb_type_name(self.N)} {kind} {self.shape} on cuda:{self.device})"
+
+    # construction
+    @classmethod
+    def empty(cls, N: int, m: int, n: Optional[int] = None, device=None) -> "MFMatrix":
+        vec = n is None
+        n = 1 if vec else n
+        dev = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+        st = torch.empty((N, max(n, 0), max(m, 1)), dtype=torch.float64, device=dev)
+        return cls(st, 0, 0, m, n, vec)
+
+    @classmethod
+    def zeros(cls, N: int, m: int, n: Optional[int] = None, device=None) -> "MFMatrix":
+        x = cls.empty(N, m, n, device)
+        x.storage.zero_()
+        return x
+
+    @classmethod
+    def from_numpy(cls, X: np.ndarray, device=None) -> "MFMatrix":
+        """X shaped (N, m, n) (matrix) or (N, m) (vector), limb-major."""
+        X = np.asarray(X, dtype=np.float64)
+        vec = X.ndim == 2
+        if vec:
+            X = X[:, :, None]
+        if X.ndim != 3:
+            raise ArgumentError("expected an (N, m, n) or (N, m) limb array")
+        dev = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+        st = torch.from_numpy(np.ascontiguousarray(X.transpose(0, 2, 1))).to(dev)
+        if st.shape[2] == 0:
+            st = torch.zeros((X.shape[0], X.shape[2], 1), dtype=torch.float64, device=dev)
+        return cls(st, 0, 0, X.shape[1], X.shape[2], vec)
+
+    @classmethod
+    def from_tensor(cls, planes: torch.Tensor, is_vector: bool = False) -> "MFMatrix":
+        """planes shaped (N, n, m): used as storage without a copy."""
+        return cls(planes, 0, 0, planes.shape[2], planes.shape[1], is_vector)
+
+    def planes(self) -> torch.Tensor:
+        """(N, n, m) torch view of this matrix's elements."""
+        return self.storage[:, self.c0:self.c0 + self.n, self.r0:self.r0 + self.m]
+
+    def to_numpy(self) -> np.ndarray:
+        a = self.planes().cpu().numpy().transpose(0, 2, 1)
+        return np.ascontiguousarray(a[:, :, 0] if self.is_vector else a)
+
+    def copy(self) -> "MFMatrix":
+        st = self.planes().contiguous().clone()
+        if st.shape[2] == 0:
+            st = torch.zeros((self.N, self.n, 1), dtype=torch.float64, device=self.storage.device)
+        return MFMatrix(st, 0, 0, self.m, self.n, self.is_vector)
+
+    def copy_(self, other: "MFMatrix") -> "MFMatrix":
+        if (other.N, other.m, other.n) != (self.N, self.m, self.n):
+            raise DimensionMismatch("copy source and destination dimensions differ")
+        self.planes().copy_(other.planes())
+        return self
+
+    def view(self, rows: slice, cols: slice = slice(None)) -> "MFMatrix":
+        r = range(self.m)[rows]
+        c = range(self.n)[cols]
+        if r.step != 1 or c.step != 1:
+            raise ArgumentError("only unit-stride views are supported")
+        return MFMatrix(self.storage, self.r0 + r.start, self.c0 + c.start, len(r), len(c), False)
+
+
+# ------------------------------------------------------------ helpers ----
+def _scalar(N: int, v) -> "C.Array":
+    arr = (C.c_double * 4)()
+    if isinstance(v, (int, float)):
+        arr[0] = float(v)
+    else:
+        vals = np.asarray(v, dtype=np.float64).ravel()
+        if len(vals) > N:
+            raise ArgumentError("scalar has more limbs than the matrix type")
+        for i, x in enumerate(vals):
+            arr[i] = float(x)
+    return arr
+
+
+def _same_type(*mats: MFMatrix) -> int:
+    N = mats[0].N
+    for x in mats:
+        if not isinstance(x, MFMatrix):
+            raise ArgumentError("expected MFMatrix operands")
+        if x.N != N:
+            raise ArgumentError("operands have different limb counts")
+        if x.device != mats[0].device:
+            raise ArgumentError("operands live on different devices")
+    if not 1 <= N <= 4:
+        raise ArgumentError("only 1-4 limb MultiFloats are supported")
+    if N == 1:
+        raise ArgumentError("Float64x1 is plain Float64; use a Float64 BLAS")
+    return N
+
+
+def _mightalias(a: MFMatrix, b: MFMatrix) -> bool:
+    """2-D index-range overlap of two views (Base.mightalias on views)."""
+    if a.storage.data_ptr() != b.storage.data_ptr():
+        sa, ea = a.storage.data_ptr(), a.storage.data_ptr() + 8 * a.storage.numel()
+        sb, eb = b.storage.data_ptr(), b.storage.data_ptr() + 8 * b.storage.numel()
+        return sa < eb and sb < ea
+    rows = a.r0 < b.r0 + b.m and b.r0 < a.r0 + a.m
+    cols = a.c0 < b.c0 + b.n and b.c0 < a.c0 + a.n
+    return rows and cols and a.m > 0 and b.m > 0 and a.n > 0 and b.n > 0
+
+
+def _no_alias(op: str, dest: MFMatrix, src: MFMatrix) -> None:
+    if _mightalias(dest, src):
+        raise ArgumentError(f"{op} does not support output/input aliasing")
+
+
+def _lib_h(x: MFMatrix):
+    return _native.load(), _handle(x.device), _stream(x.device)
+
+
+# --------------------------------------------------------------- BLAS ----
+def gemm_(C_: MFMatrix, A: MFMatrix, B: MFMatrix, alpha=1.0, beta=0.0,
+          config: KernelConfig = _DEFAULT, workspace=None) -> MFMatrix:
+    """C = alpha*A*B + beta*C (src/kernels/gemm.jl:747-774)."""
+    N = _same_type(C_, A, B)
+    m, k = A.m, A.n
+    if B.m != k:
+        raise DimensionMismatch("gemm! inner dimensions differ")
+    n = B.n
+    if (C_.m, C_.n) != (m, n):
+        raise DimensionMismatch("gemm! output dimensions differ")
+    _no_alias("gemm!", C_, A)
+    _no_alias("gemm!", C_, B)
+    plan = gemm_plan(N, m, k, n, config)
+    route = _ROUTES[plan["strategy"]]
+    lib, h, s = _lib_h(C_)
+    rc = lib.mflab_gemm(h, s, N, route, m, n, k, A.ptr(), A.ld, A.ls, B.ptr(), B.ld, B.ls,
+                        C_.ptr(), C_.ld, C_.ls, _scalar(N, alpha), _scalar(N, beta))
+    _check(rc, "gemm!")
+    return C_
+
+
+def syrk_(C_: MFMatrix, P: MFMatrix, alpha=1.0, beta=0.0, uplo: str = "lower",
+          config: KernelConfig = _DEFAULT) -> MFMatrix:
+    """lower(C) = alpha*P^T*P + beta*C (src/kernels/syrk.jl:67-108)."""
+    if uplo not in ("lower", "L"):
+        raise ArgumentError("syrk! currently supports only uplo=:lower or :L")
+    N = _same_type(C_, P)
+    n, k = P.n, P.m
+    if (C_.m, C_.n) != (n, n):
+        raise DimensionMismatch("syrk! output dimensions differ")
+    _no_alias("syrk!", C_, P)
+    lib, h, s = _lib_h(C_)
+    rc = lib.mflab_syrk_lower(h, s, N, n, k, P.ptr(), P.ld, P.ls, C_.ptr(), C_.ld, C_.ls,
+                              _scalar(N, alpha), _scalar(N, beta))
+    _check(rc, "syrk!")
+    return C_
+
+
+def gemmt_(C_: MFMatrix, A: MFMatrix, B: MFMatrix, alpha=1.0, beta=0.0,
+           config: KernelConfig = _DEFAULT) -> MFMatrix:
+    """lower(C) = alpha*A*B^T + beta*C (src/kernels/gemmt.jl:69-108)."""
+    N = _same_type(C_, A, B)
+    rows, k = A.m, A.n
+    if (B.m, B.n) != (rows, k):
+        raise DimensionMismatch("gemmt! input dimensions differ")
+    if (C_.m, C_.n) != (rows, rows):
+        raise DimensionMismatch("gemmt! output dimensions differ")
+    _no_alias("gemmt!", C_, A)
+    _no_alias("gemmt!", C_, B)
+    lib, h, s = _lib_h(C_)
+    rc = lib.mflab_gemmt_lower(h, s, N, rows, k, A.ptr(), A.ld, A.ls, B.ptr(), B.ld, B.ls,
+                               C_.ptr(), C_.ld, C_.ls, _scalar(N, alpha), _scalar(N, beta))
+    _check(rc, "gemmt!")
+    return C_
+
+
+_SIDE = {"left": 0, "right": 1}
+_UPLO = {"lower": 0, "upper": 1}
+_TRANS = {"N": 0, "T": 1}
+_DIAG = {"nonunit": 0, "unit": 1}
+
+
+def trsm_(B: MFMatrix, A: MFMatrix, alpha=1.0, side: str = "left", uplo: str = "lower",
+          trans: str = "N", diag: str = "nonunit", config: KernelConfig = _DEFAULT) -> MFMatrix:
+    """op(A) X = alpha B or X op(A) = alpha B in place (src/kernels/trsm.jl:224-302)."""
+    N = _same_type(B, A)
+    if A.m != A.n:
+        raise DimensionMismatch("trsm! requires a square triangular matrix")
+    if side not in _SIDE:
+        raise ArgumentError("side must be :left or :right")
+    if uplo not in _UPLO:
+        raise ArgumentError("uplo must be :lower or :upper")
+    if trans not in _TRANS:
+        raise ArgumentError("trans must be :N or :T")
+    if diag not in _DIAG:
+        raise ArgumentError("diag must be :unit or :nonunit")
+    if side == "left" and B.m != A.m:
+        raise DimensionMismatch("trsm! left dimensions differ")
+    if side == "right" and B.n != A.m:
+        raise DimensionMismatch("trsm! right dimensions differ")
+    _no_alias("trsm!", B, A)
+    lib, h, s = _lib_h(B)
+    rc = lib.mflab_trsm(h, s, N, _SIDE[side], _UPLO[uplo], _TRANS[trans], _DIAG[diag], B.m, B.n,
+                        A.ptr(), A.ld, A.ls, B.ptr(), B.ld, B.ls, _scalar(N, alpha))
+    _check(rc, "trsm!")
+    return B
+
+
+def trsv_(x: MFMatrix, A: MFMatrix, alpha=1.0, uplo: str = "lower", trans: str = "N",
+          diag: str = "nonunit", config: KernelConfig = _DEFAULT) -> MFMatrix:
+    """op(A) x = alpha b in place (src/kernels/trsv.jl:19-73)."""
+    if A.m != A.n:
+        raise DimensionMismatch("trsv! requires a square triangular matrix")
+    if x.m != A.m or x.n != 1:
+        raise DimensionMismatch("trsv! right-hand side length differs")
+    return trsm_(x, A, alpha, "left", uplo, trans, diag, config)
+
+
+# ------------------------------------------------------- factorizations ----
+class _Factor:
+    kind = "abstract"
+
+    def __init__(self, factors: MFMatrix, info: int):
+        self.factors = factors
+        self.info = int(info)
+
+    @property
+    def N(self) -> int:
+        return self.factors.N
+
+    def __repr__(self):
+        return (f"MF{self.kind.upper()}({limb_type_name(self.N)}, {self.factors.m}x"
+                f"{self.factors.n}, status={self.info})")
+
+
+class MFCholesky(_Factor):
+    """Lower Cholesky factor (src/factorizations/cholesky.jl:1-8)."""
+    kind = "cholesky"
+
+
+class MFLU(_Factor):
+    """Partial-pivoting LU factor (src/factorizations/lu.jl:1-14)."""
+    kind = "lu"
+
+    def __init__(self, factors, ipiv: torch.Tensor, info, original_maximum: torch.Tensor):
+        super().__init__(factors, info)
+        self.ipiv = ipiv
+        self.original_maximum = original_maximum
+
+
+def _read_info(dev_info: torch.Tensor) -> int:
+    return int(dev_info.item())
+
+
+def _finite_region(A: MFMatrix, region: int) -> bool:
+    out = torch.empty(A.N + 1, dtype=torch.float64, device=A.storage.device)
+    lib, h, s = _lib_h(A)
+    _check(lib.mflab_max_abs(h, s, A.N, A.m, A.n, A.ptr(), A.ld, A.ls, region, out.data_ptr()),
+           "max_abs")
+    return bool(out[A.N].item() == 1.0)
+
+
+def cholesky_(A: MFMatrix, check: bool = True, config: KernelConfig = _DEFAULT) -> MFCholesky:
+    """Blocked lower Cholesky in place (src/factorizations/cholesky.jl:68-107)."""
+    N = _same_type(A)
+    if A.m != A.n:
+        raise DimensionMismatch("cholesky! requires a square matrix")
+    info = torch.zeros(1, dtype=torch.int32, device=A.storage.device)
+    block = max(config.cholesky_block, 1)
+    lib, h, s = _lib_h(A)
+    _check(lib.mflab_potrf(h, s, N, A.m, A.ptr(), A.ld, A.ls, block, info.data_ptr()), "cholesky!")
+    st = _read_info(info)
+    if st == -1 and check:
+        raise DomainError("cholesky!: input matrix contains non-finite entries")
+    if st > 0 and check:
+        raise PosDefException(st)
+    return MFCholesky(A, st)
+
+
+def lu_(A: MFMatrix, check: bool = True, config: KernelConfig = _DEFAULT,
+        workspace=None) -> MFLU:
+    """Blocked partial-pivoting LU in place (src/factorizations/lu.jl:128-195)."""
+    N = _same_type(A)
+    m, n = A.m, A.n
+    kmax = min(m, n)
+    dev = A.storage.device
+    info = torch.zeros(1, dtype=torch.int32, device=dev)
+    ipiv = torch.arange(1, kmax + 1, dtype=torch.int64, device=dev)
+    omax = torch.zeros(N + 1, dtype=torch.float64, device=dev)
+    lib, h, s = _lib_h(A)
+    if m > 0 and n > 0:
+        _check(lib.mflab_max_abs(h, s, N, m, n, A.ptr(), A.ld, A.ls, 0, omax.data_ptr()), "lu!")
+    block = max(config.lu_block, 1)
+    _check(lib.mflab_getrf(h, s, N, m, n, A.ptr(), A.ld, A.ls,
+                           ipiv.data_ptr() if kmax > 0 else None, block, info.data_ptr()), "lu!")
+    st = _read_info(info)
+    if st == -1:
+        omax.zero_()
+        if check:
+            raise DomainError("lu!: input matrix contains non-finite entries")
+    if st > 0 and check:
+        raise SingularException(st)
+    return MFLU(A, ipiv, st, omax[:N].clone())
+
+
+def issuccess(F: _Factor) -> bool:
+    return F.info == 0
+
+
+def factor_status(F: _Factor) -> int:
+    return F.info
+
+
+def factor_kind(F: _Factor) -> str:
+    return F.kind
+
+
+def factor_matrix(F: _Factor) -> MFMatrix:
+    return F.factors
+
+
+def factor_precision(F: _Factor) -> str:
+    return limb_type_name(F.N)
+
+
+def factor_provider(F: _Factor) -> str:
+    return "mfla_b200"
+
+
+def factor_state(F: _Factor) -> str:
+    """types.jl:394-403"""
+    st = factor_status(F)
+    if st == 0:
+        return "success"
+    if st == -1:
+        return "nonfinite_input"
+    if st < 0:
+        return "numerical_breakdown"
+    if F.kind == "cholesky":
+        return "not_posdef"
+    if F.kind in ("lu", "ldlt"):
+        return "singular"
+    return "numerical_breakdown"
+
+
+def factor_pivots(F: _Factor) -> np.ndarray:
+    if isinstance(F, MFLU):
+        return F.ipiv.cpu().numpy().copy()
+    if hasattr(F, "pivots"):
+        return F.pivots.cpu().numpy().copy()
+    raise ArgumentError("factor has no pivots")
+
+
+def _check_solve(F: _Factor) -> None:
+    if not issuccess(F):
+        if F.kind == "cholesky":
+            raise PosDefException(F.info)
+        raise SingularException(F.info)
+
+
+def ldiv_(dest: MFMatrix, F: _Factor, source: Optional[MFMatrix] = None,
+          config: KernelConfig = _DEFAULT) -> MFMatrix:
+    """Solve in place with a successful factor (src/solve.jl:23-423)."""
+    _check_solve(F)
+    N = _same_type(dest, F.factors)
+    n = F.factors.m
+    if F.factors.n != n:
+        raise DimensionMismatch("solve requires a square factor")
+    if source is not None:
+        if (source.m, source.n) != (dest.m, dest.n):
+            raise DimensionMismatch("source and destination dimensions differ")
+    if dest.m != n:
+        raise DimensionMismatch("right-hand side dimensions differ")
+    _no_alias("ldiv!", dest, F.factors)
+    if source is not None and source is not dest:
+        if _mightalias(dest, source):
+            raise ArgumentError("ldiv! does not support partially overlapping right-hand sides")
+        dest.copy_(source)
+    lib, h, s = _lib_h(dest)
+    L = F.factors
+    if F.kind == "cholesky":
+        rc = lib.mflab_potrs(h, s, N, n, dest.n, L.ptr(), L.ld, L.ls, dest.ptr(), dest.ld, dest.ls)
+    elif F.kind == "lu":
+        rc = lib.mflab_getrs(h, s, N, n, dest.n, L.ptr(), L.ld, L.ls, F.ipiv.data_ptr(), dest.ptr(),
+                             dest.ld, dest.ls)
+    else:
+        return _ldiv_extra(dest, F, lib, h, s)
+    _check(rc, "ldiv!")
+    return dest
+
+
+def _ldiv_extra(dest, F, lib, h, s):
+    raise ArgumentError(f"ldiv! is not available for {F.kind}")
+
+
+def solve(F: _Factor, rhs: MFMatrix, config: KernelConfig = _DEFAULT) -> MFMatrix:
+    """Non-mutating solve (src/solve.jl:555-565)."""
+    return ldiv_(rhs.copy(), F, config=config)
+
+
+def _mf_values(t: torch.Tensor, N: int, count: int) -> list:
+    a = t.cpu().numpy()
+    return [a[i * N:(i + 1) * N].copy() for i in range(count)]
+
+
+def factor_diagnostics(F: _Factor) -> dict:
+    """Numerical facts about a factor (src/diagnostics.jl:32-246).  MF-valued
+    fields are numpy arrays of N limbs; absent values are None."""
+    N = F.N
+    A = F.factors
+    dev = A.storage.device
+    lib, h, s = _lib_h(A)
+    base = {
+        "kind": F.kind, "status": F.info, "state": factor_state(F), "success": issuccess(F),
+        "precision": factor_precision(F), "provider": factor_provider(F),
+        "failure_location": F.info if F.info > 0 else None,
+    }
+    out = torch.zeros(4 * N + 2, dtype=torch.float64, device=dev)
+    if F.kind == "cholesky":
+        n = A.m
+        accepted = n if F.info == 0 else (F.info - 1 if F.info > 0 else 0)
+        _check(lib.mflab_diag_summary(h, s, N, A.ptr(), A.ld, A.ls, accepted, None, None,
+                                      out.data_ptr()), "factor_diagnostics")
+        mn, mx, spread, _ = _mf_values(out, N, 4)
+        has = accepted > 0
+        base.update({
+            "accepted_pivots": accepted,
+            "minimum_diagonal": mn if has else None,
+            "maximum_diagonal": mx if has else None,
+            "diagonal_spread": spread if has else None,
+            "finite": _finite_region(A, 1),
+        })
+        return base
+    if F.kind == "lu":
+        kmax = min(A.m, A.n)
+        accepted = F.info - 1 if F.info > 0 else (kmax if F.info == 0 else 0)
+        umax = torch.zeros(N + 1, dtype=torch.float64, device=dev)
+        _check(lib.mflab_max_abs(h, s, N, A.m, A.n, A.ptr(), A.ld, A.ls, 2, umax.data_ptr()),
+               "factor_diagnostics")
+        _check(lib.mflab_diag_summary(h, s, N, A.ptr(), A.ld, A.ls, accepted, umax.data_ptr(),
+                                      F.original_maximum.data_ptr(), out.data_ptr()),
+               "factor_diagnostics")
+        mn, mx, _, growth = _mf_values(out, N, 4)
+        omax = F.original_maximum.cpu().numpy()
+        has = accepted > 0
+        base.update({
+            "accepted_pivots": accepted,
+            "pivots": F.ipiv.cpu().numpy().copy(),
+            "minimum_pivot": mn if has else None,
+            "maximum_pivot": mx if has else None,
+            "original_maximum": None if F.info == -1 else omax.copy(),
+            "maximum_u": umax[:N].cpu().numpy(),
+            "pivot_growth": None if not np.any(omax != 0) else growth,
+            "finite": _finite_region(A, 0),
+        })
+        return base
+    return _diagnostics_extra(F, base)
+
+
+def _diagnostics_extra(F, base):
+    raise ArgumentError(f"no diagnostics for {F.kind}")
+
+
+def capabilities(N: int) -> dict:
+    """Machine-readable facts about this backend (src/capabilities.jl:14-74)."""
+    supported = 2 <= N <= 4
+    return {
+        "provider": "mfla_b200", "scalar_type": limb_type_name(N), "base_type": "Float64",
+        "supported": supported, "limb_count": N,
+        "gemm": supported, "gemmt": supported, "syrk": supported, "trsv": supported,
+        "trsm": supported, "cholesky": supported, "lu": supported,
+        "factor_diagnostics": supported, "vector_rhs": supported, "multi_rhs": supported,
+        "factor_metadata_ownership": "factor_owned", "factor_matrix_ownership": "borrowed_input",
+        "factorization_destructive": True, "factor_solve_mutates_factor": False,
+        "syrk_authoritative_triangle": "lower", "syrk_inactive_triangle": "preserved",
+        "device": "cuda", "gemm_routes": ["auto", "direct", "fused", "ozaki"],
+    }

@@ -1,0 +1,109 @@
+"""Binding of the mflab200 C ABI (include/mflab200.h) and its in-tree build.
+
+The product path is the CUDA library built here for sm_100a.  Loading fails
+loudly when the library is missing or no CUDA device is present: there is no
+CPU fallback anywhere in this package.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import glob
+import os
+import subprocess
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+REPO_DIR = os.path.dirname(PKG_DIR)
+LIB_PATH = os.path.join(PKG_DIR, "libmflab200.so")
+CSRC = os.path.join(PKG_DIR, "csrc")
+INCLUDE = os.path.join(REPO_DIR, "include")
+
+NVCC_FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
+    "--fmad=false", "-Xcompiler", "-fPIC", "-shared",
+]
+
+MFLAB_OK = 0
+MFLAB_ERR_ARG = -1
+MFLAB_ERR_CUDA = -2
+MFLAB_ERR_UNSUPPORTED = -3
+MFLAB_ERR_TIMEOUT = -4
+MFLAB_ERR_ALLOC = -5
+MFLAB_ERR_ALIAS = -6
+
+
+def sources() -> list[str]:
+    return sorted(glob.glob(os.path.join(CSRC, "*.cu")))
+
+
+def build(verbose: bool = False) -> str:
+    """Compile every CUDA source into libmflab200.so (sm_100a) in the package."""
+    nvcc = os.environ.get("NVCC", "nvcc")
+    cmd = [nvcc, *NVCC_FLAGS, "-I", INCLUDE, "-o", LIB_PATH, *sources(), "-lcublasLt"]
+    out = subprocess.run(cmd, capture_output=True, text=True)
+    if out.returncode != 0:
+        raise RuntimeError("nvcc failed:\n" + " ".join(cmd) + "\n" + out.stdout + out.stderr)
+    if verbose:
+        print(out.stdout + out.stderr)
+    return LIB_PATH
+
+
+_d = C.POINTER(C.c_double)
+_i64 = C.c_int64
+_vp = C.c_void_p
+_int = C.c_int
+
+# name -> argtypes (all return int unless listed in _RESTYPE)
+SIGNATURES = {
+    "mflab_version": [],
+    "mflab_status_string": [_int],
+    "mflab_last_error": [],
+    "mflab_create": [C.POINTER(_vp), _int],
+    "mflab_destroy": [_vp],
+    "mflab_gemm": [_vp, _vp, _int, _int, _i64, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _i64, _vp,
+                   _i64, _i64, _d, _d],
+    "mflab_syrk_lower": [_vp, _vp, _int, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _i64, _d, _d],
+    "mflab_gemmt_lower": [_vp, _vp, _int, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _i64, _vp, _i64,
+                          _i64, _d, _d],
+    "mflab_trsm": [_vp, _vp, _int, _int, _int, _int, _int, _i64, _i64, _vp, _i64, _i64, _vp, _i64,
+                   _i64, _d],
+    "mflab_potrf": [_vp, _vp, _int, _i64, _vp, _i64, _i64, _i64, _vp],
+    "mflab_potrs": [_vp, _vp, _int, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _i64],
+    "mflab_getrf": [_vp, _vp, _int, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _vp],
+    "mflab_getrs": [_vp, _vp, _int, _i64, _i64, _vp, _i64, _i64, _vp, _vp, _i64, _i64],
+    "mflab_max_abs": [_vp, _vp, _int, _i64, _i64, _vp, _i64, _i64, _int, _vp],
+    "mflab_diag_summary": [_vp, _vp, _int, _vp, _i64, _i64, _i64, _vp, _vp, _vp],
+    "mflab_probe_fp64": [_vp, _int, _int, _int, _i64, _vp, _d],
+}
+_RESTYPE = {"mflab_status_string": C.c_char_p, "mflab_last_error": C.c_char_p}
+
+_lib = None
+
+
+def load(path: str | None = None):
+    """Load the built library (no build, no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = path or LIB_PATH
+    if not os.path.exists(path):
+        raise RuntimeError(
+            f"mflab200 CUDA library not found at {path}; build it with "
+            "`python -c 'import __graft_entry__ as g; g.build()'` (nvcc, sm_100a)")
+    lib = C.CDLL(path)
+    for name, args in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = _RESTYPE.get(name, _int)
+    _lib = lib
+    return lib
+
+
+def declared_symbols() -> list[str]:
+    """Every function the public headers declare (parsed from include/*.h)."""
+    import re
+    names = []
+    for h in sorted(glob.glob(os.path.join(INCLUDE, "*.h"))):
+        text = open(h).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names += re.findall(r"\b(mflab_\w+)\s*\(", text)
+    return sorted(set(names))

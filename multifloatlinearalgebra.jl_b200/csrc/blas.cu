@@ -1,0 +1,276 @@
+// Matched-order multi-double GEMM / SYRK / GEMMT on the FP64 pipe.
+//
+// Reduction-order contract (src/kernels/gemm.jl:138-265, syrk.jl:1-50,
+// gemmt.jl:1-52 of MultiFloatLinearAlgebra.jl): every output element is ONE
+// serial chain acc = 0; for k ascending: acc = acc + a(i,k)*b(k,j), followed
+// by alpha*acc (beta == 0: C is never read) or alpha*acc + beta*C.  No split-k
+// and no tree reduction, so with the same scalar networks the result is
+// bitwise the reference's.
+//
+// Mapping: a CTA owns a BM x BN output tile; each thread owns TM x TN outputs
+// strided by the thread grid so shared-memory reads are conflict-free
+// broadcasts.  k-slabs of BK columns of every limb plane are staged in shared
+// memory with cp.async into a double buffer while the previous slab is
+// consumed.  The kernel is FP64-issue bound: per k step a thread reads
+// (TM + TN)*N doubles and executes TM*TN*ops(N) FP64 instructions.
+#include "mf_device.cuh"
+#include "mflab_internal.h"
+
+namespace mfl {
+
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem, bool pred) {
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    int src_size = pred ? 8 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem),
+                 "r"(src_size)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int n>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(n) : "memory");
+}
+
+template <int N, int BM, int BN, int BK, int TM, int TN>
+struct MMShape {
+    static constexpr int TX = BM / TM;
+    static constexpr int TY = BN / TN;
+    static constexpr int NT = TX * TY;
+    static constexpr size_t smem_bytes = sizeof(double) * 2 * N * BK * (BM + BN);
+};
+
+template <int N, int BM, int BN, int BK, int TM, int TN, bool TA, bool TB, bool TRI, bool FUSED>
+__global__ void __launch_bounds__(MMShape<N, BM, BN, BK, TM, TN>::NT)
+    mm_kernel(int64_t m, int64_t n, int64_t K, Mat A, Mat B, Mat C, scal<N> alpha, scal<N> beta,
+              int overwrite, const int *info) {
+    using S = MMShape<N, BM, BN, BK, TM, TN>;
+    constexpr int NT = S::NT, TX = S::TX, TY = S::TY;
+    extern __shared__ double smem[];
+    double *As = smem;                   // [2][N][BK][BM]
+    double *Bs = smem + 2 * N * BK * BM;  // [2][N][BK][BN]
+    const int tid = threadIdx.x;
+    const int tx = tid % TX, ty = tid / TX;
+    const int64_t row0 = (int64_t)blockIdx.x * BM, col0 = (int64_t)blockIdx.y * BN;
+    if (TRI && row0 + BM - 1 < col0) return;  // tile strictly above the diagonal
+    if (info && *info) return;                 // an earlier factorization step failed
+
+    mf<N> acc[TM][TN];
+#pragma unroll
+    for (int i = 0; i < TM; ++i)
+#pragma unroll
+        for (int j = 0; j < TN; ++j) acc[i][j] = from_double<N>(0.0);
+
+    auto load_tile = [&](int buf, int64_t k0) {
+        for (int e = tid; e < BM * BK; e += NT) {
+            int i, kk;
+            if (!TA) {
+                i = e % BM;
+                kk = e / BM;
+            } else {
+                kk = e % BK;
+                i = e / BK;
+            }
+            int64_t gi = row0 + i, gk = k0 + kk;
+            bool ok = gi < m && gk < K;
+            const double *src = ok ? (TA ? A.p + gi * A.ld + gk : A.p + gk * A.ld + gi) : A.p;
+#pragma unroll
+            for (int l = 0; l < N; ++l)
+                cp_async8(&As[((buf * N + l) * BK + kk) * BM + i], src + (ok ? l * A.ls : 0), ok);
+        }
+        for (int e = tid; e < BN * BK; e += NT) {
+            int j, kk;
+            if (!TB) {
+                kk = e % BK;
+                j = e / BK;
+            } else {
+                j = e % BN;
+                kk = e / BN;
+            }
+            int64_t gj = col0 + j, gk = k0 + kk;
+            bool ok = gj < n && gk < K;
+            const double *src = ok ? (TB ? B.p + gk * B.ld + gj : B.p + gj * B.ld + gk) : B.p;
+#pragma unroll
+            for (int l = 0; l < N; ++l)
+                cp_async8(&Bs[((buf * N + l) * BK + kk) * BN + j], src + (ok ? l * B.ls : 0), ok);
+        }
+    };
+
+    auto step = [&](int buf, int kk) {
+        mf<N> a[TM], b[TN];
+#pragma unroll
+        for (int i = 0; i < TM; ++i)
+#pragma unroll
+            for (int l = 0; l < N; ++l) a[i].v[l] = As[((buf * N + l) * BK + kk) * BM + tx + i * TX];
+#pragma unroll
+        for (int j = 0; j < TN; ++j)
+#pragma unroll
+            for (int l = 0; l < N; ++l) b[j].v[l] = Bs[((buf * N + l) * BK + kk) * BN + ty + j * TY];
+#pragma unroll
+        for (int i = 0; i < TM; ++i)
+#pragma unroll
+            for (int j = 0; j < TN; ++j) acc[i][j] = mac<N, FUSED>(acc[i][j], a[i], b[j]);
+    };
+
+    const int64_t nk = (K + BK - 1) / BK;
+    if (nk > 0) {
+        load_tile(0, 0);
+        cp_async_commit();
+    }
+    for (int64_t kt = 0; kt < nk; ++kt) {
+        const int buf = (int)(kt & 1);
+        if (kt + 1 < nk) load_tile(buf ^ 1, (kt + 1) * BK);
+        cp_async_commit();
+        cp_async_wait<1>();
+        __syncthreads();
+        const int64_t rem = K - kt * BK;
+        if (rem >= BK) {
+#pragma unroll 2
+            for (int kk = 0; kk < BK; ++kk) step(buf, kk);
+        } else {
+            for (int kk = 0; kk < (int)rem; ++kk) step(buf, kk);
+        }
+        __syncthreads();
+    }
+
+    const mf<N> al = alpha.get(), be = beta.get();
+#pragma unroll
+    for (int i = 0; i < TM; ++i) {
+#pragma unroll
+        for (int j = 0; j < TN; ++j) {
+            const int64_t gi = row0 + tx + i * TX, gj = col0 + ty + j * TY;
+            if (gi < m && gj < n && (!TRI || gi >= gj)) {
+                mf<N> r = mul(al, acc[i][j]);
+                if (!overwrite) r = add(r, mul(be, load_mf<N>(C.p, C.ld, C.ls, gi, gj)));
+                store_mf<N>(C.p, C.ld, C.ls, gi, gj, r);
+            }
+        }
+    }
+}
+
+template <int N, int BM, int BN, int BK, int TM, int TN, bool TA, bool TB, bool TRI, bool FUSED>
+static int run_mm(int64_t m, int64_t n, int64_t k, Mat A, Mat B, Mat C, const double *alpha,
+                  const double *beta, cudaStream_t s, const int *info) {
+    using S = MMShape<N, BM, BN, BK, TM, TN>;
+    auto kern = mm_kernel<N, BM, BN, BK, TM, TN, TA, TB, TRI, FUSED>;
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)S::smem_bytes);
+        if (e != cudaSuccess) return record_cuda_error(e, "mm_kernel attribute");
+        configured = true;
+    }
+    scal<N> al{}, be{};
+    int overwrite = 1;
+    for (int l = 0; l < N; ++l) {
+        al.v[l] = alpha[l];
+        be.v[l] = beta[l];
+        if (beta[l] != 0.0) overwrite = 0;
+    }
+    if (m <= 0 || n <= 0) return MFLAB_OK;
+    dim3 grid((unsigned)((m + BM - 1) / BM), (unsigned)((n + BN - 1) / BN));
+    if (grid.y > 65535) return MFLAB_ERR_UNSUPPORTED;
+    kern<<<grid, S::NT, S::smem_bytes, s>>>(m, n, k, A, B, C, al, be, overwrite, info);
+    return record_cuda_error(cudaGetLastError(), "mm_kernel launch");
+}
+
+// tile shapes per limb count (FP64-issue bound; registers: TM*TN*N accumulators)
+template <int N, bool TA, bool TB, bool TRI, bool FUSED>
+static int run_mm_n(int64_t m, int64_t n, int64_t k, Mat A, Mat B, Mat C, const double *alpha,
+                    const double *beta, cudaStream_t s, const int *info) {
+    if constexpr (N == 2)
+        return run_mm<2, 64, 64, 16, 4, 4, TA, TB, TRI, FUSED>(m, n, k, A, B, C, alpha, beta, s, info);
+    else if constexpr (N == 3)
+        return run_mm<3, 64, 64, 8, 4, 4, TA, TB, TRI, FUSED>(m, n, k, A, B, C, alpha, beta, s, info);
+    else
+        return run_mm<4, 64, 32, 8, 4, 2, TA, TB, TRI, FUSED>(m, n, k, A, B, C, alpha, beta, s, info);
+}
+
+template <int N>
+static int dispatch_mm(bool ta, bool tb, int tri, bool fused3, int64_t m, int64_t n, int64_t k,
+                       Mat A, Mat B, Mat C, const double *alpha, const double *beta,
+                       cudaStream_t s, const int *info) {
+    if (!ta && !tb && !tri) {
+        if (N == 3 && fused3)
+            return run_mm_n<N, false, false, false, true>(m, n, k, A, B, C, alpha, beta, s, info);
+        return run_mm_n<N, false, false, false, false>(m, n, k, A, B, C, alpha, beta, s, info);
+    }
+    if (ta && !tb && tri) return run_mm_n<N, true, false, true, false>(m, n, k, A, B, C, alpha, beta, s, info);
+    if (!ta && tb && tri) return run_mm_n<N, false, true, true, false>(m, n, k, A, B, C, alpha, beta, s, info);
+    return MFLAB_ERR_UNSUPPORTED;
+}
+
+int launch_mm(int N, bool ta, bool tb, int tri, bool fused3, int64_t m, int64_t n, int64_t k,
+              Mat A, Mat B, Mat C, const double *alpha, const double *beta, cudaStream_t s,
+              const int *info) {
+    switch (N) {
+    case 2: return dispatch_mm<2>(ta, tb, tri, fused3, m, n, k, A, B, C, alpha, beta, s, info);
+    case 3: return dispatch_mm<3>(ta, tb, tri, fused3, m, n, k, A, B, C, alpha, beta, s, info);
+    case 4: return dispatch_mm<4>(ta, tb, tri, fused3, m, n, k, A, B, C, alpha, beta, s, info);
+    default: return MFLAB_ERR_UNSUPPORTED;
+    }
+}
+
+}  // namespace mfl
+
+using mfl::Mat;
+
+extern "C" int mflab_gemm(mflab_handle *h, void *stream, int limbs, int route, int64_t m,
+                          int64_t n, int64_t k, const double *A, int64_t lda, int64_t lsa,
+                          const double *B, int64_t ldb, int64_t lsb, double *C, int64_t ldc,
+                          int64_t lsc, const double *alpha, const double *beta);
+
+extern "C" int mflab_gemm_ozaki_route(mflab_handle *h, void *stream, int limbs, int64_t m,
+                                      int64_t n, int64_t k, const double *A, int64_t lda,
+                                      int64_t lsa, const double *B, int64_t ldb, int64_t lsb,
+                                      double *C, int64_t ldc, int64_t lsc, const double *alpha,
+                                      const double *beta);
+
+extern "C" int mflab_gemm(mflab_handle *h, void *stream, int limbs, int route, int64_t m,
+                          int64_t n, int64_t k, const double *A, int64_t lda, int64_t lsa,
+                          const double *B, int64_t ldb, int64_t lsb, double *C, int64_t ldc,
+                          int64_t lsc, const double *alpha, const double *beta) {
+    if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
+    if (m < 0 || n < 0 || k < 0 || !alpha || !beta) return MFLAB_ERR_ARG;
+    if (m == 0 || n == 0) return MFLAB_OK;
+    if (lda < (m > 0 ? m : 1) || ldb < (k > 0 ? k : 1) || ldc < m) return MFLAB_ERR_ARG;
+    if (mfl::views_overlap(C, ldc, lsc, m, n, limbs, A, lda, lsa, m, k) ||
+        mfl::views_overlap(C, ldc, lsc, m, n, limbs, B, ldb, lsb, k, n))
+        return MFLAB_ERR_ALIAS;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (route == MFLAB_GEMM_OZAKI)
+        return mflab_gemm_ozaki_route(h, stream, limbs, m, n, k, A, lda, lsa, B, ldb, lsb, C, ldc,
+                                      lsc, alpha, beta);
+    if (route != MFLAB_GEMM_AUTO && route != MFLAB_GEMM_DIRECT) return MFLAB_ERR_ARG;
+    bool fused = (limbs == 3 && route == MFLAB_GEMM_AUTO);
+    return mfl::launch_mm(limbs, false, false, 0, fused, m, n, k, Mat{(double *)A, lda, lsa},
+                          Mat{(double *)B, ldb, lsb}, Mat{C, ldc, lsc}, alpha, beta, s);
+}
+
+extern "C" int mflab_syrk_lower(mflab_handle *h, void *stream, int limbs, int64_t n, int64_t k,
+                                const double *P, int64_t ldp, int64_t lsp, double *C, int64_t ldc,
+                                int64_t lsc, const double *alpha, const double *beta) {
+    if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
+    if (n < 0 || k < 0 || !alpha || !beta) return MFLAB_ERR_ARG;
+    if (n == 0) return MFLAB_OK;
+    if (ldp < (k > 0 ? k : 1) || ldc < n) return MFLAB_ERR_ARG;
+    if (mfl::views_overlap(C, ldc, lsc, n, n, limbs, P, ldp, lsp, k, n)) return MFLAB_ERR_ALIAS;
+    return mfl::launch_mm(limbs, true, false, 1, false, n, n, k, Mat{(double *)P, ldp, lsp},
+                          Mat{(double *)P, ldp, lsp}, Mat{C, ldc, lsc}, alpha, beta,
+                          (cudaStream_t)stream);
+}
+
+extern "C" int mflab_gemmt_lower(mflab_handle *h, void *stream, int limbs, int64_t n, int64_t k,
+                                 const double *A, int64_t lda, int64_t lsa, const double *B,
+                                 int64_t ldb, int64_t lsb, double *C, int64_t ldc, int64_t lsc,
+                                 const double *alpha, const double *beta) {
+    if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
+    if (n < 0 || k < 0 || !alpha || !beta) return MFLAB_ERR_ARG;
+    if (n == 0) return MFLAB_OK;
+    if (lda < n || ldb < n || ldc < n) return MFLAB_ERR_ARG;
+    if (mfl::views_overlap(C, ldc, lsc, n, n, limbs, A, lda, lsa, n, k) ||
+        mfl::views_overlap(C, ldc, lsc, n, n, limbs, B, ldb, lsb, n, k))
+        return MFLAB_ERR_ALIAS;
+    return mfl::launch_mm(limbs, false, true, 1, false, n, n, k, Mat{(double *)A, lda, lsa},
+                          Mat{(double *)B, ldb, lsb}, Mat{C, ldc, lsc}, alpha, beta,
+                          (cudaStream_t)stream);
+}

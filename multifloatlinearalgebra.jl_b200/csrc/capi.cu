@@ -1,0 +1,89 @@
+// Library-level C-ABI entry points: version, status strings, handles.
+#include <cstring>
+#include <string>
+
+#include "mflab_internal.h"
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+namespace mfl {
+int record_cuda_error(cudaError_t e, const char *where) {
+    if (e == cudaSuccess) return MFLAB_OK;
+    g_last_error = std::string(where) + ": " + cudaGetErrorString(e);
+    return MFLAB_ERR_CUDA;
+}
+}  // namespace mfl
+
+extern "C" int mflab_version(void) { return 10000 * 0 + 100 * 1 + 0; }
+
+extern "C" const char *mflab_status_string(int code) {
+    switch (code) {
+    case MFLAB_OK: return "ok";
+    case MFLAB_ERR_ARG: return "invalid argument or dimension mismatch";
+    case MFLAB_ERR_CUDA: return "CUDA runtime error";
+    case MFLAB_ERR_UNSUPPORTED: return "unsupported limb count or option";
+    case MFLAB_ERR_TIMEOUT: return "bounded device wait timed out";
+    case MFLAB_ERR_ALLOC: return "device memory reservation failed";
+    case MFLAB_ERR_ALIAS: return "output aliases an input";
+    default: return "unknown status";
+    }
+}
+
+extern "C" const char *mflab_last_error(void) { return g_last_error.c_str(); }
+
+extern "C" int mflab_create(mflab_handle **out, int device) {
+    if (!out) return MFLAB_ERR_ARG;
+    *out = nullptr;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) return mfl::record_cuda_error(e == cudaSuccess ? cudaErrorNoDevice : e, "mflab_create");
+    if (device < 0 || device >= count) return MFLAB_ERR_ARG;
+    e = cudaSetDevice(device);
+    if (e != cudaSuccess) return mfl::record_cuda_error(e, "mflab_create cudaSetDevice");
+    mflab_handle *h = new mflab_handle();
+    h->device = device;
+    h->scratch = nullptr;
+    h->scratch_bytes = 0;
+    h->dev_flags = nullptr;
+    e = cudaMalloc((void **)&h->dev_flags, 64 * sizeof(int));
+    if (e != cudaSuccess) {
+        delete h;
+        mfl::record_cuda_error(e, "mflab_create flags");
+        return MFLAB_ERR_ALLOC;
+    }
+    cudaMemset(h->dev_flags, 0, 64 * sizeof(int));
+    *out = h;
+    return MFLAB_OK;
+}
+
+extern "C" int mflab_destroy(mflab_handle *h) {
+    if (!h) return MFLAB_OK;
+    cudaSetDevice(h->device);
+    cudaDeviceSynchronize();
+    if (h->scratch) cudaFree(h->scratch);
+    if (h->dev_flags) cudaFree(h->dev_flags);
+    delete h;
+    return MFLAB_OK;
+}
+
+int mflab_reserve_scratch(mflab_handle *h, size_t bytes) {
+    if (bytes <= h->scratch_bytes) return MFLAB_OK;
+    if (h->scratch) {
+        cudaError_t e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) return mfl::record_cuda_error(e, "scratch sync");
+        cudaFree(h->scratch);
+        h->scratch = nullptr;
+        h->scratch_bytes = 0;
+    }
+    size_t want = bytes + bytes / 8;
+    cudaError_t e = cudaMalloc(&h->scratch, want);
+    if (e != cudaSuccess) {
+        mfl::record_cuda_error(e, "scratch cudaMalloc");
+        h->scratch = nullptr;
+        return MFLAB_ERR_ALLOC;
+    }
+    h->scratch_bytes = want;
+    return MFLAB_OK;
+}

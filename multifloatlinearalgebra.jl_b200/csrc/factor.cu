@@ -1,0 +1,496 @@
+// Blocked multi-double Cholesky and LU with solves and factor diagnostics.
+//
+// Cholesky follows src/factorizations/cholesky.jl:10-107 of
+// MultiFloatLinearAlgebra.jl: per block of `block` columns, a panel kernel
+// factors the diagonal block (rows inside the panel only), the rows below are
+// solved with trsm(side=right, lower, T) and the trailing lower triangle gets
+// -1 * (A21 A21^T) + 1 * A22 from the shared mainloop.  LU follows
+// src/factorizations/lu.jl:34-195: per panel column a pivot kernel (first
+// strictly larger |A[r,k]|, full-row swap, reciprocal scaling) and a rank-1
+// panel update, then trsm(left, lower, unit) on U12 and A22 = -A21 U12 + A22.
+// Every kernel reads the device `info` word first and exits if an earlier step
+// failed, so a whole factorization is enqueued without host synchronisation.
+#include "mf_device.cuh"
+#include "mflab_internal.h"
+
+namespace mfl {
+
+__global__ void iota1_kernel(int64_t *p, int64_t count) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) p[i] = i + 1;
+}
+
+// ------------------------------------------------------------- checks ----
+template <int N>
+__global__ void nonfinite_kernel(int64_t m, int64_t n, Mat A, int lower_only, int *info) {
+    int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= m * n) return;
+    int64_t r = idx % m, c = idx / m;
+    if (lower_only && r < c) return;
+    if (!isfinite_mf(load_mf<N>(A.p, A.ld, A.ls, r, c))) *info = -1;
+}
+
+// ------------------------------------------------------------ Cholesky ---
+// one warp; w <= 32 columns of the diagonal block starting at (f, f)
+template <int N>
+__global__ void potrf_panel_kernel(Mat A, int64_t f, int w, int *info) {
+    if (*info) return;
+    __shared__ double piv[N];
+    __shared__ int fail;
+    const int t = threadIdx.x;
+    if (t == 0) fail = 0;
+    __syncthreads();
+    for (int c = 0; c < w; ++c) {
+        const int64_t col = f + c;
+        if (t == 0) {
+            mf<N> d = load_mf<N>(A.p, A.ld, A.ls, col, col);
+            for (int64_t k = f; k < col; ++k) {
+                mf<N> v = load_mf<N>(A.p, A.ld, A.ls, col, k);
+                d = submul(d, v, v);
+            }
+            if (!gt(d, from_double<N>(0.0))) {
+                fail = 1;
+                *info = (int)(col + 1);
+            } else {
+                mf<N> p = sqrt_mf(d);
+                store_mf<N>(A.p, A.ld, A.ls, col, col, p);
+#pragma unroll
+                for (int l = 0; l < N; ++l) piv[l] = p.v[l];
+            }
+        }
+        __syncthreads();
+        if (fail) return;
+        mf<N> p;
+#pragma unroll
+        for (int l = 0; l < N; ++l) p.v[l] = piv[l];
+        const int64_t row = col + 1 + t;
+        if (t < w - 1 - c) {
+            mf<N> v = load_mf<N>(A.p, A.ld, A.ls, row, col);
+            for (int64_t k = f; k < col; ++k)
+                v = submul(v, load_mf<N>(A.p, A.ld, A.ls, row, k), load_mf<N>(A.p, A.ld, A.ls, col, k));
+            store_mf<N>(A.p, A.ld, A.ls, row, col, div(v, p));
+        }
+        __syncthreads();
+    }
+}
+
+template <int N>
+static int potrf_n(int64_t n, Mat A, int64_t block, int *info, cudaStream_t s) {
+    const double mone[4] = {-1.0, 0.0, 0.0, 0.0}, one[4] = {1.0, 0.0, 0.0, 0.0};
+    cudaError_t e = cudaMemsetAsync(info, 0, sizeof(int), s);
+    if (e != cudaSuccess) return record_cuda_error(e, "potrf info");
+    if (n == 0) return MFLAB_OK;
+    int64_t tot = n * n;
+    nonfinite_kernel<N><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(n, n, A, 1, info);
+    int rc = record_cuda_error(cudaGetLastError(), "potrf check");
+    if (rc) return rc;
+    for (int64_t first = 0; first < n; first += block) {
+        const int64_t last = first + block - 1 < n - 1 ? first + block - 1 : n - 1;
+        const int w = (int)(last - first + 1);
+        potrf_panel_kernel<N><<<1, 32, 0, s>>>(A, first, w, info);
+        rc = record_cuda_error(cudaGetLastError(), "potrf panel");
+        if (rc) return rc;
+        if (last < n - 1) {
+            const int64_t t = n - 1 - last;
+            rc = launch_trsm_info(N, 1, 0, 1, 0, t, w, A.at(first, first), A.at(last + 1, first), one,
+                                  s, info);
+            if (rc) return rc;
+            rc = launch_mm(N, false, true, 1, false, t, t, w, A.at(last + 1, first),
+                           A.at(last + 1, first), A.at(last + 1, last + 1), mone, one, s, info);
+            if (rc) return rc;
+        }
+    }
+    return MFLAB_OK;
+}
+
+// ------------------------------------------------------------------ LU ---
+// single CTA: pivot search in column k (rows k..m-1), full-row swap,
+// zero-pivot test, reciprocal and scaling of the column below the pivot
+template <int N, int NT>
+__global__ void __launch_bounds__(NT) lu_pivot_kernel(int64_t m, int64_t n, Mat A, int64_t k,
+                                                      int64_t *ipiv, int *info) {
+    if (*info) return;
+    __shared__ double sval[NT][N];
+    __shared__ int64_t sidx[NT];
+    __shared__ double sinv[N];
+    __shared__ int64_t spiv;
+    const int t = threadIdx.x;
+    // strided scan: first strictly larger |A[r,k]| in ascending r
+    mf<N> best = from_double<N>(-1.0);
+    int64_t bidx = -1;
+    for (int64_t r = k + t; r < m; r += NT) {
+        mf<N> cand = abs_mf(load_mf<N>(A.p, A.ld, A.ls, r, k));
+        if (bidx < 0 || gt(cand, best)) {
+            best = cand;
+            bidx = r;
+        }
+    }
+#pragma unroll
+    for (int l = 0; l < N; ++l) sval[t][l] = best.v[l];
+    sidx[t] = bidx;
+    __syncthreads();
+    for (int off = NT / 2; off > 0; off >>= 1) {
+        if (t < off) {
+            mf<N> a, b;
+#pragma unroll
+            for (int l = 0; l < N; ++l) {
+                a.v[l] = sval[t][l];
+                b.v[l] = sval[t + off][l];
+            }
+            int64_t ia = sidx[t], ib = sidx[t + off];
+            bool take_b;
+            if (ib < 0) take_b = false;
+            else if (ia < 0) take_b = true;
+            else if (gt(b, a)) take_b = true;
+            else if (gt(a, b)) take_b = false;
+            else take_b = ib < ia;
+            if (take_b) {
+#pragma unroll
+                for (int l = 0; l < N; ++l) sval[t][l] = b.v[l];
+                sidx[t] = ib;
+            }
+        }
+        __syncthreads();
+    }
+    if (t == 0) {
+        spiv = sidx[0];
+        ipiv[k] = sidx[0] + 1;
+    }
+    __syncthreads();
+    const int64_t p = spiv;
+    if (p != k) {
+        for (int64_t c = t; c < n; c += NT) {
+#pragma unroll
+            for (int l = 0; l < N; ++l) {
+                double *x = A.p + l * A.ls + c * A.ld;
+                double tmp = x[k];
+                x[k] = x[p];
+                x[p] = tmp;
+            }
+        }
+    }
+    __syncthreads();
+    if (t == 0) {
+        mf<N> akk = load_mf<N>(A.p, A.ld, A.ls, k, k);
+        if (iszero(akk)) {
+            *info = (int)(k + 1);
+        } else {
+            mf<N> iv = inv(akk);
+#pragma unroll
+            for (int l = 0; l < N; ++l) sinv[l] = iv.v[l];
+        }
+    }
+    __syncthreads();
+    if (*info) return;
+    mf<N> iv;
+#pragma unroll
+    for (int l = 0; l < N; ++l) iv.v[l] = sinv[l];
+    for (int64_t r = k + 1 + t; r < m; r += NT)
+        store_mf<N>(A.p, A.ld, A.ls, r, k, mul(load_mf<N>(A.p, A.ld, A.ls, r, k), iv));
+}
+
+// rank-1 update of panel columns k+1..last for rows k+1..m-1 (lu.jl:47-82)
+template <int N>
+__global__ void lu_rank1_kernel(int64_t m, Mat A, int64_t k, int64_t last, const int *info) {
+    if (*info) return;
+    const int64_t r = k + 1 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= m) return;
+    const mf<N> f = load_mf<N>(A.p, A.ld, A.ls, r, k);
+    for (int64_t c = k + 1; c <= last; ++c) {
+        mf<N> v = load_mf<N>(A.p, A.ld, A.ls, r, c);
+        store_mf<N>(A.p, A.ld, A.ls, r, c, submul(v, f, load_mf<N>(A.p, A.ld, A.ls, k, c)));
+    }
+}
+
+template <int N>
+static int getrf_n(int64_t m, int64_t n, Mat A, int64_t *ipiv, int64_t block, int *info,
+                   cudaStream_t s) {
+    const double mone[4] = {-1.0, 0.0, 0.0, 0.0}, one[4] = {1.0, 0.0, 0.0, 0.0};
+    cudaError_t e = cudaMemsetAsync(info, 0, sizeof(int), s);
+    if (e != cudaSuccess) return record_cuda_error(e, "getrf info");
+    const int64_t kmax = m < n ? m : n;
+    if (kmax == 0) return MFLAB_OK;
+    int64_t tot = m * n;
+    nonfinite_kernel<N><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(m, n, A, 0, info);
+    int rc = record_cuda_error(cudaGetLastError(), "getrf check");
+    if (rc) return rc;
+    for (int64_t first = 0; first < kmax; first += block) {
+        const int64_t last = first + block - 1 < kmax - 1 ? first + block - 1 : kmax - 1;
+        for (int64_t k = first; k <= last; ++k) {
+            lu_pivot_kernel<N, 512><<<1, 512, 0, s>>>(m, n, A, k, ipiv, info);
+            rc = record_cuda_error(cudaGetLastError(), "getrf pivot");
+            if (rc) return rc;
+            if (k < last && k + 1 < m) {
+                const int64_t rows = m - k - 1;
+                lu_rank1_kernel<N><<<(unsigned)((rows + 127) / 128), 128, 0, s>>>(m, A, k, last, info);
+                rc = record_cuda_error(cudaGetLastError(), "getrf rank1");
+                if (rc) return rc;
+            }
+        }
+        if (last < n - 1) {
+            const int64_t w = last - first + 1, rest = n - 1 - last;
+            rc = launch_trsm_info(N, 0, 0, 0, 1, w, rest, A.at(first, first), A.at(first, last + 1),
+                                  one, s, info);
+            if (rc) return rc;
+            if (last < m - 1) {
+                rc = launch_mm(N, false, false, 0, N == 3, m - 1 - last, rest, w, A.at(last + 1, first),
+                               A.at(first, last + 1), A.at(last + 1, last + 1), mone, one, s, info);
+                if (rc) return rc;
+            }
+        }
+    }
+    return MFLAB_OK;
+}
+
+// apply the recorded row interchanges to the right-hand sides (solve.jl:85-113);
+// one thread per column, interchanges in ascending k
+template <int N>
+__global__ void apply_pivots_kernel(int64_t nrhs, Mat B, const int64_t *ipiv, int64_t count,
+                                    int reverse) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nrhs) return;
+    for (int64_t s = 0; s < count; ++s) {
+        const int64_t k = reverse ? count - 1 - s : s;
+        const int64_t p = ipiv[k] - 1;
+        if (p != k) {
+#pragma unroll
+            for (int l = 0; l < N; ++l) {
+                double *x = B.p + l * B.ls + c * B.ld;
+                double tmp = x[k];
+                x[k] = x[p];
+                x[p] = tmp;
+            }
+        }
+    }
+}
+
+// --------------------------------------------------------- diagnostics ---
+// Partial reductions of max |A(r,c)| and finiteness over a region
+// (0 all, 1 lower r >= c, 2 upper r <= c): one record per CTA.
+template <int N, int NT>
+__global__ void __launch_bounds__(NT) maxabs_partial_kernel(int64_t m, int64_t n, Mat A,
+                                                            int region, double *part) {
+    __shared__ double sval[NT][N];
+    __shared__ int sfin[NT];
+    const int t = threadIdx.x;
+    mf<N> best = from_double<N>(0.0);
+    int fin = 1;
+    const int64_t tot = m * n;
+    for (int64_t idx = (int64_t)blockIdx.x * NT + t; idx < tot; idx += (int64_t)gridDim.x * NT) {
+        const int64_t r = idx % m, c = idx / m;
+        if (region == 1 && r < c) continue;
+        if (region == 2 && r > c) continue;
+        mf<N> v = load_mf<N>(A.p, A.ld, A.ls, r, c);
+        if (!isfinite_mf(v)) fin = 0;
+        best = max_mf(best, abs_mf(v));
+    }
+#pragma unroll
+    for (int l = 0; l < N; ++l) sval[t][l] = best.v[l];
+    sfin[t] = fin;
+    __syncthreads();
+    for (int off = NT / 2; off > 0; off >>= 1) {
+        if (t < off) {
+            mf<N> a, b;
+#pragma unroll
+            for (int l = 0; l < N; ++l) {
+                a.v[l] = sval[t][l];
+                b.v[l] = sval[t + off][l];
+            }
+            mf<N> r = max_mf(a, b);
+#pragma unroll
+            for (int l = 0; l < N; ++l) sval[t][l] = r.v[l];
+            sfin[t] = sfin[t] && sfin[t + off];
+        }
+        __syncthreads();
+    }
+    if (t == 0) {
+#pragma unroll
+        for (int l = 0; l < N; ++l) part[blockIdx.x * (N + 1) + l] = sval[0][l];
+        part[blockIdx.x * (N + 1) + N] = sfin[0] ? 1.0 : 0.0;
+    }
+}
+
+template <int N>
+__global__ void maxabs_final_kernel(int nparts, const double *part, double *out) {
+    mf<N> best = from_double<N>(0.0);
+    int fin = 1;
+    for (int i = 0; i < nparts; ++i) {
+        mf<N> v;
+#pragma unroll
+        for (int l = 0; l < N; ++l) v.v[l] = part[i * (N + 1) + l];
+        best = max_mf(best, v);
+        if (part[i * (N + 1) + N] == 0.0) fin = 0;
+    }
+#pragma unroll
+    for (int l = 0; l < N; ++l) out[l] = best.v[l];
+    out[N] = fin ? 1.0 : 0.0;
+}
+
+// O(n) tail of the diagnostics, one thread.  Layout of `out` (N doubles per
+// value): [0] min |diag|, [1] max |diag|, [2] max/min (Inf when min == 0),
+// [3] ratio num/den of the two given values (growth), [4] accepted count,
+// [5] has-range flag.  diagonal_magnitude_range over the first `count`
+// entries (diagnostics.jl:21-31).
+template <int N>
+__global__ void diag_tail_kernel(Mat A, int64_t count, const double *num, const double *den,
+                                 double *out) {
+    mf<N> mn = from_double<N>(0.0), mx = from_double<N>(0.0);
+    if (count > 0) {
+        mn = abs_mf(load_mf<N>(A.p, A.ld, A.ls, 0, 0));
+        mx = mn;
+        for (int64_t i = 1; i < count; ++i) {
+            mf<N> v = abs_mf(load_mf<N>(A.p, A.ld, A.ls, i, i));
+            mn = min_mf(mn, v);
+            mx = max_mf(mx, v);
+        }
+    }
+    mf<N> spread;
+    if (iszero(mn)) spread = from_double<N>(__longlong_as_double(0x7ff0000000000000LL));
+    else spread = div(mx, mn);
+    mf<N> ratio = from_double<N>(0.0);
+    if (num && den) {
+        mf<N> a, b;
+#pragma unroll
+        for (int l = 0; l < N; ++l) {
+            a.v[l] = num[l];
+            b.v[l] = den[l];
+        }
+        ratio = iszero(b) ? from_double<N>(0.0) : div(a, b);
+    }
+#pragma unroll
+    for (int l = 0; l < N; ++l) {
+        out[0 * N + l] = mn.v[l];
+        out[1 * N + l] = mx.v[l];
+        out[2 * N + l] = spread.v[l];
+        out[3 * N + l] = ratio.v[l];
+    }
+    out[4 * N] = (double)count;
+    out[4 * N + 1] = count > 0 ? 1.0 : 0.0;
+}
+
+template <int N>
+static int maxabs_n(int64_t m, int64_t n, Mat A, int region, double *part, int nparts,
+                    double *out, cudaStream_t s) {
+    maxabs_partial_kernel<N, 256><<<nparts, 256, 0, s>>>(m, n, A, region, part);
+    int rc = record_cuda_error(cudaGetLastError(), "maxabs partial");
+    if (rc) return rc;
+    maxabs_final_kernel<N><<<1, 1, 0, s>>>(nparts, part, out);
+    return record_cuda_error(cudaGetLastError(), "maxabs final");
+}
+
+}  // namespace mfl
+
+using mfl::Mat;
+
+#define MFL_DISPATCH(N, call)                                       \
+    switch (N) {                                                    \
+    case 2: return call<2>;                                         \
+    case 3: return call<3>;                                         \
+    case 4: return call<4>;                                         \
+    default: return MFLAB_ERR_UNSUPPORTED;                          \
+    }
+
+extern "C" int mflab_potrf(mflab_handle *h, void *stream, int limbs, int64_t n, double *A,
+                           int64_t lda, int64_t lsa, int64_t block, int *info) {
+    if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
+    if (n < 0 || (n > 0 && lda < n) || !info) return MFLAB_ERR_ARG;
+    if (block < 1) block = 1;
+    if (block > 32) return MFLAB_ERR_UNSUPPORTED;
+    Mat a{A, lda, lsa};
+    cudaStream_t s = (cudaStream_t)stream;
+    switch (limbs) {
+    case 2: return mfl::potrf_n<2>(n, a, block, info, s);
+    case 3: return mfl::potrf_n<3>(n, a, block, info, s);
+    default: return mfl::potrf_n<4>(n, a, block, info, s);
+    }
+}
+
+extern "C" int mflab_potrs(mflab_handle *h, void *stream, int limbs, int64_t n, int64_t nrhs,
+                           const double *L, int64_t ldl, int64_t lsl, double *B, int64_t ldb,
+                           int64_t lsb) {
+    if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
+    if (n < 0 || nrhs < 0 || (n > 0 && (ldl < n || ldb < n))) return MFLAB_ERR_ARG;
+    const double one[4] = {1.0, 0.0, 0.0, 0.0};
+    cudaStream_t s = (cudaStream_t)stream;
+    Mat a{(double *)L, ldl, lsl}, b{B, ldb, lsb};
+    int rc = mfl::launch_trsm(limbs, 0, 0, 0, 0, n, nrhs, a, b, one, s);
+    if (rc) return rc;
+    return mfl::launch_trsm(limbs, 0, 0, 1, 0, n, nrhs, a, b, one, s);
+}
+
+extern "C" int mflab_getrf(mflab_handle *h, void *stream, int limbs, int64_t m, int64_t n,
+                           double *A, int64_t lda, int64_t lsa, int64_t *ipiv, int64_t block,
+                           int *info) {
+    if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
+    if (m < 0 || n < 0 || (m > 0 && lda < m) || !info || (m > 0 && n > 0 && !ipiv))
+        return MFLAB_ERR_ARG;
+    if (block < 1) block = 1;
+    Mat a{A, lda, lsa};
+    cudaStream_t s = (cudaStream_t)stream;
+    const int64_t kmax = m < n ? m : n;
+    if (kmax > 0) {
+        // ipiv = 1:kmax, as the reference initialises it (lu.jl:16-28)
+        mfl::iota1_kernel<<<(unsigned)((kmax + 255) / 256), 256, 0, s>>>(ipiv, kmax);
+        int rc = mfl::record_cuda_error(cudaGetLastError(), "getrf ipiv");
+        if (rc) return rc;
+    }
+    switch (limbs) {
+    case 2: return mfl::getrf_n<2>(m, n, a, ipiv, block, info, s);
+    case 3: return mfl::getrf_n<3>(m, n, a, ipiv, block, info, s);
+    default: return mfl::getrf_n<4>(m, n, a, ipiv, block, info, s);
+    }
+}
+
+extern "C" int mflab_getrs(mflab_handle *h, void *stream, int limbs, int64_t n, int64_t nrhs,
+                           const double *LU, int64_t ldl, int64_t lsl, const int64_t *ipiv,
+                           double *B, int64_t ldb, int64_t lsb) {
+    if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
+    if (n < 0 || nrhs < 0 || (n > 0 && (ldl < n || ldb < n || !ipiv))) return MFLAB_ERR_ARG;
+    if (n == 0 || nrhs == 0) return MFLAB_OK;
+    const double one[4] = {1.0, 0.0, 0.0, 0.0};
+    cudaStream_t s = (cudaStream_t)stream;
+    Mat a{(double *)LU, ldl, lsl}, b{B, ldb, lsb};
+    unsigned g = (unsigned)((nrhs + 127) / 128);
+    switch (limbs) {
+    case 2: mfl::apply_pivots_kernel<2><<<g, 128, 0, s>>>(nrhs, b, ipiv, n, 0); break;
+    case 3: mfl::apply_pivots_kernel<3><<<g, 128, 0, s>>>(nrhs, b, ipiv, n, 0); break;
+    default: mfl::apply_pivots_kernel<4><<<g, 128, 0, s>>>(nrhs, b, ipiv, n, 0); break;
+    }
+    int rc = mfl::record_cuda_error(cudaGetLastError(), "getrs pivots");
+    if (rc) return rc;
+    rc = mfl::launch_trsm(limbs, 0, 0, 0, 1, n, nrhs, a, b, one, s);
+    if (rc) return rc;
+    return mfl::launch_trsm(limbs, 0, 1, 0, 0, n, nrhs, a, b, one, s);
+}
+
+extern "C" int mflab_max_abs(mflab_handle *h, void *stream, int limbs, int64_t m, int64_t n,
+                             const double *A, int64_t lda, int64_t lsa, int region, double *out) {
+    if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
+    if (m < 0 || n < 0 || region < 0 || region > 2 || !out) return MFLAB_ERR_ARG;
+    const int nparts = 296;
+    int rc = mflab_reserve_scratch(h, sizeof(double) * nparts * (limbs + 1));
+    if (rc) return rc;
+    double *part = (double *)h->scratch;
+    Mat a{(double *)A, lda, lsa};
+    cudaStream_t s = (cudaStream_t)stream;
+    switch (limbs) {
+    case 2: return mfl::maxabs_n<2>(m, n, a, region, part, nparts, out, s);
+    case 3: return mfl::maxabs_n<3>(m, n, a, region, part, nparts, out, s);
+    default: return mfl::maxabs_n<4>(m, n, a, region, part, nparts, out, s);
+    }
+}
+
+extern "C" int mflab_diag_summary(mflab_handle *h, void *stream, int limbs, const double *A,
+                                  int64_t lda, int64_t lsa, int64_t count, const double *num,
+                                  const double *den, double *out) {
+    if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
+    if (count < 0 || !out) return MFLAB_ERR_ARG;
+    Mat a{(double *)A, lda, lsa};
+    cudaStream_t s = (cudaStream_t)stream;
+    switch (limbs) {
+    case 2: mfl::diag_tail_kernel<2><<<1, 1, 0, s>>>(a, count, num, den, out); break;
+    case 3: mfl::diag_tail_kernel<3><<<1, 1, 0, s>>>(a, count, num, den, out); break;
+    default: mfl::diag_tail_kernel<4><<<1, 1, 0, s>>>(a, count, num, den, out); break;
+    }
+    return mfl::record_cuda_error(cudaGetLastError(), "diag summary");
+}

@@ -1,0 +1,82 @@
+// Internal declarations shared by the library's translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+
+#include "../../include/mflab200.h"
+
+namespace mfl {
+
+struct Mat {
+    double *p;
+    int64_t ld;  // column stride (elements)
+    int64_t ls;  // limb-plane stride (elements)
+    __host__ __device__ Mat at(int64_t r, int64_t c) const { return Mat{p + c * ld + r, ld, ls}; }
+};
+
+// Operand access of the shared multi-double mainloop.
+//   a(i,k) = ta ? A[k,i] : A[i,k];   b(k,j) = tb ? B[j,k] : B[k,j]
+// tri == 1 writes only C(i,j) with i >= j (SYRK / GEMMT lower triangle).
+int launch_mm(int N, bool ta, bool tb, int tri, bool fused3, int64_t m, int64_t n, int64_t k,
+              Mat A, Mat B, Mat C, const double *alpha, const double *beta, cudaStream_t s,
+              const int *info = nullptr);
+
+// Triangular solve (trsm.jl semantics); returns an MFLAB_* code.
+int launch_trsm(int N, int side, int uplo, int trans, int diag, int64_t m, int64_t n, Mat A, Mat B,
+                const double *alpha, cudaStream_t s);
+int launch_trsm_info(int N, int side, int uplo, int trans, int diag, int64_t m, int64_t n, Mat A,
+                     Mat B, const double *alpha, cudaStream_t s, const int *info);
+
+inline int cuda_status(cudaError_t e) {
+    if (e == cudaSuccess) return MFLAB_OK;
+    return MFLAB_ERR_CUDA;
+}
+
+int record_cuda_error(cudaError_t e, const char *where);
+
+inline bool valid_limbs(int N) { return N >= 2 && N <= 4; }
+
+// Whether two limb-plane views may share an element (Base.mightalias
+// semantics, types.jl:252-267).  Views with the same column and plane strides
+// are compared by their 2-D index ranges, so disjoint blocks of one matrix
+// (e.g. A21 and A22) do not alias; otherwise the address ranges decide.
+inline int64_t floor_div(int64_t a, int64_t b) {
+    int64_t q = a / b;
+    return (a % b != 0 && ((a < 0) != (b < 0))) ? q - 1 : q;
+}
+inline bool views_overlap(const double *a, int64_t ld_a, int64_t ls_a, int64_t rows_a,
+                          int64_t cols_a, int limbs, const double *b, int64_t ld_b, int64_t ls_b,
+                          int64_t rows_b, int64_t cols_b) {
+    if (rows_a <= 0 || cols_a <= 0 || rows_b <= 0 || cols_b <= 0) return false;
+    const double *a_end = a + (int64_t)(limbs - 1) * ls_a + (cols_a - 1) * ld_a + rows_a;
+    const double *b_end = b + (int64_t)(limbs - 1) * ls_b + (cols_b - 1) * ld_b + rows_b;
+    if (!(a < b_end && b < a_end)) return false;
+    if (ld_a != ld_b || ls_a != ls_b || ld_a <= 0) return true;
+    if (rows_a > ld_a || rows_b > ld_a) return true;
+    const int64_t off = b - a;
+    for (int l = -(limbs - 1); l <= limbs - 1; ++l) {
+        const int64_t o = off - (int64_t)l * ls_a;
+        const int64_t q = floor_div(o, ld_a), r = o - q * ld_a;
+        const int64_t reps[2][2] = {{r, q}, {r - ld_a, q + 1}};
+        for (auto &rep : reps) {
+            const bool rows = rep[0] < rows_a && 0 < rep[0] + rows_b;
+            const bool cols = rep[1] < cols_a && 0 < rep[1] + cols_b;
+            if (rows && cols) return true;
+        }
+    }
+    return false;
+}
+
+}  // namespace mfl
+
+struct mflab_handle {
+    int device;
+    // device scratch owned by the handle (grown on demand, freed by destroy)
+    void *scratch;
+    size_t scratch_bytes;
+    int *dev_flags;  // small device words: info, timeout flags
+};
+
+// grow the handle's scratch to at least `bytes`; returns MFLAB_OK or an error
+int mflab_reserve_scratch(mflab_handle *h, size_t bytes);

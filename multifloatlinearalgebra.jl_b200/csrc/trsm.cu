@@ -1,0 +1,202 @@
+// Multi-double triangular solves, src/kernels/trsm.jl:1-302 and trsv.jl:19-73
+// of MultiFloatLinearAlgebra.jl.
+//
+// Order contract: the reference computes, for every unknown,
+//     v = B[i]; for k in the substitution order: v -= coef(i,k) * X[k]; v /= A[i,i]
+// (left side; right side uses B[i,k] * coef(k,j)).  Each kernel below keeps that
+// exact per-element chain:
+//   * trsm_left_cta: one CTA per right-hand-side column.  The column's running
+//     values live in registers (rows distributed cyclically over the threads).
+//     Step k finalises X[k] (owner divides by the diagonal), broadcasts it
+//     through shared memory, and every later row applies its term k.  So each
+//     row receives its terms in the reference's ascending (or descending)
+//     order, while the rows progress in parallel.
+//   * trsm_left_thread: one thread per right-hand-side column, the plain
+//     serial loop (used when the triangle is short, e.g. LU's U12 block).
+//   * trsm_right_thread: one thread per row of B, the plain serial loop (the
+//     Cholesky panel solve A21 <- A21 / L11^T).
+#include "mf_device.cuh"
+#include "mflab_internal.h"
+
+namespace mfl {
+
+template <int N>
+__device__ __forceinline__ mf<N> tri_coef(const Mat &A, int64_t r, int64_t c, bool transposed) {
+    return transposed ? load_mf<N>(A.p, A.ld, A.ls, c, r) : load_mf<N>(A.p, A.ld, A.ls, r, c);
+}
+
+template <int N>
+__global__ void scale_kernel(int64_t m, int64_t n, Mat B, scal<N> alpha) {
+    int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= m * n) return;
+    int64_t r = idx % m, c = idx / m;
+    mf<N> v = load_mf<N>(B.p, B.ld, B.ls, r, c);
+    store_mf<N>(B.p, B.ld, B.ls, r, c, mul(v, alpha.get()));
+}
+
+// one CTA per column; NT threads; each thread owns up to MAXR rows
+template <int N, int NT, int MAXR>
+__global__ void __launch_bounds__(NT) trsm_left_cta(int64_t m, int64_t n, Mat A, Mat B,
+                                                    bool eff_lower, bool transposed, bool unit,
+                                                    const int *info) {
+    if (info && *info) return;
+    __shared__ double xs[2][N];
+    const int64_t col = blockIdx.x;
+    if (col >= n) return;
+    const int t = threadIdx.x;
+    mf<N> v[MAXR];
+#pragma unroll
+    for (int q = 0; q < MAXR; ++q) {
+        int64_t r = t + (int64_t)q * NT;
+        v[q] = r < m ? load_mf<N>(B.p, B.ld, B.ls, r, col) : from_double<N>(0.0);
+    }
+    for (int64_t s = 0; s < m; ++s) {
+        const int64_t k = eff_lower ? s : m - 1 - s;  // row finalised at this step
+        const int slot = (int)(s & 1);
+        if ((k % NT) == t) {
+            const int qk = (int)(k / NT);
+            mf<N> x;
+#pragma unroll
+            for (int q = 0; q < MAXR; ++q)
+                if (q == qk) x = v[q];
+            if (!unit) x = div(x, load_mf<N>(A.p, A.ld, A.ls, k, k));
+#pragma unroll
+            for (int q = 0; q < MAXR; ++q)
+                if (q == qk) v[q] = x;
+            store_mf<N>(B.p, B.ld, B.ls, k, col, x);
+#pragma unroll
+            for (int l = 0; l < N; ++l) xs[slot][l] = x.v[l];
+        }
+        __syncthreads();
+        mf<N> xk;
+#pragma unroll
+        for (int l = 0; l < N; ++l) xk.v[l] = xs[slot][l];
+#pragma unroll
+        for (int q = 0; q < MAXR; ++q) {
+            const int64_t r = t + (int64_t)q * NT;
+            const bool later = eff_lower ? (r > k) : (r < k);
+            if (r < m && later) v[q] = submul(v[q], tri_coef<N>(A, r, k, transposed), xk);
+        }
+    }
+}
+
+template <int N>
+__global__ void trsm_left_thread(int64_t m, int64_t n, Mat A, Mat B, bool eff_lower,
+                                 bool transposed, bool unit, const int *info) {
+    if (info && *info) return;
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    if (eff_lower) {
+        for (int64_t row = 0; row < m; ++row) {
+            mf<N> v = load_mf<N>(B.p, B.ld, B.ls, row, c);
+            for (int64_t k = 0; k < row; ++k)
+                v = submul(v, tri_coef<N>(A, row, k, transposed), load_mf<N>(B.p, B.ld, B.ls, k, c));
+            if (!unit) v = div(v, load_mf<N>(A.p, A.ld, A.ls, row, row));
+            store_mf<N>(B.p, B.ld, B.ls, row, c, v);
+        }
+    } else {
+        for (int64_t row = m - 1; row >= 0; --row) {
+            mf<N> v = load_mf<N>(B.p, B.ld, B.ls, row, c);
+            for (int64_t k = row + 1; k < m; ++k)
+                v = submul(v, tri_coef<N>(A, row, k, transposed), load_mf<N>(B.p, B.ld, B.ls, k, c));
+            if (!unit) v = div(v, load_mf<N>(A.p, A.ld, A.ls, row, row));
+            store_mf<N>(B.p, B.ld, B.ls, row, c, v);
+        }
+    }
+}
+
+template <int N>
+__global__ void trsm_right_thread(int64_t m, int64_t n, Mat A, Mat B, bool eff_lower,
+                                  bool transposed, bool unit, const int *info) {
+    if (info && *info) return;
+    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= m) return;
+    if (eff_lower) {
+        for (int64_t col = n - 1; col >= 0; --col) {
+            mf<N> v = load_mf<N>(B.p, B.ld, B.ls, r, col);
+            for (int64_t k = col + 1; k < n; ++k)
+                v = submul(v, load_mf<N>(B.p, B.ld, B.ls, r, k), tri_coef<N>(A, k, col, transposed));
+            if (!unit) v = div(v, load_mf<N>(A.p, A.ld, A.ls, col, col));
+            store_mf<N>(B.p, B.ld, B.ls, r, col, v);
+        }
+    } else {
+        for (int64_t col = 0; col < n; ++col) {
+            mf<N> v = load_mf<N>(B.p, B.ld, B.ls, r, col);
+            for (int64_t k = 0; k < col; ++k)
+                v = submul(v, load_mf<N>(B.p, B.ld, B.ls, r, k), tri_coef<N>(A, k, col, transposed));
+            if (!unit) v = div(v, load_mf<N>(A.p, A.ld, A.ls, col, col));
+            store_mf<N>(B.p, B.ld, B.ls, r, col, v);
+        }
+    }
+}
+
+template <int N>
+static int run_trsm(int side, int uplo, int trans, int diag, int64_t m, int64_t n, Mat A, Mat B,
+                    const double *alpha, cudaStream_t s, const int *info) {
+    if (m <= 0 || n <= 0) return MFLAB_OK;
+    bool one = alpha[0] == 1.0;
+    for (int l = 1; l < N; ++l) one = one && alpha[l] == 0.0;
+    if (!one) {
+        scal<N> al{};
+        for (int l = 0; l < N; ++l) al.v[l] = alpha[l];
+        int64_t tot = m * n;
+        scale_kernel<N><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(m, n, B, al);
+        int rc = record_cuda_error(cudaGetLastError(), "trsm scale");
+        if (rc) return rc;
+    }
+    const bool transposed = trans == 1;
+    const bool eff_lower = (uplo == 0) == !transposed;
+    const bool unit = diag == 1;
+    if (side == 1) {
+        trsm_right_thread<N><<<(unsigned)((m + 127) / 128), 128, 0, s>>>(m, n, A, B, eff_lower,
+                                                                         transposed, unit, info);
+        return record_cuda_error(cudaGetLastError(), "trsm right");
+    }
+    if (m <= 64 || n >= 4096) {
+        trsm_left_thread<N><<<(unsigned)((n + 127) / 128), 128, 0, s>>>(m, n, A, B, eff_lower,
+                                                                        transposed, unit, info);
+        return record_cuda_error(cudaGetLastError(), "trsm left thread");
+    }
+    if (n > 2147483647LL) return MFLAB_ERR_UNSUPPORTED;
+    if (m <= 256 * 8) {
+        trsm_left_cta<N, 256, 8><<<(unsigned)n, 256, 0, s>>>(m, n, A, B, eff_lower, transposed,
+                                                             unit, info);
+    } else if (m <= 256 * 16) {
+        trsm_left_cta<N, 256, 16><<<(unsigned)n, 256, 0, s>>>(m, n, A, B, eff_lower, transposed,
+                                                              unit, info);
+    } else {
+        trsm_left_thread<N><<<(unsigned)((n + 127) / 128), 128, 0, s>>>(m, n, A, B, eff_lower,
+                                                                        transposed, unit, info);
+    }
+    return record_cuda_error(cudaGetLastError(), "trsm left cta");
+}
+
+int launch_trsm_info(int N, int side, int uplo, int trans, int diag, int64_t m, int64_t n, Mat A,
+                     Mat B, const double *alpha, cudaStream_t s, const int *info) {
+    switch (N) {
+    case 2: return run_trsm<2>(side, uplo, trans, diag, m, n, A, B, alpha, s, info);
+    case 3: return run_trsm<3>(side, uplo, trans, diag, m, n, A, B, alpha, s, info);
+    case 4: return run_trsm<4>(side, uplo, trans, diag, m, n, A, B, alpha, s, info);
+    default: return MFLAB_ERR_UNSUPPORTED;
+    }
+}
+
+int launch_trsm(int N, int side, int uplo, int trans, int diag, int64_t m, int64_t n, Mat A, Mat B,
+                const double *alpha, cudaStream_t s) {
+    return launch_trsm_info(N, side, uplo, trans, diag, m, n, A, B, alpha, s, nullptr);
+}
+
+}  // namespace mfl
+
+extern "C" int mflab_trsm(mflab_handle *h, void *stream, int limbs, int side, int uplo, int trans,
+                          int diag, int64_t m, int64_t n, const double *A, int64_t lda,
+                          int64_t lsa, double *B, int64_t ldb, int64_t lsb, const double *alpha) {
+    if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
+    if (side < 0 || side > 1 || uplo < 0 || uplo > 1 || trans < 0 || trans > 1 || diag < 0 ||
+        diag > 1 || m < 0 || n < 0 || !alpha)
+        return MFLAB_ERR_ARG;
+    const int64_t na = side == 0 ? m : n;
+    if ((na > 0 && lda < na) || (m > 0 && ldb < m)) return MFLAB_ERR_ARG;
+    return mfl::launch_trsm(limbs, side, uplo, trans, diag, m, n, mfl::Mat{(double *)A, lda, lsa},
+                            mfl::Mat{B, ldb, lsb}, alpha, (cudaStream_t)stream);
+}

@@ -1,0 +1,76 @@
+"""Seeded synthetic multi-double workloads (the benchmark shapes).
+
+All generators return limb-major arrays (N, m, n) or device MFMatrix objects
+whose values are renormalised with exact FastTwoSum passes, so every input
+satisfies the MultiFloats normalisation assumption
+(docs/MULACC_X3_PROOF_CONTRACT.md:31-33 of the reference).
+
+Lower limbs follow the workload description: limb l = randn * 2^-53 * |limb
+l-1|, a fully populated low part.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+
+def _renorm_np(X: np.ndarray) -> np.ndarray:
+    N = X.shape[0]
+    for _ in range(2):
+        for lvl in range(N - 1, 0, -1):
+            s = X[lvl - 1] + X[lvl]
+            e = X[lvl] - (s - X[lvl - 1])
+            X[lvl - 1], X[lvl] = s, e
+    return X
+
+
+def randn_mf(rng: np.random.Generator, N: int, m: int, n: int, spread: float = 0.0,
+             scale: float = 1.0) -> np.ndarray:
+    """limb0 ~ N(0,1) * 2^U(-spread, spread); lower limbs as described above."""
+    X = np.zeros((N, m, n))
+    X[0] = rng.standard_normal((m, n)) * scale
+    if spread:
+        X[0] *= np.exp2(rng.uniform(-spread, spread, (m, n)))
+    for lvl in range(1, N):
+        X[lvl] = rng.standard_normal((m, n)) * 2.0 ** -53 * np.abs(X[lvl - 1])
+    return _renorm_np(X)
+
+
+def _renorm_torch(X: torch.Tensor) -> torch.Tensor:
+    N = X.shape[0]
+    for _ in range(2):
+        for lvl in range(N - 1, 0, -1):
+            a, b = X[lvl - 1].clone(), X[lvl].clone()
+            s = a + b
+            e = b - (s - a)
+            X[lvl - 1], X[lvl] = s, e
+    return X
+
+
+def randn_mf_device(seed: int, N: int, m: int, n: int, spread: float = 0.0,
+                    device: int = 0) -> torch.Tensor:
+    """Device-generated (N, n, m) limb planes (column-major) of the same
+    distribution as randn_mf; used for benchmark-size inputs."""
+    g = torch.Generator(device=f"cuda:{device}")
+    g.manual_seed(seed)
+    X = torch.empty((N, n, m), dtype=torch.float64, device=f"cuda:{device}")
+    X[0].normal_(generator=g)
+    if spread:
+        u = torch.empty((n, m), dtype=torch.float64, device=f"cuda:{device}")
+        u.uniform_(-spread, spread, generator=g)
+        X[0] *= torch.exp2(u)
+        del u
+    for lvl in range(1, N):
+        X[lvl].normal_(generator=g)
+        X[lvl] *= 2.0 ** -53
+        X[lvl] *= X[lvl - 1].abs()
+    return _renorm_torch(X)
+
+
+def spd_matrix(rng: np.random.Generator, N: int, n: int, gemm) -> np.ndarray:
+    """S = R R^T + n I with R randn multi-double (config 2 / config 5 shape).
+    `gemm` computes the multi-double product (oracle or device)."""
+    R = randn_mf(rng, N, n, n)
+    S = gemm(R, np.ascontiguousarray(R.transpose(0, 2, 1)))
+    S[0] += n * np.eye(n)
+    return _renorm_np(S)

@@ -1,0 +1,40 @@
+"""The C-ABI library loads and exports every symbol include/*.h declares
+(no compute calls: runs without a GPU)."""
+import ctypes
+
+import pytest
+
+
+def test_library_exports_declared_symbols(mf):
+    lib = mf._native.load()
+    names = mf._native.declared_symbols()
+    assert len(names) >= 10
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_version_and_status_strings(mf):
+    lib = mf._native.load()
+    assert lib.mflab_version() >= 100
+    assert lib.mflab_status_string(0) == b"ok"
+    assert b"argument" in lib.mflab_status_string(-1)
+
+
+def test_binding_covers_header(mf):
+    """every declared entry point has a ctypes signature in the binding"""
+    assert set(mf._native.declared_symbols()) <= set(mf._native.SIGNATURES)
+
+
+def test_gemm_plan_routes(mf):
+    assert mf.gemm_plan(3, 8, 8, 8)["strategy"] == "fused"
+    assert mf.gemm_plan(2, 8, 8, 8)["strategy"] == "direct"
+    with pytest.raises(mf.ArgumentError):
+        mf.gemm_plan(2, 8, 8, 8, mf.KernelConfig(gemm_strategy="fused"))
+    with pytest.raises(mf.ArgumentError):
+        mf.gemm_plan(2, 8, 8, 8, mf.KernelConfig(gemm_strategy="bogus"))
+
+
+def test_capabilities(mf):
+    c = mf.capabilities(2)
+    assert c["supported"] and c["limb_count"] == 2 and c["syrk_authoritative_triangle"] == "lower"
+    assert not mf.capabilities(7)["supported"]
