@@ -1,0 +1,374 @@
+"""Benchmark: Float64xN GEMM at m = n = k = 8192 on B200.
+
+One step is one C = A*B over the full synthetic n = 8192 workload (entries
+randn * 2^U(-20,20), lower limbs randn * 2^-53 * |previous limb|; seeded).
+The headline path is the INT8-slice (Ozaki) tensor-core GEMM for Float64x2;
+the plain FP64 matched-order kernel is timed beside it, with the componentwise
+error of both against the exact superaccumulator oracle on sampled entries.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl mflab|reference]
+
+Multi-GPU (torchrun): every rank multiplies its own independent n = 8192
+problem (weak scaling, no data-path collective); the time is the max over
+ranks.  Prints one JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "Float64x2/x4 GEMM GFLOP/s at n=8192, INT8-slice vs plain FP64, equal oracle error"
+UNIT = "multi-double GFLOP/s (2mnk/t)"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="mflab", choices=["mflab", "reference"])
+    p.add_argument("--n", type=int, default=8192)
+    p.add_argument("--limbs", type=int, default=2)
+    p.add_argument("--route", default="auto", help="headline route: auto (ozaki if built), plain, ozaki")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+# ------------------------------------------------------------- clocks ----
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------ helpers ----
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def fp64_peak(mf, torch) -> float:
+    """Measured FP64 pipe instruction rate (instr/s), DFMA probe, burst."""
+    lib = mf._native.load()
+    dev = torch.cuda.current_device()
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    out = torch.empty(sms * 4 * 256, dtype=torch.float64, device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+    ins = C.c_double()
+    best = 0.0
+    for it in (2000, 20000, 20000):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        rc = lib.mflab_probe_fp64(s, 0, sms * 4, 256, it, out.data_ptr(), C.byref(ins))
+        e1.record()
+        torch.cuda.synchronize()
+        assert rc == 0
+        best = max(best, ins.value / (e0.elapsed_time(e1) / 1e3))
+    return best
+
+
+def read_traffic(kernel_key: str):
+    """dram bytes per launch from the committed ncu summary, if present."""
+    p = os.path.join(REPO, "profiles", "ncu_traffic.txt")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("#") or "=" not in line:
+            continue
+        kv = dict(x.split("=", 1) for x in line.split())
+        if kv.get("key") == kernel_key:
+            return float(kv["dram_bytes_per_launch"])
+    return None
+
+
+def ops_per_term(N: int) -> int:
+    """FP64 instructions of one acc + a*b in the matched networks
+    (x2: 8 mul + 20 add; x3 fused: 99; x4: 103 mul + 124 add)."""
+    return {2: 28, 3: 99, 4: 227}[N]
+
+
+def cpu_sample(mfref, N, n, threads, target_s=15.0):
+    """Time the oracle GEMM on a column sample of the same workload."""
+    import numpy as np
+    rng = np.random.default_rng(11)
+    from importlib import import_module
+    syn = import_module("mflab200.synthetic")
+    A = syn.randn_mf(rng, N, n, n, spread=20)
+    cols = 8
+    B = syn.randn_mf(rng, N, n, cols, spread=20)
+    t0 = time.perf_counter()
+    mfref.gemm(A, B, nthreads=threads)
+    dt = time.perf_counter() - t0
+    # grow the sample to ~target_s of CPU work
+    cols2 = int(min(n, max(cols, cols * target_s / max(dt, 1e-3) * 0.5)))
+    if cols2 > cols:
+        B = syn.randn_mf(rng, N, n, cols2, spread=20)
+        t0 = time.perf_counter()
+        mfref.gemm(A, B, nthreads=threads)
+        dt = time.perf_counter() - t0
+        cols = cols2
+    gf = 2.0 * n * n * cols / dt / 1e9
+    return gf, f"C[:, :{cols}] of the n={n} x{N} GEMM (k={n}), {threads} threads, {dt:.1f} s"
+
+
+# -------------------------------------------------------- reference arm --
+def run_reference(args):
+    world, rank, _ = dist_setup(args)
+    if rank != 0:
+        return
+    from oracle import mfref
+    import __graft_entry__
+    __graft_entry__.load_package()
+    threads = mfref.threads()
+    vals = []
+    sample = ""
+    for step in range(args.warmup + args.steps):
+        v, sample = cpu_sample(mfref, args.limbs, args.n, threads, target_s=6.0)
+        if step >= args.warmup:
+            vals.append(v)
+    v = statistics.median(vals)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded randn * 2^U(-20,20))",
+        "config": {"workload": f"Float64x{args.limbs} GEMM m=n=k={args.n}", "limbs": args.limbs,
+                   "n": args.n, "parallelism": f"replicas{world}"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "Julia and MultiFloats.jl are not available here: the reference arm times the "
+                "oracle's C++ restatement of the reference GEMM loop order (4-row SIMD x 2-column "
+                "micro-tile, column panels over all host threads).",
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------- main arm ----
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    import __graft_entry__
+    mf = __graft_entry__.load_package()
+    from importlib import import_module
+    syn = import_module("mflab200.synthetic")
+    lib = mf._native.load()
+
+    N, n = args.limbs, args.n
+    route = args.route
+    have_ozaki = mf.ozaki_available() if hasattr(mf, "ozaki_available") else False
+    if route == "auto":
+        route = "ozaki" if have_ozaki else "plain"
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    A = mf.MFMatrix.from_tensor(syn.randn_mf_device(1000 + rank, N, n, n, spread=20))
+    B = mf.MFMatrix.from_tensor(syn.randn_mf_device(2000 + rank, N, n, n, spread=20))
+    Cm = mf.MFMatrix.zeros(N, n, n)
+    stream = torch.cuda.current_stream()
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            fn()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        barrier()
+        t = e0.elapsed_time(e1) / 1e3
+        if world > 1:
+            tt = torch.tensor([t], device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t = float(tt.item())
+        return t
+
+    plain_cfg = mf.KernelConfig(gemm_strategy="auto")
+    oz_cfg = mf.KernelConfig(gemm_strategy="ozaki")
+    flops = 2.0 * n * n * n
+
+    clocks = ClockSampler(local)
+    results = {}
+    # headline route first, timed with clock sampling
+    head_cfg = oz_cfg if route == "ozaki" else plain_cfg
+    head_fn = lambda: mf.gemm_(Cm, A, B, config=head_cfg)
+    clocks.start()
+    t_head = timed(head_fn, args.steps, args.warmup)
+    clk = clocks.stop()
+    results["head"] = t_head / args.steps
+    # the other route (plain always reported)
+    if route == "ozaki":
+        t_plain = timed(lambda: mf.gemm_(Cm, A, B, config=plain_cfg), 1, 1)
+        results["plain"] = t_plain
+    else:
+        results["plain"] = results["head"]
+
+    # accuracy of both routes against the exact oracle on sampled entries
+    acc = {}
+    if rank == 0:
+        from oracle import mfref
+        rs = np.random.default_rng(5)
+        rows = rs.integers(0, n, 256)
+        cols = rs.integers(0, n, 256)
+        An = A.to_numpy()
+        Bn = B.to_numpy()
+        for name, cfg in (("plain", plain_cfg), ("ozaki", oz_cfg)):
+            if name == "ozaki" and not have_ozaki:
+                continue
+            mf.gemm_(Cm, A, B, config=cfg)
+            err, scale = _check_entries(mfref, An, Bn, Cm, rows, cols)
+            acc[name] = float(np.max(err / scale))
+        del An, Bn
+
+    # end to end through the public API with host buffers
+    hA = torch.empty((N, n, n), dtype=torch.float64, pin_memory=True)
+    hB = torch.empty((N, n, n), dtype=torch.float64, pin_memory=True)
+    hC = torch.empty((N, n, n), dtype=torch.float64, pin_memory=True)
+    hA.copy_(A.storage)
+    hB.copy_(B.storage)
+    dA, dB = torch.empty_like(A.storage), torch.empty_like(B.storage)
+    dC = torch.empty_like(Cm.storage)
+
+    def e2e_step():
+        dA.copy_(hA, non_blocking=True)
+        dB.copy_(hB, non_blocking=True)
+        mf.gemm_(mf.MFMatrix.from_tensor(dC), mf.MFMatrix.from_tensor(dA),
+                 mf.MFMatrix.from_tensor(dB), config=head_cfg)
+        hC.copy_(dC, non_blocking=True)
+
+    t_e2e = timed(e2e_step, max(1, args.steps // 2), 1) / max(1, args.steps // 2)
+
+    # roofline of the dominant kernel (plain: FP64 pipe; ozaki: INT8 tensor)
+    peak_fp64 = fp64_peak(mf, torch)
+    if route == "ozaki":
+        roof = mf.ozaki_roofline(N, n, results["head"])
+    else:
+        instr = float(n) ** 3 * ops_per_term(N)
+        achieved = instr / results["head"] / 1e12
+        roof = {"bound": "fp64", "achieved": achieved, "peak": peak_fp64 / 1e12,
+                "unit": "T FP64 instr/s", "frac": achieved / (peak_fp64 / 1e12),
+                "traffic": read_traffic(f"mm_x{N}_n{n}"),
+                "peak_source": "measured in this run (DFMA probe, burst)"}
+
+    value = world * flops / results["head"] / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": results["head"] * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded randn * 2^U(-20,20), lower limbs randn*2^-53*|prev|)",
+        "config": {"workload": f"Float64x{N} GEMM m=n=k={n}", "limbs": N, "n": n,
+                   "route": route, "parallelism": f"replicas{world}",
+                   "l2": "inputs larger than L2 (each operand >= 1 GiB)"},
+        "plain_fp64": {"value": world * flops / results["plain"] / 1e9,
+                       "ms_per_step": results["plain"] * 1e3,
+                       "max_rel_err": acc.get("plain")},
+        "e2e": {"value": world * flops / t_e2e / 1e9, "unit": UNIT,
+                "h2d_bytes_per_step": 2 * N * n * n * 8, "d2h_bytes_per_step": N * n * n * 8},
+        "roofline": roof,
+        "clocks": clk,
+        "gpu_launches": args.steps * (mf.gemm_launches(N, n, head_cfg)
+                                      if hasattr(mf, "gemm_launches") else 1),
+        "fp64_peak_instr_per_s": peak_fp64,
+    }
+    if route == "ozaki":
+        line["ozaki"] = {"max_rel_err": acc.get("ozaki"), "speedup_vs_plain":
+                         results["plain"] / results["head"]}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import mfref
+        threads = mfref.threads()
+        v, sample = cpu_sample(mfref, N, n, threads)
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": sample}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def _check_entries(mfref, An, Bn, Cm, rows, cols):
+    """exact check of entries (rows[j], cols[j]) of the device result"""
+    import numpy as np
+    Cs = Cm.planes()[:, cols, :].cpu().numpy()  # (N, s, m): column cols[j] at index j
+    N = An.shape[0]
+    s = len(rows)
+    # build an N x m x s matrix whose column j is C[:, cols[j]] and check (rows[j], j)
+    Csub = np.ascontiguousarray(Cs.transpose(0, 2, 1))
+    Bsub = np.ascontiguousarray(Bn[:, :, cols])
+    return mfref.exact_gemm_check(An, Bsub, Csub, rows, np.arange(s))[:2]
+
+
+if __name__ == "__main__":
+    main()

@@ -193,11 +193,14 @@ class MFMatrix:
 
     @property
     def ld(self) -> int:
-        return self.storage.stride(1)
+        st = self.storage
+        # torch reports an arbitrary stride for a size-1 dimension
+        return st.stride(1) if st.shape[1] > 1 else max(st.shape[2], 1)
 
     @property
     def ls(self) -> int:
-        return self.storage.stride(0)
+        st = self.storage
+        return st.stride(0) if st.shape[0] > 1 else st.shape[1] * max(st.shape[2], 1)
 
     @property
     def device(self) -> int:

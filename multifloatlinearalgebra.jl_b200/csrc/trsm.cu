@@ -5,12 +5,12 @@
 //     v = B[i]; for k in the substitution order: v -= coef(i,k) * X[k]; v /= A[i,i]
 // (left side; right side uses B[i,k] * coef(k,j)).  Each kernel below keeps that
 // exact per-element chain:
-//   * trsm_left_cta: one CTA per right-hand-side column.  The column's running
-//     values live in registers (rows distributed cyclically over the threads).
-//     Step k finalises X[k] (owner divides by the diagonal), broadcasts it
-//     through shared memory, and every later row applies its term k.  So each
-//     row receives its terms in the reference's ascending (or descending)
-//     order, while the rows progress in parallel.
+//   * trsm_left_cta: forward substitution, one CTA per right-hand-side column.
+//     The column's running values live in registers (rows distributed
+//     cyclically over the threads).  Step k finalises X[k] (owner divides by
+//     the diagonal), broadcasts it through shared memory, and every later row
+//     applies its term k.  Each row thus receives its terms in the reference's
+//     ascending order while the rows progress in parallel.
 //   * trsm_left_thread: one thread per right-hand-side column, the plain
 //     serial loop (used when the triangle is short, e.g. LU's U12 block).
 //   * trsm_right_thread: one thread per row of B, the plain serial loop (the
@@ -152,7 +152,13 @@ static int run_trsm(int side, int uplo, int trans, int diag, int64_t m, int64_t 
                                                                          transposed, unit, info);
         return record_cuda_error(cudaGetLastError(), "trsm right");
     }
-    if (m <= 64 || n >= 4096) {
+    // The wavefront kernel applies row r's terms as the unknowns are finalised.
+    // That is the reference's ascending-k chain only for forward substitution
+    // (effective lower): in backward substitution the reference's chain for
+    // row r starts with X[r+1], the last unknown finalised before X[r], so each
+    // row's chain is inherently serial after its predecessor and the plain
+    // per-column loop is used.
+    if (m <= 64 || n >= 4096 || !eff_lower) {
         trsm_left_thread<N><<<(unsigned)((n + 127) / 128), 128, 0, s>>>(m, n, A, B, eff_lower,
                                                                         transposed, unit, info);
         return record_cuda_error(cudaGetLastError(), "trsm left thread");
