@@ -147,27 +147,29 @@ def ops_per_term(N: int) -> int:
 
 
 def cpu_sample(mfref, N, n, threads, target_s=15.0):
-    """Time the oracle GEMM on a column sample of the same workload."""
+    """Time the oracle GEMM on a row sample of the same workload: C[:r, :] =
+    A[:r, :] * B with the full k = n reduction, r chosen for ~target_s of CPU
+    work.  All column panels run in parallel over `threads` host threads."""
     import numpy as np
-    rng = np.random.default_rng(11)
     from importlib import import_module
     syn = import_module("mflab200.synthetic")
-    A = syn.randn_mf(rng, N, n, n, spread=20)
-    cols = 8
-    B = syn.randn_mf(rng, N, n, cols, spread=20)
+    rng = np.random.default_rng(11)
+    B = syn.randn_mf(rng, N, n, n, spread=20)
+    r = 4
+    A = syn.randn_mf(rng, N, r, n, spread=20)
     t0 = time.perf_counter()
     mfref.gemm(A, B, nthreads=threads)
     dt = time.perf_counter() - t0
-    # grow the sample to ~target_s of CPU work
-    cols2 = int(min(n, max(cols, cols * target_s / max(dt, 1e-3) * 0.5)))
-    if cols2 > cols:
-        B = syn.randn_mf(rng, N, n, cols2, spread=20)
+    r2 = int(min(n, max(r, r * target_s / max(dt, 1e-3))))
+    if r2 > r:
+        r = r2
+        A = syn.randn_mf(rng, N, r, n, spread=20)
         t0 = time.perf_counter()
         mfref.gemm(A, B, nthreads=threads)
         dt = time.perf_counter() - t0
-        cols = cols2
-    gf = 2.0 * n * n * cols / dt / 1e9
-    return gf, f"C[:, :{cols}] of the n={n} x{N} GEMM (k={n}), {threads} threads, {dt:.1f} s"
+    gf = 2.0 * r * n * n / dt / 1e9
+    return gf, (f"C[:{r}, :] of the n={n} x{N} GEMM (k={n}) on {threads} host threads, "
+                f"{dt:.1f} s")
 
 
 # -------------------------------------------------------- reference arm --

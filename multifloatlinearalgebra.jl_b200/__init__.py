@@ -174,7 +174,7 @@ class MFMatrix:
             raise ArgumentError("MFMatrix storage must be a (N, ncols, ld) float64 tensor")
         if not storage.is_cuda:
             raise ArgumentError("MFMatrix storage must live on a CUDA device")
-        if storage.stride(2) != 1:
+        if storage.shape[2] > 1 and storage.stride(2) != 1:
             raise ArgumentError("limb planes must be column-major (unit row stride)")
         self.storage = storage
         self.r0, self.c0 = r0, c0
