@@ -345,10 +345,24 @@ def gemm_(C_: MFMatrix, A: MFMatrix, B: MFMatrix, alpha=1.0, beta=0.0,
     plan = gemm_plan(N, m, k, n, config)
     route = _ROUTES[plan["strategy"]]
     lib, h, s = _lib_h(C_)
-    rc = lib.mflab_gemm(h, s, N, route, m, n, k, A.ptr(), A.ld, A.ls, B.ptr(), B.ld, B.ls,
-                        C_.ptr(), C_.ld, C_.ls, _scalar(N, alpha), _scalar(N, beta))
+    if route == 2:
+        rc = lib.mflab_gemm_ozaki(h, s, N, int(config.ozaki_slices), m, n, k, A.ptr(), A.ld, A.ls,
+                                  B.ptr(), B.ld, B.ls, C_.ptr(), C_.ld, C_.ls, _scalar(N, alpha),
+                                  _scalar(N, beta))
+    else:
+        rc = lib.mflab_gemm(h, s, N, route, m, n, k, A.ptr(), A.ld, A.ls, B.ptr(), B.ld, B.ls,
+                            C_.ptr(), C_.ld, C_.ls, _scalar(N, alpha), _scalar(N, beta))
     _check(rc, "gemm!")
     return C_
+
+
+def ozaki_default_slices(N: int, k: int) -> int:
+    """Digit slices per operand of the INT8 route when KernelConfig.ozaki_slices == 0."""
+    return int(_native.load().mflab_ozaki_default_slices(N, k))
+
+
+def ozaki_available() -> bool:
+    return hasattr(_native.load(), "mflab_gemm_ozaki")
 
 
 def syrk_(C_: MFMatrix, P: MFMatrix, alpha=1.0, beta=0.0, uplo: str = "lower",

@@ -73,6 +73,9 @@ SIGNATURES = {
     "mflab_max_abs": [_vp, _vp, _int, _i64, _i64, _vp, _i64, _i64, _int, _vp],
     "mflab_diag_summary": [_vp, _vp, _int, _vp, _i64, _i64, _i64, _vp, _vp, _vp],
     "mflab_probe_fp64": [_vp, _int, _int, _int, _i64, _vp, _d],
+    "mflab_gemm_ozaki": [_vp, _vp, _int, _int, _i64, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _i64,
+                         _vp, _i64, _i64, _d, _d],
+    "mflab_ozaki_default_slices": [_int, _i64],
 }
 _RESTYPE = {"mflab_status_string": C.c_char_p, "mflab_last_error": C.c_char_p}
 

@@ -1,0 +1,348 @@
+// INT8-slice (Ozaki scheme I) multi-double GEMM on the tensor cores.
+//
+// No reference counterpart: MultiFloatLinearAlgebra.jl has only the FP64
+// networks.  Published method: Ozaki, Ogita, Oishi, Rump (2012), error-free
+// transformation of matrix products; Ootomo, Ozaki, Yokota (2024), DGEMM on
+// integer matrix multiplication units.
+//
+// 1. Scaling.  Row i of A gets the power of two 2^Ea_i with |A(i,:)| < 2^(Ea_i-1),
+//    column j of B gets 2^Eb_j likewise (leading-limb maxima, frexp).
+// 2. Exact digit split.  Each scaled multi-double x in (-1/2, 1/2) is written
+//    as sum_{s=1..S} d_s 2^(-7 s) + r with signed digits d_s = rint(128 * r_{s-1})
+//    in [-64, 64]; the running remainder is kept exact by limb-wise
+//    subtraction and a TwoSum re-distillation of the limbs after each digit.
+// 3. Level products.  Digits are stored A8[i][s][k] and B8[j][S-1-s][k]
+//    (B's slice order reversed), so for a significance level L = s + t
+//    (s, t >= 1, L <= S+1) every pair (s, L-s) is adjacent along K:
+//        I_L = A8[:, 0:(L-1)k] * B8[:, (S-L+1)k : S k]^T      (int8 x int8 -> int32)
+//    is ONE integer GEMM with K = (L-1) k, exact as long as
+//    (L-1) k 65^2 < 2^31.
+// 4. Accumulation.  C(i,j) = 2^(Ea_i + Eb_j) sum_L 2^(-7L) I_L(i,j): the S int32
+//    levels are added, least significant first, into a Float64xN accumulator
+//    with the add network, scaled by the power of two, and the alpha/beta
+//    epilogue of the plain kernel is applied.
+// The truncation (digit remainders and levels above S+1) bounds the error by
+// about k 2^(Ea+Eb) 2^(-7S); the slice count S is the accuracy knob.
+#include <cublasLt.h>
+
+#include <climits>
+#include <cmath>
+
+#include "mf_device.cuh"
+#include "mflab_internal.h"
+
+namespace mfl {
+
+constexpr int OZ_EXP_EMPTY = INT_MIN / 2;   // a row/column with no nonzero entry
+constexpr int OZ_EXP_BAD = INT_MAX;         // a row/column holding a non-finite entry
+
+__device__ __forceinline__ int exp_of(double a) {
+    int e;
+    frexp(a, &e);
+    return e;
+}
+
+// row maxima of A (m x k, column-major planes): grid (ceil(m/256), kchunks)
+template <int N>
+__global__ void oz_row_exp_kernel(int64_t m, int64_t k, Mat A, int64_t kchunk, int *rowexp) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    const int64_t k0 = (int64_t)blockIdx.y * kchunk;
+    const int64_t k1 = k0 + kchunk < k ? k0 + kchunk : k;
+    double mx = 0.0;
+    bool bad = false;
+    for (int64_t kk = k0; kk < k1; ++kk) {
+        const double *p = A.p + kk * A.ld + i;
+#pragma unroll
+        for (int l = 0; l < N; ++l) bad |= !isfinite(p[l * A.ls]);
+        mx = fmax(mx, fabs(p[0]));
+    }
+    int e = bad ? OZ_EXP_BAD : (mx > 0.0 ? exp_of(mx) : OZ_EXP_EMPTY);
+    atomicMax(&rowexp[i], e);
+}
+
+// column maxima of B (k x n): one warp per column
+template <int N>
+__global__ void oz_col_exp_kernel(int64_t k, int64_t n, Mat B, int *colexp) {
+    const int64_t j = (int64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+    const int lane = threadIdx.x % 32;
+    if (j >= n) return;
+    double mx = 0.0;
+    int bad = 0;
+    for (int64_t kk = lane; kk < k; kk += 32) {
+        const double *p = B.p + j * B.ld + kk;
+#pragma unroll
+        for (int l = 0; l < N; ++l) bad |= !isfinite(p[l * B.ls]);
+        mx = fmax(mx, fabs(p[0]));
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+        bad |= __shfl_xor_sync(0xffffffffu, bad, off);
+    }
+    if (lane == 0) colexp[j] = bad ? OZ_EXP_BAD : (mx > 0.0 ? exp_of(mx) : OZ_EXP_EMPTY);
+}
+
+__device__ __forceinline__ int oz_scale_exp(int e) {
+    // |x| < 2^e  ->  scaled by 2^-(e+1) lies in (-1/2, 1/2)
+    return (e == OZ_EXP_EMPTY || e == OZ_EXP_BAD) ? 0 : e + 1;
+}
+
+// digits of one scaled value; emit(s, d) is called for s = 0..S-1
+template <int N, typename Emit>
+__device__ __forceinline__ void oz_digits(mf<N> x, int S, Emit emit) {
+    for (int s = 0; s < S; ++s) {
+#pragma unroll
+        for (int l = 0; l < N; ++l) x.v[l] = __dmul_rn(x.v[l], 128.0);
+        const double d = rint(x.v[0]);
+        x.v[0] = __dsub_rn(x.v[0], d);  // exact: |x0| < 2^52
+        // re-distill so that x.v[0] carries the value of the remainder
+#pragma unroll
+        for (int l = N - 1; l > 0; --l) two_sum(x.v[l - 1], x.v[l], x.v[l - 1], x.v[l]);
+        emit(s, (int)d);
+    }
+}
+
+// A digits: 32 x 32 tile (rows x k) per block of 32 x 8 threads, transposed
+// through shared memory so that both the plane reads (along rows) and the
+// int8 writes (along k) are coalesced.
+template <int N>
+__global__ void __launch_bounds__(256) oz_split_a_kernel(int64_t m, int64_t k, int64_t kp, int S,
+                                                         Mat A, const int *rowexp, int8_t *A8) {
+    __shared__ double t[N][32][33];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int64_t i0 = (int64_t)blockIdx.x * 32, k0 = (int64_t)blockIdx.y * 32;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int kk = ty + 8 * j;
+        const int64_t i = i0 + tx, kg = k0 + kk;
+        const bool ok = i < m && kg < k;
+#pragma unroll
+        for (int l = 0; l < N; ++l) t[l][kk][tx] = ok ? A.p[l * A.ls + kg * A.ld + i] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int ii = ty + 8 * j;
+        const int64_t i = i0 + ii, kg = k0 + tx;
+        if (i >= m || kg >= kp) continue;
+        const int e = rowexp[i];
+        const int sh = oz_scale_exp(e);
+        mf<N> x;
+#pragma unroll
+        for (int l = 0; l < N; ++l) x.v[l] = (e == OZ_EXP_BAD) ? 0.0 : ldexp(t[l][tx][ii], -sh);
+        int8_t *dst = A8 + (size_t)i * S * kp + kg;
+        oz_digits<N>(x, S, [&](int s, int d) { dst[(size_t)s * kp] = (int8_t)d; });
+    }
+}
+
+// B digits: column j of B is contiguous along k; slice order reversed
+template <int N>
+__global__ void oz_split_b_kernel(int64_t k, int64_t n, int64_t kp, int S, Mat B,
+                                  const int *colexp, int8_t *B8) {
+    const int64_t kg = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t j = blockIdx.y;
+    if (kg >= kp || j >= n) return;
+    const int e = colexp[j];
+    const int sh = oz_scale_exp(e);
+    mf<N> x;
+#pragma unroll
+    for (int l = 0; l < N; ++l)
+        x.v[l] = (kg < k && e != OZ_EXP_BAD) ? ldexp(B.p[l * B.ls + j * B.ld + kg], -sh) : 0.0;
+    int8_t *dst = B8 + (size_t)j * S * kp + kg;
+    oz_digits<N>(x, S, [&](int s, int d) { dst[(size_t)(S - 1 - s) * kp] = (int8_t)d; });
+}
+
+// C = alpha * 2^(Ea+Eb) sum_L 2^(-7L) I_L (+ beta * C)
+template <int N>
+__global__ void oz_accum_kernel(int64_t m, int64_t n, int S, const int32_t *I, int64_t ldi,
+                                size_t plane, const int *rowexp, const int *colexp, Mat C,
+                                scal<N> alpha, scal<N> beta, int overwrite) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t j = blockIdx.y;
+    if (i >= m || j >= n) return;
+    const int ea = rowexp[i], eb = colexp[j];
+    mf<N> acc = from_double<N>(0.0);
+    if (ea == OZ_EXP_BAD || eb == OZ_EXP_BAD) {
+        acc = from_double<N>(__longlong_as_double(0x7ff8000000000000LL));
+    } else {
+        for (int L = S + 1; L >= 2; --L) {
+            const double v = (double)I[(size_t)(L - 2) * plane + (size_t)j * ldi + i];
+            acc = add(acc, from_double<N>(ldexp(v, 7 * (S + 1 - L))));
+        }
+        const int sh = oz_scale_exp(ea) + oz_scale_exp(eb) - 7 * (S + 1);
+#pragma unroll
+        for (int l = 0; l < N; ++l) acc.v[l] = ldexp(acc.v[l], sh);
+    }
+    mf<N> r = mul(alpha.get(), acc);
+    if (!overwrite) r = add(r, mul(beta.get(), load_mf<N>(C.p, C.ld, C.ls, i, j)));
+    store_mf<N>(C.p, C.ld, C.ls, i, j, r);
+}
+
+// ----------------------------------------------------------- host side ---
+struct OzPlan {
+    int S;
+    int64_t kp;     // k rounded up to 16 (int8 rows 16-byte aligned; zero digits pad)
+    int64_t ldi;    // leading dimension of an int32 level plane (m rounded up to 16)
+    size_t plane;   // elements between level planes (multiple of 64)
+    size_t a8, b8, lev, exps, ws, total;
+};
+
+static OzPlan oz_plan(int64_t m, int64_t n, int64_t k, int S) {
+    OzPlan p;
+    p.S = S;
+    p.kp = (k + 15) / 16 * 16;
+    p.ldi = (m + 15) / 16 * 16;
+    p.plane = ((size_t)p.ldi * n + 63) / 64 * 64;
+    auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+    p.a8 = al((size_t)m * S * p.kp);
+    p.b8 = al((size_t)n * S * p.kp);
+    p.lev = al((size_t)S * p.plane * sizeof(int32_t));
+    p.exps = al((size_t)(m + n) * sizeof(int));
+    p.ws = (size_t)64 << 20;
+    p.total = p.a8 + p.b8 + p.lev + p.exps + p.ws;
+    return p;
+}
+
+static cublasLtHandle_t lt_handle() {
+    static cublasLtHandle_t h = nullptr;
+    if (!h) cublasLtCreate(&h);
+    return h;
+}
+
+// I = Aop^T * Bop with int8 operands stored K-major (ld = lda / ldb bytes)
+static int int8_gemm_tn(int64_t m, int64_t n, int64_t K, const int8_t *A, int64_t lda,
+                        const int8_t *B, int64_t ldb, int32_t *I, int64_t ldi, void *ws, size_t wsb,
+                        cudaStream_t s) {
+    cublasLtHandle_t h = lt_handle();
+    if (!h) return MFLAB_ERR_CUDA;
+    cublasLtMatmulDesc_t op = nullptr;
+    cublasLtMatrixLayout_t Ad = nullptr, Bd = nullptr, Cd = nullptr;
+    cublasLtMatmulPreference_t pref = nullptr;
+    int rc = MFLAB_OK;
+    cublasOperation_t ta = CUBLAS_OP_T, tb = CUBLAS_OP_N;
+    cublasLtMatmulHeuristicResult_t res{};
+    int nres = 0;
+    int32_t one = 1, zero = 0;
+    if (cublasLtMatmulDescCreate(&op, CUBLAS_COMPUTE_32I, CUDA_R_32I) != CUBLAS_STATUS_SUCCESS ||
+        cublasLtMatmulDescSetAttribute(op, CUBLASLT_MATMUL_DESC_TRANSA, &ta, sizeof(ta)) ||
+        cublasLtMatmulDescSetAttribute(op, CUBLASLT_MATMUL_DESC_TRANSB, &tb, sizeof(tb)) ||
+        cublasLtMatrixLayoutCreate(&Ad, CUDA_R_8I, K, m, lda) ||
+        cublasLtMatrixLayoutCreate(&Bd, CUDA_R_8I, K, n, ldb) ||
+        cublasLtMatrixLayoutCreate(&Cd, CUDA_R_32I, m, n, ldi) ||
+        cublasLtMatmulPreferenceCreate(&pref) ||
+        cublasLtMatmulPreferenceSetAttribute(pref, CUBLASLT_MATMUL_PREF_MAX_WORKSPACE_BYTES, &wsb,
+                                             sizeof(wsb)) ||
+        cublasLtMatmulAlgoGetHeuristic(h, op, Ad, Bd, Cd, Cd, pref, 1, &res, &nres) ||
+        nres == 0) {
+        rc = MFLAB_ERR_UNSUPPORTED;
+    } else if (cublasLtMatmul(h, op, &one, A, Ad, B, Bd, &zero, I, Cd, I, Cd, &res.algo, ws, wsb,
+                              s) != CUBLAS_STATUS_SUCCESS) {
+        rc = MFLAB_ERR_CUDA;
+    }
+    if (pref) cublasLtMatmulPreferenceDestroy(pref);
+    if (Cd) cublasLtMatrixLayoutDestroy(Cd);
+    if (Bd) cublasLtMatrixLayoutDestroy(Bd);
+    if (Ad) cublasLtMatrixLayoutDestroy(Ad);
+    if (op) cublasLtMatmulDescDestroy(op);
+    return rc;
+}
+
+template <int N>
+static int ozaki_n(int64_t m, int64_t n, int64_t k, Mat A, Mat B, Mat C, const double *alpha,
+                   const double *beta, int S, char *base, const OzPlan &p, cudaStream_t s) {
+    int8_t *A8 = (int8_t *)base;
+    int8_t *B8 = (int8_t *)(base + p.a8);
+    int32_t *I = (int32_t *)(base + p.a8 + p.b8);
+    int *rowexp = (int *)(base + p.a8 + p.b8 + p.lev);
+    int *colexp = rowexp + m;
+    void *ws = base + p.a8 + p.b8 + p.lev + p.exps;
+    cudaError_t e = cudaMemsetAsync(rowexp, 0x80, sizeof(int) * m, s);  // 0x80808080 < any exponent
+    if (e != cudaSuccess) return record_cuda_error(e, "ozaki exps");
+    const int64_t kchunk = 512;
+    dim3 gr((unsigned)((m + 255) / 256), (unsigned)((k + kchunk - 1) / kchunk));
+    oz_row_exp_kernel<N><<<gr, 256, 0, s>>>(m, k, A, kchunk, rowexp);
+    oz_col_exp_kernel<N><<<(unsigned)((n + 7) / 8), 256, 0, s>>>(k, n, B, colexp);
+    dim3 ga((unsigned)((m + 31) / 32), (unsigned)((p.kp + 31) / 32));
+    oz_split_a_kernel<N><<<ga, dim3(32, 8), 0, s>>>(m, k, p.kp, S, A, rowexp, A8);
+    dim3 gb((unsigned)((p.kp + 255) / 256), (unsigned)n);
+    oz_split_b_kernel<N><<<gb, 256, 0, s>>>(k, n, p.kp, S, B, colexp, B8);
+    int rc = record_cuda_error(cudaGetLastError(), "ozaki split");
+    if (rc) return rc;
+    const int64_t ld8 = (int64_t)S * p.kp;
+    for (int L = 2; L <= S + 1; ++L) {
+        rc = int8_gemm_tn(m, n, (int64_t)(L - 1) * p.kp, A8, ld8, B8 + (int64_t)(S - L + 1) * p.kp,
+                          ld8, I + (size_t)(L - 2) * p.plane, p.ldi, ws, p.ws, s);
+        if (rc) return rc;
+    }
+    scal<N> al{}, be{};
+    int overwrite = 1;
+    for (int l = 0; l < N; ++l) {
+        al.v[l] = alpha[l];
+        be.v[l] = beta[l];
+        if (beta[l] != 0.0) overwrite = 0;
+    }
+    dim3 gc((unsigned)((m + 127) / 128), (unsigned)n);
+    oz_accum_kernel<N><<<gc, 128, 0, s>>>(m, n, S, I, p.ldi, p.plane, rowexp, colexp, C, al, be,
+                                          overwrite);
+    return record_cuda_error(cudaGetLastError(), "ozaki accumulate");
+}
+
+// default slice count: enough digits for N limbs, the reduction length and a
+// 2^24 margin for the ratio between the row/column scale and sum |a||b|
+int ozaki_default_slices(int N, int64_t k) {
+    int lk = 0;
+    while ((1LL << lk) < k) ++lk;
+    return (53 * N + 1 + lk + 24 + 6) / 7;
+}
+
+int ozaki_gemm(mflab_handle *h, int N, int S, int64_t m, int64_t n, int64_t k, Mat A, Mat B,
+               Mat C, const double *alpha, const double *beta, cudaStream_t s) {
+    if (S < 1 || S > 64) return MFLAB_ERR_ARG;
+    const OzPlan p = oz_plan(m, n, k, S);
+    // exactness of every int32 level sum: (L-1) kp 65^2 < 2^31 for L <= S+1
+    if ((double)S * (double)p.kp * 65.0 * 65.0 >= 2147483647.0) return MFLAB_ERR_UNSUPPORTED;
+    if ((int64_t)n > 65535 * 1LL || m > INT_MAX) return MFLAB_ERR_UNSUPPORTED;
+    int rc = mflab_reserve_scratch(h, p.total);
+    if (rc) return rc;
+    char *base = (char *)h->scratch;
+    switch (N) {
+    case 2: return ozaki_n<2>(m, n, k, A, B, C, alpha, beta, S, base, p, s);
+    case 3: return ozaki_n<3>(m, n, k, A, B, C, alpha, beta, S, base, p, s);
+    case 4: return ozaki_n<4>(m, n, k, A, B, C, alpha, beta, S, base, p, s);
+    default: return MFLAB_ERR_UNSUPPORTED;
+    }
+}
+
+}  // namespace mfl
+
+extern "C" int mflab_gemm_ozaki_route(mflab_handle *h, void *stream, int limbs, int64_t m,
+                                      int64_t n, int64_t k, const double *A, int64_t lda,
+                                      int64_t lsa, const double *B, int64_t ldb, int64_t lsb,
+                                      double *C, int64_t ldc, int64_t lsc, const double *alpha,
+                                      const double *beta) {
+    return mfl::ozaki_gemm(h, limbs, mfl::ozaki_default_slices(limbs, k), m, n, k,
+                           mfl::Mat{(double *)A, lda, lsa}, mfl::Mat{(double *)B, ldb, lsb},
+                           mfl::Mat{C, ldc, lsc}, alpha, beta, (cudaStream_t)stream);
+}
+
+extern "C" int mflab_gemm_ozaki(mflab_handle *h, void *stream, int limbs, int slices, int64_t m,
+                                int64_t n, int64_t k, const double *A, int64_t lda, int64_t lsa,
+                                const double *B, int64_t ldb, int64_t lsb, double *C, int64_t ldc,
+                                int64_t lsc, const double *alpha, const double *beta) {
+    if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
+    if (m < 0 || n < 0 || k < 0 || !alpha || !beta) return MFLAB_ERR_ARG;
+    if (m == 0 || n == 0) return MFLAB_OK;
+    if (lda < (m > 0 ? m : 1) || ldb < (k > 0 ? k : 1) || ldc < m) return MFLAB_ERR_ARG;
+    if (mfl::views_overlap(C, ldc, lsc, m, n, limbs, A, lda, lsa, m, k) ||
+        mfl::views_overlap(C, ldc, lsc, m, n, limbs, B, ldb, lsb, k, n))
+        return MFLAB_ERR_ALIAS;
+    if (slices <= 0) slices = mfl::ozaki_default_slices(limbs, k);
+    return mfl::ozaki_gemm(h, limbs, slices, m, n, k, mfl::Mat{(double *)A, lda, lsa},
+                           mfl::Mat{(double *)B, ldb, lsb}, mfl::Mat{C, ldc, lsc}, alpha, beta,
+                           (cudaStream_t)stream);
+}
+
+extern "C" int mflab_ozaki_default_slices(int limbs, int64_t k) {
+    return mfl::ozaki_default_slices(limbs, k);
+}
