@@ -73,9 +73,10 @@ int mflab_gemm(mflab_handle *h, void *stream, int limbs, int route, int64_t m, i
 
 /* C = alpha*A*B + beta*C on the INT8 tensor cores (Ozaki scheme: exact
    signed 7-bit digit slices, int8 x int8 -> int32 level products, Float64xN
-   accumulation).  slices = digit count S per operand (0: the default for
-   limbs and k); the error is about k * 2^(row scale + column scale) * 2^(-7S).
-   Requires S * roundup(k, 16) * 65^2 < 2^31.  Uses handle scratch of about
+   accumulation).  slices = digit count S per operand; 0 lets the slice tuner
+   choose S from the scale gap of 2048 sampled entries (one stream
+   synchronisation).  The error is about k * 2^(row scale + column scale) *
+   2^(-7S).  S is capped so that S * roundup(k, 16) * 65^2 < 2^31.  Uses handle scratch of about
    S*(m+n)*k bytes + 4*S*m*n bytes.  Non-finite input rows/columns give NaN.
    No reference counterpart: the gemm_strategy=:ozaki route of gemm!
    (src/kernels/gemm.jl:747-774 keeps the reference's signature). */
@@ -84,9 +85,13 @@ int mflab_gemm_ozaki(mflab_handle *h, void *stream, int limbs, int slices, int64
                      int64_t ldb, int64_t lsb, double *C, int64_t ldc, int64_t lsc,
                      const double *alpha, const double *beta);
 
-/* default digit count of mflab_gemm_ozaki for `limbs` and reduction length k
-   (no reference counterpart). */
+/* data-independent digit count for `limbs` and reduction length k (a 24-bit
+   scale-gap allowance; no reference counterpart). */
 int mflab_ozaki_default_slices(int limbs, int64_t k);
+
+/* slice count used by the last INT8-slice GEMM on this handle (no reference
+   counterpart). */
+int mflab_ozaki_last_slices(mflab_handle *h);
 
 /* lower(C) = alpha * P^T * P + beta * lower(C); P is k x n, C n x n.  The
    strict upper triangle of C is neither read nor written.

@@ -361,6 +361,12 @@ def ozaki_default_slices(N: int, k: int) -> int:
     return int(_native.load().mflab_ozaki_default_slices(N, k))
 
 
+def ozaki_last_slices(device: Optional[int] = None) -> int:
+    """Slice count chosen by the last INT8-slice GEMM issued from this thread."""
+    dev = torch.cuda.current_device() if device is None else device
+    return int(_native.load().mflab_ozaki_last_slices(_handle(dev)))
+
+
 def ozaki_available() -> bool:
     return hasattr(_native.load(), "mflab_gemm_ozaki")
 

@@ -76,6 +76,7 @@ SIGNATURES = {
     "mflab_gemm_ozaki": [_vp, _vp, _int, _int, _i64, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _i64,
                          _vp, _i64, _i64, _d, _d],
     "mflab_ozaki_default_slices": [_int, _i64],
+    "mflab_ozaki_last_slices": [_vp],
 }
 _RESTYPE = {"mflab_status_string": C.c_char_p, "mflab_last_error": C.c_char_p}
 

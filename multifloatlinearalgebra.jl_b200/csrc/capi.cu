@@ -47,6 +47,9 @@ extern "C" int mflab_create(mflab_handle **out, int device) {
     h->scratch = nullptr;
     h->scratch_bytes = 0;
     h->dev_flags = nullptr;
+    h->aux = nullptr;
+    h->aux_bytes = 0;
+    h->last_slices = 0;
     e = cudaMalloc((void **)&h->dev_flags, 64 * sizeof(int));
     if (e != cudaSuccess) {
         delete h;
@@ -63,6 +66,7 @@ extern "C" int mflab_destroy(mflab_handle *h) {
     cudaSetDevice(h->device);
     cudaDeviceSynchronize();
     if (h->scratch) cudaFree(h->scratch);
+    if (h->aux) cudaFree(h->aux);
     if (h->dev_flags) cudaFree(h->dev_flags);
     delete h;
     return MFLAB_OK;
@@ -85,5 +89,25 @@ int mflab_reserve_scratch(mflab_handle *h, size_t bytes) {
         return MFLAB_ERR_ALLOC;
     }
     h->scratch_bytes = want;
+    return MFLAB_OK;
+}
+
+int mflab_reserve_aux(mflab_handle *h, size_t bytes) {
+    if (bytes <= h->aux_bytes) return MFLAB_OK;
+    if (h->aux) {
+        cudaError_t e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) return mfl::record_cuda_error(e, "aux sync");
+        cudaFree(h->aux);
+        h->aux = nullptr;
+        h->aux_bytes = 0;
+    }
+    size_t want = bytes + bytes / 4 + 4096;
+    cudaError_t e = cudaMalloc(&h->aux, want);
+    if (e != cudaSuccess) {
+        mfl::record_cuda_error(e, "aux cudaMalloc");
+        h->aux = nullptr;
+        return MFLAB_ERR_ALLOC;
+    }
+    h->aux_bytes = want;
     return MFLAB_OK;
 }

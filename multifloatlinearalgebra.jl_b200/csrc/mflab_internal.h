@@ -76,7 +76,14 @@ struct mflab_handle {
     void *scratch;
     size_t scratch_bytes;
     int *dev_flags;  // small device words: info, timeout flags
+    // second, independent scratch for small per-call metadata that must
+    // survive a growth of `scratch` (e.g. Ozaki row/column exponents)
+    void *aux;
+    size_t aux_bytes;
+    int last_slices;  // slice count the last Ozaki call used
 };
+
+int mflab_reserve_aux(mflab_handle *h, size_t bytes);
 
 // grow the handle's scratch to at least `bytes`; returns MFLAB_OK or an error
 int mflab_reserve_scratch(mflab_handle *h, size_t bytes);

@@ -179,6 +179,34 @@ __global__ void oz_accum_kernel(int64_t m, int64_t n, int S, const int32_t *I, i
     store_mf<N>(C.p, C.ld, C.ls, i, j, r);
 }
 
+// Sampled scale gap for the slice-count tuner: for sampled entries (i, j),
+// g = log2(k 2^(Ea'_i + Eb'_j) / sum_k |a_ik| |b_kj|) (leading limbs, binary64),
+// the number of bits between the truncation scale of the digit products and
+// the entry's own magnitude scale.  One warp per sample; the maximum over
+// samples is kept in eighths of a bit (atomicMax).
+__global__ void oz_gap_kernel(int64_t m, int64_t n, int64_t k, Mat A, Mat B, const int *rowexp,
+                              const int *colexp, int samples, int *gap8) {
+    const int s = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+    const int lane = threadIdx.x % 32;
+    if (s >= samples) return;
+    // deterministic spread of the samples over the matrix (64-bit LCG)
+    unsigned long long h = 6364136223846793005ULL * (unsigned long long)(s + 1) + 1442695040888963407ULL;
+    const int64_t i = (int64_t)((h >> 17) % (unsigned long long)m);
+    h = 6364136223846793005ULL * h + 1442695040888963407ULL;
+    const int64_t j = (int64_t)((h >> 17) % (unsigned long long)n);
+    const int ea = rowexp[i], eb = colexp[j];
+    if (ea == OZ_EXP_BAD || eb == OZ_EXP_BAD || ea == OZ_EXP_EMPTY || eb == OZ_EXP_EMPTY) return;
+    double d = 0.0;
+    for (int64_t kk = lane; kk < k; kk += 32)
+        d = fma(fabs(A.p[kk * A.ld + i]), fabs(B.p[j * B.ld + kk]), d);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) d += __shfl_xor_sync(0xffffffffu, d, off);
+    if (lane == 0 && d > 0.0) {
+        const double g = log2((double)k) + (double)(oz_scale_exp(ea) + oz_scale_exp(eb)) - log2(d);
+        atomicMax(gap8, (int)ceil(8.0 * g));
+    }
+}
+
 // ----------------------------------------------------------- host side ---
 struct OzPlan {
     int S;
@@ -249,20 +277,25 @@ static int int8_gemm_tn(int64_t m, int64_t n, int64_t K, const int8_t *A, int64_
 }
 
 template <int N>
-static int ozaki_n(int64_t m, int64_t n, int64_t k, Mat A, Mat B, Mat C, const double *alpha,
-                   const double *beta, int S, char *base, const OzPlan &p, cudaStream_t s) {
-    int8_t *A8 = (int8_t *)base;
-    int8_t *B8 = (int8_t *)(base + p.a8);
-    int32_t *I = (int32_t *)(base + p.a8 + p.b8);
-    int *rowexp = (int *)(base + p.a8 + p.b8 + p.lev);
-    int *colexp = rowexp + m;
-    void *ws = base + p.a8 + p.b8 + p.lev + p.exps;
+static int oz_exponents(int64_t m, int64_t n, int64_t k, Mat A, Mat B, int *rowexp, int *colexp,
+                        cudaStream_t s) {
     cudaError_t e = cudaMemsetAsync(rowexp, 0x80, sizeof(int) * m, s);  // 0x80808080 < any exponent
     if (e != cudaSuccess) return record_cuda_error(e, "ozaki exps");
     const int64_t kchunk = 512;
     dim3 gr((unsigned)((m + 255) / 256), (unsigned)((k + kchunk - 1) / kchunk));
     oz_row_exp_kernel<N><<<gr, 256, 0, s>>>(m, k, A, kchunk, rowexp);
     oz_col_exp_kernel<N><<<(unsigned)((n + 7) / 8), 256, 0, s>>>(k, n, B, colexp);
+    return record_cuda_error(cudaGetLastError(), "ozaki exponents");
+}
+
+template <int N>
+static int ozaki_n(int64_t m, int64_t n, int64_t k, Mat A, Mat B, Mat C, const double *alpha,
+                   const double *beta, int S, char *base, const OzPlan &p, const int *rowexp,
+                   const int *colexp, cudaStream_t s) {
+    int8_t *A8 = (int8_t *)base;
+    int8_t *B8 = (int8_t *)(base + p.a8);
+    int32_t *I = (int32_t *)(base + p.a8 + p.b8);
+    void *ws = base + p.a8 + p.b8 + p.lev + p.exps;
     dim3 ga((unsigned)((m + 31) / 32), (unsigned)((p.kp + 31) / 32));
     oz_split_a_kernel<N><<<ga, dim3(32, 8), 0, s>>>(m, k, p.kp, S, A, rowexp, A8);
     dim3 gb((unsigned)((p.kp + 255) / 256), (unsigned)n);
@@ -288,29 +321,73 @@ static int ozaki_n(int64_t m, int64_t n, int64_t k, Mat A, Mat B, Mat C, const d
     return record_cuda_error(cudaGetLastError(), "ozaki accumulate");
 }
 
-// default slice count: enough digits for N limbs, the reduction length and a
-// 2^24 margin for the ratio between the row/column scale and sum |a||b|
+// data-independent slice count: N limbs, the reduction length and a 2^24
+// margin for the ratio between the row/column scales and sum |a||b|
 int ozaki_default_slices(int N, int64_t k) {
     int lk = 0;
     while ((1LL << lk) < k) ++lk;
     return (53 * N + 1 + lk + 24 + 6) / 7;
 }
 
+// largest slice count whose level sums stay exact in int32
+int ozaki_max_slices(int64_t k) {
+    const double kp = (double)((k + 15) / 16 * 16);
+    int smax = (int)(2147483647.0 / (kp * 65.0 * 65.0));
+    if (smax * kp * 65.0 * 65.0 >= 2147483647.0) --smax;
+    return smax < 64 ? smax : 64;
+}
+
+// Slice-count tuner: enough 7-bit digits to reach the working precision of
+// N limbs (53 N + 1 bits) beyond the largest sampled scale gap, plus a 6-bit
+// margin for entries the sample missed.
+static int tuned_slices(int N, int gap8) {
+    const double gap = gap8 > 0 ? gap8 / 8.0 : 0.0;
+    return (int)ceil((53.0 * N + 1.0 + gap + 6.0) / 7.0);
+}
+
+static const int OZ_SAMPLES = 2048;
+
 int ozaki_gemm(mflab_handle *h, int N, int S, int64_t m, int64_t n, int64_t k, Mat A, Mat B,
-               Mat C, const double *alpha, const double *beta, cudaStream_t s) {
-    if (S < 1 || S > 64) return MFLAB_ERR_ARG;
-    const OzPlan p = oz_plan(m, n, k, S);
-    // exactness of every int32 level sum: (L-1) kp 65^2 < 2^31 for L <= S+1
-    if ((double)S * (double)p.kp * 65.0 * 65.0 >= 2147483647.0) return MFLAB_ERR_UNSUPPORTED;
+               Mat C, const double *alpha, const double *beta, cudaStream_t s, int *S_used) {
+    if (S < 0 || S > 64) return MFLAB_ERR_ARG;
     if ((int64_t)n > 65535 * 1LL || m > INT_MAX) return MFLAB_ERR_UNSUPPORTED;
-    int rc = mflab_reserve_scratch(h, p.total);
+    // exponents (and the tuner's gap word) live in the aux scratch
+    int rc = mflab_reserve_aux(h, sizeof(int) * (size_t)(m + n + 64));
+    if (rc) return rc;
+    int *rowexp = (int *)h->aux;
+    int *colexp = rowexp + m;
+    int *gap8 = colexp + n;
+    switch (N) {
+    case 2: rc = oz_exponents<2>(m, n, k, A, B, rowexp, colexp, s); break;
+    case 3: rc = oz_exponents<3>(m, n, k, A, B, rowexp, colexp, s); break;
+    case 4: rc = oz_exponents<4>(m, n, k, A, B, rowexp, colexp, s); break;
+    default: return MFLAB_ERR_UNSUPPORTED;
+    }
+    if (rc) return rc;
+    if (S == 0) {
+        // data-dependent slice count: one synchronisation to read the gap
+        cudaError_t e = cudaMemsetAsync(gap8, 0, sizeof(int), s);
+        if (e != cudaSuccess) return record_cuda_error(e, "ozaki tune");
+        oz_gap_kernel<<<(OZ_SAMPLES + 7) / 8, 256, 0, s>>>(m, n, k, A, B, rowexp, colexp,
+                                                           OZ_SAMPLES, gap8);
+        int g = 0;
+        e = cudaMemcpyAsync(&g, gap8, sizeof(int), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return record_cuda_error(e, "ozaki tune read");
+        S = tuned_slices(N, g);
+    }
+    const int smax = ozaki_max_slices(k);
+    if (S > smax) S = smax;
+    if (S < 1) return MFLAB_ERR_UNSUPPORTED;
+    if (S_used) *S_used = S;
+    const OzPlan p = oz_plan(m, n, k, S);
+    rc = mflab_reserve_scratch(h, p.total);
     if (rc) return rc;
     char *base = (char *)h->scratch;
     switch (N) {
-    case 2: return ozaki_n<2>(m, n, k, A, B, C, alpha, beta, S, base, p, s);
-    case 3: return ozaki_n<3>(m, n, k, A, B, C, alpha, beta, S, base, p, s);
-    case 4: return ozaki_n<4>(m, n, k, A, B, C, alpha, beta, S, base, p, s);
-    default: return MFLAB_ERR_UNSUPPORTED;
+    case 2: return ozaki_n<2>(m, n, k, A, B, C, alpha, beta, S, base, p, rowexp, colexp, s);
+    case 3: return ozaki_n<3>(m, n, k, A, B, C, alpha, beta, S, base, p, rowexp, colexp, s);
+    default: return ozaki_n<4>(m, n, k, A, B, C, alpha, beta, S, base, p, rowexp, colexp, s);
     }
 }
 
@@ -321,9 +398,9 @@ extern "C" int mflab_gemm_ozaki_route(mflab_handle *h, void *stream, int limbs, 
                                       int64_t lsa, const double *B, int64_t ldb, int64_t lsb,
                                       double *C, int64_t ldc, int64_t lsc, const double *alpha,
                                       const double *beta) {
-    return mfl::ozaki_gemm(h, limbs, mfl::ozaki_default_slices(limbs, k), m, n, k,
-                           mfl::Mat{(double *)A, lda, lsa}, mfl::Mat{(double *)B, ldb, lsb},
-                           mfl::Mat{C, ldc, lsc}, alpha, beta, (cudaStream_t)stream);
+    return mfl::ozaki_gemm(h, limbs, 0, m, n, k, mfl::Mat{(double *)A, lda, lsa},
+                           mfl::Mat{(double *)B, ldb, lsb}, mfl::Mat{C, ldc, lsc}, alpha, beta,
+                           (cudaStream_t)stream, &h->last_slices);
 }
 
 extern "C" int mflab_gemm_ozaki(mflab_handle *h, void *stream, int limbs, int slices, int64_t m,
@@ -337,11 +414,13 @@ extern "C" int mflab_gemm_ozaki(mflab_handle *h, void *stream, int limbs, int sl
     if (mfl::views_overlap(C, ldc, lsc, m, n, limbs, A, lda, lsa, m, k) ||
         mfl::views_overlap(C, ldc, lsc, m, n, limbs, B, ldb, lsb, k, n))
         return MFLAB_ERR_ALIAS;
-    if (slices <= 0) slices = mfl::ozaki_default_slices(limbs, k);
+    if (slices < 0) return MFLAB_ERR_ARG;
     return mfl::ozaki_gemm(h, limbs, slices, m, n, k, mfl::Mat{(double *)A, lda, lsa},
                            mfl::Mat{(double *)B, ldb, lsb}, mfl::Mat{C, ldc, lsc}, alpha, beta,
-                           (cudaStream_t)stream);
+                           (cudaStream_t)stream, &h->last_slices);
 }
+
+extern "C" int mflab_ozaki_last_slices(mflab_handle *h) { return h ? h->last_slices : 0; }
 
 extern "C" int mflab_ozaki_default_slices(int limbs, int64_t k) {
     return mfl::ozaki_default_slices(limbs, k);

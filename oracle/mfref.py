@@ -109,7 +109,7 @@ class Planes:
         if X.ndim == 2:
             X = X[:, :, None]
         self.N, self.m, self.n = X.shape
-        self.buf = np.ascontiguousarray(X.transpose(0, 2, 1))  # (N, n, m)
+        self.buf = np.array(X.transpose(0, 2, 1), order="C", copy=True)  # (N, n, m), owned
         self.ld = max(self.m, 1)
         self.ls = self.n * self.m
 
