@@ -41,6 +41,7 @@ def parse():
     p.add_argument("--limbs", type=int, default=2)
     p.add_argument("--route", default="auto", help="headline route: auto (ozaki if built), plain, ozaki")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-x4", action="store_true", help="skip the Float64x4 companion run")
     return p.parse_args()
 
 
@@ -205,6 +206,106 @@ def run_reference(args):
 
 
 # ----------------------------------------------------------- main arm ----
+def _check_entries(mfref, An, Bn, Cm, rows, cols):
+    """exact check of entries (rows[j], cols[j]) of a device result: returns the
+    componentwise relative errors |C - C_exact| / sum_k |a_ik||b_kj|"""
+    import numpy as np
+    Cs = Cm.planes()[:, cols, :].cpu().numpy()  # (N, s, m): column cols[j] at index j
+    Csub = np.ascontiguousarray(Cs.transpose(0, 2, 1))
+    Bsub = np.ascontiguousarray(Bn[:, :, cols])
+    err, scale, _ = mfref.exact_gemm_check(An, Bsub, Csub, rows, np.arange(len(rows)))
+    return err / scale
+
+
+class Runner:
+    def __init__(self, args, torch, dist, world, rank, local):
+        self.args, self.torch, self.dist = args, torch, dist
+        self.world, self.rank, self.local = world, rank, local
+        import __graft_entry__
+        self.mf = __graft_entry__.load_package()
+        from importlib import import_module
+        self.syn = import_module("mflab200.synthetic")
+        self.stream = torch.cuda.current_stream()
+
+    def barrier(self):
+        if self.world > 1:
+            self.dist.barrier()
+        self.torch.cuda.synchronize()
+
+    def timed(self, fn, steps, warmup):
+        torch = self.torch
+        for _ in range(warmup):
+            fn()
+        self.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(self.stream)
+        for _ in range(steps):
+            fn()
+        e1.record(self.stream)
+        self.barrier()
+        t = e0.elapsed_time(e1) / 1e3
+        if self.world > 1:
+            tt = torch.tensor([t], device="cuda")
+            self.dist.all_reduce(tt, op=self.dist.ReduceOp.MAX)
+            t = float(tt.item())
+        return t
+
+    def operands(self, N, n):
+        mf, syn = self.mf, self.syn
+        A = mf.MFMatrix.from_tensor(syn.randn_mf_device(1000 + self.rank, N, n, n, spread=20))
+        B = mf.MFMatrix.from_tensor(syn.randn_mf_device(2000 + self.rank, N, n, n, spread=20))
+        return A, B
+
+    def accuracy_and_slices(self, N, n, A, B, Cm):
+        """Plain and INT8-slice errors against the exact oracle on 256 sampled
+        entries; the slice count starts at the product's tuner choice and is
+        raised until the INT8-slice error is no worse than the plain one."""
+        import numpy as np
+        mf = self.mf
+        from oracle import mfref
+        rs = np.random.default_rng(5)
+        rows, cols = rs.integers(0, n, 256), rs.integers(0, n, 256)
+        An, Bn = A.to_numpy(), B.to_numpy()
+        mf.gemm_(Cm, A, B)
+        e_plain = float(np.max(_check_entries(mfref, An, Bn, Cm, rows, cols)))
+        mf.gemm_(Cm, A, B, config=mf.KernelConfig(gemm_strategy="ozaki"))
+        S0 = mf.ozaki_last_slices()
+        S = S0
+        e_oz = float(np.max(_check_entries(mfref, An, Bn, Cm, rows, cols)))
+        while e_oz > e_plain and S < S0 + 6:
+            S += 1
+            mf.gemm_(Cm, A, B, config=mf.KernelConfig(gemm_strategy="ozaki", ozaki_slices=S))
+            e_oz = float(np.max(_check_entries(mfref, An, Bn, Cm, rows, cols)))
+        return {"plain_max_rel_err": e_plain, "ozaki_max_rel_err": e_oz, "slices": S,
+                "tuner_slices": S0, "samples": 256}
+
+    def phases(self, N, n, A, B, Cm, S):
+        import ctypes as C
+        mf = self.mf
+        lib = mf._native.load()
+        h = mf._handle(self.local)
+        ms = (C.c_float * 4)()
+        ops = C.c_double()
+        one = (C.c_double * 4)(1.0)
+        zero = (C.c_double * 4)()
+        rc = lib.mflab_gemm_ozaki_phases(h, self.stream.cuda_stream, N, S, n, n, n, A.ptr(), A.ld,
+                                         A.ls, B.ptr(), B.ld, B.ls, Cm.ptr(), Cm.ld, Cm.ls, one,
+                                         zero, ms, C.byref(ops))
+        assert rc == 0, rc
+        return [ms[i] for i in range(4)], ops.value
+
+    def int8_peak(self):
+        import ctypes as C
+        mf = self.mf
+        lib = mf._native.load()
+        ms = C.c_float()
+        n, k = 8192, 16384
+        rc = lib.mflab_probe_int8_gemm(mf._handle(self.local), self.stream.cuda_stream, n, n, k, 3,
+                                       C.byref(ms))
+        assert rc == 0, rc
+        return 2.0 * n * n * k / (ms.value / 1e3)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -219,81 +320,40 @@ def main():
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
-    import __graft_entry__
-    mf = __graft_entry__.load_package()
-    from importlib import import_module
-    syn = import_module("mflab200.synthetic")
-    lib = mf._native.load()
-
+    R = Runner(args, torch, dist, world, rank, local)
+    mf = R.mf
     N, n = args.limbs, args.n
     route = args.route
-    have_ozaki = mf.ozaki_available() if hasattr(mf, "ozaki_available") else False
     if route == "auto":
-        route = "ozaki" if have_ozaki else "plain"
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    A = mf.MFMatrix.from_tensor(syn.randn_mf_device(1000 + rank, N, n, n, spread=20))
-    B = mf.MFMatrix.from_tensor(syn.randn_mf_device(2000 + rank, N, n, n, spread=20))
-    Cm = mf.MFMatrix.zeros(N, n, n)
-    stream = torch.cuda.current_stream()
-
-    def timed(fn, steps, warmup):
-        for _ in range(warmup):
-            fn()
-        barrier()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(steps):
-            fn()
-        e1.record(stream)
-        barrier()
-        t = e0.elapsed_time(e1) / 1e3
-        if world > 1:
-            tt = torch.tensor([t], device="cuda")
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            t = float(tt.item())
-        return t
-
-    plain_cfg = mf.KernelConfig(gemm_strategy="auto")
-    oz_cfg = mf.KernelConfig(gemm_strategy="ozaki")
+        route = "ozaki" if mf.ozaki_available() else "plain"
     flops = 2.0 * n * n * n
+    plain_cfg = mf.KernelConfig(gemm_strategy="auto")
+
+    A, B = R.operands(N, n)
+    Cm = mf.MFMatrix.zeros(N, n, n)
+    acc = R.accuracy_and_slices(N, n, A, B, Cm) if rank == 0 and route == "ozaki" else {}
+    S = acc.get("slices", 0)
+    if world > 1:
+        t = torch.tensor([S], device="cuda")
+        dist.broadcast(t, 0)
+        S = int(t.item())
+    oz_cfg = mf.KernelConfig(gemm_strategy="ozaki", ozaki_slices=S)
+    head_cfg = oz_cfg if route == "ozaki" else plain_cfg
 
     clocks = ClockSampler(local)
-    results = {}
-    # headline route first, timed with clock sampling
-    head_cfg = oz_cfg if route == "ozaki" else plain_cfg
-    head_fn = lambda: mf.gemm_(Cm, A, B, config=head_cfg)
     clocks.start()
-    t_head = timed(head_fn, args.steps, args.warmup)
+    t_head = R.timed(lambda: mf.gemm_(Cm, A, B, config=head_cfg), args.steps, args.warmup)
     clk = clocks.stop()
-    results["head"] = t_head / args.steps
-    # the other route (plain always reported)
-    if route == "ozaki":
-        t_plain = timed(lambda: mf.gemm_(Cm, A, B, config=plain_cfg), 1, 1)
-        results["plain"] = t_plain
-    else:
-        results["plain"] = results["head"]
-
-    # accuracy of both routes against the exact oracle on sampled entries
-    acc = {}
-    if rank == 0:
+    t_head /= args.steps
+    t_plain = R.timed(lambda: mf.gemm_(Cm, A, B, config=plain_cfg), 1, 1) if route == "ozaki" \
+        else t_head
+    if route != "ozaki" and rank == 0:
         from oracle import mfref
         rs = np.random.default_rng(5)
-        rows = rs.integers(0, n, 256)
-        cols = rs.integers(0, n, 256)
-        An = A.to_numpy()
-        Bn = B.to_numpy()
-        for name, cfg in (("plain", plain_cfg), ("ozaki", oz_cfg)):
-            if name == "ozaki" and not have_ozaki:
-                continue
-            mf.gemm_(Cm, A, B, config=cfg)
-            err, scale = _check_entries(mfref, An, Bn, Cm, rows, cols)
-            acc[name] = float(np.max(err / scale))
-        del An, Bn
+        rows, cols = rs.integers(0, n, 256), rs.integers(0, n, 256)
+        mf.gemm_(Cm, A, B)
+        acc = {"plain_max_rel_err": float(np.max(_check_entries(
+            mfref, A.to_numpy(), B.to_numpy(), Cm, rows, cols)))}
 
     # end to end through the public API with host buffers
     hA = torch.empty((N, n, n), dtype=torch.float64, pin_memory=True)
@@ -311,43 +371,64 @@ def main():
                  mf.MFMatrix.from_tensor(dB), config=head_cfg)
         hC.copy_(dC, non_blocking=True)
 
-    t_e2e = timed(e2e_step, max(1, args.steps // 2), 1) / max(1, args.steps // 2)
+    e2e_steps = max(1, args.steps)
+    t_e2e = R.timed(e2e_step, e2e_steps, 1) / e2e_steps
+    del dA, dB, dC, hA, hB, hC
 
-    # roofline of the dominant kernel (plain: FP64 pipe; ozaki: INT8 tensor)
     peak_fp64 = fp64_peak(mf, torch)
+    instr = float(n) ** 3 * ops_per_term(N)
+    plain_roof = {"bound": "fp64", "achieved": instr / t_plain / 1e12, "peak": peak_fp64 / 1e12,
+                  "unit": "T FP64 instr/s", "frac": instr / t_plain / peak_fp64,
+                  "traffic": read_traffic(f"mm_x{N}_n{n}"),
+                  "peak_source": "measured in this run (DFMA probe, burst)"}
     if route == "ozaki":
-        roof = mf.ozaki_roofline(N, n, results["head"])
+        ph, ops = R.phases(N, n, A, B, Cm, S)
+        peak8 = R.int8_peak()
+        achieved = ops / (ph[2] / 1e3)
+        roof = {"bound": "tensor", "achieved": achieved / 1e12, "peak": peak8 / 1e12,
+                "unit": "INT8 TOP/s", "frac": achieved / peak8,
+                "traffic": read_traffic(f"int8_levels_x{N}_n{n}"),
+                "kernel": "int8 level GEMMs (int8 x int8 -> int32, K = (L-1) k)",
+                "peak_source": "measured in this run: int8 TN GEMM 8192x8192x16384 through the "
+                               "same path (burst); nominal dense INT8 is 4500 TOP/s",
+                "phases_ms": {"exponents_tune": ph[0], "split": ph[1], "int8_levels": ph[2],
+                              "accumulate": ph[3]}}
     else:
-        instr = float(n) ** 3 * ops_per_term(N)
-        achieved = instr / results["head"] / 1e12
-        roof = {"bound": "fp64", "achieved": achieved, "peak": peak_fp64 / 1e12,
-                "unit": "T FP64 instr/s", "frac": achieved / (peak_fp64 / 1e12),
-                "traffic": read_traffic(f"mm_x{N}_n{n}"),
-                "peak_source": "measured in this run (DFMA probe, burst)"}
+        roof = plain_roof
 
-    value = world * flops / results["head"] / 1e9
+    value = world * flops / t_head / 1e9
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": results["head"] * 1e3, "higher_is_better": True,
+        "warmup": args.warmup, "ms_per_step": t_head * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded randn * 2^U(-20,20), lower limbs randn*2^-53*|prev|)",
         "config": {"workload": f"Float64x{N} GEMM m=n=k={n}", "limbs": N, "n": n,
-                   "route": route, "parallelism": f"replicas{world}",
+                   "route": route, "slices": S if route == "ozaki" else None,
+                   "parallelism": f"replicas{world}",
                    "l2": "inputs larger than L2 (each operand >= 1 GiB)"},
-        "plain_fp64": {"value": world * flops / results["plain"] / 1e9,
-                       "ms_per_step": results["plain"] * 1e3,
-                       "max_rel_err": acc.get("plain")},
+        "accuracy": acc,
+        "plain_fp64": {"value": world * flops / t_plain / 1e9, "ms_per_step": t_plain * 1e3,
+                       "roofline": plain_roof},
+        "speedup_vs_plain": t_plain / t_head,
         "e2e": {"value": world * flops / t_e2e / 1e9, "unit": UNIT,
                 "h2d_bytes_per_step": 2 * N * n * n * 8, "d2h_bytes_per_step": N * n * n * 8},
         "roofline": roof,
         "clocks": clk,
-        "gpu_launches": args.steps * (mf.gemm_launches(N, n, head_cfg)
-                                      if hasattr(mf, "gemm_launches") else 1),
-        "fp64_peak_instr_per_s": peak_fp64,
+        "gpu_launches": args.steps * (5 if route == "ozaki" else 1),
+        "library_launches": args.steps * S if route == "ozaki" else 0,
     }
-    if route == "ozaki":
-        line["ozaki"] = {"max_rel_err": acc.get("ozaki"), "speedup_vs_plain":
-                         results["plain"] / results["head"]}
+    if N == 2 and route == "ozaki" and not args.no_x4 and world == 1:
+        del A, B, Cm
+        torch.cuda.empty_cache()
+        A4, B4 = R.operands(4, n)
+        C4 = mf.MFMatrix.zeros(4, n, n)
+        acc4 = R.accuracy_and_slices(4, n, A4, B4, C4)
+        cfg4 = mf.KernelConfig(gemm_strategy="ozaki", ozaki_slices=acc4["slices"])
+        t4 = R.timed(lambda: mf.gemm_(C4, A4, B4, config=cfg4), 2, 1) / 2
+        t4p = R.timed(lambda: mf.gemm_(C4, A4, B4), 1, 0)
+        line["x4"] = {"workload": f"Float64x4 GEMM m=n=k={n}", "ozaki_value": flops / t4 / 1e9,
+                      "ozaki_ms": t4 * 1e3, "plain_value": flops / t4p / 1e9,
+                      "plain_ms": t4p * 1e3, "speedup_vs_plain": t4p / t4, "accuracy": acc4}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import mfref
         threads = mfref.threads()
@@ -358,18 +439,6 @@ def main():
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
-
-
-def _check_entries(mfref, An, Bn, Cm, rows, cols):
-    """exact check of entries (rows[j], cols[j]) of the device result"""
-    import numpy as np
-    Cs = Cm.planes()[:, cols, :].cpu().numpy()  # (N, s, m): column cols[j] at index j
-    N = An.shape[0]
-    s = len(rows)
-    # build an N x m x s matrix whose column j is C[:, cols[j]] and check (rows[j], j)
-    Csub = np.ascontiguousarray(Cs.transpose(0, 2, 1))
-    Bsub = np.ascontiguousarray(Bn[:, :, cols])
-    return mfref.exact_gemm_check(An, Bsub, Csub, rows, np.arange(s))[:2]
 
 
 if __name__ == "__main__":

@@ -15,6 +15,20 @@ extern "C" {
    device buffer of blocks*threads doubles. */
 int mflab_probe_fp64(void *stream, int kind, int blocks, int threads, int64_t iters, double *out,
                      double *instructions);
+
+/* The INT8-slice GEMM (mflab_gemm_ozaki, same arguments) with per-phase device
+   times in ms[4]: exponents + slice tuning, digit split, int8 level GEMMs,
+   accumulation; *int8_ops = 2 m n roundup(k,16) S(S+1)/2.  Synchronises. */
+int mflab_gemm_ozaki_phases(struct mflab_handle *h, void *stream, int limbs, int slices, int64_t m,
+                            int64_t n, int64_t k, const double *A, int64_t lda, int64_t lsa,
+                            const double *B, int64_t ldb, int64_t lsb, double *C, int64_t ldc,
+                            int64_t lsc, const double *alpha, const double *beta, float *ms,
+                            double *int8_ops);
+
+/* Best device time (ms) of `reps` int8 x int8 -> int32 TN GEMMs of m x n x k
+   through the library path the INT8-slice route uses.  Synchronises. */
+int mflab_probe_int8_gemm(struct mflab_handle *h, void *stream, int64_t m, int64_t n, int64_t k,
+                          int reps, float *ms);
 #ifdef __cplusplus
 }
 #endif

@@ -77,6 +77,9 @@ SIGNATURES = {
                          _vp, _i64, _i64, _d, _d],
     "mflab_ozaki_default_slices": [_int, _i64],
     "mflab_ozaki_last_slices": [_vp],
+    "mflab_gemm_ozaki_phases": [_vp, _vp, _int, _int, _i64, _i64, _i64, _vp, _i64, _i64, _vp, _i64,
+                                _i64, _vp, _i64, _i64, _d, _d, C.POINTER(C.c_float), _d],
+    "mflab_probe_int8_gemm": [_vp, _vp, _i64, _i64, _i64, _int, C.POINTER(C.c_float)],
 }
 _RESTYPE = {"mflab_status_string": C.c_char_p, "mflab_last_error": C.c_char_p}
 

@@ -239,7 +239,7 @@ static cublasLtHandle_t lt_handle() {
 }
 
 // I = Aop^T * Bop with int8 operands stored K-major (ld = lda / ldb bytes)
-static int int8_gemm_tn(int64_t m, int64_t n, int64_t K, const int8_t *A, int64_t lda,
+int int8_gemm_tn(int64_t m, int64_t n, int64_t K, const int8_t *A, int64_t lda,
                         const int8_t *B, int64_t ldb, int32_t *I, int64_t ldi, void *ws, size_t wsb,
                         cudaStream_t s) {
     cublasLtHandle_t h = lt_handle();
@@ -288,10 +288,18 @@ static int oz_exponents(int64_t m, int64_t n, int64_t k, Mat A, Mat B, int *rowe
     return record_cuda_error(cudaGetLastError(), "ozaki exponents");
 }
 
+// optional phase events (profiling entry point only): [0] after exponents and
+// tuning, [1] after the digit split, [2] after the level GEMMs, [3] at the end
+static cudaEvent_t *g_phase_ev = nullptr;
+static inline void phase(int i, cudaStream_t s) {
+    if (g_phase_ev) cudaEventRecord(g_phase_ev[i], s);
+}
+
 template <int N>
 static int ozaki_n(int64_t m, int64_t n, int64_t k, Mat A, Mat B, Mat C, const double *alpha,
                    const double *beta, int S, char *base, const OzPlan &p, const int *rowexp,
                    const int *colexp, cudaStream_t s) {
+    phase(0, s);
     int8_t *A8 = (int8_t *)base;
     int8_t *B8 = (int8_t *)(base + p.a8);
     int32_t *I = (int32_t *)(base + p.a8 + p.b8);
@@ -302,12 +310,14 @@ static int ozaki_n(int64_t m, int64_t n, int64_t k, Mat A, Mat B, Mat C, const d
     oz_split_b_kernel<N><<<gb, 256, 0, s>>>(k, n, p.kp, S, B, colexp, B8);
     int rc = record_cuda_error(cudaGetLastError(), "ozaki split");
     if (rc) return rc;
+    phase(1, s);
     const int64_t ld8 = (int64_t)S * p.kp;
     for (int L = 2; L <= S + 1; ++L) {
         rc = int8_gemm_tn(m, n, (int64_t)(L - 1) * p.kp, A8, ld8, B8 + (int64_t)(S - L + 1) * p.kp,
                           ld8, I + (size_t)(L - 2) * p.plane, p.ldi, ws, p.ws, s);
         if (rc) return rc;
     }
+    phase(2, s);
     scal<N> al{}, be{};
     int overwrite = 1;
     for (int l = 0; l < N; ++l) {
@@ -318,6 +328,7 @@ static int ozaki_n(int64_t m, int64_t n, int64_t k, Mat A, Mat B, Mat C, const d
     dim3 gc((unsigned)((m + 127) / 128), (unsigned)n);
     oz_accum_kernel<N><<<gc, 128, 0, s>>>(m, n, S, I, p.ldi, p.plane, rowexp, colexp, C, al, be,
                                           overwrite);
+    phase(3, s);
     return record_cuda_error(cudaGetLastError(), "ozaki accumulate");
 }
 
@@ -424,4 +435,80 @@ extern "C" int mflab_ozaki_last_slices(mflab_handle *h) { return h ? h->last_sli
 
 extern "C" int mflab_ozaki_default_slices(int limbs, int64_t k) {
     return mfl::ozaki_default_slices(limbs, k);
+}
+
+// ------------------------------------------------------ measurement -------
+// mflab_gemm_ozaki with per-phase device times: ms[0] exponents + tuning,
+// ms[1] digit split, ms[2] int8 level GEMMs, ms[3] accumulation; *int8_ops
+// receives the integer multiply-add operations (2 m n K summed over levels).
+// Synchronises the stream.
+extern "C" int mflab_gemm_ozaki_phases(mflab_handle *h, void *stream, int limbs, int slices,
+                                       int64_t m, int64_t n, int64_t k, const double *A,
+                                       int64_t lda, int64_t lsa, const double *B, int64_t ldb,
+                                       int64_t lsb, double *C, int64_t ldc, int64_t lsc,
+                                       const double *alpha, const double *beta, float *ms,
+                                       double *int8_ops) {
+    if (!h || !ms || !int8_ops) return MFLAB_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaEvent_t ev[5];
+    for (auto &e : ev) cudaEventCreate(&e);
+    cudaEventRecord(ev[4], s);
+    mfl::g_phase_ev = ev;
+    int rc = mflab_gemm_ozaki(h, stream, limbs, slices, m, n, k, A, lda, lsa, B, ldb, lsb, C, ldc,
+                              lsc, alpha, beta);
+    mfl::g_phase_ev = nullptr;
+    if (rc == MFLAB_OK) {
+        cudaError_t e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) rc = mfl::record_cuda_error(e, "ozaki phases");
+    }
+    if (rc == MFLAB_OK) {
+        cudaEventElapsedTime(&ms[0], ev[4], ev[0]);
+        cudaEventElapsedTime(&ms[1], ev[0], ev[1]);
+        cudaEventElapsedTime(&ms[2], ev[1], ev[2]);
+        cudaEventElapsedTime(&ms[3], ev[2], ev[3]);
+        const int S = h->last_slices;
+        const double kp = (double)((k + 15) / 16 * 16);
+        *int8_ops = 2.0 * (double)m * (double)n * kp * (double)S * (S + 1) / 2.0;
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    return rc;
+}
+
+// Device time of one int8 x int8 -> int32 TN GEMM (m x n x k) through the same
+// library path as the level products, after one warm-up call; *ms receives
+// the best of `reps` timed calls.  Uses the handle scratch.  Synchronises.
+extern "C" int mflab_probe_int8_gemm(mflab_handle *h, void *stream, int64_t m, int64_t n,
+                                     int64_t k, int reps, float *ms) {
+    if (!h || !ms || m <= 0 || n <= 0 || k <= 0 || reps <= 0) return MFLAB_ERR_ARG;
+    const int64_t kp = (k + 15) / 16 * 16, ldi = (m + 15) / 16 * 16;
+    const size_t a = (size_t)m * kp, b = (size_t)n * kp, c = (size_t)ldi * n * 4, ws = 64 << 20;
+    int rc = mflab_reserve_scratch(h, a + b + c + ws + 1024);
+    if (rc) return rc;
+    char *base = (char *)h->scratch;
+    int8_t *A8 = (int8_t *)base, *B8 = (int8_t *)(base + (a + 255) / 256 * 256);
+    int32_t *I = (int32_t *)(base + (a + 255) / 256 * 256 + (b + 255) / 256 * 256);
+    char *wsp = (char *)I + (c + 255) / 256 * 256;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaMemsetAsync(A8, 0x11, a, s);
+    cudaMemsetAsync(B8, 0x23, b, s);
+    rc = mfl::int8_gemm_tn(m, n, kp, A8, kp, B8, kp, I, ldi, wsp, ws, s);
+    if (rc) return rc;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float best = 1e30f;
+    for (int r = 0; r < reps && rc == MFLAB_OK; ++r) {
+        cudaEventRecord(e0, s);
+        rc = mfl::int8_gemm_tn(m, n, kp, A8, kp, B8, kp, I, ldi, wsp, ws, s);
+        cudaEventRecord(e1, s);
+        cudaError_t e = cudaEventSynchronize(e1);
+        if (e != cudaSuccess) rc = mfl::record_cuda_error(e, "int8 probe");
+        float t = 0.f;
+        cudaEventElapsedTime(&t, e0, e1);
+        if (t < best) best = t;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms = best;
+    return rc;
 }
