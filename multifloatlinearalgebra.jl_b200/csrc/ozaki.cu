@@ -107,8 +107,9 @@ __device__ __forceinline__ void oz_digits(mf<N> x, int S, Emit emit) {
 // through shared memory so that both the plane reads (along rows) and the
 // int8 writes (along k) are coalesced.
 template <int N>
-__global__ void __launch_bounds__(256) oz_split_a_kernel(int64_t m, int64_t k, int64_t kp, int S,
-                                                         Mat A, const int *rowexp, int8_t *A8) {
+__global__ void __launch_bounds__(256) oz_split_a_kernel(int64_t m, int64_t mp, int64_t k,
+                                                         int64_t kp, int S, Mat A,
+                                                         const int *rowexp, int8_t *A8) {
     __shared__ double t[N][32][33];
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int64_t i0 = (int64_t)blockIdx.x * 32, k0 = (int64_t)blockIdx.y * 32;
@@ -125,8 +126,8 @@ __global__ void __launch_bounds__(256) oz_split_a_kernel(int64_t m, int64_t k, i
     for (int j = 0; j < 4; ++j) {
         const int ii = ty + 8 * j;
         const int64_t i = i0 + ii, kg = k0 + tx;
-        if (i >= m || kg >= kp) continue;
-        const int e = rowexp[i];
+        if (i >= mp || kg >= kp) continue;
+        const int e = i < m ? rowexp[i] : OZ_EXP_EMPTY;  // padding rows: zero digits
         const int sh = oz_scale_exp(e);
         mf<N> x;
 #pragma unroll
@@ -138,17 +139,18 @@ __global__ void __launch_bounds__(256) oz_split_a_kernel(int64_t m, int64_t k, i
 
 // B digits: column j of B is contiguous along k; slice order reversed
 template <int N>
-__global__ void oz_split_b_kernel(int64_t k, int64_t n, int64_t kp, int S, Mat B,
+__global__ void oz_split_b_kernel(int64_t k, int64_t n, int64_t np, int64_t kp, int S, Mat B,
                                   const int *colexp, int8_t *B8) {
     const int64_t kg = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t j = blockIdx.y;
-    if (kg >= kp || j >= n) return;
-    const int e = colexp[j];
+    if (kg >= kp || j >= np) return;
+    const int e = j < n ? colexp[j] : OZ_EXP_EMPTY;  // padding columns: zero digits
     const int sh = oz_scale_exp(e);
     mf<N> x;
 #pragma unroll
     for (int l = 0; l < N; ++l)
-        x.v[l] = (kg < k && e != OZ_EXP_BAD) ? ldexp(B.p[l * B.ls + j * B.ld + kg], -sh) : 0.0;
+        x.v[l] = (kg < k && j < n && e != OZ_EXP_BAD) ? ldexp(B.p[l * B.ls + j * B.ld + kg], -sh)
+                                                        : 0.0;
     int8_t *dst = B8 + (size_t)j * S * kp + kg;
     oz_digits<N>(x, S, [&](int s, int d) { dst[(size_t)(S - 1 - s) * kp] = (int8_t)d; });
 }
@@ -211,7 +213,8 @@ __global__ void oz_gap_kernel(int64_t m, int64_t n, int64_t k, Mat A, Mat B, con
 struct OzPlan {
     int S;
     int64_t kp;     // k rounded up to 16 (int8 rows 16-byte aligned; zero digits pad)
-    int64_t ldi;    // leading dimension of an int32 level plane (m rounded up to 16)
+    int64_t mp, np; // m, n rounded up to 16: the padding rows/columns hold zero digits
+    int64_t ldi;    // leading dimension of an int32 level plane (= mp)
     size_t plane;   // elements between level planes (multiple of 64)
     size_t a8, b8, lev, exps, ws, total;
 };
@@ -220,11 +223,13 @@ static OzPlan oz_plan(int64_t m, int64_t n, int64_t k, int S) {
     OzPlan p;
     p.S = S;
     p.kp = (k + 15) / 16 * 16;
-    p.ldi = (m + 15) / 16 * 16;
-    p.plane = ((size_t)p.ldi * n + 63) / 64 * 64;
+    p.mp = (m + 15) / 16 * 16;
+    p.np = (n + 15) / 16 * 16;
+    p.ldi = p.mp;
+    p.plane = ((size_t)p.ldi * p.np + 63) / 64 * 64;
     auto al = [](size_t b) { return (b + 255) / 256 * 256; };
-    p.a8 = al((size_t)m * S * p.kp);
-    p.b8 = al((size_t)n * S * p.kp);
+    p.a8 = al((size_t)p.mp * S * p.kp);
+    p.b8 = al((size_t)p.np * S * p.kp);
     p.lev = al((size_t)S * p.plane * sizeof(int32_t));
     p.exps = al((size_t)(m + n) * sizeof(int));
     p.ws = (size_t)64 << 20;
@@ -304,17 +309,18 @@ static int ozaki_n(int64_t m, int64_t n, int64_t k, Mat A, Mat B, Mat C, const d
     int8_t *B8 = (int8_t *)(base + p.a8);
     int32_t *I = (int32_t *)(base + p.a8 + p.b8);
     void *ws = base + p.a8 + p.b8 + p.lev + p.exps;
-    dim3 ga((unsigned)((m + 31) / 32), (unsigned)((p.kp + 31) / 32));
-    oz_split_a_kernel<N><<<ga, dim3(32, 8), 0, s>>>(m, k, p.kp, S, A, rowexp, A8);
-    dim3 gb((unsigned)((p.kp + 255) / 256), (unsigned)n);
-    oz_split_b_kernel<N><<<gb, 256, 0, s>>>(k, n, p.kp, S, B, colexp, B8);
+    dim3 ga((unsigned)((p.mp + 31) / 32), (unsigned)((p.kp + 31) / 32));
+    oz_split_a_kernel<N><<<ga, dim3(32, 8), 0, s>>>(m, p.mp, k, p.kp, S, A, rowexp, A8);
+    dim3 gb((unsigned)((p.kp + 255) / 256), (unsigned)p.np);
+    oz_split_b_kernel<N><<<gb, 256, 0, s>>>(k, n, p.np, p.kp, S, B, colexp, B8);
     int rc = record_cuda_error(cudaGetLastError(), "ozaki split");
     if (rc) return rc;
     phase(1, s);
     const int64_t ld8 = (int64_t)S * p.kp;
     for (int L = 2; L <= S + 1; ++L) {
-        rc = int8_gemm_tn(m, n, (int64_t)(L - 1) * p.kp, A8, ld8, B8 + (int64_t)(S - L + 1) * p.kp,
-                          ld8, I + (size_t)(L - 2) * p.plane, p.ldi, ws, p.ws, s);
+        rc = int8_gemm_tn(p.mp, p.np, (int64_t)(L - 1) * p.kp, A8, ld8,
+                          B8 + (int64_t)(S - L + 1) * p.kp, ld8, I + (size_t)(L - 2) * p.plane,
+                          p.ldi, ws, p.ws, s);
         if (rc) return rc;
     }
     phase(2, s);
@@ -361,7 +367,7 @@ static const int OZ_SAMPLES = 2048;
 int ozaki_gemm(mflab_handle *h, int N, int S, int64_t m, int64_t n, int64_t k, Mat A, Mat B,
                Mat C, const double *alpha, const double *beta, cudaStream_t s, int *S_used) {
     if (S < 0 || S > 64) return MFLAB_ERR_ARG;
-    if ((int64_t)n > 65535 * 1LL || m > INT_MAX) return MFLAB_ERR_UNSUPPORTED;
+    if ((n + 15) / 16 * 16 > 65535LL || m > INT_MAX) return MFLAB_ERR_UNSUPPORTED;
     // exponents (and the tuner's gap word) live in the aux scratch
     int rc = mflab_reserve_aux(h, sizeof(int) * (size_t)(m + n + 64));
     if (rc) return rc;
@@ -468,7 +474,8 @@ extern "C" int mflab_gemm_ozaki_phases(mflab_handle *h, void *stream, int limbs,
         cudaEventElapsedTime(&ms[3], ev[2], ev[3]);
         const int S = h->last_slices;
         const double kp = (double)((k + 15) / 16 * 16);
-        *int8_ops = 2.0 * (double)m * (double)n * kp * (double)S * (S + 1) / 2.0;
+        const double mp = (double)((m + 15) / 16 * 16), np = (double)((n + 15) / 16 * 16);
+        *int8_ops = 2.0 * mp * np * kp * (double)S * (S + 1) / 2.0;
     }
     for (auto &e : ev) cudaEventDestroy(e);
     return rc;
