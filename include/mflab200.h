@@ -153,6 +153,20 @@ int mflab_getrs(mflab_handle *h, void *stream, int limbs, int64_t n, int64_t nrh
 int mflab_max_abs(mflab_handle *h, void *stream, int limbs, int64_t m, int64_t n, const double *A,
                   int64_t lda, int64_t lsa, int region, double *out);
 
+/* mflab_max_abs without a handle and without any device allocation, for
+   callers that cannot let a library allocate: code whose device memory all
+   belongs to its own pool allocator, and code that must not take the implicit
+   device-wide synchronisation of cudaMalloc/cudaFree in an asynchronous
+   pipeline.  Partial results live in a fixed 640 KiB device array (one record
+   per column) that every device loading the library holds until exit, so n is
+   limited to 16384 columns (MFLAB_ERR_UNSUPPORTED beyond, with a message in
+   mflab_last_error).  The first call on a device looks up that array's device
+   address with the device current; make that first call before any stream
+   capture.  All calls share the array: calls that overlap on the GPU race.
+   No counterpart in the reference. */
+int mflab_max_abs_noalloc(void *stream, int limbs, int64_t m, int64_t n, const double *A,
+                          int64_t lda, int64_t lsa, int region, double *out);
+
 /* O(n) tail of factor_diagnostics (src/diagnostics.jl:21-107): out (device,
    4*limbs+2 doubles) = [min |A(i,i)|, max |A(i,i)|, max/min (Inf if min is
    zero), num/den (0 if den is zero), count, count > 0] over i < count.

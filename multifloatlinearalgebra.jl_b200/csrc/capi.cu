@@ -14,6 +14,7 @@ int record_cuda_error(cudaError_t e, const char *where) {
     g_last_error = std::string(where) + ": " + cudaGetErrorString(e);
     return MFLAB_ERR_CUDA;
 }
+void record_error_message(const char *msg) { g_last_error = msg; }
 }  // namespace mfl
 
 extern "C" int mflab_version(void) { return 10000 * 0 + 100 * 1 + 0; }

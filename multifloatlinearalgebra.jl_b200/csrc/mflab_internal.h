@@ -34,6 +34,7 @@ inline int cuda_status(cudaError_t e) {
 }
 
 int record_cuda_error(cudaError_t e, const char *where);
+void record_error_message(const char *msg);
 
 inline bool valid_limbs(int N) { return N >= 2 && N <= 4; }
 
