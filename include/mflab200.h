@@ -144,6 +144,40 @@ int mflab_getrs(mflab_handle *h, void *stream, int limbs, int64_t n, int64_t nrh
                 const double *LU, int64_t ldl, int64_t lsl, const int64_t *ipiv, double *B,
                 int64_t ldb, int64_t lsb);
 
+/* Bunch-Kaufman LDL^T in place (lower triangle authoritative on input; the
+   upper triangle is overwritten by the working mirror).  dsub (device,
+   limbs planes of n doubles, plane stride lsd >= n) receives the off-diagonal
+   of each 2x2 block, pivots (device int64, 1-based) the step pivots, blocks
+   (device uint8) 1 / 2 at a block start and 0 on a 2x2 continuation.
+   blocked = 0: the unblocked route; 1: the lazy-panel route with `block`
+   columns per panel (<= 64; the reference uses 16/12/8 for x2/x3/x4 and
+   blocks from n >= 512).  *info: 0, -1 non-finite lower triangle, k > 0 first
+   singular step.  The blocked route synchronises the stream once per panel.
+   Replaces ldlt!(A; check=false, config) — src/factorizations/ldlt.jl:654-717,
+   ldlt_gemmt.jl:36-73. */
+int mflab_sytrf(mflab_handle *h, void *stream, int limbs, int64_t n, double *A, int64_t lda,
+                int64_t lsa, double *dsub, int64_t lsd, int64_t *pivots, uint8_t *blocks,
+                int blocked, int64_t block, int *info);
+
+/* B <- A^{-1} B with a successful LDLT factor: forward interchanges,
+   unit-lower solve, block-diagonal solve, transposed unit-lower solve, reverse
+   interchanges.  *fail (device int) is set to the 1-based start of a singular
+   2x2 block, else to 0x7f7f7f7f.
+   Replaces ldiv!(B, F::MFLDLT) — src/solve.jl:298-365. */
+int mflab_sytrs(mflab_handle *h, void *stream, int limbs, int64_t n, int64_t nrhs, const double *F,
+                int64_t ldf, int64_t lsf, const double *dsub, int64_t lsd, const int64_t *pivots,
+                const uint8_t *blocks, double *B, int64_t ldb, int64_t lsb, int *fail);
+
+/* Inertia and block quality of an LDLT factor (one device thread).  out
+   (device, 6 + 4*limbs doubles): positive, negative, zero counts, 1x1 and 2x2
+   block counts, has-blocks flag, then min block |eigenvalue|, max block entry,
+   their ratios to omax (limbs doubles each; 0 when omax is zero).
+   Replaces factor_inertia / factor_diagnostics(::MFLDLT) —
+   src/diagnostics.jl:109-246. */
+int mflab_ldlt_diagnostics(mflab_handle *h, void *stream, int limbs, int64_t n, const double *F,
+                           int64_t ldf, int64_t lsf, const double *dsub, int64_t lsd,
+                           const uint8_t *blocks, const double *omax, double *out);
+
 /* ------------------------------------------------------- diagnostics --- */
 /* out (device, limbs+1 doubles) = [max |A(r,c)| over the region, finite flag]
    with region 0 all entries, 1 lower (r >= c), 2 upper (r <= c).

@@ -36,6 +36,7 @@ __all__ = [
     "factor_status", "factor_state", "factor_kind", "factor_matrix", "factor_precision",
     "factor_provider", "factor_pivots", "factor_diagnostics",
     "MFCholesky", "MFLU", "capabilities", "limb_type_name",
+    "ldlt_", "ldlt_plan", "MFLDLT", "factor_blocks", "factor_permutation", "factor_inertia",
 ]
 
 
@@ -480,6 +481,19 @@ class MFLU(_Factor):
         self.original_maximum = original_maximum
 
 
+class MFLDLT(_Factor):
+    """Bunch-Kaufman LDL^T factor (src/factorizations/ldlt.jl:1-63)."""
+    kind = "ldlt"
+
+    def __init__(self, factors, dsub: torch.Tensor, pivots: torch.Tensor, blocks: torch.Tensor,
+                 info, original_maximum: torch.Tensor):
+        super().__init__(factors, info)
+        self.dsub = dsub          # (N, n) float64 limb planes
+        self.pivots = pivots      # int64, 1-based
+        self.blocks = blocks      # uint8: 1 / 2 block start, 0 continuation
+        self.original_maximum = original_maximum
+
+
 def _read_info(dev_info: torch.Tensor) -> int:
     return int(dev_info.item())
 
@@ -533,6 +547,110 @@ def lu_(A: MFMatrix, check: bool = True, config: KernelConfig = _DEFAULT,
     if st > 0 and check:
         raise SingularException(st)
     return MFLU(A, ipiv, st, omax[:N].clone())
+
+
+def _ldlt_block_default(N: int, config: KernelConfig) -> int:
+    """src/factorizations/ldlt_tuning.jl:9-15"""
+    if config.ldlt_block > 0:
+        return config.ldlt_block
+    return 16 if N <= 2 else 12 if N == 3 else 8
+
+
+def ldlt_plan(N: int, n: int, config: KernelConfig = _DEFAULT) -> dict:
+    """Unblocked or lazy-blocked LDLT route (src/factorizations/ldlt.jl:329-350)."""
+    if not 1 <= N <= 4:
+        raise ArgumentError("only 1-4 limb MultiFloats are supported")
+    strategy = config.ldlt_strategy
+    if strategy not in ("auto", "unblocked", "blocked"):
+        raise ArgumentError("ldlt_strategy must be :auto, :unblocked, or :blocked")
+    block = max(_ldlt_block_default(N, config), 1)
+    if strategy == "unblocked":
+        return {"strategy": "unblocked", "reason": "forced_unblocked", "block_size": 1}
+    if strategy == "blocked":
+        return {"strategy": "blocked", "reason": "forced_blocked", "block_size": max(block, 2)}
+    use = block > 1 and n >= max(config.ldlt_blocked_crossover, 1)
+    return {"strategy": "blocked" if use else "unblocked",
+            "reason": "auto_above_crossover" if use else "auto_below_crossover",
+            "block_size": block if use else 1}
+
+
+def ldlt_(A: MFMatrix, check: bool = True, config: KernelConfig = _DEFAULT,
+          workspace=None) -> MFLDLT:
+    """Bunch-Kaufman LDL^T in place; the lower triangle is authoritative
+    (src/factorizations/ldlt.jl:654-717)."""
+    N = _same_type(A)
+    n = A.m
+    if A.n != n:
+        raise DimensionMismatch("ldlt! requires a square matrix")
+    plan = ldlt_plan(N, n, config)
+    dev = A.storage.device
+    info = torch.zeros(1, dtype=torch.int32, device=dev)
+    dsub = torch.zeros((N, max(n, 1)), dtype=torch.float64, device=dev)
+    pivots = torch.arange(1, n + 1, dtype=torch.int64, device=dev)
+    blocks = torch.zeros(max(n, 1), dtype=torch.uint8, device=dev)
+    omax = torch.zeros(N + 1, dtype=torch.float64, device=dev)
+    lib, h, s = _lib_h(A)
+    if n > 0:
+        _check(lib.mflab_max_abs(h, s, N, n, n, A.ptr(), A.ld, A.ls, 1, omax.data_ptr()), "ldlt!")
+    blocked = 1 if plan["strategy"] == "blocked" else 0
+    _check(lib.mflab_sytrf(h, s, N, n, A.ptr(), A.ld, A.ls, dsub.data_ptr(), dsub.shape[1],
+                           pivots.data_ptr() if n else None, blocks.data_ptr(), blocked,
+                           plan["block_size"], info.data_ptr()), "ldlt!")
+    st = _read_info(info)
+    if st == -1:
+        omax.zero_()
+        if check:
+            raise DomainError("ldlt!: input matrix contains non-finite entries")
+    if st > 0 and check:
+        raise SingularException(st)
+    return MFLDLT(A, dsub[:, :n], pivots[:n], blocks[:n], st, omax[:N].clone())
+
+
+def factor_blocks(F: MFLDLT) -> np.ndarray:
+    """caller-owned copy of the LDLT block markers (ldlt.jl:26-32)"""
+    return F.blocks.cpu().numpy().copy()
+
+
+def factor_permutation(F: MFLDLT) -> np.ndarray:
+    """final symmetric permutation p with A[p, p] = L D L^T, 1-based (ldlt.jl:34-63)"""
+    blocks = F.blocks.cpu().numpy()
+    piv = F.pivots.cpu().numpy()
+    n = len(blocks)
+    perm = np.arange(1, n + 1)
+    k = 0
+    while k < n:
+        b = blocks[k]
+        if b == 1:
+            p = piv[k] - 1
+            perm[k], perm[p] = perm[p], perm[k]
+            k += 1
+        elif b == 2 and k < n - 1:
+            p = piv[k] - 1
+            perm[k + 1], perm[p] = perm[p], perm[k + 1]
+            k += 2
+        elif b == 0:
+            break
+        else:
+            raise ArgumentError("invalid LDLT block structure")
+    return perm
+
+
+def _ldlt_diag_record(F: MFLDLT) -> np.ndarray:
+    N, A = F.N, F.factors
+    out = torch.zeros(6 + 4 * N, dtype=torch.float64, device=A.storage.device)
+    lib, h, s = _lib_h(A)
+    ds = F.dsub
+    _check(lib.mflab_ldlt_diagnostics(h, s, N, A.m, A.ptr(), A.ld, A.ls, ds.data_ptr(),
+                                      ds.stride(0) if ds.shape[0] > 1 else max(ds.shape[1], 1),
+                                      F.blocks.data_ptr(), F.original_maximum.data_ptr(),
+                                      out.data_ptr()), "factor_diagnostics")
+    return out.cpu().numpy()
+
+
+def factor_inertia(F: MFLDLT) -> dict:
+    """(positive, negative, zero) of the accepted blocks (diagnostics.jl:162-185)"""
+    r = _ldlt_diag_record(F)
+    return {"positive": int(r[0]), "negative": int(r[1]), "zero": int(r[2])}
 
 
 def issuccess(F: _Factor) -> bool:
@@ -622,7 +740,19 @@ def ldiv_(dest: MFMatrix, F: _Factor, source: Optional[MFMatrix] = None,
 
 
 def _ldiv_extra(dest, F, lib, h, s):
-    raise ArgumentError(f"ldiv! is not available for {F.kind}")
+    if F.kind != "ldlt":
+        raise ArgumentError(f"ldiv! is not available for {F.kind}")
+    N, L = F.N, F.factors
+    fail = torch.zeros(1, dtype=torch.int32, device=dest.storage.device)
+    ds = F.dsub
+    lsd = ds.stride(0) if ds.shape[0] > 1 else max(ds.shape[1], 1)
+    _check(lib.mflab_sytrs(h, s, N, L.m, dest.n, L.ptr(), L.ld, L.ls, ds.data_ptr(), lsd,
+                           F.pivots.data_ptr(), F.blocks.data_ptr(), dest.ptr(), dest.ld, dest.ls,
+                           fail.data_ptr()), "ldiv!")
+    f = int(fail.item())
+    if 0 < f < 0x7F7F7F7F:
+        raise SingularException(f)
+    return dest
 
 
 def solve(F: _Factor, rhs: MFMatrix, config: KernelConfig = _DEFAULT) -> MFMatrix:
@@ -690,7 +820,31 @@ def factor_diagnostics(F: _Factor) -> dict:
 
 
 def _diagnostics_extra(F, base):
-    raise ArgumentError(f"no diagnostics for {F.kind}")
+    if F.kind != "ldlt":
+        raise ArgumentError(f"no diagnostics for {F.kind}")
+    N = F.N
+    r = _ldlt_diag_record(F)
+    have = r[5] == 1.0
+    minb, maxe, scaled, growth = (r[6 + i * N:6 + (i + 1) * N].copy() for i in range(4))
+    omax = F.original_maximum.cpu().numpy()
+    omax_zero = not np.any(omax != 0)
+    A = F.factors
+    ds = F.dsub
+    dfin = True
+    if ds.shape[1] > 0:
+        dfin = bool(torch.isfinite(ds).all().item())
+    base.update({
+        "one_by_one_pivots": int(r[3]), "two_by_two_pivots": int(r[4]),
+        "pivots": F.pivots.cpu().numpy().copy(), "blocks": F.blocks.cpu().numpy().copy(),
+        "inertia": {"positive": int(r[0]), "negative": int(r[1]), "zero": int(r[2])},
+        "minimum_block_eigenvalue_magnitude": minb if have else None,
+        "minimum_scaled_block": None if (not have or omax_zero) else scaled,
+        "original_maximum": None if F.info == -1 else omax.copy(),
+        "maximum_block_entry": maxe,
+        "block_growth": None if omax_zero else growth,
+        "finite": _finite_region(A, 0) and dfin,
+    })
+    return base
 
 
 def capabilities(N: int) -> dict:
@@ -700,7 +854,8 @@ def capabilities(N: int) -> dict:
         "provider": "mfla_b200", "scalar_type": limb_type_name(N), "base_type": "Float64",
         "supported": supported, "limb_count": N,
         "gemm": supported, "gemmt": supported, "syrk": supported, "trsv": supported,
-        "trsm": supported, "cholesky": supported, "lu": supported,
+        "trsm": supported, "cholesky": supported, "lu": supported, "ldlt": supported,
+        "ldlt_lightweight_metadata": supported,
         "factor_diagnostics": supported, "vector_rhs": supported, "multi_rhs": supported,
         "factor_metadata_ownership": "factor_owned", "factor_matrix_ownership": "borrowed_input",
         "factorization_destructive": True, "factor_solve_mutates_factor": False,

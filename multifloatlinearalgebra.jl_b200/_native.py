@@ -71,6 +71,10 @@ SIGNATURES = {
     "mflab_getrf": [_vp, _vp, _int, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _vp],
     "mflab_getrs": [_vp, _vp, _int, _i64, _i64, _vp, _i64, _i64, _vp, _vp, _i64, _i64],
     "mflab_max_abs": [_vp, _vp, _int, _i64, _i64, _vp, _i64, _i64, _int, _vp],
+    "mflab_sytrf": [_vp, _vp, _int, _i64, _vp, _i64, _i64, _vp, _i64, _vp, _vp, _int, _i64, _vp],
+    "mflab_sytrs": [_vp, _vp, _int, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _vp, _vp, _vp, _i64,
+                    _i64, _vp],
+    "mflab_ldlt_diagnostics": [_vp, _vp, _int, _i64, _vp, _i64, _i64, _vp, _i64, _vp, _vp, _vp],
     "mflab_max_abs_noalloc": [_vp, _int, _i64, _i64, _vp, _i64, _i64, _int, _vp],
     "mflab_diag_summary": [_vp, _vp, _int, _vp, _i64, _i64, _i64, _vp, _vp, _vp],
     "mflab_probe_fp64": [_vp, _int, _int, _int, _i64, _vp, _d],
