@@ -116,6 +116,37 @@ int mflab_trsm(mflab_handle *h, void *stream, int limbs, int side, int uplo, int
                int64_t m, int64_t n, const double *A, int64_t lda, int64_t lsa, double *B,
                int64_t ldb, int64_t lsb, const double *alpha);
 
+/* ---------------------------------------------------------- residuals --- */
+/* R = B - A X (A m x k, X k x nrhs, B and R m x nrhs; R may equal B).
+   uplo: 0 general, 1 symmetric from the lower triangle, 2 from the upper
+   (m == k; the other triangle is never read).  vector_rhs selects the gemv!
+   accumulation network for Float64x3 (gemm! takes the fused route).
+   Replaces residual!(r, A, x, b; uplo) — src/residual.jl:55-125. */
+int mflab_residual(mflab_handle *h, void *stream, int limbs, int uplo, int vector_rhs, int64_t m,
+                   int64_t k, int64_t nrhs, const double *A, int64_t lda, int64_t lsa,
+                   const double *X, int64_t ldx, int64_t lsx, const double *B, int64_t ldb,
+                   int64_t lsb, double *R, int64_t ldr, int64_t lsr);
+
+/* R = B - A X with every operand widened from src_limbs (1 = binary64) to
+   res_limbs before the arithmetic; R has res_limbs planes.  Supported pairs:
+   1 -> 2/3/4, 2 -> 3/4, 3 -> 4.
+   Replaces residual_mixed!(r, A, x, b; uplo) — src/residual.jl:431-496 (which
+   has 2 -> 3/4 and 3 -> 4; binary64 sources serve the mixed-precision LU). */
+int mflab_residual_mixed(mflab_handle *h, void *stream, int src_limbs, int res_limbs, int uplo,
+                         int64_t m, int64_t k, int64_t nrhs, const double *A, int64_t lda,
+                         int64_t lsa, const double *X, int64_t ldx, int64_t lsx, const double *B,
+                         int64_t ldb, int64_t lsb, double *R, int64_t ldr, int64_t lsr);
+
+/* Normwise backward error ||r||inf / (||A||inf ||x||inf + ||b||inf) per
+   right-hand-side column in the scaled form of the reference (0 for a zero
+   denominator and zero residual, Inf otherwise, NaN for non-finite
+   authoritative inputs).  out (device): nrhs values of `limbs` doubles.
+   Replaces normwise_backward_error(A, x, b, r; uplo) — src/residual.jl:202-269. */
+int mflab_backward_error(mflab_handle *h, void *stream, int limbs, int uplo, int64_t m, int64_t k,
+                         int64_t nrhs, const double *A, int64_t lda, int64_t lsa, const double *X,
+                         int64_t ldx, int64_t lsx, const double *B, int64_t ldb, int64_t lsb,
+                         const double *R, int64_t ldr, int64_t lsr, double *out);
+
 /* ----------------------------------------------------- factorizations --- */
 /* Blocked lower Cholesky in place (block <= 32 columns; the reference default
    is 16).  Only the lower triangle is read or written.  *info (device int):

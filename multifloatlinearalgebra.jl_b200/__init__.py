@@ -37,6 +37,7 @@ __all__ = [
     "factor_provider", "factor_pivots", "factor_diagnostics",
     "MFCholesky", "MFLU", "capabilities", "limb_type_name",
     "ldlt_", "ldlt_plan", "MFLDLT", "factor_blocks", "factor_permutation", "factor_inertia",
+    "residual_", "residual_mixed_", "normwise_backward_error", "refinement_correction_",
 ]
 
 
@@ -847,6 +848,91 @@ def _diagnostics_extra(F, base):
     return base
 
 
+_UPLO_R = {"general": 0, "lower": 1, "upper": 2}
+
+
+def _check_residual_dims(R: MFMatrix, A: MFMatrix, X: MFMatrix, B: MFMatrix, uplo: str):
+    if uplo not in _UPLO_R:
+        raise ArgumentError("uplo must be :general, :lower, or :upper")
+    rows, cols = A.m, A.n
+    if (R.m, R.n) != (B.m, B.n):
+        raise DimensionMismatch("residual output dimensions differ")
+    if R.m != rows:
+        raise DimensionMismatch("residual output row count differs")
+    if X.m != cols:
+        raise DimensionMismatch("residual solution row count differs")
+    if X.n != R.n:
+        raise DimensionMismatch("residual right-hand-side count differs")
+    if uplo != "general" and rows != cols:
+        raise DimensionMismatch("symmetric residual requires a square matrix")
+
+
+def residual_(R: MFMatrix, A: MFMatrix, X: MFMatrix, B: MFMatrix, uplo: str = "general",
+              config: KernelConfig = _DEFAULT, workspace=None) -> MFMatrix:
+    """R = B - A X in caller-owned storage (src/residual.jl:55-125); R may be B."""
+    N = _same_type(R, A, X, B)
+    _check_residual_dims(R, A, X, B, uplo)
+    if _mightalias(R, X):
+        raise ArgumentError("residual output must not alias x")
+    if _mightalias(R, A):
+        raise ArgumentError("residual output must not alias A")
+    if R is not B and _mightalias(R, B) and not (R.storage.data_ptr() == B.storage.data_ptr()
+                                                  and (R.r0, R.c0) == (B.r0, B.c0)):
+        raise ArgumentError("residual output may equal b but must not partially alias it")
+    lib, h, s = _lib_h(R)
+    _check(lib.mflab_residual(h, s, N, _UPLO_R[uplo], int(R.is_vector), A.m, A.n, R.n, A.ptr(),
+                              A.ld, A.ls, X.ptr(), X.ld, X.ls, B.ptr(), B.ld, B.ls, R.ptr(), R.ld,
+                              R.ls), "residual!")
+    return R
+
+
+def residual_mixed_(R: MFMatrix, A: MFMatrix, X: MFMatrix, B: MFMatrix, uplo: str = "general",
+                    config: KernelConfig = _DEFAULT) -> MFMatrix:
+    """R = B - A X with every operand widened to R's limb count first
+    (src/residual.jl:431-496).  Source limbs 1 (binary64) to 3."""
+    src = A.N
+    for M in (X, B):
+        if M.N != src:
+            raise ArgumentError("residual_mixed! sources must share one limb count")
+    res = R.N
+    if not (1 <= src < res <= 4 and res >= 2):
+        raise ArgumentError("residual_mixed! supports only widening to a higher limb count")
+    _check_residual_dims(R, A, X, B, uplo)
+    lib, h, s = _lib_h(R)
+    _check(lib.mflab_residual_mixed(h, s, src, res, _UPLO_R[uplo], A.m, A.n, R.n, A.ptr(), A.ld,
+                                    A.ls, X.ptr(), X.ld, X.ls, B.ptr(), B.ld, B.ls, R.ptr(), R.ld,
+                                    R.ls), "residual_mixed!")
+    return R
+
+
+def normwise_backward_error(A: MFMatrix, X: MFMatrix, B: MFMatrix, R: MFMatrix,
+                            uplo: str = "general"):
+    """||r|| / (||A|| ||x|| + ||b||) (src/residual.jl:202-269): one N-limb value
+    for a vector, a list of them for a matrix right-hand side."""
+    N = _same_type(A, X, B, R)
+    _check_residual_dims(R, A, X, B, uplo)
+    out = torch.zeros(max(R.n, 1) * N, dtype=torch.float64, device=A.storage.device)
+    lib, h, s = _lib_h(A)
+    _check(lib.mflab_backward_error(h, s, N, _UPLO_R[uplo], A.m, A.n, R.n, A.ptr(), A.ld, A.ls,
+                                    X.ptr(), X.ld, X.ls, B.ptr(), B.ld, B.ls, R.ptr(), R.ld, R.ls,
+                                    out.data_ptr()), "normwise_backward_error")
+    vals = out.cpu().numpy().reshape(-1, N)[:R.n]
+    return vals[0].copy() if R.is_vector else [v.copy() for v in vals]
+
+
+def refinement_correction_(delta: MFMatrix, F: _Factor, r: MFMatrix,
+                           config: KernelConfig = _DEFAULT) -> MFMatrix:
+    """Exactly one correction delta = F \\ r (src/residual.jl:302-332)."""
+    _check_solve(F)
+    if (delta.m, delta.n) != (r.m, r.n):
+        raise DimensionMismatch("correction and residual dimensions differ")
+    if r.m != F.factors.m:
+        raise DimensionMismatch("correction residual rows differ from factor")
+    if _mightalias(delta, F.factors):
+        raise ArgumentError("correction destination must not alias factor storage")
+    return ldiv_(delta, F, None if delta is r else r, config)
+
+
 def capabilities(N: int) -> dict:
     """Machine-readable facts about this backend (src/capabilities.jl:14-74)."""
     supported = 2 <= N <= 4
@@ -861,4 +947,8 @@ def capabilities(N: int) -> dict:
         "factorization_destructive": True, "factor_solve_mutates_factor": False,
         "syrk_authoritative_triangle": "lower", "syrk_inactive_triangle": "preserved",
         "device": "cuda", "gemm_routes": ["auto", "direct", "fused", "ozaki"],
+        "residual": supported, "refinement_correction": supported,
+        "mixed_precision_residual": supported and N in (2, 3),
+        "mixed_residual_targets": {"x2": False, "x3": supported and N == 2,
+                                   "x4": supported and N in (2, 3)},
     }

@@ -71,6 +71,12 @@ SIGNATURES = {
     "mflab_getrf": [_vp, _vp, _int, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _vp],
     "mflab_getrs": [_vp, _vp, _int, _i64, _i64, _vp, _i64, _i64, _vp, _vp, _i64, _i64],
     "mflab_max_abs": [_vp, _vp, _int, _i64, _i64, _vp, _i64, _i64, _int, _vp],
+    "mflab_residual": [_vp, _vp, _int, _int, _int, _i64, _i64, _i64, _vp, _i64, _i64, _vp, _i64,
+                       _i64, _vp, _i64, _i64, _vp, _i64, _i64],
+    "mflab_residual_mixed": [_vp, _vp, _int, _int, _int, _i64, _i64, _i64, _vp, _i64, _i64, _vp,
+                             _i64, _i64, _vp, _i64, _i64, _vp, _i64, _i64],
+    "mflab_backward_error": [_vp, _vp, _int, _int, _i64, _i64, _i64, _vp, _i64, _i64, _vp, _i64,
+                             _i64, _vp, _i64, _i64, _vp, _i64, _i64, _vp],
     "mflab_sytrf": [_vp, _vp, _int, _i64, _vp, _i64, _i64, _vp, _i64, _vp, _vp, _int, _i64, _vp],
     "mflab_sytrs": [_vp, _vp, _int, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _vp, _vp, _vp, _i64,
                     _i64, _vp],

@@ -39,7 +39,9 @@ struct MMShape {
     static constexpr size_t smem_bytes = sizeof(double) * 2 * N * BK * (BM + BN);
 };
 
-template <int N, int BM, int BN, int BK, int TM, int TN, bool TA, bool TB, bool TRI, bool FUSED>
+// TA: 0 a(i,k) = A[i,k]; 1 a(i,k) = A[k,i]; 2 symmetric from the lower
+// triangle (k <= i ? A[i,k] : A[k,i]); 3 symmetric from the upper triangle.
+template <int N, int BM, int BN, int BK, int TM, int TN, int TA, bool TB, bool TRI, bool FUSED>
 __global__ void __launch_bounds__(MMShape<N, BM, BN, BK, TM, TN>::NT)
     mm_kernel(int64_t m, int64_t n, int64_t K, Mat A, Mat B, Mat C, scal<N> alpha, scal<N> beta,
               int overwrite, const int *info) {
@@ -63,7 +65,7 @@ __global__ void __launch_bounds__(MMShape<N, BM, BN, BK, TM, TN>::NT)
     auto load_tile = [&](int buf, int64_t k0) {
         for (int e = tid; e < BM * BK; e += NT) {
             int i, kk;
-            if (!TA) {
+            if (TA != 1) {
                 i = e % BM;
                 kk = e / BM;
             } else {
@@ -72,7 +74,8 @@ __global__ void __launch_bounds__(MMShape<N, BM, BN, BK, TM, TN>::NT)
             }
             int64_t gi = row0 + i, gk = k0 + kk;
             bool ok = gi < m && gk < K;
-            const double *src = ok ? (TA ? A.p + gi * A.ld + gk : A.p + gk * A.ld + gi) : A.p;
+            bool tr = TA == 1 || (TA == 2 && gk > gi) || (TA == 3 && gk < gi);
+            const double *src = ok ? (tr ? A.p + gi * A.ld + gk : A.p + gk * A.ld + gi) : A.p;
 #pragma unroll
             for (int l = 0; l < N; ++l)
                 cp_async8(&As[((buf * N + l) * BK + kk) * BM + i], src + (ok ? l * A.ls : 0), ok);
@@ -147,7 +150,7 @@ __global__ void __launch_bounds__(MMShape<N, BM, BN, BK, TM, TN>::NT)
     }
 }
 
-template <int N, int BM, int BN, int BK, int TM, int TN, bool TA, bool TB, bool TRI, bool FUSED>
+template <int N, int BM, int BN, int BK, int TM, int TN, int TA, bool TB, bool TRI, bool FUSED>
 static int run_mm(int64_t m, int64_t n, int64_t k, Mat A, Mat B, Mat C, const double *alpha,
                   const double *beta, cudaStream_t s, const int *info) {
     using S = MMShape<N, BM, BN, BK, TM, TN>;
@@ -174,7 +177,7 @@ static int run_mm(int64_t m, int64_t n, int64_t k, Mat A, Mat B, Mat C, const do
 }
 
 // tile shapes per limb count (FP64-issue bound; registers: TM*TN*N accumulators)
-template <int N, bool TA, bool TB, bool TRI, bool FUSED>
+template <int N, int TA, bool TB, bool TRI, bool FUSED>
 static int run_mm_n(int64_t m, int64_t n, int64_t k, Mat A, Mat B, Mat C, const double *alpha,
                     const double *beta, cudaStream_t s, const int *info) {
     if constexpr (N == 2)
@@ -186,20 +189,22 @@ static int run_mm_n(int64_t m, int64_t n, int64_t k, Mat A, Mat B, Mat C, const 
 }
 
 template <int N>
-static int dispatch_mm(bool ta, bool tb, int tri, bool fused3, int64_t m, int64_t n, int64_t k,
+static int dispatch_mm(int ta, bool tb, int tri, bool fused3, int64_t m, int64_t n, int64_t k,
                        Mat A, Mat B, Mat C, const double *alpha, const double *beta,
                        cudaStream_t s, const int *info) {
-    if (!ta && !tb && !tri) {
+    if (ta == 0 && !tb && !tri) {
         if (N == 3 && fused3)
-            return run_mm_n<N, false, false, false, true>(m, n, k, A, B, C, alpha, beta, s, info);
-        return run_mm_n<N, false, false, false, false>(m, n, k, A, B, C, alpha, beta, s, info);
+            return run_mm_n<N, 0, false, false, true>(m, n, k, A, B, C, alpha, beta, s, info);
+        return run_mm_n<N, 0, false, false, false>(m, n, k, A, B, C, alpha, beta, s, info);
     }
-    if (ta && !tb && tri) return run_mm_n<N, true, false, true, false>(m, n, k, A, B, C, alpha, beta, s, info);
-    if (!ta && tb && tri) return run_mm_n<N, false, true, true, false>(m, n, k, A, B, C, alpha, beta, s, info);
+    if (ta == 1 && !tb && tri) return run_mm_n<N, 1, false, true, false>(m, n, k, A, B, C, alpha, beta, s, info);
+    if (ta == 0 && tb && tri) return run_mm_n<N, 0, true, true, false>(m, n, k, A, B, C, alpha, beta, s, info);
+    if (ta == 2 && !tb && !tri) return run_mm_n<N, 2, false, false, false>(m, n, k, A, B, C, alpha, beta, s, info);
+    if (ta == 3 && !tb && !tri) return run_mm_n<N, 3, false, false, false>(m, n, k, A, B, C, alpha, beta, s, info);
     return MFLAB_ERR_UNSUPPORTED;
 }
 
-int launch_mm(int N, bool ta, bool tb, int tri, bool fused3, int64_t m, int64_t n, int64_t k,
+int launch_mm(int N, int ta, bool tb, int tri, bool fused3, int64_t m, int64_t n, int64_t k,
               Mat A, Mat B, Mat C, const double *alpha, const double *beta, cudaStream_t s,
               const int *info) {
     switch (N) {

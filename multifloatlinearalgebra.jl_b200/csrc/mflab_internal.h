@@ -16,9 +16,10 @@ struct Mat {
 };
 
 // Operand access of the shared multi-double mainloop.
-//   a(i,k) = ta ? A[k,i] : A[i,k];   b(k,j) = tb ? B[j,k] : B[k,j]
+//   a(i,k): ta 0 A[i,k], 1 A[k,i], 2 symmetric from the lower triangle,
+//           3 symmetric from the upper triangle;   b(k,j) = tb ? B[j,k] : B[k,j]
 // tri == 1 writes only C(i,j) with i >= j (SYRK / GEMMT lower triangle).
-int launch_mm(int N, bool ta, bool tb, int tri, bool fused3, int64_t m, int64_t n, int64_t k,
+int launch_mm(int N, int ta, bool tb, int tri, bool fused3, int64_t m, int64_t n, int64_t k,
               Mat A, Mat B, Mat C, const double *alpha, const double *beta, cudaStream_t s,
               const int *info = nullptr);
 

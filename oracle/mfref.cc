@@ -1267,6 +1267,32 @@ int mfr_sytrs(int N, int64_t n, int64_t nrhs, const double *A, int64_t lda, int6
     return 0;
 }
 
+/* ------------------------------------------------ mixed residual -------- */
+/* residual.jl:343-428: every operand widened from ns to nr limbs (zero limbs
+   appended), acc = B[i,j]; acc -= A[i,k] * X[k,j] for k ascending.  uplo 0
+   general, 1 lower, 2 upper (symmetric access to the authoritative triangle). */
+int mfr_residual_mixed(int ns, int nr, int uplo, int64_t m, int64_t k, int64_t nrhs,
+                       const double *A, int64_t lda, int64_t lsa, const double *X, int64_t ldx,
+                       int64_t lsx, const double *B, int64_t ldb, int64_t lsb, double *R,
+                       int64_t ldr, int64_t lsr) {
+    for (int64_t j = 0; j < nrhs; ++j)
+        for (int64_t i = 0; i < m; ++i) {
+            double acc[MAXN] = {0, 0, 0, 0};
+            for (int l = 0; l < ns; ++l) acc[l] = EL(B, ldb, lsb, i, j, l);
+            for (int64_t kk = 0; kk < k; ++kk) {
+                double a[MAXN] = {0, 0, 0, 0}, x[MAXN] = {0, 0, 0, 0};
+                int tr = (uplo == 1 && kk > i) || (uplo == 2 && kk < i);
+                for (int l = 0; l < ns; ++l) {
+                    a[l] = tr ? EL(A, lda, lsa, kk, i, l) : EL(A, lda, lsa, i, kk, l);
+                    x[l] = EL(X, ldx, lsx, kk, j, l);
+                }
+                mf_submul(nr, acc, a, x, acc);
+            }
+            for (int l = 0; l < nr; ++l) EL(R, ldr, lsr, i, j, l) = acc[l];
+        }
+    return 0;
+}
+
 /* ------------------------------------------- exact superaccumulator ----- */
 /* Kulisch-style fixed-point accumulator over the whole binary64 range: base
    2^32 digits held in int64 so that ~2^31 signed additions need no carry.

@@ -84,6 +84,8 @@ def lib():
         "mfr_exact_residual": [C.c_int, _i64, _i64, _d, _i64, _i64, _d, _i64, _i64, _d, _i64, _i64,
                                _d, _i64, C.c_int],
         "mfr_to_double": [C.c_int, _i64, _d, _i64, _d],
+        "mfr_residual_mixed": [C.c_int, C.c_int, C.c_int, _i64, _i64, _i64, _d, _i64, _i64, _d,
+                               _i64, _i64, _d, _i64, _i64, _d, _i64, _i64],
         "mfr_max_threads": [],
     }
     for name_, args in sig.items():
@@ -335,6 +337,16 @@ def exact_residual(A, X, B, nthreads=None):
     lib().mfr_exact_residual(Ap.N, n, nrhs, Ap.ptr(), Ap.ld, Ap.ls, Xp.ptr(), Xp.ld, Xp.ls,
                              Bp.ptr(), Bp.ld, Bp.ls, _p(R), n, nthreads or threads())
     return R.T.copy()
+
+
+def residual_mixed(A, X, B, res_limbs, uplo="general"):
+    """residual.jl:431-496 restated: R = B - A X widened to res_limbs limbs"""
+    Ap, Xp, Bp = Planes(A), Planes(X), Planes(B)
+    Rp = Planes(np.zeros((res_limbs, Bp.m, Bp.n)))
+    up = {"general": 0, "lower": 1, "upper": 2}[uplo]
+    lib().mfr_residual_mixed(Ap.N, res_limbs, up, Ap.m, Ap.n, Xp.n, Ap.ptr(), Ap.ld, Ap.ls,
+                             Xp.ptr(), Xp.ld, Xp.ls, Bp.ptr(), Bp.ld, Bp.ls, Rp.ptr(), Rp.ld, Rp.ls)
+    return Rp.array()
 
 
 def to_double(X):
