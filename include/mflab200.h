@@ -137,6 +137,14 @@ int mflab_residual_mixed(mflab_handle *h, void *stream, int src_limbs, int res_l
                          int64_t lsa, const double *X, int64_t ldx, int64_t lsx, const double *B,
                          int64_t ldb, int64_t lsb, double *R, int64_t ldr, int64_t lsr);
 
+/* X <- X + widen(D): adds a src_limbs-limb correction (1 = binary64) to a
+   dst_limbs-limb solution with the add network (the update step of iterative
+   refinement; the reference leaves that loop to the caller,
+   docs/SOLVER_BACKEND_CONTRACT.md:1-6).  m x n, 1 <= src < dst <= 4. */
+int mflab_add_widened(mflab_handle *h, void *stream, int src_limbs, int dst_limbs, int64_t m,
+                      int64_t n, const double *D, int64_t ldd, int64_t lsd, double *X, int64_t ldx,
+                      int64_t lsx);
+
 /* Normwise backward error ||r||inf / (||A||inf ||x||inf + ||b||inf) per
    right-hand-side column in the scaled form of the reference (0 for a zero
    denominator and zero residual, Inf otherwise, NaN for non-finite
@@ -163,7 +171,8 @@ int mflab_potrs(mflab_handle *h, void *stream, int limbs, int64_t n, int64_t nrh
 
 /* Blocked partial-pivoting LU in place; ipiv (device, min(m,n) int64,
    1-based) records the row swapped with row k at step k.  *info: 0, -1
-   non-finite input, k > 0 exactly zero pivot at column k.
+   non-finite input, k > 0 exactly zero pivot at column k.  limbs may also be 1
+   (plain binary64, the factor of the mixed-precision solver).
    Replaces lu!(A; check=false, config) — src/factorizations/lu.jl:128-195. */
 int mflab_getrf(mflab_handle *h, void *stream, int limbs, int64_t m, int64_t n, double *A,
                 int64_t lda, int64_t lsa, int64_t *ipiv, int64_t block, int *info);
@@ -208,6 +217,32 @@ int mflab_sytrs(mflab_handle *h, void *stream, int limbs, int64_t n, int64_t nrh
 int mflab_ldlt_diagnostics(mflab_handle *h, void *stream, int limbs, int64_t n, const double *F,
                            int64_t ldf, int64_t lsf, const double *dsub, int64_t lsd,
                            const uint8_t *blocks, const double *omax, double *out);
+
+/* ------------------------------------------------------- batched SPD --- */
+/* Factor (and with solve != 0 also solve) nblocks independent SPD blocks in
+   one persistent launch.  Block b is sizes[b] x sizes[b], column-major at
+   S + offsets[b] (ld = sizes[b]), its right-hand side a vector at X +
+   boffsets[b]; limb planes are ls_s / ls_x apart.  CTAs take blocks in the
+   order order[0..nblocks) from the device counter (reset here with one
+   stream-ordered memset).  Each block follows cholesky!(S_b; block) and
+   ldiv!(x_b, F_b) exactly; info[b] receives 0 or the failing column.
+   max_size <= 512.  grid <= 0 picks 4 CTAs per SM.  No allocation, no
+   synchronisation.  No reference counterpart (the reference factors one
+   matrix per call: src/factorizations/cholesky.jl:68-107). */
+int mflab_spd_batched(mflab_handle *h, void *stream, int limbs, int64_t nblocks, int64_t max_size,
+                      const int64_t *sizes, const int64_t *offsets, const int64_t *boffsets,
+                      const int64_t *order, double *S, int64_t ls_s, double *X, int64_t ls_x,
+                      int64_t block, int solve, int *info, int *counter, int grid);
+
+/* Adjoint of x_b = S_b^{-1} b_b reusing the factors of mflab_spd_batched: XB
+   holds xbar on entry and bbar = S^{-1} xbar on exit; SB (packed like S)
+   receives Sbar = -(bbar x^T + x bbar^T) / 2.  Blocks with info != 0 are
+   skipped.  No reference counterpart. */
+int mflab_spd_batched_adjoint(mflab_handle *h, void *stream, int limbs, int64_t nblocks,
+                              int64_t max_size, const int64_t *sizes, const int64_t *offsets,
+                              const int64_t *boffsets, const int64_t *order, const double *L,
+                              int64_t ls_s, const double *X, double *XB, int64_t ls_x, double *SB,
+                              const int *info, int *counter, int grid);
 
 /* ------------------------------------------------------- diagnostics --- */
 /* out (device, limbs+1 doubles) = [max |A(r,c)| over the region, finite flag]

@@ -38,6 +38,7 @@ __all__ = [
     "MFCholesky", "MFLU", "capabilities", "limb_type_name",
     "ldlt_", "ldlt_plan", "MFLDLT", "factor_blocks", "factor_permutation", "factor_inertia",
     "residual_", "residual_mixed_", "normwise_backward_error", "refinement_correction_",
+    "solve_mixed_lu", "batched",
 ]
 
 
@@ -933,6 +934,68 @@ def refinement_correction_(delta: MFMatrix, F: _Factor, r: MFMatrix,
     return ldiv_(delta, F, None if delta is r else r, config)
 
 
+def _leading_limb(X: MFMatrix) -> MFMatrix:
+    """the binary64 rounding of a normalised multi-double matrix (its leading
+    limb) as a one-limb matrix"""
+    st = X.planes()[0:1].contiguous().clone()
+    if st.shape[2] == 0:
+        st = torch.zeros((1, X.n, 1), dtype=torch.float64, device=X.storage.device)
+    return MFMatrix(st, 0, 0, X.m, X.n, X.is_vector)
+
+
+def solve_mixed_lu(A: MFMatrix, B: MFMatrix, tol: float = 0.0, maxiter: int = 40,
+                   config: KernelConfig = _DEFAULT) -> tuple:
+    """Solve A X = B for a Float64xN matrix A with a binary64 partial-pivoting
+    LU of round(A) and iterative refinement with Float64xN residuals.
+
+    Each iteration: D = LU64 \\ round(R) in binary64 (getrs), X += D in
+    Float64xN, R = B - A X with residual!, then the normwise backward error of
+    every column.  Stops when all backward errors are <= tol (default
+    2^(-53N)) or after maxiter iterations.  Returns (X, report).  The
+    reference provides the pieces (lu!, residual!, refinement_correction!) but
+    leaves the refinement loop to the caller (docs/SOLVER_BACKEND_CONTRACT.md).
+    """
+    N = _same_type(A, B)
+    n = A.m
+    if A.n != n:
+        raise DimensionMismatch("solve requires a square matrix")
+    if B.m != n:
+        raise DimensionMismatch("right-hand side dimensions differ")
+    tol = tol or 2.0 ** (-53 * N)
+    dev = A.storage.device
+    lib, h, s = _lib_h(A)
+    LU = _leading_limb(A)
+    ipiv = torch.arange(1, n + 1, dtype=torch.int64, device=dev)
+    info = torch.zeros(1, dtype=torch.int32, device=dev)
+    _check(lib.mflab_getrf(h, s, 1, n, n, LU.ptr(), LU.ld, LU.ls, ipiv.data_ptr() if n else None,
+                           max(config.lu_block, 1), info.data_ptr()), "lu! (binary64)")
+    st = _read_info(info)
+    if st == -1:
+        raise DomainError("lu!: input matrix contains non-finite entries")
+    if st > 0:
+        raise SingularException(st)
+    X = MFMatrix.zeros(N, n, None if B.is_vector else B.n, device=dev)
+    R = B.copy()
+    history = []
+    it = 0
+    for it in range(1, maxiter + 1):
+        D = _leading_limb(R)
+        _check(lib.mflab_getrs(h, s, 1, n, D.n, LU.ptr(), LU.ld, LU.ls, ipiv.data_ptr(), D.ptr(),
+                               D.ld, D.ls), "ldiv! (binary64)")
+        _check(lib.mflab_add_widened(h, s, 1, N, n, X.n, D.ptr(), D.ld, D.ls, X.ptr(), X.ld,
+                                     X.ls), "refinement update")
+        residual_(R, A, X, B)
+        be = normwise_backward_error(A, X, B, R)
+        worst = float(np.max([v[0] for v in (be if isinstance(be, list) else [be])]))
+        history.append(worst)
+        if worst <= tol:
+            break
+    report = {"iterations": it, "backward_error": history[-1] if history else None,
+              "history": history, "converged": bool(history) and history[-1] <= tol,
+              "factor": "binary64 partial-pivoting LU", "residual": limb_type_name(N)}
+    return X, report
+
+
 def capabilities(N: int) -> dict:
     """Machine-readable facts about this backend (src/capabilities.jl:14-74)."""
     supported = 2 <= N <= 4
@@ -952,3 +1015,6 @@ def capabilities(N: int) -> dict:
         "mixed_residual_targets": {"x2": False, "x3": supported and N == 2,
                                    "x4": supported and N in (2, 3)},
     }
+
+
+from . import batched  # noqa: E402  (batched SPD factor/solve and its adjoint)

@@ -77,6 +77,11 @@ SIGNATURES = {
                              _i64, _i64, _vp, _i64, _i64, _vp, _i64, _i64],
     "mflab_backward_error": [_vp, _vp, _int, _int, _i64, _i64, _i64, _vp, _i64, _i64, _vp, _i64,
                              _i64, _vp, _i64, _i64, _vp, _i64, _i64, _vp],
+    "mflab_add_widened": [_vp, _vp, _int, _int, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _i64],
+    "mflab_spd_batched": [_vp, _vp, _int, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _i64, _vp, _i64,
+                          _i64, _int, _vp, _vp, _int],
+    "mflab_spd_batched_adjoint": [_vp, _vp, _int, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _i64, _vp,
+                                  _vp, _i64, _vp, _vp, _vp, _int],
     "mflab_sytrf": [_vp, _vp, _int, _i64, _vp, _i64, _i64, _vp, _i64, _vp, _vp, _int, _i64, _vp],
     "mflab_sytrs": [_vp, _vp, _int, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _vp, _vp, _vp, _i64,
                     _i64, _vp],

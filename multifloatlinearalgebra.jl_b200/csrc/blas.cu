@@ -180,7 +180,9 @@ static int run_mm(int64_t m, int64_t n, int64_t k, Mat A, Mat B, Mat C, const do
 template <int N, int TA, bool TB, bool TRI, bool FUSED>
 static int run_mm_n(int64_t m, int64_t n, int64_t k, Mat A, Mat B, Mat C, const double *alpha,
                     const double *beta, cudaStream_t s, const int *info) {
-    if constexpr (N == 2)
+    if constexpr (N == 1)
+        return run_mm<1, 64, 64, 16, 4, 4, TA, TB, TRI, FUSED>(m, n, k, A, B, C, alpha, beta, s, info);
+    else if constexpr (N == 2)
         return run_mm<2, 64, 64, 16, 4, 4, TA, TB, TRI, FUSED>(m, n, k, A, B, C, alpha, beta, s, info);
     else if constexpr (N == 3)
         return run_mm<3, 64, 64, 8, 4, 4, TA, TB, TRI, FUSED>(m, n, k, A, B, C, alpha, beta, s, info);
@@ -208,6 +210,10 @@ int launch_mm(int N, int ta, bool tb, int tri, bool fused3, int64_t m, int64_t n
               Mat A, Mat B, Mat C, const double *alpha, const double *beta, cudaStream_t s,
               const int *info) {
     switch (N) {
+    case 1:
+        if (ta == 0 && !tb && !tri)
+            return run_mm_n<1, 0, false, false, false>(m, n, k, A, B, C, alpha, beta, s, info);
+        return MFLAB_ERR_UNSUPPORTED;
     case 2: return dispatch_mm<2>(ta, tb, tri, fused3, m, n, k, A, B, C, alpha, beta, s, info);
     case 3: return dispatch_mm<3>(ta, tb, tri, fused3, m, n, k, A, B, C, alpha, beta, s, info);
     case 4: return dispatch_mm<4>(ta, tb, tri, fused3, m, n, k, A, B, C, alpha, beta, s, info);

@@ -421,7 +421,7 @@ extern "C" int mflab_potrs(mflab_handle *h, void *stream, int limbs, int64_t n, 
 extern "C" int mflab_getrf(mflab_handle *h, void *stream, int limbs, int64_t m, int64_t n,
                            double *A, int64_t lda, int64_t lsa, int64_t *ipiv, int64_t block,
                            int *info) {
-    if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
+    if (!h || !(limbs == 1 || mfl::valid_limbs(limbs))) return MFLAB_ERR_UNSUPPORTED;
     if (m < 0 || n < 0 || (m > 0 && lda < m) || !info || (m > 0 && n > 0 && !ipiv))
         return MFLAB_ERR_ARG;
     if (block < 1) block = 1;
@@ -435,6 +435,7 @@ extern "C" int mflab_getrf(mflab_handle *h, void *stream, int limbs, int64_t m, 
         if (rc) return rc;
     }
     switch (limbs) {
+    case 1: return mfl::getrf_n<1>(m, n, a, ipiv, block, info, s);
     case 2: return mfl::getrf_n<2>(m, n, a, ipiv, block, info, s);
     case 3: return mfl::getrf_n<3>(m, n, a, ipiv, block, info, s);
     default: return mfl::getrf_n<4>(m, n, a, ipiv, block, info, s);
@@ -444,7 +445,7 @@ extern "C" int mflab_getrf(mflab_handle *h, void *stream, int limbs, int64_t m, 
 extern "C" int mflab_getrs(mflab_handle *h, void *stream, int limbs, int64_t n, int64_t nrhs,
                            const double *LU, int64_t ldl, int64_t lsl, const int64_t *ipiv,
                            double *B, int64_t ldb, int64_t lsb) {
-    if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
+    if (!h || !(limbs == 1 || mfl::valid_limbs(limbs))) return MFLAB_ERR_UNSUPPORTED;
     if (n < 0 || nrhs < 0 || (n > 0 && (ldl < n || ldb < n || !ipiv))) return MFLAB_ERR_ARG;
     if (n == 0 || nrhs == 0) return MFLAB_OK;
     const double one[4] = {1.0, 0.0, 0.0, 0.0};
@@ -452,6 +453,7 @@ extern "C" int mflab_getrs(mflab_handle *h, void *stream, int limbs, int64_t n, 
     Mat a{(double *)LU, ldl, lsl}, b{B, ldb, lsb};
     unsigned g = (unsigned)((nrhs + 127) / 128);
     switch (limbs) {
+    case 1: mfl::apply_pivots_kernel<1><<<g, 128, 0, s>>>(nrhs, b, ipiv, n, 0); break;
     case 2: mfl::apply_pivots_kernel<2><<<g, 128, 0, s>>>(nrhs, b, ipiv, n, 0); break;
     case 3: mfl::apply_pivots_kernel<3><<<g, 128, 0, s>>>(nrhs, b, ipiv, n, 0); break;
     default: mfl::apply_pivots_kernel<4><<<g, 128, 0, s>>>(nrhs, b, ipiv, n, 0); break;

@@ -55,6 +55,16 @@ __device__ __forceinline__ void two_prod(double a, double b, double &p, double &
 #define MFL_TS(a, b) two_sum((a), (b), (a), (b))
 #define MFL_FTS(a, b) fast_two_sum((a), (b), (a), (b))
 
+// --------------------------------------------------- x1 (plain binary64) ---
+// The binary64 instance of the kernels serves the FP64 factor of the
+// mixed-precision LU solver; it has no reference counterpart.
+__device__ __forceinline__ mf<1> add(const mf<1> &x, const mf<1> &y) {
+    return mf<1>{{__dadd_rn(x.v[0], y.v[0])}};
+}
+__device__ __forceinline__ mf<1> mul(const mf<1> &x, const mf<1> &y) {
+    return mf<1>{{__dmul_rn(x.v[0], y.v[0])}};
+}
+
 // ------------------------------------------------------------------ x2 ---
 __device__ __forceinline__ mf<2> add(const mf<2> &x, const mf<2> &y) {
     double sh = x.v[0], sl = y.v[0], th = x.v[1], tl = y.v[1];
@@ -345,6 +355,10 @@ __device__ __forceinline__ mf<N> div(const mf<N> &x, const mf<N> &y) {
     return acc;
 }
 
+__device__ __forceinline__ mf<1> div(const mf<1> &x, const mf<1> &y) {
+    return mf<1>{{__ddiv_rn(x.v[0], y.v[0])}};
+}
+
 template <int N>
 __device__ __forceinline__ mf<N> inv(const mf<N> &x) {
     return div(from_double<N>(1.0), x);
@@ -362,6 +376,8 @@ __device__ __forceinline__ mf<N> sqrt_mf(const mf<N> &x) {
     }
     return s;
 }
+
+__device__ __forceinline__ mf<1> sqrt_mf(const mf<1> &x) { return mf<1>{{__dsqrt_rn(x.v[0])}}; }
 
 // ----------------------------------------------------- plane access -------
 // A Float64xN matrix is N column-major planes: limb l of (r, c) is

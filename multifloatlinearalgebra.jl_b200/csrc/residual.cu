@@ -313,3 +313,36 @@ extern "C" int mflab_backward_error(mflab_handle *h, void *stream, int limbs, in
     }
     return mfl::record_cuda_error(cudaGetLastError(), "backward error");
 }
+
+namespace mfl {
+// X <- X + widen(D): the correction step of iterative refinement
+template <int NS, int NR>
+__global__ void add_widened_kernel(int64_t m, int64_t n, Mat D, Mat X) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= m * n) return;
+    const int64_t r = e % m, c = e / m;
+    store_mf<NR>(X.p, X.ld, X.ls, r, c,
+                 add(load_mf<NR>(X.p, X.ld, X.ls, r, c), widen<NS, NR>(D.p, D.ld, D.ls, r, c)));
+}
+}  // namespace mfl
+
+extern "C" int mflab_add_widened(mflab_handle *h, void *stream, int src_limbs, int dst_limbs,
+                                 int64_t m, int64_t n, const double *D, int64_t ldd, int64_t lsd,
+                                 double *X, int64_t ldx, int64_t lsx) {
+    if (!h) return MFLAB_ERR_UNSUPPORTED;
+    if (m < 0 || n < 0) return MFLAB_ERR_ARG;
+    if (m == 0 || n == 0) return MFLAB_OK;
+    Mat d{(double *)D, ldd, lsd}, x{X, ldx, lsx};
+    cudaStream_t s = (cudaStream_t)stream;
+    const unsigned g = (unsigned)((m * n + 255) / 256);
+    switch (src_limbs * 10 + dst_limbs) {
+    case 12: mfl::add_widened_kernel<1, 2><<<g, 256, 0, s>>>(m, n, d, x); break;
+    case 13: mfl::add_widened_kernel<1, 3><<<g, 256, 0, s>>>(m, n, d, x); break;
+    case 14: mfl::add_widened_kernel<1, 4><<<g, 256, 0, s>>>(m, n, d, x); break;
+    case 23: mfl::add_widened_kernel<2, 3><<<g, 256, 0, s>>>(m, n, d, x); break;
+    case 24: mfl::add_widened_kernel<2, 4><<<g, 256, 0, s>>>(m, n, d, x); break;
+    case 34: mfl::add_widened_kernel<3, 4><<<g, 256, 0, s>>>(m, n, d, x); break;
+    default: return MFLAB_ERR_UNSUPPORTED;
+    }
+    return mfl::record_cuda_error(cudaGetLastError(), "add_widened");
+}

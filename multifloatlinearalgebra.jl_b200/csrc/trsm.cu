@@ -180,6 +180,7 @@ static int run_trsm(int side, int uplo, int trans, int diag, int64_t m, int64_t 
 int launch_trsm_info(int N, int side, int uplo, int trans, int diag, int64_t m, int64_t n, Mat A,
                      Mat B, const double *alpha, cudaStream_t s, const int *info) {
     switch (N) {
+    case 1: return run_trsm<1>(side, uplo, trans, diag, m, n, A, B, alpha, s, info);
     case 2: return run_trsm<2>(side, uplo, trans, diag, m, n, A, B, alpha, s, info);
     case 3: return run_trsm<3>(side, uplo, trans, diag, m, n, A, B, alpha, s, info);
     case 4: return run_trsm<4>(side, uplo, trans, diag, m, n, A, B, alpha, s, info);

@@ -74,3 +74,42 @@ def spd_matrix(rng: np.random.Generator, N: int, n: int, gemm) -> np.ndarray:
     S = gemm(R, np.ascontiguousarray(R.transpose(0, 2, 1)))
     S[0] += n * np.eye(n)
     return _renorm_np(S)
+
+
+def _two_prod_torch(a: torch.Tensor, b: torch.Tensor):
+    """exact a*b = p + e with Veltkamp splitting (elementwise IEEE operations)"""
+    c = 134217729.0
+    p = a * b
+    ta = c * a
+    ah = ta - (ta - a)
+    al = a - ah
+    tb = c * b
+    bh = tb - (tb - b)
+    bl = b - bh
+    e = ((ah * bh - p) + ah * bl + al * bh) + al * bl
+    return p, e
+
+
+def mixed_lu_problem(mf, n: int, nrhs: int, seed: int = 4, N: int = 4, device: int = 0):
+    """A = U diag(sigma) V^T with U, V orthogonal (QR of randn), sigma geometric
+    from 1 to 1e-12, lifted to Float64xN: W = diag(sigma) V^T exactly (two
+    limbs, exact products), A = U W with the multi-double GEMM.  B = randn.
+    Returns device MFMatrix objects (A, B)."""
+    g = torch.Generator(device=f"cuda:{device}")
+    g.manual_seed(seed)
+    dev = f"cuda:{device}"
+    U, _ = torch.linalg.qr(torch.randn((n, n), dtype=torch.float64, device=dev, generator=g))
+    V, _ = torch.linalg.qr(torch.randn((n, n), dtype=torch.float64, device=dev, generator=g))
+    sigma = torch.logspace(0.0, -12.0, n, dtype=torch.float64, device=dev)
+    # W = diag(sigma) V^T, column-major planes (N, n, n): W[i, j] = sigma_i V[j, i]
+    p, e = _two_prod_torch(sigma[:, None], V.t().contiguous())
+    Wp = torch.zeros((N, n, n), dtype=torch.float64, device=dev)
+    Wp[0] = p.t()
+    Wp[1] = e.t()
+    Up = torch.zeros((N, n, n), dtype=torch.float64, device=dev)
+    Up[0] = U.t()
+    A = mf.MFMatrix.zeros(N, n, n, device=device)
+    mf.gemm_(A, mf.MFMatrix.from_tensor(Up), mf.MFMatrix.from_tensor(Wp))
+    Bp = torch.zeros((N, nrhs, n), dtype=torch.float64, device=dev)
+    Bp[0].normal_(generator=g)
+    return A, mf.MFMatrix.from_tensor(Bp)

@@ -1,0 +1,171 @@
+"""Batched SPD factor + solve in one persistent launch, its CUDA-graph replay
+and its adjoint (finite differences in Float64x4 and an mpmath reference
+gradient)."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import assert_bitwise
+from test_oracle import syn
+
+pytestmark = pytest.mark.gpu
+
+
+def _spd_blocks(ref, rng, N, sizes):
+    out = []
+    for n in sizes:
+        S = syn.spd_matrix(rng, N, int(n), ref.gemm)
+        out.append(np.tril(S) + np.transpose(np.tril(S, -1), (0, 2, 1)))
+    return out
+
+
+@pytest.mark.parametrize("N", [2, 3, 4])
+def test_batched_matches_single_block_oracle(mf, ref, rng, N):
+    sizes = rng.integers(1, 70, 23)
+    sizes[3] = 300  # one block larger than the CTA (two rows per thread)
+    blocks = _spd_blocks(ref, rng, N, sizes)
+    rhs = [syn.randn_mf(rng, N, int(n), 1)[:, :, 0] for n in sizes]
+    batch = mf.batched.SPDBatch(N, sizes)
+    for i, (S, b) in enumerate(zip(blocks, rhs)):
+        batch.set_block(i, S)
+        batch.set_rhs(i, b)
+    info = mf.batched.potrf_potrs_batched_(batch)
+    assert np.all(info == 0)
+    for i, (S, b) in enumerate(zip(blocks, rhs)):
+        L, inf = ref.potrf(S)
+        assert inf == 0
+        assert_bitwise(np.tril(batch.block(i)), np.tril(L), f"factor {i}")
+        assert_bitwise(batch.rhs(i), ref.potrs(L, b[:, :, None])[:, :, 0], f"solve {i}")
+
+
+def test_batched_failure_is_per_block(mf, ref, rng):
+    N = 2
+    sizes = np.array([5, 6, 7])
+    blocks = _spd_blocks(ref, rng, N, sizes)
+    blocks[1][0, 2, 2] = -50.0  # not positive definite at column 3
+    batch = mf.batched.SPDBatch(N, sizes)
+    for i, S in enumerate(blocks):
+        batch.set_block(i, S)
+        batch.set_rhs(i, np.ones((N, sizes[i])))
+    info = mf.batched.potrf_potrs_batched_(batch, check=False)
+    assert info[0] == 0 and info[2] == 0 and info[1] > 0
+    _, want = ref.potrf(blocks[1])
+    assert info[1] == want
+    with pytest.raises(mf.PosDefException):
+        b2 = mf.batched.SPDBatch(N, sizes)
+        for i, S in enumerate(blocks):
+            b2.set_block(i, S)
+        mf.batched.potrf_potrs_batched_(b2)
+
+
+def test_batched_graph_replay(mf, ref, rng):
+    N = 2
+    sizes = rng.integers(8, 40, 50)
+    blocks = _spd_blocks(ref, rng, N, sizes)
+    rhs = [syn.randn_mf(rng, N, int(n), 1)[:, :, 0] for n in sizes]
+    batch = mf.batched.SPDBatch(N, sizes)
+
+    def load():
+        for i, (S, b) in enumerate(zip(blocks, rhs)):
+            batch.set_block(i, S)
+            batch.set_rhs(i, b)
+
+    load()
+    torch.cuda.synchronize()
+    g = mf.batched.BatchedSPDGraph(batch)
+    load()  # capture does not run the kernel; refresh and replay twice
+    torch.cuda.synchronize()
+    g.replay()
+    torch.cuda.synchronize()
+    first = batch.X.clone()
+    load()
+    torch.cuda.synchronize()
+    g.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(first, batch.X)
+    for i in (0, 17, 49):
+        L, _ = ref.potrf(blocks[i])
+        assert_bitwise(batch.rhs(i), ref.potrs(L, rhs[i][:, :, None])[:, :, 0])
+
+
+def _loss_x4(ref, S, b, w):
+    L, info = ref.potrf(S)
+    assert info == 0
+    x = ref.potrs(L, b[:, :, None])[:, :, 0]
+    return ref.to_double(ref.mul_n(x, w)).sum(), x
+
+
+def test_batched_adjoint_vs_finite_differences_x4(mf, ref, rng):
+    """central differences of loss = sum_i <w_i, x_i> in Float64x4"""
+    N = 4
+    sizes = np.array([4, 6, 5])
+    blocks = _spd_blocks(ref, rng, N, sizes)
+    rhs = [syn.randn_mf(rng, N, int(n), 1)[:, :, 0] for n in sizes]
+    ws = [syn.randn_mf(rng, N, int(n), 1)[:, :, 0] for n in sizes]
+    batch = mf.batched.SPDBatch(N, sizes)
+    for i, (S, b) in enumerate(zip(blocks, rhs)):
+        batch.set_block(i, S)
+        batch.set_rhs(i, b)
+    x, pullback = mf.batched.solve_spd_batched_rrule(batch)
+    wbuf = torch.zeros_like(x)
+    for i, w in enumerate(ws):
+        o = int(batch.boffsets_host[i])
+        wbuf[:, o:o + sizes[i]] = torch.from_numpy(w).cuda()
+    sb, bb = pullback(wbuf)
+    h = 1e-24
+    for i in range(len(sizes)):
+        S, b, w = blocks[i], rhs[i], ws[i]
+        n = sizes[i]
+        Sbar = ref.to_double(batch.block(i, sb))
+        bbar = ref.to_double(batch.rhs(i, bb))
+        # d/db_j
+        for j in range(n):
+            bp, bm = b.copy(), b.copy()
+            bp[:, j] = ref.add(b[:, j], np.array([h, 0, 0, 0]))
+            bm[:, j] = ref.add(b[:, j], np.array([-h, 0, 0, 0]))
+            fd = (_loss_x4(ref, S, bp, w)[0] - _loss_x4(ref, S, bm, w)[0]) / (2 * h)
+            assert abs(fd - bbar[j]) <= 1e-12 * max(1.0, abs(bbar[j]))
+        # symmetric perturbation of S_jk and S_kj
+        for (j, k) in [(0, 0), (1, 0), (n - 1, 2), (n - 1, n - 1)]:
+            E = np.zeros((N, n, n))
+            E[0, j, k] = h
+            E[0, k, j] = h
+            Sp, Sm = ref.add_n(S, E), ref.add_n(S, -E)
+            fd = (_loss_x4(ref, Sp, b, w)[0] - _loss_x4(ref, Sm, b, w)[0]) / (2 * h)
+            want = Sbar[j, k] if j == k else Sbar[j, k] + Sbar[k, j]
+            assert abs(fd - want) <= 1e-12 * max(1.0, abs(want))
+
+
+def test_batched_adjoint_vs_mpmath_gradient(mf, ref, rng):
+    """Float64x2 gradient against a 300-digit mpmath gradient"""
+    import mpmath
+    N = 2
+    sizes = np.array([5, 8])
+    blocks = _spd_blocks(ref, rng, N, sizes)
+    rhs = [syn.randn_mf(rng, N, int(n), 1)[:, :, 0] for n in sizes]
+    ws = [syn.randn_mf(rng, N, int(n), 1)[:, :, 0] for n in sizes]
+    batch = mf.batched.SPDBatch(N, sizes)
+    for i, (S, b) in enumerate(zip(blocks, rhs)):
+        batch.set_block(i, S)
+        batch.set_rhs(i, b)
+    x, pullback = mf.batched.solve_spd_batched_rrule(batch)
+    wbuf = torch.zeros_like(x)
+    for i, w in enumerate(ws):
+        o = int(batch.boffsets_host[i])
+        wbuf[:, o:o + sizes[i]] = torch.from_numpy(w).cuda()
+    sb, bb = pullback(wbuf)
+    mpmath.mp.dps = 300
+    mpv = lambda limbs: sum(mpmath.mpf(float(v)) for v in limbs)
+    for i, n in enumerate(sizes):
+        S = mpmath.matrix([[mpv(blocks[i][:, r, c]) for c in range(n)] for r in range(n)])
+        b = mpmath.matrix([mpv(rhs[i][:, r]) for r in range(n)])
+        w = mpmath.matrix([mpv(ws[i][:, r]) for r in range(n)])
+        xs = mpmath.lu_solve(S, b)
+        bbar = mpmath.lu_solve(S, w)
+        got_b = batch.rhs(i, bb)
+        got_S = batch.block(i, sb)
+        for r in range(n):
+            assert abs(mpv(got_b[:, r]) - bbar[r]) <= 1e-28 * (1 + abs(bbar[r]))
+            for c in range(n):
+                want = -(bbar[r] * xs[c] + xs[r] * bbar[c]) / 2
+                assert abs(mpv(got_S[:, r, c]) - want) <= 1e-28 * (1 + abs(want))
