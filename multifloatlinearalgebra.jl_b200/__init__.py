@@ -224,6 +224,8 @@ class MFMatrix:
     def empty(cls, N: int, m: int, n: Optional[int] = None, device=None) -> "MFMatrix":
         vec = n is None
         n = 1 if vec else n
+        if isinstance(device, torch.device):
+            device = device.index
         dev = torch.device("cuda", torch.cuda.current_device() if device is None else device)
         st = torch.empty((N, max(n, 0), max(m, 1)), dtype=torch.float64, device=dev)
         return cls(st, 0, 0, m, n, vec)
@@ -243,6 +245,8 @@ class MFMatrix:
             X = X[:, :, None]
         if X.ndim != 3:
             raise ArgumentError("expected an (N, m, n) or (N, m) limb array")
+        if isinstance(device, torch.device):
+            device = device.index
         dev = torch.device("cuda", torch.cuda.current_device() if device is None else device)
         st = torch.from_numpy(np.ascontiguousarray(X.transpose(0, 2, 1))).to(dev)
         if st.shape[2] == 0:

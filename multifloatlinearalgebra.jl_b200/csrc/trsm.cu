@@ -80,6 +80,42 @@ __global__ void __launch_bounds__(NT) trsm_left_cta(int64_t m, int64_t n, Mat A,
     }
 }
 
+// Backward substitution (effective upper, left side) in the reference order:
+// row r's chain v = B[r]; v -= coef(r,k) * X[k] for k = r+1..m-1 ascending.
+// One CTA per right-hand-side column: the products of row r are formed by all
+// threads into shared memory, thread 0 runs the subtraction chain and the
+// division.  The column is read from and written to global memory.
+template <int N, int NT>
+__global__ void __launch_bounds__(NT) trsm_left_backward_cta(int64_t m, int64_t n, Mat A, Mat B,
+                                                             bool transposed, bool unit,
+                                                             const int *info) {
+    if (info && *info) return;
+    extern __shared__ double prod[];  // [m][N]
+    const int64_t col = blockIdx.x;
+    if (col >= n) return;
+    const int t = threadIdx.x;
+    for (int64_t r = m - 1; r >= 0; --r) {
+        for (int64_t k = r + 1 + t; k < m; k += NT) {
+            const mf<N> p = mul(tri_coef<N>(A, r, k, transposed), load_mf<N>(B.p, B.ld, B.ls, k, col));
+#pragma unroll
+            for (int l = 0; l < N; ++l) prod[k * N + l] = p.v[l];
+        }
+        __syncthreads();
+        if (t == 0) {
+            mf<N> v = load_mf<N>(B.p, B.ld, B.ls, r, col);
+            for (int64_t k = r + 1; k < m; ++k) {
+                mf<N> p;
+#pragma unroll
+                for (int l = 0; l < N; ++l) p.v[l] = prod[k * N + l];
+                v = sub(v, p);
+            }
+            if (!unit) v = div(v, load_mf<N>(A.p, A.ld, A.ls, r, r));
+            store_mf<N>(B.p, B.ld, B.ls, r, col, v);
+        }
+        __syncthreads();
+    }
+}
+
 template <int N>
 __global__ void trsm_left_thread(int64_t m, int64_t n, Mat A, Mat B, bool eff_lower,
                                  bool transposed, bool unit, const int *info) {
@@ -156,9 +192,25 @@ static int run_trsm(int side, int uplo, int trans, int diag, int64_t m, int64_t 
     // That is the reference's ascending-k chain only for forward substitution
     // (effective lower): in backward substitution the reference's chain for
     // row r starts with X[r+1], the last unknown finalised before X[r], so each
-    // row's chain is inherently serial after its predecessor and the plain
-    // per-column loop is used.
-    if (m <= 64 || n >= 4096 || !eff_lower) {
+    // row's chain is serial after its predecessor; those solves use the
+    // product-parallel CTA kernel (or the per-column loop for short triangles).
+    // The binary64 instance (N == 1) has no reference order to keep and uses
+    // the wavefront in both directions.
+    if (!eff_lower && N > 1 && m > 64 && n < 4096 && (size_t)m * N * 8 <= 200 * 1024) {
+        const size_t smem = (size_t)m * N * sizeof(double);
+        static bool configured = false;
+        if (!configured) {
+            cudaError_t e = cudaFuncSetAttribute(trsm_left_backward_cta<N, 256>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 200 * 1024);
+            if (e != cudaSuccess) return record_cuda_error(e, "trsm backward attribute");
+            configured = true;
+        }
+        trsm_left_backward_cta<N, 256><<<(unsigned)n, 256, smem, s>>>(m, n, A, B, transposed,
+                                                                       unit, info);
+        return record_cuda_error(cudaGetLastError(), "trsm left backward");
+    }
+    if (m <= 64 || n >= 4096 || (!eff_lower && N > 1)) {
         trsm_left_thread<N><<<(unsigned)((n + 127) / 128), 128, 0, s>>>(m, n, A, B, eff_lower,
                                                                         transposed, unit, info);
         return record_cuda_error(cudaGetLastError(), "trsm left thread");

@@ -100,7 +100,13 @@ def _loss_x4(ref, S, b, w):
 
 
 def _fd(ref, lp, lm, h):
-    return float(ref.to_double(ref.add(lp, -lm)[:, None])[0]) / (2 * h)
+    """central difference (lp - lm) / (2h) in Float64x4 (4 limbs)"""
+    return ref.div(ref.add(lp, -lm), np.array([2 * h, 0.0, 0.0, 0.0]))
+
+
+def _close_x4(ref, got, want, rel):
+    d = abs(float(ref.to_double(ref.add(got, -want)[:, None])[0]))
+    return d <= rel * max(1.0, abs(float(want[0])))
 
 
 def test_batched_adjoint_vs_finite_differences_x4(mf, ref, rng):
@@ -124,15 +130,15 @@ def test_batched_adjoint_vs_finite_differences_x4(mf, ref, rng):
     for i in range(len(sizes)):
         S, b, w = blocks[i], rhs[i], ws[i]
         n = sizes[i]
-        Sbar = ref.to_double(batch.block(i, sb))
-        bbar = ref.to_double(batch.rhs(i, bb))
+        Sbar = batch.block(i, sb)
+        bbar = batch.rhs(i, bb)
         # d/db_j
         for j in range(n):
             bp, bm = b.copy(), b.copy()
             bp[:, j] = ref.add(b[:, j], np.array([h, 0, 0, 0]))
             bm[:, j] = ref.add(b[:, j], np.array([-h, 0, 0, 0]))
             fd = _fd(ref, _loss_x4(ref, S, bp, w), _loss_x4(ref, S, bm, w), h)
-            assert abs(fd - bbar[j]) <= 1e-30 * max(1.0, abs(bbar[j]))
+            assert _close_x4(ref, fd, np.ascontiguousarray(bbar[:, j]), 1e-30)
         # symmetric perturbation of S_jk and S_kj
         for (j, k) in [(0, 0), (1, 0), (n - 1, 2), (n - 1, n - 1)]:
             E = np.zeros((N, n, n))
@@ -140,8 +146,9 @@ def test_batched_adjoint_vs_finite_differences_x4(mf, ref, rng):
             E[0, k, j] = h
             Sp, Sm = ref.add_n(S, E), ref.add_n(S, -E)
             fd = _fd(ref, _loss_x4(ref, Sp, b, w), _loss_x4(ref, Sm, b, w), h)
-            want = Sbar[j, k] if j == k else Sbar[j, k] + Sbar[k, j]
-            assert abs(fd - want) <= 1e-30 * max(1.0, abs(want))
+            sjk = np.ascontiguousarray(Sbar[:, j, k])
+            want = sjk if j == k else ref.add(sjk, np.ascontiguousarray(Sbar[:, k, j]))
+            assert _close_x4(ref, fd, want, 1e-30)
 
 
 def test_batched_adjoint_vs_mpmath_gradient(mf, ref, rng):
