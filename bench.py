@@ -42,6 +42,8 @@ def parse():
     p.add_argument("--route", default="auto", help="headline route: auto (ozaki if built), plain, ozaki")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-x4", action="store_true", help="skip the Float64x4 companion run")
+    p.add_argument("--no-configs", action="store_true",
+                   help="skip the factorization / mixed-LU / batched-SPD workloads")
     return p.parse_args()
 
 
@@ -318,6 +320,122 @@ class Runner:
         return 2.0 * n * n * k / (ms.value / 1e3)
 
 
+def _time_once(torch, fn):
+    """device time of one call (events on the current stream)"""
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    out = fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 1e3, out
+
+
+def run_configs(R, torch):
+    """Cholesky + multi-RHS solve (n=2048, 64 RHS, x2/x3/x4), mixed-precision
+    LU (n=4096, 16 RHS) against the plain Float64x4 LU, and 10,000 batched SPD
+    blocks (x2, sizes U{8..256}) with the adjoint; device times, backward
+    errors from the device residual kernels, CPU-oracle rates beside them."""
+    import numpy as np
+    mf, syn = R.mf, R.syn
+    from oracle import mfref
+    threads = mfref.threads()
+    out = {}
+    # --- Cholesky + 64-RHS solve, n = 2048 ------------------------------
+    n, nrhs = 2048, 64
+    chol = {}
+    for N in (2, 3, 4):
+        g = torch.Generator(device="cuda")
+        g.manual_seed(7 + N)
+        Rp = syn.randn_mf_device(70 + N, N, n, n)
+        Rm = mf.MFMatrix.from_tensor(Rp)
+        S = mf.MFMatrix.zeros(N, n, n)
+        # S = R R^T + n I (x4-accurate GEMM, then symmetric by construction of the lower triangle)
+        Rt = mf.MFMatrix.from_tensor(Rp.transpose(1, 2).contiguous())
+        mf.gemm_(S, Rm, Rt)
+        S.storage[0].diagonal().add_(float(n))
+        Bm = mf.MFMatrix.from_tensor(syn.randn_mf_device(80 + N, N, n, nrhs))
+        Sw = S.copy()
+        t_f, F = _time_once(torch, lambda: mf.cholesky_(Sw))
+        t_s, X = _time_once(torch, lambda: mf.solve(F, Bm))
+        Rr = mf.MFMatrix.zeros(N, n, nrhs)
+        mf.residual_(Rr, S, X, Bm, uplo="lower")
+        be = mf.normwise_backward_error(S, X, Bm, Rr, uplo="lower")
+        work = n ** 3 / 3.0 + 2.0 * n * n * nrhs
+        # CPU: the oracle's blocked Cholesky at n=512 (scaled to a rate)
+        rng = np.random.default_rng(3)
+        nc = 512
+        Sc = syn.spd_matrix(rng, N, nc, lambda a, b: mfref.gemm(a, b, nthreads=threads))
+        t0 = time.perf_counter()
+        mfref.potrf(Sc, nthreads=threads)
+        tc = time.perf_counter() - t0
+        chol[f"x{N}"] = {"factor_ms": t_f * 1e3, "solve_ms": t_s * 1e3,
+                         "md_gflops": work / (t_f + t_s) / 1e9,
+                         "max_backward_error": float(max(v[0] for v in be)),
+                         "cpu_oracle_md_gflops_n512": nc ** 3 / 3.0 / tc / 1e9,
+                         "cpu_threads": threads}
+        del S, Sw, F, X, Rr, Rm, Rt, Bm
+        torch.cuda.empty_cache()
+    out["cholesky_n2048_rhs64"] = chol
+    # --- mixed-precision LU vs plain Float64x4 LU, n = 4096 --------------
+    n, nrhs = 4096, 16
+    A, B = syn.mixed_lu_problem(mf, n, nrhs, seed=4)
+    t_m, (X, rep) = _time_once(torch, lambda: mf.solve_mixed_lu(A, B, tol=1e-60))
+    Aw = A.copy()
+
+    def plain():
+        F = mf.lu_(Aw)
+        return mf.solve(F, B)
+
+    t_p, Xp = _time_once(torch, plain)
+    Rr = mf.MFMatrix.zeros(4, n, nrhs)
+    mf.residual_(Rr, A, Xp, B)
+    be_p = float(max(v[0] for v in mf.normwise_backward_error(A, Xp, B, Rr)))
+    out["mixed_lu_n4096_rhs16"] = {
+        "mixed_ms": t_m * 1e3, "iterations": rep["iterations"],
+        "mixed_backward_error": rep["backward_error"], "plain_x4_ms": t_p * 1e3,
+        "plain_x4_backward_error": be_p, "speedup_vs_plain_x4": t_p / t_m,
+        "matrix": "U diag(sigma) V^T, sigma geometric 1 -> 1e-12, lifted to Float64x4"}
+    del A, B, X, Aw, Xp, Rr
+    torch.cuda.empty_cache()
+    # --- 10,000 batched SPD blocks, Float64x2 ------------------------------
+    rng = np.random.default_rng(5)
+    sizes = rng.integers(8, 257, 10000)
+    batch = mf.batched.SPDBatch(2, sizes)
+    tot = int(batch.total_s)
+    # S_i = R_i R_i^T + n_i I: generated per size class on the device
+    Rbuf = torch.empty((2, tot), dtype=torch.float64, device="cuda")
+    Rbuf[0].normal_()
+    Rbuf[1].normal_()
+    Rbuf[1] *= 2.0 ** -53 * Rbuf[0].abs()
+    for i in range(batch.nblocks):
+        ni, o = int(sizes[i]), int(batch.offsets_host[i])
+        Rb = Rbuf[0, o:o + ni * ni].view(ni, ni)
+        batch.S[0, o:o + ni * ni] = (Rb @ Rb.t() + ni * torch.eye(ni, dtype=torch.float64,
+                                                                  device="cuda")).reshape(-1)
+    batch.S[1].zero_()
+    batch.X[0].normal_()
+    S0, X0 = batch.S.clone(), batch.X.clone()
+    graph = mf.batched.BatchedSPDGraph(batch)
+    batch.S.copy_(S0)
+    batch.X.copy_(X0)
+    t_b, _ = _time_once(torch, graph.replay)
+    info = batch.info[:batch.nblocks].cpu().numpy()
+    x, pullback = None, None
+    batch.S.copy_(S0)
+    batch.X.copy_(X0)
+    x, pullback = mf.batched.solve_spd_batched_rrule(batch)
+    w = torch.randn_like(x)
+    w[1].zero_()
+    t_a, _ = _time_once(torch, lambda: pullback(w))
+    out["batched_spd_10000_x2"] = {
+        "factor_solve_ms": t_b * 1e3, "md_gflops": batch.flops() / t_b / 1e9,
+        "adjoint_ms": t_a * 1e3, "failed_blocks": int(np.count_nonzero(info)),
+        "launch": "one persistent kernel (+ counter memset) replayed from a CUDA graph",
+        "data": "S_i = R_i R_i^T + n_i I with binary64 R_i (seeded), sizes U{8..256}"}
+    return out
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -440,6 +558,8 @@ def main():
         line["x4"] = {"workload": f"Float64x4 GEMM m=n=k={n}", "ozaki_value": flops / t4 / 1e9,
                       "ozaki_ms": t4 * 1e3, "plain_value": flops / t4p / 1e9,
                       "plain_ms": t4p * 1e3, "speedup_vs_plain": t4p / t4, "accuracy": acc4}
+    if rank == 0 and world == 1 and not args.no_configs:
+        line["configs"] = run_configs(R, torch)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import mfref
         threads = mfref.threads()
