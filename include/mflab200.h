@@ -47,6 +47,11 @@ extern "C" {
 #define MFLAB_GEMM_DIRECT 1 /* reference :direct: acc + a*b for every limb count */
 #define MFLAB_GEMM_OZAKI 2  /* INT8-slice tensor-core route (no reference counterpart) */
 
+/* triangular-solve orders (mflab_set_solve_order) */
+#define MFLAB_ORDER_MATCHED 0 /* the reference's per-element chains: bitwise equal to it */
+#define MFLAB_ORDER_FAST 1    /* terms applied as unknowns finalise, both directions:
+                                 deterministic, not the reference's association */
+
 typedef struct mflab_handle mflab_handle;
 
 /* ------------------------------------------------------------ library --- */
@@ -61,6 +66,13 @@ const char *mflab_last_error(void);
    (types.jl:71-123): one handle per concurrent caller. */
 int mflab_create(mflab_handle **out, int device);
 int mflab_destroy(mflab_handle *h);
+
+/* Order of the backward substitutions issued through this handle (trsm,
+   potrs, getrs, sytrs): MFLAB_ORDER_MATCHED (default) keeps the reference's
+   per-row ascending chains (src/kernels/trsm.jl:18-112), which make each
+   backward row wait for the previous one; MFLAB_ORDER_FAST applies every term
+   as soon as its unknown is final.  No reference counterpart. */
+int mflab_set_solve_order(mflab_handle *h, int order);
 
 /* ---------------------------------------------------------- BLAS-like --- */
 /* C = alpha*A*B + beta*C; A m x k, B k x n, C m x n.  With beta == 0 C is not

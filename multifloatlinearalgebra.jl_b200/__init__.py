@@ -138,6 +138,7 @@ class KernelConfig:
     gemm_panel_columns: int = 0
     gemm_micro_columns: int = 0
     ozaki_slices: int = 0
+    solve_order: str = "matched"
 
 
 _DEFAULT = KernelConfig()
@@ -336,6 +337,25 @@ def _lib_h(x: MFMatrix):
     return _native.load(), _handle(x.device), _stream(x.device)
 
 
+_ORDERS = {"matched": 0, "fast": 1}
+
+
+class _solve_order:
+    """sets the handle's triangular-solve order for the duration of a call"""
+
+    def __init__(self, x: MFMatrix, config: "KernelConfig"):
+        if config.solve_order not in _ORDERS:
+            raise ArgumentError("solve_order must be :matched or :fast")
+        self.h = _handle(x.device)
+        self.order = _ORDERS[config.solve_order]
+
+    def __enter__(self):
+        _native.load().mflab_set_solve_order(self.h, self.order)
+
+    def __exit__(self, *exc):
+        _native.load().mflab_set_solve_order(self.h, 0)
+
+
 # --------------------------------------------------------------- BLAS ----
 def gemm_(C_: MFMatrix, A: MFMatrix, B: MFMatrix, alpha=1.0, beta=0.0,
           config: KernelConfig = _DEFAULT, workspace=None) -> MFMatrix:
@@ -439,8 +459,9 @@ def trsm_(B: MFMatrix, A: MFMatrix, alpha=1.0, side: str = "left", uplo: str = "
         raise DimensionMismatch("trsm! right dimensions differ")
     _no_alias("trsm!", B, A)
     lib, h, s = _lib_h(B)
-    rc = lib.mflab_trsm(h, s, N, _SIDE[side], _UPLO[uplo], _TRANS[trans], _DIAG[diag], B.m, B.n,
-                        A.ptr(), A.ld, A.ls, B.ptr(), B.ld, B.ls, _scalar(N, alpha))
+    with _solve_order(B, config):
+        rc = lib.mflab_trsm(h, s, N, _SIDE[side], _UPLO[uplo], _TRANS[trans], _DIAG[diag], B.m,
+                            B.n, A.ptr(), A.ld, A.ls, B.ptr(), B.ld, B.ls, _scalar(N, alpha))
     _check(rc, "trsm!")
     return B
 
@@ -734,13 +755,15 @@ def ldiv_(dest: MFMatrix, F: _Factor, source: Optional[MFMatrix] = None,
         dest.copy_(source)
     lib, h, s = _lib_h(dest)
     L = F.factors
-    if F.kind == "cholesky":
-        rc = lib.mflab_potrs(h, s, N, n, dest.n, L.ptr(), L.ld, L.ls, dest.ptr(), dest.ld, dest.ls)
-    elif F.kind == "lu":
-        rc = lib.mflab_getrs(h, s, N, n, dest.n, L.ptr(), L.ld, L.ls, F.ipiv.data_ptr(), dest.ptr(),
-                             dest.ld, dest.ls)
-    else:
-        return _ldiv_extra(dest, F, lib, h, s)
+    with _solve_order(dest, config):
+        if F.kind == "cholesky":
+            rc = lib.mflab_potrs(h, s, N, n, dest.n, L.ptr(), L.ld, L.ls, dest.ptr(), dest.ld,
+                                 dest.ls)
+        elif F.kind == "lu":
+            rc = lib.mflab_getrs(h, s, N, n, dest.n, L.ptr(), L.ld, L.ls, F.ipiv.data_ptr(),
+                                 dest.ptr(), dest.ld, dest.ls)
+        else:
+            return _ldiv_extra(dest, F, lib, h, s)
     _check(rc, "ldiv!")
     return dest
 

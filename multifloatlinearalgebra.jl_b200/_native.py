@@ -59,6 +59,7 @@ SIGNATURES = {
     "mflab_last_error": [],
     "mflab_create": [C.POINTER(_vp), _int],
     "mflab_destroy": [_vp],
+    "mflab_set_solve_order": [_vp, _int],
     "mflab_gemm": [_vp, _vp, _int, _int, _i64, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _i64, _vp,
                    _i64, _i64, _d, _d],
     "mflab_syrk_lower": [_vp, _vp, _int, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _i64, _d, _d],

@@ -51,6 +51,7 @@ extern "C" int mflab_create(mflab_handle **out, int device) {
     h->aux = nullptr;
     h->aux_bytes = 0;
     h->last_slices = 0;
+    h->solve_order = MFLAB_ORDER_MATCHED;
     e = cudaMalloc((void **)&h->dev_flags, 64 * sizeof(int));
     if (e != cudaSuccess) {
         delete h;
@@ -110,5 +111,12 @@ int mflab_reserve_aux(mflab_handle *h, size_t bytes) {
         return MFLAB_ERR_ALLOC;
     }
     h->aux_bytes = want;
+    return MFLAB_OK;
+}
+
+extern "C" int mflab_set_solve_order(mflab_handle *h, int order) {
+    if (!h) return MFLAB_ERR_ARG;
+    if (order != MFLAB_ORDER_MATCHED && order != MFLAB_ORDER_FAST) return MFLAB_ERR_ARG;
+    h->solve_order = order;
     return MFLAB_OK;
 }

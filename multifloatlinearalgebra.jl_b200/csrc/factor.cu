@@ -413,9 +413,9 @@ extern "C" int mflab_potrs(mflab_handle *h, void *stream, int limbs, int64_t n, 
     const double one[4] = {1.0, 0.0, 0.0, 0.0};
     cudaStream_t s = (cudaStream_t)stream;
     Mat a{(double *)L, ldl, lsl}, b{B, ldb, lsb};
-    int rc = mfl::launch_trsm(limbs, 0, 0, 0, 0, n, nrhs, a, b, one, s);
+    int rc = mfl::launch_trsm_info(limbs, 0, 0, 0, 0, n, nrhs, a, b, one, s, nullptr, h->solve_order);
     if (rc) return rc;
-    return mfl::launch_trsm(limbs, 0, 0, 1, 0, n, nrhs, a, b, one, s);
+    return mfl::launch_trsm_info(limbs, 0, 0, 1, 0, n, nrhs, a, b, one, s, nullptr, h->solve_order);
 }
 
 extern "C" int mflab_getrf(mflab_handle *h, void *stream, int limbs, int64_t m, int64_t n,
@@ -460,9 +460,9 @@ extern "C" int mflab_getrs(mflab_handle *h, void *stream, int limbs, int64_t n, 
     }
     int rc = mfl::record_cuda_error(cudaGetLastError(), "getrs pivots");
     if (rc) return rc;
-    rc = mfl::launch_trsm(limbs, 0, 0, 0, 1, n, nrhs, a, b, one, s);
+    rc = mfl::launch_trsm_info(limbs, 0, 0, 0, 1, n, nrhs, a, b, one, s, nullptr, h->solve_order);
     if (rc) return rc;
-    return mfl::launch_trsm(limbs, 0, 1, 0, 0, n, nrhs, a, b, one, s);
+    return mfl::launch_trsm_info(limbs, 0, 1, 0, 0, n, nrhs, a, b, one, s, nullptr, h->solve_order);
 }
 
 extern "C" int mflab_max_abs(mflab_handle *h, void *stream, int limbs, int64_t m, int64_t n,

@@ -813,14 +813,14 @@ extern "C" int mflab_sytrs(mflab_handle *h, void *stream, int limbs, int64_t n, 
     case 3: mfl::ldlt_pivots_kernel<3><<<g, 128, 0, s>>>(n, nrhs, b, pivots, blocks, 0); break;
     default: mfl::ldlt_pivots_kernel<4><<<g, 128, 0, s>>>(n, nrhs, b, pivots, blocks, 0); break;
     }
-    rc = mfl::launch_trsm(limbs, 0, 0, 0, 1, n, nrhs, f, b, one, s);
+    rc = mfl::launch_trsm_info(limbs, 0, 0, 0, 1, n, nrhs, f, b, one, s, nullptr, h->solve_order);
     if (rc) return rc;
     switch (limbs) {
     case 2: mfl::ldlt_dsolve_kernel<2><<<gd, 128, 0, s>>>(n, nrhs, f, dsub, lsd, blocks, b, fail); break;
     case 3: mfl::ldlt_dsolve_kernel<3><<<gd, 128, 0, s>>>(n, nrhs, f, dsub, lsd, blocks, b, fail); break;
     default: mfl::ldlt_dsolve_kernel<4><<<gd, 128, 0, s>>>(n, nrhs, f, dsub, lsd, blocks, b, fail); break;
     }
-    rc = mfl::launch_trsm(limbs, 0, 0, 1, 1, n, nrhs, f, b, one, s);
+    rc = mfl::launch_trsm_info(limbs, 0, 0, 1, 1, n, nrhs, f, b, one, s, nullptr, h->solve_order);
     if (rc) return rc;
     switch (limbs) {
     case 2: mfl::ldlt_pivots_kernel<2><<<g, 128, 0, s>>>(n, nrhs, b, pivots, blocks, 1); break;

@@ -27,7 +27,8 @@ int launch_mm(int N, int ta, bool tb, int tri, bool fused3, int64_t m, int64_t n
 int launch_trsm(int N, int side, int uplo, int trans, int diag, int64_t m, int64_t n, Mat A, Mat B,
                 const double *alpha, cudaStream_t s);
 int launch_trsm_info(int N, int side, int uplo, int trans, int diag, int64_t m, int64_t n, Mat A,
-                     Mat B, const double *alpha, cudaStream_t s, const int *info);
+                     Mat B, const double *alpha, cudaStream_t s, const int *info,
+                     int order = 0);
 
 inline int cuda_status(cudaError_t e) {
     if (e == cudaSuccess) return MFLAB_OK;
@@ -83,6 +84,7 @@ struct mflab_handle {
     void *aux;
     size_t aux_bytes;
     int last_slices;  // slice count the last Ozaki call used
+    int solve_order;  // MFLAB_ORDER_MATCHED or MFLAB_ORDER_FAST for triangular solves
 };
 
 int mflab_reserve_aux(mflab_handle *h, size_t bytes);

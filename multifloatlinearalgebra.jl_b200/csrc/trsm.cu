@@ -168,7 +168,7 @@ __global__ void trsm_right_thread(int64_t m, int64_t n, Mat A, Mat B, bool eff_l
 
 template <int N>
 static int run_trsm(int side, int uplo, int trans, int diag, int64_t m, int64_t n, Mat A, Mat B,
-                    const double *alpha, cudaStream_t s, const int *info) {
+                    const double *alpha, cudaStream_t s, const int *info, int order) {
     if (m <= 0 || n <= 0) return MFLAB_OK;
     bool one = alpha[0] == 1.0;
     for (int l = 1; l < N; ++l) one = one && alpha[l] == 0.0;
@@ -196,7 +196,10 @@ static int run_trsm(int side, int uplo, int trans, int diag, int64_t m, int64_t 
     // product-parallel CTA kernel (or the per-column loop for short triangles).
     // The binary64 instance (N == 1) has no reference order to keep and uses
     // the wavefront in both directions.
-    if (!eff_lower && N > 1 && m > 64 && n < 4096 && (size_t)m * N * 8 <= 200 * 1024) {
+    // the fast order applies every term as soon as its unknown is final, in both
+    // directions (deterministic, not the reference's association)
+    const bool wavefront_ok = eff_lower || N == 1 || order == MFLAB_ORDER_FAST;
+    if (!eff_lower && !wavefront_ok && m > 64 && n < 4096 && (size_t)m * N * 8 <= 200 * 1024) {
         const size_t smem = (size_t)m * N * sizeof(double);
         static bool configured = false;
         if (!configured) {
@@ -210,7 +213,7 @@ static int run_trsm(int side, int uplo, int trans, int diag, int64_t m, int64_t 
                                                                        unit, info);
         return record_cuda_error(cudaGetLastError(), "trsm left backward");
     }
-    if (m <= 64 || n >= 4096 || (!eff_lower && N > 1)) {
+    if (m <= 64 || n >= 4096 || !wavefront_ok) {
         trsm_left_thread<N><<<(unsigned)((n + 127) / 128), 128, 0, s>>>(m, n, A, B, eff_lower,
                                                                         transposed, unit, info);
         return record_cuda_error(cudaGetLastError(), "trsm left thread");
@@ -230,12 +233,12 @@ static int run_trsm(int side, int uplo, int trans, int diag, int64_t m, int64_t 
 }
 
 int launch_trsm_info(int N, int side, int uplo, int trans, int diag, int64_t m, int64_t n, Mat A,
-                     Mat B, const double *alpha, cudaStream_t s, const int *info) {
+                     Mat B, const double *alpha, cudaStream_t s, const int *info, int order) {
     switch (N) {
-    case 1: return run_trsm<1>(side, uplo, trans, diag, m, n, A, B, alpha, s, info);
-    case 2: return run_trsm<2>(side, uplo, trans, diag, m, n, A, B, alpha, s, info);
-    case 3: return run_trsm<3>(side, uplo, trans, diag, m, n, A, B, alpha, s, info);
-    case 4: return run_trsm<4>(side, uplo, trans, diag, m, n, A, B, alpha, s, info);
+    case 1: return run_trsm<1>(side, uplo, trans, diag, m, n, A, B, alpha, s, info, order);
+    case 2: return run_trsm<2>(side, uplo, trans, diag, m, n, A, B, alpha, s, info, order);
+    case 3: return run_trsm<3>(side, uplo, trans, diag, m, n, A, B, alpha, s, info, order);
+    case 4: return run_trsm<4>(side, uplo, trans, diag, m, n, A, B, alpha, s, info, order);
     default: return MFLAB_ERR_UNSUPPORTED;
     }
 }
@@ -256,6 +259,7 @@ extern "C" int mflab_trsm(mflab_handle *h, void *stream, int limbs, int side, in
         return MFLAB_ERR_ARG;
     const int64_t na = side == 0 ? m : n;
     if ((na > 0 && lda < na) || (m > 0 && ldb < m)) return MFLAB_ERR_ARG;
-    return mfl::launch_trsm(limbs, side, uplo, trans, diag, m, n, mfl::Mat{(double *)A, lda, lsa},
-                            mfl::Mat{B, ldb, lsb}, alpha, (cudaStream_t)stream);
+    return mfl::launch_trsm_info(limbs, side, uplo, trans, diag, m, n,
+                                 mfl::Mat{(double *)A, lda, lsa}, mfl::Mat{B, ldb, lsb}, alpha,
+                                 (cudaStream_t)stream, nullptr, h->solve_order);
 }

@@ -131,3 +131,25 @@ def test_kat_tiny_first_pivot(mf, N):
     A[0] = [[2.0 ** -300, 1], [1, 1]]
     F = mf.lu_(mf.MFMatrix.from_numpy(A), config=mf.KernelConfig(lu_block=2))
     assert mf.factor_diagnostics(F)["pivots"][0] == 2
+
+
+@pytest.mark.parametrize("N", [2, 4])
+@pytest.mark.parametrize("kind", ["cholesky", "lu", "ldlt"])
+def test_fast_solve_order(mf, ref, rng, N, kind):
+    """solve_order="fast" (wavefront backward substitution): deterministic and
+    within the reference tolerance, not bitwise the matched order"""
+    n = 130
+    S = _spd(ref, rng, N, n)
+    B = syn.randn_mf(rng, N, n, 4)
+    fac = {"cholesky": mf.cholesky_, "lu": mf.lu_, "ldlt": mf.ldlt_}[kind]
+    F = fac(mf.MFMatrix.from_numpy(S))
+    fast = mf.KernelConfig(solve_order="fast")
+    X1 = mf.solve(F, mf.MFMatrix.from_numpy(B), config=fast).to_numpy()
+    X2 = mf.solve(F, mf.MFMatrix.from_numpy(B), config=fast).to_numpy()
+    assert np.array_equal(X1.view(np.uint64), X2.view(np.uint64))
+    assert np.all(ref.backward_error(S, X1, B) < 4096 * n * 2.0 ** (-52 * N))
+    # the handle returns to the matched order afterwards
+    Xm = mf.solve(F, mf.MFMatrix.from_numpy(B)).to_numpy()
+    if kind == "cholesky":
+        L, _ = ref.potrf(S)
+        assert_bitwise(Xm, ref.potrs(L, B))
