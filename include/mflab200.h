@@ -52,6 +52,10 @@ extern "C" {
 #define MFLAB_ORDER_FAST 1    /* terms applied as unknowns finalise, both directions:
                                  deterministic, not the reference's association */
 
+/* engines of the INT8-slice level products (mflab_set_int8_engine) */
+#define MFLAB_INT8_TCGEN05 0 /* the library's own tcgen05 / TMA / TMEM kernel */
+#define MFLAB_INT8_LIBRARY 1 /* cuBLASLt int8 GEMM */
+
 typedef struct mflab_handle mflab_handle;
 
 /* ------------------------------------------------------------ library --- */
@@ -104,6 +108,15 @@ int mflab_ozaki_default_slices(int limbs, int64_t k);
 /* slice count used by the last INT8-slice GEMM on this handle (no reference
    counterpart). */
 int mflab_ozaki_last_slices(mflab_handle *h);
+
+/* Engine of the int8 level products of mflab_gemm_ozaki on this handle:
+   MFLAB_INT8_TCGEN05 or MFLAB_INT8_LIBRARY.  No reference counterpart. */
+int mflab_set_int8_engine(mflab_handle *h, int engine);
+
+/* Device-side status word of the tcgen05 kernels issued through this handle:
+   0, or the code of a bounded wait that ran out (MFLAB_ERR_TIMEOUT is then
+   the caller's conclusion).  Synchronises.  No reference counterpart. */
+int mflab_device_status(mflab_handle *h, int *status);
 
 /* lower(C) = alpha * P^T * P + beta * lower(C); P is k x n, C n x n.  The
    strict upper triangle of C is neither read nor written.

@@ -29,6 +29,16 @@ int mflab_gemm_ozaki_phases(struct mflab_handle *h, void *stream, int limbs, int
    through the library path the INT8-slice route uses.  Synchronises. */
 int mflab_probe_int8_gemm(struct mflab_handle *h, void *stream, int64_t m, int64_t n, int64_t k,
                           int reps, float *ms);
+
+/* One int8 x int8 -> int32 GEMM C = A[:, 0:K] * B[:, b_xoff:b_xoff+K]^T with
+   K-major operands (A mp x a_cols, B np x b_cols, leading dims in bytes) and
+   column-major C (ldc >= mp), through engine 0 (tcgen05 kernel: mp % 128 == 0,
+   np % 256 == 0, K % 128 == 0) or 1 (library).  *err (device int) receives the
+   kernel's bounded-wait status.  Used by the tests and the roofline probe. */
+int mflab_int8_gemm_tn(struct mflab_handle *h, void *stream, int engine, int64_t mp, int64_t np,
+                       int64_t K, const int8_t *A, int64_t lda, int64_t a_cols, const int8_t *B,
+                       int64_t ldb, int64_t b_cols, int64_t b_xoff, int32_t *C, int64_t ldc,
+                       int *err);
 #ifdef __cplusplus
 }
 #endif

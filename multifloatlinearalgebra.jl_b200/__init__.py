@@ -138,6 +138,7 @@ class KernelConfig:
     gemm_panel_columns: int = 0
     gemm_micro_columns: int = 0
     ozaki_slices: int = 0
+    ozaki_engine: str = "library"
     solve_order: str = "matched"
 
 
@@ -373,6 +374,10 @@ def gemm_(C_: MFMatrix, A: MFMatrix, B: MFMatrix, alpha=1.0, beta=0.0,
     route = _ROUTES[plan["strategy"]]
     lib, h, s = _lib_h(C_)
     if route == 2:
+        engines = {"tcgen05": 0, "library": 1}
+        if config.ozaki_engine not in engines:
+            raise ArgumentError("ozaki_engine must be :tcgen05 or :library")
+        _check(lib.mflab_set_int8_engine(h, engines[config.ozaki_engine]), "gemm!")
         rc = lib.mflab_gemm_ozaki(h, s, N, int(config.ozaki_slices), m, n, k, A.ptr(), A.ld, A.ls,
                                   B.ptr(), B.ld, B.ls, C_.ptr(), C_.ld, C_.ls, _scalar(N, alpha),
                                   _scalar(N, beta))
@@ -392,6 +397,15 @@ def ozaki_last_slices(device: Optional[int] = None) -> int:
     """Slice count chosen by the last INT8-slice GEMM issued from this thread."""
     dev = torch.cuda.current_device() if device is None else device
     return int(_native.load().mflab_ozaki_last_slices(_handle(dev)))
+
+
+def device_status(device: Optional[int] = None) -> int:
+    """0, or the status code a tcgen05 kernel of this thread's handle left
+    after a bounded wait ran out (synchronises)"""
+    dev = torch.cuda.current_device() if device is None else device
+    v = C.c_int()
+    _check(_native.load().mflab_device_status(_handle(dev), C.byref(v)), "device_status")
+    return int(v.value)
 
 
 def ozaki_available() -> bool:

@@ -94,6 +94,10 @@ SIGNATURES = {
                          _vp, _i64, _i64, _d, _d],
     "mflab_ozaki_default_slices": [_int, _i64],
     "mflab_ozaki_last_slices": [_vp],
+    "mflab_set_int8_engine": [_vp, _int],
+    "mflab_device_status": [_vp, C.POINTER(_int)],
+    "mflab_int8_gemm_tn": [_vp, _vp, _int, _i64, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _i64,
+                           _i64, _vp, _i64, _vp],
     "mflab_gemm_ozaki_phases": [_vp, _vp, _int, _int, _i64, _i64, _i64, _vp, _i64, _i64, _vp, _i64,
                                 _i64, _vp, _i64, _i64, _d, _d, C.POINTER(C.c_float), _d],
     "mflab_probe_int8_gemm": [_vp, _vp, _i64, _i64, _i64, _int, C.POINTER(C.c_float)],

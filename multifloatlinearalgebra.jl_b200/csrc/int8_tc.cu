@@ -1,0 +1,315 @@
+// int8 x int8 -> int32 GEMM on the 5th-generation tensor cores (tcgen05),
+// the level products of the INT8-slice multi-double route.
+//
+// C[m0:m0+128, n0:n0+256] = A[rows, K] * B[cols, K]^T with both operands
+// K-major int8 (rows of the digit matrices), exact int32 accumulation.
+//
+// One CTA (4 warps) per 128 x 256 output tile:
+//   * warp 0 lane 0: TMA producer.  Per 128-byte K step it loads the A tile
+//     (128 rows x 128 B) and the B tile (256 rows x 128 B) into one of 4 shared
+//     memory stages with cp.async.bulk.tensor (128-byte swizzle, no multicast),
+//     completion tracked by the stage's "full" mbarrier (expect_tx).
+//   * warp 1 lane 0: MMA issuer.  Waits for a full stage, issues four
+//     tcgen05.mma.cta_group::1.kind::i8 (M=128, N=256, K=32) into a TMEM
+//     accumulator of 256 columns, and tcgen05.commit's the stage's "empty"
+//     mbarrier so the producer can refill it once the MMAs have read it.
+//     After the last K step a commit signals the accumulator barrier.
+//   * all 4 warps: epilogue.  Each warp reads its 32 TMEM lanes (rows) with
+//     tcgen05.ld.32x32b.x16 and stores int32 rows; a warp's 32 threads write 32
+//     consecutive rows of one column (coalesced, C is column-major).
+// Every mbarrier wait is bounded: on timeout the kernel records an error code
+// in *err, waits (bounded) for its own copies in flight, frees its TMEM and
+// returns.  Operands: the padded digit matrices (rows multiple of 128 / 256, K
+// multiple of 128), so no tile needs bounds checks.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
+#include "mflab_internal.h"
+
+namespace mfl {
+
+constexpr int TC_BM = 128, TC_BN = 256, TC_BK = 128, TC_STAGES = 4;
+constexpr uint32_t TC_A_BYTES = TC_BM * TC_BK;               // 16 KiB
+constexpr uint32_t TC_B_BYTES = TC_BN * TC_BK;               // 32 KiB
+constexpr uint32_t TC_STAGE_BYTES = TC_A_BYTES + TC_B_BYTES;  // 48 KiB
+constexpr uint32_t TC_SMEM = TC_STAGES * TC_STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
+constexpr uint32_t TC_TMEM_COLS = 256;
+constexpr long long TC_WAIT_LIMIT = 1LL << 24;
+
+// error codes written to *err
+constexpr int TC_ERR_PRODUCER = 1, TC_ERR_MMA = 2, TC_ERR_EPILOGUE = 3;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, P1;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// bounded wait for the completion of phase `parity`; false on timeout
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+    for (long long i = 0; i < TC_WAIT_LIMIT; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y,
+                                            uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row atoms of
+// 1024 bytes (stride byte offset 1024, leading byte offset 16 unused)
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)1 << 16;                 // leading byte offset (16 B units)
+    d |= (uint64_t)(1024 >> 4) << 32;       // stride byte offset (16 B units)
+    d |= (uint64_t)1 << 46;                 // descriptor version for tcgen05
+    d |= (uint64_t)2 << 61;                 // SWIZZLE_128B
+    return d;
+}
+
+// instruction descriptor: s8 x s8 -> s32, both operands K-major, M = 128, N = 256
+__host__ __device__ constexpr uint32_t idesc_i8(int M, int N) {
+    return (2u << 4)      // D format s32
+           | (1u << 7)    // A signed 8-bit
+           | (1u << 10)   // B signed 8-bit
+           | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                       uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred PRED_enable_input_d;\n\t"
+        "setp.ne.b32 PRED_enable_input_d, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, PRED_enable_input_d;\n\t}"
+        ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     smem_u32(bar))
+                 : "memory");
+}
+
+__global__ void __launch_bounds__(128, 1)
+    int8_tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA,
+                        const __grid_constant__ CUtensorMap tmB, int K, int b_xoff, int32_t *C,
+                        int64_t ldc, int *err) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint64_t *full = (uint64_t *)(smem + TC_STAGES * TC_STAGE_BYTES);
+    uint64_t *empty = full + TC_STAGES;
+    uint64_t *accbar = empty + TC_STAGES;
+    uint32_t *tmem_slot = (uint32_t *)(accbar + 1);
+    int *abort_flag = (int *)(tmem_slot + 1);
+
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const int m0 = blockIdx.x * TC_BM, n0 = blockIdx.y * TC_BN;
+    const int ksteps = K / TC_BK;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < TC_STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(accbar, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(tmem_slot)),
+                     "r"(TC_TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        // ---------------- TMA producer
+        int issued = 0;
+        for (int i = 0; i < ksteps; ++i) {
+            const int s = i % TC_STAGES;
+            if (i >= TC_STAGES && !mbar_wait(&empty[s], ((i / TC_STAGES) - 1) & 1)) {
+                atomicExch(err, TC_ERR_PRODUCER);
+                atomicExch(abort_flag, 1);
+                break;
+            }
+            if (*(volatile int *)abort_flag) break;
+            uint8_t *sa = smem + s * TC_STAGE_BYTES;
+            uint8_t *sb = sa + TC_A_BYTES;
+            mbar_expect_tx(&full[s], TC_STAGE_BYTES);
+            tma_load_2d(sa, &tmA, i * TC_BK, m0, &full[s]);
+            tma_load_2d(sb, &tmB, b_xoff + i * TC_BK, n0, &full[s]);
+            ++issued;
+        }
+        // the copies issued last must have landed before the CTA can exit
+        for (int i = issued - TC_STAGES > 0 ? issued - TC_STAGES : 0; i < issued; ++i)
+            mbar_wait(&full[i % TC_STAGES], (i / TC_STAGES) & 1);
+    } else if (warp == 1 && lane == 0) {
+        // ---------------- MMA issuer
+        const uint32_t idesc = idesc_i8(TC_BM, TC_BN);
+        bool ok = true;
+        for (int i = 0; i < ksteps; ++i) {
+            const int s = i % TC_STAGES;
+            if (!mbar_wait(&full[s], (i / TC_STAGES) & 1)) {
+                atomicExch(err, TC_ERR_MMA);
+                atomicExch(abort_flag, 1);
+                ok = false;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t sa = smem_u32(smem + s * TC_STAGE_BYTES);
+            const uint32_t sb = sa + TC_A_BYTES;
+#pragma unroll
+            for (int kk = 0; kk < TC_BK / 32; ++kk)
+                mma_i8(tmem, smem_desc_sw128(sa + kk * 32), smem_desc_sw128(sb + kk * 32), idesc,
+                       (i > 0 || kk > 0) ? 1u : 0u);
+            mma_commit(&empty[s]);
+        }
+        if (ok) mma_commit(accbar);
+        else mma_commit(accbar);  // still signal: the epilogue then sees abort_flag
+    }
+    __syncwarp();
+
+    // ---------------- epilogue: TMEM -> registers -> int32 rows of C
+    const bool acc_ready = mbar_wait(accbar, 0);
+    if (!acc_ready) atomicExch(err, TC_ERR_EPILOGUE);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const bool store = acc_ready && !*(volatile int *)abort_flag;
+    const int row = m0 + warp * 32 + lane;
+#pragma unroll 1
+    for (int c0 = 0; c0 < TC_BN; c0 += 16) {
+        uint32_t v[16];
+        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+            "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+              "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
+              "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+            : "r"(taddr)
+            : "memory");
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (store) {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) C[(int64_t)(n0 + c0 + j) * ldc + row] = (int32_t)v[j];
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(TC_TMEM_COLS)
+                     : "memory");
+    }
+}
+
+// ---------------------------------------------------------------- host ----
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    });
+    return fn;
+}
+
+// rows x cols int8 row-major matrix (ld bytes), box of box_rows x 128 bytes
+static int make_map(CUtensorMap *map, const int8_t *base, int64_t rows, int64_t cols, int64_t ld,
+                    int box_rows) {
+    auto fn = encode_fn();
+    if (!fn) return MFLAB_ERR_UNSUPPORTED;
+    if (((uintptr_t)base & 15) || (ld & 15)) return MFLAB_ERR_ARG;
+    cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)ld};
+    cuuint32_t box[2] = {(cuuint32_t)TC_BK, (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, (void *)base, dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? MFLAB_OK : MFLAB_ERR_UNSUPPORTED;
+}
+
+// C (mp x np int32, ldc) = A[0:mp, a-range] * B[0:np, b_xoff : b_xoff + K]^T.
+// A is mp x a_cols, B np x b_cols, row-major int8 with leading dims lda, ldb.
+// Requires mp % 128 == 0, np % 256 == 0, K % 128 == 0, b_xoff % 16 == 0.
+int int8_gemm_tc(int64_t mp, int64_t np, int64_t K, const int8_t *A, int64_t lda, int64_t a_cols,
+                 const int8_t *B, int64_t ldb, int64_t b_cols, int64_t b_xoff, int32_t *C,
+                 int64_t ldc, int *err, cudaStream_t s) {
+    if (mp % TC_BM || np % TC_BN || K % TC_BK || b_xoff % 16 || K <= 0) return MFLAB_ERR_ARG;
+    if (K > a_cols || b_xoff + K > b_cols || K > 0x7fffffff || b_xoff > 0x7fffffff)
+        return MFLAB_ERR_ARG;
+    if (mp / TC_BM > 0x7fffffff || np / TC_BN > 65535) return MFLAB_ERR_UNSUPPORTED;
+    CUtensorMap ta, tb;
+    int rc = make_map(&ta, A, mp, a_cols, lda, TC_BM);
+    if (rc) return rc;
+    rc = make_map(&tb, B, np, b_cols, ldb, TC_BN);
+    if (rc) return rc;
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(int8_tc_gemm_kernel,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
+        if (e != cudaSuccess) return record_cuda_error(e, "int8 tc attribute");
+        configured = true;
+    }
+    dim3 grid((unsigned)(mp / TC_BM), (unsigned)(np / TC_BN));
+    int8_tc_gemm_kernel<<<grid, 128, TC_SMEM, s>>>(ta, tb, (int)K, (int)b_xoff, C, ldc, err);
+    return record_cuda_error(cudaGetLastError(), "int8 tc gemm");
+}
+
+}  // namespace mfl
+
+// Test / measurement entry: one int8 x int8 -> int32 TN GEMM through either
+// engine (0 = tcgen05 kernel, 1 = library).  Shapes as int8_gemm_tc.  The
+// tcgen05 kernel's timeout status is written to *err (device int, 0 = ok).
+extern "C" int mflab_int8_gemm_tn(mflab_handle *h, void *stream, int engine, int64_t mp,
+                                  int64_t np, int64_t K, const int8_t *A, int64_t lda,
+                                  int64_t a_cols, const int8_t *B, int64_t ldb, int64_t b_cols,
+                                  int64_t b_xoff, int32_t *C, int64_t ldc, int *err) {
+    if (!h || !A || !B || !C || !err) return MFLAB_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (engine == 0)
+        return mfl::int8_gemm_tc(mp, np, K, A, lda, a_cols, B, ldb, b_cols, b_xoff, C, ldc, err, s);
+    const size_t ws = (size_t)64 << 20;
+    int rc = mflab_reserve_scratch(h, ws);
+    if (rc) return rc;
+    return mfl::int8_gemm_tn(mp, np, K, A, lda, B + b_xoff, ldb, C, ldc, h->scratch, ws, s);
+}

@@ -36,6 +36,14 @@ inline int cuda_status(cudaError_t e) {
 }
 
 int record_cuda_error(cudaError_t e, const char *where);
+
+// int8 x int8 -> int32 TN GEMM through the library (ozaki.cu) and through the
+// tcgen05 kernel (int8_tc.cu)
+int int8_gemm_tn(int64_t m, int64_t n, int64_t K, const int8_t *A, int64_t lda, const int8_t *B,
+                 int64_t ldb, int32_t *I, int64_t ldi, void *ws, size_t wsb, cudaStream_t s);
+int int8_gemm_tc(int64_t mp, int64_t np, int64_t K, const int8_t *A, int64_t lda, int64_t a_cols,
+                 const int8_t *B, int64_t ldb, int64_t b_cols, int64_t b_xoff, int32_t *C,
+                 int64_t ldc, int *err, cudaStream_t s);
 void record_error_message(const char *msg);
 
 inline bool valid_limbs(int N) { return N >= 2 && N <= 4; }
@@ -85,6 +93,7 @@ struct mflab_handle {
     size_t aux_bytes;
     int last_slices;  // slice count the last Ozaki call used
     int solve_order;  // MFLAB_ORDER_MATCHED or MFLAB_ORDER_FAST for triangular solves
+    int int8_engine;  // MFLAB_INT8_TCGEN05 or MFLAB_INT8_LIBRARY for the level products
 };
 
 int mflab_reserve_aux(mflab_handle *h, size_t bytes);

@@ -220,11 +220,14 @@ struct OzPlan {
 };
 
 static OzPlan oz_plan(int64_t m, int64_t n, int64_t k, int S) {
+    // (kp, mp, np padding below)
     OzPlan p;
     p.S = S;
-    p.kp = (k + 15) / 16 * 16;
-    p.mp = (m + 15) / 16 * 16;
-    p.np = (n + 15) / 16 * 16;
+    // padded to the tcgen05 tile (128 x 256 outputs, 128-byte K steps); the
+    // padding rows, columns and K positions hold zero digits
+    p.kp = (k + 127) / 128 * 128;
+    p.mp = (m + 127) / 128 * 128;
+    p.np = (n + 255) / 256 * 256;
     p.ldi = p.mp;
     p.plane = ((size_t)p.ldi * p.np + 63) / 64 * 64;
     auto al = [](size_t b) { return (b + 255) / 256 * 256; };
@@ -303,7 +306,7 @@ static inline void phase(int i, cudaStream_t s) {
 template <int N>
 static int ozaki_n(int64_t m, int64_t n, int64_t k, Mat A, Mat B, Mat C, const double *alpha,
                    const double *beta, int S, char *base, const OzPlan &p, const int *rowexp,
-                   const int *colexp, cudaStream_t s) {
+                   const int *colexp, cudaStream_t s, int engine, int *tc_err) {
     phase(0, s);
     int8_t *A8 = (int8_t *)base;
     int8_t *B8 = (int8_t *)(base + p.a8);
@@ -318,9 +321,14 @@ static int ozaki_n(int64_t m, int64_t n, int64_t k, Mat A, Mat B, Mat C, const d
     phase(1, s);
     const int64_t ld8 = (int64_t)S * p.kp;
     for (int L = 2; L <= S + 1; ++L) {
-        rc = int8_gemm_tn(p.mp, p.np, (int64_t)(L - 1) * p.kp, A8, ld8,
-                          B8 + (int64_t)(S - L + 1) * p.kp, ld8, I + (size_t)(L - 2) * p.plane,
-                          p.ldi, ws, p.ws, s);
+        if (engine == MFLAB_INT8_TCGEN05)
+            rc = int8_gemm_tc(p.mp, p.np, (int64_t)(L - 1) * p.kp, A8, ld8, ld8, B8, ld8, ld8,
+                              (int64_t)(S - L + 1) * p.kp, I + (size_t)(L - 2) * p.plane, p.ldi,
+                              tc_err, s);
+        else
+            rc = int8_gemm_tn(p.mp, p.np, (int64_t)(L - 1) * p.kp, A8, ld8,
+                              B8 + (int64_t)(S - L + 1) * p.kp, ld8,
+                              I + (size_t)(L - 2) * p.plane, p.ldi, ws, p.ws, s);
         if (rc) return rc;
     }
     phase(2, s);
@@ -348,7 +356,7 @@ int ozaki_default_slices(int N, int64_t k) {
 
 // largest slice count whose level sums stay exact in int32
 int ozaki_max_slices(int64_t k) {
-    const double kp = (double)((k + 15) / 16 * 16);
+    const double kp = (double)((k + 127) / 128 * 128);
     int smax = (int)(2147483647.0 / (kp * 65.0 * 65.0));
     if (smax * kp * 65.0 * 65.0 >= 2147483647.0) --smax;
     return smax < 64 ? smax : 64;
@@ -367,7 +375,7 @@ static const int OZ_SAMPLES = 2048;
 int ozaki_gemm(mflab_handle *h, int N, int S, int64_t m, int64_t n, int64_t k, Mat A, Mat B,
                Mat C, const double *alpha, const double *beta, cudaStream_t s, int *S_used) {
     if (S < 0 || S > 64) return MFLAB_ERR_ARG;
-    if ((n + 15) / 16 * 16 > 65535LL || m > INT_MAX) return MFLAB_ERR_UNSUPPORTED;
+    if ((n + 255) / 256 * 256 > 65535LL || m > INT_MAX) return MFLAB_ERR_UNSUPPORTED;
     // exponents (and the tuner's gap word) live in the aux scratch
     int rc = mflab_reserve_aux(h, sizeof(int) * (size_t)(m + n + 64));
     if (rc) return rc;
@@ -401,10 +409,11 @@ int ozaki_gemm(mflab_handle *h, int N, int S, int64_t m, int64_t n, int64_t k, M
     rc = mflab_reserve_scratch(h, p.total);
     if (rc) return rc;
     char *base = (char *)h->scratch;
+    int *tc_err = h->dev_flags + 1;
     switch (N) {
-    case 2: return ozaki_n<2>(m, n, k, A, B, C, alpha, beta, S, base, p, rowexp, colexp, s);
-    case 3: return ozaki_n<3>(m, n, k, A, B, C, alpha, beta, S, base, p, rowexp, colexp, s);
-    default: return ozaki_n<4>(m, n, k, A, B, C, alpha, beta, S, base, p, rowexp, colexp, s);
+    case 2: return ozaki_n<2>(m, n, k, A, B, C, alpha, beta, S, base, p, rowexp, colexp, s, h->int8_engine, tc_err);
+    case 3: return ozaki_n<3>(m, n, k, A, B, C, alpha, beta, S, base, p, rowexp, colexp, s, h->int8_engine, tc_err);
+    default: return ozaki_n<4>(m, n, k, A, B, C, alpha, beta, S, base, p, rowexp, colexp, s, h->int8_engine, tc_err);
     }
 }
 
@@ -473,8 +482,8 @@ extern "C" int mflab_gemm_ozaki_phases(mflab_handle *h, void *stream, int limbs,
         cudaEventElapsedTime(&ms[2], ev[1], ev[2]);
         cudaEventElapsedTime(&ms[3], ev[2], ev[3]);
         const int S = h->last_slices;
-        const double kp = (double)((k + 15) / 16 * 16);
-        const double mp = (double)((m + 15) / 16 * 16), np = (double)((n + 15) / 16 * 16);
+        const double kp = (double)((k + 127) / 128 * 128);
+        const double mp = (double)((m + 127) / 128 * 128), np = (double)((n + 255) / 256 * 256);
         *int8_ops = 2.0 * mp * np * kp * (double)S * (S + 1) / 2.0;
     }
     for (auto &e : ev) cudaEventDestroy(e);
@@ -518,4 +527,20 @@ extern "C" int mflab_probe_int8_gemm(mflab_handle *h, void *stream, int64_t m, i
     cudaEventDestroy(e1);
     *ms = best;
     return rc;
+}
+
+extern "C" int mflab_set_int8_engine(mflab_handle *h, int engine) {
+    if (!h) return MFLAB_ERR_ARG;
+    if (engine != MFLAB_INT8_TCGEN05 && engine != MFLAB_INT8_LIBRARY) return MFLAB_ERR_ARG;
+    h->int8_engine = engine;
+    return MFLAB_OK;
+}
+
+extern "C" int mflab_device_status(mflab_handle *h, int *status) {
+    if (!h || !status) return MFLAB_ERR_ARG;
+    int v = 0;
+    cudaError_t e = cudaMemcpy(&v, h->dev_flags + 1, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return mfl::record_cuda_error(e, "device status");
+    *status = v;
+    return MFLAB_OK;
 }
