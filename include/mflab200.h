@@ -110,7 +110,8 @@ int mflab_ozaki_default_slices(int limbs, int64_t k);
 int mflab_ozaki_last_slices(mflab_handle *h);
 
 /* Engine of the int8 level products of mflab_gemm_ozaki on this handle:
-   MFLAB_INT8_TCGEN05 or MFLAB_INT8_LIBRARY.  No reference counterpart. */
+   MFLAB_INT8_TCGEN05 (default) or MFLAB_INT8_LIBRARY.  No reference
+   counterpart. */
 int mflab_set_int8_engine(mflab_handle *h, int engine);
 
 /* Device-side status word of the tcgen05 kernels issued through this handle:

@@ -138,7 +138,7 @@ class KernelConfig:
     gemm_panel_columns: int = 0
     gemm_micro_columns: int = 0
     ozaki_slices: int = 0
-    ozaki_engine: str = "library"
+    ozaki_engine: str = "tcgen05"
     solve_order: str = "matched"
 
 
