@@ -2,7 +2,8 @@
 
 One step is one C = A*B over the full synthetic n = 8192 workload (entries
 randn * 2^U(-20,20), lower limbs randn * 2^-53 * |previous limb|; seeded).
-The headline path is the INT8-slice (Ozaki) tensor-core GEMM for Float64x2;
+The headline path is the INT8 tensor-core GEMM for Float64x2 (modular residue
+scheme; the digit-slice scheme is timed beside it at its own equal-error S);
 the plain FP64 matched-order kernel is timed beside it, with the componentwise
 error of both against the exact superaccumulator oracle on sampled entries.
 
@@ -41,6 +42,11 @@ def parse():
     p.add_argument("--limbs", type=int, default=2)
     p.add_argument("--route", default="auto", help="headline route: auto (ozaki if built), plain, ozaki")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--scheme", default="modular", choices=["modular", "slices"],
+                   help="INT8 scheme of the headline route (modular falls back to slices when "
+                        "the modulus table cannot reach the accuracy)")
+    p.add_argument("--no-slices", action="store_true",
+                   help="skip the digit-slice companion of the modular headline")
     p.add_argument("--no-x4", action="store_true", help="skip the Float64x4 companion run")
     p.add_argument("--no-configs", action="store_true",
                    help="skip the factorization / mixed-LU / batched-SPD workloads")
@@ -258,42 +264,61 @@ class Runner:
         B = mf.MFMatrix.from_tensor(syn.randn_mf_device(2000 + self.rank, N, n, n, spread=20))
         return A, B
 
-    def accuracy_and_slices(self, N, n, A, B, Cm):
-        """Plain and INT8-slice errors against the exact oracle on 256 sampled
-        entries; the slice count starts at the product's tuner choice and is
-        raised until the INT8-slice error is no worse than the plain one."""
-        import numpy as np
+    def cfg(self, scheme, knob):
+        """KernelConfig of the INT8 route: scheme "modular" (knob = moduli) or
+        "slices" (knob = digit slices); knob 0 = the tuner's choice"""
         mf = self.mf
+        if scheme == "modular":
+            return mf.KernelConfig(gemm_strategy="ozaki", ozaki_scheme="modular",
+                                   ozaki_moduli=knob)
+        return mf.KernelConfig(gemm_strategy="ozaki", ozaki_scheme="slices", ozaki_slices=knob)
+
+    def checker(self, n, A, B, Cm):
+        """exact oracle check of 256 sampled entries of Cm: returns a function
+        giving the max componentwise relative error of the current Cm"""
+        import numpy as np
         from oracle import mfref
         rs = np.random.default_rng(5)
         rows, cols = rs.integers(0, n, 256), rs.integers(0, n, 256)
         An, Bn = A.to_numpy(), B.to_numpy()
-        mf.gemm_(Cm, A, B)
-        e_plain = float(np.max(_check_entries(mfref, An, Bn, Cm, rows, cols)))
-        mf.gemm_(Cm, A, B, config=mf.KernelConfig(gemm_strategy="ozaki"))
-        S0 = mf.ozaki_last_slices()
-        S = S0
-        e_oz = float(np.max(_check_entries(mfref, An, Bn, Cm, rows, cols)))
-        e_tuner = e_oz
+        return lambda: float(np.max(_check_entries(mfref, An, Bn, Cm, rows, cols)))
 
-        def err_at(S):
-            mf.gemm_(Cm, A, B, config=mf.KernelConfig(gemm_strategy="ozaki", ozaki_slices=S))
-            return float(np.max(_check_entries(mfref, An, Bn, Cm, rows, cols)))
+    def accuracy_search(self, N, n, A, B, Cm, scheme, e_plain, check):
+        """INT8 route errors against the exact oracle on the sampled entries:
+        the knob (moduli or slices) starts at the tuner's choice, is raised
+        until the route's error is no worse than the plain kernel's, then
+        lowered to the smallest value that still is."""
+        mf = self.mf
+        last = mf.ozaki_last_moduli if scheme == "modular" else mf.ozaki_last_slices
+        top = 49 if scheme == "modular" else 64
+        mf.gemm_(Cm, A, B, config=self.cfg(scheme, 0))
+        K0 = last()
+        K = K0
+        e = check()
+        e_tuner = e
 
-        # equal oracle error: the smallest S whose error is <= the plain error
-        while e_oz > e_plain and S < S0 + 6:
-            S += 1
-            e_oz = err_at(S)
-        while S > 1:
-            e_lo = err_at(S - 1)
+        def err_at(K):
+            mf.gemm_(Cm, A, B, config=self.cfg(scheme, K))
+            return check()
+
+        while e > e_plain and K < min(K0 + 6, top):
+            K += 1
+            e = err_at(K)
+        while K > 1:
+            try:
+                e_lo = err_at(K - 1)
+            except mf.ArgumentError:  # fewer moduli than the digit width needs
+                break
             if e_lo > e_plain:
                 break
-            S, e_oz = S - 1, e_lo
-        return {"plain_max_rel_err": e_plain, "ozaki_max_rel_err": e_oz, "slices": S,
-                "tuner_slices": S0, "tuner_max_rel_err": e_tuner, "samples": 256,
-                "rule": "smallest S with ozaki error <= plain error on the sampled entries"}
+            K, e = K - 1, e_lo
+        knob = "moduli" if scheme == "modular" else "slices"
+        return {"scheme": scheme, knob: K, "plain_max_rel_err": e_plain, "ozaki_max_rel_err": e,
+                f"tuner_{knob}": K0, "tuner_max_rel_err": e_tuner, "samples": 256,
+                "rule": f"smallest {knob} count with INT8-route error <= plain error on the "
+                        "sampled entries"}
 
-    def phases(self, N, n, A, B, Cm, S):
+    def phases(self, N, n, A, B, Cm, scheme, K):
         import ctypes as C
         mf = self.mf
         lib = mf._native.load()
@@ -302,9 +327,9 @@ class Runner:
         ops = C.c_double()
         one = (C.c_double * 4)(1.0)
         zero = (C.c_double * 4)()
-        rc = lib.mflab_gemm_ozaki_phases(h, self.stream.cuda_stream, N, S, n, n, n, A.ptr(), A.ld,
-                                         A.ls, B.ptr(), B.ld, B.ls, Cm.ptr(), Cm.ld, Cm.ls, one,
-                                         zero, ms, C.byref(ops))
+        fn = lib.mflab_gemm_ozaki_crt_phases if scheme == "modular" else lib.mflab_gemm_ozaki_phases
+        rc = fn(h, self.stream.cuda_stream, N, K, n, n, n, A.ptr(), A.ld, A.ls, B.ptr(), B.ld, B.ls,
+                Cm.ptr(), Cm.ld, Cm.ls, one, zero, ms, C.byref(ops))
         assert rc == 0, rc
         return [ms[i] for i in range(4)], ops.value
 
@@ -464,13 +489,28 @@ def main():
     peak_fp64 = fp64_peak(mf, torch)  # before the power-capped tensor work
     A, B = R.operands(N, n)
     Cm = mf.MFMatrix.zeros(N, n, n)
-    acc = R.accuracy_and_slices(N, n, A, B, Cm) if rank == 0 and route == "ozaki" else {}
-    S = acc.get("slices", 0)
+    scheme = args.scheme
+    acc, e_plain, check = {}, None, None
+    if rank == 0:
+        check = R.checker(n, A, B, Cm)
+        mf.gemm_(Cm, A, B)
+        e_plain = check()
+        if route != "ozaki":
+            acc = {"plain_max_rel_err": e_plain, "samples": 256}
+        else:
+            try:
+                acc = R.accuracy_search(N, n, A, B, Cm, scheme, e_plain, check)
+            except mf.ArgumentError:
+                if scheme != "modular":
+                    raise
+                scheme = "slices"  # the modulus table cannot reach the requirement
+                acc = R.accuracy_search(N, n, A, B, Cm, scheme, e_plain, check)
+    knob = acc.get("moduli", acc.get("slices", 0))
     if world > 1:
-        t = torch.tensor([S], device="cuda")
+        t = torch.tensor([knob, 1 if scheme == "modular" else 0], device="cuda")
         dist.broadcast(t, 0)
-        S = int(t.item())
-    oz_cfg = mf.KernelConfig(gemm_strategy="ozaki", ozaki_slices=S)
+        knob, scheme = int(t[0].item()), ("modular" if int(t[1].item()) else "slices")
+    oz_cfg = R.cfg(scheme, knob)
     head_cfg = oz_cfg if route == "ozaki" else plain_cfg
 
     clocks = ClockSampler(local)
@@ -480,13 +520,6 @@ def main():
     t_head /= args.steps
     t_plain = R.timed(lambda: mf.gemm_(Cm, A, B, config=plain_cfg), 1, 1) if route == "ozaki" \
         else t_head
-    if route != "ozaki" and rank == 0:
-        from oracle import mfref
-        rs = np.random.default_rng(5)
-        rows, cols = rs.integers(0, n, 256), rs.integers(0, n, 256)
-        mf.gemm_(Cm, A, B)
-        acc = {"plain_max_rel_err": float(np.max(_check_entries(
-            mfref, A.to_numpy(), B.to_numpy(), Cm, rows, cols)))}
 
     # end to end through the public API with host buffers
     hA = torch.empty((N, n, n), dtype=torch.float64, pin_memory=True)
@@ -513,22 +546,29 @@ def main():
                   "traffic": read_traffic(f"mm_x{N}_n{n}"),
                   "peak_source": "measured in this run (DFMA probe, burst)"}
     if route == "ozaki":
-        ph, ops = R.phases(N, n, A, B, Cm, S)
+        ph, ops = R.phases(N, n, A, B, Cm, scheme, knob)
         peak8 = R.int8_peak()
         achieved = ops / (ph[2] / 1e3)
         roof = {"bound": "tensor", "achieved": achieved / 1e12, "peak": peak8 / 1e12,
                 "unit": "INT8 TOP/s", "frac": achieved / peak8,
                 "frac_of_nominal_4500": achieved / 4.5e15,
-                "traffic": read_traffic(f"int8_tc_x{N}_n{n}"),
+                "traffic": read_traffic(f"int8_tc_{scheme}_x{N}_n{n}"),
                 "kernel": "mfl::int8_tc_gemm_kernel (tcgen05.mma kind::i8, TMA, TMEM): the int8 "
-                          "level GEMMs (K = (L-1) k)",
+                          + ("residue GEMMs, all moduli of a digit level in one launch"
+                             if scheme == "modular" else "level GEMMs (K = (L-1) k)"),
                 "peak_source": "measured in this run: cuBLASLt int8 TN GEMM 8192x8192x16384 "
                                "(burst); nominal dense INT8 is 4500 TOP/s",
-                "phases_ms": {"exponents_tune": ph[0], "split": ph[1], "int8_levels": ph[2],
-                              "accumulate": ph[3]}}
+                "phases_ms": {"exponents_tune": ph[0], "split": ph[1], "int8_gemms": ph[2],
+                              "reconstruct_accumulate": ph[3]}}
     else:
         roof = plain_roof
 
+    if route != "ozaki":
+        launches = 1
+    elif scheme == "modular":
+        launches = 5 + (1 if N == 2 else 2)  # scales 2, split 2, one GEMM launch per digit level, 1
+    else:
+        launches = 5 + knob                  # scales 2, split 2, one GEMM per level, accumulate
     value = world * flops / t_head / 1e9
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -536,7 +576,9 @@ def main():
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded randn * 2^U(-20,20), lower limbs randn*2^-53*|prev|)",
         "config": {"workload": f"Float64x{N} GEMM m=n=k={n}", "limbs": N, "n": n,
-                   "route": route, "slices": S if route == "ozaki" else None,
+                   "route": route, "scheme": scheme if route == "ozaki" else None,
+                   "moduli": knob if route == "ozaki" and scheme == "modular" else None,
+                   "slices": knob if route == "ozaki" and scheme == "slices" else None,
                    "parallelism": f"replicas{world}",
                    "l2": "inputs larger than L2 (each operand >= 1 GiB)"},
         "accuracy": acc,
@@ -547,21 +589,36 @@ def main():
                 "h2d_bytes_per_step": 2 * N * n * n * 8, "d2h_bytes_per_step": N * n * n * 8},
         "roofline": roof,
         "clocks": clk,
-        "gpu_launches": args.steps * (5 if route == "ozaki" else 1),
-        "library_launches": args.steps * S if route == "ozaki" else 0,
+        "gpu_launches": args.steps * launches,
+        "library_launches": 0,
     }
+    if rank == 0 and world == 1 and route == "ozaki" and scheme == "modular" \
+            and not args.no_slices:
+        # the digit-slice scheme on the same operands, at its own equal-error S
+        sacc = R.accuracy_search(N, n, A, B, Cm, "slices", e_plain, check)
+        ts = R.timed(lambda: mf.gemm_(Cm, A, B, config=R.cfg("slices", sacc["slices"])), 2, 1) / 2
+        line["slices_scheme"] = {"value": flops / ts / 1e9, "ms_per_step": ts * 1e3,
+                                 "speedup_vs_plain": t_plain / ts, "accuracy": sacc}
     if N == 2 and route == "ozaki" and not args.no_x4 and world == 1:
         del A, B, Cm
         torch.cuda.empty_cache()
         A4, B4 = R.operands(4, n)
         C4 = mf.MFMatrix.zeros(4, n, n)
-        acc4 = R.accuracy_and_slices(4, n, A4, B4, C4)
-        cfg4 = mf.KernelConfig(gemm_strategy="ozaki", ozaki_slices=acc4["slices"])
-        t4 = R.timed(lambda: mf.gemm_(C4, A4, B4, config=cfg4), 2, 1) / 2
+        chk4 = R.checker(n, A4, B4, C4)
         t4p = R.timed(lambda: mf.gemm_(C4, A4, B4), 1, 0)
-        line["x4"] = {"workload": f"Float64x4 GEMM m=n=k={n}", "ozaki_value": flops / t4 / 1e9,
-                      "ozaki_ms": t4 * 1e3, "plain_value": flops / t4p / 1e9,
-                      "plain_ms": t4p * 1e3, "speedup_vs_plain": t4p / t4, "accuracy": acc4}
+        e4p = chk4()
+        x4 = {"workload": f"Float64x4 GEMM m=n=k={n}", "plain_value": flops / t4p / 1e9,
+              "plain_ms": t4p * 1e3}
+        for sch in (("modular", "slices") if scheme == "modular" else ("slices",)):
+            try:
+                a4 = R.accuracy_search(4, n, A4, B4, C4, sch, e4p, chk4)
+            except mf.ArgumentError:
+                continue
+            k4 = a4.get("moduli", a4.get("slices"))
+            t4 = R.timed(lambda: mf.gemm_(C4, A4, B4, config=R.cfg(sch, k4)), 2, 1) / 2
+            x4[sch] = {"value": flops / t4 / 1e9, "ms": t4 * 1e3, "speedup_vs_plain": t4p / t4,
+                       "accuracy": a4}
+        line["x4"] = x4
     if rank == 0 and world == 1 and not args.no_configs:
         line["configs"] = run_configs(R, torch)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -109,6 +109,38 @@ int mflab_ozaki_default_slices(int limbs, int64_t k);
    counterpart). */
 int mflab_ozaki_last_slices(mflab_handle *h);
 
+/* C = alpha*A*B + beta*C on the INT8 tensor cores through residues (Ozaki
+   scheme II form): the scaled operands become Q integer digits of h bits
+   (Float64x2: Q = 1; Float64x3/x4: Q = 2), each digit is reduced modulo
+   `moduli` pairwise coprime numbers <= 256, one int8 GEMM per modulus and
+   digit level gives the exact residues of the integer products, and the
+   Chinese remainder theorem rebuilds them before the Float64xN accumulation.
+   moduli = 0 lets the tuner choose from the sampled scale gap (one stream
+   synchronisation); MFLAB_ERR_UNSUPPORTED when the requirement exceeds the
+   modulus table (then use mflab_gemm_ozaki).  The error is about
+   k * 2^(row scale + column scale) * 2^(-Q h).  Needs Q * roundup(k, 128) < 2^17.
+   Handle scratch: about moduli * Q * (m + n) * k bytes + 4 * moduli * Q * m * n bytes.
+   Non-finite input rows/columns give NaN.  No reference counterpart: a route
+   of gemm! (src/kernels/gemm.jl:747-774 keeps the reference's signature). */
+int mflab_gemm_ozaki_crt(mflab_handle *h, void *stream, int limbs, int moduli, int64_t m,
+                         int64_t n, int64_t k, const double *A, int64_t lda, int64_t lsa,
+                         const double *B, int64_t ldb, int64_t lsb, double *C, int64_t ldc,
+                         int64_t lsc, const double *alpha, const double *beta);
+
+/* modulus count used by the last mflab_gemm_ozaki_crt on this handle (no
+   reference counterpart). */
+int mflab_ozaki_last_moduli(mflab_handle *h);
+
+/* Host-only plan of mflab_gemm_ozaki_crt: digit count *Q, digit width *h
+   (bits) and modulus count *T for `limbs`, depth k and either moduli > 0 or,
+   with moduli == 0, a scale gap of gap8/8 bits (the tuner's input).  No
+   device work; no reference counterpart. */
+int mflab_ozaki_crt_plan(int limbs, int64_t k, int moduli, int gap8, int *Q, int *h, int *T);
+
+/* modulus number t of the route's table (0 <= t < table size), or the table
+   size when t < 0.  No reference counterpart. */
+int mflab_ozaki_crt_modulus(int t);
+
 /* Engine of the int8 level products of mflab_gemm_ozaki on this handle:
    MFLAB_INT8_TCGEN05 (default) or MFLAB_INT8_LIBRARY.  No reference
    counterpart. */

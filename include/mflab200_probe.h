@@ -25,6 +25,22 @@ int mflab_gemm_ozaki_phases(struct mflab_handle *h, void *stream, int limbs, int
                             int64_t lsc, const double *alpha, const double *beta, float *ms,
                             double *int8_ops);
 
+/* mflab_gemm_ozaki_crt (same arguments) with per-phase device times in
+   ms[4]: exponents + tuning, residue split, int8 GEMMs, reconstruction;
+   *int8_ops = 2 m n roundup(k,128) T Q(Q+1)/2 of the padded shapes.
+   Synchronises. */
+int mflab_gemm_ozaki_crt_phases(struct mflab_handle *h, void *stream, int limbs, int moduli,
+                                int64_t m, int64_t n, int64_t k, const double *A, int64_t lda,
+                                int64_t lsa, const double *B, int64_t ldb, int64_t lsb, double *C,
+                                int64_t ldc, int64_t lsc, const double *alpha, const double *beta,
+                                float *ms, double *int8_ops);
+
+/* Host copy of the modular route's reconstruction (tests): for `count`
+   problems of T int32 residue representatives each (G[e*T + t] ~ x mod p_t),
+   the 12 little-endian 32-bit words of |x| (mag[e*12 ...]) and its sign
+   (neg[e]) for the unique x in [-P/2, P/2).  No device work. */
+int mflab_ozaki_crt_reduce_host(int T, int count, const int32_t *G, uint32_t *mag, int *neg);
+
 /* Best device time (ms) of `reps` int8 x int8 -> int32 TN GEMMs of m x n x k
    through the library path the INT8-slice route uses.  Synchronises. */
 int mflab_probe_int8_gemm(struct mflab_handle *h, void *stream, int64_t m, int64_t n, int64_t k,

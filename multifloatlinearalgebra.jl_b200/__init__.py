@@ -139,6 +139,8 @@ class KernelConfig:
     gemm_micro_columns: int = 0
     ozaki_slices: int = 0
     ozaki_engine: str = "tcgen05"
+    ozaki_scheme: str = "auto"
+    ozaki_moduli: int = 0
     solve_order: str = "matched"
 
 
@@ -374,18 +376,69 @@ def gemm_(C_: MFMatrix, A: MFMatrix, B: MFMatrix, alpha=1.0, beta=0.0,
     route = _ROUTES[plan["strategy"]]
     lib, h, s = _lib_h(C_)
     if route == 2:
-        engines = {"tcgen05": 0, "library": 1}
-        if config.ozaki_engine not in engines:
-            raise ArgumentError("ozaki_engine must be :tcgen05 or :library")
-        _check(lib.mflab_set_int8_engine(h, engines[config.ozaki_engine]), "gemm!")
-        rc = lib.mflab_gemm_ozaki(h, s, N, int(config.ozaki_slices), m, n, k, A.ptr(), A.ld, A.ls,
-                                  B.ptr(), B.ld, B.ls, C_.ptr(), C_.ld, C_.ls, _scalar(N, alpha),
-                                  _scalar(N, beta))
+        rc = _gemm_ozaki(lib, h, s, N, C_, A, B, alpha, beta, config)
     else:
         rc = lib.mflab_gemm(h, s, N, route, m, n, k, A.ptr(), A.ld, A.ls, B.ptr(), B.ld, B.ls,
                             C_.ptr(), C_.ld, C_.ls, _scalar(N, alpha), _scalar(N, beta))
     _check(rc, "gemm!")
     return C_
+
+
+def ozaki_scheme(config: KernelConfig = _DEFAULT) -> str:
+    """The INT8 scheme a gemm_strategy=:ozaki call runs first: :slices when
+    ozaki_slices is set, :modular when ozaki_moduli is set, else
+    ozaki_scheme (:auto = :modular, with :slices when the modulus table
+    cannot reach the tuned requirement)."""
+    sch = config.ozaki_scheme
+    if sch not in ("auto", "slices", "modular"):
+        raise ArgumentError("ozaki_scheme must be :auto, :slices or :modular")
+    if sch == "auto":
+        if config.ozaki_slices > 0:
+            return "slices"
+        return "modular"
+    return sch
+
+
+def _gemm_ozaki(lib, h, s, N, C_, A, B, alpha, beta, config):
+    engines = {"tcgen05": 0, "library": 1}
+    if config.ozaki_engine not in engines:
+        raise ArgumentError("ozaki_engine must be :tcgen05 or :library")
+    if config.ozaki_slices < 0 or config.ozaki_moduli < 0:
+        raise ArgumentError("ozaki_slices and ozaki_moduli must be >= 0")
+    _check(lib.mflab_set_int8_engine(h, engines[config.ozaki_engine]), "gemm!")
+    m, k, n = A.m, A.n, B.n
+    args = (m, n, k, A.ptr(), A.ld, A.ls, B.ptr(), B.ld, B.ls, C_.ptr(), C_.ld, C_.ls,
+            _scalar(N, alpha), _scalar(N, beta))
+    scheme = ozaki_scheme(config)
+    if scheme == "modular":
+        rc = lib.mflab_gemm_ozaki_crt(h, s, N, int(config.ozaki_moduli), *args)
+        if rc != _native.MFLAB_ERR_UNSUPPORTED or config.ozaki_scheme == "modular" \
+                or config.ozaki_moduli > 0:
+            return rc
+    return lib.mflab_gemm_ozaki(h, s, N, int(config.ozaki_slices), *args)
+
+
+def ozaki_crt_plan(N: int, k: int, moduli: int = 0, gap_bits: float = 0.0) -> dict:
+    """Digit count Q, digit width h and modulus count T of the modular INT8
+    route for depth k: for `moduli` > 0 that count, else the tuner's choice
+    for a sampled scale gap of `gap_bits` (host-only, no device work)."""
+    Q, hh, T = C.c_int(), C.c_int(), C.c_int()
+    rc = _native.load().mflab_ozaki_crt_plan(N, k, moduli, int(round(8 * gap_bits)),
+                                             C.byref(Q), C.byref(hh), C.byref(T))
+    _check(rc, "ozaki_crt_plan")
+    return {"digits": Q.value, "digit_bits": hh.value, "moduli": T.value}
+
+
+def ozaki_crt_moduli() -> list:
+    """The modulus table of the modular INT8 route."""
+    lib = _native.load()
+    return [int(lib.mflab_ozaki_crt_modulus(t)) for t in range(lib.mflab_ozaki_crt_modulus(-1))]
+
+
+def ozaki_last_moduli(device: Optional[int] = None) -> int:
+    """Modulus count chosen by the last modular INT8 GEMM issued from this thread."""
+    dev = torch.cuda.current_device() if device is None else device
+    return int(_native.load().mflab_ozaki_last_moduli(_handle(dev)))
 
 
 def ozaki_default_slices(N: int, k: int) -> int:

@@ -93,6 +93,16 @@ SIGNATURES = {
     "mflab_gemm_ozaki": [_vp, _vp, _int, _int, _i64, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _i64,
                          _vp, _i64, _i64, _d, _d],
     "mflab_ozaki_default_slices": [_int, _i64],
+    "mflab_gemm_ozaki_crt": [_vp, _vp, _int, _int, _i64, _i64, _i64, _vp, _i64, _i64, _vp, _i64,
+                             _i64, _vp, _i64, _i64, _d, _d],
+    "mflab_ozaki_last_moduli": [_vp],
+    "mflab_ozaki_crt_plan": [_int, _i64, _int, _int, C.POINTER(_int), C.POINTER(_int),
+                             C.POINTER(_int)],
+    "mflab_ozaki_crt_modulus": [_int],
+    "mflab_ozaki_crt_reduce_host": [_int, _int, _vp, _vp, _vp],
+    "mflab_gemm_ozaki_crt_phases": [_vp, _vp, _int, _int, _i64, _i64, _i64, _vp, _i64, _i64, _vp,
+                                    _i64, _i64, _vp, _i64, _i64, _d, _d, C.POINTER(C.c_float),
+                                    _d],
     "mflab_ozaki_last_slices": [_vp],
     "mflab_set_int8_engine": [_vp, _int],
     "mflab_device_status": [_vp, C.POINTER(_int)],

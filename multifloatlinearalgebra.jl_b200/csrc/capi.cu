@@ -51,6 +51,7 @@ extern "C" int mflab_create(mflab_handle **out, int device) {
     h->aux = nullptr;
     h->aux_bytes = 0;
     h->last_slices = 0;
+    h->last_moduli = 0;
     h->solve_order = MFLAB_ORDER_MATCHED;
     h->int8_engine = MFLAB_INT8_TCGEN05;
     e = cudaMalloc((void **)&h->dev_flags, 64 * sizeof(int));

@@ -123,7 +123,7 @@ __device__ __forceinline__ void mma_commit(uint64_t *bar) {
 __global__ void __launch_bounds__(128, 1)
     int8_tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA,
                         const __grid_constant__ CUtensorMap tmB, int K, int b_xoff, int32_t *C,
-                        int64_t ldc, int *err) {
+                        int64_t ldc, int a_zrows, int b_zrows, int64_t c_zstride, int *err) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     uint64_t *full = (uint64_t *)(smem + TC_STAGES * TC_STAGE_BYTES);
@@ -133,7 +133,11 @@ __global__ void __launch_bounds__(128, 1)
     int *abort_flag = (int *)(tmem_slot + 1);
 
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    // blockIdx.z selects one of several stacked problems: its operands are the
+    // row blocks [z a_zrows, (z+1) a_zrows) of A and [z b_zrows, ...) of B
     const int m0 = blockIdx.x * TC_BM, n0 = blockIdx.y * TC_BN;
+    const int am0 = (int)blockIdx.z * a_zrows + m0, bn0 = (int)blockIdx.z * b_zrows + n0;
+    C += (int64_t)blockIdx.z * c_zstride;
     const int ksteps = K / TC_BK;
 
     if (threadIdx.x == 0) {
@@ -171,8 +175,8 @@ __global__ void __launch_bounds__(128, 1)
             uint8_t *sa = smem + s * TC_STAGE_BYTES;
             uint8_t *sb = sa + TC_A_BYTES;
             mbar_expect_tx(&full[s], TC_STAGE_BYTES);
-            tma_load_2d(sa, &tmA, i * TC_BK, m0, &full[s]);
-            tma_load_2d(sb, &tmB, b_xoff + i * TC_BK, n0, &full[s]);
+            tma_load_2d(sa, &tmA, i * TC_BK, am0, &full[s]);
+            tma_load_2d(sb, &tmB, b_xoff + i * TC_BK, bn0, &full[s]);
             ++issued;
         }
         // the copies issued last must have landed before the CTA can exit
@@ -271,17 +275,20 @@ static int make_map(CUtensorMap *map, const int8_t *base, int64_t rows, int64_t 
 // C (mp x np int32, ldc) = A[0:mp, a-range] * B[0:np, b_xoff : b_xoff + K]^T.
 // A is mp x a_cols, B np x b_cols, row-major int8 with leading dims lda, ldb.
 // Requires mp % 128 == 0, np % 256 == 0, K % 128 == 0, b_xoff % 16 == 0.
+// nz > 1 stacks problems: problem z reads rows [z mp, (z+1) mp) of A (which
+// then holds nz mp rows), rows [z np, (z+1) np) of B and writes C + z c_zstride.
 int int8_gemm_tc(int64_t mp, int64_t np, int64_t K, const int8_t *A, int64_t lda, int64_t a_cols,
                  const int8_t *B, int64_t ldb, int64_t b_cols, int64_t b_xoff, int32_t *C,
-                 int64_t ldc, int *err, cudaStream_t s) {
-    if (mp % TC_BM || np % TC_BN || K % TC_BK || b_xoff % 16 || K <= 0) return MFLAB_ERR_ARG;
+                 int64_t ldc, int *err, cudaStream_t s, int nz, int64_t c_zstride) {
+    if (mp % TC_BM || np % TC_BN || K % TC_BK || b_xoff % 16 || K <= 0 || nz < 1) return MFLAB_ERR_ARG;
     if (K > a_cols || b_xoff + K > b_cols || K > 0x7fffffff || b_xoff > 0x7fffffff)
         return MFLAB_ERR_ARG;
-    if (mp / TC_BM > 0x7fffffff || np / TC_BN > 65535) return MFLAB_ERR_UNSUPPORTED;
+    if (mp * nz > 0x7fffffff || np * nz > 0x7fffffff || np / TC_BN > 65535 || nz > 65535)
+        return MFLAB_ERR_UNSUPPORTED;
     CUtensorMap ta, tb;
-    int rc = make_map(&ta, A, mp, a_cols, lda, TC_BM);
+    int rc = make_map(&ta, A, mp * nz, a_cols, lda, TC_BM);
     if (rc) return rc;
-    rc = make_map(&tb, B, np, b_cols, ldb, TC_BN);
+    rc = make_map(&tb, B, np * nz, b_cols, ldb, TC_BN);
     if (rc) return rc;
     static bool configured = false;
     if (!configured) {
@@ -290,8 +297,9 @@ int int8_gemm_tc(int64_t mp, int64_t np, int64_t K, const int8_t *A, int64_t lda
         if (e != cudaSuccess) return record_cuda_error(e, "int8 tc attribute");
         configured = true;
     }
-    dim3 grid((unsigned)(mp / TC_BM), (unsigned)(np / TC_BN));
-    int8_tc_gemm_kernel<<<grid, 128, TC_SMEM, s>>>(ta, tb, (int)K, (int)b_xoff, C, ldc, err);
+    dim3 grid((unsigned)(mp / TC_BM), (unsigned)(np / TC_BN), (unsigned)nz);
+    int8_tc_gemm_kernel<<<grid, 128, TC_SMEM, s>>>(ta, tb, (int)K, (int)b_xoff, C, ldc, (int)mp,
+                                                   (int)np, c_zstride, err);
     return record_cuda_error(cudaGetLastError(), "int8 tc gemm");
 }
 

@@ -43,8 +43,11 @@ int int8_gemm_tn(int64_t m, int64_t n, int64_t K, const int8_t *A, int64_t lda, 
                  int64_t ldb, int32_t *I, int64_t ldi, void *ws, size_t wsb, cudaStream_t s);
 int int8_gemm_tc(int64_t mp, int64_t np, int64_t K, const int8_t *A, int64_t lda, int64_t a_cols,
                  const int8_t *B, int64_t ldb, int64_t b_cols, int64_t b_xoff, int32_t *C,
-                 int64_t ldc, int *err, cudaStream_t s);
+                 int64_t ldc, int *err, cudaStream_t s, int nz = 1, int64_t c_zstride = 0);
 void record_error_message(const char *msg);
+// modular INT8 route (ozaki_crt.cu); T = 0 lets the tuner choose
+int ozaki_crt_gemm(mflab_handle *hd, int N, int T, int64_t m, int64_t n, int64_t k, Mat A, Mat B,
+                   Mat C, const double *alpha, const double *beta, cudaStream_t s, int *T_used);
 
 inline bool valid_limbs(int N) { return N >= 2 && N <= 4; }
 
@@ -92,6 +95,7 @@ struct mflab_handle {
     void *aux;
     size_t aux_bytes;
     int last_slices;  // slice count the last Ozaki call used
+    int last_moduli;  // modulus count the last modular (CRT) INT8 call used
     int solve_order;  // MFLAB_ORDER_MATCHED or MFLAB_ORDER_FAST for triangular solves
     int int8_engine;  // MFLAB_INT8_TCGEN05 or MFLAB_INT8_LIBRARY for the level products
 };

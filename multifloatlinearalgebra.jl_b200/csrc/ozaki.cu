@@ -30,11 +30,9 @@
 
 #include "mf_device.cuh"
 #include "mflab_internal.h"
+#include "ozaki_common.cuh"
 
 namespace mfl {
-
-constexpr int OZ_EXP_EMPTY = INT_MIN / 2;   // a row/column with no nonzero entry
-constexpr int OZ_EXP_BAD = INT_MAX;         // a row/column holding a non-finite entry
 
 __device__ __forceinline__ int exp_of(double a) {
     int e;
@@ -81,11 +79,6 @@ __global__ void oz_col_exp_kernel(int64_t k, int64_t n, Mat B, int *colexp) {
         bad |= __shfl_xor_sync(0xffffffffu, bad, off);
     }
     if (lane == 0) colexp[j] = bad ? OZ_EXP_BAD : (mx > 0.0 ? exp_of(mx) : OZ_EXP_EMPTY);
-}
-
-__device__ __forceinline__ int oz_scale_exp(int e) {
-    // |x| < 2^e  ->  scaled by 2^-(e+1) lies in (-1/2, 1/2)
-    return (e == OZ_EXP_EMPTY || e == OZ_EXP_BAD) ? 0 : e + 1;
 }
 
 // digits of one scaled value; emit(s, d) is called for s = 0..S-1
@@ -299,9 +292,11 @@ static int oz_exponents(int64_t m, int64_t n, int64_t k, Mat A, Mat B, int *rowe
 // optional phase events (profiling entry point only): [0] after exponents and
 // tuning, [1] after the digit split, [2] after the level GEMMs, [3] at the end
 static cudaEvent_t *g_phase_ev = nullptr;
-static inline void phase(int i, cudaStream_t s) {
+void ozaki_phase(int i, cudaStream_t s) {
     if (g_phase_ev) cudaEventRecord(g_phase_ev[i], s);
 }
+void ozaki_set_phase_events(cudaEvent_t *ev) { g_phase_ev = ev; }
+static inline void phase(int i, cudaStream_t s) { ozaki_phase(i, s); }
 
 template <int N>
 static int ozaki_n(int64_t m, int64_t n, int64_t k, Mat A, Mat B, Mat C, const double *alpha,
@@ -372,11 +367,11 @@ static int tuned_slices(int N, int gap8) {
 
 static const int OZ_SAMPLES = 2048;
 
-int ozaki_gemm(mflab_handle *h, int N, int S, int64_t m, int64_t n, int64_t k, Mat A, Mat B,
-               Mat C, const double *alpha, const double *beta, cudaStream_t s, int *S_used) {
-    if (S < 0 || S > 64) return MFLAB_ERR_ARG;
-    if ((n + 255) / 256 * 256 > 65535LL || m > INT_MAX) return MFLAB_ERR_UNSUPPORTED;
-    // exponents (and the tuner's gap word) live in the aux scratch
+// Row / column scale exponents of A and B into the handle's aux scratch
+// (rowexp[m], colexp[n]); with tune != 0 also the sampled scale gap in
+// eighths of a bit (*gap8_host, one synchronisation).
+int ozaki_scales(mflab_handle *h, int N, int64_t m, int64_t n, int64_t k, Mat A, Mat B,
+                 cudaStream_t s, int tune, int *gap8_host, int **rowexp_out, int **colexp_out) {
     int rc = mflab_reserve_aux(h, sizeof(int) * (size_t)(m + n + 64));
     if (rc) return rc;
     int *rowexp = (int *)h->aux;
@@ -389,8 +384,9 @@ int ozaki_gemm(mflab_handle *h, int N, int S, int64_t m, int64_t n, int64_t k, M
     default: return MFLAB_ERR_UNSUPPORTED;
     }
     if (rc) return rc;
-    if (S == 0) {
-        // data-dependent slice count: one synchronisation to read the gap
+    *rowexp_out = rowexp;
+    *colexp_out = colexp;
+    if (tune) {
         cudaError_t e = cudaMemsetAsync(gap8, 0, sizeof(int), s);
         if (e != cudaSuccess) return record_cuda_error(e, "ozaki tune");
         oz_gap_kernel<<<(OZ_SAMPLES + 7) / 8, 256, 0, s>>>(m, n, k, A, B, rowexp, colexp,
@@ -399,8 +395,20 @@ int ozaki_gemm(mflab_handle *h, int N, int S, int64_t m, int64_t n, int64_t k, M
         e = cudaMemcpyAsync(&g, gap8, sizeof(int), cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) return record_cuda_error(e, "ozaki tune read");
-        S = tuned_slices(N, g);
+        *gap8_host = g;
     }
+    return MFLAB_OK;
+}
+
+int ozaki_gemm(mflab_handle *h, int N, int S, int64_t m, int64_t n, int64_t k, Mat A, Mat B,
+               Mat C, const double *alpha, const double *beta, cudaStream_t s, int *S_used) {
+    if (S < 0 || S > 64) return MFLAB_ERR_ARG;
+    if ((n + 255) / 256 * 256 > 65535LL || m > INT_MAX) return MFLAB_ERR_UNSUPPORTED;
+    int *rowexp = nullptr, *colexp = nullptr;
+    int g = 0;
+    int rc = ozaki_scales(h, N, m, n, k, A, B, s, S == 0, &g, &rowexp, &colexp);
+    if (rc) return rc;
+    if (S == 0) S = tuned_slices(N, g);
     const int smax = ozaki_max_slices(k);
     if (S > smax) S = smax;
     if (S < 1) return MFLAB_ERR_UNSUPPORTED;
@@ -424,9 +432,14 @@ extern "C" int mflab_gemm_ozaki_route(mflab_handle *h, void *stream, int limbs, 
                                       int64_t lsa, const double *B, int64_t ldb, int64_t lsb,
                                       double *C, int64_t ldc, int64_t lsc, const double *alpha,
                                       const double *beta) {
-    return mfl::ozaki_gemm(h, limbs, 0, m, n, k, mfl::Mat{(double *)A, lda, lsa},
-                           mfl::Mat{(double *)B, ldb, lsb}, mfl::Mat{C, ldc, lsc}, alpha, beta,
-                           (cudaStream_t)stream, &h->last_slices);
+    // the modular route first; the slice route when the modulus table cannot
+    // reach the tuned requirement
+    const mfl::Mat Am{(double *)A, lda, lsa}, Bm{(double *)B, ldb, lsb}, Cm{C, ldc, lsc};
+    cudaStream_t s = (cudaStream_t)stream;
+    if (k == 0) return mfl::launch_mm(limbs, false, false, 0, false, m, n, k, Am, Bm, Cm, alpha, beta, s);
+    int rc = mfl::ozaki_crt_gemm(h, limbs, 0, m, n, k, Am, Bm, Cm, alpha, beta, s, &h->last_moduli);
+    if (rc != MFLAB_ERR_UNSUPPORTED) return rc;
+    return mfl::ozaki_gemm(h, limbs, 0, m, n, k, Am, Bm, Cm, alpha, beta, s, &h->last_slices);
 }
 
 extern "C" int mflab_gemm_ozaki(mflab_handle *h, void *stream, int limbs, int slices, int64_t m,
@@ -441,6 +454,10 @@ extern "C" int mflab_gemm_ozaki(mflab_handle *h, void *stream, int limbs, int sl
         mfl::views_overlap(C, ldc, lsc, m, n, limbs, B, ldb, lsb, k, n))
         return MFLAB_ERR_ALIAS;
     if (slices < 0) return MFLAB_ERR_ARG;
+    if (k == 0)
+        return mfl::launch_mm(limbs, false, false, 0, false, m, n, k,
+                              mfl::Mat{(double *)A, lda, lsa}, mfl::Mat{(double *)B, ldb, lsb},
+                              mfl::Mat{C, ldc, lsc}, alpha, beta, (cudaStream_t)stream);
     return mfl::ozaki_gemm(h, limbs, slices, m, n, k, mfl::Mat{(double *)A, lda, lsa},
                            mfl::Mat{(double *)B, ldb, lsb}, mfl::Mat{C, ldc, lsc}, alpha, beta,
                            (cudaStream_t)stream, &h->last_slices);

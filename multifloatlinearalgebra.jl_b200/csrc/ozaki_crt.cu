@@ -1,0 +1,759 @@
+// Modular INT8 route for the multi-double GEMM: exact products of scaled
+// integer operands through residue arithmetic (Chinese remainder theorem).
+//
+// No reference counterpart: MultiFloatLinearAlgebra.jl has only the FP64
+// networks.  Published method: Ozaki, Uchino, Imamura (2025), "Ozaki scheme
+// II: a GEMM-oriented emulation of floating-point matrix multiplication using
+// an integer modular technique"; the CRT reconstruction below is plain
+// multi-word integer arithmetic of this file's own design.
+//
+// 1. Scaling (shared with the digit-slice route): row i of A is scaled by
+//    2^-sa_i, column j of B by 2^-sb_j, so that every scaled entry lies in
+//    (-1/2, 1/2).
+// 2. Integer digits.  The scaled value z is written as Q signed integer digits
+//    of h bits, z 2^(Q h) = sum_q D_q 2^(h (Q-1-q)) + remainder, |D_q| <= 2^(h+1),
+//    by the digit step of the slice route with 2^h in place of 2^7 (scale by
+//    2^h, round every limb to an integer, keep the exact remainder).  Float64x2
+//    uses one digit (Q = 1: the whole operand as one integer of h = beta bits);
+//    Float64x3/x4 use Q = 2.
+// 3. Residues.  For T pairwise coprime moduli p_t <= 256 (product P) every
+//    digit is reduced mod p_t to a signed byte; for each digit level L (pairs
+//    q + r = L, adjacent along K as in the slice route) and each modulus, ONE
+//    int8 GEMM gives G_L mod p_t exactly in int32 (|residues| <= 128, so
+//    Q k 2^14 < 2^31).  All T moduli of a level run in one launch.
+// 4. Reconstruction.  G_L = sum_t r_t U_t mod P with U_t = (P/p_t) ((P/p_t)^-1
+//    mod p_t), taken in the symmetric range (-P/2, P/2); P > 2 Q k max|D|^2
+//    makes this the exact integer sum_{q+r=L} D_q E_r.  G_L is converted to
+//    Float64xN with the add network, the levels are added least significant
+//    first, scaled by 2^(sa_i + sb_j - 2 Q h) and the alpha/beta epilogue of
+//    the plain kernel is applied.
+// The digits drop nothing but the final remainders and the levels L >= Q, so
+// the error is about k 2^(sa+sb) 2^(-Q h) (the same form as the slice route
+// with 7 S replaced by Q h) at T int8 GEMMs per level instead of S (S+1)/2.
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "mf_device.cuh"
+#include "mflab_internal.h"
+#include "ozaki_common.cuh"
+
+namespace mfl {
+
+constexpr int CRT_MAXT = 49;  // number of moduli in the table below
+constexpr int CRT_WD = 5;     // max 32-bit words of one digit magnitude (h <= 159)
+constexpr int CRT_WP = 12;    // max 32-bit words of a CRT sum (< 2^384)
+constexpr int CRT_MAXH = 32 * CRT_WD - 2;
+
+// Pairwise coprime moduli, greedy from 256 downwards (each is the largest
+// number <= 256 coprime to all before it).  Residues fit a signed byte.
+__host__ __device__ constexpr int crt_modulus(int t) {
+    switch (t) {
+    case 0: return 256;  case 1: return 255;  case 2: return 253;  case 3: return 251;
+    case 4: return 247;  case 5: return 241;  case 6: return 239;  case 7: return 233;
+    case 8: return 229;  case 9: return 227;  case 10: return 223; case 11: return 217;
+    case 12: return 211; case 13: return 199; case 14: return 197; case 15: return 193;
+    case 16: return 191; case 17: return 181; case 18: return 179; case 19: return 173;
+    case 20: return 167; case 21: return 163; case 22: return 157; case 23: return 151;
+    case 24: return 149; case 25: return 139; case 26: return 137; case 27: return 131;
+    case 28: return 127; case 29: return 113; case 30: return 109; case 31: return 107;
+    case 32: return 103; case 33: return 101; case 34: return 97;  case 35: return 89;
+    case 36: return 83;  case 37: return 79;  case 38: return 73;  case 39: return 71;
+    case 40: return 67;  case 41: return 61;  case 42: return 59;  case 43: return 53;
+    case 44: return 47;  case 45: return 43;  case 46: return 41;  case 47: return 37;
+    case 48: return 29;
+    default: return 1;
+    }
+}
+
+// weights of the digit bytes: wt[t][j] packs 2^(8 b) mod p_t for bytes
+// b = 4j .. 4j+3 of a digit magnitude (one byte each)
+struct CrtSplitConst {
+    uint32_t wt[CRT_MAXT][CRT_WD];
+};
+
+// reconstruction constants for one modulus count T
+struct CrtAccConst {
+    uint32_t U[CRT_MAXT][CRT_WP];  // U_t words, little endian
+    uint32_t P[CRT_WP];            // P words
+    double pinv;                   // 1 / P (rounded)
+};
+
+// ------------------------------------------------------------- digits ----
+// One h-bit digit of the scaled value z (updated to the remainder): the
+// magnitude as WD little-endian 32-bit words and the sign.
+template <int N, int WD>
+__device__ __forceinline__ void crt_digit(mf<N> &z, int h, uint32_t (&w)[WD], bool &neg) {
+    double d[N];
+#pragma unroll
+    for (int l = 0; l < N; ++l) {
+        z.v[l] = ldexp(z.v[l], h);                 // exact
+        d[l] = rint(z.v[l]);
+        z.v[l] = __dsub_rn(z.v[l], d[l]);          // exact: |z_l - rint(z_l)| <= 1/2
+    }
+#pragma unroll
+    for (int l = N - 1; l > 0; --l) two_sum(z.v[l - 1], z.v[l], z.v[l - 1], z.v[l]);
+    // sign of the digit = sign of its leading limb (lower limbs are below
+    // half an ulp of it, or zero when it is zero)
+    neg = d[0] < 0.0;
+    int64_t c[WD];
+#pragma unroll
+    for (int j = 0; j < WD; ++j) c[j] = 0;
+#pragma unroll
+    for (int l = 0; l < N; ++l) {
+        const double v = neg ? -d[l] : d[l];
+        if (v != 0.0) {
+            const double av = fabs(v);
+            const int64_t sg = v < 0.0 ? -1 : 1;
+            uint64_t mm;
+            int e;
+            if (av < 9007199254740992.0) {  // < 2^53: the integer itself
+                mm = (uint64_t)av;
+                e = 0;
+            } else {
+                int ex;
+                frexp(av, &ex);
+                mm = (uint64_t)ldexp(av, 53 - ex);  // 53-bit integer mantissa
+                e = ex - 53;
+            }
+#pragma unroll
+            for (int j = 0; j < WD; ++j) {
+                const int dd = 32 * j - e;  // bit of mm that lands on bit 0 of word j
+                uint32_t part = 0;
+                if (dd >= 0 && dd < 64) part = (uint32_t)(mm >> dd);
+                else if (dd < 0 && dd > -32) part = (uint32_t)(mm << (-dd));
+                c[j] += sg * (int64_t)part;
+            }
+        }
+    }
+    int64_t carry = 0;
+#pragma unroll
+    for (int j = 0; j < WD; ++j) {
+        const int64_t t = c[j] + carry;
+        w[j] = (uint32_t)t;
+        carry = t >> 32;
+    }
+}
+
+// signed-byte residue of (neg ? -1 : 1) * magnitude mod p
+template <int WD>
+__device__ __forceinline__ int crt_residue(const uint32_t (&w)[WD], const uint32_t *wt, int p,
+                                           bool neg) {
+    unsigned acc = 0;
+#pragma unroll
+    for (int j = 0; j < WD; ++j) acc = __dp4a(w[j], wt[j], acc);  // < 20 * 255^2
+    int r = (int)(acc % (unsigned)p);
+    if (neg && r) r = p - r;
+    return r >= 128 ? r - p : r;
+}
+
+// A (m x k, column-major planes) -> residue planes A8[t][i][q][k] (int8,
+// rows of Q kp bytes, plane stride plane8).  32 x 32 tile per block of
+// 32 x 8 threads, staged through shared memory; each thread then owns 4
+// consecutive k of one row and writes one 32-bit word per (t, q).
+template <int N, int WD>
+__global__ void __launch_bounds__(256)
+    crt_split_a_kernel(int64_t m, int64_t mp, int64_t k, int64_t kp, int Q, int h, int T, Mat A,
+                       const int *rowexp, int8_t *A8, size_t plane8,
+                       const __grid_constant__ CrtSplitConst c) {
+    __shared__ double tile[N][32][33];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int64_t i0 = (int64_t)blockIdx.x * 32, k0 = (int64_t)blockIdx.y * 32;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int kk = ty + 8 * j;
+        const int64_t i = i0 + tx, kg = k0 + kk;
+        const bool ok = i < m && kg < k;
+#pragma unroll
+        for (int l = 0; l < N; ++l) tile[l][kk][tx] = ok ? A.p[l * A.ls + kg * A.ld + i] : 0.0;
+    }
+    __syncthreads();
+    const int ii = ty * 4 + (tx >> 3), kq = (tx & 7) * 4;
+    const int64_t i = i0 + ii, kg = k0 + kq;
+    if (i >= mp || kg >= kp) return;  // kp is a multiple of 32: kg + 3 < kp
+    const int e = i < m ? rowexp[i] : OZ_EXP_EMPTY;
+    const int sh = oz_scale_exp(e);
+    mf<N> z[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+#pragma unroll
+        for (int l = 0; l < N; ++l)
+            z[u].v[l] = (e == OZ_EXP_BAD) ? 0.0 : ldexp(tile[l][kq + u][ii], -sh);
+#pragma unroll
+        for (int l = N - 1; l > 0; --l) two_sum(z[u].v[l - 1], z[u].v[l], z[u].v[l - 1], z[u].v[l]);
+    }
+    int8_t *dst = A8 + (size_t)i * Q * kp + kg;
+    for (int q = 0; q < Q; ++q) {
+        uint32_t w[4][WD];
+        bool ng[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) crt_digit<N, WD>(z[u], h, w[u], ng[u]);
+#pragma unroll
+        for (int t = 0; t < CRT_MAXT; ++t) {
+            if (t < T) {
+                uint32_t packed = 0;
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    packed |= (uint32_t)(uint8_t)(int8_t)crt_residue<WD>(w[u], c.wt[t],
+                                                                         crt_modulus(t), ng[u])
+                              << (8 * u);
+                *(uint32_t *)(dst + (size_t)t * plane8 + (size_t)q * kp) = packed;
+            }
+        }
+    }
+}
+
+// B (k x n) -> residue planes B8[t][j][Q-1-q][k] (digit order reversed so that
+// the pairs of one level are adjacent along K).  Each thread owns 4
+// consecutive k of one column.
+template <int N, int WD>
+__global__ void __launch_bounds__(128)
+    crt_split_b_kernel(int64_t k, int64_t n, int64_t np, int64_t kp, int Q, int h, int T, Mat B,
+                       const int *colexp, int8_t *B8, size_t plane8,
+                       const __grid_constant__ CrtSplitConst c) {
+    const int64_t kg = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * 4;
+    const int64_t j = blockIdx.y;
+    if (kg >= kp || j >= np) return;
+    const int e = j < n ? colexp[j] : OZ_EXP_EMPTY;
+    const int sh = oz_scale_exp(e);
+    mf<N> z[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int64_t kk = kg + u;
+        const bool ok = kk < k && j < n && e != OZ_EXP_BAD;
+#pragma unroll
+        for (int l = 0; l < N; ++l)
+            z[u].v[l] = ok ? ldexp(B.p[l * B.ls + j * B.ld + kk], -sh) : 0.0;
+#pragma unroll
+        for (int l = N - 1; l > 0; --l) two_sum(z[u].v[l - 1], z[u].v[l], z[u].v[l - 1], z[u].v[l]);
+    }
+    int8_t *dst = B8 + (size_t)j * Q * kp + kg;
+    for (int q = 0; q < Q; ++q) {
+        uint32_t w[4][WD];
+        bool ng[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) crt_digit<N, WD>(z[u], h, w[u], ng[u]);
+#pragma unroll
+        for (int t = 0; t < CRT_MAXT; ++t) {
+            if (t < T) {
+                uint32_t packed = 0;
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    packed |= (uint32_t)(uint8_t)(int8_t)crt_residue<WD>(w[u], c.wt[t],
+                                                                         crt_modulus(t), ng[u])
+                              << (8 * u);
+                *(uint32_t *)(dst + (size_t)t * plane8 + (size_t)(Q - 1 - q) * kp) = packed;
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------ reconstruction ----
+// X (WP words) -> the symmetric residue of X mod P as magnitude words + sign
+// (host and device: the host copy backs mflab_ozaki_crt_reduce_host)
+template <int WP>
+__host__ __device__ __forceinline__ bool crt_reduce(const uint64_t (&X)[WP], const CrtAccConst &c,
+                                           uint32_t (&mag)[WP]) {
+    uint32_t x[WP];
+    uint64_t cy = 0;
+#pragma unroll
+    for (int w = 0; w < WP; ++w) {
+        const uint64_t s = X[w] + cy;
+        x[w] = (uint32_t)s;
+        cy = s >> 32;
+    }
+    double xd = 0.0;
+#pragma unroll
+    for (int w = WP - 1; w >= 0; --w) xd = fma(xd, 4294967296.0, (double)x[w]);
+    const int64_t q = (int64_t)floor(xd * c.pinv);  // floor(X / P) or one off
+    uint32_t y[WP];
+    int64_t br = 0;
+#pragma unroll
+    for (int w = 0; w < WP; ++w) {
+        const int64_t s = (int64_t)x[w] - q * (int64_t)c.P[w] + br;
+        y[w] = (uint32_t)s;
+        br = s >> 32;
+    }
+    if (br < 0) {  // q one too large: add P back
+        uint64_t a = 0;
+#pragma unroll
+        for (int w = 0; w < WP; ++w) {
+            const uint64_t s = (uint64_t)y[w] + c.P[w] + a;
+            y[w] = (uint32_t)s;
+            a = s >> 32;
+        }
+    } else {       // q one too small: Y - P >= 0
+        uint32_t z[WP];
+        int64_t b2 = 0;
+#pragma unroll
+        for (int w = 0; w < WP; ++w) {
+            const int64_t s = (int64_t)y[w] - (int64_t)c.P[w] + b2;
+            z[w] = (uint32_t)s;
+            b2 = s >> 32;
+        }
+        if (b2 == 0) {
+#pragma unroll
+            for (int w = 0; w < WP; ++w) y[w] = z[w];
+        }
+    }
+    // Y in [0, P): Z = P - Y; the value is -Z when Y >= Z, else Y
+    uint32_t z[WP];
+    int64_t b3 = 0;
+#pragma unroll
+    for (int w = 0; w < WP; ++w) {
+        const int64_t s = (int64_t)c.P[w] - (int64_t)y[w] + b3;
+        z[w] = (uint32_t)s;
+        b3 = s >> 32;
+    }
+    int64_t b4 = 0;
+#pragma unroll
+    for (int w = 0; w < WP; ++w) b4 = ((int64_t)y[w] - (int64_t)z[w] + b4) >> 32;
+    const bool neg = (b4 == 0);
+#pragma unroll
+    for (int w = 0; w < WP; ++w) mag[w] = neg ? z[w] : y[w];
+    return neg;
+}
+
+// C = alpha * 2^(sa+sb-2Qh) sum_L 2^(h (2Q-2-L)) G_L (+ beta * C)
+template <int N, int WP>
+__global__ void __launch_bounds__(128)
+    crt_accum_kernel(int64_t m, int64_t n, int Q, int h, int T, const int32_t *I, int64_t ldi,
+                     size_t plane, const int *rowexp, const int *colexp, Mat C, scal<N> alpha,
+                     scal<N> beta, int overwrite, const __grid_constant__ CrtAccConst c) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t j = blockIdx.y;
+    if (i >= m || j >= n) return;
+    const int ea = rowexp[i], eb = colexp[j];
+    mf<N> acc = from_double<N>(0.0);
+    if (ea == OZ_EXP_BAD || eb == OZ_EXP_BAD) {
+        acc = from_double<N>(__longlong_as_double(0x7ff8000000000000LL));
+    } else {
+        for (int L = Q - 1; L >= 0; --L) {
+            uint64_t X[WP];
+#pragma unroll
+            for (int w = 0; w < WP; ++w) X[w] = 0;
+            const int32_t *src = I + (size_t)L * T * plane + (size_t)j * ldi + i;
+#pragma unroll
+            for (int t = 0; t < CRT_MAXT; ++t) {
+                if (t < T) {
+                    const int p = crt_modulus(t);
+                    int r = src[(size_t)t * plane] % p;
+                    r += r < 0 ? p : 0;
+#pragma unroll
+                    for (int w = 0; w < WP; ++w) X[w] += (uint64_t)(uint32_t)r * c.U[t][w];
+                }
+            }
+            uint32_t mag[WP];
+            const bool neg = crt_reduce<WP>(X, c, mag);
+            mf<N> g = from_double<N>(0.0);
+#pragma unroll
+            for (int w = 0; w < WP; ++w)
+                if (mag[w]) g = add(g, from_double<N>(ldexp((double)mag[w], 32 * w)));
+            const int lsh = h * (2 * Q - 2 - L);
+#pragma unroll
+            for (int l = 0; l < N; ++l) g.v[l] = ldexp(neg ? -g.v[l] : g.v[l], lsh);
+            acc = add(acc, g);
+        }
+        const int sh = oz_scale_exp(ea) + oz_scale_exp(eb) - 2 * Q * h;
+#pragma unroll
+        for (int l = 0; l < N; ++l) acc.v[l] = ldexp(acc.v[l], sh);
+    }
+    mf<N> r = mul(alpha.get(), acc);
+    if (!overwrite) r = add(r, mul(beta.get(), load_mf<N>(C.p, C.ld, C.ls, i, j)));
+    store_mf<N>(C.p, C.ld, C.ls, i, j, r);
+}
+
+// ----------------------------------------------------------- host side ---
+// little-endian base-2^32 integers for the constants
+using Big = std::vector<uint32_t>;
+
+static Big big_mul_small(const Big &a, uint32_t s) {
+    Big r(a.size() + 1, 0);
+    uint64_t cy = 0;
+    for (size_t i = 0; i < a.size(); ++i) {
+        const uint64_t v = (uint64_t)a[i] * s + cy;
+        r[i] = (uint32_t)v;
+        cy = v >> 32;
+    }
+    r[a.size()] = (uint32_t)cy;
+    while (r.size() > 1 && r.back() == 0) r.pop_back();
+    return r;
+}
+
+static Big big_div_small(const Big &a, uint32_t s, uint32_t *rem) {
+    Big r(a.size(), 0);
+    uint64_t cur = 0;
+    for (size_t i = a.size(); i-- > 0;) {
+        cur = (cur << 32) | a[i];
+        r[i] = (uint32_t)(cur / s);
+        cur %= s;
+    }
+    if (rem) *rem = (uint32_t)cur;
+    while (r.size() > 1 && r.back() == 0) r.pop_back();
+    return r;
+}
+
+static int big_bitlen(const Big &a) {
+    for (size_t i = a.size(); i-- > 0;)
+        if (a[i]) {
+            int b = 0;
+            while (b < 32 && (a[i] >> b)) ++b;
+            return (int)i * 32 + b;
+        }
+    return 0;
+}
+
+static uint32_t inv_mod(uint32_t a, uint32_t p) {
+    int64_t t = 0, nt = 1, r = p, nr = a % p;
+    while (nr) {
+        const int64_t qq = r / nr;
+        int64_t tmp = t - qq * nt;
+        t = nt;
+        nt = tmp;
+        tmp = r - qq * nr;
+        r = nr;
+        nr = tmp;
+    }
+    if (t < 0) t += p;
+    return (uint32_t)t;
+}
+
+struct CrtTables {
+    CrtAccConst acc;
+    int bitlen;  // bit length of P
+};
+
+static const CrtSplitConst &crt_split_const() {
+    static CrtSplitConst c;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        for (int t = 0; t < CRT_MAXT; ++t) {
+            const uint32_t p = (uint32_t)crt_modulus(t);
+            for (int j = 0; j < CRT_WD; ++j) {
+                uint32_t word = 0;
+                for (int u = 0; u < 4; ++u) {
+                    uint32_t v = 1 % p;  // 2^(8 b) mod p, b = 4j + u
+                    for (int b = 0; b < 4 * j + u; ++b) v = (v * 256u) % p;
+                    word |= v << (8 * u);
+                }
+                c.wt[t][j] = word;
+            }
+        }
+    });
+    return c;
+}
+
+static const CrtTables &crt_tables(int T) {
+    static CrtTables tab[CRT_MAXT + 1];
+    static std::once_flag once[CRT_MAXT + 1];
+    std::call_once(once[T], [T] {
+        CrtTables &c = tab[T];
+        memset(&c, 0, sizeof(c));
+        Big P{1};
+        for (int t = 0; t < T; ++t) P = big_mul_small(P, (uint32_t)crt_modulus(t));
+        c.bitlen = big_bitlen(P);
+        for (int t = 0; t < T; ++t) {
+            const uint32_t p = (uint32_t)crt_modulus(t);
+            uint32_t r = 0;
+            const Big M = big_div_small(P, p, nullptr);
+            big_div_small(M, p, &r);
+            const Big U = big_mul_small(M, inv_mod(r, p));
+            for (size_t w = 0; w < U.size() && w < (size_t)CRT_WP; ++w) c.acc.U[t][w] = U[w];
+        }
+        long double pd = 0.0L;
+        for (size_t w = P.size(); w-- > 0;) pd = pd * 4294967296.0L + (long double)P[w];
+        for (size_t w = 0; w < P.size() && w < (size_t)CRT_WP; ++w) c.acc.P[w] = P[w];
+        c.acc.pinv = (double)(1.0L / pd);
+    });
+    return tab[T];
+}
+
+static int ceil_log2(int64_t v) {
+    int l = 0;
+    while ((1LL << l) < v) ++l;
+    return l;
+}
+
+struct CrtPlan {
+    int Q, h, T, WD, WP;
+    int64_t kp, mp, np, ldi;
+    size_t plane, plane8a, plane8b, a8, b8, lev, ws, total;
+};
+
+// largest digit width h that T moduli support for Q digits and padded depth
+// kp: every digit is bounded by 2^h (Q = 1: |D| <= 2^(h-1) + N/2) or 2^(h+1)
+// (Q = 2: the second digit carries a remainder below 2 units), and
+// P > 2 Q kp bound^2 must hold
+static int crt_h_for(int T, int Q, int64_t kp) {
+    const int fl = crt_tables(T).bitlen - 1;  // P >= 2^fl
+    const int h = (fl - ceil_log2((int64_t)Q * kp) - (Q == 1 ? 2 : 4)) / 2;
+    return h < CRT_MAXH ? h : CRT_MAXH;
+}
+
+// Plan of one call.  T_req > 0: that many moduli, digits as wide as they
+// allow; T_req == 0: the tuner's requirement from the sampled scale gap.
+// Returns MFLAB_ERR_UNSUPPORTED when no table entry reaches the requirement.
+static int crt_plan(int N, int64_t m, int64_t n, int64_t k, int T_req, int gap8, CrtPlan &p) {
+    p.kp = (k + 127) / 128 * 128;
+    if (p.kp == 0) p.kp = 128;
+    if (T_req > 0) {
+        if (T_req > CRT_MAXT) return MFLAB_ERR_ARG;
+        p.Q = N == 2 ? 1 : 2;
+        p.T = T_req;
+        p.h = crt_h_for(p.T, p.Q, p.kp);
+    } else {
+        // bits below the row/column scale needed: working precision
+        // 53 N + 1, the sampled gap, a 6-bit margin and 1 bit for the
+        // (-1/2, 1/2) scaling; Q = 2 adds 1 bit for the dropped levels
+        const double gap = gap8 > 0 ? gap8 / 8.0 : 0.0;
+        const int beta = (int)ceil(53.0 * N + 1.0 + gap + 6.0 + 1.0);
+        p.Q = N == 2 ? 1 : 2;
+        p.h = p.Q == 1 ? beta : (beta + 2) / 2;
+        p.T = 0;
+        for (int T = 1; T <= CRT_MAXT; ++T)
+            if (crt_h_for(T, p.Q, p.kp) >= p.h) {
+                p.T = T;
+                break;
+            }
+        if (p.T == 0 || p.h > CRT_MAXH) return MFLAB_ERR_UNSUPPORTED;
+    }
+    if (p.h < 8) return MFLAB_ERR_UNSUPPORTED;
+    if ((int64_t)p.Q * p.kp * 16384 >= 2147483648LL) return MFLAB_ERR_UNSUPPORTED;
+    p.WD = (p.h + 2 + 31) / 32;
+    if (p.WD < 3) p.WD = 3;
+    const int need = crt_tables(p.T).bitlen + 14;  // X < T 256 P
+    p.WP = need <= 256 ? 8 : need <= 320 ? 10 : 12;
+    p.mp = (m + 127) / 128 * 128;
+    p.np = (n + 255) / 256 * 256;
+    p.ldi = p.mp;
+    p.plane = ((size_t)p.ldi * p.np + 63) / 64 * 64;
+    p.plane8a = (size_t)p.mp * p.Q * p.kp;
+    p.plane8b = (size_t)p.np * p.Q * p.kp;
+    auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+    p.a8 = al((size_t)p.T * p.plane8a);
+    p.b8 = al((size_t)p.T * p.plane8b);
+    p.lev = al((size_t)p.Q * p.T * p.plane * sizeof(int32_t));
+    p.ws = (size_t)64 << 20;
+    p.total = p.a8 + p.b8 + p.lev + p.ws;
+    return MFLAB_OK;
+}
+
+template <int N, int WD>
+static void crt_split(const CrtPlan &p, int64_t m, int64_t n, int64_t k, Mat A, Mat B,
+                      const int *rowexp, const int *colexp, int8_t *A8, int8_t *B8,
+                      cudaStream_t s) {
+    const CrtSplitConst &c = crt_split_const();
+    dim3 ga((unsigned)((p.mp + 31) / 32), (unsigned)(p.kp / 32));
+    crt_split_a_kernel<N, WD><<<ga, dim3(32, 8), 0, s>>>(m, p.mp, k, p.kp, p.Q, p.h, p.T, A,
+                                                         rowexp, A8, p.plane8a, c);
+    dim3 gb((unsigned)((p.kp / 4 + 127) / 128), (unsigned)p.np);
+    crt_split_b_kernel<N, WD><<<gb, 128, 0, s>>>(k, n, p.np, p.kp, p.Q, p.h, p.T, B, colexp, B8,
+                                                 p.plane8b, c);
+}
+
+template <int N>
+static void crt_split_n(const CrtPlan &p, int64_t m, int64_t n, int64_t k, Mat A, Mat B,
+                        const int *rowexp, const int *colexp, int8_t *A8, int8_t *B8,
+                        cudaStream_t s) {
+    if (p.WD <= 3) crt_split<N, 3>(p, m, n, k, A, B, rowexp, colexp, A8, B8, s);
+    else if (p.WD == 4) crt_split<N, 4>(p, m, n, k, A, B, rowexp, colexp, A8, B8, s);
+    else crt_split<N, 5>(p, m, n, k, A, B, rowexp, colexp, A8, B8, s);
+}
+
+template <int N, int WP>
+static void crt_accum(const CrtPlan &p, int64_t m, int64_t n, const int32_t *I, const int *rowexp,
+                      const int *colexp, Mat C, const scal<N> &al, const scal<N> &be,
+                      int overwrite, cudaStream_t s) {
+    dim3 g((unsigned)((m + 127) / 128), (unsigned)n);
+    crt_accum_kernel<N, WP><<<g, 128, 0, s>>>(m, n, p.Q, p.h, p.T, I, p.ldi, p.plane, rowexp,
+                                              colexp, C, al, be, overwrite,
+                                              crt_tables(p.T).acc);
+}
+
+template <int N>
+static int crt_gemm_n(mflab_handle *hd, const CrtPlan &p, int64_t m, int64_t n, int64_t k, Mat A,
+                      Mat B, Mat C, const double *alpha, const double *beta, const int *rowexp,
+                      const int *colexp, cudaStream_t s) {
+    char *base = (char *)hd->scratch;
+    int8_t *A8 = (int8_t *)base;
+    int8_t *B8 = (int8_t *)(base + p.a8);
+    int32_t *I = (int32_t *)(base + p.a8 + p.b8);
+    void *ws = base + p.a8 + p.b8 + p.lev;
+    ozaki_phase(0, s);
+    crt_split_n<N>(p, m, n, k, A, B, rowexp, colexp, A8, B8, s);
+    int rc = record_cuda_error(cudaGetLastError(), "modular split");
+    if (rc) return rc;
+    ozaki_phase(1, s);
+    const int64_t ld8 = (int64_t)p.Q * p.kp;
+    for (int L = 0; L < p.Q && rc == MFLAB_OK; ++L) {
+        const int64_t K = (int64_t)(L + 1) * p.kp, bx = (int64_t)(p.Q - 1 - L) * p.kp;
+        int32_t *IL = I + (size_t)L * p.T * p.plane;
+        if (hd->int8_engine == MFLAB_INT8_TCGEN05) {
+            rc = int8_gemm_tc(p.mp, p.np, K, A8, ld8, ld8, B8, ld8, ld8, bx, IL, p.ldi,
+                              hd->dev_flags + 1, s, p.T, (int64_t)p.plane);
+        } else {
+            for (int t = 0; t < p.T && rc == MFLAB_OK; ++t)
+                rc = int8_gemm_tn(p.mp, p.np, K, A8 + (size_t)t * p.plane8a, ld8,
+                                  B8 + (size_t)t * p.plane8b + bx, ld8, IL + (size_t)t * p.plane,
+                                  p.ldi, ws, p.ws, s);
+        }
+    }
+    if (rc) return rc;
+    ozaki_phase(2, s);
+    scal<N> al{}, be{};
+    int overwrite = 1;
+    for (int l = 0; l < N; ++l) {
+        al.v[l] = alpha[l];
+        be.v[l] = beta[l];
+        if (beta[l] != 0.0) overwrite = 0;
+    }
+    if (p.WP == 8) crt_accum<N, 8>(p, m, n, I, rowexp, colexp, C, al, be, overwrite, s);
+    else if (p.WP == 10) crt_accum<N, 10>(p, m, n, I, rowexp, colexp, C, al, be, overwrite, s);
+    else crt_accum<N, 12>(p, m, n, I, rowexp, colexp, C, al, be, overwrite, s);
+    ozaki_phase(3, s);
+    return record_cuda_error(cudaGetLastError(), "modular accumulate");
+}
+
+int ozaki_crt_gemm(mflab_handle *hd, int N, int T, int64_t m, int64_t n, int64_t k, Mat A, Mat B,
+                   Mat C, const double *alpha, const double *beta, cudaStream_t s,
+                   int *T_used) {
+    if (T < 0 || T > CRT_MAXT) return MFLAB_ERR_ARG;
+    if ((n + 255) / 256 * 256 > 65535LL || m > 0x3fffffffLL) return MFLAB_ERR_UNSUPPORTED;
+    CrtPlan p;
+    // the requirement check needs no device work when T is given
+    int rc = T > 0 ? crt_plan(N, m, n, k, T, 0, p) : MFLAB_OK;
+    if (rc) return rc;
+    if ((int64_t)(T > 0 ? p.T : CRT_MAXT) * ((m + 127) / 128 * 128) > 0x7fffffffLL)
+        return MFLAB_ERR_UNSUPPORTED;
+    int *rowexp = nullptr, *colexp = nullptr;
+    int g = 0;
+    rc = ozaki_scales(hd, N, m, n, k, A, B, s, T == 0, &g, &rowexp, &colexp);
+    if (rc) return rc;
+    if (T == 0) {
+        rc = crt_plan(N, m, n, k, 0, g, p);
+        if (rc) return rc;
+    }
+    if ((int64_t)p.T * p.mp > 0x7fffffffLL || (int64_t)p.T * p.np > 0x7fffffffLL)
+        return MFLAB_ERR_UNSUPPORTED;
+    rc = mflab_reserve_scratch(hd, p.total);
+    if (rc) return rc;
+    if (T_used) *T_used = p.T;
+    switch (N) {
+    case 2: return crt_gemm_n<2>(hd, p, m, n, k, A, B, C, alpha, beta, rowexp, colexp, s);
+    case 3: return crt_gemm_n<3>(hd, p, m, n, k, A, B, C, alpha, beta, rowexp, colexp, s);
+    default: return crt_gemm_n<4>(hd, p, m, n, k, A, B, C, alpha, beta, rowexp, colexp, s);
+    }
+}
+
+}  // namespace mfl
+
+// C = alpha*A*B + beta*C through the modular INT8 route; moduli = 0 lets the
+// sampled-gap tuner choose (one stream synchronisation).  Same argument
+// conventions and checks as mflab_gemm_ozaki.
+extern "C" int mflab_gemm_ozaki_crt(mflab_handle *h, void *stream, int limbs, int moduli,
+                                    int64_t m, int64_t n, int64_t k, const double *A, int64_t lda,
+                                    int64_t lsa, const double *B, int64_t ldb, int64_t lsb,
+                                    double *C, int64_t ldc, int64_t lsc, const double *alpha,
+                                    const double *beta) {
+    if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
+    if (m < 0 || n < 0 || k < 0 || !alpha || !beta) return MFLAB_ERR_ARG;
+    if (m == 0 || n == 0) return MFLAB_OK;
+    if (lda < (m > 0 ? m : 1) || ldb < (k > 0 ? k : 1) || ldc < m) return MFLAB_ERR_ARG;
+    if (mfl::views_overlap(C, ldc, lsc, m, n, limbs, A, lda, lsa, m, k) ||
+        mfl::views_overlap(C, ldc, lsc, m, n, limbs, B, ldb, lsb, k, n))
+        return MFLAB_ERR_ALIAS;
+    if (moduli < 0) return MFLAB_ERR_ARG;
+    if (k == 0)
+        return mfl::launch_mm(limbs, false, false, 0, false, m, n, k,
+                              mfl::Mat{(double *)A, lda, lsa}, mfl::Mat{(double *)B, ldb, lsb},
+                              mfl::Mat{C, ldc, lsc}, alpha, beta, (cudaStream_t)stream);
+    return mfl::ozaki_crt_gemm(h, limbs, moduli, m, n, k, mfl::Mat{(double *)A, lda, lsa},
+                               mfl::Mat{(double *)B, ldb, lsb}, mfl::Mat{C, ldc, lsc}, alpha,
+                               beta, (cudaStream_t)stream, &h->last_moduli);
+}
+
+extern "C" int mflab_ozaki_last_moduli(mflab_handle *h) { return h ? h->last_moduli : 0; }
+
+// Host-only planner of the modular route (no device work): for `limbs`, depth
+// k and either a modulus count (moduli > 0) or the tuner's sampled gap in
+// eighths of a bit (moduli == 0), the digit count Q, digit width h and
+// modulus count T a call would use.
+extern "C" int mflab_ozaki_crt_plan(int limbs, int64_t k, int moduli, int gap8, int *Q, int *h,
+                                    int *T) {
+    if (!mfl::valid_limbs(limbs) || k < 0 || moduli < 0 || !Q || !h || !T) return MFLAB_ERR_ARG;
+    mfl::CrtPlan p;
+    const int rc = mfl::crt_plan(limbs, 1, 1, k, moduli, gap8, p);
+    if (rc) return rc;
+    *Q = p.Q;
+    *h = p.h;
+    *T = p.T;
+    return MFLAB_OK;
+}
+
+// Host copy of the reconstruction step for tests: for `count` problems, G
+// holds T int32 values per problem (any representatives of the residues
+// mod p_t, as the int8 GEMMs produce them); mag receives 12 little-endian
+// words of |x| and neg the sign of the unique x in [-P/2, P/2) with
+// x = G_t mod p_t for all t.
+extern "C" int mflab_ozaki_crt_reduce_host(int T, int count, const int32_t *G, uint32_t *mag,
+                                           int *neg) {
+    using namespace mfl;
+    if (T < 1 || T > CRT_MAXT || count < 0 || !G || !mag || !neg) return MFLAB_ERR_ARG;
+    const CrtAccConst &c = crt_tables(T).acc;
+    for (int e = 0; e < count; ++e) {
+        uint64_t X[CRT_WP] = {0};
+        for (int t = 0; t < T; ++t) {
+            const int p = crt_modulus(t);
+            int r = G[(size_t)e * T + t] % p;
+            r += r < 0 ? p : 0;
+            for (int w = 0; w < CRT_WP; ++w) X[w] += (uint64_t)(uint32_t)r * c.U[t][w];
+        }
+        uint32_t mg[CRT_WP];
+        neg[e] = crt_reduce<CRT_WP>(X, c, mg) ? 1 : 0;
+        for (int w = 0; w < CRT_WP; ++w) mag[(size_t)e * CRT_WP + w] = mg[w];
+    }
+    return MFLAB_OK;
+}
+
+// modulus t of the table (0 <= t < count), or the table size for t < 0
+extern "C" int mflab_ozaki_crt_modulus(int t) {
+    if (t < 0) return mfl::CRT_MAXT;
+    return t < mfl::CRT_MAXT ? mfl::crt_modulus(t) : 0;
+}
+
+// mflab_gemm_ozaki_crt with per-phase device times (ms[0] scales + tuning,
+// ms[1] residue split, ms[2] int8 GEMMs, ms[3] reconstruction) and the
+// integer multiply-add operations of the GEMMs (2 m n K summed).  Synchronises.
+extern "C" int mflab_gemm_ozaki_crt_phases(mflab_handle *h, void *stream, int limbs, int moduli,
+                                           int64_t m, int64_t n, int64_t k, const double *A,
+                                           int64_t lda, int64_t lsa, const double *B,
+                                           int64_t ldb, int64_t lsb, double *C, int64_t ldc,
+                                           int64_t lsc, const double *alpha, const double *beta,
+                                           float *ms, double *int8_ops) {
+    if (!h || !ms || !int8_ops) return MFLAB_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaEvent_t ev[5];
+    for (auto &e : ev) cudaEventCreate(&e);
+    cudaEventRecord(ev[4], s);
+    mfl::ozaki_set_phase_events(ev);
+    int rc = mflab_gemm_ozaki_crt(h, stream, limbs, moduli, m, n, k, A, lda, lsa, B, ldb, lsb, C,
+                                  ldc, lsc, alpha, beta);
+    mfl::ozaki_set_phase_events(nullptr);
+    if (rc == MFLAB_OK) {
+        cudaError_t e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) rc = mfl::record_cuda_error(e, "modular phases");
+    }
+    if (rc == MFLAB_OK) {
+        cudaEventElapsedTime(&ms[0], ev[4], ev[0]);
+        cudaEventElapsedTime(&ms[1], ev[0], ev[1]);
+        cudaEventElapsedTime(&ms[2], ev[1], ev[2]);
+        cudaEventElapsedTime(&ms[3], ev[2], ev[3]);
+        mfl::CrtPlan p;
+        mfl::crt_plan(limbs, m, n, k, h->last_moduli, 0, p);
+        const double kp = (double)p.kp, mp = (double)p.mp, np = (double)p.np;
+        *int8_ops = 2.0 * mp * np * kp * (double)p.T * p.Q * (p.Q + 1) / 2.0;
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    return rc;
+}

@@ -26,7 +26,7 @@ def test_ozaki_default_slices_match_plain_accuracy(mf, ref, rng, N, shape):
     Ad, Bd = mf.MFMatrix.from_numpy(A), mf.MFMatrix.from_numpy(B)
     Cp, Co = mf.MFMatrix.zeros(N, m, n), mf.MFMatrix.zeros(N, m, n)
     mf.gemm_(Cp, Ad, Bd)
-    mf.gemm_(Co, Ad, Bd, config=mf.KernelConfig(gemm_strategy="ozaki"))
+    mf.gemm_(Co, Ad, Bd, config=mf.KernelConfig(gemm_strategy="ozaki", ozaki_scheme="slices"))
     ep = _err(ref, A, B, Cp.to_numpy(), np.random.default_rng(1))
     eo = _err(ref, A, B, Co.to_numpy(), np.random.default_rng(1))
     assert eo <= 4096 * k * 2.0 ** (-52 * N)
@@ -57,7 +57,7 @@ def test_ozaki_alpha_beta(mf, ref, rng, N):
     alpha, beta = syn.randn_mf(rng, N, 1, 1)[:, 0, 0], syn.randn_mf(rng, N, 1, 1)[:, 0, 0]
     Co = mf.MFMatrix.from_numpy(C0)
     mf.gemm_(Co, mf.MFMatrix.from_numpy(A), mf.MFMatrix.from_numpy(B), alpha, beta,
-             config=mf.KernelConfig(gemm_strategy="ozaki"))
+             config=mf.KernelConfig(gemm_strategy="ozaki", ozaki_scheme="slices"))
     want = ref.gemm(A, B, C0, alpha, beta)
     got = Co.to_numpy()
     scale = (np.abs(A[0]) @ np.abs(B[0])) * abs(alpha[0]) + np.abs(beta[0] * C0[0])
@@ -70,7 +70,7 @@ def test_ozaki_nonfinite_rows_give_nan(mf, rng):
     A[0, 3, 5] = np.inf
     Co = mf.MFMatrix.zeros(N, 8, 8)
     mf.gemm_(Co, mf.MFMatrix.from_numpy(A), mf.MFMatrix.from_numpy(B),
-             config=mf.KernelConfig(gemm_strategy="ozaki"))
+             config=mf.KernelConfig(gemm_strategy="ozaki", ozaki_scheme="slices"))
     got = Co.to_numpy()
     assert np.all(np.isnan(got[0, 3, :]))
     assert np.all(np.isfinite(np.delete(got[0], 3, axis=0)))
@@ -80,5 +80,5 @@ def test_ozaki_zero_matrix(mf):
     N = 2
     Co = mf.MFMatrix.zeros(N, 5, 7)
     mf.gemm_(Co, mf.MFMatrix.zeros(N, 5, 9), mf.MFMatrix.zeros(N, 9, 7),
-             config=mf.KernelConfig(gemm_strategy="ozaki"))
+             config=mf.KernelConfig(gemm_strategy="ozaki", ozaki_scheme="slices"))
     assert np.all(Co.to_numpy() == 0)
