@@ -27,6 +27,7 @@
 #include <mutex>
 
 #include "mflab_internal.h"
+#include "ozaki_common.cuh"
 
 namespace mfl {
 
@@ -120,9 +121,13 @@ __device__ __forceinline__ void mma_commit(uint64_t *bar) {
                  : "memory");
 }
 
+// MODE 0 stores the int32 sums; MODE 1 stores their residues modulo
+// crt_modulus(blockIdx.z) as bytes (C is then a byte matrix: ldc and
+// c_zstride in bytes), the only part of the sums the modular route needs.
+template <int MODE>
 __global__ void __launch_bounds__(128, 1)
     int8_tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA,
-                        const __grid_constant__ CUtensorMap tmB, int K, int b_xoff, int32_t *C,
+                        const __grid_constant__ CUtensorMap tmB, int K, int b_xoff, void *Cv,
                         int64_t ldc, int a_zrows, int b_zrows, int64_t c_zstride, int *err) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -137,7 +142,10 @@ __global__ void __launch_bounds__(128, 1)
     // row blocks [z a_zrows, (z+1) a_zrows) of A and [z b_zrows, ...) of B
     const int m0 = blockIdx.x * TC_BM, n0 = blockIdx.y * TC_BN;
     const int am0 = (int)blockIdx.z * a_zrows + m0, bn0 = (int)blockIdx.z * b_zrows + n0;
-    C += (int64_t)blockIdx.z * c_zstride;
+    int32_t *C = (int32_t *)Cv + (MODE == 0 ? (int64_t)blockIdx.z * c_zstride : 0);
+    uint8_t *R = (uint8_t *)Cv + (MODE == 1 ? (int64_t)blockIdx.z * c_zstride : 0);
+    const int pz = crt_modulus((int)blockIdx.z);
+    const double pzinv = 1.0 / (double)pz;
     const int ksteps = K / TC_BK;
 
     if (threadIdx.x == 0) {
@@ -228,8 +236,21 @@ __global__ void __launch_bounds__(128, 1)
             : "memory");
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
         if (store) {
+            if (MODE == 0) {
 #pragma unroll
-            for (int j = 0; j < 16; ++j) C[(int64_t)(n0 + c0 + j) * ldc + row] = (int32_t)v[j];
+                for (int j = 0; j < 16; ++j) C[(int64_t)(n0 + c0 + j) * ldc + row] = (int32_t)v[j];
+            } else {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const int g = (int)v[j];
+                    // floor(g / p) or one off; the remainder is then fixed up exactly
+                    const int q = (int)floor((double)g * pzinv);
+                    int r = g - q * pz;
+                    r += r < 0 ? pz : 0;
+                    r -= r >= pz ? pz : 0;
+                    R[(int64_t)(n0 + c0 + j) * ldc + row] = (uint8_t)r;
+                }
+            }
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -272,6 +293,34 @@ static int make_map(CUtensorMap *map, const int8_t *base, int64_t rows, int64_t 
     return r == CUDA_SUCCESS ? MFLAB_OK : MFLAB_ERR_UNSUPPORTED;
 }
 
+template <int MODE>
+static int launch_tc(int64_t mp, int64_t np, int64_t K, const int8_t *A, int64_t lda,
+                     int64_t a_cols, const int8_t *B, int64_t ldb, int64_t b_cols, int64_t b_xoff,
+                     void *C, int64_t ldc, int *err, cudaStream_t s, int nz, int64_t c_zstride) {
+    if (mp % TC_BM || np % TC_BN || K % TC_BK || b_xoff % 16 || K <= 0 || nz < 1) return MFLAB_ERR_ARG;
+    if (K > a_cols || b_xoff + K > b_cols || K > 0x7fffffff || b_xoff > 0x7fffffff)
+        return MFLAB_ERR_ARG;
+    if (mp * nz > 0x7fffffff || np * nz > 0x7fffffff || np / TC_BN > 65535 || nz > 65535)
+        return MFLAB_ERR_UNSUPPORTED;
+    if (MODE == 1 && nz > CRT_TABLE_SIZE) return MFLAB_ERR_ARG;
+    CUtensorMap ta, tb;
+    int rc = make_map(&ta, A, mp * nz, a_cols, lda, TC_BM);
+    if (rc) return rc;
+    rc = make_map(&tb, B, np * nz, b_cols, ldb, TC_BN);
+    if (rc) return rc;
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(int8_tc_gemm_kernel<MODE>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
+        if (e != cudaSuccess) return record_cuda_error(e, "int8 tc attribute");
+        configured = true;
+    }
+    dim3 grid((unsigned)(mp / TC_BM), (unsigned)(np / TC_BN), (unsigned)nz);
+    int8_tc_gemm_kernel<MODE><<<grid, 128, TC_SMEM, s>>>(ta, tb, (int)K, (int)b_xoff, C, ldc,
+                                                         (int)mp, (int)np, c_zstride, err);
+    return record_cuda_error(cudaGetLastError(), "int8 tc gemm");
+}
+
 // C (mp x np int32, ldc) = A[0:mp, a-range] * B[0:np, b_xoff : b_xoff + K]^T.
 // A is mp x a_cols, B np x b_cols, row-major int8 with leading dims lda, ldb.
 // Requires mp % 128 == 0, np % 256 == 0, K % 128 == 0, b_xoff % 16 == 0.
@@ -280,27 +329,19 @@ static int make_map(CUtensorMap *map, const int8_t *base, int64_t rows, int64_t 
 int int8_gemm_tc(int64_t mp, int64_t np, int64_t K, const int8_t *A, int64_t lda, int64_t a_cols,
                  const int8_t *B, int64_t ldb, int64_t b_cols, int64_t b_xoff, int32_t *C,
                  int64_t ldc, int *err, cudaStream_t s, int nz, int64_t c_zstride) {
-    if (mp % TC_BM || np % TC_BN || K % TC_BK || b_xoff % 16 || K <= 0 || nz < 1) return MFLAB_ERR_ARG;
-    if (K > a_cols || b_xoff + K > b_cols || K > 0x7fffffff || b_xoff > 0x7fffffff)
-        return MFLAB_ERR_ARG;
-    if (mp * nz > 0x7fffffff || np * nz > 0x7fffffff || np / TC_BN > 65535 || nz > 65535)
-        return MFLAB_ERR_UNSUPPORTED;
-    CUtensorMap ta, tb;
-    int rc = make_map(&ta, A, mp * nz, a_cols, lda, TC_BM);
-    if (rc) return rc;
-    rc = make_map(&tb, B, np * nz, b_cols, ldb, TC_BN);
-    if (rc) return rc;
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(int8_tc_gemm_kernel,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
-        if (e != cudaSuccess) return record_cuda_error(e, "int8 tc attribute");
-        configured = true;
-    }
-    dim3 grid((unsigned)(mp / TC_BM), (unsigned)(np / TC_BN), (unsigned)nz);
-    int8_tc_gemm_kernel<<<grid, 128, TC_SMEM, s>>>(ta, tb, (int)K, (int)b_xoff, C, ldc, (int)mp,
-                                                   (int)np, c_zstride, err);
-    return record_cuda_error(cudaGetLastError(), "int8 tc gemm");
+    return launch_tc<0>(mp, np, K, A, lda, a_cols, B, ldb, b_cols, b_xoff, C, ldc, err, s, nz,
+                        c_zstride);
+}
+
+// As int8_gemm_tc with nz stacked problems, but problem z stores the residues
+// of its sums modulo crt_modulus(z) as bytes: R + z r_zstride, column-major
+// with leading dimension ldr (bytes).
+int int8_gemm_tc_mod(int64_t mp, int64_t np, int64_t K, const int8_t *A, int64_t lda,
+                     int64_t a_cols, const int8_t *B, int64_t ldb, int64_t b_cols, int64_t b_xoff,
+                     uint8_t *R, int64_t ldr, int *err, cudaStream_t s, int nz,
+                     int64_t r_zstride) {
+    return launch_tc<1>(mp, np, K, A, lda, a_cols, B, ldb, b_cols, b_xoff, R, ldr, err, s, nz,
+                        r_zstride);
 }
 
 }  // namespace mfl

@@ -44,6 +44,10 @@ int int8_gemm_tn(int64_t m, int64_t n, int64_t K, const int8_t *A, int64_t lda, 
 int int8_gemm_tc(int64_t mp, int64_t np, int64_t K, const int8_t *A, int64_t lda, int64_t a_cols,
                  const int8_t *B, int64_t ldb, int64_t b_cols, int64_t b_xoff, int32_t *C,
                  int64_t ldc, int *err, cudaStream_t s, int nz = 1, int64_t c_zstride = 0);
+int int8_gemm_tc_mod(int64_t mp, int64_t np, int64_t K, const int8_t *A, int64_t lda,
+                     int64_t a_cols, const int8_t *B, int64_t ldb, int64_t b_cols, int64_t b_xoff,
+                     uint8_t *R, int64_t ldr, int *err, cudaStream_t s, int nz,
+                     int64_t r_zstride);
 void record_error_message(const char *msg);
 // modular INT8 route (ozaki_crt.cu); T = 0 lets the tuner choose
 int ozaki_crt_gemm(mflab_handle *hd, int N, int T, int64_t m, int64_t n, int64_t k, Mat A, Mat B,

@@ -41,31 +41,10 @@
 
 namespace mfl {
 
-constexpr int CRT_MAXT = 49;  // number of moduli in the table below
+constexpr int CRT_MAXT = CRT_TABLE_SIZE;
 constexpr int CRT_WD = 5;     // max 32-bit words of one digit magnitude (h <= 159)
 constexpr int CRT_WP = 12;    // max 32-bit words of a CRT sum (< 2^384)
 constexpr int CRT_MAXH = 32 * CRT_WD - 2;
-
-// Pairwise coprime moduli, greedy from 256 downwards (each is the largest
-// number <= 256 coprime to all before it).  Residues fit a signed byte.
-__host__ __device__ constexpr int crt_modulus(int t) {
-    switch (t) {
-    case 0: return 256;  case 1: return 255;  case 2: return 253;  case 3: return 251;
-    case 4: return 247;  case 5: return 241;  case 6: return 239;  case 7: return 233;
-    case 8: return 229;  case 9: return 227;  case 10: return 223; case 11: return 217;
-    case 12: return 211; case 13: return 199; case 14: return 197; case 15: return 193;
-    case 16: return 191; case 17: return 181; case 18: return 179; case 19: return 173;
-    case 20: return 167; case 21: return 163; case 22: return 157; case 23: return 151;
-    case 24: return 149; case 25: return 139; case 26: return 137; case 27: return 131;
-    case 28: return 127; case 29: return 113; case 30: return 109; case 31: return 107;
-    case 32: return 103; case 33: return 101; case 34: return 97;  case 35: return 89;
-    case 36: return 83;  case 37: return 79;  case 38: return 73;  case 39: return 71;
-    case 40: return 67;  case 41: return 61;  case 42: return 59;  case 43: return 53;
-    case 44: return 47;  case 45: return 43;  case 46: return 41;  case 47: return 37;
-    case 48: return 29;
-    default: return 1;
-    }
-}
 
 // weights of the digit bytes: wt[t][j] packs 2^(8 b) mod p_t for bytes
 // b = 4j .. 4j+3 of a digit magnitude (one byte each)
@@ -315,10 +294,11 @@ __host__ __device__ __forceinline__ bool crt_reduce(const uint64_t (&X)[WP], con
     return neg;
 }
 
-// C = alpha * 2^(sa+sb-2Qh) sum_L 2^(h (2Q-2-L)) G_L (+ beta * C)
+// C = alpha * 2^(sa+sb-2Qh) sum_L 2^(h (2Q-2-L)) G_L (+ beta * C); R holds
+// the residues G_L mod p_t as bytes, plane (L T + t) at R + (L T + t) plane
 template <int N, int WP>
 __global__ void __launch_bounds__(128)
-    crt_accum_kernel(int64_t m, int64_t n, int Q, int h, int T, const int32_t *I, int64_t ldi,
+    crt_accum_kernel(int64_t m, int64_t n, int Q, int h, int T, const uint8_t *R, int64_t ldi,
                      size_t plane, const int *rowexp, const int *colexp, Mat C, scal<N> alpha,
                      scal<N> beta, int overwrite, const __grid_constant__ CrtAccConst c) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -330,18 +310,18 @@ __global__ void __launch_bounds__(128)
         acc = from_double<N>(__longlong_as_double(0x7ff8000000000000LL));
     } else {
         for (int L = Q - 1; L >= 0; --L) {
+            const uint8_t *src = R + (size_t)L * T * plane + (size_t)j * ldi + i;
+            uint32_t r[CRT_MAXT];
+#pragma unroll
+            for (int t = 0; t < CRT_MAXT; ++t) r[t] = t < T ? (uint32_t)src[(size_t)t * plane] : 0u;
             uint64_t X[WP];
 #pragma unroll
             for (int w = 0; w < WP; ++w) X[w] = 0;
-            const int32_t *src = I + (size_t)L * T * plane + (size_t)j * ldi + i;
 #pragma unroll
             for (int t = 0; t < CRT_MAXT; ++t) {
                 if (t < T) {
-                    const int p = crt_modulus(t);
-                    int r = src[(size_t)t * plane] % p;
-                    r += r < 0 ? p : 0;
 #pragma unroll
-                    for (int w = 0; w < WP; ++w) X[w] += (uint64_t)(uint32_t)r * c.U[t][w];
+                    for (int w = 0; w < WP; ++w) X[w] += (uint64_t)r[t] * c.U[t][w];
                 }
             }
             uint32_t mag[WP];
@@ -362,6 +342,14 @@ __global__ void __launch_bounds__(128)
     mf<N> r = mul(alpha.get(), acc);
     if (!overwrite) r = add(r, mul(beta.get(), load_mf<N>(C.p, C.ld, C.ls, i, j)));
     store_mf<N>(C.p, C.ld, C.ls, i, j, r);
+}
+
+// residues of int32 sums modulo p as bytes (library-engine path)
+__global__ void crt_mod_kernel(const int32_t *G, uint8_t *R, size_t count, int p) {
+    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= count) return;
+    int r = G[e] % p;
+    R[e] = (uint8_t)(r < 0 ? r + p : r);
 }
 
 // ----------------------------------------------------------- host side ---
@@ -527,14 +515,14 @@ static int crt_plan(int N, int64_t m, int64_t n, int64_t k, int T_req, int gap8,
     p.mp = (m + 127) / 128 * 128;
     p.np = (n + 255) / 256 * 256;
     p.ldi = p.mp;
-    p.plane = ((size_t)p.ldi * p.np + 63) / 64 * 64;
+    p.plane = ((size_t)p.ldi * p.np + 255) / 256 * 256;
     p.plane8a = (size_t)p.mp * p.Q * p.kp;
     p.plane8b = (size_t)p.np * p.Q * p.kp;
     auto al = [](size_t b) { return (b + 255) / 256 * 256; };
     p.a8 = al((size_t)p.T * p.plane8a);
     p.b8 = al((size_t)p.T * p.plane8b);
-    p.lev = al((size_t)p.Q * p.T * p.plane * sizeof(int32_t));
-    p.ws = (size_t)64 << 20;
+    p.lev = al((size_t)p.Q * p.T * p.plane);                 // byte residues
+    p.ws = ((size_t)64 << 20) + al(p.plane * sizeof(int32_t));  // library path only
     p.total = p.a8 + p.b8 + p.lev + p.ws;
     return MFLAB_OK;
 }
@@ -562,7 +550,7 @@ static void crt_split_n(const CrtPlan &p, int64_t m, int64_t n, int64_t k, Mat A
 }
 
 template <int N, int WP>
-static void crt_accum(const CrtPlan &p, int64_t m, int64_t n, const int32_t *I, const int *rowexp,
+static void crt_accum(const CrtPlan &p, int64_t m, int64_t n, const uint8_t *I, const int *rowexp,
                       const int *colexp, Mat C, const scal<N> &al, const scal<N> &be,
                       int overwrite, cudaStream_t s) {
     dim3 g((unsigned)((m + 127) / 128), (unsigned)n);
@@ -578,8 +566,8 @@ static int crt_gemm_n(mflab_handle *hd, const CrtPlan &p, int64_t m, int64_t n, 
     char *base = (char *)hd->scratch;
     int8_t *A8 = (int8_t *)base;
     int8_t *B8 = (int8_t *)(base + p.a8);
-    int32_t *I = (int32_t *)(base + p.a8 + p.b8);
-    void *ws = base + p.a8 + p.b8 + p.lev;
+    uint8_t *Rs = (uint8_t *)(base + p.a8 + p.b8);
+    char *ws = base + p.a8 + p.b8 + p.lev;
     ozaki_phase(0, s);
     crt_split_n<N>(p, m, n, k, A, B, rowexp, colexp, A8, B8, s);
     int rc = record_cuda_error(cudaGetLastError(), "modular split");
@@ -588,15 +576,22 @@ static int crt_gemm_n(mflab_handle *hd, const CrtPlan &p, int64_t m, int64_t n, 
     const int64_t ld8 = (int64_t)p.Q * p.kp;
     for (int L = 0; L < p.Q && rc == MFLAB_OK; ++L) {
         const int64_t K = (int64_t)(L + 1) * p.kp, bx = (int64_t)(p.Q - 1 - L) * p.kp;
-        int32_t *IL = I + (size_t)L * p.T * p.plane;
+        uint8_t *RL = Rs + (size_t)L * p.T * p.plane;
         if (hd->int8_engine == MFLAB_INT8_TCGEN05) {
-            rc = int8_gemm_tc(p.mp, p.np, K, A8, ld8, ld8, B8, ld8, ld8, bx, IL, p.ldi,
-                              hd->dev_flags + 1, s, p.T, (int64_t)p.plane);
+            rc = int8_gemm_tc_mod(p.mp, p.np, K, A8, ld8, ld8, B8, ld8, ld8, bx, RL, p.ldi,
+                                  hd->dev_flags + 1, s, p.T, (int64_t)p.plane);
         } else {
-            for (int t = 0; t < p.T && rc == MFLAB_OK; ++t)
+            int32_t *G = (int32_t *)(ws + ((size_t)64 << 20));
+            const size_t cnt = (size_t)p.ldi * p.np;
+            for (int t = 0; t < p.T && rc == MFLAB_OK; ++t) {
                 rc = int8_gemm_tn(p.mp, p.np, K, A8 + (size_t)t * p.plane8a, ld8,
-                                  B8 + (size_t)t * p.plane8b + bx, ld8, IL + (size_t)t * p.plane,
-                                  p.ldi, ws, p.ws, s);
+                                  B8 + (size_t)t * p.plane8b + bx, ld8, G, p.ldi, ws,
+                                  (size_t)64 << 20, s);
+                if (rc) break;
+                crt_mod_kernel<<<(unsigned)((cnt + 255) / 256), 256, 0, s>>>(
+                    G, RL + (size_t)t * p.plane, cnt, crt_modulus(t));
+                rc = record_cuda_error(cudaGetLastError(), "modular residues");
+            }
         }
     }
     if (rc) return rc;
@@ -608,9 +603,9 @@ static int crt_gemm_n(mflab_handle *hd, const CrtPlan &p, int64_t m, int64_t n, 
         be.v[l] = beta[l];
         if (beta[l] != 0.0) overwrite = 0;
     }
-    if (p.WP == 8) crt_accum<N, 8>(p, m, n, I, rowexp, colexp, C, al, be, overwrite, s);
-    else if (p.WP == 10) crt_accum<N, 10>(p, m, n, I, rowexp, colexp, C, al, be, overwrite, s);
-    else crt_accum<N, 12>(p, m, n, I, rowexp, colexp, C, al, be, overwrite, s);
+    if (p.WP == 8) crt_accum<N, 8>(p, m, n, Rs, rowexp, colexp, C, al, be, overwrite, s);
+    else if (p.WP == 10) crt_accum<N, 10>(p, m, n, Rs, rowexp, colexp, C, al, be, overwrite, s);
+    else crt_accum<N, 12>(p, m, n, Rs, rowexp, colexp, C, al, be, overwrite, s);
     ozaki_phase(3, s);
     return record_cuda_error(cudaGetLastError(), "modular accumulate");
 }

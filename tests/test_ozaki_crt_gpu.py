@@ -168,7 +168,8 @@ def test_modular_zero_and_empty(mf):
     mf.gemm_(Co, mf.MFMatrix.zeros(N, 5, 9), mf.MFMatrix.zeros(N, 9, 7), config=_cfg(mf))
     assert np.all(Co.to_numpy() == 0)
     # k = 0: C = beta * C
-    C0 = np.ones((N, 4, 3))
+    C0 = np.zeros((N, 4, 3))
+    C0[0] = 1.0
     Cd = mf.MFMatrix.from_numpy(C0)
     mf.gemm_(Cd, mf.MFMatrix.zeros(N, 4, 0), mf.MFMatrix.zeros(N, 0, 3), 1.0, 2.0,
              config=_cfg(mf))
