@@ -229,11 +229,12 @@ __global__ void __launch_bounds__(128)
 }
 
 // ------------------------------------------------------ reconstruction ----
-// X (WP words) -> the symmetric residue of X mod P as magnitude words + sign
-// (host and device: the host copy backs mflab_ozaki_crt_reduce_host)
+// X (WP words of 64-bit partial sums) -> the symmetric residue of X mod P as
+// magnitude words + sign (host and device: the host copy backs
+// mflab_ozaki_crt_reduce_host).  All products are 32 x 32 -> 64 bit.
 template <int WP>
 __host__ __device__ __forceinline__ bool crt_reduce(const uint64_t (&X)[WP], const CrtAccConst &c,
-                                           uint32_t (&mag)[WP]) {
+                                                    uint32_t (&mag)[WP]) {
     uint32_t x[WP];
     uint64_t cy = 0;
 #pragma unroll
@@ -242,62 +243,109 @@ __host__ __device__ __forceinline__ bool crt_reduce(const uint64_t (&X)[WP], con
         x[w] = (uint32_t)s;
         cy = s >> 32;
     }
+    // floor(X / P) or one off (X / P < 2^14: the rounding error of the
+    // double evaluation is far below one unit)
     double xd = 0.0;
 #pragma unroll
     for (int w = WP - 1; w >= 0; --w) xd = fma(xd, 4294967296.0, (double)x[w]);
-    const int64_t q = (int64_t)floor(xd * c.pinv);  // floor(X / P) or one off
+    const uint32_t q = (uint32_t)floor(xd * c.pinv);
+    // Y = X - q P (borrow chain; the final borrow is the sign of Y)
     uint32_t y[WP];
-    int64_t br = 0;
+    uint64_t hi = 0;   // carry of q P
+    uint32_t br = 0;   // borrow
 #pragma unroll
     for (int w = 0; w < WP; ++w) {
-        const int64_t s = (int64_t)x[w] - q * (int64_t)c.P[w] + br;
-        y[w] = (uint32_t)s;
-        br = s >> 32;
+        const uint64_t qp = (uint64_t)q * c.P[w] + hi;
+        hi = qp >> 32;
+        const uint64_t d = (uint64_t)x[w] - (uint32_t)qp - br;
+        y[w] = (uint32_t)d;
+        br = (uint32_t)(d >> 63);
     }
-    if (br < 0) {  // q one too large: add P back
-        uint64_t a = 0;
+    if (br) {  // q one too large: Y + P
+        uint32_t ca = 0;
 #pragma unroll
         for (int w = 0; w < WP; ++w) {
-            const uint64_t s = (uint64_t)y[w] + c.P[w] + a;
-            y[w] = (uint32_t)s;
-            a = s >> 32;
+            const uint64_t t = (uint64_t)y[w] + c.P[w] + ca;
+            y[w] = (uint32_t)t;
+            ca = (uint32_t)(t >> 32);
         }
-    } else {       // q one too small: Y - P >= 0
+    } else {   // q one too small: Y - P when that is >= 0
         uint32_t z[WP];
-        int64_t b2 = 0;
+        uint32_t b2 = 0;
 #pragma unroll
         for (int w = 0; w < WP; ++w) {
-            const int64_t s = (int64_t)y[w] - (int64_t)c.P[w] + b2;
-            z[w] = (uint32_t)s;
-            b2 = s >> 32;
+            const uint64_t d = (uint64_t)y[w] - c.P[w] - b2;
+            z[w] = (uint32_t)d;
+            b2 = (uint32_t)(d >> 63);
         }
-        if (b2 == 0) {
+        if (!b2) {
 #pragma unroll
             for (int w = 0; w < WP; ++w) y[w] = z[w];
         }
     }
     // Y in [0, P): Z = P - Y; the value is -Z when Y >= Z, else Y
     uint32_t z[WP];
-    int64_t b3 = 0;
+    uint32_t b3 = 0, b4 = 0;
 #pragma unroll
     for (int w = 0; w < WP; ++w) {
-        const int64_t s = (int64_t)c.P[w] - (int64_t)y[w] + b3;
-        z[w] = (uint32_t)s;
-        b3 = s >> 32;
+        const uint64_t d = (uint64_t)c.P[w] - y[w] - b3;
+        z[w] = (uint32_t)d;
+        b3 = (uint32_t)(d >> 63);
+        const uint64_t e = (uint64_t)y[w] - z[w] - b4;
+        b4 = (uint32_t)(e >> 63);
     }
-    int64_t b4 = 0;
-#pragma unroll
-    for (int w = 0; w < WP; ++w) b4 = ((int64_t)y[w] - (int64_t)z[w] + b4) >> 32;
     const bool neg = (b4 == 0);
 #pragma unroll
     for (int w = 0; w < WP; ++w) mag[w] = neg ? z[w] : y[w];
     return neg;
 }
 
+// Float64xN value of a WP-word magnitude times 2^e2: the top 53 N bits as N
+// truncated 53-bit chunks (exact for values with at most 53 N significant
+// bits), combined with the add network
+template <int N, int WP>
+__device__ __forceinline__ mf<N> crt_words_to_mf(const uint32_t (&mag)[WP], int e2) {
+    int pos = -1;
+#pragma unroll
+    for (int w = 0; w < WP; ++w) pos = mag[w] ? w : pos;
+    if (pos < 0) return from_double<N>(0.0);
+    // barrel shift by whole words so that word pos lands on WP - 1
+    uint32_t a[WP];
+#pragma unroll
+    for (int w = 0; w < WP; ++w) a[w] = mag[w];
+    const int sw = WP - 1 - pos;
+#pragma unroll
+    for (int b = 8; b >= 1; b >>= 1) {
+        if (b < WP && (sw & b)) {
+#pragma unroll
+            for (int w = WP - 1; w >= 0; --w) a[w] = w >= b ? a[w - b] : 0u;
+        }
+    }
+    const int lz = __clz(a[WP - 1]);
+#pragma unroll
+    for (int w = WP - 1; w > 0; --w) a[w] = __funnelshift_l(a[w - 1], a[w], lz);
+    a[0] <<= lz;
+    // the window's bit 32 WP - 1 has weight 2^(32 pos + 31 - lz + e2)
+    const int top = 32 * pos + 32 - lz + e2;
+    mf<N> g = from_double<N>(0.0);
+#pragma unroll
+    for (int l = N - 1; l >= 0; --l) {
+        const int b0 = 32 * WP - 53 * (l + 1);  // lowest bit of chunk l in the window
+        const int wi = b0 >> 5, off = b0 & 31;
+        uint64_t ch = (uint64_t)a[wi] >> off;
+        if (wi + 1 < WP) ch |= (uint64_t)a[wi + 1] << (32 - off);
+        if (wi + 2 < WP && off > 11) ch |= (uint64_t)a[wi + 2] << (64 - off);
+        ch &= (1ULL << 53) - 1;
+        const double d = ldexp((double)ch, top - 53 * (l + 1));
+        g = l == N - 1 ? from_double<N>(d) : add(g, from_double<N>(d));
+    }
+    return g;
+}
+
 // C = alpha * 2^(sa+sb-2Qh) sum_L 2^(h (2Q-2-L)) G_L (+ beta * C); R holds
 // the residues G_L mod p_t as bytes, plane (L T + t) at R + (L T + t) plane
 template <int N, int WP>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 3)
     crt_accum_kernel(int64_t m, int64_t n, int Q, int h, int T, const uint8_t *R, int64_t ldi,
                      size_t plane, const int *rowexp, const int *colexp, Mat C, scal<N> alpha,
                      scal<N> beta, int overwrite, const __grid_constant__ CrtAccConst c) {
@@ -311,33 +359,34 @@ __global__ void __launch_bounds__(128)
     } else {
         for (int L = Q - 1; L >= 0; --L) {
             const uint8_t *src = R + (size_t)L * T * plane + (size_t)j * ldi + i;
-            uint32_t r[CRT_MAXT];
-#pragma unroll
-            for (int t = 0; t < CRT_MAXT; ++t) r[t] = t < T ? (uint32_t)src[(size_t)t * plane] : 0u;
             uint64_t X[WP];
 #pragma unroll
             for (int w = 0; w < WP; ++w) X[w] = 0;
+            // residues in groups of 8: the loads of a group are in flight together
 #pragma unroll
-            for (int t = 0; t < CRT_MAXT; ++t) {
-                if (t < T) {
+            for (int t0 = 0; t0 < CRT_MAXT; t0 += 8) {
+                if (t0 < T) {
+                    uint32_t r[8];
 #pragma unroll
-                    for (int w = 0; w < WP; ++w) X[w] += (uint64_t)r[t] * c.U[t][w];
+                    for (int u = 0; u < 8; ++u)
+                        r[u] = (t0 + u < T && t0 + u < CRT_MAXT)
+                                   ? (uint32_t)__ldg(src + (size_t)(t0 + u) * plane) : 0u;
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) {
+                        if (t0 + u < CRT_MAXT) {
+#pragma unroll
+                            for (int w = 0; w < WP; ++w) X[w] += (uint64_t)r[u] * c.U[t0 + u][w];
+                        }
+                    }
                 }
             }
             uint32_t mag[WP];
-            const bool neg = crt_reduce<WP>(X, c, mag);
-            mf<N> g = from_double<N>(0.0);
-#pragma unroll
-            for (int w = 0; w < WP; ++w)
-                if (mag[w]) g = add(g, from_double<N>(ldexp((double)mag[w], 32 * w)));
-            const int lsh = h * (2 * Q - 2 - L);
-#pragma unroll
-            for (int l = 0; l < N; ++l) g.v[l] = ldexp(neg ? -g.v[l] : g.v[l], lsh);
-            acc = add(acc, g);
+            const bool ng = crt_reduce<WP>(X, c, mag);
+            const int sh = oz_scale_exp(ea) + oz_scale_exp(eb) - 2 * Q * h + h * (2 * Q - 2 - L);
+            mf<N> g = crt_words_to_mf<N, WP>(mag, sh);
+            if (ng) g = neg(g);
+            acc = L == Q - 1 ? g : add(acc, g);
         }
-        const int sh = oz_scale_exp(ea) + oz_scale_exp(eb) - 2 * Q * h;
-#pragma unroll
-        for (int l = 0; l < N; ++l) acc.v[l] = ldexp(acc.v[l], sh);
     }
     mf<N> r = mul(alpha.get(), acc);
     if (!overwrite) r = add(r, mul(beta.get(), load_mf<N>(C.p, C.ld, C.ls, i, j)));
