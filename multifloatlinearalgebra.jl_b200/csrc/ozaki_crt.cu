@@ -300,9 +300,10 @@ __host__ __device__ __forceinline__ bool crt_reduce(const uint64_t (&X)[WP], con
     return neg;
 }
 
-// Float64xN value of a WP-word magnitude times 2^e2: the top 53 N bits as N
-// truncated 53-bit chunks (exact for values with at most 53 N significant
-// bits), combined with the add network
+// Float64xN value of a WP-word magnitude times 2^e2: the top 53 (N+1) bits as
+// N+1 truncated 53-bit chunks (exact for values with at most 53 (N+1)
+// significant bits), summed least significant first with the add network,
+// which rounds the guard chunk into the N limbs
 template <int N, int WP>
 __device__ __forceinline__ mf<N> crt_words_to_mf(const uint32_t (&mag)[WP], int e2) {
     int pos = -1;
@@ -329,15 +330,20 @@ __device__ __forceinline__ mf<N> crt_words_to_mf(const uint32_t (&mag)[WP], int 
     const int top = 32 * pos + 32 - lz + e2;
     mf<N> g = from_double<N>(0.0);
 #pragma unroll
-    for (int l = N - 1; l >= 0; --l) {
+    for (int l = N; l >= 0; --l) {
         const int b0 = 32 * WP - 53 * (l + 1);  // lowest bit of chunk l in the window
-        const int wi = b0 >> 5, off = b0 & 31;
-        uint64_t ch = (uint64_t)a[wi] >> off;
-        if (wi + 1 < WP) ch |= (uint64_t)a[wi + 1] << (32 - off);
-        if (wi + 2 < WP && off > 11) ch |= (uint64_t)a[wi + 2] << (64 - off);
+        uint64_t ch;
+        if (b0 >= 0) {
+            const int wi = b0 >> 5, off = b0 & 31;
+            ch = (uint64_t)a[wi] >> off;
+            if (wi + 1 < WP) ch |= (uint64_t)a[wi + 1] << (32 - off);
+            if (wi + 2 < WP && off > 11) ch |= (uint64_t)a[wi + 2] << (64 - off);
+        } else {  // the window ends inside the chunk: its low bits are zero
+            ch = b0 > -53 ? ((uint64_t)a[0] | ((uint64_t)a[1] << 32)) << (-b0) : 0;
+        }
         ch &= (1ULL << 53) - 1;
         const double d = ldexp((double)ch, top - 53 * (l + 1));
-        g = l == N - 1 ? from_double<N>(d) : add(g, from_double<N>(d));
+        g = l == N ? from_double<N>(d) : add(g, from_double<N>(d));
     }
     return g;
 }

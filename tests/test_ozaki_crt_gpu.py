@@ -78,12 +78,13 @@ def test_modular_error_decreases_with_moduli(mf, ref, rng, N):
     mf.gemm_(Co, Ad, Bd, config=_cfg(mf))
     base = mf.ozaki_last_moduli()
     errs = []
-    for T in (base - 8, base - 4, base):
+    for T in (base - 12, base - 8, base):
         mf.gemm_(Co, Ad, Bd, config=_cfg(mf, ozaki_moduli=T))
         assert mf.ozaki_last_moduli() == T
         errs.append(_err(ref, A, B, Co.to_numpy(), np.random.default_rng(2)))
     assert errs[0] > errs[1] > 0 and errs[1] >= errs[2]
-    # four moduli widen the digits by about 15 bits (one digit) / 7 bits per digit (two)
+    # four moduli widen the digits by about 15 bits (one digit) / 7 bits per
+    # digit (two), while truncation dominates the error
     assert errs[0] / max(errs[1], 1e-300) > 2.0 ** 6
 
 
