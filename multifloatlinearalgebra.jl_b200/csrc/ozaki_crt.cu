@@ -59,6 +59,19 @@ struct CrtAccConst {
     double pinv;                   // 1 / P (rounded)
 };
 
+// 2^k for k in [-1022, 1023]
+__device__ __forceinline__ double pow2i(int k) {
+    return __longlong_as_double((long long)(k + 1023) << 52);
+}
+
+// d * 2^e with a single rounding (exact unless the result is subnormal);
+// exponents beyond the double range saturate to 0 / inf as ldexp would
+__device__ __forceinline__ double scale2(double d, int e) {
+    e = e < -2044 ? -2044 : (e > 2046 ? 2046 : e);
+    const int e1 = e >> 1;
+    return (d * pow2i(e1)) * pow2i(e - e1);
+}
+
 // ------------------------------------------------------------- digits ----
 // One h-bit digit of the scaled value z (updated to the remainder): the
 // magnitude as WD little-endian 32-bit words and the sign.
@@ -67,7 +80,7 @@ __device__ __forceinline__ void crt_digit(mf<N> &z, int h, uint32_t (&w)[WD], bo
     double d[N];
 #pragma unroll
     for (int l = 0; l < N; ++l) {
-        z.v[l] = ldexp(z.v[l], h);                 // exact
+        z.v[l] = z.v[l] * pow2i(h);                // exact (h <= 158, |z| < 2)
         d[l] = rint(z.v[l]);
         z.v[l] = __dsub_rn(z.v[l], d[l]);          // exact: |z_l - rint(z_l)| <= 1/2
     }
@@ -83,18 +96,16 @@ __device__ __forceinline__ void crt_digit(mf<N> &z, int h, uint32_t (&w)[WD], bo
     for (int l = 0; l < N; ++l) {
         const double v = neg ? -d[l] : d[l];
         if (v != 0.0) {
-            const double av = fabs(v);
-            const int64_t sg = v < 0.0 ? -1 : 1;
-            uint64_t mm;
-            int e;
-            if (av < 9007199254740992.0) {  // < 2^53: the integer itself
-                mm = (uint64_t)av;
+            // |v| = mm 2^e from the bit pattern (v is a nonzero integer, so
+            // normal): 53-bit mantissa, shifted down when the exponent is
+            // negative (the bits shifted out are zero)
+            const uint64_t bits = (uint64_t)__double_as_longlong(v);
+            const int64_t sg = (bits >> 63) ? -1 : 1;
+            uint64_t mm = (bits & ((1ULL << 52) - 1)) | (1ULL << 52);
+            int e = (int)((bits >> 52) & 0x7ff) - 1075;
+            if (e < 0) {
+                mm >>= -e;
                 e = 0;
-            } else {
-                int ex;
-                frexp(av, &ex);
-                mm = (uint64_t)ldexp(av, 53 - ex);  // 53-bit integer mantissa
-                e = ex - 53;
             }
 #pragma unroll
             for (int j = 0; j < WD; ++j) {
@@ -158,7 +169,7 @@ __global__ void __launch_bounds__(256)
     for (int u = 0; u < 4; ++u) {
 #pragma unroll
         for (int l = 0; l < N; ++l)
-            z[u].v[l] = (e == OZ_EXP_BAD) ? 0.0 : ldexp(tile[l][kq + u][ii], -sh);
+            z[u].v[l] = (e == OZ_EXP_BAD) ? 0.0 : scale2(tile[l][kq + u][ii], -sh);
 #pragma unroll
         for (int l = N - 1; l > 0; --l) two_sum(z[u].v[l - 1], z[u].v[l], z[u].v[l - 1], z[u].v[l]);
     }
@@ -203,7 +214,7 @@ __global__ void __launch_bounds__(128)
         const bool ok = kk < k && j < n && e != OZ_EXP_BAD;
 #pragma unroll
         for (int l = 0; l < N; ++l)
-            z[u].v[l] = ok ? ldexp(B.p[l * B.ls + j * B.ld + kk], -sh) : 0.0;
+            z[u].v[l] = ok ? scale2(B.p[l * B.ls + j * B.ld + kk], -sh) : 0.0;
 #pragma unroll
         for (int l = N - 1; l > 0; --l) two_sum(z[u].v[l - 1], z[u].v[l], z[u].v[l - 1], z[u].v[l]);
     }
@@ -342,48 +353,55 @@ __device__ __forceinline__ mf<N> crt_words_to_mf(const uint32_t (&mag)[WP], int 
             ch = b0 > -53 ? ((uint64_t)a[0] | ((uint64_t)a[1] << 32)) << (-b0) : 0;
         }
         ch &= (1ULL << 53) - 1;
-        const double d = ldexp((double)ch, top - 53 * (l + 1));
+        const double d = scale2((double)ch, top - 53 * (l + 1));
         g = l == N ? from_double<N>(d) : add(g, from_double<N>(d));
     }
     return g;
 }
 
 // C = alpha * 2^(sa+sb-2Qh) sum_L 2^(h (2Q-2-L)) G_L (+ beta * C); R holds
-// the residues G_L mod p_t as bytes, plane (L T + t) at R + (L T + t) plane
+// the residues G_L mod p_t as bytes, plane (L T + t) at R + (L T + t) plane.
+// A block covers 128 rows of one column: the Q T residue segments of its rows
+// (128 bytes each, 128-byte aligned) are copied to shared memory with
+// cp.async in one round trip, then each thread reconstructs its entry.
+constexpr int CRT_ACC_ROWS = 128;
+
 template <int N, int WP>
-__global__ void __launch_bounds__(128, 3)
+__global__ void __launch_bounds__(CRT_ACC_ROWS, 3)
     crt_accum_kernel(int64_t m, int64_t n, int Q, int h, int T, const uint8_t *R, int64_t ldi,
                      size_t plane, const int *rowexp, const int *colexp, Mat C, scal<N> alpha,
                      scal<N> beta, int overwrite, const __grid_constant__ CrtAccConst c) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ __align__(16) uint8_t sres[2 * CRT_MAXT][CRT_ACC_ROWS];
+    const int tid = threadIdx.x;
+    const int64_t i0 = (int64_t)blockIdx.x * CRT_ACC_ROWS, i = i0 + tid;
     const int64_t j = blockIdx.y;
-    if (i >= m || j >= n) return;
+    // rows i0 .. i0+127 lie inside the padded planes (ldi = mp, a multiple of 128)
+    const int segs = Q * T * (CRT_ACC_ROWS / 16);
+    for (int s = tid; s < segs; s += CRT_ACC_ROWS) {
+        const int pl = s / (CRT_ACC_ROWS / 16), part = s % (CRT_ACC_ROWS / 16);
+        const uint8_t *g = R + (size_t)pl * plane + (size_t)j * ldi + i0 + part * 16;
+        const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&sres[pl][part * 16]);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(g) : "memory");
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    __syncthreads();
+    if (i >= m) return;
     const int ea = rowexp[i], eb = colexp[j];
     mf<N> acc = from_double<N>(0.0);
     if (ea == OZ_EXP_BAD || eb == OZ_EXP_BAD) {
         acc = from_double<N>(__longlong_as_double(0x7ff8000000000000LL));
     } else {
         for (int L = Q - 1; L >= 0; --L) {
-            const uint8_t *src = R + (size_t)L * T * plane + (size_t)j * ldi + i;
+            const uint8_t *src = &sres[L * T][tid];
             uint64_t X[WP];
 #pragma unroll
             for (int w = 0; w < WP; ++w) X[w] = 0;
-            // residues in groups of 8: the loads of a group are in flight together
 #pragma unroll
-            for (int t0 = 0; t0 < CRT_MAXT; t0 += 8) {
-                if (t0 < T) {
-                    uint32_t r[8];
+            for (int t = 0; t < CRT_MAXT; ++t) {
+                if (t < T) {
+                    const uint32_t r = src[t * CRT_ACC_ROWS];
 #pragma unroll
-                    for (int u = 0; u < 8; ++u)
-                        r[u] = (t0 + u < T && t0 + u < CRT_MAXT)
-                                   ? (uint32_t)__ldg(src + (size_t)(t0 + u) * plane) : 0u;
-#pragma unroll
-                    for (int u = 0; u < 8; ++u) {
-                        if (t0 + u < CRT_MAXT) {
-#pragma unroll
-                            for (int w = 0; w < WP; ++w) X[w] += (uint64_t)r[u] * c.U[t0 + u][w];
-                        }
-                    }
+                    for (int w = 0; w < WP; ++w) X[w] += (uint64_t)r * c.U[t][w];
                 }
             }
             uint32_t mag[WP];
@@ -608,8 +626,8 @@ template <int N, int WP>
 static void crt_accum(const CrtPlan &p, int64_t m, int64_t n, const uint8_t *I, const int *rowexp,
                       const int *colexp, Mat C, const scal<N> &al, const scal<N> &be,
                       int overwrite, cudaStream_t s) {
-    dim3 g((unsigned)((m + 127) / 128), (unsigned)n);
-    crt_accum_kernel<N, WP><<<g, 128, 0, s>>>(m, n, p.Q, p.h, p.T, I, p.ldi, p.plane, rowexp,
+    dim3 g((unsigned)((m + CRT_ACC_ROWS - 1) / CRT_ACC_ROWS), (unsigned)n);
+    crt_accum_kernel<N, WP><<<g, CRT_ACC_ROWS, 0, s>>>(m, n, p.Q, p.h, p.T, I, p.ldi, p.plane, rowexp,
                                               colexp, C, al, be, overwrite,
                                               crt_tables(p.T).acc);
 }
