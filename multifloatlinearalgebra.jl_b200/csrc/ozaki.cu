@@ -282,7 +282,9 @@ static int oz_exponents(int64_t m, int64_t n, int64_t k, Mat A, Mat B, int *rowe
                         cudaStream_t s) {
     cudaError_t e = cudaMemsetAsync(rowexp, 0x80, sizeof(int) * m, s);  // 0x80808080 < any exponent
     if (e != cudaSuccess) return record_cuda_error(e, "ozaki exps");
-    const int64_t kchunk = 512;
+    // short k chunks: enough blocks to cover every SM even for few rows
+    int64_t kchunk = 32;
+    if ((k + kchunk - 1) / kchunk > 65535) kchunk = (k + 65534) / 65535;
     dim3 gr((unsigned)((m + 255) / 256), (unsigned)((k + kchunk - 1) / kchunk));
     oz_row_exp_kernel<N><<<gr, 256, 0, s>>>(m, k, A, kchunk, rowexp);
     oz_col_exp_kernel<N><<<(unsigned)((n + 7) / 8), 256, 0, s>>>(k, n, B, colexp);
