@@ -42,14 +42,17 @@
 namespace mfl {
 
 constexpr int CRT_MAXT = CRT_TABLE_SIZE;
-constexpr int CRT_WD = 5;     // max 32-bit words of one digit magnitude (h <= 159)
+constexpr int CRT_WD = 5;     // max 32-bit words of one digit (h <= 157)
 constexpr int CRT_WP = 12;    // max 32-bit words of a CRT sum (< 2^384)
-constexpr int CRT_MAXH = 32 * CRT_WD - 2;
+constexpr int CRT_MAXH = 32 * CRT_WD - 3;
 
 // weights of the digit bytes: wt[t][j] packs 2^(8 b) mod p_t for bytes
-// b = 4j .. 4j+3 of a digit magnitude (one byte each)
+// b = 4j .. 4j+3 of a digit's two's-complement words (one byte each);
+// negoff[WD-3][t] = (128 - 2^(32 WD) mod p_t) mod p_t, the offset that turns
+// the residue of the words of a negative digit into (digit + 128) mod p_t
 struct CrtSplitConst {
     uint32_t wt[CRT_MAXT][CRT_WD];
+    uint32_t negoff[CRT_WD - 2][CRT_MAXT];
 };
 
 // reconstruction constants for one modulus count T
@@ -73,37 +76,33 @@ __device__ __forceinline__ double scale2(double d, int e) {
 }
 
 // ------------------------------------------------------------- digits ----
-// One h-bit digit of the scaled value z (updated to the remainder): the
-// magnitude as WD little-endian 32-bit words and the sign.
+// One h-bit digit D of the scaled value z (z is updated to the remainder):
+// WD little-endian 32-bit words holding D in two's complement
+// (|D| < 2^(32 WD - 1)) and the sign of D.
 template <int N, int WD>
 __device__ __forceinline__ void crt_digit(mf<N> &z, int h, uint32_t (&w)[WD], bool &neg) {
     double d[N];
 #pragma unroll
     for (int l = 0; l < N; ++l) {
-        z.v[l] = z.v[l] * pow2i(h);                // exact (h <= 158, |z| < 2)
+        z.v[l] = z.v[l] * pow2i(h);                // exact (h <= 157, |z| < 2)
         d[l] = rint(z.v[l]);
         z.v[l] = __dsub_rn(z.v[l], d[l]);          // exact: |z_l - rint(z_l)| <= 1/2
     }
 #pragma unroll
     for (int l = N - 1; l > 0; --l) two_sum(z.v[l - 1], z.v[l], z.v[l - 1], z.v[l]);
-    // sign of the digit = sign of its leading limb (lower limbs are below
-    // half an ulp of it, or zero when it is zero)
-    neg = d[0] < 0.0;
+    // D = sum_l d_l: every d_l is an integer, |d_l| = mm 2^e with a 53-bit
+    // mantissa; signed 32-bit slices of each are added word by word
     int64_t c[WD];
 #pragma unroll
     for (int j = 0; j < WD; ++j) c[j] = 0;
 #pragma unroll
     for (int l = 0; l < N; ++l) {
-        const double v = neg ? -d[l] : d[l];
-        if (v != 0.0) {
-            // |v| = mm 2^e from the bit pattern (v is a nonzero integer, so
-            // normal): 53-bit mantissa, shifted down when the exponent is
-            // negative (the bits shifted out are zero)
-            const uint64_t bits = (uint64_t)__double_as_longlong(v);
+        if (d[l] != 0.0) {
+            const uint64_t bits = (uint64_t)__double_as_longlong(d[l]);
             const int64_t sg = (bits >> 63) ? -1 : 1;
             uint64_t mm = (bits & ((1ULL << 52) - 1)) | (1ULL << 52);
             int e = (int)((bits >> 52) & 0x7ff) - 1075;
-            if (e < 0) {
+            if (e < 0) {  // the bits shifted out are zero: d_l is an integer
                 mm >>= -e;
                 e = 0;
             }
@@ -122,20 +121,21 @@ __device__ __forceinline__ void crt_digit(mf<N> &z, int h, uint32_t (&w)[WD], bo
     for (int j = 0; j < WD; ++j) {
         const int64_t t = c[j] + carry;
         w[j] = (uint32_t)t;
-        carry = t >> 32;
+        carry = t >> 32;  // arithmetic: ends at -1 exactly when D < 0
     }
+    neg = carry < 0;
 }
 
-// signed-byte residue of (neg ? -1 : 1) * magnitude mod p
+// (D + 128) mod p from the two's-complement words of D (off = 128 for D >= 0,
+// the modulus' negoff for D < 0); the stored byte is this value - 128, an
+// int8 congruent to D mod p
 template <int WD>
-__device__ __forceinline__ int crt_residue(const uint32_t (&w)[WD], const uint32_t *wt, int p,
-                                           bool neg) {
-    unsigned acc = 0;
+__device__ __forceinline__ uint32_t crt_residue(const uint32_t (&w)[WD], const uint32_t *wt,
+                                                uint32_t off, int p) {
+    uint32_t acc = off;
 #pragma unroll
-    for (int j = 0; j < WD; ++j) acc = __dp4a(w[j], wt[j], acc);  // < 20 * 255^2
-    int r = (int)(acc % (unsigned)p);
-    if (neg && r) r = p - r;
-    return r >= 128 ? r - p : r;
+    for (int j = 0; j < WD; ++j) acc = __dp4a(w[j], wt[j], acc);  // < 20 * 255^2 + 512
+    return acc % (uint32_t)p;
 }
 
 // A (m x k, column-major planes) -> residue planes A8[t][i][q][k] (int8,
@@ -185,10 +185,10 @@ __global__ void __launch_bounds__(256)
                 uint32_t packed = 0;
 #pragma unroll
                 for (int u = 0; u < 4; ++u)
-                    packed |= (uint32_t)(uint8_t)(int8_t)crt_residue<WD>(w[u], c.wt[t],
-                                                                         crt_modulus(t), ng[u])
+                    packed |= crt_residue<WD>(w[u], c.wt[t], ng[u] ? c.negoff[WD - 3][t] : 128u,
+                                              crt_modulus(t))
                               << (8 * u);
-                *(uint32_t *)(dst + (size_t)t * plane8 + (size_t)q * kp) = packed;
+                *(uint32_t *)(dst + (size_t)t * plane8 + (size_t)q * kp) = packed ^ 0x80808080u;
             }
         }
     }
@@ -230,10 +230,11 @@ __global__ void __launch_bounds__(128)
                 uint32_t packed = 0;
 #pragma unroll
                 for (int u = 0; u < 4; ++u)
-                    packed |= (uint32_t)(uint8_t)(int8_t)crt_residue<WD>(w[u], c.wt[t],
-                                                                         crt_modulus(t), ng[u])
+                    packed |= crt_residue<WD>(w[u], c.wt[t], ng[u] ? c.negoff[WD - 3][t] : 128u,
+                                              crt_modulus(t))
                               << (8 * u);
-                *(uint32_t *)(dst + (size_t)t * plane8 + (size_t)(Q - 1 - q) * kp) = packed;
+                *(uint32_t *)(dst + (size_t)t * plane8 + (size_t)(Q - 1 - q) * kp) =
+                    packed ^ 0x80808080u;
             }
         }
     }
@@ -370,7 +371,7 @@ template <int N, int WP>
 __global__ void __launch_bounds__(CRT_ACC_ROWS, 3)
     crt_accum_kernel(int64_t m, int64_t n, int Q, int h, int T, const uint8_t *R, int64_t ldi,
                      size_t plane, const int *rowexp, const int *colexp, Mat C, scal<N> alpha,
-                     scal<N> beta, int overwrite, const __grid_constant__ CrtAccConst c) {
+                     scal<N> beta, int flags, const __grid_constant__ CrtAccConst c) {
     __shared__ __align__(16) uint8_t sres[2 * CRT_MAXT][CRT_ACC_ROWS];
     const int tid = threadIdx.x;
     const int64_t i0 = (int64_t)blockIdx.x * CRT_ACC_ROWS, i = i0 + tid;
@@ -412,8 +413,9 @@ __global__ void __launch_bounds__(CRT_ACC_ROWS, 3)
             acc = L == Q - 1 ? g : add(acc, g);
         }
     }
-    mf<N> r = mul(alpha.get(), acc);
-    if (!overwrite) r = add(r, mul(beta.get(), load_mf<N>(C.p, C.ld, C.ls, i, j)));
+    // flags bit 0: beta == 0 (C is not read); bit 1: alpha == 1
+    mf<N> r = (flags & 2) ? acc : mul(alpha.get(), acc);
+    if (!(flags & 1)) r = add(r, mul(beta.get(), load_mf<N>(C.p, C.ld, C.ls, i, j)));
     store_mf<N>(C.p, C.ld, C.ls, i, j, r);
 }
 
@@ -500,6 +502,11 @@ static const CrtSplitConst &crt_split_const() {
                 }
                 c.wt[t][j] = word;
             }
+            for (int wd = 3; wd <= CRT_WD; ++wd) {
+                uint32_t v = 1 % p;  // 2^(32 wd) mod p
+                for (int b = 0; b < 32 * wd; ++b) v = (v * 2u) % p;
+                c.negoff[wd - 3][t] = (128u % p + p - v) % p;
+            }
         }
     });
     return c;
@@ -581,7 +588,7 @@ static int crt_plan(int N, int64_t m, int64_t n, int64_t k, int T_req, int gap8,
     }
     if (p.h < 8) return MFLAB_ERR_UNSUPPORTED;
     if ((int64_t)p.Q * p.kp * 16384 >= 2147483648LL) return MFLAB_ERR_UNSUPPORTED;
-    p.WD = (p.h + 2 + 31) / 32;
+    p.WD = (p.h + 3 + 31) / 32;  // |digit| <= 2^(h+1) plus a sign bit
     if (p.WD < 3) p.WD = 3;
     const int need = crt_tables(p.T).bitlen + 14;  // X < T 256 P
     p.WP = need <= 256 ? 8 : need <= 320 ? 10 : 12;
@@ -625,11 +632,10 @@ static void crt_split_n(const CrtPlan &p, int64_t m, int64_t n, int64_t k, Mat A
 template <int N, int WP>
 static void crt_accum(const CrtPlan &p, int64_t m, int64_t n, const uint8_t *I, const int *rowexp,
                       const int *colexp, Mat C, const scal<N> &al, const scal<N> &be,
-                      int overwrite, cudaStream_t s) {
+                      int flags, cudaStream_t s) {
     dim3 g((unsigned)((m + CRT_ACC_ROWS - 1) / CRT_ACC_ROWS), (unsigned)n);
     crt_accum_kernel<N, WP><<<g, CRT_ACC_ROWS, 0, s>>>(m, n, p.Q, p.h, p.T, I, p.ldi, p.plane, rowexp,
-                                              colexp, C, al, be, overwrite,
-                                              crt_tables(p.T).acc);
+                                              colexp, C, al, be, flags, crt_tables(p.T).acc);
 }
 
 template <int N>
@@ -670,15 +676,16 @@ static int crt_gemm_n(mflab_handle *hd, const CrtPlan &p, int64_t m, int64_t n, 
     if (rc) return rc;
     ozaki_phase(2, s);
     scal<N> al{}, be{};
-    int overwrite = 1;
+    int flags = 3;  // bit 0: beta == 0, bit 1: alpha == 1
     for (int l = 0; l < N; ++l) {
         al.v[l] = alpha[l];
         be.v[l] = beta[l];
-        if (beta[l] != 0.0) overwrite = 0;
+        if (beta[l] != 0.0) flags &= ~1;
+        if (alpha[l] != (l == 0 ? 1.0 : 0.0)) flags &= ~2;
     }
-    if (p.WP == 8) crt_accum<N, 8>(p, m, n, Rs, rowexp, colexp, C, al, be, overwrite, s);
-    else if (p.WP == 10) crt_accum<N, 10>(p, m, n, Rs, rowexp, colexp, C, al, be, overwrite, s);
-    else crt_accum<N, 12>(p, m, n, Rs, rowexp, colexp, C, al, be, overwrite, s);
+    if (p.WP == 8) crt_accum<N, 8>(p, m, n, Rs, rowexp, colexp, C, al, be, flags, s);
+    else if (p.WP == 10) crt_accum<N, 10>(p, m, n, Rs, rowexp, colexp, C, al, be, flags, s);
+    else crt_accum<N, 12>(p, m, n, Rs, rowexp, colexp, C, al, be, flags, s);
     ozaki_phase(3, s);
     return record_cuda_error(cudaGetLastError(), "modular accumulate");
 }
