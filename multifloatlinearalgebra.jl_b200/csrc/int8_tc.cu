@@ -1,26 +1,30 @@
 // int8 x int8 -> int32 GEMM on the 5th-generation tensor cores (tcgen05),
-// the level products of the INT8-slice multi-double route.
+// the level / residue products of the two INT8 multi-double routes.
 //
 // C[m0:m0+128, n0:n0+256] = A[rows, K] * B[cols, K]^T with both operands
-// K-major int8 (rows of the digit matrices), exact int32 accumulation.
+// K-major int8 (rows of the digit matrices), exact int32 accumulation;
+// blockIdx-independent problems z (moduli) are stacked in one launch.
 //
-// One CTA (4 warps) per 128 x 256 output tile:
+// Persistent kernel, one CTA (6 warps) per SM walking a static list of
+// 128 x 256 output tiles:
 //   * warp 0 lane 0: TMA producer.  Per 128-byte K step it loads the A tile
 //     (128 rows x 128 B) and the B tile (256 rows x 128 B) into one of 4 shared
 //     memory stages with cp.async.bulk.tensor (128-byte swizzle, no multicast),
-//     completion tracked by the stage's "full" mbarrier (expect_tx).
-//   * warp 1 lane 0: MMA issuer.  Waits for a full stage, issues four
-//     tcgen05.mma.cta_group::1.kind::i8 (M=128, N=256, K=32) into a TMEM
-//     accumulator of 256 columns, and tcgen05.commit's the stage's "empty"
-//     mbarrier so the producer can refill it once the MMAs have read it.
-//     After the last K step a commit signals the accumulator barrier.
-//   * all 4 warps: epilogue.  Each warp reads its 32 TMEM lanes (rows) with
-//     tcgen05.ld.32x32b.x16 and stores int32 rows; a warp's 32 threads write 32
-//     consecutive rows of one column (coalesced, C is column-major).
+//     completion tracked by the stage's "full" mbarrier (expect_tx); it runs
+//     ahead into the next tile while the MMAs of the current one execute.
+//   * warp 1: owns 512 TMEM columns (two 256-column accumulators); lane 0
+//     waits for a full stage, issues four tcgen05.mma.cta_group::1.kind::i8
+//     (M=128, N=256, K=32) and tcgen05.commit's the stage's "empty" mbarrier;
+//     after the last K step of a tile a commit marks its accumulator full.
+//   * warps 2-5: epilogue.  Each reads its 32 TMEM lanes (rows) of the full
+//     accumulator with tcgen05.ld.32x32b.x16, stores the column-major result
+//     (a warp writes 32 consecutive rows of one column) and releases the
+//     accumulator, so the epilogue of tile i overlaps the MMAs of tile i + 1.
 // Every mbarrier wait is bounded: on timeout the kernel records an error code
-// in *err, waits (bounded) for its own copies in flight, frees its TMEM and
-// returns.  Operands: the padded digit matrices (rows multiple of 128 / 256, K
-// multiple of 128), so no tile needs bounds checks.
+// in *err, raises a shared abort flag that ends every role's loop, waits
+// (bounded) for its own copies and MMAs in flight, frees its TMEM and returns.
+// Operands: the padded digit matrices (rows multiple of 128 / 256, K multiple
+// of 128), so no tile needs bounds checks.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -121,46 +125,63 @@ __device__ __forceinline__ void mma_commit(uint64_t *bar) {
                  : "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Persistent, warp-specialised kernel: one CTA per SM walks the output tiles
+// tile = blockIdx.x + i * gridDim.x (problem z outermost, then column tiles,
+// then row tiles, so that neighbouring CTAs share B tiles in L2).
+//   warp 0 lane 0   TMA producer over all k-steps of all its tiles
+//   warp 1          TMEM owner (512 columns: two 256-column accumulators);
+//                   lane 0 issues the MMAs of tile i into accumulator i % 2
+//   warps 2..5      epilogue: drain accumulator i % 2 while the MMAs of tile
+//                   i + 1 run into the other one (warp w reads TMEM lanes
+//                   32 (w % 4) .. 32 (w % 4) + 31)
 // MODE 0 stores the int32 sums; MODE 1 stores their residues modulo
-// crt_modulus(blockIdx.z) as bytes (C is then a byte matrix: ldc and
-// c_zstride in bytes), the only part of the sums the modular route needs.
+// crt_modulus(z) as bytes (C is then a byte matrix: ldc and c_zstride in
+// bytes), the only part of the sums the modular route needs.
+constexpr int TC_THREADS = 192;
+constexpr uint32_t TC_TMEM_ALLOC = 2 * TC_TMEM_COLS;
+
 template <int MODE>
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(TC_THREADS, 1)
     int8_tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA,
                         const __grid_constant__ CUtensorMap tmB, int K, int b_xoff, void *Cv,
-                        int64_t ldc, int a_zrows, int b_zrows, int64_t c_zstride, int *err) {
+                        int64_t ldc, int a_zrows, int b_zrows, int64_t c_zstride, int tiles_m,
+                        int tiles_n, int nz, int *err) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     uint64_t *full = (uint64_t *)(smem + TC_STAGES * TC_STAGE_BYTES);
     uint64_t *empty = full + TC_STAGES;
-    uint64_t *accbar = empty + TC_STAGES;
-    uint32_t *tmem_slot = (uint32_t *)(accbar + 1);
+    uint64_t *tfull = empty + TC_STAGES;   // [2] accumulator ready (MMA -> epilogue)
+    uint64_t *tempty = tfull + 2;          // [2] accumulator drained (epilogue -> MMA)
+    uint64_t *drain = tempty + 2;          // all MMAs of this CTA complete
+    uint32_t *tmem_slot = (uint32_t *)(drain + 1);
     int *abort_flag = (int *)(tmem_slot + 1);
 
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-    // blockIdx.z selects one of several stacked problems: its operands are the
-    // row blocks [z a_zrows, (z+1) a_zrows) of A and [z b_zrows, ...) of B
-    const int m0 = blockIdx.x * TC_BM, n0 = blockIdx.y * TC_BN;
-    const int am0 = (int)blockIdx.z * a_zrows + m0, bn0 = (int)blockIdx.z * b_zrows + n0;
-    int32_t *C = (int32_t *)Cv + (MODE == 0 ? (int64_t)blockIdx.z * c_zstride : 0);
-    uint8_t *R = (uint8_t *)Cv + (MODE == 1 ? (int64_t)blockIdx.z * c_zstride : 0);
-    const int pz = crt_modulus((int)blockIdx.z);
-    const double pzinv = 1.0 / (double)pz;
     const int ksteps = K / TC_BK;
+    const int per_z = tiles_m * tiles_n;
+    const int total = per_z * nz;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < TC_STAGES; ++s) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
-        mbar_init(accbar, 1);
+        for (int a = 0; a < 2; ++a) {
+            mbar_init(&tfull[a], 1);
+            mbar_init(&tempty[a], 4);  // one arrival per epilogue warp
+        }
+        mbar_init(drain, 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == 0) {
+    if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                          smem_u32(tmem_slot)),
-                     "r"(TC_TMEM_COLS)
+                     "r"(TC_TMEM_ALLOC)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -169,95 +190,137 @@ __global__ void __launch_bounds__(128, 1)
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmem_slot;
 
-    if (warp == 0 && lane == 0) {
-        // ---------------- TMA producer
-        int issued = 0;
-        for (int i = 0; i < ksteps; ++i) {
-            const int s = i % TC_STAGES;
-            if (i >= TC_STAGES && !mbar_wait(&empty[s], ((i / TC_STAGES) - 1) & 1)) {
-                atomicExch(err, TC_ERR_PRODUCER);
-                atomicExch(abort_flag, 1);
-                break;
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---------------- TMA producer
+            int ks = 0;
+            for (int tile = blockIdx.x; tile < total && !*(volatile int *)abort_flag;
+                 tile += gridDim.x) {
+                const int z = tile / per_z, r = tile % per_z;
+                const int am0 = z * a_zrows + (r % tiles_m) * TC_BM;
+                const int bn0 = z * b_zrows + (r / tiles_m) * TC_BN;
+                for (int kb = 0; kb < ksteps; ++kb, ++ks) {
+                    const int s = ks % TC_STAGES;
+                    if (ks >= TC_STAGES && !mbar_wait(&empty[s], ((ks / TC_STAGES) - 1) & 1)) {
+                        atomicExch(err, TC_ERR_PRODUCER);
+                        atomicExch(abort_flag, 1);
+                        break;
+                    }
+                    if (*(volatile int *)abort_flag) break;
+                    uint8_t *sa = smem + s * TC_STAGE_BYTES;
+                    uint8_t *sb = sa + TC_A_BYTES;
+                    mbar_expect_tx(&full[s], TC_STAGE_BYTES);
+                    tma_load_2d(sa, &tmA, kb * TC_BK, am0, &full[s]);
+                    tma_load_2d(sb, &tmB, b_xoff + kb * TC_BK, bn0, &full[s]);
+                }
             }
-            if (*(volatile int *)abort_flag) break;
-            uint8_t *sa = smem + s * TC_STAGE_BYTES;
-            uint8_t *sb = sa + TC_A_BYTES;
-            mbar_expect_tx(&full[s], TC_STAGE_BYTES);
-            tma_load_2d(sa, &tmA, i * TC_BK, am0, &full[s]);
-            tma_load_2d(sb, &tmB, b_xoff + i * TC_BK, bn0, &full[s]);
-            ++issued;
+            // the copies issued last must have landed before the CTA can exit
+            for (int i = ks - TC_STAGES > 0 ? ks - TC_STAGES : 0; i < ks; ++i)
+                mbar_wait(&full[i % TC_STAGES], (i / TC_STAGES) & 1);
         }
-        // the copies issued last must have landed before the CTA can exit
-        for (int i = issued - TC_STAGES > 0 ? issued - TC_STAGES : 0; i < issued; ++i)
-            mbar_wait(&full[i % TC_STAGES], (i / TC_STAGES) & 1);
-    } else if (warp == 1 && lane == 0) {
-        // ---------------- MMA issuer
-        const uint32_t idesc = idesc_i8(TC_BM, TC_BN);
-        bool ok = true;
-        for (int i = 0; i < ksteps; ++i) {
-            const int s = i % TC_STAGES;
-            if (!mbar_wait(&full[s], (i / TC_STAGES) & 1)) {
-                atomicExch(err, TC_ERR_MMA);
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // ---------------- MMA issuer
+            const uint32_t idesc = idesc_i8(TC_BM, TC_BN);
+            int ks = 0, it = 0;
+            for (int tile = blockIdx.x; tile < total && !*(volatile int *)abort_flag;
+                 tile += gridDim.x, ++it) {
+                const int acc = it & 1, use = it >> 1;
+                if (use > 0 && !mbar_wait(&tempty[acc], (use - 1) & 1)) {
+                    atomicExch(err, TC_ERR_MMA);
+                    atomicExch(abort_flag, 1);
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t dcol = tmem + (uint32_t)(acc * TC_TMEM_COLS);
+                bool ok = true;
+                for (int kb = 0; kb < ksteps; ++kb, ++ks) {
+                    const int s = ks % TC_STAGES;
+                    if (!mbar_wait(&full[s], (ks / TC_STAGES) & 1)) {
+                        atomicExch(err, TC_ERR_MMA);
+                        atomicExch(abort_flag, 1);
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t sa = smem_u32(smem + s * TC_STAGE_BYTES);
+                    const uint32_t sb = sa + TC_A_BYTES;
+#pragma unroll
+                    for (int kk = 0; kk < TC_BK / 32; ++kk)
+                        mma_i8(dcol, smem_desc_sw128(sa + kk * 32), smem_desc_sw128(sb + kk * 32),
+                               idesc, (kb > 0 || kk > 0) ? 1u : 0u);
+                    mma_commit(&empty[s]);
+                }
+                mma_commit(&tfull[acc]);  // also on abort: the epilogue then sees the flag
+                if (!ok) break;
+            }
+            // every MMA issued by this thread has completed once `drain` flips
+            mma_commit(drain);
+            mbar_wait(drain, 0);
+        }
+    } else {
+        // ---------------- epilogue: TMEM -> registers -> C
+        const int q = warp & 3;  // TMEM lane quarter of this warp
+        int it = 0;
+        for (int tile = blockIdx.x; tile < total; tile += gridDim.x, ++it) {
+            const int acc = it & 1, use = it >> 1;
+            if (!mbar_wait(&tfull[acc], use & 1)) {
+                atomicExch(err, TC_ERR_EPILOGUE);
                 atomicExch(abort_flag, 1);
-                ok = false;
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t sa = smem_u32(smem + s * TC_STAGE_BYTES);
-            const uint32_t sb = sa + TC_A_BYTES;
-#pragma unroll
-            for (int kk = 0; kk < TC_BK / 32; ++kk)
-                mma_i8(tmem, smem_desc_sw128(sa + kk * 32), smem_desc_sw128(sb + kk * 32), idesc,
-                       (i > 0 || kk > 0) ? 1u : 0u);
-            mma_commit(&empty[s]);
-        }
-        if (ok) mma_commit(accbar);
-        else mma_commit(accbar);  // still signal: the epilogue then sees abort_flag
-    }
-    __syncwarp();
-
-    // ---------------- epilogue: TMEM -> registers -> int32 rows of C
-    const bool acc_ready = mbar_wait(accbar, 0);
-    if (!acc_ready) atomicExch(err, TC_ERR_EPILOGUE);
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const bool store = acc_ready && !*(volatile int *)abort_flag;
-    const int row = m0 + warp * 32 + lane;
+            if (*(volatile int *)abort_flag) break;
+            const int z = tile / per_z, r = tile % per_z;
+            const int row = (r % tiles_m) * TC_BM + q * 32 + lane;
+            const int n0 = (r / tiles_m) * TC_BN;
+            int32_t *C = (int32_t *)Cv + (MODE == 0 ? (int64_t)z * c_zstride : 0);
+            uint8_t *R = (uint8_t *)Cv + (MODE == 1 ? (int64_t)z * c_zstride : 0);
+            const int pz = crt_modulus(z);
+            const double pzinv = 1.0 / (double)pz;
 #pragma unroll 1
-    for (int c0 = 0; c0 < TC_BN; c0 += 16) {
-        uint32_t v[16];
-        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-            "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
-            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
-              "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
-              "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-            : "r"(taddr)
-            : "memory");
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        if (store) {
-            if (MODE == 0) {
+            for (int c0 = 0; c0 < TC_BN; c0 += 16) {
+                uint32_t v[16];
+                const uint32_t taddr =
+                    tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * TC_TMEM_COLS + c0);
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+                    "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+                      "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
+                      "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+                    : "r"(taddr)
+                    : "memory");
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                if (MODE == 0) {
 #pragma unroll
-                for (int j = 0; j < 16; ++j) C[(int64_t)(n0 + c0 + j) * ldc + row] = (int32_t)v[j];
-            } else {
+                    for (int j = 0; j < 16; ++j)
+                        C[(int64_t)(n0 + c0 + j) * ldc + row] = (int32_t)v[j];
+                } else {
 #pragma unroll
-                for (int j = 0; j < 16; ++j) {
-                    const int g = (int)v[j];
-                    // floor(g / p) or one off; the remainder is then fixed up exactly
-                    const int q = (int)floor((double)g * pzinv);
-                    int r = g - q * pz;
-                    r += r < 0 ? pz : 0;
-                    r -= r >= pz ? pz : 0;
-                    R[(int64_t)(n0 + c0 + j) * ldc + row] = (uint8_t)r;
+                    for (int j = 0; j < 16; ++j) {
+                        const int g = (int)v[j];
+                        // floor(g / p) or one off; the remainder is then fixed up exactly
+                        const int qq = (int)floor((double)g * pzinv);
+                        int rr = g - qq * pz;
+                        rr += rr < 0 ? pz : 0;
+                        rr -= rr >= pz ? pz : 0;
+                        R[(int64_t)(n0 + c0 + j) * ldc + row] = (uint8_t)rr;
+                    }
                 }
             }
+            // accumulator drained: the MMA warp may overwrite it
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&tempty[acc]);
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    if (warp == 0) {
+    if (warp == 1) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
-                     "r"(TC_TMEM_COLS)
+                     "r"(TC_TMEM_ALLOC)
                      : "memory");
     }
 }
@@ -315,9 +378,16 @@ static int launch_tc(int64_t mp, int64_t np, int64_t K, const int8_t *A, int64_t
         if (e != cudaSuccess) return record_cuda_error(e, "int8 tc attribute");
         configured = true;
     }
-    dim3 grid((unsigned)(mp / TC_BM), (unsigned)(np / TC_BN), (unsigned)nz);
-    int8_tc_gemm_kernel<MODE><<<grid, 128, TC_SMEM, s>>>(ta, tb, (int)K, (int)b_xoff, C, ldc,
-                                                         (int)mp, (int)np, c_zstride, err);
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0)
+        sms = 148;
+    const int64_t tiles = (mp / TC_BM) * (np / TC_BN) * nz;
+    if (tiles > 0x7fffffff) return MFLAB_ERR_UNSUPPORTED;
+    const unsigned grid = (unsigned)(tiles < sms ? tiles : sms);
+    int8_tc_gemm_kernel<MODE><<<grid, TC_THREADS, TC_SMEM, s>>>(
+        ta, tb, (int)K, (int)b_xoff, C, ldc, (int)mp, (int)np, c_zstride, (int)(mp / TC_BM),
+        (int)(np / TC_BN), nz, err);
     return record_cuda_error(cudaGetLastError(), "int8 tc gemm");
 }
 
