@@ -1,30 +1,30 @@
 // int8 x int8 -> int32 GEMM on the 5th-generation tensor cores (tcgen05),
 // the level / residue products of the two INT8 multi-double routes.
 //
-// C[m0:m0+128, n0:n0+256] = A[rows, K] * B[cols, K]^T with both operands
+// C[m0:m0+256, n0:n0+256] = A[rows, K] * B[cols, K]^T with both operands
 // K-major int8 (rows of the digit matrices), exact int32 accumulation;
-// blockIdx-independent problems z (moduli) are stacked in one launch.
+// independent problems z (moduli) are stacked in one launch.
 //
-// Persistent kernel, one CTA (6 warps) per SM walking a static list of
-// 128 x 256 output tiles:
+// Persistent kernel, one CTA (10 warps) per SM walking a static list of
+// 256 x 256 output tiles:
 //   * warp 0 lane 0: TMA producer.  Per 128-byte K step it loads the A tile
-//     (128 rows x 128 B) and the B tile (256 rows x 128 B) into one of 4 shared
+//     (256 rows x 128 B) and the B tile (256 rows x 128 B) into one of 3 shared
 //     memory stages with cp.async.bulk.tensor (128-byte swizzle, no multicast),
 //     completion tracked by the stage's "full" mbarrier (expect_tx); it runs
-//     ahead into the next tile while the MMAs of the current one execute.
-//   * warp 1: owns 512 TMEM columns (two 256-column accumulators); lane 0
-//     waits for a full stage, issues four tcgen05.mma.cta_group::1.kind::i8
-//     (M=128, N=256, K=32) and tcgen05.commit's the stage's "empty" mbarrier;
-//     after the last K step of a tile a commit marks its accumulator full.
-//   * warps 2-5: epilogue.  Each reads its 32 TMEM lanes (rows) of the full
-//     accumulator with tcgen05.ld.32x32b.x16, stores the column-major result
-//     (a warp writes 32 consecutive rows of one column) and releases the
-//     accumulator, so the epilogue of tile i overlaps the MMAs of tile i + 1.
+//     ahead into the next tile while the epilogue drains the current one.
+//   * warp 1: owns 512 TMEM columns (the 128 x 256 accumulators of the tile's
+//     two row halves); lane 0 waits for a full stage, issues per 32-byte K
+//     slice two tcgen05.mma.cta_group::1.kind::i8 (M=128, N=256, K=32) that
+//     read the same B tile, so a 64 KiB stage feeds twice the MMA work of a
+//     128-row tile, and tcgen05.commit's the stage's "empty" mbarrier.
+//   * warps 2-9: epilogue.  Each reads its 32 TMEM lanes (rows) of one half
+//     with tcgen05.ld.32x32b.x16 and stores the column-major result (a warp
+//     writes 32 consecutive rows of one column).
 // Every mbarrier wait is bounded: on timeout the kernel records an error code
 // in *err, raises a shared abort flag that ends every role's loop, waits
 // (bounded) for its own copies and MMAs in flight, frees its TMEM and returns.
 // Operands: the padded digit matrices (rows multiple of 128 / 256, K multiple
-// of 128), so no tile needs bounds checks.
+// of 128), so no tile needs bounds checks beyond the last half row tile.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -35,12 +35,12 @@
 
 namespace mfl {
 
-constexpr int TC_BM = 128, TC_BN = 256, TC_BK = 128, TC_STAGES = 4;
-constexpr uint32_t TC_A_BYTES = TC_BM * TC_BK;               // 16 KiB
+constexpr int TC_BM = 256, TC_MMA_M = 128, TC_BN = 256, TC_BK = 128, TC_STAGES = 3;
+constexpr uint32_t TC_A_BYTES = TC_BM * TC_BK;               // 32 KiB
 constexpr uint32_t TC_B_BYTES = TC_BN * TC_BK;               // 32 KiB
-constexpr uint32_t TC_STAGE_BYTES = TC_A_BYTES + TC_B_BYTES;  // 48 KiB
+constexpr uint32_t TC_STAGE_BYTES = TC_A_BYTES + TC_B_BYTES;  // 64 KiB
 constexpr uint32_t TC_SMEM = TC_STAGES * TC_STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
-constexpr uint32_t TC_TMEM_COLS = 256;
+constexpr uint32_t TC_TMEM_COLS = 256;  // one 128 x 256 accumulator
 constexpr long long TC_WAIT_LIMIT = 1LL << 24;
 
 // error codes written to *err
@@ -129,19 +129,21 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
-// Persistent, warp-specialised kernel: one CTA per SM walks the output tiles
-// tile = blockIdx.x + i * gridDim.x (problem z outermost, then column tiles,
-// then row tiles, so that neighbouring CTAs share B tiles in L2).
+// Persistent, warp-specialised kernel: one CTA per SM walks the 256 x 256
+// output tiles tile = blockIdx.x + i * gridDim.x (problem z outermost, then
+// column tiles, then row tiles, so that neighbouring CTAs share B tiles in L2).
 //   warp 0 lane 0   TMA producer over all k-steps of all its tiles
-//   warp 1          TMEM owner (512 columns: two 256-column accumulators);
-//                   lane 0 issues the MMAs of tile i into accumulator i % 2
-//   warps 2..5      epilogue: drain accumulator i % 2 while the MMAs of tile
-//                   i + 1 run into the other one (warp w reads TMEM lanes
-//                   32 (w % 4) .. 32 (w % 4) + 31)
+//   warp 1          TMEM owner (512 columns: the 128 x 256 accumulators of the
+//                   tile's upper and lower row halves); lane 0 issues per
+//                   32-byte K slice two M=128 MMAs that share the B operand
+//   warps 2..9      epilogue: warps 2-5 drain the upper half, 6-9 the lower
+//                   half (warp w reads TMEM lanes 32 (w % 4) .. 32 (w % 4) + 31)
+// A row tile that starts 128 rows before the end of the matrix (m % 256 ==
+// 128) computes and stores its upper half only.
 // MODE 0 stores the int32 sums; MODE 1 stores their residues modulo
 // crt_modulus(z) as bytes (C is then a byte matrix: ldc and c_zstride in
 // bytes), the only part of the sums the modular route needs.
-constexpr int TC_THREADS = 192;
+constexpr int TC_THREADS = 320;
 constexpr uint32_t TC_TMEM_ALLOC = 2 * TC_TMEM_COLS;
 
 template <int MODE>
@@ -154,9 +156,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     uint64_t *full = (uint64_t *)(smem + TC_STAGES * TC_STAGE_BYTES);
     uint64_t *empty = full + TC_STAGES;
-    uint64_t *tfull = empty + TC_STAGES;   // [2] accumulator ready (MMA -> epilogue)
-    uint64_t *tempty = tfull + 2;          // [2] accumulator drained (epilogue -> MMA)
-    uint64_t *drain = tempty + 2;          // all MMAs of this CTA complete
+    uint64_t *tfull = empty + TC_STAGES;   // accumulators ready (MMA -> epilogue)
+    uint64_t *tempty = tfull + 1;          // accumulators drained (epilogue -> MMA)
+    uint64_t *drain = tempty + 1;          // all MMAs of this CTA complete
     uint32_t *tmem_slot = (uint32_t *)(drain + 1);
     int *abort_flag = (int *)(tmem_slot + 1);
 
@@ -170,10 +172,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
-        for (int a = 0; a < 2; ++a) {
-            mbar_init(&tfull[a], 1);
-            mbar_init(&tempty[a], 4);  // one arrival per epilogue warp
-        }
+        mbar_init(tfull, 1);
+        mbar_init(tempty, 8);  // one arrival per epilogue warp
         mbar_init(drain, 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -210,6 +210,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     uint8_t *sa = smem + s * TC_STAGE_BYTES;
                     uint8_t *sb = sa + TC_A_BYTES;
                     mbar_expect_tx(&full[s], TC_STAGE_BYTES);
+                    // rows past the last plane read the map's zero fill; rows
+                    // of the next plane (m % 256 == 128) feed no stored result
                     tma_load_2d(sa, &tmA, kb * TC_BK, am0, &full[s]);
                     tma_load_2d(sb, &tmB, b_xoff + kb * TC_BK, bn0, &full[s]);
                 }
@@ -221,18 +223,18 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     } else if (warp == 1) {
         if (lane == 0) {
             // ---------------- MMA issuer
-            const uint32_t idesc = idesc_i8(TC_BM, TC_BN);
+            const uint32_t idesc = idesc_i8(TC_MMA_M, TC_BN);
             int ks = 0, it = 0;
             for (int tile = blockIdx.x; tile < total && !*(volatile int *)abort_flag;
                  tile += gridDim.x, ++it) {
-                const int acc = it & 1, use = it >> 1;
-                if (use > 0 && !mbar_wait(&tempty[acc], (use - 1) & 1)) {
+                const int r = tile % per_z;
+                const bool lower = (r % tiles_m) * TC_BM + TC_MMA_M < a_zrows;
+                if (it > 0 && !mbar_wait(tempty, (it - 1) & 1)) {
                     atomicExch(err, TC_ERR_MMA);
                     atomicExch(abort_flag, 1);
                     break;
                 }
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const uint32_t dcol = tmem + (uint32_t)(acc * TC_TMEM_COLS);
                 bool ok = true;
                 for (int kb = 0; kb < ksteps; ++kb, ++ks) {
                     const int s = ks % TC_STAGES;
@@ -246,12 +248,18 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     const uint32_t sa = smem_u32(smem + s * TC_STAGE_BYTES);
                     const uint32_t sb = sa + TC_A_BYTES;
 #pragma unroll
-                    for (int kk = 0; kk < TC_BK / 32; ++kk)
-                        mma_i8(dcol, smem_desc_sw128(sa + kk * 32), smem_desc_sw128(sb + kk * 32),
-                               idesc, (kb > 0 || kk > 0) ? 1u : 0u);
+                    for (int kk = 0; kk < TC_BK / 32; ++kk) {
+                        const uint32_t accf = (kb > 0 || kk > 0) ? 1u : 0u;
+                        const uint64_t bd = smem_desc_sw128(sb + kk * 32);
+                        mma_i8(tmem, smem_desc_sw128(sa + kk * 32), bd, idesc, accf);
+                        if (lower)
+                            mma_i8(tmem + TC_TMEM_COLS,
+                                   smem_desc_sw128(sa + TC_MMA_M * TC_BK + kk * 32), bd, idesc,
+                                   accf);
+                    }
                     mma_commit(&empty[s]);
                 }
-                mma_commit(&tfull[acc]);  // also on abort: the epilogue then sees the flag
+                mma_commit(tfull);  // also on abort: the epilogue then sees the flag
                 if (!ok) break;
             }
             // every MMA issued by this thread has completed once `drain` flips
@@ -260,11 +268,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         }
     } else {
         // ---------------- epilogue: TMEM -> registers -> C
-        const int q = warp & 3;  // TMEM lane quarter of this warp
+        const int q = warp & 3;            // TMEM lane quarter of this warp
+        const int half = (warp - 2) >> 2;  // 0: upper 128 rows, 1: lower 128 rows
         int it = 0;
         for (int tile = blockIdx.x; tile < total; tile += gridDim.x, ++it) {
-            const int acc = it & 1, use = it >> 1;
-            if (!mbar_wait(&tfull[acc], use & 1)) {
+            if (!mbar_wait(tfull, it & 1)) {
                 atomicExch(err, TC_ERR_EPILOGUE);
                 atomicExch(abort_flag, 1);
                 break;
@@ -272,17 +280,18 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             if (*(volatile int *)abort_flag) break;
             const int z = tile / per_z, r = tile % per_z;
-            const int row = (r % tiles_m) * TC_BM + q * 32 + lane;
+            const int row = (r % tiles_m) * TC_BM + half * TC_MMA_M + q * 32 + lane;
+            const bool live = (r % tiles_m) * TC_BM + half * TC_MMA_M < a_zrows;
             const int n0 = (r / tiles_m) * TC_BN;
             int32_t *C = (int32_t *)Cv + (MODE == 0 ? (int64_t)z * c_zstride : 0);
             uint8_t *R = (uint8_t *)Cv + (MODE == 1 ? (int64_t)z * c_zstride : 0);
             const int pz = crt_modulus(z);
             const double pzinv = 1.0 / (double)pz;
 #pragma unroll 1
-            for (int c0 = 0; c0 < TC_BN; c0 += 16) {
+            for (int c0 = 0; c0 < TC_BN && live; c0 += 16) {
                 uint32_t v[16];
-                const uint32_t taddr =
-                    tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * TC_TMEM_COLS + c0);
+                const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) +
+                                       (uint32_t)(half * TC_TMEM_COLS + c0);
                 asm volatile(
                     "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
                     "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
@@ -309,10 +318,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     }
                 }
             }
-            // accumulator drained: the MMA warp may overwrite it
+            // accumulators drained: the MMA warp may overwrite them
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncwarp();
-            if (lane == 0) mbar_arrive(&tempty[acc]);
+            if (lane == 0) mbar_arrive(tempty);
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -360,7 +369,8 @@ template <int MODE>
 static int launch_tc(int64_t mp, int64_t np, int64_t K, const int8_t *A, int64_t lda,
                      int64_t a_cols, const int8_t *B, int64_t ldb, int64_t b_cols, int64_t b_xoff,
                      void *C, int64_t ldc, int *err, cudaStream_t s, int nz, int64_t c_zstride) {
-    if (mp % TC_BM || np % TC_BN || K % TC_BK || b_xoff % 16 || K <= 0 || nz < 1) return MFLAB_ERR_ARG;
+    if (mp % TC_MMA_M || np % TC_BN || K % TC_BK || b_xoff % 16 || K <= 0 || nz < 1)
+        return MFLAB_ERR_ARG;
     if (K > a_cols || b_xoff + K > b_cols || K > 0x7fffffff || b_xoff > 0x7fffffff)
         return MFLAB_ERR_ARG;
     if (mp * nz > 0x7fffffff || np * nz > 0x7fffffff || np / TC_BN > 65535 || nz > 65535)
@@ -382,11 +392,12 @@ static int launch_tc(int64_t mp, int64_t np, int64_t K, const int8_t *A, int64_t
     cudaGetDevice(&dev);
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0)
         sms = 148;
-    const int64_t tiles = (mp / TC_BM) * (np / TC_BN) * nz;
+    const int64_t tiles_m = (mp + TC_BM - 1) / TC_BM;
+    const int64_t tiles = tiles_m * (np / TC_BN) * nz;
     if (tiles > 0x7fffffff) return MFLAB_ERR_UNSUPPORTED;
     const unsigned grid = (unsigned)(tiles < sms ? tiles : sms);
     int8_tc_gemm_kernel<MODE><<<grid, TC_THREADS, TC_SMEM, s>>>(
-        ta, tb, (int)K, (int)b_xoff, C, ldc, (int)mp, (int)np, c_zstride, (int)(mp / TC_BM),
+        ta, tb, (int)K, (int)b_xoff, C, ldc, (int)mp, (int)np, c_zstride, (int)tiles_m,
         (int)(np / TC_BN), nz, err);
     return record_cuda_error(cudaGetLastError(), "int8 tc gemm");
 }
