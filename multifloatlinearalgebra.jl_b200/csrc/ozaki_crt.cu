@@ -182,12 +182,12 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
         for (int t = 0; t < CRT_MAXT; ++t) {
             if (t < T) {
-                uint32_t packed = 0;
+                uint32_t packed = 0;  // bytes of elements 3..0, by multiply-add
 #pragma unroll
-                for (int u = 0; u < 4; ++u)
-                    packed |= crt_residue<WD>(w[u], c.wt[t], ng[u] ? c.negoff[WD - 3][t] : 128u,
-                                              crt_modulus(t))
-                              << (8 * u);
+                for (int u = 3; u >= 0; --u)
+                    packed = packed * 256u +
+                             crt_residue<WD>(w[u], c.wt[t], ng[u] ? c.negoff[WD - 3][t] : 128u,
+                                             crt_modulus(t));
                 *(uint32_t *)(dst + (size_t)t * plane8 + (size_t)q * kp) = packed ^ 0x80808080u;
             }
         }
@@ -227,12 +227,12 @@ __global__ void __launch_bounds__(128)
 #pragma unroll
         for (int t = 0; t < CRT_MAXT; ++t) {
             if (t < T) {
-                uint32_t packed = 0;
+                uint32_t packed = 0;  // bytes of elements 3..0, by multiply-add
 #pragma unroll
-                for (int u = 0; u < 4; ++u)
-                    packed |= crt_residue<WD>(w[u], c.wt[t], ng[u] ? c.negoff[WD - 3][t] : 128u,
-                                              crt_modulus(t))
-                              << (8 * u);
+                for (int u = 3; u >= 0; --u)
+                    packed = packed * 256u +
+                             crt_residue<WD>(w[u], c.wt[t], ng[u] ? c.negoff[WD - 3][t] : 128u,
+                                             crt_modulus(t));
                 *(uint32_t *)(dst + (size_t)t * plane8 + (size_t)(Q - 1 - q) * kp) =
                     packed ^ 0x80808080u;
             }
@@ -550,12 +550,17 @@ struct CrtPlan {
 };
 
 // largest digit width h that T moduli support for Q digits and padded depth
-// kp: every digit is bounded by 2^h (Q = 1: |D| <= 2^(h-1) + N/2) or 2^(h+1)
-// (Q = 2: the second digit carries a remainder below 2 units), and
-// P > 2 Q kp bound^2 must hold
+// kp, with P > 2 max|G_L| for every level sum G_L:
+//   Q = 1: the scaled entry is below 2^(h-1) (1 + 2^-52) in magnitude and
+//          every limb rounds by at most 1/2, so |D| <= 2^(h-1) (1 + 2^(3-h))
+//          and |G| <= kp 2^(2h-2) 1.002; 2h <= fl - log2(kp) gives
+//          2 |G| < 2^fl <= P;
+//   Q = 2: digits are bounded by 2^(h+1) (the second one carries the
+//          remainder of the first), level sums have up to 2 kp terms, and
+//          P > 2 Q kp 2^(2h+2) is kept.
 static int crt_h_for(int T, int Q, int64_t kp) {
     const int fl = crt_tables(T).bitlen - 1;  // P >= 2^fl
-    const int h = (fl - ceil_log2((int64_t)Q * kp) - (Q == 1 ? 2 : 4)) / 2;
+    const int h = Q == 1 ? (fl - ceil_log2(kp)) / 2 : (fl - ceil_log2((int64_t)Q * kp) - 4) / 2;
     return h < CRT_MAXH ? h : CRT_MAXH;
 }
 

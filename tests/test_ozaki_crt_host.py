@@ -37,8 +37,10 @@ def _P(mods, T):
 @pytest.mark.parametrize("N", [2, 3, 4])
 @pytest.mark.parametrize("k", [1, 100, 2048, 8192, 30000])
 def test_plan_keeps_level_sums_exact(mf, N, k):
-    """for every modulus count the digit width satisfies P > 2 Q kp bound^2
-    (bound 2^h for one digit, 2^(h+1) for two) and int32 exactness"""
+    """for every modulus count the digit width keeps every level sum below
+    P / 2 (one digit: |D| <= 2^(h-1) + 2^(h-52) + 2 from the (-1/2, 1/2)
+    scaling, the lower limbs and the limb rounding; two digits: 2^(h+1), up
+    to 2 kp terms per level) and the int32 sums exact"""
     mods = _moduli(mf)
     kp = max(128, (k + 127) // 128 * 128)
     for T in range(20, 50):
@@ -48,8 +50,12 @@ def test_plan_keeps_level_sums_exact(mf, N, k):
             continue
         Q, h = plan["digits"], plan["digit_bits"]
         assert plan["moduli"] == T and Q == (1 if N == 2 else 2)
-        bound = 2 ** h if Q == 1 else 2 ** (h + 1)
-        assert _P(mods, T) > 2 * Q * kp * bound * bound
+        if Q == 1:
+            bound = 2 ** (h - 1) + 2 ** (h - 52) + 2
+            assert _P(mods, T) > 2 * kp * bound * bound
+        else:
+            bound = 2 ** (h + 1)
+            assert _P(mods, T) > 2 * Q * kp * bound * bound
         assert Q * kp * 2 ** 14 < 2 ** 31
 
 
