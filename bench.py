@@ -164,18 +164,16 @@ def cpu_sample(mfref, N, n, threads, target_s=15.0):
     syn = import_module("mflab200.synthetic")
     rng = np.random.default_rng(11)
     B = syn.randn_mf(rng, N, n, n, spread=20)
-    r = 4
-    A = syn.randn_mf(rng, N, r, n, spread=20)
-    t0 = time.perf_counter()
-    mfref.gemm(A, B, nthreads=threads)
-    dt = time.perf_counter() - t0
-    r2 = int(min(n, max(r, r * target_s / max(dt, 1e-3))))
-    if r2 > r:
-        r = r2
+    r, dt = 4, 0.0
+    while True:
         A = syn.randn_mf(rng, N, r, n, spread=20)
         t0 = time.perf_counter()
         mfref.gemm(A, B, nthreads=threads)
         dt = time.perf_counter() - t0
+        if dt >= 0.6 * target_s or r >= n:
+            break
+        # grow the sample towards target_s of CPU work (at least doubling)
+        r = int(min(n, max(2 * r, r * target_s / max(dt, 1e-3))))
     gf = 2.0 * r * n * n / dt / 1e9
     return gf, (f"C[:{r}, :] of the n={n} x{N} GEMM (k={n}) on {threads} host threads, "
                 f"{dt:.1f} s")
@@ -233,6 +231,7 @@ class Runner:
         self.mf = __graft_entry__.load_package()
         from importlib import import_module
         self.syn = import_module("mflab200.synthetic")
+        self.sharding = import_module("mflab200.sharding")
         self.stream = torch.cuda.current_stream()
 
     def barrier(self):
@@ -251,12 +250,7 @@ class Runner:
             fn()
         e1.record(self.stream)
         self.barrier()
-        t = e0.elapsed_time(e1) / 1e3
-        if self.world > 1:
-            tt = torch.tensor([t], device="cuda")
-            self.dist.all_reduce(tt, op=self.dist.ReduceOp.MAX)
-            t = float(tt.item())
-        return t
+        return self.sharding.max_over_ranks(e0.elapsed_time(e1) / 1e3)
 
     def operands(self, N, n):
         mf, syn = self.mf, self.syn
@@ -506,10 +500,9 @@ def main():
                 scheme = "slices"  # the modulus table cannot reach the requirement
                 acc = R.accuracy_search(N, n, A, B, Cm, scheme, e_plain, check)
     knob = acc.get("moduli", acc.get("slices", 0))
-    if world > 1:
-        t = torch.tensor([knob, 1 if scheme == "modular" else 0], device="cuda")
-        dist.broadcast(t, 0)
-        knob, scheme = int(t[0].item()), ("modular" if int(t[1].item()) else "slices")
+    # every rank runs the route rank 0 tuned
+    knob = R.sharding.agree(knob)
+    scheme = "modular" if R.sharding.agree(1 if scheme == "modular" else 0) else "slices"
     oz_cfg = R.cfg(scheme, knob)
     head_cfg = oz_cfg if route == "ozaki" else plain_cfg
 
