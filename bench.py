@@ -45,6 +45,9 @@ def parse():
     p.add_argument("--scheme", default="modular", choices=["modular", "slices"],
                    help="INT8 scheme of the headline route (modular falls back to slices when "
                         "the modulus table cannot reach the accuracy)")
+    p.add_argument("--knob", type=int, default=0,
+                   help="fixed modulus (modular) or slice (slices) count instead of the "
+                        "equal-error search (the error at that count is still reported)")
     p.add_argument("--no-slices", action="store_true",
                    help="skip the digit-slice companion of the modular headline")
     p.add_argument("--no-x4", action="store_true", help="skip the Float64x4 companion run")
@@ -491,6 +494,12 @@ def main():
         e_plain = check()
         if route != "ozaki":
             acc = {"plain_max_rel_err": e_plain, "samples": 256}
+        elif args.knob > 0:
+            mf.gemm_(Cm, A, B, config=R.cfg(scheme, args.knob))
+            knob_name = "moduli" if scheme == "modular" else "slices"
+            acc = {"scheme": scheme, knob_name: args.knob, "plain_max_rel_err": e_plain,
+                   "ozaki_max_rel_err": check(), "samples": 256,
+                   "rule": f"{knob_name} count fixed on the command line"}
         else:
             try:
                 acc = R.accuracy_search(N, n, A, B, Cm, scheme, e_plain, check)
