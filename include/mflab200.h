@@ -127,6 +127,28 @@ int mflab_gemm_ozaki_crt(mflab_handle *h, void *stream, int limbs, int moduli, i
                          const double *B, int64_t ldb, int64_t lsb, double *C, int64_t ldc,
                          int64_t lsc, const double *alpha, const double *beta);
 
+/* lower(C) = alpha * op(A) * op(A)^T + beta * lower(C) through the modular
+   INT8 route (the SYRK / trailing-update form of mflab_gemm_ozaki_crt):
+   trans = 1 takes A as k x n and forms A^T A (the syrk!(C, P, alpha, beta)
+   form, src/kernels/syrk.jl:67-108); trans = 0 takes A as n x k and forms
+   A A^T (the Cholesky trailing update).  Only the 256 x 256 tiles that meet
+   the lower triangle are multiplied; the strict upper triangle of C is
+   neither read nor written.  moduli = 0: tuner (one stream synchronisation).
+   No reference counterpart for the route itself. */
+int mflab_syrk_lower_ozaki(mflab_handle *h, void *stream, int limbs, int moduli, int trans,
+                           int64_t n, int64_t k, const double *A, int64_t lda, int64_t lsa,
+                           double *C, int64_t ldc, int64_t lsc, const double *alpha,
+                           const double *beta);
+
+/* Blocked lower Cholesky with INT8 trailing updates: panels of nb columns are
+   factored as in mflab_potrf (inner block `block` <= 32, reference order
+   inside the panel, cholesky.jl:68-107), then the trailing matrix gets
+   lower(A22) -= L21 L21^T through mflab_syrk_lower_ozaki (moduli = 0: tuned
+   per update).  *info as mflab_potrf; the device info word is read after
+   every panel (one synchronisation per panel). */
+int mflab_potrf_ozaki(mflab_handle *h, void *stream, int limbs, int moduli, int64_t n, double *A,
+                      int64_t lda, int64_t lsa, int64_t nb, int64_t block, int *info);
+
 /* modulus count used by the last mflab_gemm_ozaki_crt on this handle (no
    reference counterpart). */
 int mflab_ozaki_last_moduli(mflab_handle *h);

@@ -141,6 +141,7 @@ class KernelConfig:
     ozaki_engine: str = "tcgen05"
     ozaki_scheme: str = "auto"
     ozaki_moduli: int = 0
+    ozaki_block: int = 256
     solve_order: str = "matched"
 
 
@@ -399,13 +400,17 @@ def ozaki_scheme(config: KernelConfig = _DEFAULT) -> str:
     return sch
 
 
-def _gemm_ozaki(lib, h, s, N, C_, A, B, alpha, beta, config):
+def _int8_engine(config: KernelConfig) -> int:
     engines = {"tcgen05": 0, "library": 1}
     if config.ozaki_engine not in engines:
         raise ArgumentError("ozaki_engine must be :tcgen05 or :library")
     if config.ozaki_slices < 0 or config.ozaki_moduli < 0:
         raise ArgumentError("ozaki_slices and ozaki_moduli must be >= 0")
-    _check(lib.mflab_set_int8_engine(h, engines[config.ozaki_engine]), "gemm!")
+    return engines[config.ozaki_engine]
+
+
+def _gemm_ozaki(lib, h, s, N, C_, A, B, alpha, beta, config):
+    _check(lib.mflab_set_int8_engine(h, _int8_engine(config)), "gemm!")
     m, k, n = A.m, A.n, B.n
     args = (m, n, k, A.ptr(), A.ld, A.ls, B.ptr(), B.ld, B.ls, C_.ptr(), C_.ld, C_.ls,
             _scalar(N, alpha), _scalar(N, beta))
@@ -476,8 +481,16 @@ def syrk_(C_: MFMatrix, P: MFMatrix, alpha=1.0, beta=0.0, uplo: str = "lower",
         raise DimensionMismatch("syrk! output dimensions differ")
     _no_alias("syrk!", C_, P)
     lib, h, s = _lib_h(C_)
-    rc = lib.mflab_syrk_lower(h, s, N, n, k, P.ptr(), P.ld, P.ls, C_.ptr(), C_.ld, C_.ls,
-                              _scalar(N, alpha), _scalar(N, beta))
+    if config.gemm_strategy == "ozaki":
+        _check(lib.mflab_set_int8_engine(h, _int8_engine(config)), "syrk!")
+        if ozaki_scheme(config) != "modular":
+            raise ArgumentError("the INT8 syrk! route uses the modular scheme (ozaki_moduli)")
+        rc = lib.mflab_syrk_lower_ozaki(h, s, N, int(config.ozaki_moduli), 1, n, k, P.ptr(), P.ld,
+                                        P.ls, C_.ptr(), C_.ld, C_.ls, _scalar(N, alpha),
+                                        _scalar(N, beta))
+    else:
+        rc = lib.mflab_syrk_lower(h, s, N, n, k, P.ptr(), P.ld, P.ls, C_.ptr(), C_.ld, C_.ls,
+                                  _scalar(N, alpha), _scalar(N, beta))
     _check(rc, "syrk!")
     return C_
 
@@ -608,7 +621,17 @@ def cholesky_(A: MFMatrix, check: bool = True, config: KernelConfig = _DEFAULT) 
     info = torch.zeros(1, dtype=torch.int32, device=A.storage.device)
     block = max(config.cholesky_block, 1)
     lib, h, s = _lib_h(A)
-    _check(lib.mflab_potrf(h, s, N, A.m, A.ptr(), A.ld, A.ls, block, info.data_ptr()), "cholesky!")
+    if config.gemm_strategy == "ozaki":
+        # INT8 trailing updates between panels of ozaki_block columns
+        if ozaki_scheme(config) != "modular":
+            raise ArgumentError("the INT8 trailing update uses the modular scheme (ozaki_moduli)")
+        _check(lib.mflab_set_int8_engine(h, _int8_engine(config)), "cholesky!")
+        _check(lib.mflab_potrf_ozaki(h, s, N, int(config.ozaki_moduli), A.m, A.ptr(), A.ld, A.ls,
+                                     max(int(config.ozaki_block), block), block,
+                                     info.data_ptr()), "cholesky!")
+    else:
+        _check(lib.mflab_potrf(h, s, N, A.m, A.ptr(), A.ld, A.ls, block, info.data_ptr()),
+               "cholesky!")
     st = _read_info(info)
     if st == -1 and check:
         raise DomainError("cholesky!: input matrix contains non-finite entries")

@@ -96,6 +96,9 @@ SIGNATURES = {
     "mflab_gemm_ozaki_crt": [_vp, _vp, _int, _int, _i64, _i64, _i64, _vp, _i64, _i64, _vp, _i64,
                              _i64, _vp, _i64, _i64, _d, _d],
     "mflab_ozaki_last_moduli": [_vp],
+    "mflab_syrk_lower_ozaki": [_vp, _vp, _int, _int, _int, _i64, _i64, _vp, _i64, _i64, _vp, _i64,
+                               _i64, _d, _d],
+    "mflab_potrf_ozaki": [_vp, _vp, _int, _int, _i64, _vp, _i64, _i64, _i64, _i64, _vp],
     "mflab_ozaki_crt_plan": [_int, _i64, _int, _int, C.POINTER(_int), C.POINTER(_int),
                              C.POINTER(_int)],
     "mflab_ozaki_crt_modulus": [_int],

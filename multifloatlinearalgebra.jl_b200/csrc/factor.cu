@@ -103,6 +103,58 @@ static int potrf_n(int64_t n, Mat A, int64_t block, int *info, cudaStream_t s) {
     return MFLAB_OK;
 }
 
+// Cholesky with INT8 trailing updates: panels of nb columns; inside a panel
+// the blocked algorithm above (panel kernel, TRSM, lower update restricted to
+// the panel's columns) in the reference order; after each panel the trailing
+// matrix gets lower(A22) -= L21 L21^T through the modular INT8 route.  The
+// device info word is read after every panel (one synchronisation each), so a
+// failed pivot stops the factorization before the next trailing update.
+template <int N>
+static int potrf_ozaki_n(mflab_handle *h, int64_t n, Mat A, int64_t nb, int64_t block, int moduli,
+                         int *info, cudaStream_t s) {
+    const double mone[4] = {-1.0, 0.0, 0.0, 0.0}, one[4] = {1.0, 0.0, 0.0, 0.0};
+    cudaError_t e = cudaMemsetAsync(info, 0, sizeof(int), s);
+    if (e != cudaSuccess) return record_cuda_error(e, "potrf info");
+    if (n == 0) return MFLAB_OK;
+    int64_t tot = n * n;
+    nonfinite_kernel<N><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(n, n, A, 1, info);
+    int rc = record_cuda_error(cudaGetLastError(), "potrf check");
+    if (rc) return rc;
+    for (int64_t j0 = 0; j0 < n; j0 += nb) {
+        const int64_t j1 = j0 + nb < n ? j0 + nb : n;  // panel columns [j0, j1)
+        for (int64_t first = j0; first < j1; first += block) {
+            const int64_t last = first + block - 1 < j1 - 1 ? first + block - 1 : j1 - 1;
+            const int w = (int)(last - first + 1);
+            potrf_panel_kernel<N><<<1, 32, 0, s>>>(A, first, w, info);
+            rc = record_cuda_error(cudaGetLastError(), "potrf panel");
+            if (rc) return rc;
+            if (last < n - 1) {
+                const int64_t t = n - 1 - last, cols = j1 - 1 - last;
+                rc = launch_trsm_info(N, 1, 0, 1, 0, t, w, A.at(first, first), A.at(last + 1, first),
+                                      one, s, info);
+                if (rc) return rc;
+                if (cols > 0) {
+                    rc = launch_mm(N, false, true, 1, false, t, cols, w, A.at(last + 1, first),
+                                   A.at(last + 1, first), A.at(last + 1, last + 1), mone, one, s,
+                                   info);
+                    if (rc) return rc;
+                }
+            }
+        }
+        int hinfo = 0;
+        e = cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return record_cuda_error(e, "potrf info read");
+        if (hinfo != 0) return MFLAB_OK;
+        if (j1 < n) {
+            rc = ozaki_crt_syrk(h, N, moduli, 0, n - j1, j1 - j0, A.at(j1, j0), A.at(j1, j1), mone,
+                                one, s, nullptr);
+            if (rc) return rc;
+        }
+    }
+    return MFLAB_OK;
+}
+
 // ------------------------------------------------------------------ LU ---
 // single CTA: pivot search in column k (rows k..m-1), full-row swap,
 // zero-pivot test, reciprocal and scaling of the column below the pivot
@@ -402,6 +454,23 @@ extern "C" int mflab_potrf(mflab_handle *h, void *stream, int limbs, int64_t n, 
     case 2: return mfl::potrf_n<2>(n, a, block, info, s);
     case 3: return mfl::potrf_n<3>(n, a, block, info, s);
     default: return mfl::potrf_n<4>(n, a, block, info, s);
+    }
+}
+
+extern "C" int mflab_potrf_ozaki(mflab_handle *h, void *stream, int limbs, int moduli, int64_t n,
+                                 double *A, int64_t lda, int64_t lsa, int64_t nb, int64_t block,
+                                 int *info) {
+    if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
+    if (n < 0 || (n > 0 && lda < n) || !info || moduli < 0) return MFLAB_ERR_ARG;
+    if (block < 1) block = 1;
+    if (block > 32) return MFLAB_ERR_UNSUPPORTED;
+    if (nb < block) nb = block;
+    Mat a{A, lda, lsa};
+    cudaStream_t s = (cudaStream_t)stream;
+    switch (limbs) {
+    case 2: return mfl::potrf_ozaki_n<2>(h, n, a, nb, block, moduli, info, s);
+    case 3: return mfl::potrf_ozaki_n<3>(h, n, a, nb, block, moduli, info, s);
+    default: return mfl::potrf_ozaki_n<4>(h, n, a, nb, block, moduli, info, s);
     }
 }
 

@@ -143,6 +143,26 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
 // MODE 0 stores the int32 sums; MODE 1 stores their residues modulo
 // crt_modulus(z) as bytes (C is then a byte matrix: ldc and c_zstride in
 // bytes), the only part of the sums the modular route needs.
+// coordinates of tile number `tile`: all tiles_m x tiles_n tiles of each
+// problem (row tiles fastest), or with `tri` only the tiles that meet the
+// lower triangle of a square grid (column by column)
+__device__ __forceinline__ void tc_tile(int tile, int per_z, int tiles_m, int tri, int &z, int &mt,
+                                        int &nt) {
+    z = tile / per_z;
+    int r = tile % per_z;
+    if (!tri) {
+        mt = r % tiles_m;
+        nt = r / tiles_m;
+        return;
+    }
+    nt = 0;
+    while (r >= tiles_m - nt) {
+        r -= tiles_m - nt;
+        ++nt;
+    }
+    mt = nt + r;
+}
+
 constexpr int TC_THREADS = 320;
 constexpr uint32_t TC_TMEM_ALLOC = 2 * TC_TMEM_COLS;
 
@@ -151,7 +171,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     int8_tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA,
                         const __grid_constant__ CUtensorMap tmB, int K, int b_xoff, void *Cv,
                         int64_t ldc, int a_zrows, int b_zrows, int64_t c_zstride, int tiles_m,
-                        int tiles_n, int nz, int *err) {
+                        int tiles_n, int nz, int tri, int *err) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     uint64_t *full = (uint64_t *)(smem + TC_STAGES * TC_STAGE_BYTES);
@@ -164,7 +184,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
     const int ksteps = K / TC_BK;
-    const int per_z = tiles_m * tiles_n;
+    const int per_z = tri ? tiles_m * (tiles_m + 1) / 2 : tiles_m * tiles_n;
     const int total = per_z * nz;
 
     if (threadIdx.x == 0) {
@@ -196,9 +216,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             int ks = 0;
             for (int tile = blockIdx.x; tile < total && !*(volatile int *)abort_flag;
                  tile += gridDim.x) {
-                const int z = tile / per_z, r = tile % per_z;
-                const int am0 = z * a_zrows + (r % tiles_m) * TC_BM;
-                const int bn0 = z * b_zrows + (r / tiles_m) * TC_BN;
+                int z, mt, nt;
+                tc_tile(tile, per_z, tiles_m, tri, z, mt, nt);
+                const int am0 = z * a_zrows + mt * TC_BM;
+                const int bn0 = z * b_zrows + nt * TC_BN;
                 for (int kb = 0; kb < ksteps; ++kb, ++ks) {
                     const int s = ks % TC_STAGES;
                     if (ks >= TC_STAGES && !mbar_wait(&empty[s], ((ks / TC_STAGES) - 1) & 1)) {
@@ -227,8 +248,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             int ks = 0, it = 0;
             for (int tile = blockIdx.x; tile < total && !*(volatile int *)abort_flag;
                  tile += gridDim.x, ++it) {
-                const int r = tile % per_z;
-                const bool lower = (r % tiles_m) * TC_BM + TC_MMA_M < a_zrows;
+                int z, mt, nt;
+                tc_tile(tile, per_z, tiles_m, tri, z, mt, nt);
+                const bool two_halves = mt * TC_BM + TC_MMA_M < a_zrows;
                 if (it > 0 && !mbar_wait(tempty, (it - 1) & 1)) {
                     atomicExch(err, TC_ERR_MMA);
                     atomicExch(abort_flag, 1);
@@ -252,7 +274,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                         const uint32_t accf = (kb > 0 || kk > 0) ? 1u : 0u;
                         const uint64_t bd = smem_desc_sw128(sb + kk * 32);
                         mma_i8(tmem, smem_desc_sw128(sa + kk * 32), bd, idesc, accf);
-                        if (lower)
+                        if (two_halves)
                             mma_i8(tmem + TC_TMEM_COLS,
                                    smem_desc_sw128(sa + TC_MMA_M * TC_BK + kk * 32), bd, idesc,
                                    accf);
@@ -279,10 +301,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             if (*(volatile int *)abort_flag) break;
-            const int z = tile / per_z, r = tile % per_z;
-            const int row = (r % tiles_m) * TC_BM + half * TC_MMA_M + q * 32 + lane;
-            const bool live = (r % tiles_m) * TC_BM + half * TC_MMA_M < a_zrows;
-            const int n0 = (r / tiles_m) * TC_BN;
+            int z, mt, nt;
+            tc_tile(tile, per_z, tiles_m, tri, z, mt, nt);
+            const int row = mt * TC_BM + half * TC_MMA_M + q * 32 + lane;
+            const bool live = mt * TC_BM + half * TC_MMA_M < a_zrows;
+            const int n0 = nt * TC_BN;
             int32_t *C = (int32_t *)Cv + (MODE == 0 ? (int64_t)z * c_zstride : 0);
             uint8_t *R = (uint8_t *)Cv + (MODE == 1 ? (int64_t)z * c_zstride : 0);
             const int pz = crt_modulus(z);
@@ -368,7 +391,8 @@ static int make_map(CUtensorMap *map, const int8_t *base, int64_t rows, int64_t 
 template <int MODE>
 static int launch_tc(int64_t mp, int64_t np, int64_t K, const int8_t *A, int64_t lda,
                      int64_t a_cols, const int8_t *B, int64_t ldb, int64_t b_cols, int64_t b_xoff,
-                     void *C, int64_t ldc, int *err, cudaStream_t s, int nz, int64_t c_zstride) {
+                     void *C, int64_t ldc, int *err, cudaStream_t s, int nz, int64_t c_zstride,
+                     int tri) {
     if (mp % TC_MMA_M || np % TC_BN || K % TC_BK || b_xoff % 16 || K <= 0 || nz < 1)
         return MFLAB_ERR_ARG;
     if (K > a_cols || b_xoff + K > b_cols || K > 0x7fffffff || b_xoff > 0x7fffffff)
@@ -393,12 +417,14 @@ static int launch_tc(int64_t mp, int64_t np, int64_t K, const int8_t *A, int64_t
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0)
         sms = 148;
     const int64_t tiles_m = (mp + TC_BM - 1) / TC_BM;
-    const int64_t tiles = tiles_m * (np / TC_BN) * nz;
+    if (tri && tiles_m != np / TC_BN) return MFLAB_ERR_ARG;
+    const int64_t tiles =
+        (tri ? tiles_m * (tiles_m + 1) / 2 : tiles_m * (np / TC_BN)) * nz;
     if (tiles > 0x7fffffff) return MFLAB_ERR_UNSUPPORTED;
     const unsigned grid = (unsigned)(tiles < sms ? tiles : sms);
     int8_tc_gemm_kernel<MODE><<<grid, TC_THREADS, TC_SMEM, s>>>(
         ta, tb, (int)K, (int)b_xoff, C, ldc, (int)mp, (int)np, c_zstride, (int)tiles_m,
-        (int)(np / TC_BN), nz, err);
+        (int)(np / TC_BN), nz, tri, err);
     return record_cuda_error(cudaGetLastError(), "int8 tc gemm");
 }
 
@@ -411,18 +437,19 @@ int int8_gemm_tc(int64_t mp, int64_t np, int64_t K, const int8_t *A, int64_t lda
                  const int8_t *B, int64_t ldb, int64_t b_cols, int64_t b_xoff, int32_t *C,
                  int64_t ldc, int *err, cudaStream_t s, int nz, int64_t c_zstride) {
     return launch_tc<0>(mp, np, K, A, lda, a_cols, B, ldb, b_cols, b_xoff, C, ldc, err, s, nz,
-                        c_zstride);
+                        c_zstride, 0);
 }
 
 // As int8_gemm_tc with nz stacked problems, but problem z stores the residues
 // of its sums modulo crt_modulus(z) as bytes: R + z r_zstride, column-major
-// with leading dimension ldr (bytes).
+// with leading dimension ldr (bytes).  tri != 0 computes only the 256 x 256
+// tiles that meet the lower triangle (needs ceil(mp / 256) == np / 256).
 int int8_gemm_tc_mod(int64_t mp, int64_t np, int64_t K, const int8_t *A, int64_t lda,
                      int64_t a_cols, const int8_t *B, int64_t ldb, int64_t b_cols, int64_t b_xoff,
                      uint8_t *R, int64_t ldr, int *err, cudaStream_t s, int nz,
-                     int64_t r_zstride) {
+                     int64_t r_zstride, int tri) {
     return launch_tc<1>(mp, np, K, A, lda, a_cols, B, ldb, b_cols, b_xoff, R, ldr, err, s, nz,
-                        r_zstride);
+                        r_zstride, tri);
 }
 
 }  // namespace mfl

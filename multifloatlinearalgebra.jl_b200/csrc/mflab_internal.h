@@ -47,9 +47,13 @@ int int8_gemm_tc(int64_t mp, int64_t np, int64_t K, const int8_t *A, int64_t lda
 int int8_gemm_tc_mod(int64_t mp, int64_t np, int64_t K, const int8_t *A, int64_t lda,
                      int64_t a_cols, const int8_t *B, int64_t ldb, int64_t b_cols, int64_t b_xoff,
                      uint8_t *R, int64_t ldr, int *err, cudaStream_t s, int nz,
-                     int64_t r_zstride);
+                     int64_t r_zstride, int tri = 0);
 void record_error_message(const char *msg);
-// modular INT8 route (ozaki_crt.cu); T = 0 lets the tuner choose
+// modular INT8 route (ozaki_crt.cu); T = 0 lets the tuner choose.  The SYRK
+// form writes lower(C) = alpha op(A) op(A)^T + beta lower(C), op(A) = A
+// (trans 0, n x k) or A^T (trans 1, A k x n)
+int ozaki_crt_syrk(mflab_handle *hd, int N, int T, int trans, int64_t n, int64_t k, Mat A, Mat C,
+                   const double *alpha, const double *beta, cudaStream_t s, int *T_used);
 int ozaki_crt_gemm(mflab_handle *hd, int N, int T, int64_t m, int64_t n, int64_t k, Mat A, Mat B,
                    Mat C, const double *alpha, const double *beta, cudaStream_t s, int *T_used);
 

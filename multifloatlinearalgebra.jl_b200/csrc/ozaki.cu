@@ -179,6 +179,9 @@ __global__ void oz_accum_kernel(int64_t m, int64_t n, int S, const int32_t *I, i
 // the number of bits between the truncation scale of the digit products and
 // the entry's own magnitude scale.  One warp per sample; the maximum over
 // samples is kept in eighths of a bit (atomicMax).
+// TA / TB: the operand is given transposed (A as a k x m, B as an n x k
+// column-major matrix), for the Gram products of the SYRK forms.
+template <bool TA, bool TB>
 __global__ void oz_gap_kernel(int64_t m, int64_t n, int64_t k, Mat A, Mat B, const int *rowexp,
                               const int *colexp, int samples, int *gap8) {
     const int s = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
@@ -193,7 +196,8 @@ __global__ void oz_gap_kernel(int64_t m, int64_t n, int64_t k, Mat A, Mat B, con
     if (ea == OZ_EXP_BAD || eb == OZ_EXP_BAD || ea == OZ_EXP_EMPTY || eb == OZ_EXP_EMPTY) return;
     double d = 0.0;
     for (int64_t kk = lane; kk < k; kk += 32)
-        d = fma(fabs(A.p[kk * A.ld + i]), fabs(B.p[j * B.ld + kk]), d);
+        d = fma(fabs(TA ? A.p[i * A.ld + kk] : A.p[kk * A.ld + i]),
+                fabs(TB ? B.p[kk * B.ld + j] : B.p[j * B.ld + kk]), d);
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) d += __shfl_xor_sync(0xffffffffu, d, off);
     if (lane == 0 && d > 0.0) {
@@ -287,7 +291,7 @@ static int oz_exponents(int64_t m, int64_t n, int64_t k, Mat A, Mat B, int *rowe
     if ((k + kchunk - 1) / kchunk > 65535) kchunk = (k + 65534) / 65535;
     dim3 gr((unsigned)((m + 255) / 256), (unsigned)((k + kchunk - 1) / kchunk));
     oz_row_exp_kernel<N><<<gr, 256, 0, s>>>(m, k, A, kchunk, rowexp);
-    oz_col_exp_kernel<N><<<(unsigned)((n + 7) / 8), 256, 0, s>>>(k, n, B, colexp);
+    if (n > 0) oz_col_exp_kernel<N><<<(unsigned)((n + 7) / 8), 256, 0, s>>>(k, n, B, colexp);
     return record_cuda_error(cudaGetLastError(), "ozaki exponents");
 }
 
@@ -391,13 +395,58 @@ int ozaki_scales(mflab_handle *h, int N, int64_t m, int64_t n, int64_t k, Mat A,
     if (tune) {
         cudaError_t e = cudaMemsetAsync(gap8, 0, sizeof(int), s);
         if (e != cudaSuccess) return record_cuda_error(e, "ozaki tune");
-        oz_gap_kernel<<<(OZ_SAMPLES + 7) / 8, 256, 0, s>>>(m, n, k, A, B, rowexp, colexp,
-                                                           OZ_SAMPLES, gap8);
+        oz_gap_kernel<false, false><<<(OZ_SAMPLES + 7) / 8, 256, 0, s>>>(
+            m, n, k, A, B, rowexp, colexp, OZ_SAMPLES, gap8);
         int g = 0;
         e = cudaMemcpyAsync(&g, gap8, sizeof(int), cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) return record_cuda_error(e, "ozaki tune read");
         *gap8_host = g;
+    }
+    return MFLAB_OK;
+}
+
+// Scales of a Gram product lower(A A^T) (trans = 0, A n x k) or lower(A^T A)
+// (trans = 1, A k x n): one exponent per row of the left factor, which is
+// also the column exponent of the right one (*exps[n] in the aux scratch);
+// tune != 0 returns the sampled scale gap (one stream synchronisation).
+int ozaki_gram_scales(mflab_handle *h, int N, int trans, int64_t n, int64_t k, Mat A,
+                      cudaStream_t s, int tune, int *gap8_host, int **exps_out) {
+    int rc = mflab_reserve_aux(h, sizeof(int) * (size_t)(n + 64));
+    if (rc) return rc;
+    int *exps = (int *)h->aux;
+    int *gap8 = exps + n;
+    if (trans == 0) {
+        switch (N) {
+        case 2: rc = oz_exponents<2>(n, 0, k, A, A, exps, exps + n, s); break;
+        case 3: rc = oz_exponents<3>(n, 0, k, A, A, exps, exps + n, s); break;
+        case 4: rc = oz_exponents<4>(n, 0, k, A, A, exps, exps + n, s); break;
+        default: return MFLAB_ERR_UNSUPPORTED;
+        }
+    } else {
+        switch (N) {
+        case 2: oz_col_exp_kernel<2><<<(unsigned)((n + 7) / 8), 256, 0, s>>>(k, n, A, exps); break;
+        case 3: oz_col_exp_kernel<3><<<(unsigned)((n + 7) / 8), 256, 0, s>>>(k, n, A, exps); break;
+        case 4: oz_col_exp_kernel<4><<<(unsigned)((n + 7) / 8), 256, 0, s>>>(k, n, A, exps); break;
+        default: return MFLAB_ERR_UNSUPPORTED;
+        }
+        rc = record_cuda_error(cudaGetLastError(), "ozaki gram exponents");
+    }
+    if (rc) return rc;
+    *exps_out = exps;
+    if (tune) {
+        cudaError_t e = cudaMemsetAsync(gap8, 0, sizeof(int), s);
+        if (e != cudaSuccess) return record_cuda_error(e, "ozaki gram tune");
+        const unsigned g = (OZ_SAMPLES + 7) / 8;
+        if (trans == 0)  // left A (n x k), right A^T given as A
+            oz_gap_kernel<false, true><<<g, 256, 0, s>>>(n, n, k, A, A, exps, exps, OZ_SAMPLES, gap8);
+        else             // left A^T given as A (k x n), right A
+            oz_gap_kernel<true, false><<<g, 256, 0, s>>>(n, n, k, A, A, exps, exps, OZ_SAMPLES, gap8);
+        int gv = 0;
+        e = cudaMemcpyAsync(&gv, gap8, sizeof(int), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return record_cuda_error(e, "ozaki gram tune read");
+        *gap8_host = gv;
     }
     return MFLAB_OK;
 }

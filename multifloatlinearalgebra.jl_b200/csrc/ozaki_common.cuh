@@ -45,6 +45,12 @@ __host__ __device__ constexpr int crt_modulus(int t) {
 int ozaki_scales(mflab_handle *h, int N, int64_t m, int64_t n, int64_t k, Mat A, Mat B,
                  cudaStream_t s, int tune, int *gap8_host, int **rowexp, int **colexp);
 
+// Exponents of a Gram product: one per row of the left factor of
+// lower(A A^T) (trans = 0, A n x k) or lower(A^T A) (trans = 1, A k x n),
+// *exps[n] in the aux scratch; tune != 0 also returns the sampled gap.
+int ozaki_gram_scales(mflab_handle *h, int N, int trans, int64_t n, int64_t k, Mat A,
+                      cudaStream_t s, int tune, int *gap8_host, int **exps);
+
 // records phase event i on s when the phases entry point is timing a call
 void ozaki_phase(int i, cudaStream_t s);
 // ev[0..3] receive the phase events of the next route call (nullptr: off)

@@ -138,14 +138,14 @@ __device__ __forceinline__ uint32_t crt_residue(const uint32_t (&w)[WD], const u
     return acc % (uint32_t)p;
 }
 
-// A (m x k, column-major planes) -> residue planes A8[t][i][q][k] (int8,
-// rows of Q kp bytes, plane stride plane8).  32 x 32 tile per block of
+// A (m x k, column-major planes) -> residue planes A8[t][i][q'][k] (int8,
+// rows of Q kp bytes, plane stride plane8; q' = q, or Q-1-q with rev).  32 x 32 tile per block of
 // 32 x 8 threads, staged through shared memory; each thread then owns 4
 // consecutive k of one row and writes one 32-bit word per (t, q).
 template <int N, int WD>
 __global__ void __launch_bounds__(256)
     crt_split_a_kernel(int64_t m, int64_t mp, int64_t k, int64_t kp, int Q, int h, int T, Mat A,
-                       const int *rowexp, int8_t *A8, size_t plane8,
+                       const int *rowexp, int8_t *A8, size_t plane8, int rev,
                        const __grid_constant__ CrtSplitConst c) {
     __shared__ double tile[N][32][33];
     const int tx = threadIdx.x, ty = threadIdx.y;
@@ -188,19 +188,21 @@ __global__ void __launch_bounds__(256)
                     packed = packed * 256u +
                              crt_residue<WD>(w[u], c.wt[t], ng[u] ? c.negoff[WD - 3][t] : 128u,
                                              crt_modulus(t));
-                *(uint32_t *)(dst + (size_t)t * plane8 + (size_t)q * kp) = packed ^ 0x80808080u;
+                *(uint32_t *)(dst + (size_t)t * plane8 + (size_t)(rev ? Q - 1 - q : q) * kp) =
+                    packed ^ 0x80808080u;
             }
         }
     }
 }
 
-// B (k x n) -> residue planes B8[t][j][Q-1-q][k] (digit order reversed so that
-// the pairs of one level are adjacent along K).  Each thread owns 4
+// B (k x n) -> residue planes B8[t][j][q'][k] with q' = Q-1-q when rev (the
+// right operand: pairs of one level adjacent along K), q' = q otherwise (the
+// left operand of a Gram product A^T A, whose rows are B's columns).  Each thread owns 4
 // consecutive k of one column.
 template <int N, int WD>
 __global__ void __launch_bounds__(128)
     crt_split_b_kernel(int64_t k, int64_t n, int64_t np, int64_t kp, int Q, int h, int T, Mat B,
-                       const int *colexp, int8_t *B8, size_t plane8,
+                       const int *colexp, int8_t *B8, size_t plane8, int rev,
                        const __grid_constant__ CrtSplitConst c) {
     const int64_t kg = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * 4;
     const int64_t j = blockIdx.y;
@@ -233,7 +235,7 @@ __global__ void __launch_bounds__(128)
                     packed = packed * 256u +
                              crt_residue<WD>(w[u], c.wt[t], ng[u] ? c.negoff[WD - 3][t] : 128u,
                                              crt_modulus(t));
-                *(uint32_t *)(dst + (size_t)t * plane8 + (size_t)(Q - 1 - q) * kp) =
+                *(uint32_t *)(dst + (size_t)t * plane8 + (size_t)(rev ? Q - 1 - q : q) * kp) =
                     packed ^ 0x80808080u;
             }
         }
@@ -376,6 +378,8 @@ __global__ void __launch_bounds__(CRT_ACC_ROWS, 3)
     const int tid = threadIdx.x;
     const int64_t i0 = (int64_t)blockIdx.x * CRT_ACC_ROWS, i = i0 + tid;
     const int64_t j = blockIdx.y;
+    // flags bit 2: lower triangle only (the GEMM skipped the tiles above it)
+    if ((flags & 4) && i0 + CRT_ACC_ROWS - 1 < j) return;
     // rows i0 .. i0+127 lie inside the padded planes (ldi = mp, a multiple of 128)
     const int segs = Q * T * (CRT_ACC_ROWS / 16);
     for (int s = tid; s < segs; s += CRT_ACC_ROWS) {
@@ -386,7 +390,7 @@ __global__ void __launch_bounds__(CRT_ACC_ROWS, 3)
     }
     asm volatile("cp.async.wait_all;" ::: "memory");
     __syncthreads();
-    if (i >= m) return;
+    if (i >= m || ((flags & 4) && i < j)) return;
     const int ea = rowexp[i], eb = colexp[j];
     mf<N> acc = from_double<N>(0.0);
     if (ea == OZ_EXP_BAD || eb == OZ_EXP_BAD) {
@@ -564,6 +568,8 @@ static int crt_h_for(int T, int Q, int64_t kp) {
     return h < CRT_MAXH ? h : CRT_MAXH;
 }
 
+static void crt_layout(CrtPlan &p);
+
 // Plan of one call.  T_req > 0: that many moduli, digits as wide as they
 // allow; T_req == 0: the tuner's requirement from the sampled scale gap.
 // Returns MFLAB_ERR_UNSUPPORTED when no table entry reaches the requirement.
@@ -599,6 +605,12 @@ static int crt_plan(int N, int64_t m, int64_t n, int64_t k, int T_req, int gap8,
     p.WP = need <= 256 ? 8 : need <= 320 ? 10 : 12;
     p.mp = (m + 127) / 128 * 128;
     p.np = (n + 255) / 256 * 256;
+    crt_layout(p);
+    return MFLAB_OK;
+}
+
+// buffer layout of a plan whose padded shapes mp, np are set
+static void crt_layout(CrtPlan &p) {
     p.ldi = p.mp;
     p.plane = ((size_t)p.ldi * p.np + 255) / 256 * 256;
     p.plane8a = (size_t)p.mp * p.Q * p.kp;
@@ -609,7 +621,6 @@ static int crt_plan(int N, int64_t m, int64_t n, int64_t k, int T_req, int gap8,
     p.lev = al((size_t)p.Q * p.T * p.plane);                 // byte residues
     p.ws = ((size_t)64 << 20) + al(p.plane * sizeof(int32_t));  // library path only
     p.total = p.a8 + p.b8 + p.lev + p.ws;
-    return MFLAB_OK;
 }
 
 template <int N, int WD>
@@ -619,10 +630,10 @@ static void crt_split(const CrtPlan &p, int64_t m, int64_t n, int64_t k, Mat A, 
     const CrtSplitConst &c = crt_split_const();
     dim3 ga((unsigned)((p.mp + 31) / 32), (unsigned)(p.kp / 32));
     crt_split_a_kernel<N, WD><<<ga, dim3(32, 8), 0, s>>>(m, p.mp, k, p.kp, p.Q, p.h, p.T, A,
-                                                         rowexp, A8, p.plane8a, c);
+                                                         rowexp, A8, p.plane8a, 0, c);
     dim3 gb((unsigned)((p.kp / 4 + 127) / 128), (unsigned)p.np);
     crt_split_b_kernel<N, WD><<<gb, 128, 0, s>>>(k, n, p.np, p.kp, p.Q, p.h, p.T, B, colexp, B8,
-                                                 p.plane8b, c);
+                                                 p.plane8b, 1, c);
 }
 
 template <int N>
@@ -726,6 +737,115 @@ int ozaki_crt_gemm(mflab_handle *hd, int N, int T, int64_t m, int64_t n, int64_t
     }
 }
 
+// ------------------------------------------------------ Gram products ---
+// Residue digits of the one factor of lower(A A^T) (trans = 0, A n x k: the
+// left operand's rows are A's rows) or lower(A^T A) (trans = 1, A k x n: its
+// rows are A's columns).  The right operand is the same factor with the digit
+// order reversed, identical for one digit.
+template <int N, int WD>
+static void crt_split_gram(const CrtPlan &p, int trans, int64_t n, int64_t k, Mat A,
+                           const int *exps, int8_t *A8, int8_t *B8, cudaStream_t s) {
+    const CrtSplitConst &c = crt_split_const();
+    for (int role = 0; role < (p.Q == 1 ? 1 : 2); ++role) {
+        int8_t *dst = role == 0 ? A8 : B8;
+        if (trans == 0) {
+            dim3 ga((unsigned)(p.mp / 32), (unsigned)(p.kp / 32));
+            crt_split_a_kernel<N, WD><<<ga, dim3(32, 8), 0, s>>>(n, p.mp, k, p.kp, p.Q, p.h, p.T, A,
+                                                                 exps, dst, p.plane8a, role, c);
+        } else {
+            dim3 gb((unsigned)((p.kp / 4 + 127) / 128), (unsigned)p.np);
+            crt_split_b_kernel<N, WD><<<gb, 128, 0, s>>>(k, n, p.np, p.kp, p.Q, p.h, p.T, A, exps,
+                                                         dst, p.plane8b, role, c);
+        }
+    }
+}
+
+template <int N>
+static int crt_syrk_n(mflab_handle *hd, const CrtPlan &p, int trans, int64_t n, int64_t k, Mat A,
+                      Mat C, const double *alpha, const double *beta, const int *exps,
+                      cudaStream_t s) {
+    char *base = (char *)hd->scratch;
+    int8_t *A8 = (int8_t *)base;
+    int8_t *B8 = p.Q == 1 ? A8 : (int8_t *)(base + p.a8);
+    uint8_t *Rs = (uint8_t *)(base + p.a8 + p.b8);
+    char *ws = base + p.a8 + p.b8 + p.lev;
+    ozaki_phase(0, s);
+    if (p.WD <= 3) crt_split_gram<N, 3>(p, trans, n, k, A, exps, A8, B8, s);
+    else if (p.WD == 4) crt_split_gram<N, 4>(p, trans, n, k, A, exps, A8, B8, s);
+    else crt_split_gram<N, 5>(p, trans, n, k, A, exps, A8, B8, s);
+    int rc = record_cuda_error(cudaGetLastError(), "modular gram split");
+    if (rc) return rc;
+    ozaki_phase(1, s);
+    const int64_t ld8 = (int64_t)p.Q * p.kp;
+    for (int L = 0; L < p.Q && rc == MFLAB_OK; ++L) {
+        const int64_t K = (int64_t)(L + 1) * p.kp, bx = (int64_t)(p.Q - 1 - L) * p.kp;
+        uint8_t *RL = Rs + (size_t)L * p.T * p.plane;
+        if (hd->int8_engine == MFLAB_INT8_TCGEN05) {
+            rc = int8_gemm_tc_mod(p.mp, p.np, K, A8, ld8, ld8, B8, ld8, ld8, bx, RL, p.ldi,
+                                  hd->dev_flags + 1, s, p.T, (int64_t)p.plane, 1);
+        } else {  // the library computes whole products; only the lower part is used
+            int32_t *G = (int32_t *)(ws + ((size_t)64 << 20));
+            const size_t cnt = (size_t)p.ldi * p.np;
+            for (int t = 0; t < p.T && rc == MFLAB_OK; ++t) {
+                rc = int8_gemm_tn(p.mp, p.np, K, A8 + (size_t)t * p.plane8a, ld8,
+                                  B8 + (size_t)t * p.plane8b + bx, ld8, G, p.ldi, ws,
+                                  (size_t)64 << 20, s);
+                if (rc) break;
+                crt_mod_kernel<<<(unsigned)((cnt + 255) / 256), 256, 0, s>>>(
+                    G, RL + (size_t)t * p.plane, cnt, crt_modulus(t));
+                rc = record_cuda_error(cudaGetLastError(), "modular residues");
+            }
+        }
+    }
+    if (rc) return rc;
+    ozaki_phase(2, s);
+    scal<N> al{}, be{};
+    int flags = 3 | 4;  // bit 0: beta == 0, bit 1: alpha == 1, bit 2: lower triangle
+    for (int l = 0; l < N; ++l) {
+        al.v[l] = alpha[l];
+        be.v[l] = beta[l];
+        if (beta[l] != 0.0) flags &= ~1;
+        if (alpha[l] != (l == 0 ? 1.0 : 0.0)) flags &= ~2;
+    }
+    if (p.WP == 8) crt_accum<N, 8>(p, n, n, Rs, exps, exps, C, al, be, flags, s);
+    else if (p.WP == 10) crt_accum<N, 10>(p, n, n, Rs, exps, exps, C, al, be, flags, s);
+    else crt_accum<N, 12>(p, n, n, Rs, exps, exps, C, al, be, flags, s);
+    ozaki_phase(3, s);
+    return record_cuda_error(cudaGetLastError(), "modular gram accumulate");
+}
+
+// lower(C) = alpha op(A) op(A)^T + beta lower(C) through the modular route,
+// op(A) = A (trans = 0, A n x k) or A^T (trans = 1, A k x n); the strict
+// upper triangle of C is neither read nor written.
+int ozaki_crt_syrk(mflab_handle *hd, int N, int T, int trans, int64_t n, int64_t k, Mat A, Mat C,
+                   const double *alpha, const double *beta, cudaStream_t s, int *T_used) {
+    if (T < 0 || T > CRT_MAXT) return MFLAB_ERR_ARG;
+    const int64_t np = (n + 255) / 256 * 256;
+    if (np > 65535LL) return MFLAB_ERR_UNSUPPORTED;
+    CrtPlan p;
+    int rc = T > 0 ? crt_plan(N, n, n, k, T, 0, p) : MFLAB_OK;
+    if (rc) return rc;
+    int *exps = nullptr;
+    int g = 0;
+    rc = ozaki_gram_scales(hd, N, trans, n, k, A, s, T == 0, &g, &exps);
+    if (rc) return rc;
+    if (T == 0) {
+        rc = crt_plan(N, n, n, k, 0, g, p);
+        if (rc) return rc;
+    }
+    p.mp = p.np = np;  // square tile grid: the GEMM walks the lower-triangle tiles
+    crt_layout(p);
+    if ((int64_t)p.T * p.mp > 0x7fffffffLL) return MFLAB_ERR_UNSUPPORTED;
+    rc = mflab_reserve_scratch(hd, p.total);
+    if (rc) return rc;
+    if (T_used) *T_used = p.T;
+    switch (N) {
+    case 2: return crt_syrk_n<2>(hd, p, trans, n, k, A, C, alpha, beta, exps, s);
+    case 3: return crt_syrk_n<3>(hd, p, trans, n, k, A, C, alpha, beta, exps, s);
+    default: return crt_syrk_n<4>(hd, p, trans, n, k, A, C, alpha, beta, exps, s);
+    }
+}
+
 }  // namespace mfl
 
 // C = alpha*A*B + beta*C through the modular INT8 route; moduli = 0 lets the
@@ -754,6 +874,31 @@ extern "C" int mflab_gemm_ozaki_crt(mflab_handle *h, void *stream, int limbs, in
 }
 
 extern "C" int mflab_ozaki_last_moduli(mflab_handle *h) { return h ? h->last_moduli : 0; }
+
+// lower(C) = alpha * op(A) op(A)^T + beta * lower(C) through the modular
+// route: trans = 0, A n x k (the trailing-update form A A^T); trans = 1, A
+// k x n (the reference syrk! form P^T P).  moduli = 0: tuner.
+extern "C" int mflab_syrk_lower_ozaki(mflab_handle *h, void *stream, int limbs, int moduli,
+                                      int trans, int64_t n, int64_t k, const double *A,
+                                      int64_t lda, int64_t lsa, double *C, int64_t ldc,
+                                      int64_t lsc, const double *alpha, const double *beta) {
+    if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
+    if (n < 0 || k < 0 || !alpha || !beta || moduli < 0 || (trans != 0 && trans != 1))
+        return MFLAB_ERR_ARG;
+    if (n == 0) return MFLAB_OK;
+    const int64_t ar = trans ? k : n, ac = trans ? n : k;
+    if (lda < (ar > 0 ? ar : 1) || ldc < n) return MFLAB_ERR_ARG;
+    if (mfl::views_overlap(C, ldc, lsc, n, n, limbs, A, lda, lsa, ar, ac)) return MFLAB_ERR_ALIAS;
+    const mfl::Mat Am{(double *)A, lda, lsa}, Cm{C, ldc, lsc};
+    cudaStream_t s = (cudaStream_t)stream;
+    if (k == 0)  // C = beta C on the lower triangle
+        return mfl::launch_mm(limbs, trans ? 1 : 0, !trans, 1, false, n, n, 0, Am, Am, Cm, alpha,
+                              beta, s);
+    return mfl::ozaki_crt_syrk(h, limbs, moduli, trans, n, k, Am, Cm, alpha, beta, s,
+                               &h->last_moduli);
+}
+
+
 
 // Host-only planner of the modular route (no device work): for `limbs`, depth
 // k and either a modulus count (moduli > 0) or the tuner's sampled gap in
