@@ -382,10 +382,22 @@ def run_configs(R, torch):
         Sw = S.copy()
         t_f, F = _time_once(torch, lambda: mf.cholesky_(Sw))
         t_s, X = _time_once(torch, lambda: mf.solve(F, Bm))
+        # the wavefront ("fast") solve order, an option beside the matched one
+        t_sf, _ = _time_once(torch, lambda: mf.solve(F, Bm,
+                                                     config=mf.KernelConfig(solve_order="fast")))
         Rr = mf.MFMatrix.zeros(N, n, nrhs)
         mf.residual_(Rr, S, X, Bm, uplo="lower")
         be = mf.normwise_backward_error(S, X, Bm, Rr, uplo="lower")
         work = n ** 3 / 3.0 + 2.0 * n * n * nrhs
+        # the same factorization with INT8 (modular) trailing updates between
+        # 256-column panels; solved with the same matched-order solves
+        Sw2 = S.copy()
+        ocfg = mf.KernelConfig(gemm_strategy="ozaki", ozaki_scheme="modular", ozaki_block=256)
+        t_fo, Fo = _time_once(torch, lambda: mf.cholesky_(Sw2, config=ocfg))
+        Xo = mf.solve(Fo, Bm)
+        mf.residual_(Rr, S, Xo, Bm, uplo="lower")
+        beo = mf.normwise_backward_error(S, Xo, Bm, Rr, uplo="lower")
+        del Sw2, Fo, Xo
         # CPU: the oracle's blocked Cholesky at n=512 (scaled to a rate)
         rng = np.random.default_rng(3)
         nc = 512
@@ -394,10 +406,15 @@ def run_configs(R, torch):
         mfref.potrf(Sc, nthreads=threads)
         tc = time.perf_counter() - t0
         chol[f"x{N}"] = {"factor_ms": t_f * 1e3, "solve_ms": t_s * 1e3,
+                         "solve_fast_order_ms": t_sf * 1e3,
                          "md_gflops": work / (t_f + t_s) / 1e9,
                          "max_backward_error": float(max(v[0] for v in be)),
                          "cpu_oracle_md_gflops_n512": nc ** 3 / 3.0 / tc / 1e9,
-                         "cpu_threads": threads}
+                         "cpu_threads": threads,
+                         "int8_trailing": {"factor_ms": t_fo * 1e3,
+                                           "factor_speedup_vs_matched": t_f / t_fo,
+                                           "max_backward_error": float(max(v[0] for v in beo)),
+                                           "panel": 256}}
         del S, Sw, F, X, Rr, Rm, Rt, Bm
         torch.cuda.empty_cache()
     out["cholesky_n2048_rhs64"] = chol
