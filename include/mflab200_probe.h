@@ -38,7 +38,8 @@ int mflab_gemm_ozaki_crt_phases(struct mflab_handle *h, void *stream, int limbs,
 /* Host copy of the modular route's reconstruction (tests): for `count`
    problems of T int32 residue representatives each (G[e*T + t] ~ x mod p_t),
    the 12 little-endian 32-bit words of |x| (mag[e*12 ...]) and its sign
-   (neg[e]) for the unique x in [-P/2, P/2).  No device work. */
+   (neg[e]) for the x with |x| <= 3P/8 (the range the route's planner keeps
+   every level sum in).  No device work. */
 int mflab_ozaki_crt_reduce_host(int T, int count, const int32_t *G, uint32_t *mag, int *neg);
 
 /* Best device time (ms) of `reps` int8 x int8 -> int32 TN GEMMs of m x n x k

@@ -243,9 +243,13 @@ __global__ void __launch_bounds__(128)
 }
 
 // ------------------------------------------------------ reconstruction ----
-// X (WP words of 64-bit partial sums) -> the symmetric residue of X mod P as
-// magnitude words + sign (host and device: the host copy backs
-// mflab_ozaki_crt_reduce_host).  All products are 32 x 32 -> 64 bit.
+// X (WP words of 64-bit partial sums) -> G = X - round(X / P) P as magnitude
+// words + sign (host and device: the host copy backs
+// mflab_ozaki_crt_reduce_host).  Precondition, kept by the planner: the
+// represented value satisfies |G| <= 3P / 8 (it is G mod P in the symmetric
+// range), so X / P lies within 3/8 of the integer q = round(X / P) and the
+// double estimate of X / P (relative error < 2^-48) rounds to exactly q.
+// All products are 32 x 32 -> 64 bit.
 template <int WP>
 __host__ __device__ __forceinline__ bool crt_reduce(const uint64_t (&X)[WP], const CrtAccConst &c,
                                                     uint32_t (&mag)[WP]) {
@@ -257,13 +261,11 @@ __host__ __device__ __forceinline__ bool crt_reduce(const uint64_t (&X)[WP], con
         x[w] = (uint32_t)s;
         cy = s >> 32;
     }
-    // floor(X / P) or one off (X / P < 2^14: the rounding error of the
-    // double evaluation is far below one unit)
     double xd = 0.0;
 #pragma unroll
     for (int w = WP - 1; w >= 0; --w) xd = fma(xd, 4294967296.0, (double)x[w]);
-    const uint32_t q = (uint32_t)floor(xd * c.pinv);
-    // Y = X - q P (borrow chain; the final borrow is the sign of Y)
+    const uint32_t q = (uint32_t)floor(xd * c.pinv + 0.5);
+    // Y = X - q P (two's complement over WP words; the final borrow is the sign)
     uint32_t y[WP];
     uint64_t hi = 0;   // carry of q P
     uint32_t br = 0;   // borrow
@@ -275,43 +277,16 @@ __host__ __device__ __forceinline__ bool crt_reduce(const uint64_t (&X)[WP], con
         y[w] = (uint32_t)d;
         br = (uint32_t)(d >> 63);
     }
-    if (br) {  // q one too large: Y + P
-        uint32_t ca = 0;
-#pragma unroll
-        for (int w = 0; w < WP; ++w) {
-            const uint64_t t = (uint64_t)y[w] + c.P[w] + ca;
-            y[w] = (uint32_t)t;
-            ca = (uint32_t)(t >> 32);
-        }
-    } else {   // q one too small: Y - P when that is >= 0
-        uint32_t z[WP];
-        uint32_t b2 = 0;
-#pragma unroll
-        for (int w = 0; w < WP; ++w) {
-            const uint64_t d = (uint64_t)y[w] - c.P[w] - b2;
-            z[w] = (uint32_t)d;
-            b2 = (uint32_t)(d >> 63);
-        }
-        if (!b2) {
-#pragma unroll
-            for (int w = 0; w < WP; ++w) y[w] = z[w];
-        }
-    }
-    // Y in [0, P): Z = P - Y; the value is -Z when Y >= Z, else Y
-    uint32_t z[WP];
-    uint32_t b3 = 0, b4 = 0;
+    // |Y|: negate the words when Y < 0
+    const uint32_t flip = br ? 0xffffffffu : 0u;
+    uint32_t ca = br;
 #pragma unroll
     for (int w = 0; w < WP; ++w) {
-        const uint64_t d = (uint64_t)c.P[w] - y[w] - b3;
-        z[w] = (uint32_t)d;
-        b3 = (uint32_t)(d >> 63);
-        const uint64_t e = (uint64_t)y[w] - z[w] - b4;
-        b4 = (uint32_t)(e >> 63);
+        const uint64_t t = (uint64_t)(y[w] ^ flip) + ca;
+        mag[w] = (uint32_t)t;
+        ca = (uint32_t)(t >> 32);
     }
-    const bool neg = (b4 == 0);
-#pragma unroll
-    for (int w = 0; w < WP; ++w) mag[w] = neg ? z[w] : y[w];
-    return neg;
+    return br != 0;
 }
 
 // Float64xN value of a WP-word magnitude times 2^e2: the top 53 (N+1) bits as
@@ -919,8 +894,8 @@ extern "C" int mflab_ozaki_crt_plan(int limbs, int64_t k, int moduli, int gap8, 
 // Host copy of the reconstruction step for tests: for `count` problems, G
 // holds T int32 values per problem (any representatives of the residues
 // mod p_t, as the int8 GEMMs produce them); mag receives 12 little-endian
-// words of |x| and neg the sign of the unique x in [-P/2, P/2) with
-// x = G_t mod p_t for all t.
+// words of |x| and neg the sign of the x with |x| <= 3P/8 and x = G_t mod
+// p_t for all t (the range the planner guarantees for every level sum).
 extern "C" int mflab_ozaki_crt_reduce_host(int T, int count, const int32_t *G, uint32_t *mag,
                                            int *neg) {
     using namespace mfl;
