@@ -342,91 +342,60 @@ __device__ __forceinline__ mf<N> crt_words_to_mf(const uint32_t (&mag)[WP], int 
 // A block covers 128 rows of one column: the Q T residue segments of its rows
 // (128 bytes each, 128-byte aligned) are copied to shared memory with
 // cp.async in one round trip, then each thread reconstructs its entry.
-constexpr int CRT_ACC_THREADS = 128;
-constexpr int CRT_ACC_ROWS = 2 * CRT_ACC_THREADS;  // rows tid and tid + 128 per thread
+constexpr int CRT_ACC_ROWS = 128;
 
-// the value of one output (before the alpha/beta epilogue) from its Q T
-// staged residues, column stride CRT_ACC_ROWS bytes in shared memory
 template <int N, int WP>
-__device__ __forceinline__ mf<N> crt_value(const uint8_t *src, int T, int h, int sab,
-                                           const CrtAccConst &c) {
-    constexpr int Q = N == 2 ? 1 : 2;  // the planner's digit count for N limbs
-    mf<N> acc = from_double<N>(0.0);
-#pragma unroll
-    for (int L = Q - 1; L >= 0; --L) {
-        const uint8_t *sl = src + (size_t)L * T * CRT_ACC_ROWS;
-        uint64_t X[WP];
-#pragma unroll
-        for (int w = 0; w < WP; ++w) X[w] = 0;
-#pragma unroll
-        for (int t = 0; t < CRT_MAXT; ++t) {
-            if (t < T) {
-                const uint32_t r = sl[t * CRT_ACC_ROWS];
-#pragma unroll
-                for (int w = 0; w < WP; ++w) X[w] += (uint64_t)r * c.U[t][w];
-            }
-        }
-        uint32_t mag[WP];
-        const bool ng = crt_reduce<WP>(X, c, mag);
-        mf<N> g = crt_words_to_mf<N, WP>(mag, sab - 2 * Q * h + h * (2 * Q - 2 - L));
-        if (ng) g = neg(g);
-        acc = L == Q - 1 ? g : add(acc, g);
-    }
-    return acc;
-}
-
-// C = alpha * 2^(sa+sb-2Qh) sum_L 2^(h (2Q-2-L)) G_L (+ beta * C); R holds
-// the residues G_L mod p_t as bytes, plane (L T + t) at R + (L T + t) plane.
-// A block covers 256 rows of one column: the Q T residue segments of its rows
-// are copied to shared memory with cp.async in one round trip; each thread
-// then reconstructs two outputs (rows tid and tid + 128) as independent
-// chains and stores both at the end.
-template <int N, int WP>
-__global__ void __launch_bounds__(CRT_ACC_THREADS, 3)
+__global__ void __launch_bounds__(CRT_ACC_ROWS, 3)
     crt_accum_kernel(int64_t m, int64_t n, int Q, int h, int T, const uint8_t *R, int64_t ldi,
                      size_t plane, const int *rowexp, const int *colexp, Mat C, scal<N> alpha,
                      scal<N> beta, int flags, const __grid_constant__ CrtAccConst c) {
     __shared__ __align__(16) uint8_t sres[2 * CRT_MAXT][CRT_ACC_ROWS];
     const int tid = threadIdx.x;
-    const int64_t i0 = (int64_t)blockIdx.x * CRT_ACC_ROWS;
+    const int64_t i0 = (int64_t)blockIdx.x * CRT_ACC_ROWS, i = i0 + tid;
     const int64_t j = blockIdx.y;
     // flags bit 2: lower triangle only (the GEMM skipped the tiles above it)
     if ((flags & 4) && i0 + CRT_ACC_ROWS - 1 < j) return;
-    // rows i0 .. i0 + rows - 1 lie inside the padded planes (ldi = mp, a
-    // multiple of 128)
-    const int rows = ldi - i0 < CRT_ACC_ROWS ? (int)(ldi - i0) : CRT_ACC_ROWS;
-    const int per_plane = rows / 16;
-    const int segs = Q * T * per_plane;
-    for (int sg = tid; sg < segs; sg += CRT_ACC_THREADS) {
-        const int pl = sg / per_plane, part = sg % per_plane;
+    // rows i0 .. i0+127 lie inside the padded planes (ldi = mp, a multiple of 128)
+    const int segs = Q * T * (CRT_ACC_ROWS / 16);
+    for (int s = tid; s < segs; s += CRT_ACC_ROWS) {
+        const int pl = s / (CRT_ACC_ROWS / 16), part = s % (CRT_ACC_ROWS / 16);
         const uint8_t *g = R + (size_t)pl * plane + (size_t)j * ldi + i0 + part * 16;
         const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&sres[pl][part * 16]);
         asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(g) : "memory");
     }
     asm volatile("cp.async.wait_all;" ::: "memory");
     __syncthreads();
-    const int eb = colexp[j];
-    // both chains are evaluated without branches (rows past m reuse row
-    // m - 1's exponent and are not stored) so that they interleave
-    const int64_t ia = i0 + tid, ib = ia + CRT_ACC_THREADS;
-    const bool live[2] = {ia < m && !((flags & 4) && ia < j), ib < m && !((flags & 4) && ib < j)};
-    const int ea0 = rowexp[ia < m ? ia : m - 1], ea1 = rowexp[ib < m ? ib : m - 1];
-    mf<N> v[2];
-    v[0] = crt_value<N, WP>(&sres[0][tid], T, h, oz_scale_exp(ea0) + oz_scale_exp(eb), c);
-    v[1] = crt_value<N, WP>(&sres[0][tid + CRT_ACC_THREADS], T, h,
-                            oz_scale_exp(ea1) + oz_scale_exp(eb), c);
-    const mf<N> nan = from_double<N>(__longlong_as_double(0x7ff8000000000000LL));
-    if (ea0 == OZ_EXP_BAD || eb == OZ_EXP_BAD) v[0] = nan;
-    if (ea1 == OZ_EXP_BAD || eb == OZ_EXP_BAD) v[1] = nan;
+    if (i >= m || ((flags & 4) && i < j)) return;
+    const int ea = rowexp[i], eb = colexp[j];
+    mf<N> acc = from_double<N>(0.0);
+    if (ea == OZ_EXP_BAD || eb == OZ_EXP_BAD) {
+        acc = from_double<N>(__longlong_as_double(0x7ff8000000000000LL));
+    } else {
+        for (int L = Q - 1; L >= 0; --L) {
+            const uint8_t *src = &sres[L * T][tid];
+            uint64_t X[WP];
 #pragma unroll
-    for (int u = 0; u < 2; ++u) {
-        if (!live[u]) continue;
-        const int64_t i = i0 + tid + u * CRT_ACC_THREADS;
-        // flags bit 0: beta == 0 (C is not read); bit 1: alpha == 1
-        mf<N> r = (flags & 2) ? v[u] : mul(alpha.get(), v[u]);
-        if (!(flags & 1)) r = add(r, mul(beta.get(), load_mf<N>(C.p, C.ld, C.ls, i, j)));
-        store_mf<N>(C.p, C.ld, C.ls, i, j, r);
+            for (int w = 0; w < WP; ++w) X[w] = 0;
+#pragma unroll
+            for (int t = 0; t < CRT_MAXT; ++t) {
+                if (t < T) {
+                    const uint32_t r = src[t * CRT_ACC_ROWS];
+#pragma unroll
+                    for (int w = 0; w < WP; ++w) X[w] += (uint64_t)r * c.U[t][w];
+                }
+            }
+            uint32_t mag[WP];
+            const bool ng = crt_reduce<WP>(X, c, mag);
+            const int sh = oz_scale_exp(ea) + oz_scale_exp(eb) - 2 * Q * h + h * (2 * Q - 2 - L);
+            mf<N> g = crt_words_to_mf<N, WP>(mag, sh);
+            if (ng) g = neg(g);
+            acc = L == Q - 1 ? g : add(acc, g);
+        }
     }
+    // flags bit 0: beta == 0 (C is not read); bit 1: alpha == 1
+    mf<N> r = (flags & 2) ? acc : mul(alpha.get(), acc);
+    if (!(flags & 1)) r = add(r, mul(beta.get(), load_mf<N>(C.p, C.ld, C.ls, i, j)));
+    store_mf<N>(C.p, C.ld, C.ls, i, j, r);
 }
 
 // residues of int32 sums modulo p as bytes (library-engine path)
@@ -656,7 +625,7 @@ static void crt_accum(const CrtPlan &p, int64_t m, int64_t n, const uint8_t *I, 
                       const int *colexp, Mat C, const scal<N> &al, const scal<N> &be,
                       int flags, cudaStream_t s) {
     dim3 g((unsigned)((m + CRT_ACC_ROWS - 1) / CRT_ACC_ROWS), (unsigned)n);
-    crt_accum_kernel<N, WP><<<g, CRT_ACC_THREADS, 0, s>>>(m, n, p.Q, p.h, p.T, I, p.ldi, p.plane, rowexp,
+    crt_accum_kernel<N, WP><<<g, CRT_ACC_ROWS, 0, s>>>(m, n, p.Q, p.h, p.T, I, p.ldi, p.plane, rowexp,
                                               colexp, C, al, be, flags, crt_tables(p.T).acc);
 }
 
