@@ -235,6 +235,21 @@ int mflab_backward_error(mflab_handle *h, void *stream, int limbs, int uplo, int
                          int64_t ldx, int64_t lsx, const double *B, int64_t ldb, int64_t lsb,
                          const double *R, int64_t ldr, int64_t lsr, double *out);
 
+/* ||A||_inf (the matrix term of normwise_backward_error, residual.jl:178-200,
+   same row-sum order) into device buffers anorm[limbs] and *nonfinite (1 when
+   A holds a non-finite authoritative entry), for repeated backward errors
+   against one matrix. */
+int mflab_opnorm_inf(mflab_handle *h, void *stream, int limbs, int uplo, int64_t m, int64_t k,
+                     const double *A, int64_t lda, int64_t lsa, double *anorm, int *nonfinite);
+
+/* mflab_backward_error with ||A||_inf and its flag from mflab_opnorm_inf (A is
+   not read): the iterative-refinement form. */
+int mflab_backward_error_norm(mflab_handle *h, void *stream, int limbs, int64_t m, int64_t k,
+                              int64_t nrhs, const double *anorm, const int *nonfinite,
+                              const double *X, int64_t ldx, int64_t lsx, const double *B,
+                              int64_t ldb, int64_t lsb, const double *R, int64_t ldr, int64_t lsr,
+                              double *out);
+
 /* ----------------------------------------------------- factorizations --- */
 /* Blocked lower Cholesky in place (block <= 32 columns; the reference default
    is 16).  Only the lower triangle is read or written.  *info (device int):

@@ -31,7 +31,7 @@ from . import _native
 __all__ = [
     "MFMatrix", "KernelConfig", "DimensionMismatch", "ArgumentError", "DomainError",
     "PosDefException", "SingularException", "MFLABError",
-    "gemm_", "syrk_", "gemmt_", "trsm_", "trsv_", "gemm_plan",
+    "gemm_", "syrk_", "gemmt_", "trsm_", "trsv_", "gemm_plan", "OpNormInf",
     "cholesky_", "lu_", "ldiv_", "solve", "issuccess",
     "factor_status", "factor_state", "factor_kind", "factor_matrix", "factor_precision",
     "factor_provider", "factor_pivots", "factor_diagnostics",
@@ -1023,17 +1023,43 @@ def residual_mixed_(R: MFMatrix, A: MFMatrix, X: MFMatrix, B: MFMatrix, uplo: st
     return R
 
 
+class OpNormInf:
+    """||A||_inf of one matrix on its device (the matrix term of the normwise
+    backward error), for repeated backward errors against it."""
+
+    def __init__(self, A: MFMatrix, uplo: str = "general"):
+        N = _same_type(A)
+        if uplo not in _UPLO_R:
+            raise ArgumentError("uplo must be :general, :L or :U")
+        self.N, self.m, self.k = N, A.m, A.n
+        self.value = torch.zeros(N, dtype=torch.float64, device=A.storage.device)
+        self.nonfinite = torch.zeros(1, dtype=torch.int32, device=A.storage.device)
+        lib, h, s = _lib_h(A)
+        _check(lib.mflab_opnorm_inf(h, s, N, _UPLO_R[uplo], A.m, A.n, A.ptr(), A.ld, A.ls,
+                                    self.value.data_ptr(), self.nonfinite.data_ptr()),
+               "opnorm")
+
+
 def normwise_backward_error(A: MFMatrix, X: MFMatrix, B: MFMatrix, R: MFMatrix,
-                            uplo: str = "general"):
+                            uplo: str = "general", anorm: Optional[OpNormInf] = None):
     """||r|| / (||A|| ||x|| + ||b||) (src/residual.jl:202-269): one N-limb value
-    for a vector, a list of them for a matrix right-hand side."""
+    for a vector, a list of them for a matrix right-hand side.  `anorm`
+    (an OpNormInf of A) skips the pass over A."""
     N = _same_type(A, X, B, R)
     _check_residual_dims(R, A, X, B, uplo)
     out = torch.zeros(max(R.n, 1) * N, dtype=torch.float64, device=A.storage.device)
     lib, h, s = _lib_h(A)
-    _check(lib.mflab_backward_error(h, s, N, _UPLO_R[uplo], A.m, A.n, R.n, A.ptr(), A.ld, A.ls,
-                                    X.ptr(), X.ld, X.ls, B.ptr(), B.ld, B.ls, R.ptr(), R.ld, R.ls,
-                                    out.data_ptr()), "normwise_backward_error")
+    if anorm is not None:
+        if (anorm.N, anorm.m, anorm.k) != (N, A.m, A.n):
+            raise DimensionMismatch("normwise_backward_error: anorm belongs to another matrix")
+        _check(lib.mflab_backward_error_norm(h, s, N, A.m, A.n, R.n, anorm.value.data_ptr(),
+                                             anorm.nonfinite.data_ptr(), X.ptr(), X.ld, X.ls,
+                                             B.ptr(), B.ld, B.ls, R.ptr(), R.ld, R.ls,
+                                             out.data_ptr()), "normwise_backward_error")
+    else:
+        _check(lib.mflab_backward_error(h, s, N, _UPLO_R[uplo], A.m, A.n, R.n, A.ptr(), A.ld,
+                                        A.ls, X.ptr(), X.ld, X.ls, B.ptr(), B.ld, B.ls, R.ptr(),
+                                        R.ld, R.ls, out.data_ptr()), "normwise_backward_error")
     vals = out.cpu().numpy().reshape(-1, N)[:R.n]
     return vals[0].copy() if R.is_vector else [v.copy() for v in vals]
 
@@ -1061,17 +1087,22 @@ def _leading_limb(X: MFMatrix) -> MFMatrix:
 
 
 def solve_mixed_lu(A: MFMatrix, B: MFMatrix, tol: float = 0.0, maxiter: int = 40,
-                   config: KernelConfig = _DEFAULT) -> tuple:
+                   config: KernelConfig = _DEFAULT, residual: str = "int8") -> tuple:
     """Solve A X = B for a Float64xN matrix A with a binary64 partial-pivoting
     LU of round(A) and iterative refinement with Float64xN residuals.
 
     Each iteration: D = LU64 \\ round(R) in binary64 (getrs), X += D in
-    Float64xN, R = B - A X with residual!, then the normwise backward error of
-    every column.  Stops when all backward errors are <= tol (default
-    2^(-53N)) or after maxiter iterations.  Returns (X, report).  The
-    reference provides the pieces (lu!, residual!, refinement_correction!) but
-    leaves the refinement loop to the caller (docs/SOLVER_BACKEND_CONTRACT.md).
+    Float64xN, R = B - A X in Float64xN, then the normwise backward error of
+    every column (||A||_inf computed once).  The residual goes through the
+    INT8 modular GEMM (residual="int8", error at the Float64xN level of the
+    plain kernel) or residual! in the reference order (residual="matched").
+    Stops when all backward errors are <= tol (default 2^(-53N)) or after
+    maxiter iterations.  Returns (X, report).  The reference provides the
+    pieces (lu!, residual!, refinement_correction!) but leaves the refinement
+    loop to the caller.
     """
+    if residual not in ("int8", "matched"):
+        raise ArgumentError("residual must be :int8 or :matched")
     N = _same_type(A, B)
     n = A.m
     if A.n != n:
@@ -1093,6 +1124,9 @@ def solve_mixed_lu(A: MFMatrix, B: MFMatrix, tol: float = 0.0, maxiter: int = 40
         raise SingularException(st)
     X = MFMatrix.zeros(N, n, None if B.is_vector else B.n, device=dev)
     R = B.copy()
+    anorm = OpNormInf(A)
+    rcfg = dataclasses.replace(config, gemm_strategy="ozaki", ozaki_scheme="modular",
+                               ozaki_slices=0)
     history = []
     it = 0
     for it in range(1, maxiter + 1):
@@ -1101,15 +1135,21 @@ def solve_mixed_lu(A: MFMatrix, B: MFMatrix, tol: float = 0.0, maxiter: int = 40
                                D.ld, D.ls), "ldiv! (binary64)")
         _check(lib.mflab_add_widened(h, s, 1, N, n, X.n, D.ptr(), D.ld, D.ls, X.ptr(), X.ld,
                                      X.ls), "refinement update")
-        residual_(R, A, X, B)
-        be = normwise_backward_error(A, X, B, R)
+        if residual == "int8":
+            R.copy_(B)
+            gemm_(R, A, X, -1.0, 1.0, config=rcfg)
+        else:
+            residual_(R, A, X, B)
+        be = normwise_backward_error(A, X, B, R, anorm=anorm)
         worst = float(np.max([v[0] for v in (be if isinstance(be, list) else [be])]))
         history.append(worst)
         if worst <= tol:
             break
     report = {"iterations": it, "backward_error": history[-1] if history else None,
               "history": history, "converged": bool(history) and history[-1] <= tol,
-              "factor": "binary64 partial-pivoting LU", "residual": limb_type_name(N)}
+              "factor": "binary64 partial-pivoting LU",
+              "residual": limb_type_name(N) + (" (INT8 modular GEMM)" if residual == "int8"
+                                               else " (reference order)")}
     return X, report
 
 

@@ -99,6 +99,9 @@ SIGNATURES = {
     "mflab_syrk_lower_ozaki": [_vp, _vp, _int, _int, _int, _i64, _i64, _vp, _i64, _i64, _vp, _i64,
                                _i64, _d, _d],
     "mflab_potrf_ozaki": [_vp, _vp, _int, _int, _i64, _vp, _i64, _i64, _i64, _i64, _vp],
+    "mflab_opnorm_inf": [_vp, _vp, _int, _int, _i64, _i64, _vp, _i64, _i64, _vp, _vp],
+    "mflab_backward_error_norm": [_vp, _vp, _int, _i64, _i64, _i64, _vp, _vp, _vp, _i64, _i64,
+                                  _vp, _i64, _i64, _vp, _i64, _i64, _vp],
     "mflab_ozaki_crt_plan": [_int, _i64, _int, _int, C.POINTER(_int), C.POINTER(_int),
                              C.POINTER(_int)],
     "mflab_ozaki_crt_modulus": [_int],

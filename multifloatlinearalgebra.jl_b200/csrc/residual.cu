@@ -314,6 +314,72 @@ extern "C" int mflab_backward_error(mflab_handle *h, void *stream, int limbs, in
     return mfl::record_cuda_error(cudaGetLastError(), "backward error");
 }
 
+// ||A||_inf alone (the matrix term of the backward error, residual.jl:178-200)
+// into the caller's device buffers: anorm[limbs] and *nonfinite (0 / 1), for
+// repeated backward errors against one matrix (iterative refinement).
+extern "C" int mflab_opnorm_inf(mflab_handle *h, void *stream, int limbs, int uplo, int64_t m,
+                                int64_t k, const double *A, int64_t lda, int64_t lsa,
+                                double *anorm, int *nonfinite) {
+    if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
+    if (uplo < 0 || uplo > 2 || m < 0 || k < 0 || !anorm || !nonfinite) return MFLAB_ERR_ARG;
+    if (uplo != 0 && m != k) return MFLAB_ERR_ARG;
+    const size_t need = sizeof(double) * (size_t)limbs * (size_t)(m + 8) + 64;
+    int rc = mflab_reserve_scratch(h, need);
+    if (rc) return rc;
+    double *rowsum = (double *)h->scratch;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = cudaMemsetAsync(nonfinite, 0, sizeof(int), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(anorm, 0, sizeof(double) * limbs, s);
+    if (e != cudaSuccess) return mfl::record_cuda_error(e, "opnorm init");
+    if (m == 0) return MFLAB_OK;
+    mfl::Mat a{(double *)A, lda, lsa};
+    const unsigned gm = (unsigned)((m + 127) / 128);
+    switch (limbs) {
+    case 2:
+        mfl::abs_row_sum_kernel<2><<<gm, 128, 0, s>>>(m, k, a, uplo, rowsum, nonfinite);
+        mfl::max_rowsum_kernel<2, 256><<<1, 256, 0, s>>>(m, rowsum, anorm);
+        break;
+    case 3:
+        mfl::abs_row_sum_kernel<3><<<gm, 128, 0, s>>>(m, k, a, uplo, rowsum, nonfinite);
+        mfl::max_rowsum_kernel<3, 256><<<1, 256, 0, s>>>(m, rowsum, anorm);
+        break;
+    default:
+        mfl::abs_row_sum_kernel<4><<<gm, 128, 0, s>>>(m, k, a, uplo, rowsum, nonfinite);
+        mfl::max_rowsum_kernel<4, 256><<<1, 256, 0, s>>>(m, rowsum, anorm);
+        break;
+    }
+    return mfl::record_cuda_error(cudaGetLastError(), "opnorm");
+}
+
+// the backward errors of mflab_backward_error with ||A||_inf and its
+// finiteness flag from mflab_opnorm_inf (the matrix is not read)
+extern "C" int mflab_backward_error_norm(mflab_handle *h, void *stream, int limbs, int64_t m,
+                                         int64_t k, int64_t nrhs, const double *anorm,
+                                         const int *nonfinite, const double *X, int64_t ldx,
+                                         int64_t lsx, const double *B, int64_t ldb, int64_t lsb,
+                                         const double *R, int64_t ldr, int64_t lsr, double *out) {
+    if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
+    if (m < 0 || k < 0 || nrhs < 0 || !out || !anorm || !nonfinite) return MFLAB_ERR_ARG;
+    if (nrhs == 0) return MFLAB_OK;
+    mfl::Mat x{(double *)X, ldx, lsx}, b{(double *)B, ldb, lsb}, r{(double *)R, ldr, lsr};
+    cudaStream_t s = (cudaStream_t)stream;
+    switch (limbs) {
+    case 2:
+        mfl::backward_error_kernel<2, 256><<<(unsigned)nrhs, 256, 0, s>>>(m, k, x, b, r, anorm,
+                                                                         nonfinite, out);
+        break;
+    case 3:
+        mfl::backward_error_kernel<3, 256><<<(unsigned)nrhs, 256, 0, s>>>(m, k, x, b, r, anorm,
+                                                                         nonfinite, out);
+        break;
+    default:
+        mfl::backward_error_kernel<4, 256><<<(unsigned)nrhs, 256, 0, s>>>(m, k, x, b, r, anorm,
+                                                                         nonfinite, out);
+        break;
+    }
+    return mfl::record_cuda_error(cudaGetLastError(), "backward error (given norm)");
+}
+
 namespace mfl {
 // X <- X + widen(D): the correction step of iterative refinement
 template <int NS, int NR>

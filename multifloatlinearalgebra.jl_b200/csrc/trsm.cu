@@ -166,6 +166,61 @@ __global__ void trsm_right_thread(int64_t m, int64_t n, Mat A, Mat B, bool eff_l
     }
 }
 
+// Binary64 diagonal-block solve of the blocked left solve below: one CTA
+// per right-hand-side column, the jb x jb block (jb <= 64) in shared memory,
+// row t of the column in thread t.
+constexpr int TRSM64_NB = 64;
+
+__global__ void __launch_bounds__(TRSM64_NB)
+    trsm64_diag_kernel(int64_t jb, Mat A, Mat B, bool lower, bool unit) {
+    __shared__ double a[TRSM64_NB][TRSM64_NB + 1];
+    __shared__ double xk;
+    const int t = threadIdx.x;
+    const int64_t col = blockIdx.x;
+    for (int c = 0; c < jb; ++c)
+        if (t < jb) a[t][c] = A.p[(int64_t)c * A.ld + t];
+    double v = t < jb ? B.p[col * B.ld + t] : 0.0;
+    __syncthreads();
+    for (int s = 0; s < jb; ++s) {
+        const int k = lower ? s : (int)jb - 1 - s;
+        if (t == k) {
+            if (!unit) v = __ddiv_rn(v, a[k][k]);
+            xk = v;
+        }
+        __syncthreads();
+        if (t < jb && (lower ? t > k : t < k)) v = __dsub_rn(v, __dmul_rn(a[t][k], xk));
+        __syncthreads();
+    }
+    if (t < jb) B.p[col * B.ld + t] = v;
+}
+
+// Blocked left solve op(A) X = B for binary64 (no reference order to keep):
+// 64 x 64 diagonal blocks solved from shared memory, the rows below (forward)
+// or above (backward) updated with the FP64 GEMM kernel.  A not transposed.
+static int trsm64_blocked(int64_t m, int64_t n, Mat A, Mat B, bool lower, bool unit,
+                          cudaStream_t s, const int *info) {
+    const double mone[1] = {-1.0}, one[1] = {1.0};
+    const int64_t nblk = (m + TRSM64_NB - 1) / TRSM64_NB;
+    for (int64_t bi = 0; bi < nblk; ++bi) {
+        const int64_t blk = lower ? bi : nblk - 1 - bi;
+        const int64_t j0 = blk * TRSM64_NB;
+        const int64_t jb = m - j0 < TRSM64_NB ? m - j0 : TRSM64_NB;
+        trsm64_diag_kernel<<<(unsigned)n, TRSM64_NB, 0, s>>>(jb, A.at(j0, j0), B.at(j0, 0), lower,
+                                                             unit);
+        int rc = record_cuda_error(cudaGetLastError(), "trsm64 diagonal");
+        if (rc) return rc;
+        if (lower && j0 + jb < m) {
+            rc = launch_mm(1, false, false, 0, false, m - j0 - jb, n, jb, A.at(j0 + jb, j0),
+                           B.at(j0, 0), B.at(j0 + jb, 0), mone, one, s, info);
+        } else if (!lower && j0 > 0) {
+            rc = launch_mm(1, false, false, 0, false, j0, n, jb, A.at(0, j0), B.at(j0, 0),
+                           B.at(0, 0), mone, one, s, info);
+        }
+        if (rc) return rc;
+    }
+    return MFLAB_OK;
+}
+
 template <int N>
 static int run_trsm(int side, int uplo, int trans, int diag, int64_t m, int64_t n, Mat A, Mat B,
                     const double *alpha, cudaStream_t s, const int *info, int order) {
@@ -199,6 +254,8 @@ static int run_trsm(int side, int uplo, int trans, int diag, int64_t m, int64_t 
     // the fast order applies every term as soon as its unknown is final, in both
     // directions (deterministic, not the reference's association)
     const bool wavefront_ok = eff_lower || N == 1 || order == MFLAB_ORDER_FAST;
+    if (N == 1 && !transposed && m > 2 * TRSM64_NB && n <= 65535 && !info)
+        return trsm64_blocked(m, n, A, B, eff_lower, unit, s, info);
     if (!eff_lower && !wavefront_ok && m > 64 && n < 4096 && (size_t)m * N * 8 <= 200 * 1024) {
         const size_t smem = (size_t)m * N * sizeof(double);
         static bool configured = false;

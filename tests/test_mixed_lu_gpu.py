@@ -49,3 +49,51 @@ def test_binary64_lu_factor(mf, rng):
     for k, p in enumerate(ipiv.cpu().numpy()):
         PA[[k, p - 1]] = PA[[p - 1, k]]
     assert np.max(np.abs(PA - L @ U)) <= 1e-12 * np.max(np.abs(A)) * n
+
+
+@pytest.mark.parametrize("n,nrhs", [(129, 3), (300, 16), (1000, 5)])
+def test_binary64_getrs_blocked(mf, rng, n, nrhs):
+    """limbs = 1 solve (blocked 64 x 64 diagonal solves + FP64 GEMM updates):
+    P A X = B to binary64 backward accuracy"""
+    A = rng.standard_normal((n, n)) + n ** 0.5 * np.eye(n)
+    B = rng.standard_normal((n, nrhs))
+    Ad = mf.MFMatrix(torch.tensor(A.T.copy()[None], device="cuda"))
+    Bd = mf.MFMatrix(torch.tensor(B.T.copy()[None], device="cuda"))
+    lib, h, s = mf._lib_h(Ad)
+    ipiv = torch.arange(1, n + 1, dtype=torch.int64, device="cuda")
+    info = torch.zeros(1, dtype=torch.int32, device="cuda")
+    assert lib.mflab_getrf(h, s, 1, n, n, Ad.ptr(), Ad.ld, Ad.ls, ipiv.data_ptr(), 16,
+                           info.data_ptr()) == 0
+    assert lib.mflab_getrs(h, s, 1, n, nrhs, Ad.ptr(), Ad.ld, Ad.ls, ipiv.data_ptr(), Bd.ptr(),
+                           Bd.ld, Bd.ls) == 0
+    X = Bd.storage[0].cpu().numpy().T
+    r = B - A @ X
+    be = np.max(np.abs(r)) / (np.max(np.sum(np.abs(A), 1)) * np.max(np.abs(X)) + np.max(np.abs(B)))
+    assert be <= 64 * n * 2.0 ** -53, be
+
+
+@pytest.mark.parametrize("N", [2, 4])
+def test_mixed_lu_residual_routes(mf, ref, rng, N):
+    """the INT8 residual and the reference-order residual both refine to the
+    Float64xN backward error"""
+    n = 200
+    A = syn.randn_mf(rng, N, n, n)
+    B = syn.randn_mf(rng, N, n, 4)
+    for route in ("int8", "matched"):
+        X, rep = mf.solve_mixed_lu(mf.MFMatrix.from_numpy(A), mf.MFMatrix.from_numpy(B),
+                                   residual=route)
+        assert rep["converged"], (route, rep)
+        be = ref.backward_error(A, X.to_numpy(), B)
+        assert np.all(be <= 4 * 2.0 ** (-53 * N)), (route, be)
+
+
+@pytest.mark.parametrize("N", [2, 3, 4])
+def test_backward_error_with_cached_norm(mf, rng, N):
+    """normwise_backward_error with an OpNormInf equals the one-call form bit for bit"""
+    n, k = 120, 6
+    A, X, B, R = (syn.randn_mf(rng, N, n, n), syn.randn_mf(rng, N, n, k),
+                  syn.randn_mf(rng, N, n, k), syn.randn_mf(rng, N, n, k))
+    Ad, Xd, Bd, Rd = (mf.MFMatrix.from_numpy(v) for v in (A, X, B, R))
+    a = mf.normwise_backward_error(Ad, Xd, Bd, Rd)
+    b = mf.normwise_backward_error(Ad, Xd, Bd, Rd, anorm=mf.OpNormInf(Ad))
+    assert np.array_equal(np.array(a).view(np.uint64), np.array(b).view(np.uint64))
