@@ -254,6 +254,154 @@ __global__ void lu_rank1_kernel(int64_t m, Mat A, int64_t k, int64_t last, const
     }
 }
 
+// ------------------------------------------------- binary64 LU (fast) ---
+// The binary64 instance (the factor of the mixed-precision solver) has no
+// reference order to keep; it is factored LAPACK-style: one CTA factors a
+// panel of w <= 32 columns with partial pivoting, exchanging rows inside the
+// panel only; one kernel then applies the panel's interchanges to the other
+// columns, and the U block row and the trailing matrix are updated with the
+// TRSM and FP64 GEMM kernels.
+constexpr int LU64_NT = 1024;
+
+__global__ void __launch_bounds__(LU64_NT)
+    lu64_panel_kernel(int64_t m, Mat A, int64_t k0, int w, int64_t *ipiv, int *info) {
+    if (*info) return;
+    __shared__ double sv[LU64_NT / 32];
+    __shared__ int64_t si[LU64_NT / 32];
+    __shared__ int64_t spiv;
+    __shared__ double sinv;
+    const int t = threadIdx.x, lane = t % 32, wid = t / 32;
+    double *a = A.p;
+    const int64_t ld = A.ld;
+    for (int c = 0; c < w; ++c) {
+        const int64_t k = k0 + c;
+        // pivot: the first row of largest |A[r, k]|, r >= k
+        double best = -1.0;
+        int64_t bi = -1;
+        for (int64_t r = k + t; r < m; r += LU64_NT) {
+            const double v = fabs(a[k * ld + r]);
+            if (v > best) {
+                best = v;
+                bi = r;
+            }
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            const double ov = __shfl_xor_sync(0xffffffffu, best, off);
+            const int64_t oi = __shfl_xor_sync(0xffffffffu, bi, off);
+            if (oi >= 0 && (bi < 0 || ov > best || (ov == best && oi < bi))) {
+                best = ov;
+                bi = oi;
+            }
+        }
+        if (lane == 0) {
+            sv[wid] = best;
+            si[wid] = bi;
+        }
+        __syncthreads();
+        if (wid == 0) {
+            best = lane < LU64_NT / 32 ? sv[lane] : -1.0;
+            bi = lane < LU64_NT / 32 ? si[lane] : -1;
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                const double ov = __shfl_xor_sync(0xffffffffu, best, off);
+                const int64_t oi = __shfl_xor_sync(0xffffffffu, bi, off);
+                if (oi >= 0 && (bi < 0 || ov > best || (ov == best && oi < bi))) {
+                    best = ov;
+                    bi = oi;
+                }
+            }
+            if (lane == 0) {
+                spiv = bi;
+                ipiv[k] = bi + 1;
+            }
+        }
+        __syncthreads();
+        const int64_t p = spiv;
+        if (p != k && t < w) {  // exchange rows k and p inside the panel
+            const double tmp = a[(k0 + t) * ld + k];
+            a[(k0 + t) * ld + k] = a[(k0 + t) * ld + p];
+            a[(k0 + t) * ld + p] = tmp;
+        }
+        __syncthreads();
+        if (t == 0) {
+            const double akk = a[k * ld + k];
+            if (akk == 0.0) *info = (int)(k + 1);
+            sinv = 1.0 / akk;
+        }
+        __syncthreads();
+        if (*info) return;
+        const double iv = sinv;
+        for (int64_t r = k + 1 + t; r < m; r += LU64_NT) a[k * ld + r] *= iv;
+        __syncthreads();
+        // rank-1 update of the panel columns right of k
+        const int rest = w - 1 - c;
+        if (rest > 0) {
+            const int64_t rows = m - k - 1;
+            for (int64_t e = t; e < rows * rest; e += LU64_NT) {
+                const int64_t r = k + 1 + e % rows, cc = k + 1 + e / rows;
+                a[cc * ld + r] -= a[k * ld + r] * a[cc * ld + k];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// the interchanges ipiv[k0 .. k0+w) (1-based) applied, in ascending order, to
+// the columns outside the panel [k0, k0+w): one thread per column
+__global__ void lu64_swap_kernel(int64_t n, Mat A, int64_t k0, int w, const int64_t *ipiv,
+                                 const int *info) {
+    if (*info) return;
+    int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n - w) return;
+    if (c >= k0) c += w;
+    double *col = A.p + c * A.ld;
+    for (int i = 0; i < w; ++i) {
+        const int64_t k = k0 + i, p = ipiv[k] - 1;
+        if (p != k) {
+            const double tmp = col[k];
+            col[k] = col[p];
+            col[p] = tmp;
+        }
+    }
+}
+
+static int getrf64_fast(int64_t m, int64_t n, Mat A, int64_t *ipiv, int *info, cudaStream_t s) {
+    const double mone[1] = {-1.0}, one[1] = {1.0};
+    cudaError_t e = cudaMemsetAsync(info, 0, sizeof(int), s);
+    if (e != cudaSuccess) return record_cuda_error(e, "getrf info");
+    const int64_t kmax = m < n ? m : n;
+    if (kmax == 0) return MFLAB_OK;
+    int64_t tot = m * n;
+    nonfinite_kernel<1><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(m, n, A, 0, info);
+    int rc = record_cuda_error(cudaGetLastError(), "getrf check");
+    if (rc) return rc;
+    const int NB = 32;
+    for (int64_t k0 = 0; k0 < kmax; k0 += NB) {
+        const int w = (int)(kmax - k0 < NB ? kmax - k0 : NB);
+        lu64_panel_kernel<<<1, LU64_NT, 0, s>>>(m, A, k0, w, ipiv, info);
+        if (n > w)
+            lu64_swap_kernel<<<(unsigned)((n - w + 255) / 256), 256, 0, s>>>(n, A, k0, w, ipiv,
+                                                                           info);
+        rc = record_cuda_error(cudaGetLastError(), "getrf64 panel");
+        if (rc) return rc;
+        const int64_t last = k0 + w - 1;
+        if (last < n - 1) {
+            const int64_t rest = n - 1 - last;
+            rc = launch_trsm_info(1, 0, 0, 0, 1, w, rest, A.at(k0, k0), A.at(k0, last + 1), one, s,
+                                  info);
+            if (rc) return rc;
+            if (last < m - 1) {
+                rc = launch_mm(1, false, false, 0, false, m - 1 - last, rest, w,
+                               A.at(last + 1, k0), A.at(k0, last + 1), A.at(last + 1, last + 1),
+                               mone, one, s, info);
+                if (rc) return rc;
+            }
+        }
+    }
+    return MFLAB_OK;
+}
+
 template <int N>
 static int getrf_n(int64_t m, int64_t n, Mat A, int64_t *ipiv, int64_t block, int *info,
                    cudaStream_t s) {
@@ -504,7 +652,7 @@ extern "C" int mflab_getrf(mflab_handle *h, void *stream, int limbs, int64_t m, 
         if (rc) return rc;
     }
     switch (limbs) {
-    case 1: return mfl::getrf_n<1>(m, n, a, ipiv, block, info, s);
+    case 1: return mfl::getrf64_fast(m, n, a, ipiv, info, s);
     case 2: return mfl::getrf_n<2>(m, n, a, ipiv, block, info, s);
     case 3: return mfl::getrf_n<3>(m, n, a, ipiv, block, info, s);
     default: return mfl::getrf_n<4>(m, n, a, ipiv, block, info, s);

@@ -97,3 +97,31 @@ def test_backward_error_with_cached_norm(mf, rng, N):
     a = mf.normwise_backward_error(Ad, Xd, Bd, Rd)
     b = mf.normwise_backward_error(Ad, Xd, Bd, Rd, anorm=mf.OpNormInf(Ad))
     assert np.array_equal(np.array(a).view(np.uint64), np.array(b).view(np.uint64))
+
+
+@pytest.mark.parametrize("m,n", [(300, 300), (257, 130), (130, 257)])
+def test_binary64_lu_panels(mf, rng, m, n):
+    """the 32-column panel binary64 LU: P A = L U for square and rectangular
+    shapes, and a zero column reported at its index"""
+    A = rng.standard_normal((m, n))
+    Ad = mf.MFMatrix(torch.tensor(A.T.copy()[None], device="cuda"))
+    lib, h, s = mf._lib_h(Ad)
+    kmax = min(m, n)
+    ipiv = torch.arange(1, kmax + 1, dtype=torch.int64, device="cuda")
+    info = torch.zeros(1, dtype=torch.int32, device="cuda")
+    assert lib.mflab_getrf(h, s, 1, m, n, Ad.ptr(), Ad.ld, Ad.ls, ipiv.data_ptr(), 16,
+                           info.data_ptr()) == 0
+    assert int(info.item()) == 0
+    LU = Ad.storage[0].cpu().numpy().T
+    L = np.tril(LU, -1)[:, :kmax] + np.eye(m, kmax)
+    U = np.triu(LU)[:kmax, :]
+    PA = A.copy()
+    for k, p in enumerate(ipiv.cpu().numpy()):
+        PA[[k, p - 1]] = PA[[p - 1, k]]
+    assert np.max(np.abs(PA - L @ U)) <= 1e-12 * np.max(np.abs(A)) * max(m, n)
+    Z = A.copy()
+    Z[:, 57] = 0.0
+    Zd = mf.MFMatrix(torch.tensor(Z.T.copy()[None], device="cuda"))
+    assert lib.mflab_getrf(h, s, 1, m, n, Zd.ptr(), Zd.ld, Zd.ls, ipiv.data_ptr(), 16,
+                           info.data_ptr()) == 0
+    assert int(info.item()) == 58
