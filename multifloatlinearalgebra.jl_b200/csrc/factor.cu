@@ -270,6 +270,7 @@ __global__ void __launch_bounds__(LU64_NT)
     __shared__ int64_t si[LU64_NT / 32];
     __shared__ int64_t spiv;
     __shared__ double sinv;
+    __shared__ double su[32];
     const int t = threadIdx.x, lane = t % 32, wid = t / 32;
     double *a = A.p;
     const int64_t ld = A.ld;
@@ -332,15 +333,19 @@ __global__ void __launch_bounds__(LU64_NT)
         __syncthreads();
         if (*info) return;
         const double iv = sinv;
-        for (int64_t r = k + 1 + t; r < m; r += LU64_NT) a[k * ld + r] *= iv;
-        __syncthreads();
-        // rank-1 update of the panel columns right of k
+        // U row k of the panel in shared memory, then per row: scale the
+        // multiplier and update the panel columns right of k (independent
+        // loads along the row, so they are in flight together)
         const int rest = w - 1 - c;
-        if (rest > 0) {
-            const int64_t rows = m - k - 1;
-            for (int64_t e = t; e < rows * rest; e += LU64_NT) {
-                const int64_t r = k + 1 + e % rows, cc = k + 1 + e / rows;
-                a[cc * ld + r] -= a[k * ld + r] * a[cc * ld + k];
+        if (t < rest) su[t] = a[(k + 1 + t) * ld + k];
+        __syncthreads();
+        for (int64_t r = k + 1 + t; r < m; r += LU64_NT) {
+            const double l = a[k * ld + r] * iv;
+            a[k * ld + r] = l;
+#pragma unroll 8
+            for (int j = 0; j < rest; ++j) {
+                double *x = a + (k + 1 + j) * ld + r;
+                *x -= l * su[j];
             }
         }
         __syncthreads();
