@@ -149,6 +149,16 @@ int mflab_syrk_lower_ozaki(mflab_handle *h, void *stream, int limbs, int moduli,
 int mflab_potrf_ozaki(mflab_handle *h, void *stream, int limbs, int moduli, int64_t n, double *A,
                       int64_t lda, int64_t lsa, int64_t nb, int64_t block, int *info);
 
+/* Blocked partial-pivoting LU with INT8 trailing updates: panels of nb
+   columns are factored as in mflab_getrf (inner block `block`, reference
+   order and full-row interchanges inside the panel, lu.jl:34-195), then U12
+   by TRSM and A22 -= L21 U12 through mflab_gemm_ozaki_crt (moduli = 0: tuned
+   per update).  ipiv and *info as mflab_getrf; the device info word is read
+   after every panel (one synchronisation per panel). */
+int mflab_getrf_ozaki(mflab_handle *h, void *stream, int limbs, int moduli, int64_t m, int64_t n,
+                      double *A, int64_t lda, int64_t lsa, int64_t *ipiv, int64_t nb,
+                      int64_t block, int *info);
+
 /* modulus count used by the last mflab_gemm_ozaki_crt on this handle (no
    reference counterpart). */
 int mflab_ozaki_last_moduli(mflab_handle *h);

@@ -654,8 +654,19 @@ def lu_(A: MFMatrix, check: bool = True, config: KernelConfig = _DEFAULT,
     if m > 0 and n > 0:
         _check(lib.mflab_max_abs(h, s, N, m, n, A.ptr(), A.ld, A.ls, 0, omax.data_ptr()), "lu!")
     block = max(config.lu_block, 1)
-    _check(lib.mflab_getrf(h, s, N, m, n, A.ptr(), A.ld, A.ls,
-                           ipiv.data_ptr() if kmax > 0 else None, block, info.data_ptr()), "lu!")
+    if config.gemm_strategy == "ozaki":
+        # INT8 trailing updates between panels of ozaki_block columns
+        if ozaki_scheme(config) != "modular":
+            raise ArgumentError("the INT8 trailing update uses the modular scheme (ozaki_moduli)")
+        _check(lib.mflab_set_int8_engine(h, _int8_engine(config)), "lu!")
+        _check(lib.mflab_getrf_ozaki(h, s, N, int(config.ozaki_moduli), m, n, A.ptr(), A.ld,
+                                     A.ls, ipiv.data_ptr() if kmax > 0 else None,
+                                     max(int(config.ozaki_block), block), block,
+                                     info.data_ptr()), "lu!")
+    else:
+        _check(lib.mflab_getrf(h, s, N, m, n, A.ptr(), A.ld, A.ls,
+                               ipiv.data_ptr() if kmax > 0 else None, block, info.data_ptr()),
+               "lu!")
     st = _read_info(info)
     if st == -1:
         omax.zero_()

@@ -99,6 +99,8 @@ SIGNATURES = {
     "mflab_syrk_lower_ozaki": [_vp, _vp, _int, _int, _int, _i64, _i64, _vp, _i64, _i64, _vp, _i64,
                                _i64, _d, _d],
     "mflab_potrf_ozaki": [_vp, _vp, _int, _int, _i64, _vp, _i64, _i64, _i64, _i64, _vp],
+    "mflab_getrf_ozaki": [_vp, _vp, _int, _int, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _i64,
+                          _vp],
     "mflab_opnorm_inf": [_vp, _vp, _int, _int, _i64, _i64, _vp, _i64, _i64, _vp, _vp],
     "mflab_backward_error_norm": [_vp, _vp, _int, _i64, _i64, _i64, _vp, _vp, _vp, _i64, _i64,
                                   _vp, _i64, _i64, _vp, _i64, _i64, _vp],

@@ -447,6 +447,73 @@ static int getrf_n(int64_t m, int64_t n, Mat A, int64_t *ipiv, int64_t block, in
     return MFLAB_OK;
 }
 
+// LU with INT8 trailing updates: panels of nb columns factored by the blocked
+// algorithm above (pivot search and full-row interchanges, rank-1 updates,
+// TRSM and GEMM restricted to the panel's columns), then U12 = L11^-1 A12 and
+// A22 -= L21 U12 through the modular INT8 route.  The device info word is read
+// after every panel (one synchronisation each) so that a zero pivot stops the
+// factorization before the next trailing update.
+template <int N>
+static int getrf_ozaki_n(mflab_handle *h, int64_t m, int64_t n, Mat A, int64_t *ipiv, int64_t nb,
+                         int64_t block, int moduli, int *info, cudaStream_t s) {
+    const double mone[4] = {-1.0, 0.0, 0.0, 0.0}, one[4] = {1.0, 0.0, 0.0, 0.0};
+    cudaError_t e = cudaMemsetAsync(info, 0, sizeof(int), s);
+    if (e != cudaSuccess) return record_cuda_error(e, "getrf info");
+    const int64_t kmax = m < n ? m : n;
+    if (kmax == 0) return MFLAB_OK;
+    int64_t tot = m * n;
+    nonfinite_kernel<N><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(m, n, A, 0, info);
+    int rc = record_cuda_error(cudaGetLastError(), "getrf check");
+    if (rc) return rc;
+    for (int64_t j0 = 0; j0 < kmax; j0 += nb) {
+        const int64_t j1 = j0 + nb < kmax ? j0 + nb : kmax;  // panel columns [j0, j1)
+        for (int64_t first = j0; first < j1; first += block) {
+            const int64_t last = first + block - 1 < j1 - 1 ? first + block - 1 : j1 - 1;
+            for (int64_t k = first; k <= last; ++k) {
+                lu_pivot_kernel<N, 512><<<1, 512, 0, s>>>(m, n, A, k, ipiv, info);
+                rc = record_cuda_error(cudaGetLastError(), "getrf pivot");
+                if (rc) return rc;
+                if (k < last && k + 1 < m) {
+                    const int64_t rows = m - k - 1;
+                    lu_rank1_kernel<N><<<(unsigned)((rows + 127) / 128), 128, 0, s>>>(m, A, k, last,
+                                                                                     info);
+                    rc = record_cuda_error(cudaGetLastError(), "getrf rank1");
+                    if (rc) return rc;
+                }
+            }
+            if (last < j1 - 1) {
+                const int64_t w = last - first + 1, cols = j1 - 1 - last;
+                rc = launch_trsm_info(N, 0, 0, 0, 1, w, cols, A.at(first, first),
+                                      A.at(first, last + 1), one, s, info);
+                if (rc) return rc;
+                if (last < m - 1) {
+                    rc = launch_mm(N, false, false, 0, N == 3, m - 1 - last, cols, w,
+                                   A.at(last + 1, first), A.at(first, last + 1),
+                                   A.at(last + 1, last + 1), mone, one, s, info);
+                    if (rc) return rc;
+                }
+            }
+        }
+        int hinfo = 0;
+        e = cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return record_cuda_error(e, "getrf info read");
+        if (hinfo != 0) return MFLAB_OK;
+        if (j1 < n) {
+            const int64_t w = j1 - j0;
+            rc = launch_trsm_info(N, 0, 0, 0, 1, w, n - j1, A.at(j0, j0), A.at(j0, j1), one, s,
+                                  info);
+            if (rc) return rc;
+            if (j1 < m) {
+                rc = ozaki_crt_gemm(h, N, moduli, m - j1, n - j1, w, A.at(j1, j0), A.at(j0, j1),
+                                    A.at(j1, j1), mone, one, s, nullptr);
+                if (rc) return rc;
+            }
+        }
+    }
+    return MFLAB_OK;
+}
+
 // apply the recorded row interchanges to the right-hand sides (solve.jl:85-113);
 // one thread per column, interchanges in ascending k
 template <int N>
@@ -661,6 +728,29 @@ extern "C" int mflab_getrf(mflab_handle *h, void *stream, int limbs, int64_t m, 
     case 2: return mfl::getrf_n<2>(m, n, a, ipiv, block, info, s);
     case 3: return mfl::getrf_n<3>(m, n, a, ipiv, block, info, s);
     default: return mfl::getrf_n<4>(m, n, a, ipiv, block, info, s);
+    }
+}
+
+extern "C" int mflab_getrf_ozaki(mflab_handle *h, void *stream, int limbs, int moduli, int64_t m,
+                                 int64_t n, double *A, int64_t lda, int64_t lsa, int64_t *ipiv,
+                                 int64_t nb, int64_t block, int *info) {
+    if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
+    if (m < 0 || n < 0 || (m > 0 && lda < m) || !info || (m > 0 && n > 0 && !ipiv) || moduli < 0)
+        return MFLAB_ERR_ARG;
+    if (block < 1) block = 1;
+    if (nb < block) nb = block;
+    Mat a{A, lda, lsa};
+    cudaStream_t s = (cudaStream_t)stream;
+    const int64_t kmax = m < n ? m : n;
+    if (kmax > 0) {
+        mfl::iota1_kernel<<<(unsigned)((kmax + 255) / 256), 256, 0, s>>>(ipiv, kmax);
+        int rc = mfl::record_cuda_error(cudaGetLastError(), "getrf ipiv");
+        if (rc) return rc;
+    }
+    switch (limbs) {
+    case 2: return mfl::getrf_ozaki_n<2>(h, m, n, a, ipiv, nb, block, moduli, info, s);
+    case 3: return mfl::getrf_ozaki_n<3>(h, m, n, a, ipiv, nb, block, moduli, info, s);
+    default: return mfl::getrf_ozaki_n<4>(h, m, n, a, ipiv, nb, block, moduli, info, s);
     }
 }
 

@@ -126,3 +126,38 @@ def test_cholesky_int8_trailing_failure(mf, ref, rng, N):
     S[0, 5, 2] = np.inf
     with pytest.raises(mf.DomainError):
         mf.cholesky_(mf.MFMatrix.from_numpy(S), config=mf.KernelConfig(**LOWER))
+
+
+@pytest.mark.parametrize("N", [2, 3, 4])
+@pytest.mark.parametrize("m,n,nb", [(40, 40, 256), (300, 300, 128), (520, 400, 256),
+                                    (300, 520, 128)], ids=str)
+def test_lu_int8_trailing(mf, ref, rng, N, m, n, nb):
+    """LU with INT8 trailing updates: the first panel (pivots and factors)
+    equals the matched factorization bit for bit; square systems solve to the
+    backward error of the matched LU"""
+    A = syn.randn_mf(rng, N, m, n)
+    Ad = mf.MFMatrix.from_numpy(A)
+    F = mf.lu_(Ad, config=mf.KernelConfig(ozaki_block=nb, **LOWER))
+    LU, piv, info = ref.getrf(A)
+    assert mf.factor_status(F) == info == 0
+    w = min(nb, m, n)
+    assert np.array_equal(mf.factor_pivots(F)[:w], piv[:w])
+    assert_bitwise(Ad.to_numpy()[:, :, :w], LU[:, :, :w], "first panel")
+    if m == n:
+        B = syn.randn_mf(rng, N, n, 3)
+        X = mf.solve(F, mf.MFMatrix.from_numpy(B)).to_numpy()
+        be = ref.backward_error(A, X, B)
+        assert np.all(be < 4096 * n * 2.0 ** (-52 * N)), be
+
+
+@pytest.mark.parametrize("N", [2, 4])
+def test_lu_int8_trailing_singular(mf, rng, N):
+    """a zero pivot in the second panel is reported at the matched position"""
+    n = 400
+    A = syn.randn_mf(rng, N, n, n)
+    A[:, :, 300] = 0.0  # an exactly zero column stays zero through the updates
+    Fm = mf.lu_(mf.MFMatrix.from_numpy(A), check=False)
+    Fo = mf.lu_(mf.MFMatrix.from_numpy(A), check=False,
+                config=mf.KernelConfig(ozaki_block=256, **LOWER))
+    assert mf.factor_status(Fm) == 301
+    assert mf.factor_status(Fo) == mf.factor_status(Fm)
