@@ -290,9 +290,9 @@ __host__ __device__ __forceinline__ bool crt_reduce(const uint64_t (&X)[WP], con
 }
 
 // Float64xN value of a WP-word magnitude times 2^e2: the top 53 (N+1) bits as
-// N+1 truncated 53-bit chunks (exact for values with at most 53 (N+1)
-// significant bits), summed least significant first with the add network,
-// which rounds the guard chunk into the N limbs
+// N+1 truncated 53-bit chunks (the guard chunk rounds into the N limbs),
+// renormalised with fast two-sums (exact for values of at most 53 N
+// significant bits)
 template <int N, int WP>
 __device__ __forceinline__ mf<N> crt_words_to_mf(const uint32_t (&mag)[WP], int e2) {
     int pos = -1;
@@ -317,7 +317,7 @@ __device__ __forceinline__ mf<N> crt_words_to_mf(const uint32_t (&mag)[WP], int 
     a[0] <<= lz;
     // the window's bit 32 WP - 1 has weight 2^(32 pos + 31 - lz + e2)
     const int top = 32 * pos + 32 - lz + e2;
-    mf<N> g = from_double<N>(0.0);
+    double c[N + 1];
 #pragma unroll
     for (int l = N; l >= 0; --l) {
         const int b0 = 32 * WP - 53 * (l + 1);  // lowest bit of chunk l in the window
@@ -331,9 +331,22 @@ __device__ __forceinline__ mf<N> crt_words_to_mf(const uint32_t (&mag)[WP], int 
             ch = b0 > -53 ? ((uint64_t)a[0] | ((uint64_t)a[1] << 32)) << (-b0) : 0;
         }
         ch &= (1ULL << 53) - 1;
-        const double d = scale2((double)ch, top - 53 * (l + 1));
-        g = l == N ? from_double<N>(d) : add(g, from_double<N>(d));
+        c[l] = scale2((double)ch, top - 53 * (l + 1));
     }
+    // The chunks are exact, of one sign, and each nonzero one lies above the sum
+    // of those below it (they fill lower units of its 53-bit grid), so a
+    // bottom-up sweep of error-free fast two-sums carries the rounding of the
+    // lower chunks into the upper ones; a top-down sweep of two-sums (no order
+    // condition) leaves every term below half an ulp of the one above; the last
+    // term is folded into limb N-1.
+#pragma unroll
+    for (int l = N - 1; l >= 0; --l) fast_two_sum(c[l], c[l + 1], c[l], c[l + 1]);
+#pragma unroll
+    for (int l = 0; l < N; ++l) two_sum(c[l], c[l + 1], c[l], c[l + 1]);
+    mf<N> g;
+#pragma unroll
+    for (int l = 0; l < N; ++l) g.v[l] = c[l];
+    g.v[N - 1] = __dadd_rn(g.v[N - 1], c[N]);
     return g;
 }
 
