@@ -349,6 +349,23 @@ int mflab_spd_batched_adjoint(mflab_handle *h, void *stream, int limbs, int64_t 
                               int64_t ls_s, const double *X, double *XB, int64_t ls_x, double *SB,
                               const int *info, int *counter, int grid);
 
+/* mflab_spd_batched / mflab_spd_batched_adjoint with the CTA size chosen:
+   threads = 128, 256 or 512 (the plain entries use 256).  Neither the CTA
+   size nor the number of persistent CTAs (grid) changes any result: every
+   block's arithmetic is per element in the reference order; they are the
+   knobs of the batched autotuner.  No reference counterpart. */
+int mflab_spd_batched_ex(mflab_handle *h, void *stream, int limbs, int64_t nblocks,
+                         int64_t max_size, const int64_t *sizes, const int64_t *offsets,
+                         const int64_t *boffsets, const int64_t *order, double *S, int64_t ls_s,
+                         double *X, int64_t ls_x, int64_t block, int solve, int *info,
+                         int *counter, int grid, int threads);
+int mflab_spd_batched_adjoint_ex(mflab_handle *h, void *stream, int limbs, int64_t nblocks,
+                                 int64_t max_size, const int64_t *sizes, const int64_t *offsets,
+                                 const int64_t *boffsets, const int64_t *order, const double *L,
+                                 int64_t ls_s, const double *X, double *XB, int64_t ls_x,
+                                 double *SB, const int *info, int *counter, int grid,
+                                 int threads);
+
 /* ------------------------------------------------------- diagnostics --- */
 /* out (device, limbs+1 doubles) = [max |A(r,c)| over the region, finite flag]
    with region 0 all entries, 1 lower (r >= c), 2 upper (r <= c).

@@ -83,6 +83,10 @@ SIGNATURES = {
                           _i64, _int, _vp, _vp, _int],
     "mflab_spd_batched_adjoint": [_vp, _vp, _int, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _i64, _vp,
                                   _vp, _i64, _vp, _vp, _vp, _int],
+    "mflab_spd_batched_ex": [_vp, _vp, _int, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _i64, _vp, _i64,
+                             _i64, _int, _vp, _vp, _int, _int],
+    "mflab_spd_batched_adjoint_ex": [_vp, _vp, _int, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _i64,
+                                     _vp, _vp, _i64, _vp, _vp, _vp, _int, _int],
     "mflab_sytrf": [_vp, _vp, _int, _i64, _vp, _i64, _i64, _vp, _i64, _vp, _vp, _int, _i64, _vp],
     "mflab_sytrs": [_vp, _vp, _int, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _vp, _vp, _vp, _i64,
                     _i64, _vp],

@@ -11,11 +11,12 @@ results equal the single-matrix routines.
     Sbar, bbar = pullback(xbar)             # ChainRulesCore-style pullback
 
 `BatchedSPDGraph` captures the whole launch (counter reset + persistent
-kernel) in a CUDA graph and replays it.
+kernel) in a CUDA graph and replays it.  `autotune` picks the launch shape
+(CTA size, number of persistent CTAs) by timing the batch itself.
 """
 from __future__ import annotations
 
-from typing import Optional, Sequence
+from typing import Dict, Optional, Sequence
 
 import numpy as np
 import torch
@@ -84,26 +85,93 @@ class SPDBatch:
 
 
 def _launch(batch: SPDBatch, solve: bool, block: int, stream: Optional[int] = None,
-            grid: int = 0) -> None:
+            grid: int = 0, threads: int = 256) -> None:
     from . import _check, _handle
     lib = _native.load()
     s = torch.cuda.current_stream(batch.device).cuda_stream if stream is None else stream
-    rc = lib.mflab_spd_batched(_handle(batch.device), s, batch.N, batch.nblocks,
-                               int(batch.sizes_host.max()) if batch.nblocks else 0,
-                               batch.sizes.data_ptr(), batch.offsets.data_ptr(),
-                               batch.boffsets.data_ptr(), batch.order.data_ptr(),
-                               batch.S.data_ptr(), batch.S.shape[1], batch.X.data_ptr(),
-                               batch.X.shape[1], block, int(solve), batch.info.data_ptr(),
-                               batch.counter.data_ptr(), grid)
+    rc = lib.mflab_spd_batched_ex(_handle(batch.device), s, batch.N, batch.nblocks,
+                                  int(batch.sizes_host.max()) if batch.nblocks else 0,
+                                  batch.sizes.data_ptr(), batch.offsets.data_ptr(),
+                                  batch.boffsets.data_ptr(), batch.order.data_ptr(),
+                                  batch.S.data_ptr(), batch.S.shape[1], batch.X.data_ptr(),
+                                  batch.X.shape[1], block, int(solve), batch.info.data_ptr(),
+                                  batch.counter.data_ptr(), grid, threads)
     _check(rc, "spd_batched")
 
 
-def potrf_potrs_batched_(batch: SPDBatch, block: int = 16, check: bool = True) -> np.ndarray:
+_TUNED: Dict[tuple, dict] = {}
+
+
+def _signature(batch: SPDBatch, block: int) -> tuple:
+    n = batch.sizes_host.astype(np.int64)
+    return (batch.N, block, batch.nblocks, int(n.max()) if len(n) else 0, int(n.sum()),
+            int((n * n).sum()))
+
+
+def autotune(batch: SPDBatch, block: int = 16, candidates: Optional[Sequence] = None,
+             reps: int = 2) -> dict:
+    """Launch shape of the batched factor + solve for this batch: the CTA size
+    (128, 256 or 512 threads) and the number of persistent CTAs (1, 2, 4 or 8
+    per SM), picked by timing the real launch on the batch's own blocks
+    (restored afterwards).  Neither knob changes any result (each block's
+    arithmetic is per element in the reference order), so the choice is free.
+    Cached per (limbs, block, size signature of the batch).
+    Returns {"threads", "grid", "ms", "timings"}."""
+    key = _signature(batch, block)
+    if key in _TUNED:
+        return _TUNED[key]
+    if batch.nblocks == 0:
+        return {"threads": 256, "grid": 0, "ms": 0.0, "timings": {}}
+    sms = torch.cuda.get_device_properties(batch.device).multi_processor_count
+    cands = list(candidates) if candidates is not None else [
+        (nt, cps) for nt in (128, 256, 512) for cps in (1, 2, 4, 8) if nt * cps <= 2048]
+    S0, X0 = batch.S.clone(), batch.X.clone()
+    timings = {}
+    best = None
+    for nt, cps in cands:
+        grid = int(min(sms * cps, batch.nblocks))
+        times = []
+        for r in range(reps + 1):
+            batch.S.copy_(S0)
+            batch.X.copy_(X0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            _launch(batch, True, block, grid=grid, threads=nt)
+            e1.record()
+            e1.synchronize()
+            if r > 0:
+                times.append(e0.elapsed_time(e1))
+        t = min(times)
+        timings[f"{nt}x{grid}"] = t
+        if best is None or t < best[0]:
+            best = (t, nt, grid)
+    batch.S.copy_(S0)
+    batch.X.copy_(X0)
+    del S0, X0
+    res = {"threads": best[1], "grid": best[2], "ms": best[0], "timings": timings}
+    _TUNED[key] = res
+    return res
+
+
+def _shape(batch: SPDBatch, block: int, tuning) -> tuple:
+    """(threads, grid) from tuning: None = defaults, "auto" = autotune, or a
+    dict as autotune returns"""
+    if tuning is None:
+        return 256, 0
+    if tuning == "auto":
+        tuning = autotune(batch, block)
+    return int(tuning["threads"]), int(tuning["grid"])
+
+
+def potrf_potrs_batched_(batch: SPDBatch, block: int = 16, check: bool = True,
+                         tuning=None) -> np.ndarray:
     """Factor every block in place (S_i <- L_i) and overwrite every right-hand
     side with its solution.  Returns the per-block status (0 or the failing
-    column, as cholesky!'s info)."""
+    column, as cholesky!'s info).  tuning: None (default launch shape),
+    "auto" (autotune) or an autotune result."""
     from . import PosDefException
-    _launch(batch, True, block)
+    threads, grid = _shape(batch, block, tuning)
+    _launch(batch, True, block, grid=grid, threads=threads)
     info = batch.info[:batch.nblocks].cpu().numpy().copy()
     if check and np.any(info != 0):
         bad = int(np.flatnonzero(info)[0])
@@ -113,10 +181,12 @@ def potrf_potrs_batched_(batch: SPDBatch, block: int = 16, check: bool = True) -
 
 class BatchedSPDGraph:
     """The batched factor + solve captured once in a CUDA graph and replayed
-    (inputs are refreshed in place between replays)."""
+    (inputs are refreshed in place between replays).  tuning as in
+    potrf_potrs_batched_ (an autotune runs before the capture)."""
 
-    def __init__(self, batch: SPDBatch, block: int = 16):
+    def __init__(self, batch: SPDBatch, block: int = 16, tuning=None):
         self.batch = batch
+        self.threads, self.grid = _shape(batch, block, tuning)
         self.graph = torch.cuda.CUDAGraph()
         self.stream = torch.cuda.Stream(device=batch.device)
         _native.load()
@@ -124,13 +194,14 @@ class BatchedSPDGraph:
         _handle(batch.device)  # create the handle before capture
         with torch.cuda.stream(self.stream):
             with torch.cuda.graph(self.graph, stream=self.stream):
-                _launch(batch, True, block, stream=self.stream.cuda_stream)
+                _launch(batch, True, block, stream=self.stream.cuda_stream, grid=self.grid,
+                        threads=self.threads)
 
     def replay(self) -> None:
         self.graph.replay()
 
 
-def solve_spd_batched_rrule(batch: SPDBatch, block: int = 16):
+def solve_spd_batched_rrule(batch: SPDBatch, block: int = 16, tuning=None):
     """x_i = S_i^{-1} b_i for every block, with a pullback.
 
     Mirrors a ChainRulesCore rrule: returns (x, pullback) where x is the packed
@@ -138,20 +209,21 @@ def solve_spd_batched_rrule(batch: SPDBatch, block: int = 16):
     block, bbar = S^{-1} xbar and Sbar = -(bbar x^T + x bbar^T)/2 (symmetric
     parametrisation), reusing the factors."""
     from . import _check, _handle
-    potrf_potrs_batched_(batch, block)
+    threads, grid = _shape(batch, block, tuning)
+    potrf_potrs_batched_(batch, block, tuning={"threads": threads, "grid": grid})
     x = batch.X.clone()
 
     def pullback(xbar: torch.Tensor):
         lib = _native.load()
         xb = xbar.clone()
         sb = torch.zeros_like(batch.S)
-        rc = lib.mflab_spd_batched_adjoint(
+        rc = lib.mflab_spd_batched_adjoint_ex(
             _handle(batch.device), torch.cuda.current_stream(batch.device).cuda_stream, batch.N,
             batch.nblocks, int(batch.sizes_host.max()) if batch.nblocks else 0,
             batch.sizes.data_ptr(), batch.offsets.data_ptr(), batch.boffsets.data_ptr(),
             batch.order.data_ptr(), batch.S.data_ptr(), batch.S.shape[1], x.data_ptr(),
             xb.data_ptr(), x.shape[1], sb.data_ptr(), batch.info.data_ptr(),
-            batch.counter.data_ptr(), 0)
+            batch.counter.data_ptr(), grid, threads)
         _check(rc, "spd_batched adjoint")
         return sb, xb
 

@@ -18,7 +18,7 @@
 
 namespace mfl {
 
-constexpr int BATCH_NT = 256;
+constexpr int BATCH_NT = 256;   // default threads per CTA
 constexpr int BATCH_MAXN = 512;  // largest block size the shared buffers hold
 
 template <int N>
@@ -31,8 +31,9 @@ struct BlockView {
     }
 };
 
-// blocked Cholesky of one block by the whole CTA; returns info (0 / column)
-template <int N>
+// blocked Cholesky of one block by the whole CTA of NT threads; returns info
+// (0 / column)
+template <int N, int NT>
 __device__ int cta_potrf(const BlockView<N> &F, int64_t block, double (*bc)[4], int *flag) {
     const int t = threadIdx.x;
     const int64_t n = F.n;
@@ -61,7 +62,7 @@ __device__ int cta_potrf(const BlockView<N> &F, int64_t block, double (*bc)[4], 
             mf<N> p;
 #pragma unroll
             for (int l = 0; l < N; ++l) p.v[l] = bc[0][l];
-            for (int64_t row = col + 1 + t; row <= last; row += BATCH_NT) {
+            for (int64_t row = col + 1 + t; row <= last; row += NT) {
                 mf<N> v = F.at(row, col);
                 for (int64_t k = first; k < col; ++k) v = submul(v, F.at(row, k), F.at(col, k));
                 F.put(row, col, div(v, p));
@@ -70,7 +71,7 @@ __device__ int cta_potrf(const BlockView<N> &F, int64_t block, double (*bc)[4], 
         }
         if (last < n - 1) {
             // A21 <- A21 / L11^T: trsm(side=right, lower, T), one row per thread
-            for (int64_t row = last + 1 + t; row < n; row += BATCH_NT) {
+            for (int64_t row = last + 1 + t; row < n; row += NT) {
                 for (int64_t col = first; col <= last; ++col) {
                     mf<N> v = F.at(row, col);
                     for (int64_t k = first; k < col; ++k) v = submul(v, F.at(row, k), F.at(col, k));
@@ -81,7 +82,7 @@ __device__ int cta_potrf(const BlockView<N> &F, int64_t block, double (*bc)[4], 
             // lower trailing update: -1 * (A21 A21^T) + 1 * A22 (syrk.jl:1-50)
             const int64_t m = n - 1 - last;
             const int64_t tot = m * (m + 1) / 2;
-            for (int64_t e = t; e < tot; e += BATCH_NT) {
+            for (int64_t e = t; e < tot; e += NT) {
                 int64_t c = (int64_t)((2.0 * m + 1.0 - sqrt((2.0 * m + 1.0) * (2.0 * m + 1.0) - 8.0 * e)) / 2.0);
                 while (c > 0 && c * m - c * (c - 1) / 2 > e) --c;
                 while ((c + 1) * m - (c + 1) * c / 2 <= e) ++c;
@@ -97,10 +98,12 @@ __device__ int cta_potrf(const BlockView<N> &F, int64_t block, double (*bc)[4], 
     return 0;
 }
 
-// x <- L^{-T} L^{-1} x (solve.jl:54-83), one vector, in place
-template <int N>
+// x <- L^{-T} L^{-1} x (solve.jl:54-83), one vector, in place, by a CTA of NT
+// threads (thread t holds rows t, t + NT, ... of the forward wavefront)
+template <int N, int NT>
 __device__ void cta_potrs(const BlockView<N> &F, double *x, int64_t ls_x, double (*bc)[4],
                           double (*prod)[4]) {
+    constexpr int MAXR = BATCH_MAXN / NT;
     const int t = threadIdx.x;
     const int64_t n = F.n;
     auto xget = [&](int64_t i) {
@@ -115,51 +118,59 @@ __device__ void cta_potrs(const BlockView<N> &F, double *x, int64_t ls_x, double
     };
     // forward substitution, wavefront: row r receives its terms k = 0..r-1 in
     // ascending order as the unknowns are finalised
-    mf<N> v0 = from_double<N>(0.0), v1 = from_double<N>(0.0);
-    if (t < n) v0 = xget(t);
-    if (t + BATCH_NT < n) v1 = xget(t + BATCH_NT);
-    for (int64_t k = 0; k < n; ++k) {
-        if ((k % BATCH_NT) == t) {
-            mf<N> v = (k < BATCH_NT) ? v0 : v1;
-            v = div(v, F.at(k, k));
-            xput(k, v);
+    mf<N> v[MAXR];
 #pragma unroll
-            for (int l = 0; l < N; ++l) bc[k & 1][l] = v.v[l];
+    for (int q = 0; q < MAXR; ++q)
+        v[q] = t + q * NT < n ? xget(t + q * NT) : from_double<N>(0.0);
+    for (int64_t k = 0; k < n; ++k) {
+        if ((k % NT) == t) {
+            const int qk = (int)(k / NT);
+            mf<N> vk;
+#pragma unroll
+            for (int q = 0; q < MAXR; ++q)
+                if (q == qk) vk = v[q];
+            vk = div(vk, F.at(k, k));
+            xput(k, vk);
+#pragma unroll
+            for (int l = 0; l < N; ++l) bc[k & 1][l] = vk.v[l];
         }
         __syncthreads();
         mf<N> xk;
 #pragma unroll
         for (int l = 0; l < N; ++l) xk.v[l] = bc[k & 1][l];
-        if (t > k && t < n) v0 = submul(v0, F.at(t, k), xk);
-        if (t + BATCH_NT > k && t + BATCH_NT < n) v1 = submul(v1, F.at(t + BATCH_NT, k), xk);
+#pragma unroll
+        for (int q = 0; q < MAXR; ++q) {
+            const int64_t r = t + q * NT;
+            if (r > k && r < n) v[q] = submul(v[q], F.at(r, k), xk);
+        }
     }
     __syncthreads();
     // backward substitution with L^T: the reference's chain for row r is
     // v = x[r]; v -= L[k, r] * x[k] for k = r+1..n-1 ascending; v /= L[r, r].
     // The products are formed in parallel, the subtraction chain stays serial.
     for (int64_t r = n - 1; r >= 0; --r) {
-        for (int64_t k = r + 1 + t; k < n; k += BATCH_NT) {
+        for (int64_t k = r + 1 + t; k < n; k += NT) {
             const mf<N> p = mul(F.at(k, r), xget(k));
 #pragma unroll
             for (int l = 0; l < N; ++l) prod[k][l] = p.v[l];
         }
         __syncthreads();
         if (t == 0) {
-            mf<N> v = xget(r);
+            mf<N> vr = xget(r);
             for (int64_t k = r + 1; k < n; ++k) {
                 mf<N> p;
 #pragma unroll
                 for (int l = 0; l < N; ++l) p.v[l] = prod[k][l];
-                v = sub(v, p);
+                vr = sub(vr, p);
             }
-            xput(r, div(v, F.at(r, r)));
+            xput(r, div(vr, F.at(r, r)));
         }
         __syncthreads();
     }
 }
 
-template <int N>
-__global__ void __launch_bounds__(BATCH_NT)
+template <int N, int NT>
+__global__ void __launch_bounds__(NT)
     spd_batched_kernel(int64_t nblocks, const int64_t *sizes, const int64_t *offsets,
                        const int64_t *boffsets, const int64_t *order, double *S, int64_t ls_s,
                        double *X, int64_t ls_x, int64_t block, int *info, int *counter,
@@ -180,9 +191,9 @@ __global__ void __launch_bounds__(BATCH_NT)
         const int64_t b = order[idx];
         const int64_t n = sizes[b];
         BlockView<N> F{Mat{S + offsets[b], n > 0 ? n : 1, ls_s}, n};
-        const int st = cta_potrf<N>(F, block, bc, &flag);
+        const int st = cta_potrf<N, NT>(F, block, bc, &flag);
         if (t == 0) info[b] = st;
-        if (st == 0 && solve) cta_potrs<N>(F, X + boffsets[b], ls_x, bc, prod);
+        if (st == 0 && solve) cta_potrs<N, NT>(F, X + boffsets[b], ls_x, bc, prod);
         __syncthreads();
     }
 }
@@ -190,8 +201,8 @@ __global__ void __launch_bounds__(BATCH_NT)
 // Adjoint of x = S^{-1} b for loss gradients: given the factor L (in place),
 // x and xbar, writes bbar = S^{-1} xbar (over xbar) and
 // Sbar = -(bbar x^T + x bbar^T) / 2 into the packed Sbar buffer.
-template <int N>
-__global__ void __launch_bounds__(BATCH_NT)
+template <int N, int NT>
+__global__ void __launch_bounds__(NT)
     spd_batched_adjoint_kernel(int64_t nblocks, const int64_t *sizes, const int64_t *offsets,
                                const int64_t *boffsets, const int64_t *order, const double *L,
                                int64_t ls_s, const double *X, double *XB, int64_t ls_x,
@@ -209,12 +220,12 @@ __global__ void __launch_bounds__(BATCH_NT)
         const int64_t n = sizes[b];
         if (info[b] == 0) {
             BlockView<N> F{Mat{(double *)L + offsets[b], n > 0 ? n : 1, ls_s}, n};
-            cta_potrs<N>(F, XB + boffsets[b], ls_x, bc, prod);
+            cta_potrs<N, NT>(F, XB + boffsets[b], ls_x, bc, prod);
             __syncthreads();
             const double *x = X + boffsets[b];
             const double *xb = XB + boffsets[b];
             double *sb = SB + offsets[b];
-            for (int64_t e = t; e < n * n; e += BATCH_NT) {
+            for (int64_t e = t; e < n * n; e += NT) {
                 const int64_t r = e % n, c = e / n;
                 mf<N> xr, xc, br, bcv;
 #pragma unroll
@@ -242,26 +253,88 @@ static int batched_check(int limbs, int64_t nblocks, int64_t maxn) {
     return MFLAB_OK;
 }
 
-extern "C" int mflab_spd_batched(mflab_handle *h, void *stream, int limbs, int64_t nblocks,
-                                 int64_t max_size, const int64_t *sizes, const int64_t *offsets,
-                                 const int64_t *boffsets, const int64_t *order, double *S,
-                                 int64_t ls_s, double *X, int64_t ls_x, int64_t block, int solve,
-                                 int *info, int *counter, int grid) {
+template <int NT>
+static void launch_batched(int limbs, int grid, cudaStream_t s, int64_t nblocks,
+                           const int64_t *sizes, const int64_t *offsets, const int64_t *boffsets,
+                           const int64_t *order, double *S, int64_t ls_s, double *X, int64_t ls_x,
+                           int64_t block, int *info, int *counter, int solve) {
+    switch (limbs) {
+    case 2: mfl::spd_batched_kernel<2, NT><<<grid, NT, 0, s>>>(nblocks, sizes, offsets, boffsets, order, S, ls_s, X, ls_x, block, info, counter, solve); break;
+    case 3: mfl::spd_batched_kernel<3, NT><<<grid, NT, 0, s>>>(nblocks, sizes, offsets, boffsets, order, S, ls_s, X, ls_x, block, info, counter, solve); break;
+    default: mfl::spd_batched_kernel<4, NT><<<grid, NT, 0, s>>>(nblocks, sizes, offsets, boffsets, order, S, ls_s, X, ls_x, block, info, counter, solve); break;
+    }
+}
+
+template <int NT>
+static void launch_adjoint(int limbs, int grid, cudaStream_t s, int64_t nblocks,
+                           const int64_t *sizes, const int64_t *offsets, const int64_t *boffsets,
+                           const int64_t *order, const double *L, int64_t ls_s, const double *X,
+                           double *XB, int64_t ls_x, double *SB, const int *info, int *counter) {
+    switch (limbs) {
+    case 2: mfl::spd_batched_adjoint_kernel<2, NT><<<grid, NT, 0, s>>>(nblocks, sizes, offsets, boffsets, order, L, ls_s, X, XB, ls_x, SB, info, counter); break;
+    case 3: mfl::spd_batched_adjoint_kernel<3, NT><<<grid, NT, 0, s>>>(nblocks, sizes, offsets, boffsets, order, L, ls_s, X, XB, ls_x, SB, info, counter); break;
+    default: mfl::spd_batched_adjoint_kernel<4, NT><<<grid, NT, 0, s>>>(nblocks, sizes, offsets, boffsets, order, L, ls_s, X, XB, ls_x, SB, info, counter); break;
+    }
+}
+
+extern "C" int mflab_spd_batched_ex(mflab_handle *h, void *stream, int limbs, int64_t nblocks,
+                                    int64_t max_size, const int64_t *sizes,
+                                    const int64_t *offsets, const int64_t *boffsets,
+                                    const int64_t *order, double *S, int64_t ls_s, double *X,
+                                    int64_t ls_x, int64_t block, int solve, int *info,
+                                    int *counter, int grid, int threads) {
     if (!h) return MFLAB_ERR_UNSUPPORTED;
     int rc = batched_check(limbs, nblocks, max_size);
     if (rc) return rc;
+    if (threads != 128 && threads != 256 && threads != 512) return MFLAB_ERR_ARG;
     if (block < 1) block = 1;
     if (nblocks == 0) return MFLAB_OK;
     cudaStream_t s = (cudaStream_t)stream;
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), s);
     if (e != cudaSuccess) return mfl::record_cuda_error(e, "spd batched counter");
     if (grid <= 0) grid = 148 * 4;
-    switch (limbs) {
-    case 2: mfl::spd_batched_kernel<2><<<grid, mfl::BATCH_NT, 0, s>>>(nblocks, sizes, offsets, boffsets, order, S, ls_s, X, ls_x, block, info, counter, solve); break;
-    case 3: mfl::spd_batched_kernel<3><<<grid, mfl::BATCH_NT, 0, s>>>(nblocks, sizes, offsets, boffsets, order, S, ls_s, X, ls_x, block, info, counter, solve); break;
-    default: mfl::spd_batched_kernel<4><<<grid, mfl::BATCH_NT, 0, s>>>(nblocks, sizes, offsets, boffsets, order, S, ls_s, X, ls_x, block, info, counter, solve); break;
-    }
+    if (threads == 128)
+        launch_batched<128>(limbs, grid, s, nblocks, sizes, offsets, boffsets, order, S, ls_s, X, ls_x, block, info, counter, solve);
+    else if (threads == 256)
+        launch_batched<256>(limbs, grid, s, nblocks, sizes, offsets, boffsets, order, S, ls_s, X, ls_x, block, info, counter, solve);
+    else
+        launch_batched<512>(limbs, grid, s, nblocks, sizes, offsets, boffsets, order, S, ls_s, X, ls_x, block, info, counter, solve);
     return mfl::record_cuda_error(cudaGetLastError(), "spd batched");
+}
+
+extern "C" int mflab_spd_batched(mflab_handle *h, void *stream, int limbs, int64_t nblocks,
+                                 int64_t max_size, const int64_t *sizes, const int64_t *offsets,
+                                 const int64_t *boffsets, const int64_t *order, double *S,
+                                 int64_t ls_s, double *X, int64_t ls_x, int64_t block, int solve,
+                                 int *info, int *counter, int grid) {
+    return mflab_spd_batched_ex(h, stream, limbs, nblocks, max_size, sizes, offsets, boffsets,
+                                order, S, ls_s, X, ls_x, block, solve, info, counter, grid,
+                                mfl::BATCH_NT);
+}
+
+extern "C" int mflab_spd_batched_adjoint_ex(mflab_handle *h, void *stream, int limbs,
+                                            int64_t nblocks, int64_t max_size,
+                                            const int64_t *sizes, const int64_t *offsets,
+                                            const int64_t *boffsets, const int64_t *order,
+                                            const double *L, int64_t ls_s, const double *X,
+                                            double *XB, int64_t ls_x, double *SB, const int *info,
+                                            int *counter, int grid, int threads) {
+    if (!h) return MFLAB_ERR_UNSUPPORTED;
+    int rc = batched_check(limbs, nblocks, max_size);
+    if (rc) return rc;
+    if (threads != 128 && threads != 256 && threads != 512) return MFLAB_ERR_ARG;
+    if (nblocks == 0) return MFLAB_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), s);
+    if (e != cudaSuccess) return mfl::record_cuda_error(e, "spd adjoint counter");
+    if (grid <= 0) grid = 148 * 4;
+    if (threads == 128)
+        launch_adjoint<128>(limbs, grid, s, nblocks, sizes, offsets, boffsets, order, L, ls_s, X, XB, ls_x, SB, info, counter);
+    else if (threads == 256)
+        launch_adjoint<256>(limbs, grid, s, nblocks, sizes, offsets, boffsets, order, L, ls_s, X, XB, ls_x, SB, info, counter);
+    else
+        launch_adjoint<512>(limbs, grid, s, nblocks, sizes, offsets, boffsets, order, L, ls_s, X, XB, ls_x, SB, info, counter);
+    return mfl::record_cuda_error(cudaGetLastError(), "spd adjoint");
 }
 
 extern "C" int mflab_spd_batched_adjoint(mflab_handle *h, void *stream, int limbs,
@@ -270,18 +343,7 @@ extern "C" int mflab_spd_batched_adjoint(mflab_handle *h, void *stream, int limb
                                          const int64_t *order, const double *L, int64_t ls_s,
                                          const double *X, double *XB, int64_t ls_x, double *SB,
                                          const int *info, int *counter, int grid) {
-    if (!h) return MFLAB_ERR_UNSUPPORTED;
-    int rc = batched_check(limbs, nblocks, max_size);
-    if (rc) return rc;
-    if (nblocks == 0) return MFLAB_OK;
-    cudaStream_t s = (cudaStream_t)stream;
-    cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), s);
-    if (e != cudaSuccess) return mfl::record_cuda_error(e, "spd adjoint counter");
-    if (grid <= 0) grid = 148 * 4;
-    switch (limbs) {
-    case 2: mfl::spd_batched_adjoint_kernel<2><<<grid, mfl::BATCH_NT, 0, s>>>(nblocks, sizes, offsets, boffsets, order, L, ls_s, X, XB, ls_x, SB, info, counter); break;
-    case 3: mfl::spd_batched_adjoint_kernel<3><<<grid, mfl::BATCH_NT, 0, s>>>(nblocks, sizes, offsets, boffsets, order, L, ls_s, X, XB, ls_x, SB, info, counter); break;
-    default: mfl::spd_batched_adjoint_kernel<4><<<grid, mfl::BATCH_NT, 0, s>>>(nblocks, sizes, offsets, boffsets, order, L, ls_s, X, XB, ls_x, SB, info, counter); break;
-    }
-    return mfl::record_cuda_error(cudaGetLastError(), "spd adjoint");
+    return mflab_spd_batched_adjoint_ex(h, stream, limbs, nblocks, max_size, sizes, offsets,
+                                        boffsets, order, L, ls_s, X, XB, ls_x, SB, info, counter,
+                                        grid, mfl::BATCH_NT);
 }

@@ -184,3 +184,40 @@ def test_batched_adjoint_vs_mpmath_gradient(mf, ref, rng):
             for c in range(n):
                 want = -(bbar[r] * xs[c] + xs[r] * bbar[c]) / 2
                 assert abs(mpv(got_S[:, r, c]) - want) <= 1e-28 * (1 + abs(want))
+
+
+@pytest.mark.parametrize("N", [2, 4])
+def test_batched_launch_shapes_bitwise(mf, ref, rng, N):
+    """every CTA size and persistent-CTA count the autotuner may pick gives the
+    same factors, solutions and adjoint bit for bit (blocks up to 500, so the
+    128-thread CTA holds four rows per thread); the tuner returns one of them"""
+    sizes = rng.integers(1, 90, 30)
+    sizes[5], sizes[11] = 500, 260
+    blocks = _spd_blocks(ref, rng, N, sizes)
+    rhs = [syn.randn_mf(rng, N, int(n), 1)[:, :, 0] for n in sizes]
+    outs = []
+    for threads, grid in [(256, 0), (128, 7), (512, 3), (128, 0), (512, 148)]:
+        batch = mf.batched.SPDBatch(N, sizes)
+        for i, (S, b) in enumerate(zip(blocks, rhs)):
+            batch.set_block(i, S)
+            batch.set_rhs(i, b)
+        x, pullback = mf.batched.solve_spd_batched_rrule(
+            batch, tuning={"threads": threads, "grid": grid})
+        w = torch.ones_like(x)
+        sb, bb = pullback(w)
+        outs.append((batch.S.cpu().numpy(), x.cpu().numpy(), sb.cpu().numpy(),
+                     bb.cpu().numpy()))
+    for o in outs[1:]:
+        for a, b in zip(outs[0], o):
+            assert_bitwise(a, b, "launch shape")
+    batch = mf.batched.SPDBatch(N, sizes)
+    for i, (S, b) in enumerate(zip(blocks, rhs)):
+        batch.set_block(i, S)
+        batch.set_rhs(i, b)
+    S_before = batch.S.clone()
+    t = mf.batched.autotune(batch, reps=1)
+    assert t["threads"] in (128, 256, 512) and t["grid"] >= 1 and len(t["timings"]) == 12
+    assert torch.equal(batch.S, S_before), "autotune must restore the batch"
+    info = mf.batched.potrf_potrs_batched_(batch, tuning="auto")
+    assert np.all(info == 0)
+    assert_bitwise(batch.S.cpu().numpy(), outs[0][0], "tuned launch")
