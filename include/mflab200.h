@@ -183,6 +183,27 @@ int mflab_set_int8_engine(mflab_handle *h, int engine);
    the caller's conclusion).  Synchronises.  No reference counterpart. */
 int mflab_device_status(mflab_handle *h, int *status);
 
+/* y = alpha * op(A) * x + beta * y: op(A) = A (trans 0, A m x n) or A^T
+   (trans 1); one ascending chain per output with the plain network, y unread
+   when beta == 0.  x, y contiguous with limb strides lsx, lsy.
+   Replaces gemv!(y, A, x, alpha, beta; trans) — src/kernels/gemv.jl:99-167. */
+int mflab_gemv(mflab_handle *h, void *stream, int limbs, int trans, int64_t m, int64_t n,
+               const double *A, int64_t lda, int64_t lsa, const double *x, int64_t lsx, double *y,
+               int64_t lsy, const double *alpha, const double *beta);
+
+/* y = alpha * A * x + beta * y, A symmetric read from its lower (uplo 0) or
+   upper (uplo 1) triangle only.
+   Replaces symv!(y, A, x, alpha, beta; uplo) — src/kernels/symv.jl:43-89. */
+int mflab_symv(mflab_handle *h, void *stream, int limbs, int uplo, int64_t n, const double *A,
+               int64_t lda, int64_t lsa, const double *x, int64_t lsx, double *y, int64_t lsy,
+               const double *alpha, const double *beta);
+
+/* out (device, limbs doubles) = sum over the column-major index of x .* y for
+   two m x n arrays, one ascending chain.
+   Replaces mfdot(x, y) — src/kernels/dot.jl:1-22. */
+int mflab_dot(mflab_handle *h, void *stream, int limbs, int64_t m, int64_t n, const double *x,
+              int64_t ldx, int64_t lsx, const double *y, int64_t ldy, int64_t lsy, double *out);
+
 /* lower(C) = alpha * P^T * P + beta * lower(C); P is k x n, C n x n.  The
    strict upper triangle of C is neither read nor written.
    Replaces syrk!(C, P, alpha, beta; uplo=:lower) — src/kernels/syrk.jl:67-108. */

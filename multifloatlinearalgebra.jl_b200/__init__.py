@@ -31,7 +31,8 @@ from . import _native
 __all__ = [
     "MFMatrix", "KernelConfig", "DimensionMismatch", "ArgumentError", "DomainError",
     "PosDefException", "SingularException", "MFLABError",
-    "gemm_", "syrk_", "gemmt_", "trsm_", "trsv_", "gemm_plan", "OpNormInf",
+    "gemm_", "syrk_", "gemmt_", "trsm_", "trsv_", "gemm_plan", "OpNormInf", "gemv_", "symv_",
+    "mfdot",
     "cholesky_", "lu_", "ldiv_", "solve", "issuccess",
     "factor_status", "factor_state", "factor_kind", "factor_matrix", "factor_precision",
     "factor_provider", "factor_pivots", "factor_diagnostics",
@@ -468,6 +469,67 @@ def device_status(device: Optional[int] = None) -> int:
 
 def ozaki_available() -> bool:
     return hasattr(_native.load(), "mflab_gemm_ozaki")
+
+
+def _vec_len(v: MFMatrix, what: str) -> int:
+    if v.n != 1:
+        raise DimensionMismatch(f"{what} must be a vector")
+    return v.m
+
+
+def gemv_(y: MFMatrix, A: MFMatrix, x: MFMatrix, alpha=1.0, beta=0.0, trans: str = "N",
+          config: KernelConfig = _DEFAULT) -> MFMatrix:
+    """y = alpha*op(A)*x + beta*y (src/kernels/gemv.jl:99-167)."""
+    if trans not in ("N", "T"):
+        raise ArgumentError("trans must be :N or :T")
+    N = _same_type(y, A, x)
+    m, n = A.m, A.n
+    lx, ly = _vec_len(x, "gemv! input"), _vec_len(y, "gemv! output")
+    if lx != (n if trans == "N" else m):
+        raise DimensionMismatch("gemv! input length differs")
+    if ly != (m if trans == "N" else n):
+        raise DimensionMismatch("gemv! output length differs")
+    _no_alias("gemv!", y, A)
+    _no_alias("gemv!", y, x)
+    lib, h, s = _lib_h(y)
+    _check(lib.mflab_gemv(h, s, N, 0 if trans == "N" else 1, m, n, A.ptr(), A.ld, A.ls, x.ptr(),
+                          x.ls, y.ptr(), y.ls, _scalar(N, alpha), _scalar(N, beta)), "gemv!")
+    return y
+
+
+def symv_(y: MFMatrix, A: MFMatrix, x: MFMatrix, alpha=1.0, beta=0.0, uplo: str = "lower",
+          config: KernelConfig = _DEFAULT) -> MFMatrix:
+    """y = alpha*A*x + beta*y, A symmetric from its uplo triangle
+    (src/kernels/symv.jl:43-89)."""
+    if uplo not in ("lower", "upper"):
+        raise ArgumentError("uplo must be :lower or :upper")
+    N = _same_type(y, A, x)
+    n = A.m
+    if A.n != n:
+        raise DimensionMismatch("symv! requires a square matrix")
+    if _vec_len(x, "symv! input") != n:
+        raise DimensionMismatch("symv! input length differs")
+    if _vec_len(y, "symv! output") != n:
+        raise DimensionMismatch("symv! output length differs")
+    _no_alias("symv!", y, A)
+    _no_alias("symv!", y, x)
+    lib, h, s = _lib_h(y)
+    _check(lib.mflab_symv(h, s, N, 0 if uplo == "lower" else 1, n, A.ptr(), A.ld, A.ls, x.ptr(),
+                          x.ls, y.ptr(), y.ls, _scalar(N, alpha), _scalar(N, beta)), "symv!")
+    return y
+
+
+def mfdot(x: MFMatrix, y: MFMatrix) -> np.ndarray:
+    """Inner product over the column-major index, one ascending chain
+    (src/kernels/dot.jl:1-22); returns the N limbs."""
+    N = _same_type(x, y)
+    if (x.m, x.n) != (y.m, y.n):
+        raise DimensionMismatch("dot product shapes differ")
+    out = torch.zeros(N, dtype=torch.float64, device=x.storage.device)
+    lib, h, s = _lib_h(x)
+    _check(lib.mflab_dot(h, s, N, x.m, x.n, x.ptr(), x.ld, x.ls, y.ptr(), y.ld, y.ls,
+                         out.data_ptr()), "mfdot")
+    return out.cpu().numpy()
 
 
 def syrk_(C_: MFMatrix, P: MFMatrix, alpha=1.0, beta=0.0, uplo: str = "lower",

@@ -97,6 +97,10 @@ SIGNATURES = {
     "mflab_gemm_ozaki": [_vp, _vp, _int, _int, _i64, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _i64,
                          _vp, _i64, _i64, _d, _d],
     "mflab_ozaki_default_slices": [_int, _i64],
+    "mflab_gemv": [_vp, _vp, _int, _int, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _vp, _i64, _d,
+                   _d],
+    "mflab_symv": [_vp, _vp, _int, _int, _i64, _vp, _i64, _i64, _vp, _i64, _vp, _i64, _d, _d],
+    "mflab_dot": [_vp, _vp, _int, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _i64, _vp],
     "mflab_gemm_ozaki_crt": [_vp, _vp, _int, _int, _i64, _i64, _i64, _vp, _i64, _i64, _vp, _i64,
                              _i64, _vp, _i64, _i64, _d, _d],
     "mflab_ozaki_last_moduli": [_vp],

@@ -200,6 +200,7 @@ static int dispatch_mm(int ta, bool tb, int tri, bool fused3, int64_t m, int64_t
         return run_mm_n<N, 0, false, false, false>(m, n, k, A, B, C, alpha, beta, s, info);
     }
     if (ta == 1 && !tb && tri) return run_mm_n<N, 1, false, true, false>(m, n, k, A, B, C, alpha, beta, s, info);
+    if (ta == 1 && !tb && !tri) return run_mm_n<N, 1, false, false, false>(m, n, k, A, B, C, alpha, beta, s, info);
     if (ta == 0 && tb && tri) return run_mm_n<N, 0, true, true, false>(m, n, k, A, B, C, alpha, beta, s, info);
     if (ta == 2 && !tb && !tri) return run_mm_n<N, 2, false, false, false>(m, n, k, A, B, C, alpha, beta, s, info);
     if (ta == 3 && !tb && !tri) return run_mm_n<N, 3, false, false, false>(m, n, k, A, B, C, alpha, beta, s, info);
@@ -255,6 +256,77 @@ extern "C" int mflab_gemm(mflab_handle *h, void *stream, int limbs, int route, i
     bool fused = (limbs == 3 && route == MFLAB_GEMM_AUTO);
     return mfl::launch_mm(limbs, false, false, 0, fused, m, n, k, Mat{(double *)A, lda, lsa},
                           Mat{(double *)B, ldb, lsb}, Mat{C, ldc, lsc}, alpha, beta, s);
+}
+
+// y = alpha * op(A) x + beta * y (gemv.jl:1-167): one ascending chain per
+// output (columns for trans = 0, rows for trans = 1), the plain network (no
+// fused Float64x3 step), y unread when beta == 0; the GEMM kernel with one
+// right-hand column.  x and y are contiguous vectors with limb strides lsx, lsy.
+extern "C" int mflab_gemv(mflab_handle *h, void *stream, int limbs, int trans, int64_t m,
+                          int64_t n, const double *A, int64_t lda, int64_t lsa, const double *x,
+                          int64_t lsx, double *y, int64_t lsy, const double *alpha,
+                          const double *beta) {
+    if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
+    if (m < 0 || n < 0 || !alpha || !beta || (trans != 0 && trans != 1)) return MFLAB_ERR_ARG;
+    if (m > 0 && lda < m) return MFLAB_ERR_ARG;
+    const int64_t rows = trans ? n : m, len = trans ? m : n;
+    if (rows == 0) return MFLAB_OK;
+    if (mfl::views_overlap(y, rows, lsy, rows, 1, limbs, A, lda, lsa, m, n) ||
+        mfl::views_overlap(y, rows, lsy, rows, 1, limbs, x, len > 0 ? len : 1, lsx, len, 1))
+        return MFLAB_ERR_ALIAS;
+    return mfl::launch_mm(limbs, trans, false, 0, false, rows, 1, len, Mat{(double *)A, lda, lsa},
+                          Mat{(double *)x, len > 0 ? len : 1, lsx}, Mat{y, rows, lsy}, alpha, beta,
+                          (cudaStream_t)stream);
+}
+
+// y = alpha * A x + beta * y with A symmetric, read only from its uplo
+// triangle (symv.jl:1-89): row r's chain runs over ascending columns, taking
+// A[r, c] from the authoritative triangle and A[c, r] across it.
+extern "C" int mflab_symv(mflab_handle *h, void *stream, int limbs, int uplo, int64_t n,
+                          const double *A, int64_t lda, int64_t lsa, const double *x, int64_t lsx,
+                          double *y, int64_t lsy, const double *alpha, const double *beta) {
+    if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
+    if (n < 0 || !alpha || !beta || (uplo != 0 && uplo != 1)) return MFLAB_ERR_ARG;
+    if (n == 0) return MFLAB_OK;
+    if (lda < n) return MFLAB_ERR_ARG;
+    if (mfl::views_overlap(y, n, lsy, n, 1, limbs, A, lda, lsa, n, n) ||
+        mfl::views_overlap(y, n, lsy, n, 1, limbs, x, n, lsx, n, 1))
+        return MFLAB_ERR_ALIAS;
+    return mfl::launch_mm(limbs, 2 + uplo, false, 0, false, n, 1, n, Mat{(double *)A, lda, lsa},
+                          Mat{(double *)x, n, lsx}, Mat{y, n, lsy}, alpha, beta,
+                          (cudaStream_t)stream);
+}
+
+namespace mfl {
+// sum over the column-major linear index of x .* y, one ascending chain
+// (dot.jl:1-22) by one thread
+template <int N>
+__global__ void dot_kernel(int64_t m, int64_t n, Mat X, Mat Y, double *out) {
+    mf<N> acc = from_double<N>(0.0);
+    for (int64_t c = 0; c < n; ++c)
+        for (int64_t r = 0; r < m; ++r)
+            acc = add(acc, mul(load_mf<N>(X.p, X.ld, X.ls, r, c), load_mf<N>(Y.p, Y.ld, Y.ls, r, c)));
+#pragma unroll
+    for (int l = 0; l < N; ++l) out[l] = acc.v[l];
+}
+}  // namespace mfl
+
+// out (device, limbs doubles) = mfdot(x, y) for two m x n arrays (vectors:
+// n = 1), in ascending column-major order (dot.jl:1-22).  One serial chain,
+// as the reference's.
+extern "C" int mflab_dot(mflab_handle *h, void *stream, int limbs, int64_t m, int64_t n,
+                         const double *x, int64_t ldx, int64_t lsx, const double *y, int64_t ldy,
+                         int64_t lsy, double *out) {
+    if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
+    if (m < 0 || n < 0 || !out || (m > 0 && (ldx < m || ldy < m))) return MFLAB_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    Mat X{(double *)x, ldx, lsx}, Y{(double *)y, ldy, lsy};
+    switch (limbs) {
+    case 2: mfl::dot_kernel<2><<<1, 1, 0, s>>>(m, n, X, Y, out); break;
+    case 3: mfl::dot_kernel<3><<<1, 1, 0, s>>>(m, n, X, Y, out); break;
+    default: mfl::dot_kernel<4><<<1, 1, 0, s>>>(m, n, X, Y, out); break;
+    }
+    return mfl::record_cuda_error(cudaGetLastError(), "dot");
 }
 
 extern "C" int mflab_syrk_lower(mflab_handle *h, void *stream, int limbs, int64_t n, int64_t k,
