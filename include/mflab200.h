@@ -211,6 +211,16 @@ int mflab_syrk_lower(mflab_handle *h, void *stream, int limbs, int64_t n, int64_
                      const double *P, int64_t ldp, int64_t lsp, double *C, int64_t ldc,
                      int64_t lsc, const double *alpha, const double *beta);
 
+/* Packed lower triangle C (column-major packed: (0,0),(1,0)..(n-1,0),(1,1)..,
+   n(n+1)/2 entries per limb plane, limb stride lsc) = alpha * P[k0:k1,:]^T *
+   P[k0:k1,:] + beta * C, P kp x n, 0 <= k0 < k1 <= kp (the reference's
+   reduction_first - 1 and reduction_last); beta == 0 never reads C.
+   Replaces syrk_packed!(packed, panel, alpha, beta; reduction_first,
+   reduction_last) — src/kernels/syrk.jl:110-254. */
+int mflab_syrk_packed(mflab_handle *h, void *stream, int limbs, int64_t n, int64_t kp,
+                      int64_t k0, int64_t k1, const double *P, int64_t ldp, int64_t lsp,
+                      double *C, int64_t lsc, const double *alpha, const double *beta);
+
 /* lower(C) = alpha * A * B^T + beta * lower(C); A, B are n x k.
    Replaces gemmt!(C, A, B, alpha, beta) — src/kernels/gemmt.jl:69-108. */
 int mflab_gemmt_lower(mflab_handle *h, void *stream, int limbs, int64_t n, int64_t k,
@@ -224,6 +234,15 @@ int mflab_gemmt_lower(mflab_handle *h, void *stream, int limbs, int64_t n, int64
    Replaces trsm!(B, A, alpha; side, uplo, trans, diag) — src/kernels/trsm.jl:224-302,
    and for n == 1, side == 0 also trsv! — src/kernels/trsv.jl:19-73. */
 int mflab_trsm(mflab_handle *h, void *stream, int limbs, int side, int uplo, int trans, int diag,
+               int64_t m, int64_t n, const double *A, int64_t lda, int64_t lsa, double *B,
+               int64_t ldb, int64_t lsb, const double *alpha);
+
+/* B = alpha * op(A) * B (side 0, A m x m) or alpha * B * op(A) (side 1,
+   A n x n), in place; uplo selects the triangle of A that is read, trans 0/1,
+   diag 1 takes op(A)'s diagonal as one (never read).  Uses the handle's
+   scratch for a copy of B (m n limbs doubles).
+   Replaces trmm!(B, A, alpha; side, uplo, trans, diag) — src/kernels/trmm.jl:82-131. */
+int mflab_trmm(mflab_handle *h, void *stream, int limbs, int side, int uplo, int trans, int diag,
                int64_t m, int64_t n, const double *A, int64_t lda, int64_t lsa, double *B,
                int64_t ldb, int64_t lsb, const double *alpha);
 

@@ -32,7 +32,7 @@ __all__ = [
     "MFMatrix", "KernelConfig", "DimensionMismatch", "ArgumentError", "DomainError",
     "PosDefException", "SingularException", "MFLABError",
     "gemm_", "syrk_", "gemmt_", "trsm_", "trsv_", "gemm_plan", "OpNormInf", "gemv_", "symv_",
-    "mfdot",
+    "mfdot", "syrk_packed_", "trmm_", "BoundsError",
     "cholesky_", "lu_", "ldiv_", "solve", "issuccess",
     "factor_status", "factor_state", "factor_kind", "factor_matrix", "factor_precision",
     "factor_provider", "factor_pivots", "factor_diagnostics",
@@ -50,6 +50,10 @@ class DimensionMismatch(ValueError):
 
 class ArgumentError(ValueError):
     """Julia's ArgumentError."""
+
+
+class BoundsError(IndexError):
+    """Julia's BoundsError (an index range outside the operand)."""
 
 
 class DomainError(ValueError):
@@ -532,6 +536,28 @@ def mfdot(x: MFMatrix, y: MFMatrix) -> np.ndarray:
     return out.cpu().numpy()
 
 
+def syrk_packed_(packed: MFMatrix, panel: MFMatrix, alpha=1.0, beta=0.0, reduction_first: int = 1,
+                 reduction_last: Optional[int] = None,
+                 config: KernelConfig = _DEFAULT) -> MFMatrix:
+    """Packed lower triangle (column-major packed, (1,1),(2,1)..(n,1),(2,2)..)
+    = alpha * panel[rf:rl, :]^T panel[rf:rl, :] + beta * packed, with the
+    inclusive 1-based reduction bounds of src/kernels/syrk.jl:173-254."""
+    N = _same_type(packed, panel)
+    n, kp = panel.n, panel.m
+    if reduction_last is None:
+        reduction_last = kp
+    if packed.n != 1 or packed.m != n * (n + 1) // 2:
+        raise DimensionMismatch("syrk_packed! output length differs")
+    if not 1 <= reduction_first <= reduction_last <= kp:
+        raise BoundsError(f"reduction range {reduction_first}:{reduction_last} outside 1:{kp}")
+    _no_alias("syrk_packed!", packed, panel)
+    lib, h, s = _lib_h(packed)
+    _check(lib.mflab_syrk_packed(h, s, N, n, kp, reduction_first - 1, reduction_last, panel.ptr(),
+                                 panel.ld, panel.ls, packed.ptr(), packed.ls, _scalar(N, alpha),
+                                 _scalar(N, beta)), "syrk_packed!")
+    return packed
+
+
 def syrk_(C_: MFMatrix, P: MFMatrix, alpha=1.0, beta=0.0, uplo: str = "lower",
           config: KernelConfig = _DEFAULT) -> MFMatrix:
     """lower(C) = alpha*P^T*P + beta*C (src/kernels/syrk.jl:67-108)."""
@@ -605,6 +631,32 @@ def trsm_(B: MFMatrix, A: MFMatrix, alpha=1.0, side: str = "left", uplo: str = "
         rc = lib.mflab_trsm(h, s, N, _SIDE[side], _UPLO[uplo], _TRANS[trans], _DIAG[diag], B.m,
                             B.n, A.ptr(), A.ld, A.ls, B.ptr(), B.ld, B.ls, _scalar(N, alpha))
     _check(rc, "trsm!")
+    return B
+
+
+def trmm_(B: MFMatrix, A: MFMatrix, alpha=1.0, side: str = "left", uplo: str = "lower",
+          trans: str = "N", diag: str = "nonunit", config: KernelConfig = _DEFAULT) -> MFMatrix:
+    """B = alpha op(A) B or alpha B op(A) in place, reading only the uplo
+    triangle of A (src/kernels/trmm.jl:82-131)."""
+    N = _same_type(B, A)
+    if A.m != A.n:
+        raise DimensionMismatch("trmm! requires a square triangular matrix")
+    if side not in _SIDE:
+        raise ArgumentError("side must be :left or :right")
+    if uplo not in _UPLO:
+        raise ArgumentError("uplo must be :lower or :upper")
+    if trans not in _TRANS:
+        raise ArgumentError("trans must be :N or :T")
+    if diag not in _DIAG:
+        raise ArgumentError("diag must be :unit or :nonunit")
+    if side == "left" and B.m != A.m:
+        raise DimensionMismatch("trmm! left dimensions differ")
+    if side == "right" and B.n != A.m:
+        raise DimensionMismatch("trmm! right dimensions differ")
+    _no_alias("trmm!", B, A)
+    lib, h, s = _lib_h(B)
+    _check(lib.mflab_trmm(h, s, N, _SIDE[side], _UPLO[uplo], _TRANS[trans], _DIAG[diag], B.m, B.n,
+                          A.ptr(), A.ld, A.ls, B.ptr(), B.ld, B.ls, _scalar(N, alpha)), "trmm!")
     return B
 
 

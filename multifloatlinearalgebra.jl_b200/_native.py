@@ -63,6 +63,10 @@ SIGNATURES = {
     "mflab_gemm": [_vp, _vp, _int, _int, _i64, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _i64, _vp,
                    _i64, _i64, _d, _d],
     "mflab_syrk_lower": [_vp, _vp, _int, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _i64, _d, _d],
+    "mflab_syrk_packed": [_vp, _vp, _int, _i64, _i64, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _d,
+                          _d],
+    "mflab_trmm": [_vp, _vp, _int, _int, _int, _int, _int, _i64, _i64, _vp, _i64, _i64, _vp, _i64,
+                   _i64, _d],
     "mflab_gemmt_lower": [_vp, _vp, _int, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _i64, _vp, _i64,
                           _i64, _d, _d],
     "mflab_trsm": [_vp, _vp, _int, _int, _int, _int, _int, _i64, _i64, _vp, _i64, _i64, _vp, _i64,

@@ -41,10 +41,16 @@ struct MMShape {
 
 // TA: 0 a(i,k) = A[i,k]; 1 a(i,k) = A[k,i]; 2 symmetric from the lower
 // triangle (k <= i ? A[i,k] : A[k,i]); 3 symmetric from the upper triangle.
-template <int N, int BM, int BN, int BK, int TM, int TN, int TA, bool TB, bool TRI, bool FUSED>
+// mode bits: MM_PACKED C is a packed lower triangle (column-major
+// (0,0),(1,0)..(n-1,0),(1,1)..), limb stride C.ls; with TRMM the chain of
+// C(i,j) runs over k <= idx (or k >= idx with MM_KGE), idx = i (or j with
+// MM_RIGHT), and with MM_UNIT its diagonal term k == idx adds the other
+// operand's entry instead of a product (trmm.jl:1-80).
+template <int N, int BM, int BN, int BK, int TM, int TN, int TA, bool TB, bool TRI, bool FUSED,
+          bool TRMM>
 __global__ void __launch_bounds__(MMShape<N, BM, BN, BK, TM, TN>::NT)
     mm_kernel(int64_t m, int64_t n, int64_t K, Mat A, Mat B, Mat C, scal<N> alpha, scal<N> beta,
-              int overwrite, const int *info) {
+              int overwrite, const int *info, int mode) {
     using S = MMShape<N, BM, BN, BK, TM, TN>;
     constexpr int NT = S::NT, TX = S::TX, TY = S::TY;
     extern __shared__ double smem[];
@@ -55,6 +61,14 @@ __global__ void __launch_bounds__(MMShape<N, BM, BN, BK, TM, TN>::NT)
     const int64_t row0 = (int64_t)blockIdx.x * BM, col0 = (int64_t)blockIdx.y * BN;
     if (TRI && row0 + BM - 1 < col0) return;  // tile strictly above the diagonal
     if (info && *info) return;                 // an earlier factorization step failed
+    // reduction range of this tile: all of K, or the triangular part TRMM needs
+    int64_t kbeg = 0, kend = K;
+    if (TRMM) {
+        const bool right = mode & MM_RIGHT;
+        const int64_t lo = right ? col0 : row0, hi = right ? col0 + BN : row0 + BM;
+        if (mode & MM_KGE) kbeg = lo < K ? lo : K;
+        else kend = hi < K ? hi : K;
+    }
 
     mf<N> acc[TM][TN];
 #pragma unroll
@@ -73,7 +87,7 @@ __global__ void __launch_bounds__(MMShape<N, BM, BN, BK, TM, TN>::NT)
                 i = e / BK;
             }
             int64_t gi = row0 + i, gk = k0 + kk;
-            bool ok = gi < m && gk < K;
+            bool ok = gi < m && gk < kend;
             bool tr = TA == 1 || (TA == 2 && gk > gi) || (TA == 3 && gk < gi);
             const double *src = ok ? (tr ? A.p + gi * A.ld + gk : A.p + gk * A.ld + gi) : A.p;
 #pragma unroll
@@ -90,7 +104,7 @@ __global__ void __launch_bounds__(MMShape<N, BM, BN, BK, TM, TN>::NT)
                 kk = e / BN;
             }
             int64_t gj = col0 + j, gk = k0 + kk;
-            bool ok = gj < n && gk < K;
+            bool ok = gj < n && gk < kend;
             const double *src = ok ? (TB ? B.p + gk * B.ld + gj : B.p + gj * B.ld + gk) : B.p;
 #pragma unroll
             for (int l = 0; l < N; ++l)
@@ -98,7 +112,7 @@ __global__ void __launch_bounds__(MMShape<N, BM, BN, BK, TM, TN>::NT)
         }
     };
 
-    auto step = [&](int buf, int kk) {
+    auto step = [&](int buf, int kk, int64_t gk) {
         mf<N> a[TM], b[TN];
 #pragma unroll
         for (int i = 0; i < TM; ++i)
@@ -108,29 +122,46 @@ __global__ void __launch_bounds__(MMShape<N, BM, BN, BK, TM, TN>::NT)
         for (int j = 0; j < TN; ++j)
 #pragma unroll
             for (int l = 0; l < N; ++l) b[j].v[l] = Bs[((buf * N + l) * BK + kk) * BN + ty + j * TY];
+        if constexpr (!TRMM) {
 #pragma unroll
-        for (int i = 0; i < TM; ++i)
+            for (int i = 0; i < TM; ++i)
 #pragma unroll
-            for (int j = 0; j < TN; ++j) acc[i][j] = mac<N, FUSED>(acc[i][j], a[i], b[j]);
+                for (int j = 0; j < TN; ++j) acc[i][j] = mac<N, FUSED>(acc[i][j], a[i], b[j]);
+        } else {
+            const bool right = mode & MM_RIGHT, kge = mode & MM_KGE, unit = mode & MM_UNIT;
+#pragma unroll
+            for (int i = 0; i < TM; ++i)
+#pragma unroll
+                for (int j = 0; j < TN; ++j) {
+                    const int64_t idx = right ? col0 + ty + j * TY : row0 + tx + i * TX;
+                    if (gk == idx) {
+                        if (unit) acc[i][j] = add(acc[i][j], right ? a[i] : b[j]);
+                        else acc[i][j] = mac<N, false>(acc[i][j], a[i], b[j]);
+                    } else if (kge ? gk > idx : gk < idx) {
+                        acc[i][j] = mac<N, false>(acc[i][j], a[i], b[j]);
+                    }
+                }
+        }
     };
 
-    const int64_t nk = (K + BK - 1) / BK;
+    const int64_t nk = kend > kbeg ? (kend - kbeg + BK - 1) / BK : 0;
     if (nk > 0) {
-        load_tile(0, 0);
+        load_tile(0, kbeg);
         cp_async_commit();
     }
     for (int64_t kt = 0; kt < nk; ++kt) {
         const int buf = (int)(kt & 1);
-        if (kt + 1 < nk) load_tile(buf ^ 1, (kt + 1) * BK);
+        const int64_t k0 = kbeg + kt * BK;
+        if (kt + 1 < nk) load_tile(buf ^ 1, k0 + BK);
         cp_async_commit();
         cp_async_wait<1>();
         __syncthreads();
-        const int64_t rem = K - kt * BK;
+        const int64_t rem = kend - k0;
         if (rem >= BK) {
 #pragma unroll 2
-            for (int kk = 0; kk < BK; ++kk) step(buf, kk);
+            for (int kk = 0; kk < BK; ++kk) step(buf, kk, k0 + kk);
         } else {
-            for (int kk = 0; kk < (int)rem; ++kk) step(buf, kk);
+            for (int kk = 0; kk < (int)rem; ++kk) step(buf, kk, k0 + kk);
         }
         __syncthreads();
     }
@@ -143,18 +174,31 @@ __global__ void __launch_bounds__(MMShape<N, BM, BN, BK, TM, TN>::NT)
             const int64_t gi = row0 + tx + i * TX, gj = col0 + ty + j * TY;
             if (gi < m && gj < n && (!TRI || gi >= gj)) {
                 mf<N> r = mul(al, acc[i][j]);
-                if (!overwrite) r = add(r, mul(be, load_mf<N>(C.p, C.ld, C.ls, gi, gj)));
-                store_mf<N>(C.p, C.ld, C.ls, gi, gj, r);
+                if (mode & MM_PACKED) {
+                    double *c = C.p + gj * (2 * n - gj + 1) / 2 + (gi - gj);
+                    if (!overwrite) {
+                        mf<N> old;
+#pragma unroll
+                        for (int l = 0; l < N; ++l) old.v[l] = c[l * C.ls];
+                        r = add(r, mul(be, old));
+                    }
+#pragma unroll
+                    for (int l = 0; l < N; ++l) c[l * C.ls] = r.v[l];
+                } else {
+                    if (!overwrite) r = add(r, mul(be, load_mf<N>(C.p, C.ld, C.ls, gi, gj)));
+                    store_mf<N>(C.p, C.ld, C.ls, gi, gj, r);
+                }
             }
         }
     }
 }
 
-template <int N, int BM, int BN, int BK, int TM, int TN, int TA, bool TB, bool TRI, bool FUSED>
+template <int N, int BM, int BN, int BK, int TM, int TN, int TA, bool TB, bool TRI, bool FUSED,
+          bool TRMM>
 static int run_mm(int64_t m, int64_t n, int64_t k, Mat A, Mat B, Mat C, const double *alpha,
-                  const double *beta, cudaStream_t s, const int *info) {
+                  const double *beta, cudaStream_t s, const int *info, int mode) {
     using S = MMShape<N, BM, BN, BK, TM, TN>;
-    auto kern = mm_kernel<N, BM, BN, BK, TM, TN, TA, TB, TRI, FUSED>;
+    auto kern = mm_kernel<N, BM, BN, BK, TM, TN, TA, TB, TRI, FUSED, TRMM>;
     static bool configured = false;
     if (!configured) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -172,52 +216,75 @@ static int run_mm(int64_t m, int64_t n, int64_t k, Mat A, Mat B, Mat C, const do
     if (m <= 0 || n <= 0) return MFLAB_OK;
     dim3 grid((unsigned)((m + BM - 1) / BM), (unsigned)((n + BN - 1) / BN));
     if (grid.y > 65535) return MFLAB_ERR_UNSUPPORTED;
-    kern<<<grid, S::NT, S::smem_bytes, s>>>(m, n, k, A, B, C, al, be, overwrite, info);
+    kern<<<grid, S::NT, S::smem_bytes, s>>>(m, n, k, A, B, C, al, be, overwrite, info, mode);
     return record_cuda_error(cudaGetLastError(), "mm_kernel launch");
 }
 
 // tile shapes per limb count (FP64-issue bound; registers: TM*TN*N accumulators)
-template <int N, int TA, bool TB, bool TRI, bool FUSED>
+template <int N, int TA, bool TB, bool TRI, bool FUSED, bool TRMM = false>
 static int run_mm_n(int64_t m, int64_t n, int64_t k, Mat A, Mat B, Mat C, const double *alpha,
-                    const double *beta, cudaStream_t s, const int *info) {
+                    const double *beta, cudaStream_t s, const int *info, int mode) {
     if constexpr (N == 1)
-        return run_mm<1, 64, 64, 16, 4, 4, TA, TB, TRI, FUSED>(m, n, k, A, B, C, alpha, beta, s, info);
+        return run_mm<1, 64, 64, 16, 4, 4, TA, TB, TRI, FUSED, TRMM>(m, n, k, A, B, C, alpha, beta, s, info, mode);
     else if constexpr (N == 2)
-        return run_mm<2, 64, 64, 16, 4, 4, TA, TB, TRI, FUSED>(m, n, k, A, B, C, alpha, beta, s, info);
+        return run_mm<2, 64, 64, 16, 4, 4, TA, TB, TRI, FUSED, TRMM>(m, n, k, A, B, C, alpha, beta, s, info, mode);
     else if constexpr (N == 3)
-        return run_mm<3, 64, 64, 8, 4, 4, TA, TB, TRI, FUSED>(m, n, k, A, B, C, alpha, beta, s, info);
+        return run_mm<3, 64, 64, 8, 4, 4, TA, TB, TRI, FUSED, TRMM>(m, n, k, A, B, C, alpha, beta, s, info, mode);
     else
-        return run_mm<4, 64, 32, 8, 4, 2, TA, TB, TRI, FUSED>(m, n, k, A, B, C, alpha, beta, s, info);
+        return run_mm<4, 64, 32, 8, 4, 2, TA, TB, TRI, FUSED, TRMM>(m, n, k, A, B, C, alpha, beta, s, info, mode);
 }
 
 template <int N>
 static int dispatch_mm(int ta, bool tb, int tri, bool fused3, int64_t m, int64_t n, int64_t k,
                        Mat A, Mat B, Mat C, const double *alpha, const double *beta,
-                       cudaStream_t s, const int *info) {
+                       cudaStream_t s, const int *info, int mode) {
     if (ta == 0 && !tb && !tri) {
         if (N == 3 && fused3)
-            return run_mm_n<N, 0, false, false, true>(m, n, k, A, B, C, alpha, beta, s, info);
-        return run_mm_n<N, 0, false, false, false>(m, n, k, A, B, C, alpha, beta, s, info);
+            return run_mm_n<N, 0, false, false, true>(m, n, k, A, B, C, alpha, beta, s, info, mode);
+        return run_mm_n<N, 0, false, false, false>(m, n, k, A, B, C, alpha, beta, s, info, mode);
     }
-    if (ta == 1 && !tb && tri) return run_mm_n<N, 1, false, true, false>(m, n, k, A, B, C, alpha, beta, s, info);
-    if (ta == 1 && !tb && !tri) return run_mm_n<N, 1, false, false, false>(m, n, k, A, B, C, alpha, beta, s, info);
-    if (ta == 0 && tb && tri) return run_mm_n<N, 0, true, true, false>(m, n, k, A, B, C, alpha, beta, s, info);
-    if (ta == 2 && !tb && !tri) return run_mm_n<N, 2, false, false, false>(m, n, k, A, B, C, alpha, beta, s, info);
-    if (ta == 3 && !tb && !tri) return run_mm_n<N, 3, false, false, false>(m, n, k, A, B, C, alpha, beta, s, info);
+    if (ta == 1 && !tb && tri) return run_mm_n<N, 1, false, true, false>(m, n, k, A, B, C, alpha, beta, s, info, mode);
+    if (ta == 1 && !tb && !tri) return run_mm_n<N, 1, false, false, false>(m, n, k, A, B, C, alpha, beta, s, info, mode);
+    if (ta == 0 && tb && tri) return run_mm_n<N, 0, true, true, false>(m, n, k, A, B, C, alpha, beta, s, info, mode);
+    if (ta == 2 && !tb && !tri) return run_mm_n<N, 2, false, false, false>(m, n, k, A, B, C, alpha, beta, s, info, mode);
+    if (ta == 3 && !tb && !tri) return run_mm_n<N, 3, false, false, false>(m, n, k, A, B, C, alpha, beta, s, info, mode);
     return MFLAB_ERR_UNSUPPORTED;
 }
 
 int launch_mm(int N, int ta, bool tb, int tri, bool fused3, int64_t m, int64_t n, int64_t k,
               Mat A, Mat B, Mat C, const double *alpha, const double *beta, cudaStream_t s,
-              const int *info) {
+              const int *info, int mode) {
     switch (N) {
     case 1:
         if (ta == 0 && !tb && !tri)
-            return run_mm_n<1, 0, false, false, false>(m, n, k, A, B, C, alpha, beta, s, info);
+            return run_mm_n<1, 0, false, false, false>(m, n, k, A, B, C, alpha, beta, s, info, mode);
         return MFLAB_ERR_UNSUPPORTED;
-    case 2: return dispatch_mm<2>(ta, tb, tri, fused3, m, n, k, A, B, C, alpha, beta, s, info);
-    case 3: return dispatch_mm<3>(ta, tb, tri, fused3, m, n, k, A, B, C, alpha, beta, s, info);
-    case 4: return dispatch_mm<4>(ta, tb, tri, fused3, m, n, k, A, B, C, alpha, beta, s, info);
+    case 2: return dispatch_mm<2>(ta, tb, tri, fused3, m, n, k, A, B, C, alpha, beta, s, info, mode);
+    case 3: return dispatch_mm<3>(ta, tb, tri, fused3, m, n, k, A, B, C, alpha, beta, s, info, mode);
+    case 4: return dispatch_mm<4>(ta, tb, tri, fused3, m, n, k, A, B, C, alpha, beta, s, info, mode);
+    default: return MFLAB_ERR_UNSUPPORTED;
+    }
+}
+
+// C = alpha * a * b with the triangular chain of the mode bits (beta = 0):
+// left products a = op(A) (ta 0/1), b = the saved B; right products a = the
+// saved B, b = op(A) (tb 0/1).
+template <int N>
+static int dispatch_trmm(int ta, bool tb, int64_t m, int64_t n, int64_t k, Mat A, Mat B, Mat C,
+                         const double *alpha, const double *zero, cudaStream_t s, int mode) {
+    if (ta == 0 && !tb) return run_mm_n<N, 0, false, false, false, true>(m, n, k, A, B, C, alpha, zero, s, nullptr, mode);
+    if (ta == 1 && !tb) return run_mm_n<N, 1, false, false, false, true>(m, n, k, A, B, C, alpha, zero, s, nullptr, mode);
+    if (ta == 0 && tb) return run_mm_n<N, 0, true, false, false, true>(m, n, k, A, B, C, alpha, zero, s, nullptr, mode);
+    return MFLAB_ERR_UNSUPPORTED;
+}
+
+int launch_trmm_mm(int N, int ta, bool tb, int mode, int64_t m, int64_t n, int64_t k, Mat A, Mat B,
+                   Mat C, const double *alpha, cudaStream_t s) {
+    const double zero[4] = {0.0, 0.0, 0.0, 0.0};
+    switch (N) {
+    case 2: return dispatch_trmm<2>(ta, tb, m, n, k, A, B, C, alpha, zero, s, mode);
+    case 3: return dispatch_trmm<3>(ta, tb, m, n, k, A, B, C, alpha, zero, s, mode);
+    case 4: return dispatch_trmm<4>(ta, tb, m, n, k, A, B, C, alpha, zero, s, mode);
     default: return MFLAB_ERR_UNSUPPORTED;
     }
 }
@@ -327,6 +394,62 @@ extern "C" int mflab_dot(mflab_handle *h, void *stream, int limbs, int64_t m, in
     default: mfl::dot_kernel<4><<<1, 1, 0, s>>>(m, n, X, Y, out); break;
     }
     return mfl::record_cuda_error(cudaGetLastError(), "dot");
+}
+
+// packed lower(C) = alpha * P[k0:k1, :]^T P[k0:k1, :] + beta * packed lower(C)
+// (syrk.jl:110-254): the SYRK chains over the reduction rows k0 .. k1-1, stored
+// column-major packed, (0,0),(1,0)..(n-1,0),(1,1)..; limb stride lsc.
+extern "C" int mflab_syrk_packed(mflab_handle *h, void *stream, int limbs, int64_t n, int64_t kp,
+                                 int64_t k0, int64_t k1, const double *P, int64_t ldp, int64_t lsp,
+                                 double *C, int64_t lsc, const double *alpha, const double *beta) {
+    if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
+    if (n < 0 || kp < 0 || !alpha || !beta) return MFLAB_ERR_ARG;
+    if (!(0 <= k0 && k0 < k1 && k1 <= kp)) return MFLAB_ERR_ARG;
+    if (n == 0) return MFLAB_OK;
+    const int64_t len = n * (n + 1) / 2;
+    if (ldp < kp || lsc < len) return MFLAB_ERR_ARG;
+    if (mfl::views_overlap(C, len, lsc, len, 1, limbs, P, ldp, lsp, kp, n)) return MFLAB_ERR_ALIAS;
+    return mfl::launch_mm(limbs, true, false, 1, false, n, n, k1 - k0,
+                          Mat{(double *)P + k0, ldp, lsp}, Mat{(double *)P + k0, ldp, lsp},
+                          Mat{C, len, lsc}, alpha, beta, (cudaStream_t)stream, nullptr,
+                          mfl::MM_PACKED);
+}
+
+// B = alpha * op(A) * B (side 0) or alpha * B * op(A) (side 1), in place
+// (trmm.jl:82-131).  Each B(i,j) is one ascending chain over the triangle of
+// op(A) (trmm.jl:1-80): left lower k = 0..i, left upper k = i..m-1, right
+// lower k = j..n-1, right upper k = 0..j, the diagonal term B(i,j) itself for
+// diag = unit.  B is saved to the handle's scratch and the product written
+// back, so every chain reads the original B.
+extern "C" int mflab_trmm(mflab_handle *h, void *stream, int limbs, int side, int uplo, int trans,
+                          int diag, int64_t m, int64_t n, const double *A, int64_t lda,
+                          int64_t lsa, double *B, int64_t ldb, int64_t lsb, const double *alpha) {
+    if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
+    if (m < 0 || n < 0 || !alpha || (side | uplo | trans | diag) & ~1) return MFLAB_ERR_ARG;
+    const int64_t na = side ? n : m;
+    if (m == 0 || n == 0) return MFLAB_OK;
+    if (lda < na || ldb < m) return MFLAB_ERR_ARG;
+    if (mfl::views_overlap(B, ldb, lsb, m, n, limbs, A, lda, lsa, na, na)) return MFLAB_ERR_ALIAS;
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t plane = (size_t)m * n;
+    int rc = mflab_reserve_scratch(h, plane * limbs * sizeof(double));
+    if (rc) return rc;
+    double *saved = (double *)h->scratch;
+    for (int l = 0; l < limbs; ++l) {
+        cudaError_t e = cudaMemcpy2DAsync(saved + l * plane, m * sizeof(double), B + l * lsb,
+                                          ldb * sizeof(double), m * sizeof(double), n,
+                                          cudaMemcpyDeviceToDevice, s);
+        if (e != cudaSuccess) return mfl::record_cuda_error(e, "trmm save");
+    }
+    const Mat Bs{saved, m, (int64_t)plane}, Am{(double *)A, lda, lsa}, Bm{B, ldb, lsb};
+    const bool eff_lower = (uplo == 0) == (trans == 0);
+    const int unit = diag ? mfl::MM_UNIT : 0;
+    if (side == 0)
+        return mfl::launch_trmm_mm(limbs, trans, false, (eff_lower ? 0 : mfl::MM_KGE) | unit, m,
+                                   n, m, Am, Bs, Bm, alpha, s);
+    return mfl::launch_trmm_mm(limbs, 0, trans != 0,
+                               mfl::MM_RIGHT | (eff_lower ? mfl::MM_KGE : 0) | unit, m, n, n, Bs,
+                               Am, Bm, alpha, s);
 }
 
 extern "C" int mflab_syrk_lower(mflab_handle *h, void *stream, int limbs, int64_t n, int64_t k,

@@ -19,9 +19,14 @@ struct Mat {
 //   a(i,k): ta 0 A[i,k], 1 A[k,i], 2 symmetric from the lower triangle,
 //           3 symmetric from the upper triangle;   b(k,j) = tb ? B[j,k] : B[k,j]
 // tri == 1 writes only C(i,j) with i >= j (SYRK / GEMMT lower triangle).
+enum { MM_PACKED = 1, MM_RIGHT = 2, MM_KGE = 4, MM_UNIT = 8 };
 int launch_mm(int N, int ta, bool tb, int tri, bool fused3, int64_t m, int64_t n, int64_t k,
               Mat A, Mat B, Mat C, const double *alpha, const double *beta, cudaStream_t s,
-              const int *info = nullptr);
+              const int *info = nullptr, int mode = 0);
+// triangular products (trmm.jl): C(i,j) = alpha * chain over the k range the
+// MM_RIGHT / MM_KGE / MM_UNIT bits select; C must not overlap A or B.
+int launch_trmm_mm(int N, int ta, bool tb, int mode, int64_t m, int64_t n, int64_t k, Mat A, Mat B,
+                   Mat C, const double *alpha, cudaStream_t s);
 
 // Triangular solve (trsm.jl semantics); returns an MFLAB_* code.
 int launch_trsm(int N, int side, int uplo, int trans, int diag, int64_t m, int64_t n, Mat A, Mat B,

@@ -15,12 +15,20 @@ import torch
 
 
 def _renorm_np(X: np.ndarray) -> np.ndarray:
+    """bottom-up FastTwoSum passes until none changes a limb: every adjacent
+    pair then satisfies |x[l]| <= ulp(x[l-1]) / 2 (a pass can move a limb
+    down and leave it overlapping the one below, so a fixed number of passes
+    is not enough for four limbs)"""
     N = X.shape[0]
-    for _ in range(2):
+    for _ in range(4 * N):
+        changed = False
         for lvl in range(N - 1, 0, -1):
             s = X[lvl - 1] + X[lvl]
             e = X[lvl] - (s - X[lvl - 1])
+            changed = changed or not (np.array_equal(s, X[lvl - 1]) and np.array_equal(e, X[lvl]))
             X[lvl - 1], X[lvl] = s, e
+        if not changed:
+            break
     return X
 
 
@@ -38,12 +46,16 @@ def randn_mf(rng: np.random.Generator, N: int, m: int, n: int, spread: float = 0
 
 def _renorm_torch(X: torch.Tensor) -> torch.Tensor:
     N = X.shape[0]
-    for _ in range(2):
+    for _ in range(4 * N):
+        changed = False
         for lvl in range(N - 1, 0, -1):
             a, b = X[lvl - 1].clone(), X[lvl].clone()
             s = a + b
             e = b - (s - a)
+            changed = changed or not (torch.equal(s, a) and torch.equal(e, b))
             X[lvl - 1], X[lvl] = s, e
+        if not changed:
+            break
     return X
 
 

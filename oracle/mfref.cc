@@ -414,6 +414,38 @@ par_for(n, threads, [&](int64_t col) {
     return 0;
 }
 
+/* packed lower triangle of C (column-major packed, (0,0),(1,0)..(n-1,0),(1,1)..,
+   limb stride lsc) = alpha * P[k0:k1,:]^T P[k0:k1,:] + beta * C
+   (syrk.jl:110-254, _packed_lower_index syrk.jl:110-117): the SYRK chain over
+   the reduction rows k0..k1-1 in ascending order. */
+int mfr_syrk_packed(int N, int64_t n, int64_t k0, int64_t k1, const double *P, int64_t ldp,
+                    int64_t lsp, double *C, int64_t lsc, const double *alpha, const double *beta,
+                    int threads) {
+    int overwrite = mf_iszero(N, beta);
+    par_for(n, threads, [&](int64_t col) {
+        int64_t idx = col * (2 * n - col + 1) / 2;
+        for (int64_t row = col; row < n; ++row, ++idx) {
+            double acc[MAXN], a[MAXN], b[MAXN], res[MAXN], cv[MAXN];
+            mf_set(N, 0.0, acc);
+            for (int64_t kk = k0; kk < k1; ++kk) {
+                getm(N, P, ldp, lsp, kk, row, a);
+                getm(N, P, ldp, lsp, kk, col, b);
+                double p[MAXN];
+                mf_mul(N, a, b, p);
+                mf_add(N, acc, p, acc);
+            }
+            mf_mul(N, alpha, acc, res);
+            if (!overwrite) {
+                getm(N, C, 1, lsc, idx, 0, cv);
+                mf_mul(N, beta, cv, cv);
+                mf_add(N, res, cv, res);
+            }
+            putm(N, C, 1, lsc, idx, 0, res);
+        }
+    });
+    return 0;
+}
+
 /* lower triangle of C = alpha * A * B^T + beta * C, A and B are n x k
    (gemmt.jl:1-52): chain of A[row,k]*B[col,k]. */
 int mfr_gemmt_lower(int N, int64_t n, int64_t k, const double *A, int64_t lda, int64_t lsa,
@@ -450,6 +482,72 @@ static inline void trsm_coef(int N, const double *A, int64_t lda, int64_t lsa, i
         getm(N, A, lda, lsa, c, r, out);
     else
         getm(N, A, lda, lsa, r, c, out);
+}
+
+/* B = alpha * op(A) * B (side 0) or alpha * B * op(A) (side 1) in place
+   (trmm.jl:1-131), in the reference's element order so every chain reads
+   B entries that are not yet overwritten: left, effective lower: rows
+   bottom-up, chain coef(i,k) B[k,j] for k = 0..i-1, then the diagonal term;
+   left, effective upper: diagonal term, then k = i+1..m-1; right, effective
+   lower: columns left to right, diagonal term B[i,j] A[j,j] then B[i,k]
+   coef(k,j) for k = j+1..n-1; right, effective upper: columns right to left,
+   k = 0..j-1, then the diagonal term.  diag = unit adds B[i,j] itself. */
+int mfr_trmm(int N, int side, int uplo, int trans, int diag, int64_t m, int64_t n,
+             const double *A, int64_t lda, int64_t lsa, double *B, int64_t ldb, int64_t lsb,
+             const double *alpha, int threads) {
+    const int eff_lower = (uplo == 0) == (trans == 0);
+    auto diag_term = [&](int64_t i, int64_t j, int64_t d, double *acc) {
+        double bv[MAXN], av[MAXN], p[MAXN];
+        getm(N, B, ldb, lsb, i, j, bv);
+        if (diag) {
+            mf_add(N, acc, bv, acc);
+            return;
+        }
+        getm(N, A, lda, lsa, d, d, av);
+        if (side == 0) mf_mul(N, av, bv, p);
+        else mf_mul(N, bv, av, p);
+        mf_add(N, acc, p, acc);
+    };
+    if (side == 0) {
+        par_for(n, threads, [&](int64_t j) {
+            for (int64_t t = 0; t < m; ++t) {
+                const int64_t i = eff_lower ? m - 1 - t : t;
+                double acc[MAXN], c[MAXN], bv[MAXN], p[MAXN], res[MAXN];
+                mf_set(N, 0.0, acc);
+                if (!eff_lower) diag_term(i, j, i, acc);
+                const int64_t lo = eff_lower ? 0 : i + 1, hi = eff_lower ? i : m;
+                for (int64_t k = lo; k < hi; ++k) {
+                    trsm_coef(N, A, lda, lsa, i, k, trans, c);
+                    getm(N, B, ldb, lsb, k, j, bv);
+                    mf_mul(N, c, bv, p);
+                    mf_add(N, acc, p, acc);
+                }
+                if (eff_lower) diag_term(i, j, i, acc);
+                mf_mul(N, alpha, acc, res);
+                putm(N, B, ldb, lsb, i, j, res);
+            }
+        });
+    } else {
+        par_for(m, threads, [&](int64_t i) {
+            for (int64_t t = 0; t < n; ++t) {
+                const int64_t j = eff_lower ? t : n - 1 - t;
+                double acc[MAXN], c[MAXN], bv[MAXN], p[MAXN], res[MAXN];
+                mf_set(N, 0.0, acc);
+                if (eff_lower) diag_term(i, j, j, acc);
+                const int64_t lo = eff_lower ? j + 1 : 0, hi = eff_lower ? n : j;
+                for (int64_t k = lo; k < hi; ++k) {
+                    getm(N, B, ldb, lsb, i, k, bv);
+                    trsm_coef(N, A, lda, lsa, k, j, trans, c);
+                    mf_mul(N, bv, c, p);
+                    mf_add(N, acc, p, acc);
+                }
+                if (!eff_lower) diag_term(i, j, j, acc);
+                mf_mul(N, alpha, acc, res);
+                putm(N, B, ldb, lsb, i, j, res);
+            }
+        });
+    }
+    return 0;
 }
 
 /* side: 0 left, 1 right; uplo: 0 lower, 1 upper; trans: 0 N, 1 T; diag: 0

@@ -72,6 +72,9 @@ def lib():
                             _d, _d, C.c_int],
         "mfr_trsm": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _i64, _i64, _d, _i64, _i64, _d,
                      _i64, _i64, _d, C.c_int],
+        "mfr_trmm": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _i64, _i64, _d, _i64, _i64, _d,
+                     _i64, _i64, _d, C.c_int],
+        "mfr_syrk_packed": [C.c_int, _i64, _i64, _i64, _d, _i64, _i64, _d, _i64, _d, _d, C.c_int],
         "mfr_potrf": [C.c_int, _i64, _d, _i64, _i64, _i64, C.c_int],
         "mfr_potrs": [C.c_int, _i64, _i64, _d, _i64, _i64, _d, _i64, _i64, C.c_int],
         "mfr_getrf": [C.c_int, _i64, _i64, _d, _i64, _i64, _pi64, _i64, C.c_int],
@@ -243,6 +246,32 @@ def trsm(B, A, alpha=1.0, side="left", uplo="lower", trans="N", diag="nonunit", 
     lib().mfr_trsm(N, _SIDE[side], _UPLO[uplo], _TRANS[trans], _DIAG[diag], Bp.m, Bp.n, Ap.ptr(),
                    Ap.ld, Ap.ls, Bp.ptr(), Bp.ld, Bp.ls, _p(al), nthreads or threads())
     return Bp.array()
+
+
+def trmm(B, A, alpha=1.0, side="left", uplo="lower", trans="N", diag="nonunit", nthreads=None):
+    """trmm.jl:82-131; returns the product that overwrites B."""
+    Bp, Ap = Planes(B), Planes(A)
+    N = Bp.N
+    al = _scalar(N, alpha)
+    lib().mfr_trmm(N, _SIDE[side], _UPLO[uplo], _TRANS[trans], _DIAG[diag], Bp.m, Bp.n, Ap.ptr(),
+                   Ap.ld, Ap.ls, Bp.ptr(), Bp.ld, Bp.ls, _p(al), nthreads or threads())
+    return Bp.array()
+
+
+def syrk_packed(packed, P, alpha=1.0, beta=0.0, reduction_first=1, reduction_last=None,
+                nthreads=None):
+    """syrk.jl:173-254: packed (N, n(n+1)/2) lower triangle of
+    alpha * P[rf:rl,:]^T P[rf:rl,:] + beta * packed, 1-based inclusive bounds."""
+    Pp = Planes(P)
+    N, n = Pp.N, Pp.n
+    rl = Pp.m if reduction_last is None else reduction_last
+    out = np.ascontiguousarray(np.asarray(packed, dtype=np.float64).reshape(N, -1).copy())
+    assert out.shape[1] == n * (n + 1) // 2 and 1 <= reduction_first <= rl <= Pp.m
+    al, be = _scalar(N, alpha), _scalar(N, beta)
+    lib().mfr_syrk_packed(N, n, reduction_first - 1, rl, Pp.ptr(), Pp.ld, Pp.ls,
+                          out.ctypes.data_as(C.POINTER(C.c_double)), out.shape[1], _p(al), _p(be),
+                          nthreads or threads())
+    return out
 
 
 # ------------------------------------------------------- factorizations --
