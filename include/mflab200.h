@@ -309,6 +309,17 @@ int mflab_backward_error_norm(mflab_handle *h, void *stream, int limbs, int64_t 
 int mflab_potrf(mflab_handle *h, void *stream, int limbs, int64_t n, double *A, int64_t lda,
                 int64_t lsa, int64_t block, int *info);
 
+/* Rank-revealing pivoted Cholesky in place: the lower triangle is read,
+   mirrored, and factored with symmetric diagonal pivoting; tol (host, limbs
+   doubles, finite, >= 0) is the relative pivot threshold.  perm (device
+   int64[n], 1-based) receives the symmetric permutation and rank_info
+   (device int64[2]) the retained rank and the status: 0, -1 non-finite lower
+   triangle (A unchanged), k > 0 the first non-positive pivot.
+   Replaces cholesky_pivoted!(A; tol, check=false) —
+   src/factorizations/cholesky_pivoted.jl:65-175. */
+int mflab_pstrf(mflab_handle *h, void *stream, int limbs, int64_t n, double *A, int64_t lda,
+                int64_t lsa, const double *tol, int64_t *perm, int64_t *rank_info);
+
 /* B <- S^{-1} B with a successful Cholesky factor L (n x n), B n x nrhs.
    Replaces ldiv!(B, F::MFCholesky) — src/solve.jl:54-83 (vector form :23-50). */
 int mflab_potrs(mflab_handle *h, void *stream, int limbs, int64_t n, int64_t nrhs,

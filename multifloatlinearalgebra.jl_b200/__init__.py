@@ -32,7 +32,8 @@ __all__ = [
     "MFMatrix", "KernelConfig", "DimensionMismatch", "ArgumentError", "DomainError",
     "PosDefException", "SingularException", "MFLABError",
     "gemm_", "syrk_", "gemmt_", "trsm_", "trsv_", "gemm_plan", "OpNormInf", "gemv_", "symv_",
-    "mfdot", "syrk_packed_", "trmm_", "BoundsError",
+    "mfdot", "syrk_packed_", "trmm_", "BoundsError", "cholesky_pivoted_", "MFCholeskyPivoted",
+    "factor_rdiag",
     "cholesky_", "lu_", "ldiv_", "solve", "issuccess",
     "factor_status", "factor_state", "factor_kind", "factor_matrix", "factor_precision",
     "factor_provider", "factor_pivots", "factor_diagnostics",
@@ -692,6 +693,17 @@ class MFCholesky(_Factor):
     kind = "cholesky"
 
 
+class MFCholeskyPivoted(_Factor):
+    """Rank-revealing pivoted Cholesky: the lower triangle of factors holds L,
+    A[p, p] ~ L[:, :rank] L[:, :rank]^T (src/factorizations/cholesky_pivoted.jl:1-22)."""
+    kind = "cholesky_pivoted"
+
+    def __init__(self, factors: MFMatrix, permutation: torch.Tensor, rank: int, info: int):
+        super().__init__(factors, info)
+        self.permutation = permutation
+        self.rank = int(rank)
+
+
 class MFLU(_Factor):
     """Partial-pivoting LU factor (src/factorizations/lu.jl:1-14)."""
     kind = "lu"
@@ -752,6 +764,44 @@ def cholesky_(A: MFMatrix, check: bool = True, config: KernelConfig = _DEFAULT) 
     if st > 0 and check:
         raise PosDefException(st)
     return MFCholesky(A, st)
+
+
+def cholesky_pivoted_(A: MFMatrix, tol=0.0, check: bool = True,
+                      config: KernelConfig = _DEFAULT) -> MFCholeskyPivoted:
+    """Rank-revealing pivoted Cholesky in place; tol is the relative pivot
+    threshold, a tolerance stop is reported by rank, not by the status
+    (src/factorizations/cholesky_pivoted.jl:65-175)."""
+    N = _same_type(A)
+    n = A.m
+    if A.n != n:
+        raise DimensionMismatch("cholesky_pivoted! requires a square matrix")
+    t = np.zeros(N)
+    tv = np.atleast_1d(np.asarray(tol, dtype=np.float64)).ravel()
+    if len(tv) > N:
+        raise ArgumentError("tol has more limbs than the matrix type")
+    t[:len(tv)] = tv
+    if not np.all(np.isfinite(t)) or t[0] < 0 or (t[0] == 0 and np.any(t[1:] < 0)):
+        raise ArgumentError("tol must be finite and nonnegative")
+    dev = A.storage.device
+    perm = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
+    rank_info = torch.zeros(2, dtype=torch.int64, device=dev)
+    lib, h, s = _lib_h(A)
+    _check(lib.mflab_pstrf(h, s, N, n, A.ptr(), A.ld, A.ls, _scalar(N, t), perm.data_ptr(),
+                           rank_info.data_ptr()), "cholesky_pivoted!")
+    rank, info = (int(v) for v in rank_info.cpu().tolist())
+    if info == -1 and check:
+        raise DomainError("cholesky_pivoted!: input matrix contains non-finite entries")
+    if info > 0 and check:
+        raise PosDefException(info)
+    return MFCholeskyPivoted(A, perm[:n], rank, info)
+
+
+def factor_rdiag(F: _Factor) -> np.ndarray:
+    """copy of the stored diagonal pivots, (N, min(m, n)) limbs
+    (src/factorizations/cholesky_pivoted.jl:40-48)"""
+    A = F.factors
+    view = A.storage[:, A.c0:A.c0 + A.n, A.r0:A.r0 + A.m]
+    return torch.diagonal(view, dim1=1, dim2=2).cpu().numpy().copy()
 
 
 def lu_(A: MFMatrix, check: bool = True, config: KernelConfig = _DEFAULT,
@@ -853,8 +903,12 @@ def factor_blocks(F: MFLDLT) -> np.ndarray:
     return F.blocks.cpu().numpy().copy()
 
 
-def factor_permutation(F: MFLDLT) -> np.ndarray:
-    """final symmetric permutation p with A[p, p] = L D L^T, 1-based (ldlt.jl:34-63)"""
+def factor_permutation(F: _Factor) -> np.ndarray:
+    """final symmetric permutation p, 1-based: A[p, p] = L D L^T for LDLT
+    (ldlt.jl:34-63), the retained block of A[p, p] for pivoted Cholesky
+    (cholesky_pivoted.jl:30-38)"""
+    if isinstance(F, MFCholeskyPivoted):
+        return F.permutation.cpu().numpy().copy()
     blocks = F.blocks.cpu().numpy()
     piv = F.pivots.cpu().numpy()
     n = len(blocks)
@@ -928,7 +982,7 @@ def factor_state(F: _Factor) -> str:
         return "nonfinite_input"
     if st < 0:
         return "numerical_breakdown"
-    if F.kind == "cholesky":
+    if F.kind in ("cholesky", "cholesky_pivoted"):
         return "not_posdef"
     if F.kind in ("lu", "ldlt"):
         return "singular"
@@ -1031,6 +1085,22 @@ def factor_diagnostics(F: _Factor) -> dict:
         has = accepted > 0
         base.update({
             "accepted_pivots": accepted,
+            "minimum_diagonal": mn if has else None,
+            "maximum_diagonal": mx if has else None,
+            "diagonal_spread": spread if has else None,
+            "finite": _finite_region(A, 1),
+        })
+        return base
+    if F.kind == "cholesky_pivoted":
+        # diagnostics.jl:53-70: the retained rank is the accepted pivot count
+        accepted = F.rank
+        _check(lib.mflab_diag_summary(h, s, N, A.ptr(), A.ld, A.ls, accepted, None, None,
+                                      out.data_ptr()), "factor_diagnostics")
+        mn, mx, spread, _ = _mf_values(out, N, 4)
+        has = accepted > 0
+        base.update({
+            "rank": accepted,
+            "permutation": factor_permutation(F),
             "minimum_diagonal": mn if has else None,
             "maximum_diagonal": mx if has else None,
             "diagonal_spread": spread if has else None,

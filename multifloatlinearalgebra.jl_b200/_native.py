@@ -72,6 +72,7 @@ SIGNATURES = {
     "mflab_trsm": [_vp, _vp, _int, _int, _int, _int, _int, _i64, _i64, _vp, _i64, _i64, _vp, _i64,
                    _i64, _d],
     "mflab_potrf": [_vp, _vp, _int, _i64, _vp, _i64, _i64, _i64, _vp],
+    "mflab_pstrf": [_vp, _vp, _int, _i64, _vp, _i64, _i64, _d, _vp, _vp],
     "mflab_potrs": [_vp, _vp, _int, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _i64],
     "mflab_getrf": [_vp, _vp, _int, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _vp],
     "mflab_getrs": [_vp, _vp, _int, _i64, _i64, _vp, _i64, _i64, _vp, _vp, _i64, _i64],

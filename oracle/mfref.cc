@@ -725,6 +725,117 @@ par_for(t, threads, [&](int64_t col) {
 }
 
 /* B <- A^{-1} B with a Cholesky factor (solve.jl:54-83) */
+/* Rank-revealing pivoted Cholesky (cholesky_pivoted.jl:65-175), in place.
+   perm (1-based) and out[0] = rank, out[1] = info (0, -1 non-finite lower
+   triangle with A unchanged, k > 0 first non-positive pivot).  The lower
+   triangle is mirrored once; each step picks the first largest remaining
+   diagonal, swaps rows then columns, stores sqrt at (k,k), divides the column
+   below and applies the full-square rank-one update A[r,c] -= A[r,k]*A[c,k]. */
+int mfr_pstrf(int N, int64_t n, double *A, int64_t lda, int64_t lsa, const double *tol,
+              int64_t *perm, int64_t *out, int threads) {
+    for (int64_t c = 0; c < n; ++c)
+        for (int64_t r = c; r < n; ++r) {
+            double v[MAXN];
+            getm(N, A, lda, lsa, r, c, v);
+            if (!mf_isfinite(N, v)) {
+                for (int64_t i = 0; i < n; ++i) perm[i] = i + 1;
+                out[0] = 0;
+                out[1] = -1;
+                return 0;
+            }
+        }
+    for (int64_t c = 0; c < n; ++c)
+        for (int64_t r = 0; r < c; ++r) {
+            double v[MAXN];
+            getm(N, A, lda, lsa, c, r, v);
+            putm(N, A, lda, lsa, r, c, v);
+        }
+    for (int64_t i = 0; i < n; ++i) perm[i] = i + 1;
+    int64_t rank = n, info = 0;
+    double zero[MAXN], first[MAXN];
+    mf_set(N, 0.0, zero);
+    mf_set(N, 0.0, first);
+    const int use_tol = !mf_iszero(N, tol);
+    for (int64_t k = 0; k < n; ++k) {
+        int64_t p = k;
+        double pd[MAXN], cand[MAXN], piv[MAXN];
+        getm(N, A, lda, lsa, k, k, pd);
+        for (int64_t i = k + 1; i < n; ++i) {
+            getm(N, A, lda, lsa, i, i, cand);
+            if (mf_gt(N, cand, pd)) {
+                p = i;
+                memcpy(pd, cand, sizeof(double) * N);
+            }
+        }
+        if (k == 0) {
+            if (!mf_gt(N, pd, zero)) {
+                rank = 0;
+                info = 1;
+                break;
+            }
+            mf_sqrt(N, pd, first);
+        }
+        if (mf_ge(N, zero, pd)) {
+            double thr[MAXN], thr2[MAXN], apd[MAXN];
+            mf_mul(N, tol, first, thr);
+            mf_mul(N, thr, thr, thr2);
+            mf_abs(N, pd, apd);
+            rank = k;
+            if (!(use_tol && mf_ge(N, thr2, apd))) info = k + 1;
+            break;
+        }
+        mf_sqrt(N, pd, piv);
+        if (use_tol) {
+            double lim[MAXN];
+            mf_mul(N, tol, first, lim);
+            if (mf_ge(N, lim, piv)) {
+                rank = k;
+                break;
+            }
+        }
+        if (p != k) {
+            for (int64_t c = 0; c < n; ++c) {
+                double a[MAXN], b[MAXN];
+                getm(N, A, lda, lsa, k, c, a);
+                getm(N, A, lda, lsa, p, c, b);
+                putm(N, A, lda, lsa, k, c, b);
+                putm(N, A, lda, lsa, p, c, a);
+            }
+            for (int64_t r = 0; r < n; ++r) {
+                double a[MAXN], b[MAXN];
+                getm(N, A, lda, lsa, r, k, a);
+                getm(N, A, lda, lsa, r, p, b);
+                putm(N, A, lda, lsa, r, k, b);
+                putm(N, A, lda, lsa, r, p, a);
+            }
+            const int64_t t = perm[k];
+            perm[k] = perm[p];
+            perm[p] = t;
+        }
+        putm(N, A, lda, lsa, k, k, piv);
+        for (int64_t r = k + 1; r < n; ++r) {
+            double v[MAXN];
+            getm(N, A, lda, lsa, r, k, v);
+            mf_div(N, v, piv, v);
+            putm(N, A, lda, lsa, r, k, v);
+        }
+        par_for(n - k - 1, threads, [&](int64_t cc) {
+            const int64_t c = k + 1 + cc;
+            double f[MAXN], lr[MAXN], v[MAXN];
+            getm(N, A, lda, lsa, c, k, f);
+            for (int64_t r = k + 1; r < n; ++r) {
+                getm(N, A, lda, lsa, r, k, lr);
+                getm(N, A, lda, lsa, r, c, v);
+                mf_submul(N, v, lr, f, v);
+                putm(N, A, lda, lsa, r, c, v);
+            }
+        });
+    }
+    out[0] = rank;
+    out[1] = info;
+    return 0;
+}
+
 int mfr_potrs(int N, int64_t n, int64_t nrhs, const double *A, int64_t lda, int64_t lsa, double *B,
               int64_t ldb, int64_t lsb, int threads) {
     double one[MAXN];

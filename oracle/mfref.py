@@ -76,6 +76,7 @@ def lib():
                      _i64, _i64, _d, C.c_int],
         "mfr_syrk_packed": [C.c_int, _i64, _i64, _i64, _d, _i64, _i64, _d, _i64, _d, _d, C.c_int],
         "mfr_potrf": [C.c_int, _i64, _d, _i64, _i64, _i64, C.c_int],
+        "mfr_pstrf": [C.c_int, _i64, _d, _i64, _i64, _d, _pi64, _pi64, C.c_int],
         "mfr_potrs": [C.c_int, _i64, _i64, _d, _i64, _i64, _d, _i64, _i64, C.c_int],
         "mfr_getrf": [C.c_int, _i64, _i64, _d, _i64, _i64, _pi64, _i64, C.c_int],
         "mfr_getrs": [C.c_int, _i64, _i64, _d, _i64, _i64, _pi64, _d, _i64, _i64, C.c_int],
@@ -280,6 +281,18 @@ def potrf(A, block=16, nthreads=None):
     Ap = Planes(A)
     info = lib().mfr_potrf(Ap.N, Ap.m, Ap.ptr(), Ap.ld, Ap.ls, block, nthreads or threads())
     return Ap.array(), int(info)
+
+
+def pstrf(A, tol=0.0, nthreads=None):
+    """cholesky_pivoted.jl:65-175 -> (factor array, 1-based permutation, rank, info)"""
+    Ap = Planes(A)
+    N, n = Ap.N, Ap.m
+    perm = np.zeros(max(n, 1), dtype=np.int64)
+    out = np.zeros(2, dtype=np.int64)
+    t = _scalar(N, tol)
+    lib().mfr_pstrf(N, n, Ap.ptr(), Ap.ld, Ap.ls, _p(t), perm.ctypes.data_as(_pi64),
+                    out.ctypes.data_as(_pi64), nthreads or threads())
+    return Ap.array(), perm[:n], int(out[0]), int(out[1])
 
 
 def potrs(L, B, nthreads=None):
