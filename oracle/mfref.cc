@@ -32,6 +32,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
 #include <atomic>
 #include <thread>
 #include <vector>
@@ -1652,5 +1653,8 @@ int mfr_max_threads(void) {
     unsigned n = std::thread::hardware_concurrency();
     return n ? (int)n : 1;
 }
+
+
+#include "qr_body.inc"
 
 } /* extern "C" */

@@ -77,6 +77,11 @@ def lib():
         "mfr_syrk_packed": [C.c_int, _i64, _i64, _i64, _d, _i64, _i64, _d, _i64, _d, _d, C.c_int],
         "mfr_potrf": [C.c_int, _i64, _d, _i64, _i64, _i64, C.c_int],
         "mfr_pstrf": [C.c_int, _i64, _d, _i64, _i64, _d, _pi64, _pi64, C.c_int],
+        "mfr_qr": [C.c_int, _i64, _i64, _d, _i64, _i64, _d, _pi64, _pi64, C.c_int],
+        "mfr_rrqr": [C.c_int, _i64, _i64, _d, _i64, _i64, _d, _pi64, _pi64, C.c_int],
+        "mfr_apply_q": [C.c_int, _i64, _i64, _d, _i64, _i64, _d, _d, _i64, _i64, _i64, C.c_int,
+                        C.c_int],
+        "mfr_qr_numerical_rank": [C.c_int, _i64, _i64, _d, _i64, _i64, _d, _d],
         "mfr_potrs": [C.c_int, _i64, _i64, _d, _i64, _i64, _d, _i64, _i64, C.c_int],
         "mfr_getrf": [C.c_int, _i64, _i64, _d, _i64, _i64, _pi64, _i64, C.c_int],
         "mfr_getrs": [C.c_int, _i64, _i64, _d, _i64, _i64, _pi64, _d, _i64, _i64, C.c_int],
@@ -95,7 +100,7 @@ def lib():
     for name_, args in sig.items():
         fn = getattr(L, name_)
         fn.argtypes = args
-        fn.restype = None if name_ in ("mfr_add", "mfr_sub", "mfr_mul", "mfr_div", "mfr_sqrt",
+        fn.restype = C.c_int64 if name_ == "mfr_qr_numerical_rank" else None if name_ in ("mfr_add", "mfr_sub", "mfr_mul", "mfr_div", "mfr_sqrt",
                                        "mfr_inv", "mfr_mulacc_x3", "mfr_add_n", "mfr_mul_n",
                                        "mfr_to_double") else C.c_int
     _lib = L
@@ -293,6 +298,47 @@ def pstrf(A, tol=0.0, nthreads=None):
     lib().mfr_pstrf(N, n, Ap.ptr(), Ap.ld, Ap.ls, _p(t), perm.ctypes.data_as(_pi64),
                     out.ctypes.data_as(_pi64), nthreads or threads())
     return Ap.array(), perm[:n], int(out[0]), int(out[1])
+
+
+def _qr_run(fn, A, nthreads):
+    Ap = Planes(A)
+    N, m, n = Ap.N, Ap.m, Ap.n
+    r = min(m, n)
+    tau = np.zeros(max(N * r, 1))
+    perm = np.zeros(max(n, 1), dtype=np.int64)
+    info = np.zeros(1, dtype=np.int64)
+    fn(N, m, n, Ap.ptr(), Ap.ld, Ap.ls, _p(tau), perm.ctypes.data_as(_pi64),
+       info.ctypes.data_as(_pi64), nthreads or threads())
+    return Ap.array(), tau[:N * r].reshape(N, r).copy(), perm[:n], int(info[0])
+
+
+def qr(A, nthreads=None):
+    """qr.jl:763-811 -> (factors, tau (N, r), 1-based permutation, info)"""
+    return _qr_run(lib().mfr_qr, A, nthreads)
+
+
+def rrqr(A, nthreads=None):
+    """qr.jl:692-761 (unblocked hybrid or blocked DLAQPS path) -> (factors,
+    tau (N, r), 1-based permutation, info)"""
+    return _qr_run(lib().mfr_rrqr, A, nthreads)
+
+
+def apply_q(F, tau, D, trans="N", nthreads=None):
+    """qr.jl:890-956: Q D (trans N) or Q^T D (trans T) from the compact factor"""
+    Fp, Dp = Planes(F), Planes(D)
+    N, r = Fp.N, min(Fp.m, Fp.n)
+    t = np.ascontiguousarray(np.asarray(tau, dtype=np.float64).reshape(N, r))
+    lib().mfr_apply_q(N, Fp.m, r, Fp.ptr(), Fp.ld, Fp.ls, _p(t), Dp.ptr(), Dp.ld, Dp.ls, Dp.n,
+                      1 if trans == "T" else 0, nthreads or threads())
+    return Dp.array()
+
+
+def qr_numerical_rank(F, atol=0.0, rtol=0.0):
+    """qr.jl:863-888"""
+    Fp = Planes(F)
+    N = Fp.N
+    return int(lib().mfr_qr_numerical_rank(N, Fp.m, Fp.n, Fp.ptr(), Fp.ld, Fp.ls,
+                                           _p(_scalar(N, atol)), _p(_scalar(N, rtol))))
 
 
 def potrs(L, B, nthreads=None):
