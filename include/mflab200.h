@@ -320,6 +320,32 @@ int mflab_potrf(mflab_handle *h, void *stream, int limbs, int64_t n, double *A, 
 int mflab_pstrf(mflab_handle *h, void *stream, int limbs, int64_t n, double *A, int64_t lda,
                 int64_t lsa, const double *tol, int64_t *perm, int64_t *rank_info);
 
+/* Householder QR in place (pivoted = 0: qr!, the columns in their given
+   order; pivoted = 1: rrqr!, deterministic column pivoting).  Reflectors
+   below the diagonal, R on and above it; tau (device, r = min(m, n) values
+   per limb plane, plane stride lst >= r); perm (device int64[n], 1-based):
+   A_original[:, perm] = Q R; *info (device int): 0, or -1 for non-finite
+   input (A unchanged, tau zero, identity permutation).
+   Replaces qr!(A) — src/factorizations/qr.jl:763-811, and rrqr!(A) —
+   src/factorizations/qr.jl:692-761. */
+int mflab_qr(mflab_handle *h, void *stream, int limbs, int pivoted, int64_t m, int64_t n,
+             double *A, int64_t lda, int64_t lsa, double *tau, int64_t lst, int64_t *perm,
+             int *info);
+
+/* D (m x nd) <- Q D (trans 0) or Q^T D (trans 1) with the first r reflectors
+   of a QR factor F (m x >= r) and its tau.
+   Replaces apply_q!(B, F; trans) — src/factorizations/qr.jl:890-956. */
+int mflab_apply_q(mflab_handle *h, void *stream, int limbs, int trans, int64_t m, int64_t r,
+                  const double *F, int64_t ldf, int64_t lsf, const double *tau, int64_t lst,
+                  double *D, int64_t ldd, int64_t lsd, int64_t nd);
+
+/* *rank (device int64) = leading count of |R[i,i]| > max(atol, rtol *
+   max_i |R[i,i]|); atol, rtol host limbs.
+   Replaces numerical_rank(F; atol, rtol) — src/factorizations/qr.jl:863-888. */
+int mflab_qr_numerical_rank(mflab_handle *h, void *stream, int limbs, int64_t m, int64_t n,
+                            const double *F, int64_t ldf, int64_t lsf, const double *atol,
+                            const double *rtol, int64_t *rank);
+
 /* B <- S^{-1} B with a successful Cholesky factor L (n x n), B n x nrhs.
    Replaces ldiv!(B, F::MFCholesky) — src/solve.jl:54-83 (vector form :23-50). */
 int mflab_potrs(mflab_handle *h, void *stream, int limbs, int64_t n, int64_t nrhs,

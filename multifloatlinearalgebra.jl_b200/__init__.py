@@ -33,7 +33,7 @@ __all__ = [
     "PosDefException", "SingularException", "MFLABError",
     "gemm_", "syrk_", "gemmt_", "trsm_", "trsv_", "gemm_plan", "OpNormInf", "gemv_", "symv_",
     "mfdot", "syrk_packed_", "trmm_", "BoundsError", "cholesky_pivoted_", "MFCholeskyPivoted",
-    "factor_rdiag",
+    "factor_rdiag", "MFQR", "qr_", "rrqr_", "apply_q_", "solve_r_", "numerical_rank",
     "cholesky_", "lu_", "ldiv_", "solve", "issuccess",
     "factor_status", "factor_state", "factor_kind", "factor_matrix", "factor_precision",
     "factor_provider", "factor_pivots", "factor_diagnostics",
@@ -704,6 +704,18 @@ class MFCholeskyPivoted(_Factor):
         self.rank = int(rank)
 
 
+class MFQR(_Factor):
+    """Compact Householder QR: reflectors below the diagonal of factors, R on
+    and above it, A[:, permutation] = Q R (src/factorizations/qr.jl:1-16)."""
+    kind = "qr"
+
+    def __init__(self, factors: MFMatrix, tau: torch.Tensor, permutation: torch.Tensor,
+                 info: int):
+        super().__init__(factors, info)
+        self.tau = tau
+        self.permutation = permutation
+
+
 class MFLU(_Factor):
     """Partial-pivoting LU factor (src/factorizations/lu.jl:1-14)."""
     kind = "lu"
@@ -794,6 +806,162 @@ def cholesky_pivoted_(A: MFMatrix, tol=0.0, check: bool = True,
     if info > 0 and check:
         raise PosDefException(info)
     return MFCholeskyPivoted(A, perm[:n], rank, info)
+
+
+def _qr_run(A: MFMatrix, pivoted: int, check: bool, what: str) -> MFQR:
+    N = _same_type(A)
+    m, n = A.m, A.n
+    r = min(m, n)
+    dev = A.storage.device
+    tau = torch.zeros((N, max(r, 1)), dtype=torch.float64, device=dev)
+    perm = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
+    info = torch.zeros(1, dtype=torch.int32, device=dev)
+    lib, h, s = _lib_h(A)
+    _check(lib.mflab_qr(h, s, N, pivoted, m, n, A.ptr(), A.ld, A.ls, tau.data_ptr(), tau.stride(0),
+                        perm.data_ptr(), info.data_ptr()), what)
+    st = _read_info(info)
+    if st == -1 and check:
+        raise DomainError(f"{what}: input matrix contains non-finite entries")
+    return MFQR(A, tau[:, :r], perm[:n], st)
+
+
+def rrqr_(A: MFMatrix, check: bool = True, config: KernelConfig = _DEFAULT) -> MFQR:
+    """Deterministic column-pivoted Householder QR in place
+    (src/factorizations/qr.jl:692-761)."""
+    return _qr_run(A, 1, check, "rrqr!")
+
+
+def qr_(A: MFMatrix, permutation=None, check: bool = True,
+        config: KernelConfig = _DEFAULT) -> MFQR:
+    """Unpivoted Householder QR in place (src/factorizations/qr.jl:763-811);
+    with a permutation the columns are first reordered physically and the
+    factor records the caller's order (qr.jl:813-861)."""
+    if permutation is None:
+        return _qr_run(A, 0, check, "qr!")
+    p = np.asarray(permutation).astype(np.int64).ravel()
+    n = A.n
+    if len(p) != n:
+        raise DimensionMismatch(f"permutation length {len(p)} does not match {n} columns")
+    seen = np.zeros(n, dtype=bool)
+    for c in p:
+        if not 1 <= c <= n:
+            raise ArgumentError(f"permutation entry {c} is outside 1:{n}")
+        if seen[c - 1]:
+            raise ArgumentError(f"permutation repeats column {c}")
+        seen[c - 1] = True
+    view = A.storage[:, A.c0:A.c0 + n, A.r0:A.r0 + A.m]
+    idx = torch.as_tensor(p - 1, device=A.storage.device)
+    view.copy_(view.index_select(1, idx))
+    F = _qr_run(A, 0, check, "qr!")
+    F.permutation = torch.as_tensor(p, device=A.storage.device)
+    return F
+
+
+def _qr_ok(F: MFQR, what: str) -> None:
+    if not issuccess(F):
+        raise ArgumentError(f"{what} requires a successful QR factorization")
+
+
+def apply_q_(B: MFMatrix, F: MFQR, trans: str = "N") -> MFMatrix:
+    """B = Q B (trans N) or Q^T B (trans T) from the compact reflectors
+    (src/factorizations/qr.jl:938-956)."""
+    _qr_ok(F, "apply_q!")
+    if trans not in ("N", "T"):
+        raise ArgumentError("trans must be :N or :T")
+    N = _same_type(B, F.factors)
+    if B.m != F.factors.m:
+        raise DimensionMismatch("apply_q! destination row count differs")
+    if _mightalias(B, F.factors):
+        raise ArgumentError("apply_q! destination must not alias QR storage")
+    Fm = F.factors
+    r = min(Fm.m, Fm.n)
+    lib, h, s = _lib_h(B)
+    _check(lib.mflab_apply_q(h, s, N, 1 if trans == "T" else 0, Fm.m, r, Fm.ptr(), Fm.ld, Fm.ls,
+                             F.tau.data_ptr(), F.tau.stride(0), B.ptr(), B.ld, B.ls, B.n),
+           "apply_q!")
+    return B
+
+
+def solve_r_(B: MFMatrix, F: MFQR, rank: int, trans: str = "N",
+             config: KernelConfig = _DEFAULT) -> MFMatrix:
+    """Solve the leading rank x rank block of R (or its transpose) in place
+    (src/factorizations/qr.jl:958-1014)."""
+    _qr_ok(F, "solve_r!")
+    if trans not in ("N", "T"):
+        raise ArgumentError("trans must be :N or :T")
+    kmax = min(F.factors.m, F.factors.n)
+    rank = int(rank)
+    if not 0 <= rank <= kmax:
+        raise ArgumentError(f"rank must be between zero and {kmax}")
+    if B.m != rank:
+        raise DimensionMismatch("solve_r! destination row count must equal rank")
+    d = factor_rdiag(F)
+    for i in range(rank):
+        if np.all(d[:, i] == 0):
+            raise SingularException(i + 1)
+    if rank == 0:
+        return B
+    lead = F.factors.view(slice(0, rank), slice(0, rank))
+    return trsm_(B, lead, 1.0, side="left", uplo="upper", trans=trans, diag="nonunit",
+                 config=config)
+
+
+def _mf_tol(N: int, v, what: str) -> np.ndarray:
+    t = np.zeros(N)
+    tv = np.atleast_1d(np.asarray(v, dtype=np.float64)).ravel()
+    if len(tv) > N:
+        raise ArgumentError(f"{what} has more limbs than the matrix type")
+    t[:len(tv)] = tv
+    nz = t[t != 0]
+    if not np.all(np.isfinite(t)) or (len(nz) and nz[0] < 0):
+        raise ArgumentError(f"{what} must be finite and nonnegative")
+    return t
+
+
+def numerical_rank(F: MFQR, atol=0.0, rtol=0.0) -> int:
+    """Leading count of |R[i,i]| > max(atol, rtol * max |R[i,i]|)
+    (src/factorizations/qr.jl:863-888)."""
+    _qr_ok(F, "numerical_rank")
+    N = F.N
+    a, r = _mf_tol(N, atol, "atol"), _mf_tol(N, rtol, "rtol")
+    out = torch.zeros(1, dtype=torch.int64, device=F.factors.storage.device)
+    Fm = F.factors
+    lib, h, s = _lib_h(Fm)
+    _check(lib.mflab_qr_numerical_rank(h, s, N, Fm.m, Fm.n, Fm.ptr(), Fm.ld, Fm.ls,
+                                       _scalar(N, a), _scalar(N, r), out.data_ptr()),
+           "numerical_rank")
+    return int(out.item())
+
+
+def _ldiv_qr(dest: MFMatrix, F: MFQR, source: Optional[MFMatrix], config) -> MFMatrix:
+    """square pivoted-QR solve: Q^T, leading R, column permutation
+    (src/solve.jl:425-545)"""
+    if not issuccess(F):
+        raise ArgumentError("ldiv! requires a successful QR factorization")
+    n = F.factors.m
+    if F.factors.n != n:
+        raise DimensionMismatch("QR ldiv! is defined only for square factors; use apply_q! and "
+                                "solve_r! for caller-selected rectangular/rank routes")
+    if dest.m != n:
+        raise DimensionMismatch("right-hand side dimensions differ")
+    d = factor_rdiag(F)
+    for i in range(n):
+        if np.all(d[:, i] == 0):
+            raise SingularException(i + 1)
+    if source is not None:
+        if (source.m, source.n) != (dest.m, dest.n):
+            raise DimensionMismatch("right-hand side length differs")
+    _no_alias("ldiv!", dest, F.factors)
+    if source is not None and source is not dest:
+        if _mightalias(dest, source):
+            raise ArgumentError("ldiv! does not support partially overlapping right-hand sides")
+        dest.copy_(source)
+    apply_q_(dest, F, trans="T")
+    solve_r_(dest, F, n, config=config)
+    view = dest.storage[:, dest.c0:dest.c0 + dest.n, dest.r0:dest.r0 + dest.m]
+    tmp = view.clone()
+    view.index_copy_(2, F.permutation.to(torch.int64) - 1, tmp)
+    return dest
 
 
 def factor_rdiag(F: _Factor) -> np.ndarray:
@@ -907,7 +1075,7 @@ def factor_permutation(F: _Factor) -> np.ndarray:
     """final symmetric permutation p, 1-based: A[p, p] = L D L^T for LDLT
     (ldlt.jl:34-63), the retained block of A[p, p] for pivoted Cholesky
     (cholesky_pivoted.jl:30-38)"""
-    if isinstance(F, MFCholeskyPivoted):
+    if isinstance(F, (MFCholeskyPivoted, MFQR)):
         return F.permutation.cpu().numpy().copy()
     blocks = F.blocks.cpu().numpy()
     piv = F.pivots.cpu().numpy()
@@ -1006,7 +1174,9 @@ def _check_solve(F: _Factor) -> None:
 
 def ldiv_(dest: MFMatrix, F: _Factor, source: Optional[MFMatrix] = None,
           config: KernelConfig = _DEFAULT) -> MFMatrix:
-    """Solve in place with a successful factor (src/solve.jl:23-423)."""
+    """Solve in place with a successful factor (src/solve.jl:23-545)."""
+    if F.kind == "qr":
+        return _ldiv_qr(dest, F, source, config)
     _check_solve(F)
     N = _same_type(dest, F.factors)
     n = F.factors.m
@@ -1063,7 +1233,7 @@ def _mf_values(t: torch.Tensor, N: int, count: int) -> list:
     return [a[i * N:(i + 1) * N].copy() for i in range(count)]
 
 
-def factor_diagnostics(F: _Factor) -> dict:
+def factor_diagnostics(F: _Factor, atol=0.0, rtol=0.0) -> dict:
     """Numerical facts about a factor (src/diagnostics.jl:32-246).  MF-valued
     fields are numpy arrays of N limbs; absent values are None."""
     N = F.N
@@ -1089,6 +1259,26 @@ def factor_diagnostics(F: _Factor) -> dict:
             "maximum_diagonal": mx if has else None,
             "diagonal_spread": spread if has else None,
             "finite": _finite_region(A, 1),
+        })
+        return base
+    if F.kind == "qr":
+        # diagnostics.jl:248-275; atol / rtol are forwarded to numerical_rank
+        r = min(A.m, A.n)
+        _check(lib.mflab_diag_summary(h, s, N, A.ptr(), A.ld, A.ls, r, None, None,
+                                      out.data_ptr()), "factor_diagnostics")
+        mn, mx, spread, _ = _mf_values(out, N, 4)
+        has = r > 0
+        base.update({
+            "failure_location": None,
+            "permutation": factor_permutation(F),
+            "rdiag": factor_rdiag(F),
+            "minimum_rdiag": mn if has else None,
+            "maximum_rdiag": mx if has else None,
+            "rdiag_spread": spread if has else None,
+            "rank_at_threshold": numerical_rank(F, atol, rtol) if issuccess(F) else 0,
+            "atol": _mf_tol(N, atol, "atol"),
+            "rtol": _mf_tol(N, rtol, "rtol"),
+            "finite": _finite_region(A, 0) and bool(torch.isfinite(F.tau).all().item()),
         })
         return base
     if F.kind == "cholesky_pivoted":

@@ -73,6 +73,10 @@ SIGNATURES = {
                    _i64, _d],
     "mflab_potrf": [_vp, _vp, _int, _i64, _vp, _i64, _i64, _i64, _vp],
     "mflab_pstrf": [_vp, _vp, _int, _i64, _vp, _i64, _i64, _d, _vp, _vp],
+    "mflab_qr": [_vp, _vp, _int, _int, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _vp, _vp],
+    "mflab_apply_q": [_vp, _vp, _int, _int, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _vp, _i64,
+                      _i64, _i64],
+    "mflab_qr_numerical_rank": [_vp, _vp, _int, _i64, _i64, _vp, _i64, _i64, _d, _d, _vp],
     "mflab_potrs": [_vp, _vp, _int, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _i64],
     "mflab_getrf": [_vp, _vp, _int, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _vp],
     "mflab_getrs": [_vp, _vp, _int, _i64, _i64, _vp, _i64, _i64, _vp, _vp, _i64, _i64],
