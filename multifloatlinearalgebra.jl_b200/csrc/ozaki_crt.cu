@@ -62,6 +62,45 @@ struct CrtAccConst {
     double pinv;                   // 1 / P (rounded)
 };
 
+// The reconstruction sum X = sum_t r_t U_t on the FP64 pipe: U_t is cut into
+// CRT_CW-bit chunks held as doubles, so every product r_t * chunk (r_t < 2^8)
+// is below 2^47 and a chunk's sum over at most 49 moduli stays below 2^53:
+// exact in binary64.  The chunk sums are then moved into 64-bit partial word
+// sums at bit 39 c.
+constexpr int CRT_CW = 39;
+constexpr int CRT_NC = 9;  // chunks of a U_t (P < 2^342)
+static_assert(CRT_MAXT * 255.0 * 549755813888.0 < 9007199254740992.0,
+              "chunk sums must stay exact in binary64");
+
+// kernel copy of the constants (a kernel parameter, under 4 KB)
+struct CrtAccDev {
+    double Ud[CRT_MAXT][CRT_NC];  // chunk c of U_t: bits [39 c, 39 c + 39)
+    uint32_t P[CRT_WP];
+    double pinv;
+};
+
+// chunks a WP-word sum can need: P < 2^(32 WP), at most CRT_NC
+template <int WP>
+struct CrtChunks {
+    static constexpr int value =
+        (32 * WP + CRT_CW - 1) / CRT_CW < CRT_NC ? (32 * WP + CRT_CW - 1) / CRT_CW : CRT_NC;
+};
+
+// chunk sums (exact integers below 2^53) -> 64-bit partial word sums
+template <int WP>
+__host__ __device__ __forceinline__ void crt_chunks_to_words(const double (&A)[CrtChunks<WP>::value],
+                                                             uint64_t (&X)[WP]) {
+#pragma unroll
+    for (int w = 0; w < WP; ++w) X[w] = 0;
+#pragma unroll
+    for (int cc = 0; cc < CrtChunks<WP>::value; ++cc) {
+        const uint64_t a = (uint64_t)A[cc];
+        const int bit = CRT_CW * cc, w0 = bit >> 5, sh = bit & 31;
+        if (w0 < WP) X[w0] += (uint32_t)(a << sh);
+        if (w0 + 1 < WP) X[w0 + 1] += a >> (32 - sh);
+    }
+}
+
 // 2^k for k in [-1022, 1023]
 __device__ __forceinline__ double pow2i(int k) {
     return __longlong_as_double((long long)(k + 1023) << 52);
@@ -251,8 +290,8 @@ __global__ void __launch_bounds__(128)
 // double estimate of X / P (relative error < 2^-48) rounds to exactly q.
 // All products are 32 x 32 -> 64 bit.
 template <int WP>
-__host__ __device__ __forceinline__ bool crt_reduce(const uint64_t (&X)[WP], const CrtAccConst &c,
-                                                    uint32_t (&mag)[WP]) {
+__host__ __device__ __forceinline__ bool crt_reduce(const uint64_t (&X)[WP], const uint32_t *Pw,
+                                                    double pinv, uint32_t (&mag)[WP]) {
     uint32_t x[WP];
     uint64_t cy = 0;
 #pragma unroll
@@ -264,14 +303,14 @@ __host__ __device__ __forceinline__ bool crt_reduce(const uint64_t (&X)[WP], con
     double xd = 0.0;
 #pragma unroll
     for (int w = WP - 1; w >= 0; --w) xd = fma(xd, 4294967296.0, (double)x[w]);
-    const uint32_t q = (uint32_t)floor(xd * c.pinv + 0.5);
+    const uint32_t q = (uint32_t)floor(xd * pinv + 0.5);
     // Y = X - q P (two's complement over WP words; the final borrow is the sign)
     uint32_t y[WP];
     uint64_t hi = 0;   // carry of q P
     uint32_t br = 0;   // borrow
 #pragma unroll
     for (int w = 0; w < WP; ++w) {
-        const uint64_t qp = (uint64_t)q * c.P[w] + hi;
+        const uint64_t qp = (uint64_t)q * Pw[w] + hi;
         hi = qp >> 32;
         const uint64_t d = (uint64_t)x[w] - (uint32_t)qp - br;
         y[w] = (uint32_t)d;
@@ -361,7 +400,7 @@ template <int N, int WP>
 __global__ void __launch_bounds__(CRT_ACC_ROWS, 3)
     crt_accum_kernel(int64_t m, int64_t n, int Q, int h, int T, const uint8_t *R, int64_t ldi,
                      size_t plane, const int *rowexp, const int *colexp, Mat C, scal<N> alpha,
-                     scal<N> beta, int flags, const __grid_constant__ CrtAccConst c) {
+                     scal<N> beta, int flags, const __grid_constant__ CrtAccDev c) {
     __shared__ __align__(16) uint8_t sres[2 * CRT_MAXT][CRT_ACC_ROWS];
     const int tid = threadIdx.x;
     const int64_t i0 = (int64_t)blockIdx.x * CRT_ACC_ROWS, i = i0 + tid;
@@ -386,19 +425,23 @@ __global__ void __launch_bounds__(CRT_ACC_ROWS, 3)
     } else {
         for (int L = Q - 1; L >= 0; --L) {
             const uint8_t *src = &sres[L * T][tid];
-            uint64_t X[WP];
+            constexpr int NC = CrtChunks<WP>::value;
+            double A[NC];
 #pragma unroll
-            for (int w = 0; w < WP; ++w) X[w] = 0;
+            for (int cc = 0; cc < NC; ++cc) A[cc] = 0.0;
 #pragma unroll
             for (int t = 0; t < CRT_MAXT; ++t) {
-                if (t < T) {
-                    const uint32_t r = src[t * CRT_ACC_ROWS];
+                if (t >= T) break;
+                // the residue byte as an exact double: 2^52 + r minus 2^52
+                const double rd = __hiloint2double(0x43300000, (int)src[t * CRT_ACC_ROWS]) -
+                                  4503599627370496.0;
 #pragma unroll
-                    for (int w = 0; w < WP; ++w) X[w] += (uint64_t)r * c.U[t][w];
-                }
+                for (int cc = 0; cc < NC; ++cc) A[cc] = fma(rd, c.Ud[t][cc], A[cc]);
             }
+            uint64_t X[WP];
+            crt_chunks_to_words<WP>(A, X);
             uint32_t mag[WP];
-            const bool ng = crt_reduce<WP>(X, c, mag);
+            const bool ng = crt_reduce<WP>(X, c.P, c.pinv, mag);
             const int sh = oz_scale_exp(ea) + oz_scale_exp(eb) - 2 * Q * h + h * (2 * Q - 2 - L);
             mf<N> g = crt_words_to_mf<N, WP>(mag, sh);
             if (ng) g = neg(g);
@@ -476,6 +519,7 @@ static uint32_t inv_mod(uint32_t a, uint32_t p) {
 
 struct CrtTables {
     CrtAccConst acc;
+    CrtAccDev dev;
     int bitlen;  // bit length of P
 };
 
@@ -520,11 +564,21 @@ static const CrtTables &crt_tables(int T) {
             big_div_small(M, p, &r);
             const Big U = big_mul_small(M, inv_mod(r, p));
             for (size_t w = 0; w < U.size() && w < (size_t)CRT_WP; ++w) c.acc.U[t][w] = U[w];
+            for (int cc = 0; cc < CRT_NC; ++cc) {
+                uint64_t v = 0;  // bits [39 cc, 39 cc + 39) of U_t
+                for (int b = 0; b < CRT_CW; ++b) {
+                    const int bit = CRT_CW * cc + b, w = bit >> 5;
+                    if ((size_t)w < U.size() && ((U[w] >> (bit & 31)) & 1u)) v |= 1ULL << b;
+                }
+                c.dev.Ud[t][cc] = (double)v;
+            }
         }
         long double pd = 0.0L;
         for (size_t w = P.size(); w-- > 0;) pd = pd * 4294967296.0L + (long double)P[w];
         for (size_t w = 0; w < P.size() && w < (size_t)CRT_WP; ++w) c.acc.P[w] = P[w];
         c.acc.pinv = (double)(1.0L / pd);
+        memcpy(c.dev.P, c.acc.P, sizeof(c.dev.P));
+        c.dev.pinv = c.acc.pinv;
     });
     return tab[T];
 }
@@ -639,7 +693,7 @@ static void crt_accum(const CrtPlan &p, int64_t m, int64_t n, const uint8_t *I, 
                       int flags, cudaStream_t s) {
     dim3 g((unsigned)((m + CRT_ACC_ROWS - 1) / CRT_ACC_ROWS), (unsigned)n);
     crt_accum_kernel<N, WP><<<g, CRT_ACC_ROWS, 0, s>>>(m, n, p.Q, p.h, p.T, I, p.ldi, p.plane, rowexp,
-                                              colexp, C, al, be, flags, crt_tables(p.T).acc);
+                                              colexp, C, al, be, flags, crt_tables(p.T).dev);
 }
 
 template <int N>
@@ -913,17 +967,21 @@ extern "C" int mflab_ozaki_crt_reduce_host(int T, int count, const int32_t *G, u
                                            int *neg) {
     using namespace mfl;
     if (T < 1 || T > CRT_MAXT || count < 0 || !G || !mag || !neg) return MFLAB_ERR_ARG;
-    const CrtAccConst &c = crt_tables(T).acc;
+    // the device's arithmetic: residues as exact doubles, FMA chunk sums
+    const CrtAccDev &c = crt_tables(T).dev;
     for (int e = 0; e < count; ++e) {
-        uint64_t X[CRT_WP] = {0};
+        double A[CrtChunks<CRT_WP>::value] = {0.0};
         for (int t = 0; t < T; ++t) {
             const int p = crt_modulus(t);
             int r = G[(size_t)e * T + t] % p;
             r += r < 0 ? p : 0;
-            for (int w = 0; w < CRT_WP; ++w) X[w] += (uint64_t)(uint32_t)r * c.U[t][w];
+            for (int cc = 0; cc < CrtChunks<CRT_WP>::value; ++cc)
+                A[cc] = fma((double)r, c.Ud[t][cc], A[cc]);
         }
+        uint64_t X[CRT_WP];
+        crt_chunks_to_words<CRT_WP>(A, X);
         uint32_t mg[CRT_WP];
-        neg[e] = crt_reduce<CRT_WP>(X, c, mg) ? 1 : 0;
+        neg[e] = crt_reduce<CRT_WP>(X, c.P, c.pinv, mg) ? 1 : 0;
         for (int w = 0; w < CRT_WP; ++w) mag[(size_t)e * CRT_WP + w] = mg[w];
     }
     return MFLAB_OK;
