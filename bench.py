@@ -110,6 +110,84 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+_NVML_CHILD = r"""
+import sys, time
+import pynvml as nv
+nv.nvmlInit()
+bus = sys.argv[1]
+try:
+    h = nv.nvmlDeviceGetHandleByPciBusId(bus)
+except Exception:
+    h = nv.nvmlDeviceGetHandleByIndex(int(sys.argv[2]))
+fn = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+    nv.nvmlDeviceGetCurrentClocksThrottleReasons
+print("max", nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM), flush=True)
+while True:
+    print(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM), int(fn(h)), flush=True)
+    time.sleep(0.005)
+"""
+
+
+class NvmlClockSampler:
+    """Clock / throttle-reason sampling through NVML (read-only queries) every
+    5 ms in a child process, so that short timed regions still get many
+    samples whatever the benchmark thread holds; falls back to the
+    nvidia-smi sampler when NVML is unavailable."""
+
+    BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+            "hw_thermal_slowdown": 0x40}
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc, self.fallback, self.lines = None, None, []
+
+    def start(self):
+        try:
+            import torch
+            pr = torch.cuda.get_device_properties(self.index)
+            bus = f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+            self.proc = subprocess.Popen([sys.executable, "-c", _NVML_CHILD, bus, str(self.index)],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                                         text=True)
+            first = self.proc.stdout.readline().split()
+            if len(first) != 2 or first[0] != "max":
+                raise OSError("nvml child did not start")
+            self.max_mhz = float(first[1])
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            if self.proc is not None:
+                self.proc.kill()
+            self.proc = None
+            self.fallback = ClockSampler(self.index)
+            self.fallback.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line)
+
+    def stop(self) -> dict:
+        if self.fallback is not None:
+            return self.fallback.stop()
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=5)
+        sm, reasons = [], set()
+        for line in self.lines:
+            f = line.split()
+            if len(f) != 2:
+                continue
+            sm.append(float(f[0]))
+            for name, b in self.BITS.items():
+                if int(f[1]) & b:
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvml, 5 ms"}
+
+
 # ------------------------------------------------------------ helpers ----
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -549,7 +627,7 @@ def main():
     oz_cfg = R.cfg(scheme, knob)
     head_cfg = oz_cfg if route == "ozaki" else plain_cfg
 
-    clocks = ClockSampler(local)
+    clocks = NvmlClockSampler(local)
     clocks.start()
     t_head = R.timed(lambda: mf.gemm_(Cm, A, B, config=head_cfg), args.steps, args.warmup)
     clk = clocks.stop()

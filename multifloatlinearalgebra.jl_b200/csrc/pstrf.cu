@@ -69,7 +69,7 @@ __global__ void pstrf_mirror_kernel(int64_t n, Mat A, const PstrfState *st) {
     }
 }
 
-constexpr int PSTRF_PIVOT_THREADS = 256;
+constexpr int PSTRF_PIVOT_THREADS = 1024;
 
 template <int N>
 __global__ void __launch_bounds__(PSTRF_PIVOT_THREADS)
