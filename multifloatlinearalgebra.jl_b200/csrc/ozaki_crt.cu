@@ -177,20 +177,59 @@ __device__ __forceinline__ uint32_t crt_residue(const uint32_t (&w)[WD], const u
     return acc % (uint32_t)p;
 }
 
+// elements per thread of the split kernels: 8 for Float64x2, 4 for more limbs
+// (their staging tile and registers would not fit twice the elements)
+template <int N>
+struct CrtSplitU {
+    static constexpr int value = N == 2 ? 8 : 4;
+};
+
+// residue bytes of U consecutive elements (digit words w[u], signs ng[u]) for
+// the moduli t < T: one U-byte store per modulus plane
+template <int WD, int U>
+__device__ __forceinline__ void crt_emit(const uint32_t (&w)[U][WD], const bool (&ng)[U], int T,
+                                         int8_t *dst, size_t plane8, const CrtSplitConst &c) {
+#pragma unroll
+    for (int t = 0; t < CRT_MAXT; ++t) {
+        if (t >= T) break;
+        const int p = crt_modulus(t);
+        const uint32_t noff = c.negoff[WD - 3][t];
+        uint32_t wt[WD];
+#pragma unroll
+        for (int j = 0; j < WD; ++j) wt[j] = c.wt[t][j];
+        uint32_t packed[U / 4];
+#pragma unroll
+        for (int g = 0; g < U / 4; ++g) {
+            packed[g] = 0;  // bytes of elements 4g+3 .. 4g, by multiply-add
+#pragma unroll
+            for (int u = 3; u >= 0; --u)
+                packed[g] = packed[g] * 256u +
+                            crt_residue<WD>(w[4 * g + u], wt, ng[4 * g + u] ? noff : 128u, p);
+        }
+        if constexpr (U == 8)
+            *(uint2 *)(dst + (size_t)t * plane8) =
+                make_uint2(packed[0] ^ 0x80808080u, packed[1] ^ 0x80808080u);
+        else
+            *(uint32_t *)(dst + (size_t)t * plane8) = packed[0] ^ 0x80808080u;
+    }
+}
+
 // A (m x k, column-major planes) -> residue planes A8[t][i][q'][k] (int8,
-// rows of Q kp bytes, plane stride plane8; q' = q, or Q-1-q with rev).  32 x 32 tile per block of
-// 32 x 8 threads, staged through shared memory; each thread then owns 4
-// consecutive k of one row and writes one 32-bit word per (t, q).
+// rows of Q kp bytes, plane stride plane8; q' = q, or Q-1-q with rev).  A
+// block stages a 32-row x 64-k tile of every limb plane in shared memory; each
+// of its 32 x 8 threads then owns 8 consecutive k of one row and writes 8
+// bytes per (t, q) (4 of each for more than two limbs).
 template <int N, int WD>
 __global__ void __launch_bounds__(256)
     crt_split_a_kernel(int64_t m, int64_t mp, int64_t k, int64_t kp, int Q, int h, int T, Mat A,
                        const int *rowexp, int8_t *A8, size_t plane8, int rev,
                        const __grid_constant__ CrtSplitConst c) {
-    __shared__ double tile[N][32][33];
+    constexpr int U = CrtSplitU<N>::value, AK = 8 * U;  // k extent of the tile
+    __shared__ double tile[N][AK][33];
     const int tx = threadIdx.x, ty = threadIdx.y;
-    const int64_t i0 = (int64_t)blockIdx.x * 32, k0 = (int64_t)blockIdx.y * 32;
+    const int64_t i0 = (int64_t)blockIdx.x * 32, k0 = (int64_t)blockIdx.y * AK;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
+    for (int j = 0; j < AK / 8; ++j) {
         const int kk = ty + 8 * j;
         const int64_t i = i0 + tx, kg = k0 + kk;
         const bool ok = i < m && kg < k;
@@ -198,14 +237,14 @@ __global__ void __launch_bounds__(256)
         for (int l = 0; l < N; ++l) tile[l][kk][tx] = ok ? A.p[l * A.ls + kg * A.ld + i] : 0.0;
     }
     __syncthreads();
-    const int ii = ty * 4 + (tx >> 3), kq = (tx & 7) * 4;
+    const int ii = ty * 4 + (tx >> 3), kq = (tx & 7) * U;
     const int64_t i = i0 + ii, kg = k0 + kq;
-    if (i >= mp || kg >= kp) return;  // kp is a multiple of 32: kg + 3 < kp
+    if (i >= mp || kg >= kp) return;  // kp is a multiple of 128: kg + U - 1 < kp
     const int e = i < m ? rowexp[i] : OZ_EXP_EMPTY;
     const int sh = oz_scale_exp(e);
-    mf<N> z[4];
+    mf<N> z[U];
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
+    for (int u = 0; u < U; ++u) {
 #pragma unroll
         for (int l = 0; l < N; ++l)
             z[u].v[l] = (e == OZ_EXP_BAD) ? 0.0 : scale2(tile[l][kq + u][ii], -sh);
@@ -214,43 +253,32 @@ __global__ void __launch_bounds__(256)
     }
     int8_t *dst = A8 + (size_t)i * Q * kp + kg;
     for (int q = 0; q < Q; ++q) {
-        uint32_t w[4][WD];
-        bool ng[4];
+        uint32_t w[U][WD];
+        bool ng[U];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) crt_digit<N, WD>(z[u], h, w[u], ng[u]);
-#pragma unroll
-        for (int t = 0; t < CRT_MAXT; ++t) {
-            if (t < T) {
-                uint32_t packed = 0;  // bytes of elements 3..0, by multiply-add
-#pragma unroll
-                for (int u = 3; u >= 0; --u)
-                    packed = packed * 256u +
-                             crt_residue<WD>(w[u], c.wt[t], ng[u] ? c.negoff[WD - 3][t] : 128u,
-                                             crt_modulus(t));
-                *(uint32_t *)(dst + (size_t)t * plane8 + (size_t)(rev ? Q - 1 - q : q) * kp) =
-                    packed ^ 0x80808080u;
-            }
-        }
+        for (int u = 0; u < U; ++u) crt_digit<N, WD>(z[u], h, w[u], ng[u]);
+        crt_emit<WD, U>(w, ng, T, dst + (size_t)(rev ? Q - 1 - q : q) * kp, plane8, c);
     }
 }
 
 // B (k x n) -> residue planes B8[t][j][q'][k] with q' = Q-1-q when rev (the
 // right operand: pairs of one level adjacent along K), q' = q otherwise (the
-// left operand of a Gram product A^T A, whose rows are B's columns).  Each thread owns 4
-// consecutive k of one column.
+// left operand of a Gram product A^T A, whose rows are B's columns).  Each
+// thread owns U consecutive k of one column.
 template <int N, int WD>
 __global__ void __launch_bounds__(128)
     crt_split_b_kernel(int64_t k, int64_t n, int64_t np, int64_t kp, int Q, int h, int T, Mat B,
                        const int *colexp, int8_t *B8, size_t plane8, int rev,
                        const __grid_constant__ CrtSplitConst c) {
-    const int64_t kg = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * 4;
+    constexpr int U = CrtSplitU<N>::value;
+    const int64_t kg = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * U;
     const int64_t j = blockIdx.y;
     if (kg >= kp || j >= np) return;
     const int e = j < n ? colexp[j] : OZ_EXP_EMPTY;
     const int sh = oz_scale_exp(e);
-    mf<N> z[4];
+    mf<N> z[U];
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
+    for (int u = 0; u < U; ++u) {
         const int64_t kk = kg + u;
         const bool ok = kk < k && j < n && e != OZ_EXP_BAD;
 #pragma unroll
@@ -261,24 +289,22 @@ __global__ void __launch_bounds__(128)
     }
     int8_t *dst = B8 + (size_t)j * Q * kp + kg;
     for (int q = 0; q < Q; ++q) {
-        uint32_t w[4][WD];
-        bool ng[4];
+        uint32_t w[U][WD];
+        bool ng[U];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) crt_digit<N, WD>(z[u], h, w[u], ng[u]);
-#pragma unroll
-        for (int t = 0; t < CRT_MAXT; ++t) {
-            if (t < T) {
-                uint32_t packed = 0;  // bytes of elements 3..0, by multiply-add
-#pragma unroll
-                for (int u = 3; u >= 0; --u)
-                    packed = packed * 256u +
-                             crt_residue<WD>(w[u], c.wt[t], ng[u] ? c.negoff[WD - 3][t] : 128u,
-                                             crt_modulus(t));
-                *(uint32_t *)(dst + (size_t)t * plane8 + (size_t)(rev ? Q - 1 - q : q) * kp) =
-                    packed ^ 0x80808080u;
-            }
-        }
+        for (int u = 0; u < U; ++u) crt_digit<N, WD>(z[u], h, w[u], ng[u]);
+        crt_emit<WD, U>(w, ng, T, dst + (size_t)(rev ? Q - 1 - q : q) * kp, plane8, c);
     }
+}
+
+// launch shapes of the two split kernels
+template <int N>
+static inline dim3 crt_split_a_grid(int64_t mp, int64_t kp) {
+    return dim3((unsigned)((mp + 31) / 32), (unsigned)(kp / (8 * CrtSplitU<N>::value)));
+}
+template <int N>
+static inline dim3 crt_split_b_grid(int64_t np, int64_t kp) {
+    return dim3((unsigned)((kp / CrtSplitU<N>::value + 127) / 128), (unsigned)np);
 }
 
 // ------------------------------------------------------ reconstruction ----
@@ -670,10 +696,10 @@ static void crt_split(const CrtPlan &p, int64_t m, int64_t n, int64_t k, Mat A, 
                       const int *rowexp, const int *colexp, int8_t *A8, int8_t *B8,
                       cudaStream_t s) {
     const CrtSplitConst &c = crt_split_const();
-    dim3 ga((unsigned)((p.mp + 31) / 32), (unsigned)(p.kp / 32));
+    const dim3 ga = crt_split_a_grid<N>(p.mp, p.kp);
     crt_split_a_kernel<N, WD><<<ga, dim3(32, 8), 0, s>>>(m, p.mp, k, p.kp, p.Q, p.h, p.T, A,
                                                          rowexp, A8, p.plane8a, 0, c);
-    dim3 gb((unsigned)((p.kp / 4 + 127) / 128), (unsigned)p.np);
+    const dim3 gb = crt_split_b_grid<N>(p.np, p.kp);
     crt_split_b_kernel<N, WD><<<gb, 128, 0, s>>>(k, n, p.np, p.kp, p.Q, p.h, p.T, B, colexp, B8,
                                                  p.plane8b, 1, c);
 }
@@ -791,11 +817,11 @@ static void crt_split_gram(const CrtPlan &p, int trans, int64_t n, int64_t k, Ma
     for (int role = 0; role < (p.Q == 1 ? 1 : 2); ++role) {
         int8_t *dst = role == 0 ? A8 : B8;
         if (trans == 0) {
-            dim3 ga((unsigned)(p.mp / 32), (unsigned)(p.kp / 32));
+            const dim3 ga = crt_split_a_grid<N>(p.mp, p.kp);
             crt_split_a_kernel<N, WD><<<ga, dim3(32, 8), 0, s>>>(n, p.mp, k, p.kp, p.Q, p.h, p.T, A,
                                                                  exps, dst, p.plane8a, role, c);
         } else {
-            dim3 gb((unsigned)((p.kp / 4 + 127) / 128), (unsigned)p.np);
+            const dim3 gb = crt_split_b_grid<N>(p.np, p.kp);
             crt_split_b_kernel<N, WD><<<gb, 128, 0, s>>>(k, n, p.np, p.kp, p.Q, p.h, p.T, A, exps,
                                                          dst, p.plane8b, role, c);
         }
