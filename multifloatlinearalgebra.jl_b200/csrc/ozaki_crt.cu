@@ -138,7 +138,7 @@ __device__ __forceinline__ void crt_digit(mf<N> &z, int h, uint32_t (&w)[WD], bo
     for (int l = 0; l < N; ++l) {
         if (d[l] != 0.0) {
             const uint64_t bits = (uint64_t)__double_as_longlong(d[l]);
-            const int64_t sg = (bits >> 63) ? -1 : 1;
+            const bool sneg = (bits >> 63) != 0;
             uint64_t mm = (bits & ((1ULL << 52) - 1)) | (1ULL << 52);
             int e = (int)((bits >> 52) & 0x7ff) - 1075;
             if (e < 0) {  // the bits shifted out are zero: d_l is an integer
@@ -151,7 +151,7 @@ __device__ __forceinline__ void crt_digit(mf<N> &z, int h, uint32_t (&w)[WD], bo
                 uint32_t part = 0;
                 if (dd >= 0 && dd < 64) part = (uint32_t)(mm >> dd);
                 else if (dd < 0 && dd > -32) part = (uint32_t)(mm << (-dd));
-                c[j] += sg * (int64_t)part;
+                c[j] += sneg ? -(int64_t)part : (int64_t)part;
             }
         }
     }
