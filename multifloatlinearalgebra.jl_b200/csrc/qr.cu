@@ -103,6 +103,92 @@ __device__ void norm_state(const Mat &A, int64_t m, int64_t r0, int64_t c, const
     }
 }
 
+// The same scaled sum of squares computed by one warp, bit for bit: per chunk
+// of 32 rows the lanes load their magnitudes, a warp scan gives every row the
+// running maximum before it (the reference's `scale` at that row: the scale
+// only ever moves to a new maximum), each lane forms its ratio and square in
+// parallel, and lane 0 folds the chunk in row order with the reference's own
+// operations (sum += ratio^2, or sum = 1 + sum*ratio*ratio at a new maximum,
+// or sum = 1 at the first nonzero).  The divisions and products leave the
+// sequential path; only the additions stay on it.  All 32 lanes must call it;
+// buf is this warp's shared scratch of QR_NORM_BUF(N) doubles.
+#define QR_NORM_BUF(N) (32 * (3 * (N) + 1))
+template <int N>
+__device__ void norm_state_warp(const Mat &A, int64_t m, int64_t r0, int64_t c, double *buf,
+                                mf<N> &scale, mf<N> &sum) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const mf<N> one = from_double<N>(1.0), zero = from_double<N>(0.0);
+    scale = zero;
+    sum = one;
+    bool seen = false;
+    double *bmag = buf, *brat = buf + 32 * N, *bsq = buf + 64 * N;
+    int *bflag = (int *)(buf + 96 * N);
+    for (int64_t base = r0; base < m; base += 32) {
+        const int64_t r = base + lane;
+        const mf<N> mag = r < m ? abs_mf(load_mf<N>(A.p, A.ld, A.ls, r, c)) : zero;
+        const bool nz = !iszero(mag);
+        // inclusive running maximum over the lanes, then shifted by one and
+        // merged with the scale carried from the previous chunks
+        mf<N> pm = mag;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            mf<N> o;
+#pragma unroll
+            for (int l = 0; l < N; ++l) o.v[l] = __shfl_up_sync(FULL, pm.v[l], off);
+            if (lane >= off && gt(o, pm)) pm = o;
+        }
+        mf<N> before;
+#pragma unroll
+        for (int l = 0; l < N; ++l) before.v[l] = __shfl_up_sync(FULL, pm.v[l], 1);
+        if (lane == 0 || gt(scale, before)) before = scale;
+        const bool isnew = nz && gt(mag, before);
+        mf<N> ratio = zero, sq = zero;
+        if (nz && !iszero(before)) {
+            ratio = isnew ? div(before, mag) : div(mag, before);
+            sq = mul(ratio, ratio);
+        }
+#pragma unroll
+        for (int l = 0; l < N; ++l) {
+            bmag[l * 32 + lane] = mag.v[l];
+            brat[l * 32 + lane] = ratio.v[l];
+            bsq[l * 32 + lane] = sq.v[l];
+        }
+        bflag[lane] = (nz ? 1 : 0) | (isnew ? 2 : 0);
+        __syncwarp();
+        if (lane == 0) {
+            for (int i = 0; i < 32; ++i) {
+                const int f = bflag[i];
+                if (!(f & 1)) continue;
+                mf<N> mi, ri, si;
+#pragma unroll
+                for (int l = 0; l < N; ++l) {
+                    mi.v[l] = bmag[l * 32 + i];
+                    ri.v[l] = brat[l * 32 + i];
+                    si.v[l] = bsq[l * 32 + i];
+                }
+                if (!seen) {
+                    scale = mi;
+                    sum = one;
+                    seen = true;
+                } else if (f & 2) {
+                    sum = add(one, mul(mul(sum, ri), ri));
+                    scale = mi;
+                } else {
+                    sum = add(sum, si);
+                }
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int l = 0; l < N; ++l) {
+            scale.v[l] = __shfl_sync(FULL, scale.v[l], 0);
+            sum.v[l] = __shfl_sync(FULL, sum.v[l], 0);
+        }
+        seen = __shfl_sync(FULL, seen ? 1 : 0, 0) != 0;
+    }
+}
+
 // _qr_norm_from_state (qr.jl:157-165)
 template <int N>
 __device__ __forceinline__ mf<N> norm_value(const mf<N> &scale, const mf<N> &sum) {
@@ -134,11 +220,11 @@ __global__ void __launch_bounds__(QR_CTA)
                         double *diag, int64_t bs, int64_t ls, double *aux) {
     __shared__ double slead[N];
     __shared__ int go;
+    __shared__ double nbuf[QR_NORM_BUF(N)];
     const int tid = threadIdx.x;
+    mf<N> scale, sum;
+    if (tid < 32) norm_state_warp<N>(A, m, s, s, nbuf, scale, sum);
     if (tid == 0) {
-        mf<N> scale, sum;
-        const Mat none{nullptr, 1, 1};
-        norm_state<N>(A, m, s, s, none, 0, 0, scale, sum);
         const mf<N> nrm = norm_value(scale, sum);
         mf<N> t = from_double<N>(0.0);
         go = 0;
@@ -186,40 +272,85 @@ __global__ void __launch_bounds__(QR_CTA)
     }
 }
 
-// reflector s of V (implicit one at row s) applied to columns c0.. of D,
-// one column per thread (qr.jl:624-642); skipped when tau is zero
+// acc folded over rows r0..m-1 in ascending order, acc = acc + X[r,cx] *
+// Y[r,cy], by one warp: the lanes form 32 products at a time, lane 0 adds
+// them in row order (the reference's chain; only the additions are
+// sequential).  All 32 lanes call it; buf holds 32 N doubles of this warp;
+// the result is returned in every lane.
 template <int N>
-__device__ __forceinline__ void apply_reflector_col(int64_t m, int64_t s, const Mat &V,
-                                                    const mf<N> &t, const Mat &D, int64_t c) {
-    mf<N> proj = load_mf<N>(D.p, D.ld, D.ls, s, c);
-    for (int64_t r = s + 1; r < m; ++r)
-        proj = add(proj, mul(load_mf<N>(V.p, V.ld, V.ls, r, s), load_mf<N>(D.p, D.ld, D.ls, r, c)));
+__device__ mf<N> chain_warp(mf<N> acc, int64_t r0, int64_t m, const Mat &X, int64_t cx,
+                            const Mat &Y, int64_t cy, double *buf) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    for (int64_t base = r0; base < m; base += 32) {
+        const int64_t r = base + lane;
+        mf<N> pr = from_double<N>(0.0);
+        if (r < m) pr = mul(load_mf<N>(X.p, X.ld, X.ls, r, cx), load_mf<N>(Y.p, Y.ld, Y.ls, r, cy));
+#pragma unroll
+        for (int l = 0; l < N; ++l) buf[l * 32 + lane] = pr.v[l];
+        __syncwarp();
+        if (lane == 0) {
+            const int cnt = m - base < 32 ? (int)(m - base) : 32;
+            for (int i = 0; i < cnt; ++i) {
+                mf<N> x;
+#pragma unroll
+                for (int l = 0; l < N; ++l) x.v[l] = buf[l * 32 + i];
+                acc = add(acc, x);
+            }
+        }
+        __syncwarp();
+    }
+#pragma unroll
+    for (int l = 0; l < N; ++l) acc.v[l] = __shfl_sync(FULL, acc.v[l], 0);
+    return acc;
+}
+
+// reflector s of V (implicit one at row s) applied to column c of D by one
+// warp (qr.jl:624-642): the projection chain, then the rank-one update with
+// the rows spread over the lanes
+template <int N>
+__device__ __forceinline__ void apply_reflector_col_warp(int64_t m, int64_t s, const Mat &V,
+                                                         const mf<N> &t, const Mat &D, int64_t c,
+                                                         double *buf) {
+    const int lane = threadIdx.x & 31;
+    mf<N> proj = chain_warp<N>(load_mf<N>(D.p, D.ld, D.ls, s, c), s + 1, m, V, s, D, c, buf);
     proj = mul(proj, t);
-    store_mf<N>(D.p, D.ld, D.ls, s, c, sub(load_mf<N>(D.p, D.ld, D.ls, s, c), proj));
-    for (int64_t r = s + 1; r < m; ++r)
+    if (lane == 0) store_mf<N>(D.p, D.ld, D.ls, s, c, sub(load_mf<N>(D.p, D.ld, D.ls, s, c), proj));
+    for (int64_t r = s + 1 + lane; r < m; r += 32)
         store_mf<N>(D.p, D.ld, D.ls, r, c,
                     submul(load_mf<N>(D.p, D.ld, D.ls, r, c), load_mf<N>(V.p, V.ld, V.ls, r, s), proj));
+    __syncwarp();
+}
+
+constexpr int QR_COL_WARPS = 4;  // columns (one warp each) per CTA
+
+static inline unsigned warp_col_grid(int64_t cols) {
+    return (unsigned)((cols + QR_COL_WARPS - 1) / QR_COL_WARPS);
 }
 
 template <int N>
-__global__ void __launch_bounds__(QR_COLS_PER_CTA)
+__global__ void __launch_bounds__(32 * QR_COL_WARPS)
     qr_apply_kernel(int64_t m, int64_t s, Mat V, const double *tau, int64_t lt, Mat D, int64_t c0,
                     int64_t nd) {
-    const int64_t j = (int64_t)blockIdx.x * QR_COLS_PER_CTA + threadIdx.x;
-    if (j >= nd) return;
+    __shared__ double buf[QR_COL_WARPS][32 * N];
+    const int w = threadIdx.x >> 5;
+    const int64_t j = (int64_t)blockIdx.x * QR_COL_WARPS + w;
+    if (j >= nd) return;  // whole warps leave together
     mf<N> t;
 #pragma unroll
     for (int l = 0; l < N; ++l) t.v[l] = tau[l * lt + s];
     if (iszero(t)) return;
-    apply_reflector_col<N>(m, s, V, t, D, c0 + j);
+    apply_reflector_col_warp<N>(m, s, V, t, D, c0 + j, buf[w]);
 }
 
 // apply_q! (qr.jl:890-956): every reflector in order on one column of D
 template <int N>
-__global__ void __launch_bounds__(QR_COLS_PER_CTA)
+__global__ void __launch_bounds__(32 * QR_COL_WARPS)
     qr_apply_all_kernel(int64_t m, int64_t r, Mat V, const double *tau, int64_t lt, Mat D,
                         int64_t nd, int trans) {
-    const int64_t c = (int64_t)blockIdx.x * QR_COLS_PER_CTA + threadIdx.x;
+    __shared__ double buf[QR_COL_WARPS][32 * N];
+    const int w = threadIdx.x >> 5;
+    const int64_t c = (int64_t)blockIdx.x * QR_COL_WARPS + w;
     if (c >= nd) return;
     for (int64_t i = 0; i < r; ++i) {
         const int64_t s = trans ? i : r - 1 - i;
@@ -227,21 +358,31 @@ __global__ void __launch_bounds__(QR_COLS_PER_CTA)
 #pragma unroll
         for (int l = 0; l < N; ++l) t.v[l] = tau[l * lt + s];
         if (iszero(t)) continue;
-        apply_reflector_col<N>(m, s, V, t, D, c);
+        apply_reflector_col_warp<N>(m, s, V, t, D, c, buf[w]);
     }
 }
 
-// norm state of columns c0..n-1 from rows r0 (qr.jl:143-155, 417-448)
+// norm state of columns c0..n-1 from rows r0 (qr.jl:143-155, 417-448), one
+// warp per column
+constexpr int QR_NORM_WARPS = 4;
+
 template <int N>
-__global__ void __launch_bounds__(QR_COLS_PER_CTA)
+__global__ void __launch_bounds__(32 * QR_NORM_WARPS)
     qr_norm_init_kernel(int64_t m, int64_t r0, int64_t c0, Mat A, QRNorms<N> S) {
-    const int64_t c = c0 + (int64_t)blockIdx.x * QR_COLS_PER_CTA + threadIdx.x;
-    if (c >= S.n) return;
+    __shared__ double nbuf[QR_NORM_WARPS][QR_NORM_BUF(N)];
+    const int w = threadIdx.x >> 5;
+    const int64_t c = c0 + (int64_t)blockIdx.x * QR_NORM_WARPS + w;
+    if (c >= S.n) return;  // whole warps leave together
     mf<N> scale, sum;
-    const Mat none{nullptr, 1, 1};
-    norm_state<N>(A, m, r0, c, none, 0, 0, scale, sum);
-    S.set(c, scale, sum);
-    S.dirty[c] = 0;
+    norm_state_warp<N>(A, m, r0, c, nbuf[w], scale, sum);
+    if ((threadIdx.x & 31) == 0) {
+        S.set(c, scale, sum);
+        S.dirty[c] = 0;
+    }
+}
+
+static inline unsigned norm_grid(int64_t cols) {
+    return (unsigned)((cols + QR_NORM_WARPS - 1) / QR_NORM_WARPS);
 }
 
 // _qr_update_norm_state! for one column (qr.jl:264-304)
@@ -302,21 +443,31 @@ __global__ void __launch_bounds__(QR_CTA)
     qr_hybrid_pivot_kernel(int64_t m, int64_t step, Mat A, int64_t *perm, QRNorms<N> S,
                            scal<N> one_minus_margin) {
     __shared__ int64_t sp;
-    if (threadIdx.x == 0) {
-        const Mat none{nullptr, 1, 1};
+    __shared__ double nbuf[QR_NORM_BUF(N)];
+    if (threadIdx.x < 32) {
+        // warp 0 walks the columns in order; every lane takes the same
+        // branches (the state it reads is the same), lane 0 writes
+        const bool w0 = threadIdx.x == 0;
         const mf<N> om = one_minus_margin.get();
         int64_t piv = step;
         mf<N> sc, su;
-        norm_state<N>(A, m, step, step, none, 0, 0, sc, su);
-        S.set(step, sc, su);
-        S.dirty[step] = 0;
+        norm_state_warp<N>(A, m, step, step, nbuf, sc, su);
+        if (w0) {
+            S.set(step, sc, su);
+            S.dirty[step] = 0;
+        }
+        __syncwarp();
         mf<N> pn = norm_value(sc, su);
         for (int64_t c = step + 1; c < S.n; ++c) {
             mf<N> cn = norm_value(S.sc(c), S.su(c));
             if (S.dirty[c] || iszero(pn) || ge(cn, mul(om, pn))) {
-                norm_state<N>(A, m, step, c, none, 0, 0, sc, su);
-                S.set(c, sc, su);
-                S.dirty[c] = 0;
+                norm_state_warp<N>(A, m, step, c, nbuf, sc, su);
+                __syncwarp();
+                if (w0) {
+                    S.set(c, sc, su);
+                    S.dirty[c] = 0;
+                }
+                __syncwarp();
                 cn = norm_value(sc, su);
             }
             bool eq = true;
@@ -327,7 +478,7 @@ __global__ void __launch_bounds__(QR_CTA)
                 pn = cn;
             }
         }
-        sp = piv;
+        if (w0) sp = piv;
     }
     __syncthreads();
     const int64_t piv = sp;
@@ -422,18 +573,20 @@ __global__ void __launch_bounds__(QR_PIVOT_CTA)
 // F row (gemv! trans = :T, then the correction through aux), the R row, and
 // the norm downdate; any column left unreliable raises *unreliable
 template <int N>
-__global__ void __launch_bounds__(QR_COLS_PER_CTA)
+__global__ void __launch_bounds__(32 * QR_COL_WARPS)
     qr_dlaqps_columns_kernel(int64_t m, int64_t step, int64_t bs, int64_t ls, Mat A,
                              const double *tau, int64_t lt, const double *aux, Mat F, QRNorms<N> S,
                              scal<N> floor_, int *unreliable) {
-    const int64_t c = step + 1 + (int64_t)blockIdx.x * QR_COLS_PER_CTA + threadIdx.x;
-    if (c >= S.n) return;
+    __shared__ double buf[QR_COL_WARPS][32 * N];
+    const int w = threadIdx.x >> 5;
+    const int64_t c = step + 1 + (int64_t)blockIdx.x * QR_COL_WARPS + w;
+    if (c >= S.n) return;  // whole warps leave together
     mf<N> t;
 #pragma unroll
     for (int l = 0; l < N; ++l) t.v[l] = tau[l * lt + step];
-    mf<N> acc = from_double<N>(0.0);
-    for (int64_t r = step; r < m; ++r)
-        acc = mac<N, false>(acc, load_mf<N>(A.p, A.ld, A.ls, r, c), load_mf<N>(A.p, A.ld, A.ls, r, step));
+    // gemv! trans = :T chain of column c with the reflector (rows step..m-1)
+    const mf<N> acc = chain_warp<N>(from_double<N>(0.0), step, m, A, c, A, step, buf[w]);
+    if ((threadIdx.x & 31) != 0) return;
     mf<N> f = mul(t, acc);
     if (ls > 0) {
         mf<N> corr = from_double<N>(0.0);
@@ -528,7 +681,7 @@ static int qr_n(mflab_handle *h, cudaStream_t s, int pivoted, int64_t m, int64_t
         for (int64_t st = 0; st < r; ++st) {
             qr_reflector_kernel<N><<<1, QR_CTA, 0, s>>>(m, st, A, tau, lt, 0, nullptr, 0, 0, nullptr);
             if (st + 1 < n)
-                qr_apply_kernel<N><<<col_grid(n - st - 1), QR_COLS_PER_CTA, 0, s>>>(
+                qr_apply_kernel<N><<<warp_col_grid(n - st - 1), 32 * QR_COL_WARPS, 0, s>>>(
                     m, st, A, tau, lt, A, st + 1, n - st - 1);
         }
     } else {
@@ -543,14 +696,14 @@ static int qr_n(mflab_handle *h, cudaStream_t s, int pivoted, int64_t m, int64_t
         }
         fl.v[0] = ldexp(1.0, 4 - 52 * N);
         if (n > 0)
-            qr_norm_init_kernel<N><<<col_grid(n), QR_COLS_PER_CTA, 0, s>>>(m, 0, 0, A, S);
+            qr_norm_init_kernel<N><<<norm_grid(n), 32 * QR_NORM_WARPS, 0, s>>>(m, 0, 0, A, S);
         const bool blocked = r >= QR_BLOCK && m * n >= 16384;
         if (!blocked) {
             for (int64_t st = 0; st < r; ++st) {
                 qr_hybrid_pivot_kernel<N><<<1, QR_CTA, 0, s>>>(m, st, A, perm, S, om);
                 qr_reflector_kernel<N><<<1, QR_CTA, 0, s>>>(m, st, A, tau, lt, 0, nullptr, 0, 0, nullptr);
                 if (st + 1 < n) {
-                    qr_apply_kernel<N><<<col_grid(n - st - 1), QR_COLS_PER_CTA, 0, s>>>(
+                    qr_apply_kernel<N><<<warp_col_grid(n - st - 1), 32 * QR_COL_WARPS, 0, s>>>(
                         m, st, A, tau, lt, A, st + 1, n - st - 1);
                     qr_update_norms_kernel<N><<<col_grid(n - st - 1), QR_COLS_PER_CTA, 0, s>>>(
                         m, st, A, tau, lt, S, fl);
@@ -576,7 +729,7 @@ static int qr_n(mflab_handle *h, cudaStream_t s, int pivoted, int64_t m, int64_t
                     qr_reflector_kernel<N><<<1, QR_CTA, 0, s>>>(m, st, A, tau, lt, 1, diag, bs, ls, aux);
                     qr_finite_kernel_init<<<1, 1, 0, s>>>(flag);
                     if (st + 1 < n)
-                        qr_dlaqps_columns_kernel<N><<<col_grid(n - st - 1), QR_COLS_PER_CTA, 0, s>>>(
+                        qr_dlaqps_columns_kernel<N><<<warp_col_grid(n - st - 1), 32 * QR_COL_WARPS, 0, s>>>(
                             m, st, bs, ls, A, tau, lt, aux, F, S, fl, flag);
                     qr_restore_diag_kernel<<<1, 1, 0, s>>>(N, A, st, diag);
                     actual = ls + 1;
@@ -597,7 +750,7 @@ static int qr_n(mflab_handle *h, cudaStream_t s, int pivoted, int64_t m, int64_t
                     if (rc) break;
                 }
                 if (be < n)
-                    qr_norm_init_kernel<N><<<col_grid(n - be), QR_COLS_PER_CTA, 0, s>>>(m, be, be, A, S);
+                    qr_norm_init_kernel<N><<<norm_grid(n - be), 32 * QR_NORM_WARPS, 0, s>>>(m, be, be, A, S);
                 bs = be;
             }
             cudaFreeHost(hflag);
@@ -642,11 +795,12 @@ extern "C" int mflab_apply_q(mflab_handle *h, void *stream, int limbs, int trans
     if (mfl::views_overlap(D, ldd, lsd, m, nd, limbs, F, ldf, lsf, m, r)) return MFLAB_ERR_ALIAS;
     const Mat Fm{(double *)F, ldf, lsf}, Dm{D, ldd, lsd};
     cudaStream_t s = (cudaStream_t)stream;
-    const unsigned g = mfl::col_grid(nd);
+    const unsigned g = mfl::warp_col_grid(nd);
+    const unsigned bt = 32 * mfl::QR_COL_WARPS;
     switch (limbs) {
-    case 2: mfl::qr_apply_all_kernel<2><<<g, mfl::QR_COLS_PER_CTA, 0, s>>>(m, r, Fm, tau, lst, Dm, nd, trans); break;
-    case 3: mfl::qr_apply_all_kernel<3><<<g, mfl::QR_COLS_PER_CTA, 0, s>>>(m, r, Fm, tau, lst, Dm, nd, trans); break;
-    default: mfl::qr_apply_all_kernel<4><<<g, mfl::QR_COLS_PER_CTA, 0, s>>>(m, r, Fm, tau, lst, Dm, nd, trans); break;
+    case 2: mfl::qr_apply_all_kernel<2><<<g, bt, 0, s>>>(m, r, Fm, tau, lst, Dm, nd, trans); break;
+    case 3: mfl::qr_apply_all_kernel<3><<<g, bt, 0, s>>>(m, r, Fm, tau, lst, Dm, nd, trans); break;
+    default: mfl::qr_apply_all_kernel<4><<<g, bt, 0, s>>>(m, r, Fm, tau, lst, Dm, nd, trans); break;
     }
     return mfl::record_cuda_error(cudaGetLastError(), "apply_q launch");
 }
