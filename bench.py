@@ -216,18 +216,32 @@ def fp64_peak(mf, torch) -> float:
     return best
 
 
-def read_traffic(kernel_key: str):
-    """dram bytes per launch from the committed ncu summary, if present."""
+def read_traffic(kernel_key: str, scale_from_smaller: bool = False):
+    """dram bytes per launch from the committed ncu summary, if present.  With
+    scale_from_smaller, a key "<prefix>_n<N>" missing at this N is taken from
+    the largest captured smaller N, times (N / N0)^2: for the residue GEMMs
+    at a fixed modulus count the operand and result bytes grow as n^2 (the
+    captures at n = 2048 and 4096 differ by 4.27x)."""
     p = os.path.join(REPO, "profiles", "ncu_traffic.txt")
     if not os.path.exists(p):
         return None
+    found = {}
     for line in open(p):
         if line.startswith("#") or "=" not in line:
             continue
         kv = dict(x.split("=", 1) for x in line.split())
-        if kv.get("key") == kernel_key:
-            return float(kv["dram_bytes_per_launch"])
-    return None
+        found[kv.get("key")] = float(kv["dram_bytes_per_launch"])
+    if kernel_key in found:
+        return found[kernel_key]
+    if not scale_from_smaller or "_n" not in kernel_key:
+        return None
+    prefix, n = kernel_key.rsplit("_n", 1)
+    smaller = [(int(k.rsplit("_n", 1)[1]), v) for k, v in found.items()
+               if k and k.rsplit("_n", 1)[0] == prefix and int(k.rsplit("_n", 1)[1]) < int(n)]
+    if not smaller:
+        return None
+    n0, v0 = max(smaller)
+    return v0 * (int(n) / n0) ** 2
 
 
 def ops_per_term(N: int) -> int:
@@ -701,7 +715,10 @@ def main():
         roof = {"bound": "tensor", "achieved": achieved / 1e12, "peak": peak8 / 1e12,
                 "unit": "INT8 TOP/s", "frac": achieved / peak8,
                 "frac_of_nominal_4500": achieved / 4.5e15,
-                "traffic": read_traffic(f"int8_tc_{scheme}_x{N}_n{n}"),
+                "traffic": read_traffic(f"int8_tc_{scheme}_x{N}_n{n}", scale_from_smaller=True),
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch "
+                                  "(profiles/ncu_traffic.txt); sizes above the largest capture "
+                                  "scaled by (n / n_capture)^2",
                 "kernel": "mfl::int8_tc_gemm_kernel (tcgen05.mma kind::i8, TMA, TMEM): the int8 "
                           + ("residue GEMMs, all moduli of a digit level in one launch"
                              if scheme == "modular" else "level GEMMs (K = (L-1) k)"),
