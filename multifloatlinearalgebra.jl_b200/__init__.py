@@ -1471,6 +1471,12 @@ def _leading_limb(X: MFMatrix) -> MFMatrix:
     return MFMatrix(st, 0, 0, X.m, X.n, X.is_vector)
 
 
+# panel width of the binary64 factor of solve_mixed_lu: its single-CTA panel
+# streams the panel through one SM, so narrow panels win (n = 4096 on B200:
+# 46 ms at 12, 50 ms at 16, 73 ms at 32)
+_LU64_PANEL = 12
+
+
 def solve_mixed_lu(A: MFMatrix, B: MFMatrix, tol: float = 0.0, maxiter: int = 40,
                    config: KernelConfig = _DEFAULT, residual: str = "int8") -> tuple:
     """Solve A X = B for a Float64xN matrix A with a binary64 partial-pivoting
@@ -1501,7 +1507,7 @@ def solve_mixed_lu(A: MFMatrix, B: MFMatrix, tol: float = 0.0, maxiter: int = 40
     ipiv = torch.arange(1, n + 1, dtype=torch.int64, device=dev)
     info = torch.zeros(1, dtype=torch.int32, device=dev)
     _check(lib.mflab_getrf(h, s, 1, n, n, LU.ptr(), LU.ld, LU.ls, ipiv.data_ptr() if n else None,
-                           max(config.lu_block, 1), info.data_ptr()), "lu! (binary64)")
+                           _LU64_PANEL, info.data_ptr()), "lu! (binary64)")
     st = _read_info(info)
     if st == -1:
         raise DomainError("lu!: input matrix contains non-finite entries")

@@ -371,7 +371,11 @@ __global__ void lu64_swap_kernel(int64_t n, Mat A, int64_t k0, int w, const int6
     }
 }
 
-static int getrf64_fast(int64_t m, int64_t n, Mat A, int64_t *ipiv, int *info, cudaStream_t s) {
+// panel width nb (4..32): the single-CTA panel update streams the panel
+// through one SM (its traffic grows with the width), the trailing GEMM is
+// the rest of the work
+static int getrf64_fast(int64_t m, int64_t n, Mat A, int64_t *ipiv, int *info, cudaStream_t s,
+                        int nb) {
     const double mone[1] = {-1.0}, one[1] = {1.0};
     cudaError_t e = cudaMemsetAsync(info, 0, sizeof(int), s);
     if (e != cudaSuccess) return record_cuda_error(e, "getrf info");
@@ -381,7 +385,7 @@ static int getrf64_fast(int64_t m, int64_t n, Mat A, int64_t *ipiv, int *info, c
     nonfinite_kernel<1><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(m, n, A, 0, info);
     int rc = record_cuda_error(cudaGetLastError(), "getrf check");
     if (rc) return rc;
-    const int NB = 32;
+    const int NB = nb < 4 ? 4 : (nb > 32 ? 32 : nb);
     for (int64_t k0 = 0; k0 < kmax; k0 += NB) {
         const int w = (int)(kmax - k0 < NB ? kmax - k0 : NB);
         lu64_panel_kernel<<<1, LU64_NT, 0, s>>>(m, A, k0, w, ipiv, info);
@@ -534,6 +538,74 @@ __global__ void apply_pivots_kernel(int64_t nrhs, Mat B, const int64_t *ipiv, in
             }
         }
     }
+}
+
+// The interchanges ipiv[0..n) (1-based, applied in ascending order) as one
+// gather: a single thread replays the swaps on an index array in shared
+// memory (row k ends up holding original row perm[k]), then every entry
+// moves once.  Same result as the sequential swaps, without a dependent
+// global-memory chain per right-hand side.
+__global__ void pivot_perm_kernel(int64_t n, const int64_t *ipiv, int *perm) {
+    extern __shared__ int sidx[];  // [n] indices, then [n] pivots
+    int *spiv = sidx + n;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+        sidx[i] = (int)i;
+        spiv[i] = (int)(ipiv[i] - 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int64_t k = 0; k < n; ++k) {
+            const int64_t p = spiv[k];
+            if (p != k) {
+                const int t = sidx[k];
+                sidx[k] = sidx[p];
+                sidx[p] = t;
+            }
+        }
+    }
+    __syncthreads();
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) perm[i] = sidx[i];
+}
+
+template <int N>
+__global__ void gather_rows_kernel(int64_t n, int64_t nrhs, Mat B, const double *src,
+                                   const int *perm) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n * nrhs) return;
+    const int64_t i = e % n, j = e / n;
+#pragma unroll
+    for (int l = 0; l < N; ++l)
+        B.p[l * B.ls + j * B.ld + i] = src[(l * nrhs + j) * n + perm[i]];
+}
+
+constexpr int64_t PIVOT_PERM_MAXN = 24576;  // indices and pivots in shared memory (192 KB)
+
+template <int N>
+static int apply_pivots_gather(mflab_handle *h, int64_t n, int64_t nrhs, Mat B,
+                               const int64_t *ipiv, cudaStream_t s) {
+    const size_t plane = (size_t)n * nrhs;
+    int rc = mflab_reserve_scratch(h, plane * N * sizeof(double) + (size_t)n * sizeof(int));
+    if (rc) return rc;
+    double *copy = (double *)h->scratch;
+    int *perm = (int *)(copy + plane * N);
+    const size_t smem = 2 * (size_t)n * sizeof(int);
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(pivot_perm_kernel,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)(2 * PIVOT_PERM_MAXN * sizeof(int)));
+        if (e != cudaSuccess) return record_cuda_error(e, "pivot perm attribute");
+        configured = true;
+    }
+    pivot_perm_kernel<<<1, 256, smem, s>>>(n, ipiv, perm);
+    for (int l = 0; l < N; ++l) {
+        cudaError_t e = cudaMemcpy2DAsync(copy + l * plane, n * sizeof(double), B.p + l * B.ls,
+                                          B.ld * sizeof(double), n * sizeof(double), nrhs,
+                                          cudaMemcpyDeviceToDevice, s);
+        if (e != cudaSuccess) return record_cuda_error(e, "getrs pivot copy");
+    }
+    gather_rows_kernel<N><<<(unsigned)((plane + 255) / 256), 256, 0, s>>>(n, nrhs, B, copy, perm);
+    return record_cuda_error(cudaGetLastError(), "getrs pivots");
 }
 
 // --------------------------------------------------------- diagnostics ---
@@ -724,7 +796,7 @@ extern "C" int mflab_getrf(mflab_handle *h, void *stream, int limbs, int64_t m, 
         if (rc) return rc;
     }
     switch (limbs) {
-    case 1: return mfl::getrf64_fast(m, n, a, ipiv, info, s);
+    case 1: return mfl::getrf64_fast(m, n, a, ipiv, info, s, (int)block);
     case 2: return mfl::getrf_n<2>(m, n, a, ipiv, block, info, s);
     case 3: return mfl::getrf_n<3>(m, n, a, ipiv, block, info, s);
     default: return mfl::getrf_n<4>(m, n, a, ipiv, block, info, s);
@@ -764,13 +836,23 @@ extern "C" int mflab_getrs(mflab_handle *h, void *stream, int limbs, int64_t n, 
     cudaStream_t s = (cudaStream_t)stream;
     Mat a{(double *)LU, ldl, lsl}, b{B, ldb, lsb};
     unsigned g = (unsigned)((nrhs + 127) / 128);
-    switch (limbs) {
-    case 1: mfl::apply_pivots_kernel<1><<<g, 128, 0, s>>>(nrhs, b, ipiv, n, 0); break;
-    case 2: mfl::apply_pivots_kernel<2><<<g, 128, 0, s>>>(nrhs, b, ipiv, n, 0); break;
-    case 3: mfl::apply_pivots_kernel<3><<<g, 128, 0, s>>>(nrhs, b, ipiv, n, 0); break;
-    default: mfl::apply_pivots_kernel<4><<<g, 128, 0, s>>>(nrhs, b, ipiv, n, 0); break;
+    int rc = MFLAB_OK;
+    if (n <= mfl::PIVOT_PERM_MAXN) {
+        switch (limbs) {
+        case 1: rc = mfl::apply_pivots_gather<1>(h, n, nrhs, b, ipiv, s); break;
+        case 2: rc = mfl::apply_pivots_gather<2>(h, n, nrhs, b, ipiv, s); break;
+        case 3: rc = mfl::apply_pivots_gather<3>(h, n, nrhs, b, ipiv, s); break;
+        default: rc = mfl::apply_pivots_gather<4>(h, n, nrhs, b, ipiv, s); break;
+        }
+    } else {
+        switch (limbs) {
+        case 1: mfl::apply_pivots_kernel<1><<<g, 128, 0, s>>>(nrhs, b, ipiv, n, 0); break;
+        case 2: mfl::apply_pivots_kernel<2><<<g, 128, 0, s>>>(nrhs, b, ipiv, n, 0); break;
+        case 3: mfl::apply_pivots_kernel<3><<<g, 128, 0, s>>>(nrhs, b, ipiv, n, 0); break;
+        default: mfl::apply_pivots_kernel<4><<<g, 128, 0, s>>>(nrhs, b, ipiv, n, 0); break;
+        }
+        rc = mfl::record_cuda_error(cudaGetLastError(), "getrs pivots");
     }
-    int rc = mfl::record_cuda_error(cudaGetLastError(), "getrs pivots");
     if (rc) return rc;
     rc = mfl::launch_trsm_info(limbs, 0, 0, 0, 1, n, nrhs, a, b, one, s, nullptr, h->solve_order);
     if (rc) return rc;
