@@ -199,13 +199,10 @@ static int run_mm(int64_t m, int64_t n, int64_t k, Mat A, Mat B, Mat C, const do
                   const double *beta, cudaStream_t s, const int *info, int mode) {
     using S = MMShape<N, BM, BN, BK, TM, TN>;
     auto kern = mm_kernel<N, BM, BN, BK, TM, TN, TA, TB, TRI, FUSED, TRMM>;
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)S::smem_bytes);
-        if (e != cudaSuccess) return record_cuda_error(e, "mm_kernel attribute");
-        configured = true;
-    }
+    static std::atomic<unsigned long long> configured{0};
+    if (int rc = set_smem_once((const void *)kern, (int)S::smem_bytes, configured,
+                               "mm_kernel attribute"))
+        return rc;
     scal<N> al{}, be{};
     int overwrite = 1;
     for (int l = 0; l < N; ++l) {

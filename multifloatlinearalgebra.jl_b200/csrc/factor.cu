@@ -589,14 +589,10 @@ static int apply_pivots_gather(mflab_handle *h, int64_t n, int64_t nrhs, Mat B,
     double *copy = (double *)h->scratch;
     int *perm = (int *)(copy + plane * N);
     const size_t smem = 2 * (size_t)n * sizeof(int);
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(pivot_perm_kernel,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)(2 * PIVOT_PERM_MAXN * sizeof(int)));
-        if (e != cudaSuccess) return record_cuda_error(e, "pivot perm attribute");
-        configured = true;
-    }
+    static std::atomic<unsigned long long> configured{0};
+    rc = set_smem_once((const void *)pivot_perm_kernel, (int)(2 * PIVOT_PERM_MAXN * sizeof(int)),
+                       configured, "pivot perm attribute");
+    if (rc) return rc;
     pivot_perm_kernel<<<1, 256, smem, s>>>(n, ipiv, perm);
     for (int l = 0; l < N; ++l) {
         cudaError_t e = cudaMemcpy2DAsync(copy + l * plane, n * sizeof(double), B.p + l * B.ls,

@@ -405,13 +405,10 @@ static int launch_tc(int64_t mp, int64_t np, int64_t K, const int8_t *A, int64_t
     if (rc) return rc;
     rc = make_map(&tb, B, np * nz, b_cols, ldb, TC_BN);
     if (rc) return rc;
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(int8_tc_gemm_kernel<MODE>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
-        if (e != cudaSuccess) return record_cuda_error(e, "int8 tc attribute");
-        configured = true;
-    }
+    static std::atomic<unsigned long long> configured{0};
+    rc = set_smem_once((const void *)int8_tc_gemm_kernel<MODE>, (int)TC_SMEM, configured,
+                       "int8 tc attribute");
+    if (rc) return rc;
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0)

@@ -4,6 +4,8 @@
 #include <cstdint>
 #include <cstdio>
 
+#include <atomic>
+
 #include "../../include/mflab200.h"
 
 namespace mfl {
@@ -35,12 +37,29 @@ int launch_trsm_info(int N, int side, int uplo, int trans, int diag, int64_t m, 
                      Mat B, const double *alpha, cudaStream_t s, const int *info,
                      int order = 0);
 
+int record_cuda_error(cudaError_t e, const char *where);
+
+// cudaFuncSetAttribute(MaxDynamicSharedMemorySize) of a kernel once per
+// device of the process (the attribute is per device); `done` is the
+// kernel's own bit mask of configured devices.  Thread-safe.
+inline int set_smem_once(const void *func, int bytes, std::atomic<unsigned long long> &done,
+                         const char *what) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return record_cuda_error(e, what);
+    const unsigned long long bit = 1ULL << (dev & 63);
+    if (done.load(std::memory_order_acquire) & bit) return 0;
+    e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return record_cuda_error(e, what);
+    done.fetch_or(bit, std::memory_order_release);
+    return 0;
+}
+
 inline int cuda_status(cudaError_t e) {
     if (e == cudaSuccess) return MFLAB_OK;
     return MFLAB_ERR_CUDA;
 }
 
-int record_cuda_error(cudaError_t e, const char *where);
 
 // int8 x int8 -> int32 TN GEMM through the library (ozaki.cu) and through the
 // tcgen05 kernel (int8_tc.cu)

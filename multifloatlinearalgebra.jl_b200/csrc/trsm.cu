@@ -258,14 +258,10 @@ static int run_trsm(int side, int uplo, int trans, int diag, int64_t m, int64_t 
         return trsm64_blocked(m, n, A, B, eff_lower, unit, s, info);
     if (!eff_lower && !wavefront_ok && m > 64 && n < 4096 && (size_t)m * N * 8 <= 200 * 1024) {
         const size_t smem = (size_t)m * N * sizeof(double);
-        static bool configured = false;
-        if (!configured) {
-            cudaError_t e = cudaFuncSetAttribute(trsm_left_backward_cta<N, 256>,
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 200 * 1024);
-            if (e != cudaSuccess) return record_cuda_error(e, "trsm backward attribute");
-            configured = true;
-        }
+        static std::atomic<unsigned long long> configured{0};
+        if (int rc = set_smem_once((const void *)trsm_left_backward_cta<N, 256>, 200 * 1024,
+                                   configured, "trsm backward attribute"))
+            return rc;
         trsm_left_backward_cta<N, 256><<<(unsigned)n, 256, smem, s>>>(m, n, A, B, transposed,
                                                                        unit, info);
         return record_cuda_error(cudaGetLastError(), "trsm left backward");
