@@ -308,16 +308,28 @@ static inline dim3 crt_split_b_grid(int64_t np, int64_t kp) {
 }
 
 // ------------------------------------------------------ reconstruction ----
+// q = round(X / P) from the chunk sums: X ~ sum_c A_c 2^(39 c) by Horner
+// (relative error below 2^-49), and X / P lies within 3/8 of an integer
+template <int WP>
+__host__ __device__ __forceinline__ uint32_t crt_quotient(const double (&A)[CrtChunks<WP>::value],
+                                                         double pinv) {
+    constexpr int NC = CrtChunks<WP>::value;
+    double xd = A[NC - 1];
+#pragma unroll
+    for (int cc = NC - 2; cc >= 0; --cc) xd = fma(xd, 549755813888.0, A[cc]);  // 2^39
+    return (uint32_t)floor(xd * pinv + 0.5);
+}
+
 // X (WP words of 64-bit partial sums) -> G = X - round(X / P) P as magnitude
 // words + sign (host and device: the host copy backs
 // mflab_ozaki_crt_reduce_host).  Precondition, kept by the planner: the
 // represented value satisfies |G| <= 3P / 8 (it is G mod P in the symmetric
 // range), so X / P lies within 3/8 of the integer q = round(X / P) and the
-// double estimate of X / P (relative error < 2^-48) rounds to exactly q.
-// All products are 32 x 32 -> 64 bit.
+// double estimate of X / P (crt_quotient, relative error < 2^-48) rounds to
+// exactly the q passed in.  All products are 32 x 32 -> 64 bit.
 template <int WP>
 __host__ __device__ __forceinline__ bool crt_reduce(const uint64_t (&X)[WP], const uint32_t *Pw,
-                                                    double pinv, uint32_t (&mag)[WP]) {
+                                                    uint32_t q, uint32_t (&mag)[WP]) {
     uint32_t x[WP];
     uint64_t cy = 0;
 #pragma unroll
@@ -326,10 +338,6 @@ __host__ __device__ __forceinline__ bool crt_reduce(const uint64_t (&X)[WP], con
         x[w] = (uint32_t)s;
         cy = s >> 32;
     }
-    double xd = 0.0;
-#pragma unroll
-    for (int w = WP - 1; w >= 0; --w) xd = fma(xd, 4294967296.0, (double)x[w]);
-    const uint32_t q = (uint32_t)floor(xd * pinv + 0.5);
     // Y = X - q P (two's complement over WP words; the final borrow is the sign)
     uint32_t y[WP];
     uint64_t hi = 0;   // carry of q P
@@ -467,7 +475,7 @@ __global__ void __launch_bounds__(CRT_ACC_ROWS, 3)
             uint64_t X[WP];
             crt_chunks_to_words<WP>(A, X);
             uint32_t mag[WP];
-            const bool ng = crt_reduce<WP>(X, c.P, c.pinv, mag);
+            const bool ng = crt_reduce<WP>(X, c.P, crt_quotient<WP>(A, c.pinv), mag);
             const int sh = oz_scale_exp(ea) + oz_scale_exp(eb) - 2 * Q * h + h * (2 * Q - 2 - L);
             mf<N> g = crt_words_to_mf<N, WP>(mag, sh);
             if (ng) g = neg(g);
@@ -1007,7 +1015,7 @@ extern "C" int mflab_ozaki_crt_reduce_host(int T, int count, const int32_t *G, u
         uint64_t X[CRT_WP];
         crt_chunks_to_words<CRT_WP>(A, X);
         uint32_t mg[CRT_WP];
-        neg[e] = crt_reduce<CRT_WP>(X, c.P, c.pinv, mg) ? 1 : 0;
+        neg[e] = crt_reduce<CRT_WP>(X, c.P, crt_quotient<CRT_WP>(A, c.pinv), mg) ? 1 : 0;
         for (int w = 0; w < CRT_WP; ++w) mag[(size_t)e * CRT_WP + w] = mg[w];
     }
     return MFLAB_OK;
