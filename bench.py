@@ -53,6 +53,8 @@ def parse():
     p.add_argument("--no-x4", action="store_true", help="skip the Float64x4 companion run")
     p.add_argument("--no-configs", action="store_true",
                    help="skip the factorization / mixed-LU / batched-SPD workloads")
+    p.add_argument("--config-reps", type=int, default=3,
+                   help="timed repeats (after one warm-up) of each of those workloads")
     return p.parse_args()
 
 
@@ -436,154 +438,264 @@ class Runner:
         return 2.0 * n * n * k / (ms.value / 1e3)
 
 
-def _time_once(torch, fn):
-    """device time of one call (events on the current stream)"""
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    e0.record()
+def _time_median(torch, fn, setup=None, reps=3, warmup=1):
+    """median device time (CUDA events on the current stream) of fn over
+    `reps` calls after `warmup` untimed ones; setup() restores the inputs
+    before every call, outside the timed region.  Returns (median s, all
+    times in ms, last result)."""
+    times, out = [], None
+    for r in range(warmup + reps):
+        if setup is not None:
+            setup()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        out = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        if r >= warmup:
+            times.append(e0.elapsed_time(e1))
+    return statistics.median(times) / 1e3, [round(t, 3) for t in times], out
+
+
+def _fp64_roof(instr: float, seconds: float, peak: float) -> dict:
+    """FP64-pipe roofline of a multi-double kernel sequence: FP64
+    instructions of its multiply-add networks over the DFMA probe rate"""
+    a = instr / seconds
+    return {"bound": "fp64", "achieved": a / 1e12, "peak": peak / 1e12, "unit": "T FP64 instr/s",
+            "frac": a / peak, "peak_source": "measured in this run (DFMA probe, burst)"}
+
+
+def _cpu_timed(fn):
+    t0 = time.perf_counter()
     out = fn()
-    e1.record()
-    torch.cuda.synchronize()
-    return e0.elapsed_time(e1) / 1e3, out
+    return time.perf_counter() - t0, out
 
 
-def run_configs(R, torch):
-    """Cholesky + multi-RHS solve (n=2048, 64 RHS, x2/x3/x4), mixed-precision
-    LU (n=4096, 16 RHS) against the plain Float64x4 LU, and 10,000 batched SPD
-    blocks (x2, sizes U{8..256}) with the adjoint; device times, backward
-    errors from the device residual kernels, CPU-oracle rates beside them."""
+def config_cholesky(R, torch, peak, reps):
+    """Cholesky + 64-RHS solve, n = 2048, Float64x2/x3/x4 (S = R R^T + n I)"""
     import numpy as np
     mf, syn = R.mf, R.syn
     from oracle import mfref
     threads = mfref.threads()
-    out = {}
-    # --- Cholesky + 64-RHS solve, n = 2048 ------------------------------
     n, nrhs = 2048, 64
-    chol = {}
+    out = {}
     for N in (2, 3, 4):
-        g = torch.Generator(device="cuda")
-        g.manual_seed(7 + N)
-        Rp = syn.randn_mf_device(70 + N, N, n, n)
-        Rm = mf.MFMatrix.from_tensor(Rp)
-        S = mf.MFMatrix.zeros(N, n, n)
-        # S = R R^T + n I (x4-accurate GEMM, then symmetric by construction of the lower triangle)
-        Rt = mf.MFMatrix.from_tensor(Rp.transpose(1, 2).contiguous())
-        mf.gemm_(S, Rm, Rt)
-        S.storage[0].diagonal().add_(float(n))
-        Bm = mf.MFMatrix.from_tensor(syn.randn_mf_device(80 + N, N, n, nrhs))
+        S = syn.spd_matrix_device(mf, 70 + N, N, n)
+        Bn = syn.randn_mf(np.random.default_rng(80 + N), N, n, nrhs)
+        Bm = mf.MFMatrix.from_numpy(Bn)
         Sw = S.copy()
-        t_f, F = _time_once(torch, lambda: mf.cholesky_(Sw))
-        t_s, X = _time_once(torch, lambda: mf.solve(F, Bm))
-        # the wavefront ("fast") solve order, an option beside the matched one
-        t_sf, _ = _time_once(torch, lambda: mf.solve(F, Bm,
-                                                     config=mf.KernelConfig(solve_order="fast")))
-        Rr = mf.MFMatrix.zeros(N, n, nrhs)
-        mf.residual_(Rr, S, X, Bm, uplo="lower")
-        be = mf.normwise_backward_error(S, X, Bm, Rr, uplo="lower")
-        work = n ** 3 / 3.0 + 2.0 * n * n * nrhs
+        t_f, ts_f, F = _time_median(torch, lambda: mf.cholesky_(Sw), lambda: Sw.copy_(S), reps)
+        t_s, ts_s, X = _time_median(torch, lambda: mf.solve(F, Bm), None, reps)
+        fast = mf.KernelConfig(solve_order="fast")
+        t_sf, _, _ = _time_median(torch, lambda: mf.solve(F, Bm, config=fast), None, reps)
         # the same factorization with INT8 (modular) trailing updates between
-        # 256-column panels; solved with the same matched-order solves
+        # 256-column panels, solved with the matched-order solves
         Sw2 = S.copy()
         ocfg = mf.KernelConfig(gemm_strategy="ozaki", ozaki_scheme="modular", ozaki_block=256)
-        t_fo, Fo = _time_once(torch, lambda: mf.cholesky_(Sw2, config=ocfg))
+        t_fo, ts_fo, Fo = _time_median(torch, lambda: mf.cholesky_(Sw2, config=ocfg),
+                                       lambda: Sw2.copy_(S), reps)
         Xo = mf.solve(Fo, Bm)
-        mf.residual_(Rr, S, Xo, Bm, uplo="lower")
-        beo = mf.normwise_backward_error(S, Xo, Bm, Rr, uplo="lower")
-        del Sw2, Fo, Xo
-        # CPU: the oracle's blocked Cholesky at n=512 (scaled to a rate)
-        rng = np.random.default_rng(3)
-        nc = 512
-        Sc = syn.spd_matrix(rng, N, nc, lambda a, b: mfref.gemm(a, b, nthreads=threads))
-        t0 = time.perf_counter()
-        mfref.potrf(Sc, nthreads=threads)
-        tc = time.perf_counter() - t0
-        chol[f"x{N}"] = {"factor_ms": t_f * 1e3, "solve_ms": t_s * 1e3,
-                         "solve_fast_order_ms": t_sf * 1e3,
-                         "md_gflops": work / (t_f + t_s) / 1e9,
-                         "max_backward_error": float(max(v[0] for v in be)),
-                         "cpu_oracle_md_gflops_n512": nc ** 3 / 3.0 / tc / 1e9,
-                         "cpu_threads": threads,
-                         "int8_trailing": {"factor_ms": t_fo * 1e3,
-                                           "factor_speedup_vs_matched": t_f / t_fo,
-                                           "max_backward_error": float(max(v[0] for v in beo)),
-                                           "panel": 256}}
-        del S, Sw, F, X, Rr, Rm, Rt, Bm
+        # parity: exact (superaccumulator) backward errors of four columns, and
+        # for Float64x2 the full factor and solve bitwise against the oracle
+        Sn, Xn, Xon = S.to_numpy(), X.to_numpy(), Xo.to_numpy()
+        cols = [0, 21, 42, 63]
+        be = mfref.backward_error(Sn, Xn[:, :, cols], Bn[:, :, cols])
+        beo = mfref.backward_error(Sn, Xon[:, :, cols], Bn[:, :, cols])
+        parity = {"exact_backward_error_max": float(be.max()),
+                  "int8_trailing_exact_backward_error_max": float(beo.max()),
+                  "columns_checked": cols, "bound": 4096 * n * 2.0 ** (-52 * N),
+                  "oracle": "superaccumulator residual ||b - S x||_inf / (||S|| ||x|| + ||b||)"}
+        cpu = {}
+        if N == 2:
+            t_cf, (L, info) = _cpu_timed(lambda: mfref.potrf(Sn, nthreads=threads))
+            t_cs, Xr = _cpu_timed(lambda: mfref.potrs(L, Bn, nthreads=threads))
+            parity["bitwise_factor_and_solve_vs_oracle"] = bool(
+                info == 0 and np.array_equal(np.tril(Sw.to_numpy()).view(np.uint64),
+                                             np.tril(L).view(np.uint64))
+                and np.array_equal(Xn.view(np.uint64), Xr.view(np.uint64)))
+            cpu["all_cores"] = {"md_gflops": (n ** 3 / 3.0 + 2.0 * n * n * nrhs) / (t_cf + t_cs)
+                                / 1e9, "cores": threads, "factor_s": t_cf, "solve_s": t_cs,
+                                "sample": f"full n={n}, {nrhs} RHS"}
+        else:
+            nc = 1024
+            Sc = syn.spd_matrix(np.random.default_rng(3), N, nc,
+                                lambda a, b: mfref.gemm(a, b, nthreads=threads))
+            Bc = syn.randn_mf(np.random.default_rng(4), N, nc, nrhs)
+            t_cf, (L, _) = _cpu_timed(lambda: mfref.potrf(Sc, nthreads=threads))
+            t_cs, _ = _cpu_timed(lambda: mfref.potrs(L, Bc, nthreads=threads))
+            cpu["all_cores"] = {"md_gflops": (nc ** 3 / 3.0 + 2.0 * nc * nc * nrhs) / (t_cf + t_cs)
+                                / 1e9, "cores": threads, "factor_s": t_cf, "solve_s": t_cs,
+                                "sample": f"n={nc}, {nrhs} RHS (rate; the n={n} time scales "
+                                          "as n^3 for the factor, n^2 for the solves)"}
+        n1 = 512
+        S1 = syn.spd_matrix(np.random.default_rng(5), N, n1,
+                            lambda a, b: mfref.gemm(a, b, nthreads=threads))
+        B1 = syn.randn_mf(np.random.default_rng(6), N, n1, nrhs)
+        t1f, (L1, _) = _cpu_timed(lambda: mfref.potrf(S1, nthreads=1))
+        t1s, _ = _cpu_timed(lambda: mfref.potrs(L1, B1, nthreads=1))
+        cpu["one_core"] = {"md_gflops": (n1 ** 3 / 3.0 + 2.0 * n1 * n1 * nrhs) / (t1f + t1s) / 1e9,
+                           "cores": 1, "factor_s": t1f, "solve_s": t1s,
+                           "sample": f"n={n1}, {nrhs} RHS (rate)"}
+        cpu["kind"] = "port"
+        work = n ** 3 / 3.0 + 2.0 * n * n * nrhs
+        ops = ops_per_term(N)
+        out[f"x{N}"] = {
+            "factor_ms": t_f * 1e3, "solve_ms": t_s * 1e3, "solve_fast_order_ms": t_sf * 1e3,
+            "repeats_ms": {"factor": ts_f, "solve": ts_s, "int8_trailing_factor": ts_fo},
+            "md_gflops": work / (t_f + t_s) / 1e9,
+            "roofline_factor": _fp64_roof(n ** 3 / 6.0 * ops, t_f, peak),
+            "roofline_solve": _fp64_roof(float(n) * n * nrhs * ops, t_s, peak),
+            "int8_trailing": {"factor_ms": t_fo * 1e3, "factor_speedup_vs_matched": t_f / t_fo,
+                              "panel": 256},
+            "parity": parity, "cpu_baseline": cpu}
+        del S, Sw, Sw2, F, Fo, X, Xo, Bm
         torch.cuda.empty_cache()
-    out["cholesky_n2048_rhs64"] = chol
-    # --- mixed-precision LU vs plain Float64x4 LU, n = 4096 --------------
+    return out
+
+
+def config_mixed_lu(R, torch, peak, reps):
+    """mixed-precision LU solve (binary64 factor, Float64x4 refinement), n =
+    4096, 16 RHS, against the plain Float64x4 LU"""
+    import numpy as np
+    mf, syn = R.mf, R.syn
+    from oracle import mfref
+    threads = mfref.threads()
     n, nrhs = 4096, 16
     A, B = syn.mixed_lu_problem(mf, n, nrhs, seed=4)
-    t_m, (X, rep) = _time_once(torch, lambda: mf.solve_mixed_lu(A, B, tol=1e-60))
+    t_m, ts_m, (X, rep) = _time_median(
+        torch, lambda: mf.solve_mixed_lu(A, B, tol=1e-60, timing=True), None, reps)
     Aw = A.copy()
-
-    def plain():
-        F = mf.lu_(Aw)
-        return mf.solve(F, B)
-
-    t_p, Xp = _time_once(torch, plain)
-    Rr = mf.MFMatrix.zeros(4, n, nrhs)
-    mf.residual_(Rr, A, Xp, B)
-    be_p = float(max(v[0] for v in mf.normwise_backward_error(A, Xp, B, Rr)))
-    # the same Float64x4 LU with INT8 (modular) trailing updates between
-    # 256-column panels, solved with the same matched-order solves
+    t_p, ts_p, Xp = _time_median(torch, lambda: mf.solve(mf.lu_(Aw), B), lambda: Aw.copy_(A),
+                                 reps)
     Aw2 = A.copy()
     ocfg = mf.KernelConfig(gemm_strategy="ozaki", ozaki_scheme="modular", ozaki_block=256)
-
-    def int8_lu():
-        F = mf.lu_(Aw2, config=ocfg)
-        return mf.solve(F, B)
-
-    t_o, Xo = _time_once(torch, int8_lu)
-    mf.residual_(Rr, A, Xo, B)
-    be_o = float(max(v[0] for v in mf.normwise_backward_error(A, Xo, B, Rr)))
-    del Aw2, Xo
-    out["mixed_lu_n4096_rhs16"] = {
-        "mixed_ms": t_m * 1e3, "iterations": rep["iterations"],
-        "mixed_backward_error": rep["backward_error"], "plain_x4_ms": t_p * 1e3,
-        "plain_x4_backward_error": be_p, "speedup_vs_plain_x4": t_p / t_m,
-        "int8_trailing_x4_ms": t_o * 1e3, "int8_trailing_x4_backward_error": be_o,
+    t_o, ts_o, Xo = _time_median(torch, lambda: mf.solve(mf.lu_(Aw2, config=ocfg), B),
+                                 lambda: Aw2.copy_(A), reps)
+    # parity: exact backward errors of four columns of every solution
+    An, Bn = A.to_numpy(), B.to_numpy()
+    cols = [0, 5, 10, 15]
+    be = lambda Xm: float(mfref.backward_error(An, Xm.to_numpy()[:, :, cols], Bn[:, :, cols]).max())
+    parity = {"mixed_exact_backward_error_max": be(X), "plain_x4_exact_backward_error_max": be(Xp),
+              "int8_trailing_x4_exact_backward_error_max": be(Xo), "columns_checked": cols,
+              "target": 1e-60,
+              "oracle": "superaccumulator residual ||b - A x||_inf / (||A|| ||x|| + ||b||)"}
+    # CPU: the reference's route for a Float64x4 system (lu! + ldiv! in x4)
+    cpu = {"kind": "port"}
+    for key, nc, th in (("all_cores", 512, threads), ("one_core", 256, 1)):
+        Ac = syn.randn_mf(np.random.default_rng(7), 4, nc, nc)
+        Bc = syn.randn_mf(np.random.default_rng(8), 4, nc, nrhs)
+        t_cf, (LU, piv, _) = _cpu_timed(lambda: mfref.getrf(Ac, nthreads=th))
+        t_cs, _ = _cpu_timed(lambda: mfref.getrs(LU, piv, Bc, nthreads=th))
+        w = 2.0 * nc ** 3 / 3.0 + 2.0 * nc * nc * nrhs
+        cpu[key] = {"md_gflops": w / (t_cf + t_cs) / 1e9, "cores": th,
+                    "extrapolated_n4096_s": (t_cf * (n / nc) ** 3 + t_cs * (n / nc) ** 2),
+                    "sample": f"Float64x4 LU + {nrhs}-RHS solve at n={nc}, scaled as n^3 (factor) "
+                              "and n^2 (solves) to n=4096"}
+    flops64 = 2.0 * n ** 3 / 3.0
+    out = {
+        "mixed_ms": t_m * 1e3, "repeats_ms": {"mixed": ts_m, "plain_x4": ts_p, "int8_x4": ts_o},
+        "binary64_factor_ms": rep["factor_ms"], "refinement_ms": rep["refine_ms"],
+        "iterations": rep["iterations"], "mixed_backward_error": rep["backward_error"],
+        "plain_x4_ms": t_p * 1e3, "speedup_vs_plain_x4": t_p / t_m,
+        "int8_trailing_x4_ms": t_o * 1e3,
+        "roofline_binary64_factor": {"bound": "fp64", "unit": "TFLOP/s",
+                                     "achieved": flops64 / (rep["factor_ms"] / 1e3) / 1e12,
+                                     "peak": 2 * peak / 1e12,
+                                     "frac": flops64 / (rep["factor_ms"] / 1e3) / (2 * peak),
+                                     "peak_source": "2 x DFMA probe instruction rate"},
+        "roofline_plain_x4": _fp64_roof(n ** 3 / 3.0 * ops_per_term(4) + float(n) * n * nrhs
+                                        * ops_per_term(4), t_p, peak),
+        "parity": parity, "cpu_baseline": cpu,
         "matrix": "U diag(sigma) V^T, sigma geometric 1 -> 1e-12, lifted to Float64x4"}
-    del A, B, X, Aw, Xp, Rr
+    del A, B, X, Aw, Aw2, Xp, Xo
     torch.cuda.empty_cache()
-    # --- 10,000 batched SPD blocks, Float64x2 ------------------------------
+    return out
+
+
+def config_batched(R, torch, peak, reps):
+    """10,000 batched Float64x2 SPD blocks, sizes U{8..256}, factor + solve in
+    one graph-captured persistent launch, and the adjoint"""
+    import numpy as np
+    from concurrent.futures import ThreadPoolExecutor
+    mf, syn = R.mf, R.syn
+    from oracle import mfref
+    threads = mfref.threads()
     rng = np.random.default_rng(5)
     sizes = rng.integers(8, 257, 10000)
     batch = mf.batched.SPDBatch(2, sizes)
-    tot = int(batch.total_s)
-    # S_i = R_i R_i^T + n_i I: generated per size class on the device
-    Rbuf = torch.empty((2, tot), dtype=torch.float64, device="cuda")
-    Rbuf[0].normal_()
-    Rbuf[1].normal_()
-    Rbuf[1] *= 2.0 ** -53 * Rbuf[0].abs()
-    for i in range(batch.nblocks):
-        ni, o = int(sizes[i]), int(batch.offsets_host[i])
-        Rb = Rbuf[0, o:o + ni * ni].view(ni, ni)
-        batch.S[0, o:o + ni * ni] = (Rb @ Rb.t() + ni * torch.eye(ni, dtype=torch.float64,
-                                                                  device="cuda")).reshape(-1)
-    batch.S[1].zero_()
-    batch.X[0].normal_()
+    syn.spd_batch_fill(mf, batch, seed=5)
     S0, X0 = batch.S.clone(), batch.X.clone()
     tuned = mf.batched.autotune(batch)  # launch shape timed on the batch itself
     graph = mf.batched.BatchedSPDGraph(batch, tuning=tuned)
-    batch.S.copy_(S0)
-    batch.X.copy_(X0)
-    t_b, _ = _time_once(torch, graph.replay)
+
+    def restore():
+        batch.S.copy_(S0)
+        batch.X.copy_(X0)
+
+    t_b, ts_b, _ = _time_median(torch, graph.replay, restore, reps)
     info = batch.info[:batch.nblocks].cpu().numpy()
-    x, pullback = None, None
-    batch.S.copy_(S0)
-    batch.X.copy_(X0)
+    restore()
     x, pullback = mf.batched.solve_spd_batched_rrule(batch, tuning=tuned)
-    w = torch.randn_like(x)
-    w[1].zero_()
-    t_a, _ = _time_once(torch, lambda: pullback(w))
-    out["batched_spd_10000_x2"] = {
-        "factor_solve_ms": t_b * 1e3, "md_gflops": batch.flops() / t_b / 1e9,
-        "adjoint_ms": t_a * 1e3, "failed_blocks": int(np.count_nonzero(info)),
+    w = syn.randn_planes_device(17, 2, x.shape[1])
+    t_a, ts_a, _ = _time_median(torch, lambda: pullback(w), None, reps)
+    # parity: 16 blocks (the 4 largest, the 4 smallest, 8 random) bitwise
+    # against the oracle's per-block Cholesky and solve
+    picks = np.concatenate([np.argsort(-sizes)[:4], np.argsort(sizes)[:4],
+                            np.random.default_rng(9).choice(len(sizes), 8, replace=False)])
+    ok, bes = True, []
+    for i in picks:
+        Si, bi = batch.block(i, S0), batch.rhs(i, X0)
+        L, inf = mfref.potrf(Si)
+        xr = mfref.potrs(L, bi[:, :, None])
+        ok = ok and inf == 0 and np.array_equal(np.tril(batch.block(i)).view(np.uint64),
+                                                np.tril(L).view(np.uint64)) \
+            and np.array_equal(batch.rhs(i).view(np.uint64), xr[:, :, 0].view(np.uint64))
+        Ss = np.tril(Si) + np.transpose(np.tril(Si, -1), (0, 2, 1))
+        bes.append(float(mfref.backward_error(Ss, xr, bi[:, :, None]).max()))
+    parity = {"blocks_checked": [int(i) for i in picks], "bitwise_vs_oracle": bool(ok),
+              "exact_backward_error_max": max(bes)}
+    # CPU: the oracle's Cholesky + solve per block on a 300-block sample,
+    # blocks spread over the host threads (all cores) and one after another
+    samp = np.random.default_rng(11).choice(len(sizes), 300, replace=False)
+    blocks = [(batch.block(i, S0), batch.rhs(i, X0)[:, :, None]) for i in samp]
+
+    def one(b):
+        L, _ = mfref.potrf(b[0], nthreads=1)
+        return mfref.potrs(L, b[1], nthreads=1)
+
+    wsamp = float(np.sum(sizes[samp].astype(float) ** 3 / 3 + 2.0 * sizes[samp].astype(float) ** 2))
+    t_all, _ = _cpu_timed(lambda: list(ThreadPoolExecutor(threads).map(one, blocks)))
+    t_one, _ = _cpu_timed(lambda: [one(b) for b in blocks])
+    cpu = {"kind": "port",
+           "all_cores": {"md_gflops": wsamp / t_all / 1e9, "cores": threads,
+                         "sample": "300 random blocks, one block per host thread at a time"},
+           "one_core": {"md_gflops": wsamp / t_one / 1e9, "cores": 1, "sample": "the same blocks"}}
+    nn = sizes.astype(np.float64)
+    instr = float(np.sum(nn ** 3 / 6.0 + nn * nn)) * ops_per_term(2)
+    out = {
+        "factor_solve_ms": t_b * 1e3, "repeats_ms": {"factor_solve": ts_b, "adjoint": ts_a},
+        "md_gflops": batch.flops() / t_b / 1e9, "adjoint_ms": t_a * 1e3,
+        "failed_blocks": int(np.count_nonzero(info)),
+        "roofline": _fp64_roof(instr, t_b, peak),
         "launch": "one persistent kernel (+ counter memset) replayed from a CUDA graph",
         "autotuned": {"threads": tuned["threads"], "grid": tuned["grid"],
                       "default_256x592_ms": tuned["timings"].get("256x592")},
-        "data": "S_i = R_i R_i^T + n_i I with binary64 R_i (seeded), sizes U{8..256}"}
+        "parity": parity, "cpu_baseline": cpu,
+        "data": "S_i = R_i R_i^T + n_i I, R_i randn Float64x2 with a populated low limb, one "
+                "randn Float64x2 right-hand side per block (seeded)"}
+    del graph, batch, S0, X0, x
+    torch.cuda.empty_cache()
     return out
+
+
+def run_configs(R, torch, peak, reps=3):
+    """The other benchmark workloads beside the GEMM headline: device times
+    (median of `reps` after a warm-up), FP64-pipe rooflines, oracle parity
+    and CPU-oracle rates on all host cores and on one core."""
+    return {"cholesky_n2048_rhs64": config_cholesky(R, torch, peak, reps),
+            "mixed_lu_n4096_rhs16": config_mixed_lu(R, torch, peak, reps),
+            "batched_spd_10000_x2": config_batched(R, torch, peak, reps)}
 
 
 def main():
@@ -649,17 +761,22 @@ def main():
     t_plain = R.timed(lambda: mf.gemm_(Cm, A, B, config=plain_cfg), 1, 1) if route == "ozaki" \
         else t_head
 
-    # end to end through the public API with host buffers: every step uploads
-    # its A and B from pinned host memory, multiplies, and downloads C; the
-    # upload of step i+1 and the download of step i-1 run on their own streams
-    # while step i multiplies (two device buffer sets)
-    hA = torch.empty((N, n, n), dtype=torch.float64, pin_memory=True)
-    hB = torch.empty((N, n, n), dtype=torch.float64, pin_memory=True)
-    hC = torch.empty((N, n, n), dtype=torch.float64, pin_memory=True)
-    hA.copy_(A.storage)
-    hB.copy_(B.storage)
-    bufs = [(torch.empty_like(A.storage), torch.empty_like(B.storage),
-             torch.empty_like(Cm.storage)) for _ in range(2)]
+    # end to end through the public API with host buffers in the reference's
+    # own storage order (a Julia Matrix{Float64xN} keeps the N limbs of an
+    # element together): every step uploads A and B from pinned interleaved
+    # host memory into limb planes (mflab_h2d_interleaved), multiplies, and
+    # downloads C back to interleaved host memory (mflab_d2h_interleaved);
+    # the upload of step i+1 and the download of step i-1 run on their own
+    # streams (each with its own handle, whose staging they use) while step
+    # i multiplies (two device buffer sets)
+    hA = torch.empty((n, n, N), dtype=torch.float64, pin_memory=True)
+    hB = torch.empty((n, n, N), dtype=torch.float64, pin_memory=True)
+    hC = torch.empty((n, n, N), dtype=torch.float64, pin_memory=True)
+    A.copy_to_interleaved_(hA)
+    B.copy_to_interleaved_(hB)
+    torch.cuda.synchronize()
+    bufs = [tuple(mf.MFMatrix.empty(N, n, n) for _ in range(3)) for _ in range(2)]
+    h_up, h_down = mf.create_handle(local), mf.create_handle(local)
 
     def e2e_run(steps):
         cs = torch.cuda.current_stream()
@@ -675,34 +792,35 @@ def main():
         for i in range(steps):
             b = i % 2
             dA, dB, dC = bufs[b]
-            with torch.cuda.stream(hs):
-                if i >= 2:
-                    hs.wait_event(done[b])  # step i-2 no longer reads this set
-                dA.copy_(hA, non_blocking=True)
-                dB.copy_(hB, non_blocking=True)
-                up[b].record(hs)
+            if i >= 2:
+                hs.wait_event(done[b])  # step i-2 no longer reads this set
+            dA.copy_from_interleaved_(hA, stream=hs, handle=h_up)
+            dB.copy_from_interleaved_(hB, stream=hs, handle=h_up)
+            up[b].record(hs)
             cs.wait_event(up[b])
             if i >= 2:
-                cs.wait_event(down[b])      # step i-2's result has left dC
-            mf.gemm_(mf.MFMatrix.from_tensor(dC), mf.MFMatrix.from_tensor(dA),
-                     mf.MFMatrix.from_tensor(dB), config=head_cfg)
+                cs.wait_event(down[b])  # step i-2's result has left dC
+            mf.gemm_(dC, dA, dB, config=head_cfg)
             done[b].record(cs)
-            with torch.cuda.stream(ds):
-                ds.wait_event(done[b])
-                hC.copy_(dC, non_blocking=True)
-                down[b].record(ds)
+            ds.wait_event(done[b])
+            dC.copy_to_interleaved_(hC, stream=ds, handle=h_down)
+            down[b].record(ds)
         cs.wait_stream(hs)
         cs.wait_stream(ds)
         e1.record(cs)
         R.barrier()
         return R.sharding.max_over_ranks(e0.elapsed_time(e1) / 1e3)
 
-    e2e_run(2)  # warm-up (scratch, host page mappings)
+    e2e_run(2)  # warm-up (scratch, staging, host page mappings)
     e2e_steps = max(2, args.steps)
     t_e2e = e2e_run(e2e_steps) / e2e_steps
-    dA = dB = dC = None
-    del bufs
-    del dA, dB, dC, hA, hB, hC
+    # the downloaded result equals the device-resident call on the same operands
+    mf.gemm_(Cm, A, B, config=head_cfg)
+    e2e_ok = bool(torch.equal(torch.from_numpy(Cm.to_interleaved()), hC))
+    torch.cuda.synchronize()
+    mf.destroy_handle(h_up)
+    mf.destroy_handle(h_down)
+    del bufs, hA, hB, hC
     instr = float(n) ** 3 * ops_per_term(N)
     plain_roof = {"bound": "fp64", "achieved": instr / t_plain / 1e12, "peak": peak_fp64 / 1e12,
                   "unit": "T FP64 instr/s", "frac": instr / t_plain / peak_fp64,
@@ -752,7 +870,11 @@ def main():
                        "roofline": plain_roof},
         "speedup_vs_plain": t_plain / t_head,
         "e2e": {"value": world * flops / t_e2e / 1e9, "unit": UNIT,
-                "h2d_bytes_per_step": 2 * N * n * n * 8, "d2h_bytes_per_step": N * n * n * 8},
+                "h2d_bytes_per_step": 2 * N * n * n * 8, "d2h_bytes_per_step": N * n * n * 8,
+                "host_layout": "interleaved (n, n, N) pinned host arrays, as a Julia "
+                               "Matrix{Float64xN}; converted to and from limb planes by "
+                               "mflab_h2d_interleaved / mflab_d2h_interleaved inside the step",
+                "result_equals_device_resident_call": e2e_ok},
         "roofline": roof,
         "clocks": clk,
         "gpu_launches": args.steps * launches,
@@ -786,7 +908,7 @@ def main():
                        "accuracy": a4}
         line["x4"] = x4
     if rank == 0 and world == 1 and not args.no_configs:
-        line["configs"] = run_configs(R, torch)
+        line["configs"] = run_configs(R, torch, peak_fp64, args.config_reps)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import mfref
         threads = mfref.threads()

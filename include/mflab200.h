@@ -17,8 +17,8 @@
  *   - `stream` is a cudaStream_t (NULL = the legacy default stream).  All
  *     work is stream-ordered; nothing synchronises unless stated.
  *   - Return value: MFLAB_OK (0) or a negative MFLAB_ERR_* code for bad
- *     arguments (the reference's DimensionMismatch / ArgumentError), CUDA
- *     failures or bounded-wait timeouts.  Numerical status of a
+ *     shapes (the reference's DimensionMismatch), bad option codes
+ *     (ArgumentError), CUDA failures or bounded-wait timeouts.  Numerical status of a
  *     factorization (0, -1 non-finite input, k > 0 failing pivot) is written
  *     to a DEVICE int, exactly the reference's `info` field.
  *   - Pivot vectors are 1-based int64 on the device, as in the reference.
@@ -35,12 +35,15 @@ extern "C" {
 #endif
 
 #define MFLAB_OK 0
-#define MFLAB_ERR_ARG (-1)         /* shape / argument error (DimensionMismatch, ArgumentError) */
+#define MFLAB_ERR_ARG (-1)         /* shape / size / pointer error (DimensionMismatch) */
 #define MFLAB_ERR_CUDA (-2)        /* a CUDA runtime call failed */
 #define MFLAB_ERR_UNSUPPORTED (-3) /* limb count or option not supported */
 #define MFLAB_ERR_TIMEOUT (-4)     /* a bounded device wait ran out */
 #define MFLAB_ERR_ALLOC (-5)       /* device memory could not be reserved */
 #define MFLAB_ERR_ALIAS (-6)       /* output aliases an input (types.jl:261-267) */
+#define MFLAB_ERR_FLAG (-7)        /* an option code (side, uplo, trans, diag, route, order,
+                                      region, engine) outside its range (ArgumentError,
+                                      as trsv.jl:32-34 raises for a bad uplo / trans) */
 
 /* GEMM routes (gemm.jl:44-136 gemm_plan strategies) */
 #define MFLAB_GEMM_AUTO 0   /* reference :auto: fused mulacc for x3, direct otherwise */
@@ -77,6 +80,29 @@ int mflab_destroy(mflab_handle *h);
    backward row wait for the previous one; MFLAB_ORDER_FAST applies every term
    as soon as its unknown is final.  No reference counterpart. */
 int mflab_set_solve_order(mflab_handle *h, int order);
+
+/* ------------------------------------------- interleaved <-> limb planes --- */
+/* A Julia Matrix{MultiFloat{Float64,N}} — the reference's operand type
+   (AbstractMatrix{MultiFloat{Float64,N}}, src/kernels/gemm.jl:747-755,
+   src/MultiFloatLinearAlgebra.jl:34-49) — stores the N limbs of each element
+   together: limb l of element (r, c) at X[(c*ldx + r)*limbs + l], ldx in
+   elements.  These four calls move such a matrix onto / off the limb planes
+   P[l*ls + c*ld + r] the other entry points take, bit for bit (a permutation
+   of doubles; limbs 1..4).  Stream-ordered.
+
+   Host forms: `host` is host memory (pinned for an asynchronous copy;
+   pageable memory is accepted, the copy then completes before the call
+   returns).  They stage chunks through a 64 MiB buffer the handle allocates
+   on first use, so two streams converting at once need two handles.
+   Device forms: X is device memory; no staging, no allocation. */
+int mflab_h2d_interleaved(mflab_handle *h, void *stream, int limbs, int64_t m, int64_t n,
+                          const double *host, int64_t ldh, double *P, int64_t ld, int64_t ls);
+int mflab_d2h_interleaved(mflab_handle *h, void *stream, int limbs, int64_t m, int64_t n,
+                          const double *P, int64_t ld, int64_t ls, double *host, int64_t ldh);
+int mflab_interleaved_to_planes(mflab_handle *h, void *stream, int limbs, int64_t m, int64_t n,
+                                const double *X, int64_t ldx, double *P, int64_t ld, int64_t ls);
+int mflab_planes_to_interleaved(mflab_handle *h, void *stream, int limbs, int64_t m, int64_t n,
+                                const double *P, int64_t ld, int64_t ls, double *X, int64_t ldx);
 
 /* ---------------------------------------------------------- BLAS-like --- */
 /* C = alpha*A*B + beta*C; A m x k, B k x n, C m x n.  With beta == 0 C is not

@@ -91,6 +91,8 @@ def _check(rc: int, what: str) -> None:
         msg += f" ({detail})"
     if rc == _native.MFLAB_ERR_ARG:
         raise DimensionMismatch(msg)
+    if rc == _native.MFLAB_ERR_FLAG:
+        raise ArgumentError(msg)
     if rc == _native.MFLAB_ERR_ALIAS:
         raise ArgumentError(f"{what} does not support output/input aliasing")
     if rc == _native.MFLAB_ERR_UNSUPPORTED:
@@ -114,6 +116,20 @@ def _handle(device: int):
             h = out
             _handles[key] = h
         return h
+
+
+def create_handle(device: Optional[int] = None) -> C.c_void_p:
+    """A new library handle (its own scratch and staging buffers) for work
+    issued on a stream of its own; the default per-thread handle serves
+    everything else.  Release it with destroy_handle."""
+    dev = torch.cuda.current_device() if device is None else device
+    out = C.c_void_p()
+    _check(_native.load().mflab_create(C.byref(out), dev), "mflab_create")
+    return out
+
+
+def destroy_handle(h: C.c_void_p) -> None:
+    _check(_native.load().mflab_destroy(h), "mflab_destroy")
 
 
 def _stream(device: int) -> int:
@@ -268,6 +284,74 @@ class MFMatrix:
     def from_tensor(cls, planes: torch.Tensor, is_vector: bool = False) -> "MFMatrix":
         """planes shaped (N, n, m): used as storage without a copy."""
         return cls(planes, 0, 0, planes.shape[2], planes.shape[1], is_vector)
+
+    # Interleaved storage is the memory order of a Julia
+    # Matrix{MultiFloat{Float64,N}} (the reference's operand type,
+    # gemm.jl:747-755): limb l of element (r, c) at X[(c*ld + r)*N + l],
+    # i.e. a C-contiguous host array of shape (n, ld, N).
+    @staticmethod
+    def _host_ptr(X) -> tuple:
+        """(address, shape, pinned) of a C-contiguous float64 host array"""
+        if isinstance(X, torch.Tensor):
+            if X.is_cuda or X.dtype != torch.float64 or not X.is_contiguous():
+                raise ArgumentError("interleaved host data must be a contiguous float64 CPU tensor")
+            return X.data_ptr(), tuple(X.shape), X.is_pinned()
+        if not isinstance(X, np.ndarray) or X.dtype != np.float64 or \
+                not X.flags["C_CONTIGUOUS"]:
+            raise ArgumentError("interleaved host data must be a C-contiguous float64 array")
+        return X.ctypes.data, X.shape, False
+
+    def copy_from_interleaved_(self, X, stream=None, handle=None) -> "MFMatrix":
+        """Upload interleaved host data of shape (n, ld, N) (ld >= m) into
+        this matrix (mflab_h2d_interleaved).  Stream-ordered and not
+        synchronised: a pinned X must stay alive until `stream` (default:
+        the current stream) has passed this point.  `handle` (a raw
+        mflab_handle) lets concurrent streams use their own staging."""
+        ptr, shape, _ = self._host_ptr(X)
+        if len(shape) != 3 or shape[0] != self.n or shape[1] < self.m or shape[2] != self.N:
+            raise DimensionMismatch(f"interleaved data of shape {shape} does not hold a "
+                                    f"{self.m}x{self.n} {limb_type_name(self.N)} matrix")
+        lib = _native.load()
+        h = handle or _handle(self.device)
+        s = _stream(self.device) if stream is None else stream.cuda_stream
+        _check(lib.mflab_h2d_interleaved(h, s, self.N, self.m, self.n, ptr, shape[1], self.ptr(),
+                                         self.ld, self.ls), "h2d_interleaved")
+        return self
+
+    def copy_to_interleaved_(self, X, stream=None, handle=None):
+        """Download this matrix into interleaved host data of shape (n, ld, N)
+        (mflab_d2h_interleaved); not synchronised."""
+        ptr, shape, _ = self._host_ptr(X)
+        if len(shape) != 3 or shape[0] != self.n or shape[1] < self.m or shape[2] != self.N:
+            raise DimensionMismatch(f"interleaved data of shape {shape} cannot take a "
+                                    f"{self.m}x{self.n} {limb_type_name(self.N)} matrix")
+        lib = _native.load()
+        h = handle or _handle(self.device)
+        s = _stream(self.device) if stream is None else stream.cuda_stream
+        _check(lib.mflab_d2h_interleaved(h, s, self.N, self.m, self.n, self.ptr(), self.ld,
+                                         self.ls, ptr, shape[1]), "d2h_interleaved")
+        return X
+
+    @classmethod
+    def from_interleaved(cls, X, m: Optional[int] = None, device=None) -> "MFMatrix":
+        """A new device matrix from interleaved host data (n, ld, N): the
+        first m (default ld) rows of each column.  Returns after the copy."""
+        _, shape, _ = cls._host_ptr(X)
+        if len(shape) != 3 or not 1 <= shape[2] <= 4:
+            raise ArgumentError("interleaved data must have shape (n, ld, N), N in 1..4")
+        n, ld, N = shape
+        M = cls.empty(N, ld if m is None else m, n, device)
+        M.copy_from_interleaved_(X)
+        torch.cuda.current_stream(M.device).synchronize()
+        return M
+
+    def to_interleaved(self) -> np.ndarray:
+        """This matrix as an interleaved host array of shape (n, m, N)."""
+        out = np.empty((self.n, self.m, self.N), dtype=np.float64)
+        if out.size:
+            self.copy_to_interleaved_(out)
+            torch.cuda.current_stream(self.device).synchronize()
+        return out
 
     def planes(self) -> torch.Tensor:
         """(N, n, m) torch view of this matrix's elements."""
@@ -1478,7 +1562,8 @@ _LU64_PANEL = 12
 
 
 def solve_mixed_lu(A: MFMatrix, B: MFMatrix, tol: float = 0.0, maxiter: int = 40,
-                   config: KernelConfig = _DEFAULT, residual: str = "int8") -> tuple:
+                   config: KernelConfig = _DEFAULT, residual: str = "int8",
+                   timing: bool = False) -> tuple:
     """Solve A X = B for a Float64xN matrix A with a binary64 partial-pivoting
     LU of round(A) and iterative refinement with Float64xN residuals.
 
@@ -1488,7 +1573,9 @@ def solve_mixed_lu(A: MFMatrix, B: MFMatrix, tol: float = 0.0, maxiter: int = 40
     INT8 modular GEMM (residual="int8", error at the Float64xN level of the
     plain kernel) or residual! in the reference order (residual="matched").
     Stops when all backward errors are <= tol (default 2^(-53N)) or after
-    maxiter iterations.  Returns (X, report).  The reference provides the
+    maxiter iterations.  Returns (X, report); with timing=True the report
+    also holds the device times of the binary64 factor and of the
+    refinement loop (CUDA events on the current stream).  The reference provides the
     pieces (lu!, residual!, refinement_correction!) but leaves the refinement
     loop to the caller.
     """
@@ -1503,11 +1590,16 @@ def solve_mixed_lu(A: MFMatrix, B: MFMatrix, tol: float = 0.0, maxiter: int = 40
     tol = tol or 2.0 ** (-53 * N)
     dev = A.storage.device
     lib, h, s = _lib_h(A)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)] if timing else None
+    if timing:
+        ev[0].record()
     LU = _leading_limb(A)
     ipiv = torch.arange(1, n + 1, dtype=torch.int64, device=dev)
     info = torch.zeros(1, dtype=torch.int32, device=dev)
     _check(lib.mflab_getrf(h, s, 1, n, n, LU.ptr(), LU.ld, LU.ls, ipiv.data_ptr() if n else None,
                            _LU64_PANEL, info.data_ptr()), "lu! (binary64)")
+    if timing:
+        ev[1].record()
     st = _read_info(info)
     if st == -1:
         raise DomainError("lu!: input matrix contains non-finite entries")
@@ -1536,11 +1628,17 @@ def solve_mixed_lu(A: MFMatrix, B: MFMatrix, tol: float = 0.0, maxiter: int = 40
         history.append(worst)
         if worst <= tol:
             break
+    if timing:
+        ev[2].record()
+        ev[2].synchronize()
     report = {"iterations": it, "backward_error": history[-1] if history else None,
               "history": history, "converged": bool(history) and history[-1] <= tol,
               "factor": "binary64 partial-pivoting LU",
               "residual": limb_type_name(N) + (" (INT8 modular GEMM)" if residual == "int8"
                                                else " (reference order)")}
+    if timing:
+        report["factor_ms"] = ev[0].elapsed_time(ev[1])
+        report["refine_ms"] = ev[1].elapsed_time(ev[2])
     return X, report
 
 

@@ -29,21 +29,53 @@ MFLAB_ERR_UNSUPPORTED = -3
 MFLAB_ERR_TIMEOUT = -4
 MFLAB_ERR_ALLOC = -5
 MFLAB_ERR_ALIAS = -6
+MFLAB_ERR_FLAG = -7
+
+
+OBJ_DIR = os.path.join(PKG_DIR, "_build")
 
 
 def sources() -> list[str]:
     return sorted(glob.glob(os.path.join(CSRC, "*.cu")))
 
 
-def build(verbose: bool = False) -> str:
-    """Compile every CUDA source into libmflab200.so (sm_100a) in the package."""
-    nvcc = os.environ.get("NVCC", "nvcc")
-    cmd = [nvcc, *NVCC_FLAGS, "-I", INCLUDE, "-o", LIB_PATH, *sources(), "-lcublasLt"]
+def _headers() -> list[str]:
+    return (glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h"))
+            + glob.glob(os.path.join(INCLUDE, "*.h")))
+
+
+def _run(cmd: list[str]) -> str:
     out = subprocess.run(cmd, capture_output=True, text=True)
     if out.returncode != 0:
         raise RuntimeError("nvcc failed:\n" + " ".join(cmd) + "\n" + out.stdout + out.stderr)
+    return out.stdout + out.stderr
+
+
+def build(verbose: bool = False, jobs: int | None = None) -> str:
+    """Compile every CUDA source (sm_100a) into libmflab200.so in the package:
+    one nvcc per translation unit in parallel (objects under _build/, rebuilt
+    when the source or any header is newer), then one link."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    nvcc = os.environ.get("NVCC", "nvcc")
+    os.makedirs(OBJ_DIR, exist_ok=True)
+    newest_header = max((os.path.getmtime(h) for h in _headers()), default=0.0)
+    compile_flags = [f for f in NVCC_FLAGS if f != "-shared"]
+    objs, todo = [], []
+    for src in sources():
+        obj = os.path.join(OBJ_DIR, os.path.basename(src)[:-3] + ".o")
+        objs.append(obj)
+        if not os.path.exists(obj) or os.path.getmtime(obj) < max(os.path.getmtime(src),
+                                                                    newest_header):
+            todo.append([nvcc, *compile_flags, "-I", INCLUDE, "-c", "-o", obj, src])
+    logs = []
+    if todo:
+        with ThreadPoolExecutor(max_workers=jobs or min(len(todo), os.cpu_count() or 4)) as ex:
+            logs = list(ex.map(_run, todo))
+    if todo or not os.path.exists(LIB_PATH):
+        logs.append(_run([nvcc, *NVCC_FLAGS, "-o", LIB_PATH, *objs, "-lcublasLt"]))
     if verbose:
-        print(out.stdout + out.stderr)
+        print("".join(logs))
     return LIB_PATH
 
 
@@ -136,6 +168,10 @@ SIGNATURES = {
     "mflab_gemm_ozaki_phases": [_vp, _vp, _int, _int, _i64, _i64, _i64, _vp, _i64, _i64, _vp, _i64,
                                 _i64, _vp, _i64, _i64, _d, _d, C.POINTER(C.c_float), _d],
     "mflab_probe_int8_gemm": [_vp, _vp, _i64, _i64, _i64, _int, C.POINTER(C.c_float)],
+    "mflab_h2d_interleaved": [_vp, _vp, _int, _i64, _i64, _vp, _i64, _vp, _i64, _i64],
+    "mflab_d2h_interleaved": [_vp, _vp, _int, _i64, _i64, _vp, _i64, _i64, _vp, _i64],
+    "mflab_interleaved_to_planes": [_vp, _vp, _int, _i64, _i64, _vp, _i64, _vp, _i64, _i64],
+    "mflab_planes_to_interleaved": [_vp, _vp, _int, _i64, _i64, _vp, _i64, _i64, _vp, _i64],
 }
 _RESTYPE = {"mflab_status_string": C.c_char_p, "mflab_last_error": C.c_char_p}
 

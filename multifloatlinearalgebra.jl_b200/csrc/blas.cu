@@ -316,7 +316,7 @@ extern "C" int mflab_gemm(mflab_handle *h, void *stream, int limbs, int route, i
     if (route == MFLAB_GEMM_OZAKI)
         return mflab_gemm_ozaki_route(h, stream, limbs, m, n, k, A, lda, lsa, B, ldb, lsb, C, ldc,
                                       lsc, alpha, beta);
-    if (route != MFLAB_GEMM_AUTO && route != MFLAB_GEMM_DIRECT) return MFLAB_ERR_ARG;
+    if (route != MFLAB_GEMM_AUTO && route != MFLAB_GEMM_DIRECT) return MFLAB_ERR_FLAG;
     bool fused = (limbs == 3 && route == MFLAB_GEMM_AUTO);
     return mfl::launch_mm(limbs, false, false, 0, fused, m, n, k, Mat{(double *)A, lda, lsa},
                           Mat{(double *)B, ldb, lsb}, Mat{C, ldc, lsc}, alpha, beta, s);
@@ -331,7 +331,8 @@ extern "C" int mflab_gemv(mflab_handle *h, void *stream, int limbs, int trans, i
                           int64_t lsx, double *y, int64_t lsy, const double *alpha,
                           const double *beta) {
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
-    if (m < 0 || n < 0 || !alpha || !beta || (trans != 0 && trans != 1)) return MFLAB_ERR_ARG;
+    if (trans != 0 && trans != 1) return MFLAB_ERR_FLAG;
+    if (m < 0 || n < 0 || !alpha || !beta) return MFLAB_ERR_ARG;
     if (m > 0 && lda < m) return MFLAB_ERR_ARG;
     const int64_t rows = trans ? n : m, len = trans ? m : n;
     if (rows == 0) return MFLAB_OK;
@@ -350,7 +351,8 @@ extern "C" int mflab_symv(mflab_handle *h, void *stream, int limbs, int uplo, in
                           const double *A, int64_t lda, int64_t lsa, const double *x, int64_t lsx,
                           double *y, int64_t lsy, const double *alpha, const double *beta) {
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
-    if (n < 0 || !alpha || !beta || (uplo != 0 && uplo != 1)) return MFLAB_ERR_ARG;
+    if (uplo != 0 && uplo != 1) return MFLAB_ERR_FLAG;
+    if (n < 0 || !alpha || !beta) return MFLAB_ERR_ARG;
     if (n == 0) return MFLAB_OK;
     if (lda < n) return MFLAB_ERR_ARG;
     if (mfl::views_overlap(y, n, lsy, n, 1, limbs, A, lda, lsa, n, n) ||
@@ -422,7 +424,8 @@ extern "C" int mflab_trmm(mflab_handle *h, void *stream, int limbs, int side, in
                           int diag, int64_t m, int64_t n, const double *A, int64_t lda,
                           int64_t lsa, double *B, int64_t ldb, int64_t lsb, const double *alpha) {
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
-    if (m < 0 || n < 0 || !alpha || (side | uplo | trans | diag) & ~1) return MFLAB_ERR_ARG;
+    if ((side | uplo | trans | diag) & ~1) return MFLAB_ERR_FLAG;
+    if (m < 0 || n < 0 || !alpha) return MFLAB_ERR_ARG;
     const int64_t na = side ? n : m;
     if (m == 0 || n == 0) return MFLAB_OK;
     if (lda < na || ldb < m) return MFLAB_ERR_ARG;

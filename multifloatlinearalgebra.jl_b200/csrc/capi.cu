@@ -22,12 +22,13 @@ extern "C" int mflab_version(void) { return 10000 * 0 + 100 * 1 + 0; }
 extern "C" const char *mflab_status_string(int code) {
     switch (code) {
     case MFLAB_OK: return "ok";
-    case MFLAB_ERR_ARG: return "invalid argument or dimension mismatch";
+    case MFLAB_ERR_ARG: return "dimension mismatch or invalid size";
     case MFLAB_ERR_CUDA: return "CUDA runtime error";
     case MFLAB_ERR_UNSUPPORTED: return "unsupported limb count or option";
     case MFLAB_ERR_TIMEOUT: return "bounded device wait timed out";
     case MFLAB_ERR_ALLOC: return "device memory reservation failed";
     case MFLAB_ERR_ALIAS: return "output aliases an input";
+    case MFLAB_ERR_FLAG: return "invalid option code";
     default: return "unknown status";
     }
 }
@@ -54,6 +55,7 @@ extern "C" int mflab_create(mflab_handle **out, int device) {
     h->last_moduli = 0;
     h->solve_order = MFLAB_ORDER_MATCHED;
     h->int8_engine = MFLAB_INT8_TCGEN05;
+    h->stage = nullptr;
     e = cudaMalloc((void **)&h->dev_flags, 64 * sizeof(int));
     if (e != cudaSuccess) {
         delete h;
@@ -71,6 +73,7 @@ extern "C" int mflab_destroy(mflab_handle *h) {
     cudaDeviceSynchronize();
     if (h->scratch) cudaFree(h->scratch);
     if (h->aux) cudaFree(h->aux);
+    if (h->stage) cudaFree(h->stage);
     if (h->dev_flags) cudaFree(h->dev_flags);
     delete h;
     return MFLAB_OK;
@@ -118,7 +121,7 @@ int mflab_reserve_aux(mflab_handle *h, size_t bytes) {
 
 extern "C" int mflab_set_solve_order(mflab_handle *h, int order) {
     if (!h) return MFLAB_ERR_ARG;
-    if (order != MFLAB_ORDER_MATCHED && order != MFLAB_ORDER_FAST) return MFLAB_ERR_ARG;
+    if (order != MFLAB_ORDER_MATCHED && order != MFLAB_ORDER_FAST) return MFLAB_ERR_FLAG;
     h->solve_order = order;
     return MFLAB_OK;
 }

@@ -858,7 +858,8 @@ extern "C" int mflab_getrs(mflab_handle *h, void *stream, int limbs, int64_t n, 
 extern "C" int mflab_max_abs(mflab_handle *h, void *stream, int limbs, int64_t m, int64_t n,
                              const double *A, int64_t lda, int64_t lsa, int region, double *out) {
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
-    if (m < 0 || n < 0 || region < 0 || region > 2 || !out) return MFLAB_ERR_ARG;
+    if (region < 0 || region > 2) return MFLAB_ERR_FLAG;
+    if (m < 0 || n < 0 || !out) return MFLAB_ERR_ARG;
     const int nparts = 296;
     int rc = mflab_reserve_scratch(h, sizeof(double) * nparts * (limbs + 1));
     if (rc) return rc;

@@ -1,0 +1,212 @@
+// Interleaved Float64xN storage <-> limb planes.
+//
+// A Julia Matrix{MultiFloat{Float64,N}} (the reference's operand type,
+// src/kernels/gemm.jl:747-755) stores the N limbs of each element next to
+// each other: limb l of element (r, c) at X[(c*ldx + r)*N + l].  The device
+// kernels of this library read N separate column-major planes instead.  The
+// conversion is a pure permutation of doubles (no arithmetic), so it is
+// bit-exact and HBM-bound: one read and one write of 8 N bytes per element.
+//
+// Host <-> device forms stage the host block through two 32 MiB halves of a
+// handle-owned buffer (chunks of whole columns, or of rows of one column
+// when a column is larger): the copy engine moves chunk j
+// (cudaMemcpy2DAsync, which also takes the host leading dimension) into
+// half j mod 2 and a permutation kernel turns it into planes (or planes into
+// the chunk before it leaves).  Everything is ordered on the caller's
+// stream; the staging is why concurrent callers need their own handles.
+#include <algorithm>
+#include <cstdint>
+
+#include "mflab_internal.h"
+
+namespace mfl {
+
+namespace {
+
+constexpr int IL_THREADS = 256;
+constexpr size_t IL_STAGE_HALF = size_t(32) << 20;  // bytes per staging half
+
+// dst planes <- src interleaved (to_planes = true), or the reverse.  One
+// thread per element: the N limbs of an element are contiguous in the
+// interleaved form (a 16-byte load / store for N = 2 and two for N = 4 when
+// aligned), and consecutive threads touch consecutive rows of each plane,
+// so both sides are coalesced.
+template <int N, bool TO_PLANES, bool VEC>
+__global__ void __launch_bounds__(IL_THREADS)
+    interleave_kernel(int64_t m, int64_t n, double *__restrict__ X, int64_t ldx,
+                      double *__restrict__ P, int64_t ld, int64_t ls) {
+    const int64_t r = (int64_t)blockIdx.x * IL_THREADS + threadIdx.x;
+    if (r >= m) return;
+    for (int64_t c = blockIdx.y; c < n; c += gridDim.y) {
+        double *x = X + (c * ldx + r) * N;
+        double *p = P + c * ld + r;
+        if constexpr (TO_PLANES) {
+            double v[N];
+            if constexpr (VEC) {
+#pragma unroll
+                for (int l = 0; l < N; l += 2) {
+                    const double2 t = *reinterpret_cast<const double2 *>(x + l);
+                    v[l] = t.x;
+                    v[l + 1] = t.y;
+                }
+            } else {
+#pragma unroll
+                for (int l = 0; l < N; ++l) v[l] = x[l];
+            }
+#pragma unroll
+            for (int l = 0; l < N; ++l) p[l * ls] = v[l];
+        } else {
+            double v[N];
+#pragma unroll
+            for (int l = 0; l < N; ++l) v[l] = p[l * ls];
+            if constexpr (VEC) {
+#pragma unroll
+                for (int l = 0; l < N; l += 2)
+                    *reinterpret_cast<double2 *>(x + l) = make_double2(v[l], v[l + 1]);
+            } else {
+#pragma unroll
+                for (int l = 0; l < N; ++l) x[l] = v[l];
+            }
+        }
+    }
+}
+
+template <int N, bool TO_PLANES>
+int launch_n(int64_t m, int64_t n, double *X, int64_t ldx, double *P, int64_t ld, int64_t ls,
+             cudaStream_t s) {
+    const dim3 grid((unsigned)((m + IL_THREADS - 1) / IL_THREADS),
+                    (unsigned)std::min<int64_t>(n, 32768));
+    // 16-byte vector access needs an even limb count and a 16-byte aligned base
+    const bool vec = (N % 2 == 0) && ((reinterpret_cast<uintptr_t>(X) & 15) == 0);
+    if (vec)
+        interleave_kernel<N, TO_PLANES, (N % 2 == 0)><<<grid, IL_THREADS, 0, s>>>(m, n, X, ldx, P,
+                                                                                ld, ls);
+    else
+        interleave_kernel<N, TO_PLANES, false><<<grid, IL_THREADS, 0, s>>>(m, n, X, ldx, P, ld, ls);
+    return record_cuda_error(cudaGetLastError(), "interleave kernel");
+}
+
+template <bool TO_PLANES>
+int launch(int N, int64_t m, int64_t n, double *X, int64_t ldx, double *P, int64_t ld, int64_t ls,
+           cudaStream_t s) {
+    switch (N) {
+    case 1: return launch_n<1, TO_PLANES>(m, n, X, ldx, P, ld, ls, s);
+    case 2: return launch_n<2, TO_PLANES>(m, n, X, ldx, P, ld, ls, s);
+    case 3: return launch_n<3, TO_PLANES>(m, n, X, ldx, P, ld, ls, s);
+    case 4: return launch_n<4, TO_PLANES>(m, n, X, ldx, P, ld, ls, s);
+    }
+    return MFLAB_ERR_UNSUPPORTED;
+}
+
+// common argument checks; returns MFLAB_OK when there is work to do, or a
+// code (MFLAB_OK with *empty = true for an empty matrix)
+int check_args(mflab_handle *h, int limbs, int64_t m, int64_t n, const void *X, int64_t ldx,
+               const void *P, int64_t ld, int64_t ls, bool *empty) {
+    *empty = false;
+    if (!h || limbs < 1 || limbs > 4) return MFLAB_ERR_UNSUPPORTED;
+    if (m < 0 || n < 0) return MFLAB_ERR_ARG;
+    if (m == 0 || n == 0) {
+        *empty = true;
+        return MFLAB_OK;
+    }
+    // planes must not overlap one another
+    if (!X || !P || ldx < m || ld < m || (limbs > 1 && ls < ld * (n - 1) + m))
+        return MFLAB_ERR_ARG;
+    return MFLAB_OK;
+}
+
+int reserve_stage(mflab_handle *h) {
+    if (h->stage) return MFLAB_OK;
+    cudaError_t e = cudaMalloc(&h->stage, 2 * IL_STAGE_HALF);
+    if (e != cudaSuccess) {
+        record_cuda_error(e, "staging cudaMalloc");
+        h->stage = nullptr;
+        return MFLAB_ERR_ALLOC;
+    }
+    return MFLAB_OK;
+}
+
+// Staged chunks: rb rows x cb columns fill at most one staging half (whole
+// columns when a column fits, otherwise row blocks of single columns).
+struct Chunks {
+    int64_t rb, cb;
+};
+Chunks chunking(int N, int64_t m) {
+    const int64_t elem = N * (int64_t)sizeof(double);
+    const int64_t rows_per_half = (int64_t)IL_STAGE_HALF / elem;
+    if (m <= rows_per_half) return {m, std::max<int64_t>(1, rows_per_half / m)};
+    return {rows_per_half, 1};
+}
+
+// host <-> device through the staging halves, chunk by chunk on one stream
+template <bool H2D>
+int staged(mflab_handle *h, int N, int64_t m, int64_t n, double *host, int64_t ldh, double *P,
+           int64_t ld, int64_t ls, cudaStream_t s) {
+    int rc = reserve_stage(h);
+    if (rc) return rc;
+    const Chunks ch = chunking(N, m);
+    const size_t hpitch = (size_t)ldh * N * sizeof(double);
+    int64_t j = 0;
+    for (int64_t c0 = 0; c0 < n; c0 += ch.cb) {
+        const int64_t w = std::min(ch.cb, n - c0);
+        for (int64_t r0 = 0; r0 < m; r0 += ch.rb, ++j) {
+            const int64_t hgt = std::min(ch.rb, m - r0);
+            const size_t row_bytes = (size_t)hgt * N * sizeof(double);
+            double *st = (double *)((char *)h->stage + (j & 1) * IL_STAGE_HALF);
+            double *hp = host + (c0 * ldh + r0) * N;
+            double *pp = P + c0 * ld + r0;
+            if (H2D) {
+                cudaError_t e = cudaMemcpy2DAsync(st, row_bytes, hp, hpitch, row_bytes, (size_t)w,
+                                                  cudaMemcpyHostToDevice, s);
+                if (e != cudaSuccess) return record_cuda_error(e, "mflab_h2d_interleaved copy");
+                if ((rc = launch<true>(N, hgt, w, st, hgt, pp, ld, ls, s))) return rc;
+            } else {
+                if ((rc = launch<false>(N, hgt, w, st, hgt, pp, ld, ls, s))) return rc;
+                cudaError_t e = cudaMemcpy2DAsync(hp, hpitch, st, row_bytes, row_bytes, (size_t)w,
+                                                  cudaMemcpyDeviceToHost, s);
+                if (e != cudaSuccess) return record_cuda_error(e, "mflab_d2h_interleaved copy");
+            }
+        }
+    }
+    return MFLAB_OK;
+}
+
+}  // namespace
+}  // namespace mfl
+
+extern "C" int mflab_interleaved_to_planes(mflab_handle *h, void *stream, int limbs, int64_t m,
+                                           int64_t n, const double *X, int64_t ldx, double *P,
+                                           int64_t ld, int64_t ls) {
+    bool empty;
+    int rc = mfl::check_args(h, limbs, m, n, X, ldx, P, ld, ls, &empty);
+    if (rc || empty) return rc;
+    return mfl::launch<true>(limbs, m, n, (double *)X, ldx, P, ld, ls, (cudaStream_t)stream);
+}
+
+extern "C" int mflab_planes_to_interleaved(mflab_handle *h, void *stream, int limbs, int64_t m,
+                                           int64_t n, const double *P, int64_t ld, int64_t ls,
+                                           double *X, int64_t ldx) {
+    bool empty;
+    int rc = mfl::check_args(h, limbs, m, n, X, ldx, P, ld, ls, &empty);
+    if (rc || empty) return rc;
+    return mfl::launch<false>(limbs, m, n, X, ldx, (double *)P, ld, ls, (cudaStream_t)stream);
+}
+
+extern "C" int mflab_h2d_interleaved(mflab_handle *h, void *stream, int limbs, int64_t m, int64_t n,
+                                     const double *host, int64_t ldh, double *P, int64_t ld,
+                                     int64_t ls) {
+    bool empty;
+    int rc = mfl::check_args(h, limbs, m, n, host, ldh, P, ld, ls, &empty);
+    if (rc || empty) return rc;
+    return mfl::staged<true>(h, limbs, m, n, (double *)host, ldh, P, ld, ls, (cudaStream_t)stream);
+}
+
+extern "C" int mflab_d2h_interleaved(mflab_handle *h, void *stream, int limbs, int64_t m, int64_t n,
+                                     const double *P, int64_t ld, int64_t ls, double *host,
+                                     int64_t ldh) {
+    bool empty;
+    int rc = mfl::check_args(h, limbs, m, n, host, ldh, P, ld, ls, &empty);
+    if (rc || empty) return rc;
+    return mfl::staged<false>(h, limbs, m, n, host, ldh, (double *)P, ld, ls,
+                              (cudaStream_t)stream);
+}

@@ -130,6 +130,8 @@ struct mflab_handle {
     int last_moduli;  // modulus count the last modular (CRT) INT8 call used
     int solve_order;  // MFLAB_ORDER_MATCHED or MFLAB_ORDER_FAST for triangular solves
     int int8_engine;  // MFLAB_INT8_TCGEN05 or MFLAB_INT8_LIBRARY for the level products
+    // staging of the interleaved host <-> limb-plane copies (64 MiB, on first use)
+    void *stage;
 };
 
 int mflab_reserve_aux(mflab_handle *h, size_t bytes);

@@ -125,8 +125,8 @@ extern "C" int mflab_max_abs_noalloc(void *stream, int limbs, int64_t m, int64_t
                                      const double *A, int64_t lda, int64_t lsa, int region,
                                      double *out) {
     if (!mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
-    if (m < 0 || n < 0 || region < 0 || region > 2 || !out || (m > 0 && n > 0 && lda < m))
-        return MFLAB_ERR_ARG;
+    if (region < 0 || region > 2) return MFLAB_ERR_FLAG;
+    if (m < 0 || n < 0 || !out || (m > 0 && n > 0 && lda < m)) return MFLAB_ERR_ARG;
     if (n > mfl::NOALLOC_MAX_COLUMNS) {
         mfl::record_error_message(("mflab_max_abs_noalloc: " + std::to_string(n) +
                                    " columns exceed the fixed scratch of " +

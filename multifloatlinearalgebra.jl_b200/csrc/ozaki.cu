@@ -599,7 +599,7 @@ extern "C" int mflab_probe_int8_gemm(mflab_handle *h, void *stream, int64_t m, i
 
 extern "C" int mflab_set_int8_engine(mflab_handle *h, int engine) {
     if (!h) return MFLAB_ERR_ARG;
-    if (engine != MFLAB_INT8_TCGEN05 && engine != MFLAB_INT8_LIBRARY) return MFLAB_ERR_ARG;
+    if (engine != MFLAB_INT8_TCGEN05 && engine != MFLAB_INT8_LIBRARY) return MFLAB_ERR_FLAG;
     h->int8_engine = engine;
     return MFLAB_OK;
 }

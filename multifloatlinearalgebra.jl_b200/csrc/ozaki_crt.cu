@@ -959,8 +959,8 @@ extern "C" int mflab_syrk_lower_ozaki(mflab_handle *h, void *stream, int limbs, 
                                       int64_t lda, int64_t lsa, double *C, int64_t ldc,
                                       int64_t lsc, const double *alpha, const double *beta) {
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
-    if (n < 0 || k < 0 || !alpha || !beta || moduli < 0 || (trans != 0 && trans != 1))
-        return MFLAB_ERR_ARG;
+    if (trans != 0 && trans != 1) return MFLAB_ERR_FLAG;
+    if (n < 0 || k < 0 || !alpha || !beta || moduli < 0) return MFLAB_ERR_ARG;
     if (n == 0) return MFLAB_OK;
     const int64_t ar = trans ? k : n, ac = trans ? n : k;
     if (lda < (ar > 0 ? ar : 1) || ldc < n) return MFLAB_ERR_ARG;

@@ -772,7 +772,8 @@ extern "C" int mflab_qr(mflab_handle *h, void *stream, int limbs, int pivoted, i
                         int64_t n, double *A, int64_t lda, int64_t lsa, double *tau, int64_t lst,
                         int64_t *perm, int *info) {
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
-    if (m < 0 || n < 0 || !tau || !perm || !info || (pivoted & ~1)) return MFLAB_ERR_ARG;
+    if (pivoted & ~1) return MFLAB_ERR_FLAG;
+    if (m < 0 || n < 0 || !tau || !perm || !info) return MFLAB_ERR_ARG;
     const int64_t r = m < n ? m : n;
     if ((m > 0 && lda < m) || lst < r) return MFLAB_ERR_ARG;
     const Mat Am{A, lda, lsa};
@@ -789,7 +790,8 @@ extern "C" int mflab_apply_q(mflab_handle *h, void *stream, int limbs, int trans
                              const double *tau, int64_t lst, double *D, int64_t ldd, int64_t lsd,
                              int64_t nd) {
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
-    if (m < 0 || r < 0 || nd < 0 || (trans & ~1) || r > m) return MFLAB_ERR_ARG;
+    if (trans & ~1) return MFLAB_ERR_FLAG;
+    if (m < 0 || r < 0 || nd < 0 || r > m) return MFLAB_ERR_ARG;
     if (m == 0 || nd == 0 || r == 0) return MFLAB_OK;
     if (ldf < m || ldd < m || lst < r) return MFLAB_ERR_ARG;
     if (mfl::views_overlap(D, ldd, lsd, m, nd, limbs, F, ldf, lsf, m, r)) return MFLAB_ERR_ALIAS;

@@ -219,7 +219,8 @@ extern "C" int mflab_residual(mflab_handle *h, void *stream, int limbs, int uplo
                               const double *B, int64_t ldb, int64_t lsb, double *R, int64_t ldr,
                               int64_t lsr) {
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
-    if (uplo < 0 || uplo > 2 || m < 0 || k < 0 || nrhs < 0) return MFLAB_ERR_ARG;
+    if (uplo < 0 || uplo > 2) return MFLAB_ERR_FLAG;
+    if (m < 0 || k < 0 || nrhs < 0) return MFLAB_ERR_ARG;
     if (uplo != 0 && m != k) return MFLAB_ERR_ARG;
     if (m == 0 || nrhs == 0) return MFLAB_OK;
     if (lda < m || ldx < (k > 0 ? k : 1) || ldb < m || ldr < m) return MFLAB_ERR_ARG;
@@ -245,7 +246,8 @@ extern "C" int mflab_residual_mixed(mflab_handle *h, void *stream, int src_limbs
     if (!h) return MFLAB_ERR_UNSUPPORTED;
     if (!(src_limbs >= 1 && src_limbs < res_limbs && res_limbs <= 4 && res_limbs >= 2))
         return MFLAB_ERR_UNSUPPORTED;
-    if (uplo < 0 || uplo > 2 || m < 0 || k < 0 || nrhs < 0) return MFLAB_ERR_ARG;
+    if (uplo < 0 || uplo > 2) return MFLAB_ERR_FLAG;
+    if (m < 0 || k < 0 || nrhs < 0) return MFLAB_ERR_ARG;
     if (uplo != 0 && m != k) return MFLAB_ERR_ARG;
     if (m == 0 || nrhs == 0) return MFLAB_OK;
     if (nrhs > 65535) return MFLAB_ERR_UNSUPPORTED;
@@ -272,7 +274,8 @@ extern "C" int mflab_backward_error(mflab_handle *h, void *stream, int limbs, in
                                     const double *B, int64_t ldb, int64_t lsb, const double *R,
                                     int64_t ldr, int64_t lsr, double *out) {
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
-    if (uplo < 0 || uplo > 2 || m < 0 || k < 0 || nrhs < 0 || !out) return MFLAB_ERR_ARG;
+    if (uplo < 0 || uplo > 2) return MFLAB_ERR_FLAG;
+    if (m < 0 || k < 0 || nrhs < 0 || !out) return MFLAB_ERR_ARG;
     if (uplo != 0 && m != k) return MFLAB_ERR_ARG;
     if (nrhs == 0) return MFLAB_OK;
     const size_t need = sizeof(double) * (size_t)limbs * (size_t)(m + 8) + 64;
@@ -321,7 +324,8 @@ extern "C" int mflab_opnorm_inf(mflab_handle *h, void *stream, int limbs, int up
                                 int64_t k, const double *A, int64_t lda, int64_t lsa,
                                 double *anorm, int *nonfinite) {
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
-    if (uplo < 0 || uplo > 2 || m < 0 || k < 0 || !anorm || !nonfinite) return MFLAB_ERR_ARG;
+    if (uplo < 0 || uplo > 2) return MFLAB_ERR_FLAG;
+    if (m < 0 || k < 0 || !anorm || !nonfinite) return MFLAB_ERR_ARG;
     if (uplo != 0 && m != k) return MFLAB_ERR_ARG;
     const size_t need = sizeof(double) * (size_t)limbs * (size_t)(m + 8) + 64;
     int rc = mflab_reserve_scratch(h, need);

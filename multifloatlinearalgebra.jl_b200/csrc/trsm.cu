@@ -308,8 +308,9 @@ extern "C" int mflab_trsm(mflab_handle *h, void *stream, int limbs, int side, in
                           int64_t lsa, double *B, int64_t ldb, int64_t lsb, const double *alpha) {
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
     if (side < 0 || side > 1 || uplo < 0 || uplo > 1 || trans < 0 || trans > 1 || diag < 0 ||
-        diag > 1 || m < 0 || n < 0 || !alpha)
-        return MFLAB_ERR_ARG;
+        diag > 1)
+        return MFLAB_ERR_FLAG;
+    if (m < 0 || n < 0 || !alpha) return MFLAB_ERR_ARG;
     const int64_t na = side == 0 ? m : n;
     if ((na > 0 && lda < na) || (m > 0 && ldb < m)) return MFLAB_ERR_ARG;
     return mfl::launch_trsm_info(limbs, side, uplo, trans, diag, m, n,

@@ -125,3 +125,73 @@ def mixed_lu_problem(mf, n: int, nrhs: int, seed: int = 4, N: int = 4, device: i
     Bp = torch.zeros((N, nrhs, n), dtype=torch.float64, device=dev)
     Bp[0].normal_(generator=g)
     return A, mf.MFMatrix.from_tensor(Bp)
+
+
+def _symmetric_from_lower_(P: torch.Tensor) -> torch.Tensor:
+    """(N, n, n) column-major planes made symmetric from their lower triangle"""
+    for lvl in range(P.shape[0]):
+        S = P[lvl].t()  # S[r, c]
+        P[lvl].copy_(torch.tril(S) + torch.tril(S, -1).t())
+    return P
+
+
+def spd_matrix_device(mf, seed: int, N: int, n: int, device: int = 0):
+    """S = R R^T + n I in Float64xN with R as randn_mf_device (the Cholesky
+    workload's matrix), formed with the device GEMM, made symmetric from its
+    lower triangle and renormalised.  Returns a device MFMatrix."""
+    Rp = randn_mf_device(seed, N, n, n, device=device)
+    S = mf.MFMatrix.zeros(N, n, n, device=device)
+    mf.gemm_(S, mf.MFMatrix.from_tensor(Rp),
+             mf.MFMatrix.from_tensor(Rp.transpose(1, 2).contiguous()))
+    del Rp
+    P = _symmetric_from_lower_(S.storage)
+    P[0].diagonal().add_(float(n))
+    _renorm_torch(P)
+    return S
+
+
+def randn_planes_device(seed: int, N: int, length: int, device: int = 0) -> torch.Tensor:
+    """(N, length) planes: limb 0 ~ N(0,1), limb l = randn 2^-53 |limb l-1|,
+    renormalised"""
+    g = torch.Generator(device=f"cuda:{device}")
+    g.manual_seed(seed)
+    X = torch.empty((N, max(length, 1)), dtype=torch.float64, device=f"cuda:{device}")
+    X[0].normal_(generator=g)
+    for lvl in range(1, N):
+        X[lvl].normal_(generator=g)
+        X[lvl] *= 2.0 ** -53
+        X[lvl] *= X[lvl - 1].abs()
+    return _renorm_torch(X)
+
+
+def spd_batch_fill(mf, batch, seed: int = 5) -> None:
+    """Fill an SPDBatch with the batched workload: S_i = R_i R_i^T + n_i I in
+    Float64xN, R_i n_i x n_i randn with populated lower limbs (product by the
+    device GEMM, symmetric from its lower triangle, renormalised), and one
+    randn right-hand side b_i with populated lower limbs per block."""
+    N, dev = batch.N, batch.device
+    R = randn_planes_device(seed, N, batch.total_s, device=dev)
+    sizes, offs = batch.sizes_host, batch.offsets_host
+    for i in range(batch.nblocks):
+        ni, o = int(sizes[i]), int(offs[i])
+        if ni == 0:
+            continue
+        Rb = R[:, o:o + ni * ni].view(N, ni, ni)
+        mf.gemm_(mf.MFMatrix.from_tensor(batch.S[:, o:o + ni * ni].view(N, ni, ni)),
+                 mf.MFMatrix.from_tensor(Rb), mf.MFMatrix.from_tensor(Rb.transpose(1, 2).contiguous()))
+    del R
+    # symmetric from the lower triangle and n_i on the diagonal, per size class
+    for s in np.unique(sizes):
+        s = int(s)
+        if s == 0:
+            continue
+        idx = np.flatnonzero(sizes == s)
+        cols = torch.as_tensor(offs[idx][:, None] + np.arange(s * s)[None, :], device=batch.S.device)
+        blk = batch.S[:, cols].view(N, len(idx), s, s)  # [l, b, c, r]
+        for lvl in range(N):
+            Sb = blk[lvl].transpose(1, 2)  # [b, r, c]
+            blk[lvl] = torch.tril(Sb) + torch.tril(Sb, -1).transpose(1, 2)
+        blk[0].diagonal(dim1=1, dim2=2).add_(float(s))
+        batch.S[:, cols] = blk.view(N, len(idx), s * s)
+    _renorm_torch(batch.S)
+    batch.X.copy_(randn_planes_device(seed + 1, N, batch.total_b, device=dev)[:, :batch.X.shape[1]])

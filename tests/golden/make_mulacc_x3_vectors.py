@@ -15,7 +15,9 @@ import sys
 
 
 def main() -> None:
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_mulacc_x3_vectors.py <reference checkout>")
+    ref = sys.argv[1]
     src = os.path.join(ref, "test", "mulacc_x3_proof_vectors.jl")
     text = open(src).read()
     block = text[: text.index("@testset")]

@@ -17,7 +17,21 @@ def test_version_and_status_strings(mf):
     lib = mf._native.load()
     assert lib.mflab_version() >= 100
     assert lib.mflab_status_string(0) == b"ok"
-    assert b"argument" in lib.mflab_status_string(-1)
+    assert b"dimension" in lib.mflab_status_string(-1)
+    assert b"option" in lib.mflab_status_string(-7)
+
+
+def test_status_codes_map_to_reference_exceptions(mf):
+    """shape errors are DimensionMismatch, option codes / aliasing /
+    unsupported options ArgumentError (trsv.jl:28-34 raises both kinds)"""
+    nat = mf._native
+    with pytest.raises(mf.DimensionMismatch):
+        mf._check(nat.MFLAB_ERR_ARG, "x")
+    for rc in (nat.MFLAB_ERR_FLAG, nat.MFLAB_ERR_ALIAS, nat.MFLAB_ERR_UNSUPPORTED):
+        with pytest.raises(mf.ArgumentError):
+            mf._check(rc, "x")
+    with pytest.raises(mf.MFLABError):
+        mf._check(nat.MFLAB_ERR_TIMEOUT, "x")
 
 
 def test_binding_covers_header(mf):
