@@ -55,9 +55,10 @@ extern "C" {
 #define MFLAB_ORDER_FAST 1    /* terms applied as unknowns finalise, both directions:
                                  deterministic, not the reference's association */
 
-/* engines of the INT8-slice level products (mflab_set_int8_engine) */
-#define MFLAB_INT8_TCGEN05 0 /* the library's own tcgen05 / TMA / TMEM kernel */
-#define MFLAB_INT8_LIBRARY 1 /* cuBLASLt int8 GEMM */
+/* engines of the int8 products of the INT8 routes (mflab_set_int8_engine) */
+#define MFLAB_INT8_TCGEN05 0      /* the library's own tcgen05 / TMA / TMEM kernel, one CTA per SM */
+#define MFLAB_INT8_LIBRARY 1      /* cuBLASLt int8 GEMM */
+#define MFLAB_INT8_TCGEN05_PAIR 2 /* the library's own tcgen05 kernel on SM pairs (cta_group::2) */
 
 typedef struct mflab_handle mflab_handle;
 
@@ -206,7 +207,8 @@ int mflab_set_int8_engine(mflab_handle *h, int engine);
 
 /* Device-side status word of the tcgen05 kernels issued through this handle:
    0, or the code of a bounded wait that ran out (MFLAB_ERR_TIMEOUT is then
-   the caller's conclusion).  Synchronises.  No reference counterpart. */
+   the caller's conclusion: 1 producer, 2 MMA issuer, 3 epilogue, 4 drain).
+   Reading it resets it to 0.  Synchronises.  No reference counterpart. */
 int mflab_device_status(mflab_handle *h, int *status);
 
 /* y = alpha * op(A) * x + beta * y: op(A) = A (trans 0, A m x n) or A^T

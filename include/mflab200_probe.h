@@ -49,13 +49,24 @@ int mflab_probe_int8_gemm(struct mflab_handle *h, void *stream, int64_t m, int64
 
 /* One int8 x int8 -> int32 GEMM C = A[:, 0:K] * B[:, b_xoff:b_xoff+K]^T with
    K-major operands (A mp x a_cols, B np x b_cols, leading dims in bytes) and
-   column-major C (ldc >= mp), through engine 0 (tcgen05 kernel: mp % 128 == 0,
-   np % 256 == 0, K % 128 == 0) or 1 (library).  *err (device int) receives the
-   kernel's bounded-wait status.  Used by the tests and the roofline probe. */
+   column-major C (ldc >= mp), through engine MFLAB_INT8_TCGEN05 (one-SM
+   tcgen05 kernel), MFLAB_INT8_TCGEN05_PAIR (SM-pair kernel) — both need
+   mp % 128 == 0, np % 256 == 0, K % 128 == 0 — or MFLAB_INT8_LIBRARY.  *err
+   (device int) receives the kernel's bounded-wait status.  Used by the tests
+   and the roofline probe. */
 int mflab_int8_gemm_tn(struct mflab_handle *h, void *stream, int engine, int64_t mp, int64_t np,
                        int64_t K, const int8_t *A, int64_t lda, int64_t a_cols, const int8_t *B,
                        int64_t ldb, int64_t b_cols, int64_t b_xoff, int32_t *C, int64_t ldc,
                        int *err);
+
+/* Test hooks of the tcgen05 kernels issued through this handle: wait_limit
+   bounds their waits of one role on another (mbarrier polls; 0 restores the
+   default), inject = 1 makes the MMA issuer of each launch first wait a
+   short fixed bound on a barrier nothing arrives on, so that wait runs out
+   with copies in flight and the kernel takes its timeout path (error code in the device status word,
+   every issued copy and MMA drained, TMEM freed).  Nothing faults or hangs;
+   the next launch with inject = 0 runs normally.  No reference counterpart. */
+int mflab_set_tc_debug(struct mflab_handle *h, int64_t wait_limit, int inject);
 #ifdef __cplusplus
 }
 #endif

@@ -490,10 +490,17 @@ def ozaki_scheme(config: KernelConfig = _DEFAULT) -> str:
     return sch
 
 
+# int8 engines: the library's own tcgen05 kernels (one CTA per SM, or CTA
+# pairs with cta_group::2) and cuBLASLt; :tcgen05 is the default kernel
+_TC_DEFAULT = 0
+_ENGINES = {"tcgen05": _TC_DEFAULT, "tcgen05_1sm": 0, "tcgen05_pair": 2, "library": 1}
+
+
 def _int8_engine(config: KernelConfig) -> int:
-    engines = {"tcgen05": 0, "library": 1}
+    engines = _ENGINES
     if config.ozaki_engine not in engines:
-        raise ArgumentError("ozaki_engine must be :tcgen05 or :library")
+        raise ArgumentError("ozaki_engine must be :tcgen05, :tcgen05_1sm, :tcgen05_pair or "
+                            ":library")
     if config.ozaki_slices < 0 or config.ozaki_moduli < 0:
         raise ArgumentError("ozaki_slices and ozaki_moduli must be >= 0")
     return engines[config.ozaki_engine]
@@ -549,7 +556,8 @@ def ozaki_last_slices(device: Optional[int] = None) -> int:
 
 def device_status(device: Optional[int] = None) -> int:
     """0, or the status code a tcgen05 kernel of this thread's handle left
-    after a bounded wait ran out (synchronises)"""
+    after a bounded wait ran out (1 producer, 2 MMA issuer, 3 epilogue, 4
+    drain); reading resets it (synchronises)"""
     dev = torch.cuda.current_device() if device is None else device
     v = C.c_int()
     _check(_native.load().mflab_device_status(_handle(dev), C.byref(v)), "device_status")

@@ -55,7 +55,11 @@ extern "C" int mflab_create(mflab_handle **out, int device) {
     h->last_moduli = 0;
     h->solve_order = MFLAB_ORDER_MATCHED;
     h->int8_engine = MFLAB_INT8_TCGEN05;
+    h->tc_limit = 0;
+    h->tc_inject = 0;
     h->stage = nullptr;
+    h->il_stream[0] = h->il_stream[1] = nullptr;
+    h->il_fork = h->il_done[0] = h->il_done[1] = nullptr;
     e = cudaMalloc((void **)&h->dev_flags, 64 * sizeof(int));
     if (e != cudaSuccess) {
         delete h;
@@ -74,6 +78,11 @@ extern "C" int mflab_destroy(mflab_handle *h) {
     if (h->scratch) cudaFree(h->scratch);
     if (h->aux) cudaFree(h->aux);
     if (h->stage) cudaFree(h->stage);
+    for (int i = 0; i < 2; ++i) {
+        if (h->il_stream[i]) cudaStreamDestroy(h->il_stream[i]);
+        if (h->il_done[i]) cudaEventDestroy(h->il_done[i]);
+    }
+    if (h->il_fork) cudaEventDestroy(h->il_fork);
     if (h->dev_flags) cudaFree(h->dev_flags);
     delete h;
     return MFLAB_OK;
@@ -123,5 +132,14 @@ extern "C" int mflab_set_solve_order(mflab_handle *h, int order) {
     if (!h) return MFLAB_ERR_ARG;
     if (order != MFLAB_ORDER_MATCHED && order != MFLAB_ORDER_FAST) return MFLAB_ERR_FLAG;
     h->solve_order = order;
+    return MFLAB_OK;
+}
+
+extern "C" int mflab_set_tc_debug(mflab_handle *h, int64_t wait_limit, int inject) {
+    if (!h) return MFLAB_ERR_ARG;
+    if (wait_limit < 0) return MFLAB_ERR_ARG;
+    if (inject != 0 && inject != 1) return MFLAB_ERR_FLAG;
+    h->tc_limit = wait_limit;
+    h->tc_inject = inject;
     return MFLAB_OK;
 }

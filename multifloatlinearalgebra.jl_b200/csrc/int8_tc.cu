@@ -20,94 +20,26 @@
 //   * warps 2-9: epilogue.  Each reads its 32 TMEM lanes (rows) of one half
 //     with tcgen05.ld.32x32b.x16 and stores the column-major result (a warp
 //     writes 32 consecutive rows of one column).
-// Every mbarrier wait is bounded: on timeout the kernel records an error code
-// in *err, raises a shared abort flag that ends every role's loop, waits
-// (bounded) for its own copies and MMAs in flight, frees its TMEM and returns.
+// Every mbarrier wait is bounded.  A wait of one role on another that runs out
+// (the launch's role bound) records an error code in *err and raises a shared
+// abort flag that ends every role's loop; the CTA then drains what it has
+// itself issued — the producer waits for its copies in flight, the MMA
+// issuer for its MMAs (both with the larger drain bound, which only runs out
+// if the hardware stops completing them) — frees its TMEM and returns.
 // Operands: the padded digit matrices (rows multiple of 128 / 256, K multiple
 // of 128), so no tile needs bounds checks beyond the last half row tile.
-#include <cuda.h>
-#include <cudaTypedefs.h>
-
 #include <mutex>
 
-#include "mflab_internal.h"
-#include "ozaki_common.cuh"
+#include "int8_tc_common.cuh"
 
 namespace mfl {
 
-constexpr int TC_BM = 256, TC_MMA_M = 128, TC_BN = 256, TC_BK = 128, TC_STAGES = 3;
+constexpr int TC_BM = 256, TC_MMA_M = 128, TC_BN = 256, TC_STAGES = 3;
 constexpr uint32_t TC_A_BYTES = TC_BM * TC_BK;               // 32 KiB
 constexpr uint32_t TC_B_BYTES = TC_BN * TC_BK;               // 32 KiB
 constexpr uint32_t TC_STAGE_BYTES = TC_A_BYTES + TC_B_BYTES;  // 64 KiB
 constexpr uint32_t TC_SMEM = TC_STAGES * TC_STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
 constexpr uint32_t TC_TMEM_COLS = 256;  // one 128 x 256 accumulator
-constexpr long long TC_WAIT_LIMIT = 1LL << 24;
-
-// error codes written to *err
-constexpr int TC_ERR_PRODUCER = 1, TC_ERR_MMA = 2, TC_ERR_EPILOGUE = 3;
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
-                 : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-                 "r"(bytes)
-                 : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred P1;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, P1;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-// bounded wait for the completion of phase `parity`; false on timeout
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
-    for (long long i = 0; i < TC_WAIT_LIMIT; ++i)
-        if (mbar_try_wait(bar, parity)) return true;
-    return false;
-}
-
-__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y,
-                                            uint64_t *bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
-        " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
-        : "memory");
-}
-
-// shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row atoms of
-// 1024 bytes (stride byte offset 1024, leading byte offset 16 unused)
-__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t saddr) {
-    uint64_t d = 0;
-    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
-    d |= (uint64_t)1 << 16;                 // leading byte offset (16 B units)
-    d |= (uint64_t)(1024 >> 4) << 32;       // stride byte offset (16 B units)
-    d |= (uint64_t)1 << 46;                 // descriptor version for tcgen05
-    d |= (uint64_t)2 << 61;                 // SWIZZLE_128B
-    return d;
-}
-
-// instruction descriptor: s8 x s8 -> s32, both operands K-major, M = 128, N = 256
-__host__ __device__ constexpr uint32_t idesc_i8(int M, int N) {
-    return (2u << 4)      // D format s32
-           | (1u << 7)    // A signed 8-bit
-           | (1u << 10)   // B signed 8-bit
-           | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
-}
 
 __device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
                                        uint32_t idesc, uint32_t accumulate) {
@@ -125,10 +57,6 @@ __device__ __forceinline__ void mma_commit(uint64_t *bar) {
                  : "memory");
 }
 
-__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-
 // Persistent, warp-specialised kernel: one CTA per SM walks the 256 x 256
 // output tiles tile = blockIdx.x + i * gridDim.x (problem z outermost, then
 // column tiles, then row tiles, so that neighbouring CTAs share B tiles in L2).
@@ -143,26 +71,6 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
 // MODE 0 stores the int32 sums; MODE 1 stores their residues modulo
 // crt_modulus(z) as bytes (C is then a byte matrix: ldc and c_zstride in
 // bytes), the only part of the sums the modular route needs.
-// coordinates of tile number `tile`: all tiles_m x tiles_n tiles of each
-// problem (row tiles fastest), or with `tri` only the tiles that meet the
-// lower triangle of a square grid (column by column)
-__device__ __forceinline__ void tc_tile(int tile, int per_z, int tiles_m, int tri, int &z, int &mt,
-                                        int &nt) {
-    z = tile / per_z;
-    int r = tile % per_z;
-    if (!tri) {
-        mt = r % tiles_m;
-        nt = r / tiles_m;
-        return;
-    }
-    nt = 0;
-    while (r >= tiles_m - nt) {
-        r -= tiles_m - nt;
-        ++nt;
-    }
-    mt = nt + r;
-}
-
 constexpr int TC_THREADS = 320;
 constexpr uint32_t TC_TMEM_ALLOC = 2 * TC_TMEM_COLS;
 
@@ -171,7 +79,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     int8_tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA,
                         const __grid_constant__ CUtensorMap tmB, int K, int b_xoff, void *Cv,
                         int64_t ldc, int a_zrows, int b_zrows, int64_t c_zstride, int tiles_m,
-                        int tiles_n, int nz, int tri, int *err) {
+                        int tiles_n, int nz, int tri, int *err, TcDebug dbg) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     uint64_t *full = (uint64_t *)(smem + TC_STAGES * TC_STAGE_BYTES);
@@ -179,13 +87,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     uint64_t *tfull = empty + TC_STAGES;   // accumulators ready (MMA -> epilogue)
     uint64_t *tempty = tfull + 1;          // accumulators drained (epilogue -> MMA)
     uint64_t *drain = tempty + 1;          // all MMAs of this CTA complete
-    uint32_t *tmem_slot = (uint32_t *)(drain + 1);
+    uint64_t *never = drain + 1;           // injected timeouts wait here (no arrivals)
+    uint32_t *tmem_slot = (uint32_t *)(never + 1);
     int *abort_flag = (int *)(tmem_slot + 1);
 
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
     const int ksteps = K / TC_BK;
     const int per_z = tri ? tiles_m * (tiles_m + 1) / 2 : tiles_m * tiles_n;
     const int total = per_z * nz;
+    const long long lim = dbg.limit;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < TC_STAGES; ++s) {
@@ -195,6 +105,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         mbar_init(tfull, 1);
         mbar_init(tempty, 8);  // one arrival per epilogue warp
         mbar_init(drain, 1);
+        mbar_init(never, 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -220,14 +131,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 tc_tile(tile, per_z, tiles_m, tri, z, mt, nt);
                 const int am0 = z * a_zrows + mt * TC_BM;
                 const int bn0 = z * b_zrows + nt * TC_BN;
+                bool ok = true;
                 for (int kb = 0; kb < ksteps; ++kb, ++ks) {
                     const int s = ks % TC_STAGES;
-                    if (ks >= TC_STAGES && !mbar_wait(&empty[s], ((ks / TC_STAGES) - 1) & 1)) {
-                        atomicExch(err, TC_ERR_PRODUCER);
+                    if (ks >= TC_STAGES &&
+                        !mbar_wait(&empty[s], ((ks / TC_STAGES) - 1) & 1, lim, abort_flag)) {
+                        if (!*(volatile int *)abort_flag) atomicExch(err, TC_ERR_PRODUCER);
                         atomicExch(abort_flag, 1);
+                        ok = false;
                         break;
                     }
-                    if (*(volatile int *)abort_flag) break;
                     uint8_t *sa = smem + s * TC_STAGE_BYTES;
                     uint8_t *sb = sa + TC_A_BYTES;
                     mbar_expect_tx(&full[s], TC_STAGE_BYTES);
@@ -236,23 +149,33 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     tma_load_2d(sa, &tmA, kb * TC_BK, am0, &full[s]);
                     tma_load_2d(sb, &tmB, b_xoff + kb * TC_BK, bn0, &full[s]);
                 }
+                if (!ok) break;
             }
-            // the copies issued last must have landed before the CTA can exit
+            // Drain: the copies of the last (up to TC_STAGES) issued steps must
+            // have landed before the CTA exits.  Each of those steps is the
+            // latest phase of its stage (a stage is refilled only after the
+            // MMAs consumed it), and its phase completes when its bytes land,
+            // whether or not the MMA issuer got to it.
             for (int i = ks - TC_STAGES > 0 ? ks - TC_STAGES : 0; i < ks; ++i)
-                mbar_wait(&full[i % TC_STAGES], (i / TC_STAGES) & 1);
+                if (!mbar_wait(&full[i % TC_STAGES], (i / TC_STAGES) & 1, TC_DRAIN_LIMIT))
+                    atomicExch(err, TC_ERR_DRAIN);
         }
     } else if (warp == 1) {
         if (lane == 0) {
             // ---------------- MMA issuer
             const uint32_t idesc = idesc_i8(TC_MMA_M, TC_BN);
+            if (dbg.inject && !mbar_wait(never, 0, TC_INJECT_POLLS)) {
+                atomicExch(err, TC_ERR_MMA);
+                atomicExch(abort_flag, 1);
+            }
             int ks = 0, it = 0;
             for (int tile = blockIdx.x; tile < total && !*(volatile int *)abort_flag;
                  tile += gridDim.x, ++it) {
                 int z, mt, nt;
                 tc_tile(tile, per_z, tiles_m, tri, z, mt, nt);
                 const bool two_halves = mt * TC_BM + TC_MMA_M < a_zrows;
-                if (it > 0 && !mbar_wait(tempty, (it - 1) & 1)) {
-                    atomicExch(err, TC_ERR_MMA);
+                if (it > 0 && !mbar_wait(tempty, (it - 1) & 1, lim, abort_flag)) {
+                    if (!*(volatile int *)abort_flag) atomicExch(err, TC_ERR_MMA);
                     atomicExch(abort_flag, 1);
                     break;
                 }
@@ -260,8 +183,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 bool ok = true;
                 for (int kb = 0; kb < ksteps; ++kb, ++ks) {
                     const int s = ks % TC_STAGES;
-                    if (!mbar_wait(&full[s], (ks / TC_STAGES) & 1)) {
-                        atomicExch(err, TC_ERR_MMA);
+                    if (!mbar_wait(&full[s], (ks / TC_STAGES) & 1, lim, abort_flag)) {
+                        if (!*(volatile int *)abort_flag) atomicExch(err, TC_ERR_MMA);
                         atomicExch(abort_flag, 1);
                         ok = false;
                         break;
@@ -286,7 +209,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             }
             // every MMA issued by this thread has completed once `drain` flips
             mma_commit(drain);
-            mbar_wait(drain, 0);
+            if (!mbar_wait(drain, 0, TC_DRAIN_LIMIT)) atomicExch(err, TC_ERR_DRAIN);
         }
     } else {
         // ---------------- epilogue: TMEM -> registers -> C
@@ -294,8 +217,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         const int half = (warp - 2) >> 2;  // 0: upper 128 rows, 1: lower 128 rows
         int it = 0;
         for (int tile = blockIdx.x; tile < total; tile += gridDim.x, ++it) {
-            if (!mbar_wait(tfull, it & 1)) {
-                atomicExch(err, TC_ERR_EPILOGUE);
+            if (!mbar_wait(tfull, it & 1, lim, abort_flag)) {
+                if (!*(volatile int *)abort_flag) atomicExch(err, TC_ERR_EPILOGUE);
                 atomicExch(abort_flag, 1);
                 break;
             }
@@ -306,40 +229,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             const int row = mt * TC_BM + half * TC_MMA_M + q * 32 + lane;
             const bool live = mt * TC_BM + half * TC_MMA_M < a_zrows;
             const int n0 = nt * TC_BN;
-            int32_t *C = (int32_t *)Cv + (MODE == 0 ? (int64_t)z * c_zstride : 0);
-            uint8_t *R = (uint8_t *)Cv + (MODE == 1 ? (int64_t)z * c_zstride : 0);
+            void *Cz = MODE == 0 ? (void *)((int32_t *)Cv + (int64_t)z * c_zstride)
+                                 : (void *)((uint8_t *)Cv + (int64_t)z * c_zstride);
             const int pz = crt_modulus(z);
             const double pzinv = 1.0 / (double)pz;
 #pragma unroll 1
             for (int c0 = 0; c0 < TC_BN && live; c0 += 16) {
                 uint32_t v[16];
-                const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) +
-                                       (uint32_t)(half * TC_TMEM_COLS + c0);
-                asm volatile(
-                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-                    "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
-                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
-                      "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
-                      "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-                    : "r"(taddr)
-                    : "memory");
-                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                if (MODE == 0) {
-#pragma unroll
-                    for (int j = 0; j < 16; ++j)
-                        C[(int64_t)(n0 + c0 + j) * ldc + row] = (int32_t)v[j];
-                } else {
-#pragma unroll
-                    for (int j = 0; j < 16; ++j) {
-                        const int g = (int)v[j];
-                        // floor(g / p) or one off; the remainder is then fixed up exactly
-                        const int qq = (int)floor((double)g * pzinv);
-                        int rr = g - qq * pz;
-                        rr += rr < 0 ? pz : 0;
-                        rr -= rr >= pz ? pz : 0;
-                        R[(int64_t)(n0 + c0 + j) * ldc + row] = (uint8_t)rr;
-                    }
-                }
+                tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(half * TC_TMEM_COLS + c0),
+                          v);
+                tc_store16<MODE>(Cz, ldc, row, n0 + c0, v, pz, pzinv);
             }
             // accumulators drained: the MMA warp may overwrite them
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -373,8 +272,8 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 }
 
 // rows x cols int8 row-major matrix (ld bytes), box of box_rows x 128 bytes
-static int make_map(CUtensorMap *map, const int8_t *base, int64_t rows, int64_t cols, int64_t ld,
-                    int box_rows) {
+int tc_make_map(CUtensorMap *map, const int8_t *base, int64_t rows, int64_t cols, int64_t ld,
+                int box_rows) {
     auto fn = encode_fn();
     if (!fn) return MFLAB_ERR_UNSUPPORTED;
     if (((uintptr_t)base & 15) || (ld & 15)) return MFLAB_ERR_ARG;
@@ -389,10 +288,15 @@ static int make_map(CUtensorMap *map, const int8_t *base, int64_t rows, int64_t 
 }
 
 template <int MODE>
+int launch_tc_pair(const CUtensorMap &ta, const CUtensorMap &tb, int64_t mp, int64_t np,
+                   int64_t K, int64_t b_xoff, void *C, int64_t ldc, int *err, cudaStream_t s,
+                   int nz, int64_t c_zstride, int tri, const TcDebug &dbg);
+
+template <int MODE>
 static int launch_tc(int64_t mp, int64_t np, int64_t K, const int8_t *A, int64_t lda,
                      int64_t a_cols, const int8_t *B, int64_t ldb, int64_t b_cols, int64_t b_xoff,
                      void *C, int64_t ldc, int *err, cudaStream_t s, int nz, int64_t c_zstride,
-                     int tri) {
+                     int tri, const TcOpts &o) {
     if (mp % TC_MMA_M || np % TC_BN || K % TC_BK || b_xoff % 16 || K <= 0 || nz < 1)
         return MFLAB_ERR_ARG;
     if (K > a_cols || b_xoff + K > b_cols || K > 0x7fffffff || b_xoff > 0x7fffffff)
@@ -400,11 +304,19 @@ static int launch_tc(int64_t mp, int64_t np, int64_t K, const int8_t *A, int64_t
     if (mp * nz > 0x7fffffff || np * nz > 0x7fffffff || np / TC_BN > 65535 || nz > 65535)
         return MFLAB_ERR_UNSUPPORTED;
     if (MODE == 1 && nz > CRT_TABLE_SIZE) return MFLAB_ERR_ARG;
+    TcDebug dbg;
+    dbg.limit = o.limit > 0 ? o.limit : TC_ROLE_LIMIT;
+    dbg.inject = o.inject;
+    // a CTA stages 256-row boxes of both operands, a CTA of a pair 128-row ones
+    const int box = o.pair ? TC_MMA_M : TC_BM;
     CUtensorMap ta, tb;
-    int rc = make_map(&ta, A, mp * nz, a_cols, lda, TC_BM);
+    int rc = tc_make_map(&ta, A, mp * nz, a_cols, lda, box);
     if (rc) return rc;
-    rc = make_map(&tb, B, np * nz, b_cols, ldb, TC_BN);
+    rc = tc_make_map(&tb, B, np * nz, b_cols, ldb, box);
     if (rc) return rc;
+    if (o.pair)
+        return launch_tc_pair<MODE>(ta, tb, mp, np, K, b_xoff, C, ldc, err, s, nz, c_zstride, tri,
+                                    dbg);
     static std::atomic<unsigned long long> configured{0};
     rc = set_smem_once((const void *)int8_tc_gemm_kernel<MODE>, (int)TC_SMEM, configured,
                        "int8 tc attribute");
@@ -421,7 +333,7 @@ static int launch_tc(int64_t mp, int64_t np, int64_t K, const int8_t *A, int64_t
     const unsigned grid = (unsigned)(tiles < sms ? tiles : sms);
     int8_tc_gemm_kernel<MODE><<<grid, TC_THREADS, TC_SMEM, s>>>(
         ta, tb, (int)K, (int)b_xoff, C, ldc, (int)mp, (int)np, c_zstride, (int)tiles_m,
-        (int)(np / TC_BN), nz, tri, err);
+        (int)(np / TC_BN), nz, tri, err, dbg);
     return record_cuda_error(cudaGetLastError(), "int8 tc gemm");
 }
 
@@ -432,9 +344,10 @@ static int launch_tc(int64_t mp, int64_t np, int64_t K, const int8_t *A, int64_t
 // then holds nz mp rows), rows [z np, (z+1) np) of B and writes C + z c_zstride.
 int int8_gemm_tc(int64_t mp, int64_t np, int64_t K, const int8_t *A, int64_t lda, int64_t a_cols,
                  const int8_t *B, int64_t ldb, int64_t b_cols, int64_t b_xoff, int32_t *C,
-                 int64_t ldc, int *err, cudaStream_t s, int nz, int64_t c_zstride) {
+                 int64_t ldc, int *err, cudaStream_t s, const TcOpts &o, int nz,
+                 int64_t c_zstride) {
     return launch_tc<0>(mp, np, K, A, lda, a_cols, B, ldb, b_cols, b_xoff, C, ldc, err, s, nz,
-                        c_zstride, 0);
+                        c_zstride, 0, o);
 }
 
 // As int8_gemm_tc with nz stacked problems, but problem z stores the residues
@@ -443,10 +356,10 @@ int int8_gemm_tc(int64_t mp, int64_t np, int64_t K, const int8_t *A, int64_t lda
 // tiles that meet the lower triangle (needs ceil(mp / 256) == np / 256).
 int int8_gemm_tc_mod(int64_t mp, int64_t np, int64_t K, const int8_t *A, int64_t lda,
                      int64_t a_cols, const int8_t *B, int64_t ldb, int64_t b_cols, int64_t b_xoff,
-                     uint8_t *R, int64_t ldr, int *err, cudaStream_t s, int nz,
+                     uint8_t *R, int64_t ldr, int *err, cudaStream_t s, const TcOpts &o, int nz,
                      int64_t r_zstride, int tri) {
     return launch_tc<1>(mp, np, K, A, lda, a_cols, B, ldb, b_cols, b_xoff, R, ldr, err, s, nz,
-                        r_zstride, tri);
+                        r_zstride, tri, o);
 }
 
 }  // namespace mfl
@@ -459,9 +372,16 @@ extern "C" int mflab_int8_gemm_tn(mflab_handle *h, void *stream, int engine, int
                                   int64_t a_cols, const int8_t *B, int64_t ldb, int64_t b_cols,
                                   int64_t b_xoff, int32_t *C, int64_t ldc, int *err) {
     if (!h || !A || !B || !C || !err) return MFLAB_ERR_ARG;
+    if (engine != MFLAB_INT8_TCGEN05 && engine != MFLAB_INT8_LIBRARY &&
+        engine != MFLAB_INT8_TCGEN05_PAIR)
+        return MFLAB_ERR_FLAG;
     cudaStream_t s = (cudaStream_t)stream;
-    if (engine == 0)
-        return mfl::int8_gemm_tc(mp, np, K, A, lda, a_cols, B, ldb, b_cols, b_xoff, C, ldc, err, s);
+    if (engine != MFLAB_INT8_LIBRARY) {
+        mfl::TcOpts o = mfl::tc_opts(h);
+        o.pair = engine == MFLAB_INT8_TCGEN05_PAIR;
+        return mfl::int8_gemm_tc(mp, np, K, A, lda, a_cols, B, ldb, b_cols, b_xoff, C, ldc, err, s,
+                                 o);
+    }
     const size_t ws = (size_t)64 << 20;
     int rc = mflab_reserve_scratch(h, ws);
     if (rc) return rc;

@@ -12,8 +12,8 @@
 // when a column is larger): the copy engine moves chunk j
 // (cudaMemcpy2DAsync, which also takes the host leading dimension) into
 // half j mod 2 and a permutation kernel turns it into planes (or planes into
-// the chunk before it leaves).  Everything is ordered on the caller's
-// stream; the staging is why concurrent callers need their own handles.
+// the chunk before it leaves).  The call is ordered on the caller's stream;
+// the staging is why concurrent callers need their own handles.
 #include <algorithm>
 #include <cstdint>
 
@@ -115,9 +115,22 @@ int check_args(mflab_handle *h, int limbs, int64_t m, int64_t n, const void *X, 
     return MFLAB_OK;
 }
 
+// the staging buffer, two non-blocking streams of the highest priority and
+// their events, created on the first host <-> device conversion
 int reserve_stage(mflab_handle *h) {
     if (h->stage) return MFLAB_OK;
-    cudaError_t e = cudaMalloc(&h->stage, 2 * IL_STAGE_HALF);
+    int lo = 0, hi = 0;
+    cudaError_t e = cudaDeviceGetStreamPriorityRange(&lo, &hi);
+    for (int i = 0; i < 2 && e == cudaSuccess; ++i) {
+        if (!h->il_stream[i])
+            e = cudaStreamCreateWithPriority(&h->il_stream[i], cudaStreamNonBlocking, hi);
+        if (e == cudaSuccess && !h->il_done[i])
+            e = cudaEventCreateWithFlags(&h->il_done[i], cudaEventDisableTiming);
+    }
+    if (e == cudaSuccess && !h->il_fork)
+        e = cudaEventCreateWithFlags(&h->il_fork, cudaEventDisableTiming);
+    if (e != cudaSuccess) return record_cuda_error(e, "staging streams");
+    e = cudaMalloc(&h->stage, 2 * IL_STAGE_HALF);
     if (e != cudaSuccess) {
         record_cuda_error(e, "staging cudaMalloc");
         h->stage = nullptr;
@@ -138,12 +151,24 @@ Chunks chunking(int N, int64_t m) {
     return {rows_per_half, 1};
 }
 
-// host <-> device through the staging halves, chunk by chunk on one stream
+// Host <-> device through the staging halves.  Chunk j uses half j mod 2
+// and runs on internal stream j mod 2: its copy and its permutation kernel
+// are ordered on that stream (so chunk j + 2 reuses the half only after
+// chunk j is done with it), while the copy engine moves chunk j + 1 on the
+// other stream during chunk j's kernel.  Both streams start after the
+// caller's stream reaches this point (fork event) and the caller's stream
+// continues after both (join events), so the call is stream-ordered like
+// the others.  The high priority lets the small permutation kernels start
+// ahead of pending blocks of long kernels on other streams.
 template <bool H2D>
 int staged(mflab_handle *h, int N, int64_t m, int64_t n, double *host, int64_t ldh, double *P,
            int64_t ld, int64_t ls, cudaStream_t s) {
     int rc = reserve_stage(h);
     if (rc) return rc;
+    const char *what = H2D ? "mflab_h2d_interleaved" : "mflab_d2h_interleaved";
+    cudaError_t e = cudaEventRecord(h->il_fork, s);
+    for (int i = 0; i < 2 && e == cudaSuccess; ++i) e = cudaStreamWaitEvent(h->il_stream[i], h->il_fork, 0);
+    if (e != cudaSuccess) return record_cuda_error(e, what);
     const Chunks ch = chunking(N, m);
     const size_t hpitch = (size_t)ldh * N * sizeof(double);
     int64_t j = 0;
@@ -152,23 +177,28 @@ int staged(mflab_handle *h, int N, int64_t m, int64_t n, double *host, int64_t l
         for (int64_t r0 = 0; r0 < m; r0 += ch.rb, ++j) {
             const int64_t hgt = std::min(ch.rb, m - r0);
             const size_t row_bytes = (size_t)hgt * N * sizeof(double);
+            cudaStream_t cs = h->il_stream[j & 1];
             double *st = (double *)((char *)h->stage + (j & 1) * IL_STAGE_HALF);
             double *hp = host + (c0 * ldh + r0) * N;
             double *pp = P + c0 * ld + r0;
             if (H2D) {
-                cudaError_t e = cudaMemcpy2DAsync(st, row_bytes, hp, hpitch, row_bytes, (size_t)w,
-                                                  cudaMemcpyHostToDevice, s);
-                if (e != cudaSuccess) return record_cuda_error(e, "mflab_h2d_interleaved copy");
-                if ((rc = launch<true>(N, hgt, w, st, hgt, pp, ld, ls, s))) return rc;
+                e = cudaMemcpy2DAsync(st, row_bytes, hp, hpitch, row_bytes, (size_t)w,
+                                      cudaMemcpyHostToDevice, cs);
+                if (e != cudaSuccess) return record_cuda_error(e, what);
+                if ((rc = launch<true>(N, hgt, w, st, hgt, pp, ld, ls, cs))) return rc;
             } else {
-                if ((rc = launch<false>(N, hgt, w, st, hgt, pp, ld, ls, s))) return rc;
-                cudaError_t e = cudaMemcpy2DAsync(hp, hpitch, st, row_bytes, row_bytes, (size_t)w,
-                                                  cudaMemcpyDeviceToHost, s);
-                if (e != cudaSuccess) return record_cuda_error(e, "mflab_d2h_interleaved copy");
+                if ((rc = launch<false>(N, hgt, w, st, hgt, pp, ld, ls, cs))) return rc;
+                e = cudaMemcpy2DAsync(hp, hpitch, st, row_bytes, row_bytes, (size_t)w,
+                                      cudaMemcpyDeviceToHost, cs);
+                if (e != cudaSuccess) return record_cuda_error(e, what);
             }
         }
     }
-    return MFLAB_OK;
+    for (int i = 0; i < 2 && e == cudaSuccess; ++i) {
+        e = cudaEventRecord(h->il_done[i], h->il_stream[i]);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(s, h->il_done[i], 0);
+    }
+    return e == cudaSuccess ? MFLAB_OK : record_cuda_error(e, what);
 }
 
 }  // namespace

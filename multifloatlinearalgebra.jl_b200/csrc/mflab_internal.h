@@ -61,16 +61,27 @@ inline int cuda_status(cudaError_t e) {
 }
 
 
+// Launch options of the tcgen05 int8 GEMM kernels: the CTA-pair kernel
+// (int8_tc2.cu) or the one-SM kernel (int8_tc.cu), the bound of their
+// role-to-role waits in mbarrier polls (0: the default) and, for tests of
+// the timeout path, an injected wait that runs out.
+struct TcOpts {
+    int pair = 0;
+    long long limit = 0;
+    int inject = 0;
+};
+
 // int8 x int8 -> int32 TN GEMM through the library (ozaki.cu) and through the
-// tcgen05 kernel (int8_tc.cu)
+// tcgen05 kernels (int8_tc.cu, int8_tc2.cu)
 int int8_gemm_tn(int64_t m, int64_t n, int64_t K, const int8_t *A, int64_t lda, const int8_t *B,
                  int64_t ldb, int32_t *I, int64_t ldi, void *ws, size_t wsb, cudaStream_t s);
 int int8_gemm_tc(int64_t mp, int64_t np, int64_t K, const int8_t *A, int64_t lda, int64_t a_cols,
                  const int8_t *B, int64_t ldb, int64_t b_cols, int64_t b_xoff, int32_t *C,
-                 int64_t ldc, int *err, cudaStream_t s, int nz = 1, int64_t c_zstride = 0);
+                 int64_t ldc, int *err, cudaStream_t s, const TcOpts &o, int nz = 1,
+                 int64_t c_zstride = 0);
 int int8_gemm_tc_mod(int64_t mp, int64_t np, int64_t K, const int8_t *A, int64_t lda,
                      int64_t a_cols, const int8_t *B, int64_t ldb, int64_t b_cols, int64_t b_xoff,
-                     uint8_t *R, int64_t ldr, int *err, cudaStream_t s, int nz,
+                     uint8_t *R, int64_t ldr, int *err, cudaStream_t s, const TcOpts &o, int nz,
                      int64_t r_zstride, int tri = 0);
 void record_error_message(const char *msg);
 // modular INT8 route (ozaki_crt.cu); T = 0 lets the tuner choose.  The SYRK
@@ -130,11 +141,29 @@ struct mflab_handle {
     int last_moduli;  // modulus count the last modular (CRT) INT8 call used
     int solve_order;  // MFLAB_ORDER_MATCHED or MFLAB_ORDER_FAST for triangular solves
     int int8_engine;  // MFLAB_INT8_TCGEN05 or MFLAB_INT8_LIBRARY for the level products
-    // staging of the interleaved host <-> limb-plane copies (64 MiB, on first use)
+    // role-wait bound (0: default) and timeout injection of the tcgen05 kernels
+    long long tc_limit;
+    int tc_inject;
+    // staging of the interleaved host <-> limb-plane copies (64 MiB, on first
+    // use) and the two high-priority streams that alternate over its halves
     void *stage;
+    cudaStream_t il_stream[2];
+    cudaEvent_t il_fork, il_done[2];
 };
 
 int mflab_reserve_aux(mflab_handle *h, size_t bytes);
 
 // grow the handle's scratch to at least `bytes`; returns MFLAB_OK or an error
 int mflab_reserve_scratch(mflab_handle *h, size_t bytes);
+
+namespace mfl {
+// launch options of the tcgen05 kernels issued through handle h
+inline TcOpts tc_opts(const mflab_handle *h) {
+    TcOpts o;
+    o.pair = h->int8_engine == MFLAB_INT8_TCGEN05_PAIR;
+    o.limit = h->tc_limit;
+    o.inject = h->tc_inject;
+    return o;
+}
+inline bool tc_engine(const mflab_handle *h) { return h->int8_engine != MFLAB_INT8_LIBRARY; }
+}  // namespace mfl

@@ -307,7 +307,8 @@ static inline void phase(int i, cudaStream_t s) { ozaki_phase(i, s); }
 template <int N>
 static int ozaki_n(int64_t m, int64_t n, int64_t k, Mat A, Mat B, Mat C, const double *alpha,
                    const double *beta, int S, char *base, const OzPlan &p, const int *rowexp,
-                   const int *colexp, cudaStream_t s, int engine, int *tc_err) {
+                   const int *colexp, cudaStream_t s, int engine, int *tc_err,
+                   const TcOpts &opts) {
     phase(0, s);
     int8_t *A8 = (int8_t *)base;
     int8_t *B8 = (int8_t *)(base + p.a8);
@@ -322,10 +323,10 @@ static int ozaki_n(int64_t m, int64_t n, int64_t k, Mat A, Mat B, Mat C, const d
     phase(1, s);
     const int64_t ld8 = (int64_t)S * p.kp;
     for (int L = 2; L <= S + 1; ++L) {
-        if (engine == MFLAB_INT8_TCGEN05)
+        if (engine != MFLAB_INT8_LIBRARY)
             rc = int8_gemm_tc(p.mp, p.np, (int64_t)(L - 1) * p.kp, A8, ld8, ld8, B8, ld8, ld8,
                               (int64_t)(S - L + 1) * p.kp, I + (size_t)(L - 2) * p.plane, p.ldi,
-                              tc_err, s);
+                              tc_err, s, opts);
         else
             rc = int8_gemm_tn(p.mp, p.np, (int64_t)(L - 1) * p.kp, A8, ld8,
                               B8 + (int64_t)(S - L + 1) * p.kp, ld8,
@@ -470,9 +471,9 @@ int ozaki_gemm(mflab_handle *h, int N, int S, int64_t m, int64_t n, int64_t k, M
     char *base = (char *)h->scratch;
     int *tc_err = h->dev_flags + 1;
     switch (N) {
-    case 2: return ozaki_n<2>(m, n, k, A, B, C, alpha, beta, S, base, p, rowexp, colexp, s, h->int8_engine, tc_err);
-    case 3: return ozaki_n<3>(m, n, k, A, B, C, alpha, beta, S, base, p, rowexp, colexp, s, h->int8_engine, tc_err);
-    default: return ozaki_n<4>(m, n, k, A, B, C, alpha, beta, S, base, p, rowexp, colexp, s, h->int8_engine, tc_err);
+    case 2: return ozaki_n<2>(m, n, k, A, B, C, alpha, beta, S, base, p, rowexp, colexp, s, h->int8_engine, tc_err, tc_opts(h));
+    case 3: return ozaki_n<3>(m, n, k, A, B, C, alpha, beta, S, base, p, rowexp, colexp, s, h->int8_engine, tc_err, tc_opts(h));
+    default: return ozaki_n<4>(m, n, k, A, B, C, alpha, beta, S, base, p, rowexp, colexp, s, h->int8_engine, tc_err, tc_opts(h));
     }
 }
 
@@ -599,7 +600,9 @@ extern "C" int mflab_probe_int8_gemm(mflab_handle *h, void *stream, int64_t m, i
 
 extern "C" int mflab_set_int8_engine(mflab_handle *h, int engine) {
     if (!h) return MFLAB_ERR_ARG;
-    if (engine != MFLAB_INT8_TCGEN05 && engine != MFLAB_INT8_LIBRARY) return MFLAB_ERR_FLAG;
+    if (engine != MFLAB_INT8_TCGEN05 && engine != MFLAB_INT8_LIBRARY &&
+        engine != MFLAB_INT8_TCGEN05_PAIR)
+        return MFLAB_ERR_FLAG;
     h->int8_engine = engine;
     return MFLAB_OK;
 }
@@ -608,6 +611,8 @@ extern "C" int mflab_device_status(mflab_handle *h, int *status) {
     if (!h || !status) return MFLAB_ERR_ARG;
     int v = 0;
     cudaError_t e = cudaMemcpy(&v, h->dev_flags + 1, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && v != 0) e = cudaMemset(h->dev_flags + 1, 0, sizeof(int));
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return mfl::record_cuda_error(e, "device status");
     *status = v;
     return MFLAB_OK;

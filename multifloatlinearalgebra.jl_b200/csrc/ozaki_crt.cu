@@ -748,9 +748,9 @@ static int crt_gemm_n(mflab_handle *hd, const CrtPlan &p, int64_t m, int64_t n, 
     for (int L = 0; L < p.Q && rc == MFLAB_OK; ++L) {
         const int64_t K = (int64_t)(L + 1) * p.kp, bx = (int64_t)(p.Q - 1 - L) * p.kp;
         uint8_t *RL = Rs + (size_t)L * p.T * p.plane;
-        if (hd->int8_engine == MFLAB_INT8_TCGEN05) {
+        if (tc_engine(hd)) {
             rc = int8_gemm_tc_mod(p.mp, p.np, K, A8, ld8, ld8, B8, ld8, ld8, bx, RL, p.ldi,
-                                  hd->dev_flags + 1, s, p.T, (int64_t)p.plane);
+                                  hd->dev_flags + 1, s, tc_opts(hd), p.T, (int64_t)p.plane);
         } else {
             int32_t *G = (int32_t *)(ws + ((size_t)64 << 20));
             const size_t cnt = (size_t)p.ldi * p.np;
@@ -856,9 +856,9 @@ static int crt_syrk_n(mflab_handle *hd, const CrtPlan &p, int trans, int64_t n, 
     for (int L = 0; L < p.Q && rc == MFLAB_OK; ++L) {
         const int64_t K = (int64_t)(L + 1) * p.kp, bx = (int64_t)(p.Q - 1 - L) * p.kp;
         uint8_t *RL = Rs + (size_t)L * p.T * p.plane;
-        if (hd->int8_engine == MFLAB_INT8_TCGEN05) {
+        if (tc_engine(hd)) {
             rc = int8_gemm_tc_mod(p.mp, p.np, K, A8, ld8, ld8, B8, ld8, ld8, bx, RL, p.ldi,
-                                  hd->dev_flags + 1, s, p.T, (int64_t)p.plane, 1);
+                                  hd->dev_flags + 1, s, tc_opts(hd), p.T, (int64_t)p.plane, 1);
         } else {  // the library computes whole products; only the lower part is used
             int32_t *G = (int32_t *)(ws + ((size_t)64 << 20));
             const size_t cnt = (size_t)p.ldi * p.np;
