@@ -424,16 +424,19 @@ class Runner:
         assert rc == 0, rc
         return [ms[i] for i in range(4)], ops.value
 
-    def int8_peak(self):
-        """library int8 GEMM throughput: the measured denominator of the
-        tensor roofline (the route itself runs the tcgen05 kernel)"""
+    def int8_peak(self, fill=1):
+        """library int8 GEMM throughput, the measured denominator of the
+        tensor roofline (the route itself runs the tcgen05 kernel): fill 1 on
+        uniformly distributed bytes like the route's residues, fill 0 on
+        constant bytes (less switching power, so a higher clock under the
+        power cap)"""
         import ctypes as C
         mf = self.mf
         lib = mf._native.load()
         ms = C.c_float()
         n, k = 8192, 16384
         rc = lib.mflab_probe_int8_gemm(mf._handle(self.local), self.stream.cuda_stream, n, n, k, 3,
-                                       C.byref(ms))
+                                       fill, C.byref(ms))
         assert rc == 0, rc
         return 2.0 * n * n * k / (ms.value / 1e3)
 
@@ -828,10 +831,13 @@ def main():
                   "peak_source": "measured in this run (DFMA probe, burst)"}
     if route == "ozaki":
         ph, ops = R.phases(N, n, A, B, Cm, scheme, knob)
-        peak8 = R.int8_peak()
+        peak8 = R.int8_peak(fill=1)
+        peak8c = R.int8_peak(fill=0)
         achieved = ops / (ph[2] / 1e3)
         roof = {"bound": "tensor", "achieved": achieved / 1e12, "peak": peak8 / 1e12,
                 "unit": "INT8 TOP/s", "frac": achieved / peak8,
+                "frac_of_constant_data_peak": achieved / peak8c,
+                "peak_constant_data": peak8c / 1e12,
                 "frac_of_nominal_4500": achieved / 4.5e15,
                 "traffic": read_traffic(f"int8_tc_{scheme}_x{N}_n{n}", scale_from_smaller=True),
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch "
@@ -841,7 +847,10 @@ def main():
                           + ("residue GEMMs, all moduli of a digit level in one launch"
                              if scheme == "modular" else "level GEMMs (K = (L-1) k)"),
                 "peak_source": "measured in this run: cuBLASLt int8 TN GEMM 8192x8192x16384 "
-                               "(burst); nominal dense INT8 is 4500 TOP/s",
+                               "(burst) on uniformly distributed bytes, like the residues; "
+                               "peak_constant_data is the same GEMM on constant bytes, which "
+                               "draws less power and runs faster under the power cap; nominal "
+                               "dense INT8 is 4500 TOP/s",
                 "phases_ms": {"exponents_tune": ph[0], "split": ph[1], "int8_gemms": ph[2],
                               "reconstruct_accumulate": ph[3]}}
     else:

@@ -28,6 +28,7 @@
 #ifndef MFLAB200_H
 #define MFLAB200_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -81,6 +82,20 @@ int mflab_destroy(mflab_handle *h);
    backward row wait for the previous one; MFLAB_ORDER_FAST applies every term
    as soon as its unknown is final.  No reference counterpart. */
 int mflab_set_solve_order(mflab_handle *h, int order);
+
+/* ----------------------------------------------------- device memory --- */
+/* Device memory and stream-ordered copies for bindings without a CUDA
+   runtime of their own (the Julia layer's MFDeviceMatrix planes and the
+   4-byte info words of the factorizations live here).  kind: 0 host to
+   device, 1 device to host, 2 device to device.  The reference works on host
+   arrays and has no counterpart; these replace the Matrix{Float64xN}
+   allocations a caller of gemm!/cholesky! (gemm.jl:747-755,
+   cholesky.jl:68-107) would make. */
+int mflab_malloc(int device, size_t bytes, void **ptr);
+int mflab_free(void *ptr);
+int mflab_memcpy(void *dst, const void *src, size_t bytes, int kind, void *stream);
+int mflab_memset(void *dst, int value, size_t bytes, void *stream);
+int mflab_stream_synchronize(void *stream);
 
 /* ------------------------------------------- interleaved <-> limb planes --- */
 /* A Julia Matrix{MultiFloat{Float64,N}} — the reference's operand type

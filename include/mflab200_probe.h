@@ -43,9 +43,12 @@ int mflab_gemm_ozaki_crt_phases(struct mflab_handle *h, void *stream, int limbs,
 int mflab_ozaki_crt_reduce_host(int T, int count, const int32_t *G, uint32_t *mag, int *neg);
 
 /* Best device time (ms) of `reps` int8 x int8 -> int32 TN GEMMs of m x n x k
-   through the library path the INT8-slice route uses.  Synchronises. */
+   through the library path the INT8 routes can use, on operands of constant
+   bytes (fill 0) or of uniformly distributed bytes (fill 1, the operand
+   statistics of the routes: the tensor pipe's power, and so its clock under
+   the power cap, depends on the data).  Synchronises. */
 int mflab_probe_int8_gemm(struct mflab_handle *h, void *stream, int64_t m, int64_t n, int64_t k,
-                          int reps, float *ms);
+                          int reps, int fill, float *ms);
 
 /* One int8 x int8 -> int32 GEMM C = A[:, 0:K] * B[:, b_xoff:b_xoff+K]^T with
    K-major operands (A mp x a_cols, B np x b_cols, leading dims in bytes) and

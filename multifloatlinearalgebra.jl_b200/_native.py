@@ -167,8 +167,13 @@ SIGNATURES = {
                            _i64, _vp, _i64, _vp],
     "mflab_gemm_ozaki_phases": [_vp, _vp, _int, _int, _i64, _i64, _i64, _vp, _i64, _i64, _vp, _i64,
                                 _i64, _vp, _i64, _i64, _d, _d, C.POINTER(C.c_float), _d],
-    "mflab_probe_int8_gemm": [_vp, _vp, _i64, _i64, _i64, _int, C.POINTER(C.c_float)],
+    "mflab_probe_int8_gemm": [_vp, _vp, _i64, _i64, _i64, _int, _int, C.POINTER(C.c_float)],
     "mflab_set_tc_debug": [_vp, _i64, _int],
+    "mflab_malloc": [_int, C.c_size_t, C.POINTER(_vp)],
+    "mflab_free": [_vp],
+    "mflab_memcpy": [_vp, _vp, C.c_size_t, _int, _vp],
+    "mflab_memset": [_vp, _int, C.c_size_t, _vp],
+    "mflab_stream_synchronize": [_vp],
     "mflab_h2d_interleaved": [_vp, _vp, _int, _i64, _i64, _vp, _i64, _vp, _i64, _i64],
     "mflab_d2h_interleaved": [_vp, _vp, _int, _i64, _i64, _vp, _i64, _i64, _vp, _i64],
     "mflab_interleaved_to_planes": [_vp, _vp, _int, _i64, _i64, _vp, _i64, _vp, _i64, _i64],

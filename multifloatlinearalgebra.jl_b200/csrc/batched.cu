@@ -283,6 +283,7 @@ extern "C" int mflab_spd_batched_ex(mflab_handle *h, void *stream, int limbs, in
                                     const int64_t *order, double *S, int64_t ls_s, double *X,
                                     int64_t ls_x, int64_t block, int solve, int *info,
                                     int *counter, int grid, int threads) {
+    MFLAB_RANGE("mflab_spd_batched_ex");
     if (!h) return MFLAB_ERR_UNSUPPORTED;
     int rc = batched_check(limbs, nblocks, max_size);
     if (rc) return rc;
@@ -307,6 +308,7 @@ extern "C" int mflab_spd_batched(mflab_handle *h, void *stream, int limbs, int64
                                  const int64_t *boffsets, const int64_t *order, double *S,
                                  int64_t ls_s, double *X, int64_t ls_x, int64_t block, int solve,
                                  int *info, int *counter, int grid) {
+    MFLAB_RANGE("mflab_spd_batched");
     return mflab_spd_batched_ex(h, stream, limbs, nblocks, max_size, sizes, offsets, boffsets,
                                 order, S, ls_s, X, ls_x, block, solve, info, counter, grid,
                                 mfl::BATCH_NT);
@@ -319,6 +321,7 @@ extern "C" int mflab_spd_batched_adjoint_ex(mflab_handle *h, void *stream, int l
                                             const double *L, int64_t ls_s, const double *X,
                                             double *XB, int64_t ls_x, double *SB, const int *info,
                                             int *counter, int grid, int threads) {
+    MFLAB_RANGE("mflab_spd_batched_adjoint_ex");
     if (!h) return MFLAB_ERR_UNSUPPORTED;
     int rc = batched_check(limbs, nblocks, max_size);
     if (rc) return rc;
@@ -343,6 +346,7 @@ extern "C" int mflab_spd_batched_adjoint(mflab_handle *h, void *stream, int limb
                                          const int64_t *order, const double *L, int64_t ls_s,
                                          const double *X, double *XB, int64_t ls_x, double *SB,
                                          const int *info, int *counter, int grid) {
+    MFLAB_RANGE("mflab_spd_batched_adjoint");
     return mflab_spd_batched_adjoint_ex(h, stream, limbs, nblocks, max_size, sizes, offsets,
                                         boffsets, order, L, ls_s, X, XB, ls_x, SB, info, counter,
                                         grid, mfl::BATCH_NT);

@@ -305,6 +305,7 @@ extern "C" int mflab_gemm(mflab_handle *h, void *stream, int limbs, int route, i
                           int64_t n, int64_t k, const double *A, int64_t lda, int64_t lsa,
                           const double *B, int64_t ldb, int64_t lsb, double *C, int64_t ldc,
                           int64_t lsc, const double *alpha, const double *beta) {
+    MFLAB_RANGE("mflab_gemm");
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
     if (m < 0 || n < 0 || k < 0 || !alpha || !beta) return MFLAB_ERR_ARG;
     if (m == 0 || n == 0) return MFLAB_OK;
@@ -330,6 +331,7 @@ extern "C" int mflab_gemv(mflab_handle *h, void *stream, int limbs, int trans, i
                           int64_t n, const double *A, int64_t lda, int64_t lsa, const double *x,
                           int64_t lsx, double *y, int64_t lsy, const double *alpha,
                           const double *beta) {
+    MFLAB_RANGE("mflab_gemv");
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
     if (trans != 0 && trans != 1) return MFLAB_ERR_FLAG;
     if (m < 0 || n < 0 || !alpha || !beta) return MFLAB_ERR_ARG;
@@ -350,6 +352,7 @@ extern "C" int mflab_gemv(mflab_handle *h, void *stream, int limbs, int trans, i
 extern "C" int mflab_symv(mflab_handle *h, void *stream, int limbs, int uplo, int64_t n,
                           const double *A, int64_t lda, int64_t lsa, const double *x, int64_t lsx,
                           double *y, int64_t lsy, const double *alpha, const double *beta) {
+    MFLAB_RANGE("mflab_symv");
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
     if (uplo != 0 && uplo != 1) return MFLAB_ERR_FLAG;
     if (n < 0 || !alpha || !beta) return MFLAB_ERR_ARG;
@@ -383,6 +386,7 @@ __global__ void dot_kernel(int64_t m, int64_t n, Mat X, Mat Y, double *out) {
 extern "C" int mflab_dot(mflab_handle *h, void *stream, int limbs, int64_t m, int64_t n,
                          const double *x, int64_t ldx, int64_t lsx, const double *y, int64_t ldy,
                          int64_t lsy, double *out) {
+    MFLAB_RANGE("mflab_dot");
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
     if (m < 0 || n < 0 || !out || (m > 0 && (ldx < m || ldy < m))) return MFLAB_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
@@ -401,6 +405,7 @@ extern "C" int mflab_dot(mflab_handle *h, void *stream, int limbs, int64_t m, in
 extern "C" int mflab_syrk_packed(mflab_handle *h, void *stream, int limbs, int64_t n, int64_t kp,
                                  int64_t k0, int64_t k1, const double *P, int64_t ldp, int64_t lsp,
                                  double *C, int64_t lsc, const double *alpha, const double *beta) {
+    MFLAB_RANGE("mflab_syrk_packed");
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
     if (n < 0 || kp < 0 || !alpha || !beta) return MFLAB_ERR_ARG;
     if (!(0 <= k0 && k0 < k1 && k1 <= kp)) return MFLAB_ERR_ARG;
@@ -423,6 +428,7 @@ extern "C" int mflab_syrk_packed(mflab_handle *h, void *stream, int limbs, int64
 extern "C" int mflab_trmm(mflab_handle *h, void *stream, int limbs, int side, int uplo, int trans,
                           int diag, int64_t m, int64_t n, const double *A, int64_t lda,
                           int64_t lsa, double *B, int64_t ldb, int64_t lsb, const double *alpha) {
+    MFLAB_RANGE("mflab_trmm");
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
     if ((side | uplo | trans | diag) & ~1) return MFLAB_ERR_FLAG;
     if (m < 0 || n < 0 || !alpha) return MFLAB_ERR_ARG;
@@ -455,6 +461,7 @@ extern "C" int mflab_trmm(mflab_handle *h, void *stream, int limbs, int side, in
 extern "C" int mflab_syrk_lower(mflab_handle *h, void *stream, int limbs, int64_t n, int64_t k,
                                 const double *P, int64_t ldp, int64_t lsp, double *C, int64_t ldc,
                                 int64_t lsc, const double *alpha, const double *beta) {
+    MFLAB_RANGE("mflab_syrk_lower");
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
     if (n < 0 || k < 0 || !alpha || !beta) return MFLAB_ERR_ARG;
     if (n == 0) return MFLAB_OK;
@@ -469,6 +476,7 @@ extern "C" int mflab_gemmt_lower(mflab_handle *h, void *stream, int limbs, int64
                                  const double *A, int64_t lda, int64_t lsa, const double *B,
                                  int64_t ldb, int64_t lsb, double *C, int64_t ldc, int64_t lsc,
                                  const double *alpha, const double *beta) {
+    MFLAB_RANGE("mflab_gemmt_lower");
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
     if (n < 0 || k < 0 || !alpha || !beta) return MFLAB_ERR_ARG;
     if (n == 0) return MFLAB_OK;

@@ -143,3 +143,51 @@ extern "C" int mflab_set_tc_debug(mflab_handle *h, int64_t wait_limit, int injec
     h->tc_inject = inject;
     return MFLAB_OK;
 }
+
+// ------------------------------------------------ memory for bindings ---
+// Device memory and copies for a binding that has no CUDA runtime of its own
+// (the Julia layer holds MFDeviceMatrix planes allocated here).
+
+extern "C" int mflab_malloc(int device, size_t bytes, void **ptr) {
+    if (!ptr) return MFLAB_ERR_ARG;
+    *ptr = nullptr;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess && bytes > 0) e = cudaMalloc(ptr, bytes);
+    if (e != cudaSuccess) {
+        mfl::record_cuda_error(e, "mflab_malloc");
+        *ptr = nullptr;
+        return MFLAB_ERR_ALLOC;
+    }
+    return MFLAB_OK;
+}
+
+extern "C" int mflab_free(void *ptr) {
+    if (!ptr) return MFLAB_OK;
+    return mfl::record_cuda_error(cudaFree(ptr), "mflab_free");
+}
+
+extern "C" int mflab_memcpy(void *dst, const void *src, size_t bytes, int kind, void *stream) {
+    if (bytes == 0) return MFLAB_OK;
+    if (!dst || !src) return MFLAB_ERR_ARG;
+    cudaMemcpyKind k;
+    switch (kind) {
+    case 0: k = cudaMemcpyHostToDevice; break;
+    case 1: k = cudaMemcpyDeviceToHost; break;
+    case 2: k = cudaMemcpyDeviceToDevice; break;
+    default: return MFLAB_ERR_FLAG;
+    }
+    return mfl::record_cuda_error(cudaMemcpyAsync(dst, src, bytes, k, (cudaStream_t)stream),
+                                  "mflab_memcpy");
+}
+
+extern "C" int mflab_memset(void *dst, int value, size_t bytes, void *stream) {
+    if (bytes == 0) return MFLAB_OK;
+    if (!dst) return MFLAB_ERR_ARG;
+    return mfl::record_cuda_error(cudaMemsetAsync(dst, value, bytes, (cudaStream_t)stream),
+                                  "mflab_memset");
+}
+
+extern "C" int mflab_stream_synchronize(void *stream) {
+    return mfl::record_cuda_error(cudaStreamSynchronize((cudaStream_t)stream),
+                                  "mflab_stream_synchronize");
+}

@@ -732,6 +732,7 @@ using mfl::Mat;
 
 extern "C" int mflab_potrf(mflab_handle *h, void *stream, int limbs, int64_t n, double *A,
                            int64_t lda, int64_t lsa, int64_t block, int *info) {
+    MFLAB_RANGE("mflab_potrf");
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
     if (n < 0 || (n > 0 && lda < n) || !info) return MFLAB_ERR_ARG;
     if (block < 1) block = 1;
@@ -748,6 +749,7 @@ extern "C" int mflab_potrf(mflab_handle *h, void *stream, int limbs, int64_t n, 
 extern "C" int mflab_potrf_ozaki(mflab_handle *h, void *stream, int limbs, int moduli, int64_t n,
                                  double *A, int64_t lda, int64_t lsa, int64_t nb, int64_t block,
                                  int *info) {
+    MFLAB_RANGE("mflab_potrf_ozaki");
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
     if (n < 0 || (n > 0 && lda < n) || !info || moduli < 0) return MFLAB_ERR_ARG;
     if (block < 1) block = 1;
@@ -765,6 +767,7 @@ extern "C" int mflab_potrf_ozaki(mflab_handle *h, void *stream, int limbs, int m
 extern "C" int mflab_potrs(mflab_handle *h, void *stream, int limbs, int64_t n, int64_t nrhs,
                            const double *L, int64_t ldl, int64_t lsl, double *B, int64_t ldb,
                            int64_t lsb) {
+    MFLAB_RANGE("mflab_potrs");
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
     if (n < 0 || nrhs < 0 || (n > 0 && (ldl < n || ldb < n))) return MFLAB_ERR_ARG;
     const double one[4] = {1.0, 0.0, 0.0, 0.0};
@@ -778,6 +781,7 @@ extern "C" int mflab_potrs(mflab_handle *h, void *stream, int limbs, int64_t n, 
 extern "C" int mflab_getrf(mflab_handle *h, void *stream, int limbs, int64_t m, int64_t n,
                            double *A, int64_t lda, int64_t lsa, int64_t *ipiv, int64_t block,
                            int *info) {
+    MFLAB_RANGE("mflab_getrf");
     if (!h || !(limbs == 1 || mfl::valid_limbs(limbs))) return MFLAB_ERR_UNSUPPORTED;
     if (m < 0 || n < 0 || (m > 0 && lda < m) || !info || (m > 0 && n > 0 && !ipiv))
         return MFLAB_ERR_ARG;
@@ -802,6 +806,7 @@ extern "C" int mflab_getrf(mflab_handle *h, void *stream, int limbs, int64_t m, 
 extern "C" int mflab_getrf_ozaki(mflab_handle *h, void *stream, int limbs, int moduli, int64_t m,
                                  int64_t n, double *A, int64_t lda, int64_t lsa, int64_t *ipiv,
                                  int64_t nb, int64_t block, int *info) {
+    MFLAB_RANGE("mflab_getrf_ozaki");
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
     if (m < 0 || n < 0 || (m > 0 && lda < m) || !info || (m > 0 && n > 0 && !ipiv) || moduli < 0)
         return MFLAB_ERR_ARG;
@@ -825,6 +830,7 @@ extern "C" int mflab_getrf_ozaki(mflab_handle *h, void *stream, int limbs, int m
 extern "C" int mflab_getrs(mflab_handle *h, void *stream, int limbs, int64_t n, int64_t nrhs,
                            const double *LU, int64_t ldl, int64_t lsl, const int64_t *ipiv,
                            double *B, int64_t ldb, int64_t lsb) {
+    MFLAB_RANGE("mflab_getrs");
     if (!h || !(limbs == 1 || mfl::valid_limbs(limbs))) return MFLAB_ERR_UNSUPPORTED;
     if (n < 0 || nrhs < 0 || (n > 0 && (ldl < n || ldb < n || !ipiv))) return MFLAB_ERR_ARG;
     if (n == 0 || nrhs == 0) return MFLAB_OK;
@@ -857,6 +863,7 @@ extern "C" int mflab_getrs(mflab_handle *h, void *stream, int limbs, int64_t n, 
 
 extern "C" int mflab_max_abs(mflab_handle *h, void *stream, int limbs, int64_t m, int64_t n,
                              const double *A, int64_t lda, int64_t lsa, int region, double *out) {
+    MFLAB_RANGE("mflab_max_abs");
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
     if (region < 0 || region > 2) return MFLAB_ERR_FLAG;
     if (m < 0 || n < 0 || !out) return MFLAB_ERR_ARG;
@@ -876,6 +883,7 @@ extern "C" int mflab_max_abs(mflab_handle *h, void *stream, int limbs, int64_t m
 extern "C" int mflab_diag_summary(mflab_handle *h, void *stream, int limbs, const double *A,
                                   int64_t lda, int64_t lsa, int64_t count, const double *num,
                                   const double *den, double *out) {
+    MFLAB_RANGE("mflab_diag_summary");
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
     if (count < 0 || !out) return MFLAB_ERR_ARG;
     Mat a{(double *)A, lda, lsa};

@@ -371,6 +371,7 @@ extern "C" int mflab_int8_gemm_tn(mflab_handle *h, void *stream, int engine, int
                                   int64_t np, int64_t K, const int8_t *A, int64_t lda,
                                   int64_t a_cols, const int8_t *B, int64_t ldb, int64_t b_cols,
                                   int64_t b_xoff, int32_t *C, int64_t ldc, int *err) {
+    MFLAB_RANGE("mflab_int8_gemm_tn");
     if (!h || !A || !B || !C || !err) return MFLAB_ERR_ARG;
     if (engine != MFLAB_INT8_TCGEN05 && engine != MFLAB_INT8_LIBRARY &&
         engine != MFLAB_INT8_TCGEN05_PAIR)

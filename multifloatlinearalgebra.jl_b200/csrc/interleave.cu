@@ -207,6 +207,7 @@ int staged(mflab_handle *h, int N, int64_t m, int64_t n, double *host, int64_t l
 extern "C" int mflab_interleaved_to_planes(mflab_handle *h, void *stream, int limbs, int64_t m,
                                            int64_t n, const double *X, int64_t ldx, double *P,
                                            int64_t ld, int64_t ls) {
+    MFLAB_RANGE("mflab_interleaved_to_planes");
     bool empty;
     int rc = mfl::check_args(h, limbs, m, n, X, ldx, P, ld, ls, &empty);
     if (rc || empty) return rc;
@@ -216,6 +217,7 @@ extern "C" int mflab_interleaved_to_planes(mflab_handle *h, void *stream, int li
 extern "C" int mflab_planes_to_interleaved(mflab_handle *h, void *stream, int limbs, int64_t m,
                                            int64_t n, const double *P, int64_t ld, int64_t ls,
                                            double *X, int64_t ldx) {
+    MFLAB_RANGE("mflab_planes_to_interleaved");
     bool empty;
     int rc = mfl::check_args(h, limbs, m, n, X, ldx, P, ld, ls, &empty);
     if (rc || empty) return rc;
@@ -225,6 +227,7 @@ extern "C" int mflab_planes_to_interleaved(mflab_handle *h, void *stream, int li
 extern "C" int mflab_h2d_interleaved(mflab_handle *h, void *stream, int limbs, int64_t m, int64_t n,
                                      const double *host, int64_t ldh, double *P, int64_t ld,
                                      int64_t ls) {
+    MFLAB_RANGE("mflab_h2d_interleaved");
     bool empty;
     int rc = mfl::check_args(h, limbs, m, n, host, ldh, P, ld, ls, &empty);
     if (rc || empty) return rc;
@@ -234,6 +237,7 @@ extern "C" int mflab_h2d_interleaved(mflab_handle *h, void *stream, int limbs, i
 extern "C" int mflab_d2h_interleaved(mflab_handle *h, void *stream, int limbs, int64_t m, int64_t n,
                                      const double *P, int64_t ld, int64_t ls, double *host,
                                      int64_t ldh) {
+    MFLAB_RANGE("mflab_d2h_interleaved");
     bool empty;
     int rc = mfl::check_args(h, limbs, m, n, host, ldh, P, ld, ls, &empty);
     if (rc || empty) return rc;

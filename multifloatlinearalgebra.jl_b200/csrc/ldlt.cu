@@ -778,6 +778,7 @@ using mfl::Mat;
 extern "C" int mflab_sytrf(mflab_handle *h, void *stream, int limbs, int64_t n, double *A,
                            int64_t lda, int64_t lsa, double *dsub, int64_t lsd, int64_t *pivots,
                            uint8_t *blocks, int blocked, int64_t block, int *info) {
+    MFLAB_RANGE("mflab_sytrf");
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
     if (n < 0 || (n > 0 && (lda < n || !dsub || !pivots || !blocks || lsd < n)) || !info)
         return MFLAB_ERR_ARG;
@@ -796,6 +797,7 @@ extern "C" int mflab_sytrs(mflab_handle *h, void *stream, int limbs, int64_t n, 
                            const double *F, int64_t ldf, int64_t lsf, const double *dsub,
                            int64_t lsd, const int64_t *pivots, const uint8_t *blocks, double *B,
                            int64_t ldb, int64_t lsb, int *fail) {
+    MFLAB_RANGE("mflab_sytrs");
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
     if (n < 0 || nrhs < 0 || (n > 0 && (ldf < n || ldb < n)) || !fail) return MFLAB_ERR_ARG;
     if (n == 0 || nrhs == 0) return MFLAB_OK;
@@ -834,6 +836,7 @@ extern "C" int mflab_ldlt_diagnostics(mflab_handle *h, void *stream, int limbs, 
                                       const double *F, int64_t ldf, int64_t lsf,
                                       const double *dsub, int64_t lsd, const uint8_t *blocks,
                                       const double *omax, double *out) {
+    MFLAB_RANGE("mflab_ldlt_diagnostics");
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
     if (n < 0 || !out) return MFLAB_ERR_ARG;
     Mat f{(double *)F, ldf, lsf};

@@ -6,6 +6,8 @@
 
 #include <atomic>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/mflab200.h"
 
 namespace mfl {
@@ -38,6 +40,17 @@ int launch_trsm_info(int N, int side, int uplo, int trans, int diag, int64_t m, 
                      int order = 0);
 
 int record_cuda_error(cudaError_t e, const char *where);
+
+// An NVTX range named after the C entry point for the duration of the call,
+// so profiles (Nsight Systems timelines, ncu --nvtx filters) attribute the
+// kernels to the API call that issued them; a no-op without a tool attached.
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
+#define MFLAB_RANGE(name) ::mfl::NvtxRange mflab_nvtx_range_(name)
 
 // cudaFuncSetAttribute(MaxDynamicSharedMemorySize) of a kernel once per
 // device of the process (the attribute is per device); `done` is the

@@ -484,6 +484,7 @@ extern "C" int mflab_gemm_ozaki_route(mflab_handle *h, void *stream, int limbs, 
                                       int64_t lsa, const double *B, int64_t ldb, int64_t lsb,
                                       double *C, int64_t ldc, int64_t lsc, const double *alpha,
                                       const double *beta) {
+    MFLAB_RANGE("mflab_gemm_ozaki_route");
     // the modular route first; the slice route when the modulus table cannot
     // reach the tuned requirement
     const mfl::Mat Am{(double *)A, lda, lsa}, Bm{(double *)B, ldb, lsb}, Cm{C, ldc, lsc};
@@ -498,6 +499,7 @@ extern "C" int mflab_gemm_ozaki(mflab_handle *h, void *stream, int limbs, int sl
                                 int64_t n, int64_t k, const double *A, int64_t lda, int64_t lsa,
                                 const double *B, int64_t ldb, int64_t lsb, double *C, int64_t ldc,
                                 int64_t lsc, const double *alpha, const double *beta) {
+    MFLAB_RANGE("mflab_gemm_ozaki");
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
     if (m < 0 || n < 0 || k < 0 || !alpha || !beta) return MFLAB_ERR_ARG;
     if (m == 0 || n == 0) return MFLAB_OK;
@@ -532,6 +534,7 @@ extern "C" int mflab_gemm_ozaki_phases(mflab_handle *h, void *stream, int limbs,
                                        int64_t lsb, double *C, int64_t ldc, int64_t lsc,
                                        const double *alpha, const double *beta, float *ms,
                                        double *int8_ops) {
+    MFLAB_RANGE("mflab_gemm_ozaki_phases");
     if (!h || !ms || !int8_ops) return MFLAB_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     cudaEvent_t ev[5];
@@ -562,9 +565,24 @@ extern "C" int mflab_gemm_ozaki_phases(mflab_handle *h, void *stream, int limbs,
 // Device time of one int8 x int8 -> int32 TN GEMM (m x n x k) through the same
 // library path as the level products, after one warm-up call; *ms receives
 // the best of `reps` timed calls.  Uses the handle scratch.  Synchronises.
+namespace mfl {
+// uniformly distributed bytes from a counter hash (splitmix64 finaliser)
+__global__ void fill_random_bytes_kernel(uint64_t *p, size_t words, uint64_t seed) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < words;
+         i += (size_t)gridDim.x * blockDim.x) {
+        uint64_t z = seed + (i + 1) * 0x9E3779B97F4A7C15ULL;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+        p[i] = z ^ (z >> 31);
+    }
+}
+}  // namespace mfl
+
 extern "C" int mflab_probe_int8_gemm(mflab_handle *h, void *stream, int64_t m, int64_t n,
-                                     int64_t k, int reps, float *ms) {
+                                     int64_t k, int reps, int fill, float *ms) {
+    MFLAB_RANGE("mflab_probe_int8_gemm");
     if (!h || !ms || m <= 0 || n <= 0 || k <= 0 || reps <= 0) return MFLAB_ERR_ARG;
+    if (fill != 0 && fill != 1) return MFLAB_ERR_FLAG;
     const int64_t kp = (k + 15) / 16 * 16, ldi = (m + 15) / 16 * 16;
     const size_t a = (size_t)m * kp, b = (size_t)n * kp, c = (size_t)ldi * n * 4, ws = 64 << 20;
     int rc = mflab_reserve_scratch(h, a + b + c + ws + 1024);
@@ -574,8 +592,13 @@ extern "C" int mflab_probe_int8_gemm(mflab_handle *h, void *stream, int64_t m, i
     int32_t *I = (int32_t *)(base + (a + 255) / 256 * 256 + (b + 255) / 256 * 256);
     char *wsp = (char *)I + (c + 255) / 256 * 256;
     cudaStream_t s = (cudaStream_t)stream;
-    cudaMemsetAsync(A8, 0x11, a, s);
-    cudaMemsetAsync(B8, 0x23, b, s);
+    if (fill == 0) {
+        cudaMemsetAsync(A8, 0x11, a, s);
+        cudaMemsetAsync(B8, 0x23, b, s);
+    } else {  // the operand bytes of the INT8 routes are close to uniform
+        mfl::fill_random_bytes_kernel<<<1184, 256, 0, s>>>((uint64_t *)A8, a / 8, 1);
+        mfl::fill_random_bytes_kernel<<<1184, 256, 0, s>>>((uint64_t *)B8, b / 8, 2);
+    }
     rc = mfl::int8_gemm_tn(m, n, kp, A8, kp, B8, kp, I, ldi, wsp, ws, s);
     if (rc) return rc;
     cudaEvent_t e0, e1;

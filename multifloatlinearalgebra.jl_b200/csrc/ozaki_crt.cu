@@ -932,6 +932,7 @@ extern "C" int mflab_gemm_ozaki_crt(mflab_handle *h, void *stream, int limbs, in
                                     int64_t lsa, const double *B, int64_t ldb, int64_t lsb,
                                     double *C, int64_t ldc, int64_t lsc, const double *alpha,
                                     const double *beta) {
+    MFLAB_RANGE("mflab_gemm_ozaki_crt");
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
     if (m < 0 || n < 0 || k < 0 || !alpha || !beta) return MFLAB_ERR_ARG;
     if (m == 0 || n == 0) return MFLAB_OK;
@@ -958,6 +959,7 @@ extern "C" int mflab_syrk_lower_ozaki(mflab_handle *h, void *stream, int limbs, 
                                       int trans, int64_t n, int64_t k, const double *A,
                                       int64_t lda, int64_t lsa, double *C, int64_t ldc,
                                       int64_t lsc, const double *alpha, const double *beta) {
+    MFLAB_RANGE("mflab_syrk_lower_ozaki");
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
     if (trans != 0 && trans != 1) return MFLAB_ERR_FLAG;
     if (n < 0 || k < 0 || !alpha || !beta || moduli < 0) return MFLAB_ERR_ARG;
@@ -1036,6 +1038,7 @@ extern "C" int mflab_gemm_ozaki_crt_phases(mflab_handle *h, void *stream, int li
                                            int64_t ldb, int64_t lsb, double *C, int64_t ldc,
                                            int64_t lsc, const double *alpha, const double *beta,
                                            float *ms, double *int8_ops) {
+    MFLAB_RANGE("mflab_gemm_ozaki_crt_phases");
     if (!h || !ms || !int8_ops) return MFLAB_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     cudaEvent_t ev[5];

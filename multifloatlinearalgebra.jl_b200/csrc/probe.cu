@@ -37,6 +37,7 @@ __global__ void fp64_probe_kernel(int64_t iters, double seed, double *out) {
 // hold blocks*threads doubles on the device.  Timing is the caller's.
 extern "C" int mflab_probe_fp64(void *stream, int kind, int blocks, int threads, int64_t iters,
                                 double *out, double *instructions) {
+    MFLAB_RANGE("mflab_probe_fp64");
     if (blocks <= 0 || threads <= 0 || threads > 1024 || iters <= 0 || !out || !instructions)
         return MFLAB_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;

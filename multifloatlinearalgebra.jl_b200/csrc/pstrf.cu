@@ -248,6 +248,7 @@ using mfl::Mat;
 extern "C" int mflab_pstrf(mflab_handle *h, void *stream, int limbs, int64_t n, double *A,
                            int64_t lda, int64_t lsa, const double *tol, int64_t *perm,
                            int64_t *rank_info) {
+    MFLAB_RANGE("mflab_pstrf");
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
     if (n < 0 || !tol || !perm || !rank_info) return MFLAB_ERR_ARG;
     for (int l = 0; l < limbs; ++l)

@@ -771,6 +771,7 @@ using mfl::Mat;
 extern "C" int mflab_qr(mflab_handle *h, void *stream, int limbs, int pivoted, int64_t m,
                         int64_t n, double *A, int64_t lda, int64_t lsa, double *tau, int64_t lst,
                         int64_t *perm, int *info) {
+    MFLAB_RANGE("mflab_qr");
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
     if (pivoted & ~1) return MFLAB_ERR_FLAG;
     if (m < 0 || n < 0 || !tau || !perm || !info) return MFLAB_ERR_ARG;
@@ -789,6 +790,7 @@ extern "C" int mflab_apply_q(mflab_handle *h, void *stream, int limbs, int trans
                              int64_t r, const double *F, int64_t ldf, int64_t lsf,
                              const double *tau, int64_t lst, double *D, int64_t ldd, int64_t lsd,
                              int64_t nd) {
+    MFLAB_RANGE("mflab_apply_q");
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
     if (trans & ~1) return MFLAB_ERR_FLAG;
     if (m < 0 || r < 0 || nd < 0 || r > m) return MFLAB_ERR_ARG;
@@ -810,6 +812,7 @@ extern "C" int mflab_apply_q(mflab_handle *h, void *stream, int limbs, int trans
 extern "C" int mflab_qr_numerical_rank(mflab_handle *h, void *stream, int limbs, int64_t m,
                                        int64_t n, const double *F, int64_t ldf, int64_t lsf,
                                        const double *atol, const double *rtol, int64_t *rank) {
+    MFLAB_RANGE("mflab_qr_numerical_rank");
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
     if (m < 0 || n < 0 || !atol || !rtol || !rank) return MFLAB_ERR_ARG;
     const int64_t r = m < n ? m : n;

@@ -218,6 +218,7 @@ extern "C" int mflab_residual(mflab_handle *h, void *stream, int limbs, int uplo
                               int64_t lsa, const double *X, int64_t ldx, int64_t lsx,
                               const double *B, int64_t ldb, int64_t lsb, double *R, int64_t ldr,
                               int64_t lsr) {
+    MFLAB_RANGE("mflab_residual");
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
     if (uplo < 0 || uplo > 2) return MFLAB_ERR_FLAG;
     if (m < 0 || k < 0 || nrhs < 0) return MFLAB_ERR_ARG;
@@ -243,6 +244,7 @@ extern "C" int mflab_residual_mixed(mflab_handle *h, void *stream, int src_limbs
                                     int64_t lda, int64_t lsa, const double *X, int64_t ldx,
                                     int64_t lsx, const double *B, int64_t ldb, int64_t lsb,
                                     double *R, int64_t ldr, int64_t lsr) {
+    MFLAB_RANGE("mflab_residual_mixed");
     if (!h) return MFLAB_ERR_UNSUPPORTED;
     if (!(src_limbs >= 1 && src_limbs < res_limbs && res_limbs <= 4 && res_limbs >= 2))
         return MFLAB_ERR_UNSUPPORTED;
@@ -273,6 +275,7 @@ extern "C" int mflab_backward_error(mflab_handle *h, void *stream, int limbs, in
                                     int64_t lsa, const double *X, int64_t ldx, int64_t lsx,
                                     const double *B, int64_t ldb, int64_t lsb, const double *R,
                                     int64_t ldr, int64_t lsr, double *out) {
+    MFLAB_RANGE("mflab_backward_error");
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
     if (uplo < 0 || uplo > 2) return MFLAB_ERR_FLAG;
     if (m < 0 || k < 0 || nrhs < 0 || !out) return MFLAB_ERR_ARG;
@@ -323,6 +326,7 @@ extern "C" int mflab_backward_error(mflab_handle *h, void *stream, int limbs, in
 extern "C" int mflab_opnorm_inf(mflab_handle *h, void *stream, int limbs, int uplo, int64_t m,
                                 int64_t k, const double *A, int64_t lda, int64_t lsa,
                                 double *anorm, int *nonfinite) {
+    MFLAB_RANGE("mflab_opnorm_inf");
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
     if (uplo < 0 || uplo > 2) return MFLAB_ERR_FLAG;
     if (m < 0 || k < 0 || !anorm || !nonfinite) return MFLAB_ERR_ARG;
@@ -362,6 +366,7 @@ extern "C" int mflab_backward_error_norm(mflab_handle *h, void *stream, int limb
                                          const int *nonfinite, const double *X, int64_t ldx,
                                          int64_t lsx, const double *B, int64_t ldb, int64_t lsb,
                                          const double *R, int64_t ldr, int64_t lsr, double *out) {
+    MFLAB_RANGE("mflab_backward_error_norm");
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
     if (m < 0 || k < 0 || nrhs < 0 || !out || !anorm || !nonfinite) return MFLAB_ERR_ARG;
     if (nrhs == 0) return MFLAB_OK;
@@ -399,6 +404,7 @@ __global__ void add_widened_kernel(int64_t m, int64_t n, Mat D, Mat X) {
 extern "C" int mflab_add_widened(mflab_handle *h, void *stream, int src_limbs, int dst_limbs,
                                  int64_t m, int64_t n, const double *D, int64_t ldd, int64_t lsd,
                                  double *X, int64_t ldx, int64_t lsx) {
+    MFLAB_RANGE("mflab_add_widened");
     if (!h) return MFLAB_ERR_UNSUPPORTED;
     if (m < 0 || n < 0) return MFLAB_ERR_ARG;
     if (m == 0 || n == 0) return MFLAB_OK;

@@ -306,6 +306,7 @@ int launch_trsm(int N, int side, int uplo, int trans, int diag, int64_t m, int64
 extern "C" int mflab_trsm(mflab_handle *h, void *stream, int limbs, int side, int uplo, int trans,
                           int diag, int64_t m, int64_t n, const double *A, int64_t lda,
                           int64_t lsa, double *B, int64_t ldb, int64_t lsb, const double *alpha) {
+    MFLAB_RANGE("mflab_trsm");
     if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
     if (side < 0 || side > 1 || uplo < 0 || uplo > 1 || trans < 0 || trans > 1 || diag < 0 ||
         diag > 1)
