@@ -55,6 +55,10 @@ def parse():
                    help="skip the factorization / mixed-LU / batched-SPD workloads")
     p.add_argument("--config-reps", type=int, default=3,
                    help="timed repeats (after one warm-up) of each of those workloads")
+    p.add_argument("--split", default="replicas", choices=["replicas", "tiles"],
+                   help="replicas: one independent problem per rank (weak scaling); tiles: "
+                        "one problem held by rank 0, its 2-D output tiles computed by all "
+                        "ranks (panels scattered, tiles gathered; strong scaling)")
     return p.parse_args()
 
 
@@ -701,6 +705,43 @@ def run_configs(R, torch, peak, reps=3):
             "batched_spd_10000_x2": config_batched(R, torch, peak, reps)}
 
 
+def run_tiles(args, R, torch, dist, world, rank):
+    """One n x n x n Float64xN GEMM whose operands live on rank 0, split into
+    2-D output tiles over all ranks (sharding.gemm_sharded_: panels scattered
+    from rank 0, tiles gathered back): the timed step includes both
+    transfers.  Strong scaling: the total work is fixed."""
+    mf = R.mf
+    N, n = args.limbs, args.n
+    cfg = R.cfg("modular", args.knob or 30) if args.route != "plain" else mf.KernelConfig()
+    A = B = C = None
+    if rank == 0:
+        A, B = R.operands(N, n)
+        C = mf.MFMatrix.zeros(N, n, n)
+    step = lambda: R.sharding.gemm_sharded_(C.storage if rank == 0 else None,
+                                            A.storage if rank == 0 else None,
+                                            B.storage if rank == 0 else None, config=cfg)
+    clocks = NvmlClockSampler(R.local)
+    clocks.start()
+    t = R.timed(step, args.steps, args.warmup) / args.steps
+    clk = clocks.stop()
+    line = {
+        "metric": METRIC, "value": 2.0 * n ** 3 / t / 1e9, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded randn * 2^U(-20,20), lower limbs randn*2^-53*|prev|)",
+        "config": {"workload": f"Float64x{N} GEMM m=n=k={n}", "limbs": N, "n": n,
+                   "route": "plain" if args.route == "plain" else "ozaki",
+                   "moduli": None if args.route == "plain" else (args.knob or 30),
+                   "parallelism": f"tiles{world}",
+                   "l2": "inputs larger than L2 (each operand >= 1 GiB)"},
+        "clocks": clk,
+        "note": "rank 0 holds A, B and C; each step scatters the row panels of A and column "
+                "panels of B, multiplies one 2-D tile per rank and gathers the tiles to rank 0",
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -717,6 +758,11 @@ def main():
                                 device_id=torch.device("cuda", local))
     R = Runner(args, torch, dist, world, rank, local)
     mf = R.mf
+    if args.split == "tiles":
+        run_tiles(args, R, torch, dist, world, rank)
+        if world > 1:
+            dist.destroy_process_group()
+        return
     N, n = args.limbs, args.n
     route = args.route
     if route == "auto":

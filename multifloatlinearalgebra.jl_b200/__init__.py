@@ -40,7 +40,7 @@ __all__ = [
     "MFCholesky", "MFLU", "capabilities", "limb_type_name",
     "ldlt_", "ldlt_plan", "MFLDLT", "factor_blocks", "factor_permutation", "factor_inertia",
     "residual_", "residual_mixed_", "normwise_backward_error", "refinement_correction_",
-    "solve_mixed_lu", "batched",
+    "solve_mixed_lu", "batched", "tuning", "create_handle", "destroy_handle",
 ]
 
 
@@ -1672,3 +1672,4 @@ def capabilities(N: int) -> dict:
 
 
 from . import batched  # noqa: E402  (batched SPD factor/solve and its adjoint)
+from . import tuning  # noqa: E402  (persisted device tuning profiles)

@@ -109,14 +109,22 @@ def _signature(batch: SPDBatch, block: int) -> tuple:
 
 
 def autotune(batch: SPDBatch, block: int = 16, candidates: Optional[Sequence] = None,
-             reps: int = 2) -> dict:
+             reps: int = 2, profile=None) -> dict:
     """Launch shape of the batched factor + solve for this batch: the CTA size
     (128, 256 or 512 threads) and the number of persistent CTAs (1, 2, 4 or 8
     per SM), picked by timing the real launch on the batch's own blocks
     (restored afterwards).  Neither knob changes any result (each block's
     arithmetic is per element in the reference order), so the choice is free.
-    Cached per (limbs, block, size signature of the batch).
+    Cached per (limbs, block, size signature of the batch); a tuning
+    profile (tuning.TuneProfile, fingerprint checked) that holds this
+    signature supplies the shape without any timing.
     Returns {"threads", "grid", "ms", "timings"}."""
+    if profile is not None:
+        from .tuning import stored_batched_shape
+        got = stored_batched_shape(profile, batch.N, block, batch.sizes_host)
+        if got is not None:
+            return {"threads": got["threads"], "grid": got["grid"], "ms": got["ms"],
+                    "timings": {}, "source": "profile"}
     key = _signature(batch, block)
     if key in _TUNED:
         return _TUNED[key]

@@ -1,12 +1,14 @@
 """Multi-rank plumbing for the paths that shard (one process per GPU).
 
 No reference counterpart: MultiFloatLinearAlgebra.jl runs in one process.
-Two paths split into independent work without a data-path collective:
+Two paths split into independent work:
 
 * GEMM: C = A*B splits into 2-D output tiles; rank r multiplies its row panel
   of A by its column panel of B (matched order is preserved: no k split, so
-  every entry is the same ascending-k chain as on one GPU).  Independent
-  problems (one per rank, the weak-scaling benchmark) need no split at all.
+  every entry is the same ascending-k chain as on one GPU).  With the
+  operands on one rank (gemm_sharded_), the panels are scattered from it and
+  the tiles gathered back to it; independent problems (one per rank, the
+  weak-scaling benchmark) need no split and no collective at all.
 * batched SPD solve: the blocks are dealt to ranks by cost (n^3/3 + 2 n^2,
   longest first onto the least loaded rank).
 
@@ -173,3 +175,91 @@ def solve_spd_sharded(sizes: Sequence[int], solve_blocks: Callable[[np.ndarray],
             out[i] = flat[:, o:o + ni].copy()
             o += ni
     return out
+
+
+def gemm_sharded_(C, A, B, alpha=1.0, beta=0.0, config=None, group=None, root: int = 0,
+                  multiply: Optional[Callable] = None):
+    """C = alpha A B + beta C over the ranks of `group`, with the operands
+    resident on `root` as limb-plane tensors (the storage of an MFMatrix:
+    A (N, k, m), B (N, n, k), C (N, n, m), column-major planes); the other
+    ranks pass None for A, B and C.
+
+    1. The shapes are broadcast from root; the row panel of A and the column
+       panel of B of every rank's 2-D output tile (gemm_tile) are scattered
+       from root, zero-padded to one size (one scatter collective each, over
+       NCCL on GPUs: the transfers are plain device buffers, no kernel reads
+       another GPU's memory); with beta != 0 the C tiles are scattered too.
+    2. Every rank multiplies its tile: multiply(Ap, Bp, Ct) with the panels
+       and the tile as views of the padded buffers (MFMatrix objects on a
+       GPU; by default gemm_(Ct, Ap, Bp, alpha, beta, config), so each entry
+       is the same ascending-k chain as on one GPU: no k split, the matched
+       order is kept).  CPU tests pass the oracle instead.
+    3. The tiles are gathered to root and written into C.
+
+    Returns C on root, None on the other ranks."""
+    world, rank = _world(group)
+    dev = _device(group)
+    if rank == root:
+        N, k, m = (int(x) for x in A.shape)
+        n = int(B.shape[1])
+        if B.shape[0] != N or B.shape[2] != k or tuple(C.shape) != (N, n, m):
+            raise ValueError("gemm_sharded_: operand shapes differ")
+        hdr = torch.tensor([N, m, k, n, int(beta != 0)], dtype=torch.int64, device=dev)
+    else:
+        hdr = torch.zeros(5, dtype=torch.int64, device=dev)
+    if world > 1:
+        dist.broadcast(hdr, root, group=group)
+    N, m, k, n, use_beta = (int(x) for x in hdr.tolist())
+    pr, pc = tile_grid(world)
+    rmax, cmax = max(-(-m // pr), 1), max(-(-n // pc), 1)
+    tiles = [gemm_tile(m, n, world, r) for r in range(world)]
+    f64 = torch.float64
+
+    def scatter(make_part, shape):
+        mine = torch.zeros(shape, dtype=f64, device=dev)
+        parts = None
+        if rank == root:
+            parts = []
+            for r in range(world):
+                buf = torch.zeros(shape, dtype=f64, device=dev)
+                make_part(buf, *tiles[r])
+                parts.append(buf)
+        if world > 1:
+            dist.scatter(mine, parts, src=root, group=group)
+        else:
+            mine.copy_(parts[0])
+        return mine
+
+    def a_part(buf, rs, cs):
+        buf[:, :, :rs.stop - rs.start] = A[:, :, rs]
+
+    def b_part(buf, rs, cs):
+        buf[:, :cs.stop - cs.start, :] = B[:, cs, :]
+
+    def c_part(buf, rs, cs):
+        buf[:, :cs.stop - cs.start, :rs.stop - rs.start] = C[:, cs, rs]
+
+    a_mine = scatter(a_part, (N, max(k, 1), rmax))
+    b_mine = scatter(b_part, (N, cmax, max(k, 1)))
+    c_mine = scatter(c_part, (N, cmax, rmax)) if use_beta else \
+        torch.zeros((N, cmax, rmax), dtype=f64, device=dev)
+    rs, cs = tiles[rank]
+    rows, cols = rs.stop - rs.start, cs.stop - cs.start
+    if multiply is None:
+        from . import KernelConfig, MFMatrix, gemm_
+        Ap = MFMatrix(a_mine, 0, 0, rows, k)
+        Bp = MFMatrix(b_mine, 0, 0, k, cols)
+        Ct = MFMatrix(c_mine, 0, 0, rows, cols)
+        gemm_(Ct, Ap, Bp, alpha, beta, config=config if config is not None else KernelConfig())
+    else:
+        multiply(a_mine[:, :k, :rows], b_mine[:, :cols, :k], c_mine[:, :cols, :rows])
+    parts = [torch.zeros_like(c_mine) for _ in range(world)] if rank == root else None
+    if world > 1:
+        dist.gather(c_mine, parts, dst=root, group=group)
+    else:
+        parts[0].copy_(c_mine)
+    if rank != root:
+        return None
+    for r, (rs_r, cs_r) in enumerate(tiles):
+        C[:, cs_r, rs_r] = parts[r][:, :cs_r.stop - cs_r.start, :rs_r.stop - rs_r.start]
+    return C

@@ -60,6 +60,23 @@ def _worker(rank, world, port, outdir):
 
         res["spd"] = sharding.solve_spd_sharded(sizes, solve)
         res["mine"] = seen
+        # the device data path of the GEMM split: operands on rank 0 as limb
+        # planes, panels scattered, tiles gathered back (oracle as multiply)
+        planes = lambda X: torch.from_numpy(np.ascontiguousarray(X.transpose(0, 2, 1)))
+        rng = np.random.default_rng(5)
+        A2, B2 = syn.randn_mf(rng, 2, 41, 30, spread=6), syn.randn_mf(rng, 2, 30, 26, spread=6)
+        C0 = syn.randn_mf(rng, 2, 41, 26)
+        for beta in (0.0, 1.0):
+            def mult(a, b, c, beta=beta):
+                lm = lambda t: np.ascontiguousarray(t.permute(0, 2, 1).numpy())
+                got = mfref.gemm(lm(a), lm(b), lm(c), 1.0, beta, nthreads=1)
+                c.copy_(torch.from_numpy(np.ascontiguousarray(got.transpose(0, 2, 1))))
+            Cp = planes(C0).clone() if rank == 0 else None
+            out = sharding.gemm_sharded_(Cp, planes(A2) if rank == 0 else None,
+                                         planes(B2) if rank == 0 else None, 1.0, beta,
+                                         multiply=mult)
+            res[f"gemm_dev_beta{int(beta)}"] = None if out is None else \
+                np.ascontiguousarray(out.numpy().transpose(0, 2, 1))
         np.save(os.path.join(outdir, f"rank{rank}.npy"), np.array(res, dtype=object),
                 allow_pickle=True)
     finally:
@@ -123,5 +140,12 @@ def test_two_gloo_ranks_match_one_process(mf, ref, tmp_path):
         assert np.array_equal(res[r]["gemm"].view(np.uint64), C.view(np.uint64))
         for i in range(len(sizes)):
             assert np.array_equal(res[r]["spd"][i].view(np.uint64), xs[i].view(np.uint64))
+    rng = np.random.default_rng(5)
+    A2, B2 = syn.randn_mf(rng, 2, 41, 30, spread=6), syn.randn_mf(rng, 2, 30, 26, spread=6)
+    C0 = syn.randn_mf(rng, 2, 41, 26)
+    for beta in (0, 1):
+        want = ref.gemm(A2, B2, C0.copy(), 1.0, float(beta), nthreads=1)
+        assert np.array_equal(res[0][f"gemm_dev_beta{beta}"].view(np.uint64), want.view(np.uint64))
+        assert res[1][f"gemm_dev_beta{beta}"] is None
     # every block was solved by exactly one rank
     assert sorted(res[0]["mine"] + res[1]["mine"]) == list(range(len(sizes)))
