@@ -169,6 +169,23 @@ int mflab_gemm_ozaki_crt(mflab_handle *h, void *stream, int limbs, int moduli, i
                          const double *B, int64_t ldb, int64_t lsb, double *C, int64_t ldc,
                          int64_t lsc, const double *alpha, const double *beta);
 
+/* A prepared left operand of the modular INT8 route, for many products
+   C = alpha A B + beta C with one A (the residuals B - A X of iterative
+   refinement): mflab_ozaki_crt_prepare stores A's row exponents and residue
+   planes for `moduli` (1..49, fixed; else MFLAB_ERR_FLAG) in `prep`, caller-owned device memory of
+   mflab_ozaki_crt_prepare_bytes(limbs, moduli, m, k) bytes; A is not read
+   again.  mflab_gemm_ozaki_crt_prepared then splits only B and runs the same
+   int8 GEMMs and reconstruction as mflab_gemm_ozaki_crt(moduli), with the
+   same result bit for bit; limbs, moduli, m and k must be those of the
+   preparation.  k >= 1.  No reference counterpart. */
+int mflab_ozaki_crt_prepare_bytes(int limbs, int moduli, int64_t m, int64_t k, size_t *bytes);
+int mflab_ozaki_crt_prepare(mflab_handle *h, void *stream, int limbs, int moduli, int64_t m,
+                            int64_t k, const double *A, int64_t lda, int64_t lsa, void *prep);
+int mflab_gemm_ozaki_crt_prepared(mflab_handle *h, void *stream, int limbs, int moduli, int64_t m,
+                                  int64_t n, int64_t k, const void *prep, const double *B,
+                                  int64_t ldb, int64_t lsb, double *C, int64_t ldc, int64_t lsc,
+                                  const double *alpha, const double *beta);
+
 /* lower(C) = alpha * op(A) * op(A)^T + beta * lower(C) through the modular
    INT8 route (the SYRK / trailing-update form of mflab_gemm_ozaki_crt):
    trans = 1 takes A as k x n and forms A^T A (the syrk!(C, P, alpha, beta)
@@ -408,6 +425,20 @@ int mflab_getrf(mflab_handle *h, void *stream, int limbs, int64_t m, int64_t n, 
 int mflab_getrs(mflab_handle *h, void *stream, int limbs, int64_t n, int64_t nrhs,
                 const double *LU, int64_t ldl, int64_t lsl, const int64_t *ipiv, double *B,
                 int64_t ldb, int64_t lsb);
+
+/* Repeated solves with one binary64 LU factor (the correction solves of the
+   mixed-precision LU solver; no reference counterpart).  After mflab_getrf
+   (limbs = 1), mflab_lu64_prepare stores in `work` (mflab_lu64_work_bytes(n)
+   bytes of device memory, owned by the caller) the row permutation of ipiv
+   and the inverses of the 128 x 128 diagonal blocks of L and U;
+   mflab_lu64_solve then overwrites B (n x nrhs binary64, column-major) with
+   inv(A) B: one gather and one kernel per block row and direction.  Results
+   differ from mflab_getrs in rounding only.  n <= 24576. */
+int mflab_lu64_work_bytes(int64_t n, size_t *bytes);
+int mflab_lu64_prepare(mflab_handle *h, void *stream, int64_t n, const double *LU, int64_t ldl,
+                       const int64_t *ipiv, void *work);
+int mflab_lu64_solve(mflab_handle *h, void *stream, int64_t n, int64_t nrhs, const double *LU,
+                     int64_t ldl, const void *work, double *B, int64_t ldb);
 
 /* Bunch-Kaufman LDL^T in place (lower triangle authoritative on input; the
    upper triangle is overwritten by the working mirror).  dsub (device,

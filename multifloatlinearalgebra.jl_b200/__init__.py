@@ -41,6 +41,7 @@ __all__ = [
     "ldlt_", "ldlt_plan", "MFLDLT", "factor_blocks", "factor_permutation", "factor_inertia",
     "residual_", "residual_mixed_", "normwise_backward_error", "refinement_correction_",
     "solve_mixed_lu", "batched", "tuning", "create_handle", "destroy_handle",
+    "PreparedInt8Operand", "gemm_prepared_",
 ]
 
 
@@ -541,6 +542,50 @@ def ozaki_last_moduli(device: Optional[int] = None) -> int:
     """Modulus count chosen by the last modular INT8 GEMM issued from this thread."""
     dev = torch.cuda.current_device() if device is None else device
     return int(_native.load().mflab_ozaki_last_moduli(_handle(dev)))
+
+
+class PreparedInt8Operand:
+    """A Float64xN matrix prepared once as the left operand of many modular
+    INT8 products with a fixed modulus count (mflab_ozaki_crt_prepare): its
+    row scales and residue planes live in a device buffer of this object.
+    gemm_prepared_(C, P, B) equals gemm_(C, A, B) with ozaki_moduli =
+    P.moduli, bit for bit, without reading or splitting A again."""
+
+    def __init__(self, A: MFMatrix, moduli: int):
+        N = _same_type(A)
+        if A.n < 1:
+            raise DimensionMismatch("a prepared operand needs at least one column")
+        nbytes = C.c_size_t()
+        lib, h, s = _lib_h(A)
+        _check(lib.mflab_ozaki_crt_prepare_bytes(N, int(moduli), A.m, A.n, C.byref(nbytes)),
+               "ozaki prepare")
+        self.N, self.m, self.k, self.moduli = N, A.m, A.n, int(moduli)
+        self.device = A.device
+        self.buffer = torch.empty(max(nbytes.value, 1), dtype=torch.uint8,
+                                  device=A.storage.device)
+        _check(lib.mflab_ozaki_crt_prepare(h, s, N, self.moduli, A.m, A.n, A.ptr(), A.ld, A.ls,
+                                           self.buffer.data_ptr()), "ozaki prepare")
+
+
+def gemm_prepared_(C_: MFMatrix, P: PreparedInt8Operand, B: MFMatrix, alpha=1.0, beta=0.0,
+                   config: KernelConfig = _DEFAULT) -> MFMatrix:
+    """C = alpha*A*B + beta*C with A prepared (PreparedInt8Operand) on the
+    modular INT8 route."""
+    N = _same_type(C_, B)
+    if N != P.N or C_.device != P.device:
+        raise ArgumentError("prepared operand of another type or device")
+    if B.m != P.k:
+        raise DimensionMismatch("gemm! inner dimensions differ")
+    if (C_.m, C_.n) != (P.m, B.n):
+        raise DimensionMismatch("gemm! output dimensions differ")
+    _no_alias("gemm!", C_, B)
+    lib, h, s = _lib_h(C_)
+    _check(lib.mflab_set_int8_engine(h, _int8_engine(config)), "gemm!")
+    _check(lib.mflab_gemm_ozaki_crt_prepared(h, s, N, P.moduli, P.m, B.n, P.k,
+                                             P.buffer.data_ptr(), B.ptr(), B.ld, B.ls, C_.ptr(),
+                                             C_.ld, C_.ls, _scalar(N, alpha), _scalar(N, beta)),
+           "gemm!")
+    return C_
 
 
 def ozaki_default_slices(N: int, k: int) -> int:
@@ -1563,10 +1608,10 @@ def _leading_limb(X: MFMatrix) -> MFMatrix:
     return MFMatrix(st, 0, 0, X.m, X.n, X.is_vector)
 
 
-# panel width of the binary64 factor of solve_mixed_lu: its single-CTA panel
-# streams the panel through one SM, so narrow panels win (n = 4096 on B200:
-# 46 ms at 12, 50 ms at 16, 73 ms at 32)
-_LU64_PANEL = 12
+# panel width of the binary64 factor of solve_mixed_lu: the panel lives in
+# the shared memory of an 8-CTA cluster, one cluster barrier per column, so
+# wide panels (fewer trailing updates) win
+_LU64_PANEL = 32
 
 
 def solve_mixed_lu(A: MFMatrix, B: MFMatrix, tol: float = 0.0, maxiter: int = 40,
@@ -1575,7 +1620,8 @@ def solve_mixed_lu(A: MFMatrix, B: MFMatrix, tol: float = 0.0, maxiter: int = 40
     """Solve A X = B for a Float64xN matrix A with a binary64 partial-pivoting
     LU of round(A) and iterative refinement with Float64xN residuals.
 
-    Each iteration: D = LU64 \\ round(R) in binary64 (getrs), X += D in
+    Each iteration: D = LU64 \\ round(R) in binary64 (the factor's
+    permutation and inverted diagonal blocks, prepared once), X += D in
     Float64xN, R = B - A X in Float64xN, then the normwise backward error of
     every column (||A||_inf computed once).  The residual goes through the
     INT8 modular GEMM (residual="int8", error at the Float64xN level of the
@@ -1613,22 +1659,37 @@ def solve_mixed_lu(A: MFMatrix, B: MFMatrix, tol: float = 0.0, maxiter: int = 40
         raise DomainError("lu!: input matrix contains non-finite entries")
     if st > 0:
         raise SingularException(st)
+    # the permutation and the inverted 128 x 128 diagonal blocks, once for all
+    # correction solves
+    wb = C.c_size_t()
+    _check(lib.mflab_lu64_work_bytes(n, C.byref(wb)), "lu64 workspace")
+    work = torch.empty(max(wb.value, 1), dtype=torch.uint8, device=dev)
+    _check(lib.mflab_lu64_prepare(h, s, n, LU.ptr(), LU.ld, ipiv.data_ptr(), work.data_ptr()),
+           "lu64 prepare")
     X = MFMatrix.zeros(N, n, None if B.is_vector else B.n, device=dev)
     R = B.copy()
+    D = MFMatrix.empty(1, n, None if B.is_vector else B.n, device=dev)
     anorm = OpNormInf(A)
     rcfg = dataclasses.replace(config, gemm_strategy="ozaki", ozaki_scheme="modular",
                                ozaki_slices=0)
     history = []
     it = 0
+    prepared = None
     for it in range(1, maxiter + 1):
-        D = _leading_limb(R)
-        _check(lib.mflab_getrs(h, s, 1, n, D.n, LU.ptr(), LU.ld, LU.ls, ipiv.data_ptr(), D.ptr(),
-                               D.ld, D.ls), "ldiv! (binary64)")
+        D.planes().copy_(R.planes()[0:1])  # round(R): the leading limbs
+        _check(lib.mflab_lu64_solve(h, s, n, D.n, LU.ptr(), LU.ld, work.data_ptr(), D.ptr(),
+                                    D.ld), "ldiv! (binary64)")
         _check(lib.mflab_add_widened(h, s, 1, N, n, X.n, D.ptr(), D.ld, D.ls, X.ptr(), X.ld,
                                      X.ls), "refinement update")
         if residual == "int8":
             R.copy_(B)
-            gemm_(R, A, X, -1.0, 1.0, config=rcfg)
+            if prepared is None:
+                # the first residual tunes the modulus count; A is then
+                # prepared once for the later ones
+                gemm_(R, A, X, -1.0, 1.0, config=rcfg)
+                prepared = PreparedInt8Operand(A, ozaki_last_moduli(A.device))
+            else:
+                gemm_prepared_(R, prepared, X, -1.0, 1.0, config=rcfg)
         else:
             residual_(R, A, X, B)
         be = normwise_backward_error(A, X, B, R, anorm=anorm)

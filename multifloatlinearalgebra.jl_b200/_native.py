@@ -169,6 +169,13 @@ SIGNATURES = {
                                 _i64, _vp, _i64, _i64, _d, _d, C.POINTER(C.c_float), _d],
     "mflab_probe_int8_gemm": [_vp, _vp, _i64, _i64, _i64, _int, _int, C.POINTER(C.c_float)],
     "mflab_set_tc_debug": [_vp, _i64, _int],
+    "mflab_ozaki_crt_prepare_bytes": [_int, _int, _i64, _i64, C.POINTER(C.c_size_t)],
+    "mflab_ozaki_crt_prepare": [_vp, _vp, _int, _int, _i64, _i64, _vp, _i64, _i64, _vp],
+    "mflab_gemm_ozaki_crt_prepared": [_vp, _vp, _int, _int, _i64, _i64, _i64, _vp, _vp, _i64,
+                                      _i64, _vp, _i64, _i64, _d, _d],
+    "mflab_lu64_work_bytes": [_i64, C.POINTER(C.c_size_t)],
+    "mflab_lu64_prepare": [_vp, _vp, _i64, _vp, _i64, _vp, _vp],
+    "mflab_lu64_solve": [_vp, _vp, _i64, _i64, _vp, _i64, _vp, _vp, _i64],
     "mflab_malloc": [_int, C.c_size_t, C.POINTER(_vp)],
     "mflab_free": [_vp],
     "mflab_memcpy": [_vp, _vp, C.c_size_t, _int, _vp],

@@ -11,6 +11,8 @@
 // Every kernel reads the device `info` word first and exits if an earlier step
 // failed, so a whole factorization is enqueued without host synchronisation.
 #include "mf_device.cuh"
+#include <algorithm>
+
 #include "mflab_internal.h"
 
 namespace mfl {
@@ -352,30 +354,332 @@ __global__ void __launch_bounds__(LU64_NT)
     }
 }
 
-// the interchanges ipiv[k0 .. k0+w) (1-based) applied, in ascending order, to
-// the columns outside the panel [k0, k0+w): one thread per column
-__global__ void lu64_swap_kernel(int64_t n, Mat A, int64_t k0, int w, const int64_t *ipiv,
-                                 const int *info) {
-    if (*info) return;
-    int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= n - w) return;
-    if (c >= k0) c += w;
-    double *col = A.p + c * A.ld;
-    for (int i = 0; i < w; ++i) {
-        const int64_t k = k0 + i, p = ipiv[k] - 1;
-        if (p != k) {
-            const double tmp = col[k];
-            col[k] = col[p];
-            col[p] = tmp;
+// Panel of the binary64 LU held in the shared memory of a cluster of CL
+// CTAs (distributed shared memory) instead of streamed through one SM:
+// CTA q of the cluster keeps panel rows k0 + q R .. k0 + q R + R - 1 (R =
+// ceil((m - k0) / CL)) of the w <= 32 columns.  Partial pivoting with the
+// first-largest rule of lu64_panel_kernel (the largest |A[r, k]|, ties to the
+// smallest row), one cluster barrier and one CTA barrier per column:
+//   * every CTA publishes the best active row of the next column (value,
+//     current row, slot) together with that row's values in its own shared
+//     memory;
+//   * after the cluster barrier every warp reads the CL candidates, picks
+//     the same pivot and takes the pivot row's values from the winner's
+//     published copy (one round of remote loads, issued together);
+//   * the interchange is logical: every CTA keeps the same map from current
+//     row to (CTA, slot), each thread the current row of its own slots; the
+//     data stay in place until the panel is written back;
+//   * each thread updates its active slots (current row > k) and forms the
+//     candidate of the next column in the same pass.
+// The panel is written back with each slot's row at its final position,
+// which equals physical row interchanges, and the moved rows are listed for
+// the interchanges outside the panel: src[i] = the original row that ends in
+// row k0 + i (i < w), and ext pairs (row >= k0 + w, original row) with a
+// count in ext[0].
+constexpr int LUC_CL = 8;       // CTAs of the cluster
+constexpr int LUC_W = 32;       // panel width
+constexpr int LUC_NT = 512;
+constexpr int LUC_SMEM_MAX = 220 * 1024;
+
+struct LucCand {
+    double v;   // |A[row, c]|, -1 for none
+    int row;    // current row index (absolute)
+    int code;   // owner CTA * R + slot
+    double vals[LUC_W];  // the row's values, columns c .. w-1
+};
+
+__device__ __forceinline__ uint32_t luc_map(const void *p, uint32_t rank) {
+    uint32_t a = (uint32_t)__cvta_generic_to_shared(p), r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+    return r;
+}
+__device__ __forceinline__ double luc_ld_f64(uint32_t addr) {
+    double v;
+    asm volatile("ld.shared::cluster.f64 %0, [%1];" : "=d"(v) : "r"(addr) : "memory");
+    return v;
+}
+__device__ __forceinline__ int luc_ld_s32(uint32_t addr) {
+    int v;
+    asm volatile("ld.shared::cluster.s32 %0, [%1];" : "=r"(v) : "r"(addr) : "memory");
+    return v;
+}
+__device__ __forceinline__ void luc_cluster_sync() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\t"
+                 "barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ bool luc_better(double v, int row, double bv, int brow) {
+    return v > bv || (v == bv && v >= 0.0 && row < brow);
+}
+// warp-wide best of (v, row, code)
+__device__ __forceinline__ void luc_warp_best(double &v, int &row, int &code) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, v, off);
+        const int orow = __shfl_xor_sync(0xffffffffu, row, off);
+        const int ocode = __shfl_xor_sync(0xffffffffu, code, off);
+        if (luc_better(ov, orow, v, row)) {
+            v = ov;
+            row = orow;
+            code = ocode;
         }
     }
 }
 
-// panel width nb (4..32): the single-CTA panel update streams the panel
-// through one SM (its traffic grows with the width), the trailing GEMM is
-// the rest of the work
-static int getrf64_fast(int64_t m, int64_t n, Mat A, int64_t *ipiv, int *info, cudaStream_t s,
-                        int nb) {
+// shared memory of the cluster panel kernel for R rows per CTA and mr panel rows
+__host__ __device__ inline size_t luc_smem(int64_t R, int64_t mr) {
+    return (size_t)R * LUC_W * sizeof(double) + (size_t)R * sizeof(int) +
+           (size_t)mr * sizeof(int) + 2 * sizeof(LucCand) + 64;
+}
+
+__global__ void __cluster_dims__(LUC_CL, 1, 1) __launch_bounds__(LUC_NT, 1)
+    lu64_cluster_panel_kernel(int64_t m, Mat A, int64_t k0, int w, int R, int64_t *ipiv,
+                              int *info, int *moved) {
+    extern __shared__ __align__(16) uint8_t luc_raw[];
+    double *panel = (double *)luc_raw;                        // [w][R]
+    int *slot_row = (int *)(panel + (size_t)R * LUC_W);       // [R] current row of a slot
+    int *where = slot_row + R;                                // [mr] code of a current row
+    const int64_t mr = m - k0;
+    LucCand *cand = (LucCand *)(((uintptr_t)(where + mr) + 15) & ~(uintptr_t)15);  // [2]
+    __shared__ double red_v[LUC_NT / 32];
+    __shared__ int red_r[LUC_NT / 32], red_c[LUC_NT / 32];
+
+    const int t = threadIdx.x, lane = t % 32, wid = t / 32;
+    uint32_t rank;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(rank));
+    const int64_t base = k0 + (int64_t)rank * R;  // absolute row of slot 0
+    const int64_t left = mr - (int64_t)rank * R;
+    const int nloc = (int)(left < 0 ? 0 : (left < R ? left : R));
+    const int stop0 = *info;  // every CTA reads the same value
+    if (rank == 0 && t == 0) moved[2 * LUC_W] = 0;  // count of the ext pairs
+
+    for (int j = 0; j < w; ++j)
+        for (int s = t; s < nloc; s += LUC_NT) panel[j * R + s] = A.p[(k0 + j) * A.ld + base + s];
+    for (int s = t; s < R; s += LUC_NT) slot_row[s] = (int)(base + s);
+    for (int64_t i = t; i < mr; i += LUC_NT) where[i] = (int)i;  // code = CTA * R + slot
+    __syncthreads();
+
+    // the best of this CTA's active rows for column c (values v, row, code per
+    // thread) reduced over the CTA and published with the row's values
+    auto publish = [&](int c, int buf, double v, int row, int code) {
+        luc_warp_best(v, row, code);
+        if (lane == 0) {
+            red_v[wid] = v;
+            red_r[wid] = row;
+            red_c[wid] = code;
+        }
+        __syncthreads();
+        if (wid == 0) {
+            v = lane < LUC_NT / 32 ? red_v[lane] : -1.0;
+            row = lane < LUC_NT / 32 ? red_r[lane] : 0x7fffffff;
+            code = lane < LUC_NT / 32 ? red_c[lane] : -1;
+            luc_warp_best(v, row, code);
+            if (lane == 0) {
+                cand[buf].v = v;
+                cand[buf].row = row;
+                cand[buf].code = code;
+            }
+            if (code >= 0 && c + lane < w) cand[buf].vals[c + lane] = panel[(c + lane) * R + code % R];
+        }
+    };
+    {
+        double v = -1.0;
+        int row = 0x7fffffff, code = -1;
+        for (int s = t; s < nloc; s += LUC_NT) {
+            const double a = fabs(panel[s]);
+            if (luc_better(a, slot_row[s], v, row)) {
+                v = a;
+                row = slot_row[s];
+                code = (int)rank * R + s;
+            }
+        }
+        publish(0, 0, v, row, code);
+    }
+    luc_cluster_sync();  // the candidates of column 0 and all shared memory initialised
+
+    __shared__ double s_u[LUC_W];   // the pivot row, columns c .. w-1 at s_u[c ..]
+    __shared__ int s_prow, s_pcode, s_ck, s_stop;
+    for (int c = 0; c < w; ++c) {
+        const int64_t k = k0 + c;
+        const int buf = c & 1;
+        if (wid == 0) {
+            // warp 0: the CL candidates and their published row values (one
+            // round of remote loads), the winner, the pivot row into s_u
+            double v = -1.0, vals[LUC_CL];
+            int prow = 0x7fffffff, q = -1;
+            if (lane < LUC_CL) {
+                const uint32_t a = luc_map(&cand[buf], (uint32_t)lane);
+                v = luc_ld_f64(a);
+                prow = luc_ld_s32(a + 8);
+                q = lane;
+            }
+#pragma unroll
+            for (int qq = 0; qq < LUC_CL; ++qq)
+                vals[qq] = c + lane < w ? luc_ld_f64(luc_map(&cand[buf].vals[c + lane], (uint32_t)qq))
+                                        : 0.0;
+            luc_warp_best(v, prow, q);
+            const int qb = q < 0 ? 0 : q;
+            double u = 0.0;
+#pragma unroll
+            for (int qq = 0; qq < LUC_CL; ++qq) u = qq == qb ? vals[qq] : u;
+            if (c + lane < w) s_u[c + lane] = u;
+            if (lane == 0) {
+                const uint32_t a = luc_map(&cand[buf], (uint32_t)qb);
+                s_prow = prow;
+                s_pcode = luc_ld_s32(a + 12);
+                s_ck = where[k - k0];
+                s_stop = stop0 != 0 || !(v > 0.0);
+                if (rank == 0) {
+                    if (stop0 == 0 && !(v > 0.0)) *info = (int)(k + 1);
+                    if (stop0 == 0 && v > 0.0) ipiv[k] = (int64_t)prow + 1;
+                }
+            }
+        }
+        __syncthreads();
+        if (s_stop) break;  // the same decision in every CTA
+        const int prow = s_prow, pcode = s_pcode, ck = s_ck;
+        const int po = pcode / R, ps = pcode % R;
+        const double ivp = 1.0 / s_u[c];
+        double bv = -1.0;
+        int br = 0x7fffffff, bc = -1;
+        for (int s = t; s < nloc; s += LUC_NT) {
+            int row = slot_row[s];
+            if ((int)rank == po && s == ps) row = (int)k;
+            else if (prow != k && (int)rank * R + s == ck) row = prow;
+            slot_row[s] = row;
+            if (row <= k) continue;  // the pivot rows so far are final
+            const double l = panel[c * R + s] * ivp;
+            panel[c * R + s] = l;
+            // independent updates of columns c+1 .. w-1, unrolled so that the
+            // loads of all columns are in flight together
+#pragma unroll
+            for (int j = 1; j < LUC_W; ++j)
+                if (c + j < w) panel[(c + j) * R + s] = fma(-l, s_u[c + j], panel[(c + j) * R + s]);
+            if (c + 1 < w) {
+                const double a = fabs(panel[(c + 1) * R + s]);
+                if (luc_better(a, row, bv, br)) {
+                    bv = a;
+                    br = row;
+                    bc = (int)rank * R + s;
+                }
+            }
+        }
+        if (c + 1 < w) {
+            publish(c + 1, buf ^ 1, bv, br, bc);  // its barrier also orders the map update
+        } else {
+            __syncthreads();
+        }
+        if (t == 0) {  // logical interchange in the replicated row map (s_ck read above)
+            where[prow - k0] = ck;
+            where[k - k0] = pcode;
+        }
+        luc_cluster_sync();  // next candidates published; this step's remote reads done
+    }
+    luc_cluster_sync();  // no CTA leaves while another may still read its shared memory
+    // write the panel back, every slot's row at its final position, and list
+    // the moved rows
+    for (int j = 0; j < w; ++j)
+        for (int s = t; s < nloc; s += LUC_NT) A.p[(k0 + j) * A.ld + slot_row[s]] = panel[j * R + s];
+    for (int s = t; s < nloc; s += LUC_NT) {
+        const int dest = slot_row[s], orig = (int)(base + s);
+        if (dest < k0 + w) {
+            moved[dest - k0] = orig;
+        } else if (dest != orig) {
+            const int e = atomicAdd(&moved[2 * LUC_W], 1);
+            moved[LUC_W + e] = dest;              // ext rows
+            moved[2 * LUC_W + 1 + e] = orig;      // ext sources
+        }
+    }
+}
+
+// The panel's interchanges (ipiv[k0 .. k0+w), ascending, as sequential
+// swaps) applied to every column outside the panel and, right of it, the
+// block row U12 = inv(L11) A12 (L11 the panel's unit-lower w x w block): one
+// warp per column.  The swaps permute the at most 2w rows involved (rows
+// k0 .. k0+w-1 and the pivot rows below them): `moved` lists, for each, the
+// original row whose value it receives (written by the cluster panel
+// kernel); without the list (the streamed panel) thread 0 replays the swaps
+// on the short list of involved rows.  A column is then one gather of its
+// involved rows (coalesced across the panel rows) and a 32-step solve in
+// registers.
+constexpr int LUS_WARPS = 8;
+
+__global__ void __launch_bounds__(32 * LUS_WARPS)
+    lu64_swap_trsm_kernel(int64_t n, Mat A, int64_t k0, int w, const int64_t *ipiv,
+                          const int *moved, const int *info) {
+    if (*info) return;
+    __shared__ int rows[2 * LUC_W], src[2 * LUC_W], cnt_s;
+    __shared__ double L[LUC_W][LUC_W + 1];
+    const int t = threadIdx.x, lane = t % 32, warp = t / 32;
+    if (moved) {
+        const int ext = moved[2 * LUC_W];
+        if (t < w) {
+            rows[t] = (int)(k0 + t);
+            src[t] = moved[t];
+        } else if (t >= LUC_W && t - LUC_W < ext) {
+            rows[w + t - LUC_W] = moved[t];
+            src[w + t - LUC_W] = moved[2 * LUC_W + 1 + t - LUC_W];
+        }
+        if (t == 0) cnt_s = w + ext;
+    } else if (t == 0) {
+        int content[2 * LUC_W];
+        int cnt = w;
+        for (int i = 0; i < w; ++i) rows[i] = (int)(k0 + i);
+        for (int i = 0; i < w; ++i) {
+            const int p = (int)(ipiv[k0 + i] - 1);
+            bool seen = p < k0 + w;
+            for (int j = w; j < cnt && !seen; ++j) seen = rows[j] == p;
+            if (!seen) rows[cnt++] = p;
+        }
+        for (int j = 0; j < cnt; ++j) content[j] = j;
+        for (int i = 0; i < w; ++i) {
+            const int p = (int)(ipiv[k0 + i] - 1);
+            int b = p - (int)k0;
+            if (p >= k0 + w)
+                for (int j = w; j < cnt; ++j)
+                    if (rows[j] == p) b = j;
+            const int x = content[i];
+            content[i] = content[b];
+            content[b] = x;
+        }
+        for (int j = 0; j < cnt; ++j) src[j] = rows[content[j]];
+        cnt_s = cnt;
+    }
+    for (int e = t; e < w * w; e += 32 * LUS_WARPS) {
+        const int i = e % w, j = e / w;
+        L[i][j] = A.p[(k0 + j) * A.ld + k0 + i];
+    }
+    __syncthreads();
+    const int cnt = cnt_s;
+    const int r0 = rows[lane], s0 = src[lane];
+    const bool two = lane + 32 < cnt;
+    const int r1 = two ? rows[lane + 32] : 0, s1 = two ? src[lane + 32] : 0;
+    for (int64_t col = (int64_t)blockIdx.x * LUS_WARPS + warp; col < n - w;
+         col += (int64_t)gridDim.x * LUS_WARPS) {
+        const int64_t c = col < k0 ? col : col + w;
+        double *x = A.p + c * A.ld;
+        // gather the involved rows (all reads before any write of this column)
+        double v0 = lane < cnt ? x[s0] : 0.0;
+        const double v1 = two ? x[s1] : 0.0;
+        __syncwarp();
+        if (two) x[r1] = v1;
+        if (c >= k0 + w) {
+            // rows k0 .. k0+w-1 are lanes 0 .. w-1 (rows[i] = k0 + i): solve L11 y = v
+            for (int j = 0; j < w; ++j) {
+                const double yj = __shfl_sync(0xffffffffu, v0, j);
+                if (lane > j && lane < w) v0 = fma(-L[lane][j], yj, v0);
+            }
+        }
+        if (lane < cnt) x[r0] = v0;
+    }
+}
+
+// panel width nb (4..32): a panel of up to about 6000 rows lives in the
+// shared memory of an 8-CTA cluster (lu64_cluster_panel_kernel); a taller
+// one streams through one CTA (lu64_panel_kernel, whose traffic grows with
+// the width); the U block row (TRSM) and the trailing update (FP64 GEMM)
+// follow each panel
+static int getrf64_fast(mflab_handle *h, int64_t m, int64_t n, Mat A, int64_t *ipiv, int *info,
+                        cudaStream_t s, int nb) {
     const double mone[1] = {-1.0}, one[1] = {1.0};
     cudaError_t e = cudaMemsetAsync(info, 0, sizeof(int), s);
     if (e != cudaSuccess) return record_cuda_error(e, "getrf info");
@@ -385,29 +689,60 @@ static int getrf64_fast(int64_t m, int64_t n, Mat A, int64_t *ipiv, int *info, c
     nonfinite_kernel<1><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(m, n, A, 0, info);
     int rc = record_cuda_error(cudaGetLastError(), "getrf check");
     if (rc) return rc;
-    const int NB = nb < 4 ? 4 : (nb > 32 ? 32 : nb);
+    // workspace of the library's binary64 GEMM (the trailing updates), then
+    // the moved-row list of the cluster panel
+    const size_t wsb = (size_t)32 << 20;
+    rc = mflab_reserve_scratch(h, wsb + 4 * LUC_W * sizeof(int));
+    if (rc) return rc;
+    int *moved = (int *)((char *)h->scratch + wsb);
+    const int NB = nb < 4 ? 4 : (nb > LUC_W ? LUC_W : nb);
+    static std::atomic<unsigned long long> luc_configured{0};
+    rc = set_smem_once((const void *)lu64_cluster_panel_kernel, LUC_SMEM_MAX, luc_configured,
+                       "lu64 cluster panel attribute");
+    if (rc) return rc;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     for (int64_t k0 = 0; k0 < kmax; k0 += NB) {
         const int w = (int)(kmax - k0 < NB ? kmax - k0 : NB);
-        lu64_panel_kernel<<<1, LU64_NT, 0, s>>>(m, A, k0, w, ipiv, info);
-        if (n > w)
-            lu64_swap_kernel<<<(unsigned)((n - w + 255) / 256), 256, 0, s>>>(n, A, k0, w, ipiv,
-                                                                           info);
+        // the panel in a cluster's shared memory when it fits, else streamed
+        // through one CTA
+        const int64_t mr = m - k0, R = (mr + LUC_CL - 1) / LUC_CL;
+        const size_t smem = luc_smem(R, mr);
+        const bool cluster = smem <= (size_t)LUC_SMEM_MAX && R <= 0x7fffffff;
+        if (cluster)
+            lu64_cluster_panel_kernel<<<LUC_CL, LUC_NT, smem, s>>>(m, A, k0, w, (int)R, ipiv,
+                                                                   info, moved);
+        else
+            lu64_panel_kernel<<<1, LU64_NT, 0, s>>>(m, A, k0, w, ipiv, info);
         rc = record_cuda_error(cudaGetLastError(), "getrf64 panel");
         if (rc) return rc;
-        const int64_t last = k0 + w - 1;
-        if (last < n - 1) {
-            const int64_t rest = n - 1 - last;
-            rc = launch_trsm_info(1, 0, 0, 0, 1, w, rest, A.at(k0, k0), A.at(k0, last + 1), one, s,
-                                  info);
+        // interchanges outside the panel and the U block row right of it
+        if (n > w) {
+            const int64_t cols = n - w;
+            const int64_t grid = std::min<int64_t>((cols + LUS_WARPS - 1) / LUS_WARPS, 4 * sms);
+            lu64_swap_trsm_kernel<<<(unsigned)grid, 32 * LUS_WARPS, 0, s>>>(
+                n, A, k0, w, ipiv, cluster ? moved : nullptr, info);
+            rc = record_cuda_error(cudaGetLastError(), "getrf64 swap + trsm");
             if (rc) return rc;
-            if (last < m - 1) {
-                rc = launch_mm(1, false, false, 0, false, m - 1 - last, rest, w,
+        }
+        const int64_t last = k0 + w - 1;
+        if (last < n - 1 && last < m - 1) {
+            // A22 -= L21 U12 (a plain binary64 GEMM; the factor has no
+            // reference order to keep).  A zero pivot stops the panels, and
+            // the updates after it only touch a failed factor.
+            rc = dgemm_lt(m - 1 - last, n - 1 - last, w, A.p + k0 * A.ld + last + 1, A.ld,
+                          A.p + (last + 1) * A.ld + k0, A.ld,
+                          A.p + (last + 1) * A.ld + last + 1, A.ld, -1.0, 1.0, h->scratch, wsb,
+                          s);
+            if (rc == MFLAB_ERR_UNSUPPORTED)  // no library algorithm: the device kernel
+                rc = launch_mm(1, false, false, 0, false, m - 1 - last, n - 1 - last, w,
                                A.at(last + 1, k0), A.at(k0, last + 1), A.at(last + 1, last + 1),
                                mone, one, s, info);
-                if (rc) return rc;
-            }
+            if (rc) return rc;
         }
     }
+    (void)one;
     return MFLAB_OK;
 }
 
@@ -796,7 +1131,7 @@ extern "C" int mflab_getrf(mflab_handle *h, void *stream, int limbs, int64_t m, 
         if (rc) return rc;
     }
     switch (limbs) {
-    case 1: return mfl::getrf64_fast(m, n, a, ipiv, info, s, (int)block);
+    case 1: return mfl::getrf64_fast(h, m, n, a, ipiv, info, s, (int)block);
     case 2: return mfl::getrf_n<2>(m, n, a, ipiv, block, info, s);
     case 3: return mfl::getrf_n<3>(m, n, a, ipiv, block, info, s);
     default: return mfl::getrf_n<4>(m, n, a, ipiv, block, info, s);

@@ -88,6 +88,10 @@ struct TcOpts {
 // tcgen05 kernels (int8_tc.cu, int8_tc2.cu)
 int int8_gemm_tn(int64_t m, int64_t n, int64_t K, const int8_t *A, int64_t lda, const int8_t *B,
                  int64_t ldb, int32_t *I, int64_t ldi, void *ws, size_t wsb, cudaStream_t s);
+// binary64 C = alpha A B + beta C through the library (ozaki.cu)
+int dgemm_lt(int64_t m, int64_t n, int64_t k, const double *A, int64_t lda, const double *B,
+             int64_t ldb, double *C, int64_t ldc, double alpha, double beta, void *ws, size_t wsb,
+             cudaStream_t s);
 int int8_gemm_tc(int64_t mp, int64_t np, int64_t K, const int8_t *A, int64_t lda, int64_t a_cols,
                  const int8_t *B, int64_t ldb, int64_t b_cols, int64_t b_xoff, int32_t *C,
                  int64_t ldc, int *err, cudaStream_t s, const TcOpts &o, int nz = 1,

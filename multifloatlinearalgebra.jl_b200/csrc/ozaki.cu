@@ -281,6 +281,42 @@ int int8_gemm_tn(int64_t m, int64_t n, int64_t K, const int8_t *A, int64_t lda,
     return rc;
 }
 
+// C = alpha A B + beta C in binary64 through the library (column-major, no
+// transposes): the plain trailing update of the binary64 LU
+int dgemm_lt(int64_t m, int64_t n, int64_t k, const double *A, int64_t lda, const double *B,
+             int64_t ldb, double *C, int64_t ldc, double alpha, double beta, void *ws, size_t wsb,
+             cudaStream_t s) {
+    if (m <= 0 || n <= 0) return MFLAB_OK;
+    cublasLtHandle_t h = lt_handle();
+    if (!h) return MFLAB_ERR_CUDA;
+    cublasLtMatmulDesc_t op = nullptr;
+    cublasLtMatrixLayout_t Ad = nullptr, Bd = nullptr, Cd = nullptr;
+    cublasLtMatmulPreference_t pref = nullptr;
+    int rc = MFLAB_OK;
+    cublasLtMatmulHeuristicResult_t res{};
+    int nres = 0;
+    if (cublasLtMatmulDescCreate(&op, CUBLAS_COMPUTE_64F, CUDA_R_64F) != CUBLAS_STATUS_SUCCESS ||
+        cublasLtMatrixLayoutCreate(&Ad, CUDA_R_64F, m, k, lda) ||
+        cublasLtMatrixLayoutCreate(&Bd, CUDA_R_64F, k, n, ldb) ||
+        cublasLtMatrixLayoutCreate(&Cd, CUDA_R_64F, m, n, ldc) ||
+        cublasLtMatmulPreferenceCreate(&pref) ||
+        cublasLtMatmulPreferenceSetAttribute(pref, CUBLASLT_MATMUL_PREF_MAX_WORKSPACE_BYTES, &wsb,
+                                             sizeof(wsb)) ||
+        cublasLtMatmulAlgoGetHeuristic(h, op, Ad, Bd, Cd, Cd, pref, 1, &res, &nres) ||
+        nres == 0) {
+        rc = MFLAB_ERR_UNSUPPORTED;
+    } else if (cublasLtMatmul(h, op, &alpha, A, Ad, B, Bd, &beta, C, Cd, C, Cd, &res.algo, ws, wsb,
+                              s) != CUBLAS_STATUS_SUCCESS) {
+        rc = MFLAB_ERR_CUDA;
+    }
+    if (pref) cublasLtMatmulPreferenceDestroy(pref);
+    if (Cd) cublasLtMatrixLayoutDestroy(Cd);
+    if (Bd) cublasLtMatrixLayoutDestroy(Bd);
+    if (Ad) cublasLtMatrixLayoutDestroy(Ad);
+    if (op) cublasLtMatmulDescDestroy(op);
+    return rc;
+}
+
 template <int N>
 static int oz_exponents(int64_t m, int64_t n, int64_t k, Mat A, Mat B, int *rowexp, int *colexp,
                         cudaStream_t s) {
@@ -293,6 +329,29 @@ static int oz_exponents(int64_t m, int64_t n, int64_t k, Mat A, Mat B, int *rowe
     oz_row_exp_kernel<N><<<gr, 256, 0, s>>>(m, k, A, kchunk, rowexp);
     if (n > 0) oz_col_exp_kernel<N><<<(unsigned)((n + 7) / 8), 256, 0, s>>>(k, n, B, colexp);
     return record_cuda_error(cudaGetLastError(), "ozaki exponents");
+}
+
+// row exponents of A alone / column exponents of B alone (the prepared
+// operand of the modular route and its per-call right operand)
+int ozaki_row_exps(int N, int64_t m, int64_t k, Mat A, int *rowexp, cudaStream_t s) {
+    if (m <= 0) return MFLAB_OK;
+    switch (N) {
+    case 2: return oz_exponents<2>(m, 0, k, A, A, rowexp, nullptr, s);
+    case 3: return oz_exponents<3>(m, 0, k, A, A, rowexp, nullptr, s);
+    case 4: return oz_exponents<4>(m, 0, k, A, A, rowexp, nullptr, s);
+    default: return MFLAB_ERR_UNSUPPORTED;
+    }
+}
+
+int ozaki_col_exps(int N, int64_t k, int64_t n, Mat B, int *colexp, cudaStream_t s) {
+    if (n <= 0) return MFLAB_OK;
+    switch (N) {
+    case 2: oz_col_exp_kernel<2><<<(unsigned)((n + 7) / 8), 256, 0, s>>>(k, n, B, colexp); break;
+    case 3: oz_col_exp_kernel<3><<<(unsigned)((n + 7) / 8), 256, 0, s>>>(k, n, B, colexp); break;
+    case 4: oz_col_exp_kernel<4><<<(unsigned)((n + 7) / 8), 256, 0, s>>>(k, n, B, colexp); break;
+    default: return MFLAB_ERR_UNSUPPORTED;
+    }
+    return record_cuda_error(cudaGetLastError(), "ozaki column exponents");
 }
 
 // optional phase events (profiling entry point only): [0] after exponents and

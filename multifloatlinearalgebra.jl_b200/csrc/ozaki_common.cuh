@@ -51,6 +51,10 @@ int ozaki_scales(mflab_handle *h, int N, int64_t m, int64_t n, int64_t k, Mat A,
 int ozaki_gram_scales(mflab_handle *h, int N, int trans, int64_t n, int64_t k, Mat A,
                       cudaStream_t s, int tune, int *gap8_host, int **exps);
 
+// row exponents of A alone, column exponents of B alone (device arrays)
+int ozaki_row_exps(int N, int64_t m, int64_t k, Mat A, int *rowexp, cudaStream_t s);
+int ozaki_col_exps(int N, int64_t k, int64_t n, Mat B, int *colexp, cudaStream_t s);
+
 // records phase event i on s when the phases entry point is timing a call
 void ozaki_phase(int i, cudaStream_t s);
 // ev[0..3] receive the phase events of the next route call (nullptr: off)

@@ -712,6 +712,30 @@ static void crt_split(const CrtPlan &p, int64_t m, int64_t n, int64_t k, Mat A, 
                                                  p.plane8b, 1, c);
 }
 
+// the left operand alone (rows of A -> A8) or the right one alone (B -> B8)
+template <int N, int WD>
+static void crt_split_one(const CrtPlan &p, bool left, int64_t rows, int64_t k, Mat X,
+                          const int *exps, int8_t *X8, cudaStream_t s) {
+    const CrtSplitConst &c = crt_split_const();
+    if (left) {
+        const dim3 ga = crt_split_a_grid<N>(p.mp, p.kp);
+        crt_split_a_kernel<N, WD><<<ga, dim3(32, 8), 0, s>>>(rows, p.mp, k, p.kp, p.Q, p.h, p.T, X,
+                                                             exps, X8, p.plane8a, 0, c);
+    } else {
+        const dim3 gb = crt_split_b_grid<N>(p.np, p.kp);
+        crt_split_b_kernel<N, WD><<<gb, 128, 0, s>>>(k, rows, p.np, p.kp, p.Q, p.h, p.T, X, exps,
+                                                     X8, p.plane8b, 1, c);
+    }
+}
+
+template <int N>
+static void crt_split_one_n(const CrtPlan &p, bool left, int64_t rows, int64_t k, Mat X,
+                            const int *exps, int8_t *X8, cudaStream_t s) {
+    if (p.WD <= 3) crt_split_one<N, 3>(p, left, rows, k, X, exps, X8, s);
+    else if (p.WD == 4) crt_split_one<N, 4>(p, left, rows, k, X, exps, X8, s);
+    else crt_split_one<N, 5>(p, left, rows, k, X, exps, X8, s);
+}
+
 template <int N>
 static void crt_split_n(const CrtPlan &p, int64_t m, int64_t n, int64_t k, Mat A, Mat B,
                         const int *rowexp, const int *colexp, int8_t *A8, int8_t *B8,
@@ -730,17 +754,21 @@ static void crt_accum(const CrtPlan &p, int64_t m, int64_t n, const uint8_t *I, 
                                               colexp, C, al, be, flags, crt_tables(p.T).dev);
 }
 
+// A8_ready: the residue planes of A from mflab_ozaki_crt_prepare (then the
+// scratch holds no A planes and A is not read), or nullptr
 template <int N>
 static int crt_gemm_n(mflab_handle *hd, const CrtPlan &p, int64_t m, int64_t n, int64_t k, Mat A,
                       Mat B, Mat C, const double *alpha, const double *beta, const int *rowexp,
-                      const int *colexp, cudaStream_t s) {
+                      const int *colexp, cudaStream_t s, const int8_t *A8_ready = nullptr) {
     char *base = (char *)hd->scratch;
-    int8_t *A8 = (int8_t *)base;
-    int8_t *B8 = (int8_t *)(base + p.a8);
-    uint8_t *Rs = (uint8_t *)(base + p.a8 + p.b8);
-    char *ws = base + p.a8 + p.b8 + p.lev;
+    const size_t a8 = A8_ready ? 0 : p.a8;
+    int8_t *A8 = A8_ready ? (int8_t *)A8_ready : (int8_t *)base;
+    int8_t *B8 = (int8_t *)(base + a8);
+    uint8_t *Rs = (uint8_t *)(base + a8 + p.b8);
+    char *ws = base + a8 + p.b8 + p.lev;
     ozaki_phase(0, s);
-    crt_split_n<N>(p, m, n, k, A, B, rowexp, colexp, A8, B8, s);
+    if (A8_ready) crt_split_one_n<N>(p, false, n, k, B, colexp, B8, s);
+    else crt_split_n<N>(p, m, n, k, A, B, rowexp, colexp, A8, B8, s);
     int rc = record_cuda_error(cudaGetLastError(), "modular split");
     if (rc) return rc;
     ozaki_phase(1, s);
@@ -1064,4 +1092,94 @@ extern "C" int mflab_gemm_ozaki_crt_phases(mflab_handle *h, void *stream, int li
     }
     for (auto &e : ev) cudaEventDestroy(e);
     return rc;
+}
+
+// ------------------------------------------------ prepared left operand ---
+// A Float64xN matrix used as the left operand of many modular GEMMs (the
+// residual B - A X of every refinement step): its row exponents and residue
+// planes for a fixed modulus count, computed once into caller memory.
+// Layout: rowexp[m] int32 (rounded up to 256 bytes), then the residue planes
+// A8[T][mp][Q kp] of the plan.
+namespace {
+size_t prep_rowexp_bytes(int64_t m) { return ((size_t)m * sizeof(int) + 255) / 256 * 256; }
+int prep_plan(int N, int T, int64_t m, int64_t n, int64_t k, mfl::CrtPlan &p) {
+    if (!mfl::valid_limbs(N)) return MFLAB_ERR_UNSUPPORTED;
+    if (T <= 0 || T > mfl::CRT_MAXT) return MFLAB_ERR_FLAG;
+    if (m < 0 || n < 0 || k < 1) return MFLAB_ERR_ARG;
+    if ((n + 255) / 256 * 256 > 65535LL || m > 0x3fffffffLL) return MFLAB_ERR_UNSUPPORTED;
+    int rc = mfl::crt_plan(N, m, n, k, T, 0, p);
+    if (rc) return rc;
+    if ((int64_t)p.T * p.mp > 0x7fffffffLL || (int64_t)p.T * p.np > 0x7fffffffLL)
+        return MFLAB_ERR_UNSUPPORTED;
+    return MFLAB_OK;
+}
+}  // namespace
+
+extern "C" int mflab_ozaki_crt_prepare_bytes(int limbs, int moduli, int64_t m, int64_t k,
+                                             size_t *bytes) {
+    if (!bytes) return MFLAB_ERR_ARG;
+    mfl::CrtPlan p;
+    int rc = prep_plan(limbs, moduli, m, 1, k, p);
+    if (rc) return rc;
+    *bytes = prep_rowexp_bytes(m) + p.a8;
+    return MFLAB_OK;
+}
+
+extern "C" int mflab_ozaki_crt_prepare(mflab_handle *h, void *stream, int limbs, int moduli,
+                                       int64_t m, int64_t k, const double *A, int64_t lda,
+                                       int64_t lsa, void *prep) {
+    MFLAB_RANGE("mflab_ozaki_crt_prepare");
+    if (!h) return MFLAB_ERR_UNSUPPORTED;
+    mfl::CrtPlan p;
+    int rc = prep_plan(limbs, moduli, m, 1, k, p);
+    if (rc) return rc;
+    if (!prep || (m > 0 && k > 0 && (!A || lda < m))) return MFLAB_ERR_ARG;
+    if (m == 0) return MFLAB_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    const mfl::Mat Am{(double *)A, lda, lsa};
+    int *rowexp = (int *)prep;
+    int8_t *A8 = (int8_t *)prep + prep_rowexp_bytes(m);
+    rc = mfl::ozaki_row_exps(limbs, m, k, Am, rowexp, s);
+    if (rc) return rc;
+    switch (limbs) {
+    case 2: mfl::crt_split_one_n<2>(p, true, m, k, Am, rowexp, A8, s); break;
+    case 3: mfl::crt_split_one_n<3>(p, true, m, k, Am, rowexp, A8, s); break;
+    default: mfl::crt_split_one_n<4>(p, true, m, k, Am, rowexp, A8, s); break;
+    }
+    return mfl::record_cuda_error(cudaGetLastError(), "modular prepare");
+}
+
+extern "C" int mflab_gemm_ozaki_crt_prepared(mflab_handle *h, void *stream, int limbs, int moduli,
+                                             int64_t m, int64_t n, int64_t k, const void *prep,
+                                             const double *B, int64_t ldb, int64_t lsb, double *C,
+                                             int64_t ldc, int64_t lsc, const double *alpha,
+                                             const double *beta) {
+    MFLAB_RANGE("mflab_gemm_ozaki_crt_prepared");
+    if (!h) return MFLAB_ERR_UNSUPPORTED;
+    mfl::CrtPlan p;
+    int rc = prep_plan(limbs, moduli, m, n, k, p);
+    if (rc) return rc;
+    if (!prep || !alpha || !beta || (n > 0 && k > 0 && (!B || ldb < k)) ||
+        (m > 0 && n > 0 && ldc < m))
+        return MFLAB_ERR_ARG;
+    if (m == 0 || n == 0) return MFLAB_OK;
+    if (mfl::views_overlap(C, ldc, lsc, m, n, limbs, B, ldb, lsb, k, n)) return MFLAB_ERR_ALIAS;
+    cudaStream_t s = (cudaStream_t)stream;
+    rc = mflab_reserve_scratch(h, p.total - p.a8);
+    if (rc) return rc;
+    rc = mflab_reserve_aux(h, sizeof(int) * (size_t)(n + 64));
+    if (rc) return rc;
+    int *colexp = (int *)h->aux;
+    const mfl::Mat Bm{(double *)B, ldb, lsb}, Cm{C, ldc, lsc};
+    rc = mfl::ozaki_col_exps(limbs, k, n, Bm, colexp, s);
+    if (rc) return rc;
+    const int *rowexp = (const int *)prep;
+    const int8_t *A8 = (const int8_t *)prep + prep_rowexp_bytes(m);
+    h->last_moduli = p.T;
+    const mfl::Mat none{nullptr, 0, 0};
+    switch (limbs) {
+    case 2: return mfl::crt_gemm_n<2>(h, p, m, n, k, none, Bm, Cm, alpha, beta, rowexp, colexp, s, A8);
+    case 3: return mfl::crt_gemm_n<3>(h, p, m, n, k, none, Bm, Cm, alpha, beta, rowexp, colexp, s, A8);
+    default: return mfl::crt_gemm_n<4>(h, p, m, n, k, none, Bm, Cm, alpha, beta, rowexp, colexp, s, A8);
+    }
 }

@@ -198,7 +198,9 @@ def gemm_sharded_(C, A, B, alpha=1.0, beta=0.0, config=None, group=None, root: i
 
     Returns C on root, None on the other ranks."""
     world, rank = _world(group)
-    dev = _device(group)
+    # the collectives' device (CUDA under NCCL, the CPU under gloo); one rank
+    # without a process group keeps the operands where they are
+    dev = _device(group) if world > 1 else A.device
     if rank == root:
         N, k, m = (int(x) for x in A.shape)
         n = int(B.shape[1])
