@@ -41,22 +41,6 @@ constexpr uint32_t TC_STAGE_BYTES = TC_A_BYTES + TC_B_BYTES;  // 64 KiB
 constexpr uint32_t TC_SMEM = TC_STAGES * TC_STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
 constexpr uint32_t TC_TMEM_COLS = 256;  // one 128 x 256 accumulator
 
-__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
-                                       uint32_t idesc, uint32_t accumulate) {
-    asm volatile(
-        "{\n\t.reg .pred PRED_enable_input_d;\n\t"
-        "setp.ne.b32 PRED_enable_input_d, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, PRED_enable_input_d;\n\t}"
-        ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
-        : "memory");
-}
-
-__device__ __forceinline__ void mma_commit(uint64_t *bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                     smem_u32(bar))
-                 : "memory");
-}
-
 // Persistent, warp-specialised kernel: one CTA per SM walks the 256 x 256
 // output tiles tile = blockIdx.x + i * gridDim.x (problem z outermost, then
 // column tiles, then row tiles, so that neighbouring CTAs share B tiles in L2).

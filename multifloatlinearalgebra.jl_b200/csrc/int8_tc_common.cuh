@@ -1,7 +1,8 @@
-// PTX helpers shared by the two tcgen05 int8 GEMM kernels (int8_tc.cu: one
-// CTA per SM; int8_tc2.cu: CTA pairs with cta_group::2): mbarriers, TMA
-// tile loads, shared-memory and instruction descriptors, the bounded waits
-// and the int8 -> int32 / residue-byte epilogue store.
+// PTX helpers shared by the tcgen05 kernels (int8_tc.cu: the int8 GEMM with
+// one CTA per SM; int8_tc2.cu: CTA pairs with cta_group::2; ozaki_crt.cu: the
+// CRT reconstruction): mbarriers, TMA tile loads, shared-memory and
+// instruction descriptors, MMA issue, TMEM loads, the bounded waits and the
+// int8 -> int32 / residue-byte epilogue store.
 #pragma once
 
 #include <cuda.h>
@@ -129,6 +130,55 @@ __host__ __device__ constexpr uint32_t idesc_i8(int M, int N) {
            | (1u << 7)    // A signed 8-bit
            | (1u << 10)   // B signed 8-bit
            | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+// instruction descriptor: u8 x u8 -> s32, both operands K-major, M x N
+__host__ __device__ constexpr uint32_t idesc_u8(int M, int N) {
+    return (2u << 4)  // D format s32; A and B formats 0: unsigned 8-bit
+           | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+// D (+)= A * B^T on this CTA's tensor core (accumulate = 0: D = A * B^T)
+__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                       uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred PRED_enable_input_d;\n\t"
+        "setp.ne.b32 PRED_enable_input_d, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, PRED_enable_input_d;\n\t}"
+        ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+// arrive once on `bar` when every MMA this thread issued so far has completed
+__device__ __forceinline__ void mma_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     smem_u32(bar))
+                 : "memory");
+}
+
+// 32 lanes x 16 columns of 32-bit accumulators, without waiting (the caller
+// issues tmem_wait_ld before reading v)
+__device__ __forceinline__ void tmem_ld16_async(uint32_t taddr, uint32_t (&v)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+          "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+          "=r"(v[14]), "=r"(v[15])
+        : "r"(taddr)
+        : "memory");
+}
+
+__device__ __forceinline__ void tmem_wait_ld() {
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// after tmem_wait_ld: ties the loaded registers to a point after the wait,
+// so that no use of them is scheduled before it
+template <int K>
+__device__ __forceinline__ void tmem_pin(uint32_t (&v)[K]) {
+#pragma unroll
+    for (int i = 0; i < K; ++i) asm volatile("" : "+r"(v[i])::"memory");
 }
 
 // 32 lanes x 16 columns of 32-bit accumulators from TMEM address taddr

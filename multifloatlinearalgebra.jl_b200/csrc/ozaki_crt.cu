@@ -35,6 +35,7 @@
 #include <mutex>
 #include <vector>
 
+#include "int8_tc_common.cuh"
 #include "mf_device.cuh"
 #include "mflab_internal.h"
 #include "ozaki_common.cuh"
@@ -488,6 +489,302 @@ __global__ void __launch_bounds__(CRT_ACC_ROWS, 3)
     store_mf<N>(C.p, C.ld, C.ls, i, j, r);
 }
 
+// ---------------------------------- reconstruction on the tensor cores ----
+// The sum X = sum_t r_t U_t of the reconstruction as an int8 product: the
+// residues r_t (unsigned bytes, r_t < p_t <= 256) of 128 entries of one
+// column of C are the rows of A (K runs over the moduli, zero beyond T) and
+// the little-endian bytes u_{t,b} of the U_t are the rows of B, so one
+// tcgen05.mma.kind::i8 (u8 x u8 -> s32, M = 128, N = CrtTcN bytes, K = 32)
+// per 32 moduli yields the byte sums S_b = sum_t r_t u_{t,b} exactly (below
+// 49 * 255^2 < 2^22), and X = sum_b S_b 2^(8 b).  From X on (q = round(X / P),
+// X - q P, conversion, levels, epilogue) the arithmetic is crt_accum_kernel's
+// on the same integer, so the two kernels give the same bits.
+//
+// Persistent CTAs of 4 warps walk tasks of 128 rows x J columns (J = 2 for
+// one digit level, 1 for two: J Q slots of one column and level):
+//   1. the warps turn residue segments into K-major operand rows: lane l loads
+//      the 32-bit words (entries 4l .. 4l+3) of 16 moduli (coalesced), then
+//      transposes the 4 x 16 bytes with byte permutes and stores one 16-byte
+//      chunk per entry into the 128-byte swizzled row layout (the entries are
+//      visited in a lane-rotated order, so a warp's stores hit every bank).
+//      A slot takes 32 bytes of a row per 32 moduli, so 128 / (32 ksteps)
+//      slots share one 128-row operand tile;
+//   2. thread 0 issues the task's MMAs (one per slot and 32 moduli; a slot's
+//      operand starts at its byte offset inside the swizzled rows) and commits
+//      them to an mbarrier;
+//   3. after the bounded wait, warp w reads TMEM lanes 32w .. 32w+31, one
+//      entry per thread, and finishes the entries.
+// Occupancy hides the latency of the load -> MMA -> epilogue chain of a task:
+// the TMEM allocation is J Q NB columns (rounded up to a power of two), and
+// as many CTAs as fit into 512 columns share an SM.
+constexpr int CRT_TC_THREADS = 128;
+constexpr uint32_t CRT_TC_ATILE = 128 * 128;  // one operand tile: 128 rows x 128 B
+
+// bytes of U_t (< P < 2^(32 WP - 14)) rounded up to the MMA's N step
+template <int WP>
+struct CrtTcN {
+    static constexpr int value = WP == 8 ? 32 : 48;
+};
+
+// kernel copy of the tensor-core reconstruction constants
+struct __align__(16) CrtTcDev {
+    uint32_t ub[48][16];  // byte (t % 4) of ub[b][t / 4] = byte b of U_t; zero for t >= T
+    uint32_t P[CRT_WP];
+    double pinv;
+};
+
+// 32-bit add / subtract with the carry flag (a chain keeps its order: the
+// statements are volatile and no other instruction touches the flag)
+__device__ __forceinline__ uint32_t add_cc(uint32_t a, uint32_t b) {
+    uint32_t r;
+    asm volatile("add.cc.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+    return r;
+}
+__device__ __forceinline__ uint32_t addc_cc(uint32_t a, uint32_t b) {
+    uint32_t r;
+    asm volatile("addc.cc.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+    return r;
+}
+__device__ __forceinline__ uint32_t sub_cc(uint32_t a, uint32_t b) {
+    uint32_t r;
+    asm volatile("sub.cc.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+    return r;
+}
+__device__ __forceinline__ uint32_t subc_cc(uint32_t a, uint32_t b) {
+    uint32_t r;
+    asm volatile("subc.cc.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+    return r;
+}
+__device__ __forceinline__ uint32_t subc(uint32_t a, uint32_t b) {
+    uint32_t r;
+    asm volatile("subc.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+    return r;
+}
+
+// X from the byte sums S_b < 2^22: WP normalized 32-bit words.  With
+// lo_w = S_4w + 2^8 S_4w+1 and hi_w = S_4w+2 + 2^8 S_4w+3 (both < 2^31),
+// X = sum_w (lo_w + 2^16 hi_w) 2^(32 w): word w adds lo_w + (hi_(w-1) >> 16)
+// (no overflow) and hi_w << 16 in one carry chain; X < 2^(32 WP) leaves no
+// carry out of the top word.
+template <int WP, int NB>
+__device__ __forceinline__ void crt_bytesums_to_words(const uint32_t (&S)[NB], uint32_t (&x)[WP]) {
+    uint32_t lo[WP], hi[WP];
+#pragma unroll
+    for (int w = 0; w < WP; ++w) {
+        const uint32_t s0 = 4 * w < NB ? S[4 * w] : 0u, s1 = 4 * w + 1 < NB ? S[4 * w + 1] : 0u;
+        const uint32_t s2 = 4 * w + 2 < NB ? S[4 * w + 2] : 0u,
+                       s3 = 4 * w + 3 < NB ? S[4 * w + 3] : 0u;
+        lo[w] = s0 + (s1 << 8);
+        hi[w] = s2 + (s3 << 8);
+    }
+    x[0] = add_cc(lo[0], hi[0] << 16);
+#pragma unroll
+    for (int w = 1; w < WP; ++w) x[w] = addc_cc(lo[w] + (hi[w - 1] >> 16), hi[w] << 16);
+}
+
+// crt_reduce for normalized words x (0 <= x < 2^(32 WP)) with carry chains:
+// G = X - q P as magnitude words + sign, the same words crt_reduce gives
+template <int WP>
+__device__ __forceinline__ bool crt_reduce_norm(const uint32_t (&x)[WP], const uint32_t *Pw,
+                                                uint32_t q, uint32_t (&mag)[WP]) {
+    uint32_t qp[WP], hi = 0;
+#pragma unroll
+    for (int w = 0; w < WP; ++w) {
+        const uint64_t t = (uint64_t)q * Pw[w] + hi;
+        qp[w] = (uint32_t)t;
+        hi = (uint32_t)(t >> 32);
+    }
+    uint32_t y[WP];
+    y[0] = sub_cc(x[0], qp[0]);
+#pragma unroll
+    for (int w = 1; w < WP; ++w) y[w] = subc_cc(x[w], qp[w]);
+    const uint32_t flip = subc(0u, 0u);  // all ones when X < q P
+    // |Y| = (Y ^ flip) - flip over all words (flip in every word is -1 or 0)
+    mag[0] = sub_cc(y[0] ^ flip, flip);
+#pragma unroll
+    for (int w = 1; w < WP; ++w) mag[w] = subc_cc(y[w] ^ flip, flip);
+    return flip != 0u;
+}
+
+// levels and columns of one task: Q = 1 digit level and 2 columns for
+// Float64x2, 2 levels and 1 column for more limbs (2 slots either way)
+template <int N>
+struct CrtTcShape {
+    static constexpr int Q = N == 2 ? 1 : 2, J = N == 2 ? 2 : 1, SLOTS = Q * J;
+};
+
+template <int N, int WP>
+__global__ void __launch_bounds__(CRT_TC_THREADS)
+    crt_accum_tc_kernel(int64_t m, int64_t n, int h, int T, const uint8_t *R, int64_t ldi,
+                        size_t plane, const int *rowexp, const int *colexp, Mat C, scal<N> alpha,
+                        scal<N> beta, int flags, uint32_t tmem_cols, int *err,
+                        const __grid_constant__ CrtTcDev c) {
+    constexpr int NB = CrtTcN<WP>::value, Q = CrtTcShape<N>::Q, J = CrtTcShape<N>::J,
+                  SLOTS = CrtTcShape<N>::SLOTS;
+    const int ksteps = (T + 31) >> 5, kchunks = 2 * ksteps;
+    const int spt = 8 / kchunks;  // slots per operand tile
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint8_t *sB = smem;            // NB rows x 128 B (a multiple of 1024 B)
+    uint8_t *sA = smem + NB * 128;  // ceil(SLOTS / spt) tiles of 128 rows x 128 B
+    uint64_t *done = (uint64_t *)(sA + (size_t)((SLOTS + spt - 1) / spt) * CRT_TC_ATILE);
+    uint32_t *tmem_slot = (uint32_t *)(done + 1);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    // B: row b = bytes b of U_0 .. U_63; 16-byte chunk ch of a row sits at
+    // chunk position ch ^ (b & 7) of the 128-byte swizzle
+    for (int e = threadIdx.x; e < NB * 4; e += CRT_TC_THREADS) {
+        const int b = e >> 2, ch = e & 3;
+        const uint4 v = make_uint4(c.ub[b][4 * ch], c.ub[b][4 * ch + 1], c.ub[b][4 * ch + 2],
+                                   c.ub[b][4 * ch + 3]);
+        *(uint4 *)(sB + (b >> 3) * 1024 + (b & 7) * 128 + ((ch ^ (b & 7)) << 4)) = v;
+    }
+    if (threadIdx.x == 0) {
+        mbar_init(done, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(tmem_slot)),
+                     "r"(tmem_cols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+    constexpr uint32_t idesc = idesc_u8(128, NB);
+
+    const int64_t mblk = (m + 127) >> 7, tasks = mblk * ((n + J - 1) / J);
+    uint32_t phase = 0;
+    for (int64_t task = blockIdx.x; task < tasks; task += gridDim.x) {
+        const int64_t i0 = (task % mblk) * 128, j0 = (task / mblk) * J;
+        // flags bit 2: lower triangle only (the GEMM skipped the tiles above it)
+        if ((flags & 4) && i0 + 127 < j0) continue;
+        // 1. residue segments -> K-major rows (rows i0 .. i0+127 lie inside the
+        //    padded planes; columns j >= n read nothing)
+        for (int pr = warp; pr < SLOTS * kchunks; pr += CRT_TC_THREADS / 32) {
+            const int ch = pr % kchunks, sl = pr / kchunks, jj = sl / Q, L = sl % Q;
+            const int64_t j = j0 + jj;
+            const uint8_t *src = R + (size_t)L * T * plane + (size_t)j * ldi + i0 + 4 * lane;
+            uint32_t w[16];
+#pragma unroll
+            for (int u = 0; u < 16; ++u) {
+                const int t = 16 * ch + u;
+                w[u] = (t < T && j < n) ? __ldg((const uint32_t *)(src + (size_t)t * plane)) : 0u;
+            }
+            uint8_t *dst = sA + (size_t)(sl / spt) * CRT_TC_ATILE;
+            const int cl = (sl % spt) * kchunks + ch;  // logical chunk of the row
+#pragma unroll
+            for (int st = 0; st < 4; ++st) {
+                const int rr = (st + (lane >> 1)) & 3, row = 4 * lane + rr;
+                const uint32_t sel = (uint32_t)rr | ((uint32_t)(rr + 4) << 4);
+                uint32_t o[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const uint32_t lo = __byte_perm(w[4 * q], w[4 * q + 1], sel);
+                    const uint32_t hi = __byte_perm(w[4 * q + 2], w[4 * q + 3], sel);
+                    o[q] = __byte_perm(lo, hi, 0x5410);
+                }
+                *(uint4 *)(dst + row * 128 + ((cl ^ (row & 7)) << 4)) =
+                    make_uint4(o[0], o[1], o[2], o[3]);
+            }
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        // 2. the task's MMAs
+        if (threadIdx.x == 0) {
+            for (int sl = 0; sl < SLOTS; ++sl) {
+                const uint32_t a0 = smem_u32(sA + (size_t)(sl / spt) * CRT_TC_ATILE) +
+                                    (uint32_t)(sl % spt) * 32u * (uint32_t)ksteps;
+                for (int ks = 0; ks < ksteps; ++ks)
+                    mma_i8(tmem + (uint32_t)(sl * NB), smem_desc_sw128(a0 + 32 * ks),
+                           smem_desc_sw128(smem_u32(sB) + 32 * ks), idesc, (uint32_t)ks);
+            }
+            mma_commit(done);
+        }
+        // the CTA's own MMAs: the drain bound, one decision for the whole CTA
+        const bool ok = mbar_wait(done, phase, TC_DRAIN_LIMIT);
+        phase ^= 1;
+        if (__syncthreads_or(!ok)) {
+            if (threadIdx.x == 0) atomicExch(err, TC_ERR_DRAIN);
+            break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        // 3. one row per thread: the SLOTS sums of its entries side by side
+        const int64_t i = i0 + 32 * warp + lane;
+        const int ea = i < m ? rowexp[i] : 0;
+        uint32_t S[SLOTS][NB];
+        __syncwarp();
+#pragma unroll
+        for (int sl = 0; sl < SLOTS; ++sl) {
+            uint32_t v0[16], v1[16], v2[16];
+            const uint32_t ta = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(sl * NB);
+            tmem_ld16_async(ta, v0);
+            tmem_ld16_async(ta + 16, v1);
+            if constexpr (NB > 32) tmem_ld16_async(ta + 32, v2);
+            tmem_wait_ld();
+            tmem_pin(v0);
+            tmem_pin(v1);
+            if constexpr (NB > 32) tmem_pin(v2);
+#pragma unroll
+            for (int b = 0; b < 16; ++b) {
+                S[sl][b] = v0[b];
+                S[sl][16 + b] = v1[b];
+                if constexpr (NB > 32) S[sl][32 + b] = v2[b];
+            }
+        }
+        mf<N> g[SLOTS];
+#pragma unroll
+        for (int sl = 0; sl < SLOTS; ++sl) {
+            const int jj = sl / Q, L = sl % Q;
+            const int64_t j = j0 + jj;
+            const int eb = j < n ? colexp[j] : 0;
+            uint32_t x[WP];
+            crt_bytesums_to_words<WP, NB>(S[sl], x);
+            double xd = (double)x[WP - 1];
+#pragma unroll
+            for (int w = WP - 2; w >= 0; --w) xd = fma(xd, 4294967296.0, (double)x[w]);
+            const uint32_t q = (uint32_t)floor(xd * c.pinv + 0.5);
+            uint32_t mag[WP];
+            const bool ng = crt_reduce_norm<WP>(x, c.P, q, mag);
+            const int sh = oz_scale_exp(ea) + oz_scale_exp(eb) - 2 * Q * h + h * (2 * Q - 2 - L);
+            g[sl] = crt_words_to_mf<N, WP>(mag, sh);
+            if (ng) g[sl] = neg(g[sl]);
+        }
+#pragma unroll
+        for (int jj = 0; jj < J; ++jj) {
+            const int64_t j = j0 + jj;
+            mf<N> acc = g[jj * Q + Q - 1];
+#pragma unroll
+            for (int L = Q - 2; L >= 0; --L) acc = add(acc, g[jj * Q + L]);
+            if (j < n && i < m && !((flags & 4) && i < j)) {
+                const int eb = colexp[j];
+                if (ea == OZ_EXP_BAD || eb == OZ_EXP_BAD)
+                    acc = from_double<N>(__longlong_as_double(0x7ff8000000000000LL));
+                // flags bit 0: beta == 0 (C is not read); bit 1: alpha == 1
+                mf<N> r = (flags & 2) ? acc : mul(alpha.get(), acc);
+                if (!(flags & 1)) r = add(r, mul(beta.get(), load_mf<N>(C.p, C.ld, C.ls, i, j)));
+                store_mf<N>(C.p, C.ld, C.ls, i, j, r);
+            }
+        }
+        __syncwarp();
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(tmem_cols)
+                     : "memory");
+    }
+}
+
 // residues of int32 sums modulo p as bytes (library-engine path)
 __global__ void crt_mod_kernel(const int32_t *G, uint8_t *R, size_t count, int p) {
     const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -554,6 +851,7 @@ static uint32_t inv_mod(uint32_t a, uint32_t p) {
 struct CrtTables {
     CrtAccConst acc;
     CrtAccDev dev;
+    CrtTcDev tc;
     int bitlen;  // bit length of P
 };
 
@@ -598,6 +896,10 @@ static const CrtTables &crt_tables(int T) {
             big_div_small(M, p, &r);
             const Big U = big_mul_small(M, inv_mod(r, p));
             for (size_t w = 0; w < U.size() && w < (size_t)CRT_WP; ++w) c.acc.U[t][w] = U[w];
+            for (int b = 0; b < 48; ++b) {
+                const uint32_t byte = (size_t)(b >> 2) < U.size() ? (U[b >> 2] >> (8 * (b & 3))) & 0xffu : 0u;
+                c.tc.ub[b][t >> 2] |= byte << (8 * (t & 3));
+            }
             for (int cc = 0; cc < CRT_NC; ++cc) {
                 uint64_t v = 0;  // bits [39 cc, 39 cc + 39) of U_t
                 for (int b = 0; b < CRT_CW; ++b) {
@@ -613,6 +915,8 @@ static const CrtTables &crt_tables(int T) {
         c.acc.pinv = (double)(1.0L / pd);
         memcpy(c.dev.P, c.acc.P, sizeof(c.dev.P));
         c.dev.pinv = c.acc.pinv;
+        memcpy(c.tc.P, c.acc.P, sizeof(c.tc.P));
+        c.tc.pinv = c.acc.pinv;
     });
     return tab[T];
 }
@@ -754,6 +1058,78 @@ static void crt_accum(const CrtPlan &p, int64_t m, int64_t n, const uint8_t *I, 
                                               colexp, C, al, be, flags, crt_tables(p.T).dev);
 }
 
+// The tensor-core reconstruction: persistent CTAs, as many per SM as their
+// TMEM allocations fit into the SM's 512 columns (the dynamic shared memory
+// is raised until the occupancy says so, so no allocation ever waits).
+// Returns false when the launch shape cannot be had (the caller then runs
+// crt_accum).
+template <int N, int WP>
+static bool crt_accum_tc(const CrtPlan &p, int64_t m, int64_t n, const uint8_t *I,
+                         const int *rowexp, const int *colexp, Mat C, const scal<N> &al,
+                         const scal<N> &be, int flags, int *err, cudaStream_t s) {
+    constexpr int NB = CrtTcN<WP>::value;
+    if (p.T > 64 || m <= 0 || n <= 0 || p.Q != CrtTcShape<N>::Q) return false;
+    constexpr int J = CrtTcShape<N>::J, slots = CrtTcShape<N>::SLOTS;
+    const int spt = 8 / (2 * ((p.T + 31) / 32));
+    uint32_t cols = 32;
+    while ((int)cols < slots * NB) cols <<= 1;
+    const int max_ctas = 512 / (int)cols;
+    int dev = 0, sms = 0, smem_sm = 0, smem_blk = 0, reserved = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) !=
+            cudaSuccess ||
+        cudaDeviceGetAttribute(&smem_blk, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) !=
+            cudaSuccess ||
+        cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev) !=
+            cudaSuccess)
+        return false;
+    size_t smem = 1024 + (size_t)NB * 128 + (size_t)((slots + spt - 1) / spt) * CRT_TC_ATILE + 16;
+    // at most max_ctas blocks of (smem + reserved) bytes on one SM
+    const size_t floor_smem = (size_t)smem_sm / (size_t)(max_ctas + 1) + 1;
+    if (smem + (size_t)reserved < floor_smem) smem = floor_smem - (size_t)reserved;
+    smem = (smem + 127) / 128 * 128;
+    if (smem > (size_t)smem_blk) return false;
+    auto kern = crt_accum_tc_kernel<N, WP>;
+    // the largest shared-memory carveout, so that as many CTAs as the
+    // shared memory allows share an SM (the default lets the driver pick a
+    // carveout that holds one)
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared) != cudaSuccess)
+        return false;
+    // max_ctas per SM by the shared memory; the grid does not depend on how
+    // many of them are resident at once (tasks carry no dependencies)
+    const int64_t tasks = (m + 127) / 128 * ((n + J - 1) / J);
+    const int64_t slots_all = (int64_t)sms * max_ctas;
+    const int grid = (int)(tasks < slots_all ? tasks : slots_all);
+    kern<<<grid, CRT_TC_THREADS, smem, s>>>(m, n, p.h, p.T, I, p.ldi, p.plane, rowexp,
+                                            colexp, C, al, be, flags, cols, err,
+                                            crt_tables(p.T).tc);
+    return true;
+}
+
+// the reconstruction: on the tensor cores with a tcgen05 engine, else (or
+// when that launch shape is unavailable) crt_accum
+template <int N>
+static void crt_reconstruct(mflab_handle *hd, const CrtPlan &p, int64_t m, int64_t n,
+                            const uint8_t *Rs, const int *rowexp, const int *colexp, Mat C,
+                            const scal<N> &al, const scal<N> &be, int flags, cudaStream_t s) {
+    if (tc_engine(hd)) {
+        int *err = hd->dev_flags + 1;
+        bool done = false;
+        if (p.WP == 8) done = crt_accum_tc<N, 8>(p, m, n, Rs, rowexp, colexp, C, al, be, flags, err, s);
+        else if (p.WP == 10) done = crt_accum_tc<N, 10>(p, m, n, Rs, rowexp, colexp, C, al, be, flags, err, s);
+        else done = crt_accum_tc<N, 12>(p, m, n, Rs, rowexp, colexp, C, al, be, flags, err, s);
+        if (done) return;
+        (void)cudaGetLastError();
+    }
+    if (p.WP == 8) crt_accum<N, 8>(p, m, n, Rs, rowexp, colexp, C, al, be, flags, s);
+    else if (p.WP == 10) crt_accum<N, 10>(p, m, n, Rs, rowexp, colexp, C, al, be, flags, s);
+    else crt_accum<N, 12>(p, m, n, Rs, rowexp, colexp, C, al, be, flags, s);
+}
+
 // A8_ready: the residue planes of A from mflab_ozaki_crt_prepare (then the
 // scratch holds no A planes and A is not read), or nullptr
 template <int N>
@@ -803,9 +1179,7 @@ static int crt_gemm_n(mflab_handle *hd, const CrtPlan &p, int64_t m, int64_t n, 
         if (beta[l] != 0.0) flags &= ~1;
         if (alpha[l] != (l == 0 ? 1.0 : 0.0)) flags &= ~2;
     }
-    if (p.WP == 8) crt_accum<N, 8>(p, m, n, Rs, rowexp, colexp, C, al, be, flags, s);
-    else if (p.WP == 10) crt_accum<N, 10>(p, m, n, Rs, rowexp, colexp, C, al, be, flags, s);
-    else crt_accum<N, 12>(p, m, n, Rs, rowexp, colexp, C, al, be, flags, s);
+    crt_reconstruct<N>(hd, p, m, n, Rs, rowexp, colexp, C, al, be, flags, s);
     ozaki_phase(3, s);
     return record_cuda_error(cudaGetLastError(), "modular accumulate");
 }
@@ -911,9 +1285,7 @@ static int crt_syrk_n(mflab_handle *hd, const CrtPlan &p, int trans, int64_t n, 
         if (beta[l] != 0.0) flags &= ~1;
         if (alpha[l] != (l == 0 ? 1.0 : 0.0)) flags &= ~2;
     }
-    if (p.WP == 8) crt_accum<N, 8>(p, n, n, Rs, exps, exps, C, al, be, flags, s);
-    else if (p.WP == 10) crt_accum<N, 10>(p, n, n, Rs, exps, exps, C, al, be, flags, s);
-    else crt_accum<N, 12>(p, n, n, Rs, exps, exps, C, al, be, flags, s);
+    crt_reconstruct<N>(hd, p, n, n, Rs, exps, exps, C, al, be, flags, s);
     ozaki_phase(3, s);
     return record_cuda_error(cudaGetLastError(), "modular gram accumulate");
 }

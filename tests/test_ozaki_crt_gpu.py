@@ -103,6 +103,51 @@ def test_modular_engines_bitwise_equal(mf, rng, N):
     assert mf.device_status() == 0
 
 
+@pytest.mark.parametrize("N", [2, 3, 4])
+@pytest.mark.parametrize("T", [8, 30, 36, 49])
+@pytest.mark.parametrize("shape", [(129, 200, 257), (256, 130, 256), (1, 64, 3), (300, 33, 1)],
+                         ids=str)
+def test_reconstruction_engines_bitwise(mf, rng, N, T, shape):
+    """the tensor-core reconstruction (tcgen05 engines: byte sums of the
+    residues by an int8 MMA) and the CUDA-core one (library engine) give the
+    same bits for every word count of the CRT sum (T = 8, 30: 8 words; 36:
+    10; 49: 12), ragged shapes (rows past a 128-row block, an odd column past
+    a column pair) and a general alpha/beta epilogue"""
+    from conftest import assert_bitwise
+    m, k, n = shape
+    A, B = syn.randn_mf(rng, N, m, k, spread=12), syn.randn_mf(rng, N, k, n, spread=12)
+    C0 = syn.randn_mf(rng, N, m, n)
+    alpha, beta = syn.randn_mf(rng, N, 1, 1)[:, 0, 0], syn.randn_mf(rng, N, 1, 1)[:, 0, 0]
+    Ad, Bd = mf.MFMatrix.from_numpy(A), mf.MFMatrix.from_numpy(B)
+    out = []
+    for engine in ("tcgen05", "tcgen05_pair", "library"):
+        Cd = mf.MFMatrix.from_numpy(C0)
+        mf.gemm_(Cd, Ad, Bd, alpha, beta, config=_cfg(mf, ozaki_moduli=T, ozaki_engine=engine))
+        out.append(Cd.to_numpy())
+    assert_bitwise(out[0], out[2], "tensor-core vs CUDA-core reconstruction")
+    assert_bitwise(out[1], out[2], "pair engine vs CUDA-core reconstruction")
+    assert mf.device_status() == 0
+
+
+def test_reconstruction_nonfinite_rows_and_columns(mf, rng):
+    """a row of A or a column of B with a non-finite entry gives NaN in its
+    row / column of C on both reconstructions, the rest is unchanged"""
+    from conftest import assert_bitwise
+    N, m, k, n = 2, 140, 50, 9
+    A, B = syn.randn_mf(rng, N, m, k), syn.randn_mf(rng, N, k, n)
+    A[0, 5, 7] = np.inf
+    B[0, 3, 4] = np.nan
+    Ad, Bd = mf.MFMatrix.from_numpy(A), mf.MFMatrix.from_numpy(B)
+    out = []
+    for engine in ("tcgen05", "library"):
+        Cd = mf.MFMatrix.zeros(N, m, n)
+        mf.gemm_(Cd, Ad, Bd, config=_cfg(mf, ozaki_moduli=20, ozaki_engine=engine))
+        out.append(Cd.to_numpy())
+    assert np.all(np.isnan(out[0][0, 5, :])) and np.all(np.isnan(out[0][0, :, 4]))
+    assert np.all(np.isfinite(np.delete(np.delete(out[0][0], 5, 0), 4, 1)))
+    assert_bitwise(out[0], out[1], "non-finite")
+
+
 @pytest.mark.parametrize("N", [2, 4])
 def test_modular_alpha_beta(mf, ref, rng, N):
     m, k, n = 40, 60, 30
