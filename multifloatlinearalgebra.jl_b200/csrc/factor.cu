@@ -591,6 +591,214 @@ __global__ void __cluster_dims__(LUC_CL, 1, 1) __launch_bounds__(LUC_NT, 1)
     }
 }
 
+// The same panel with its rows in registers: 256 threads hold two slots each
+// (R <= 512 rows per CTA).  Register j of a row holds column c + j at step c:
+// the rank-1 update writes its results one register down,
+//     row[j] = fma(-l, u[j + 1], row[j + 1]),
+// so the step's column is always register 0 and no register index depends
+// on the column (the column loop stays rolled and its code small).  Every
+// final value goes to shared memory when it is formed — the multiplier of
+// an active row at its column, the whole remaining row of the pivot when it
+// is chosen — and the panel is written back from there.  Pivot rule, logical
+// interchanges (the slot holding row k recognises itself by its current row)
+// and the moved-row list are those of lu64_cluster_panel_kernel; candidates
+// and the pivot row's values are published relative to their column, the
+// CTA's winning thread writing its row after the CTA reduction.
+constexpr int LUR_NT = 256, LUR_RPT = 2;
+
+// shared memory of the register panel kernel: the final values [w][R], two
+// candidates
+__host__ __device__ inline size_t lur_smem(int64_t R) {
+    return (size_t)LUC_W * R * sizeof(double) + 2 * sizeof(LucCand) + 64;
+}
+
+__global__ void __cluster_dims__(LUC_CL, 1, 1) __launch_bounds__(LUR_NT, 1)
+    lu64_cluster_panel_reg_kernel(int64_t m, Mat A, int64_t k0, int w, int R, int64_t *ipiv,
+                                  int *info, int *moved) {
+    extern __shared__ __align__(16) uint8_t lur_raw[];
+    double *fin = (double *)lur_raw;  // [w][R] final values
+    LucCand *cand = (LucCand *)(((uintptr_t)(fin + (size_t)LUC_W * R) + 15) & ~(uintptr_t)15);
+    __shared__ double red_v[LUR_NT / 32];
+    __shared__ int red_r[LUR_NT / 32], red_c[LUR_NT / 32];
+    __shared__ double s_u[LUC_W];  // the pivot row, columns c .. c+31
+    __shared__ int s_prow, s_pcode, s_stop, s_win;
+
+    const int t = threadIdx.x, lane = t % 32, wid = t / 32;
+    uint32_t rank;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(rank));
+    const int64_t mr = m - k0;
+    const int64_t base = k0 + (int64_t)rank * R;  // absolute row of slot 0
+    const int64_t left = mr - (int64_t)rank * R;
+    const int nloc = (int)(left < 0 ? 0 : (left < R ? left : R));
+    const int stop0 = *info;  // every CTA reads the same value
+    if (rank == 0 && t == 0) moved[2 * LUC_W] = 0;  // count of the ext pairs
+
+    double row[LUR_RPT][LUC_W];
+    bool has[LUR_RPT], act[LUR_RPT];
+    int cur[LUR_RPT], code[LUR_RPT], sl[LUR_RPT];
+#pragma unroll
+    for (int r = 0; r < LUR_RPT; ++r) {
+        sl[r] = t + LUR_NT * r;
+        has[r] = sl[r] < nloc;
+        act[r] = has[r];
+        cur[r] = (int)(base + sl[r]);
+        code[r] = (int)rank * R + sl[r];
+#pragma unroll
+        for (int j = 0; j < LUC_W; ++j)
+            row[r][j] = has[r] && j < w ? A.p[(k0 + j) * A.ld + base + sl[r]] : 0.0;
+    }
+
+    // the best active row of this CTA for column c (its value in register 0)
+    // published in cand[buf] with its values relative to column c
+    auto publish = [&](int c, int buf) {
+        double v = -1.0;
+        int rw = 0x7fffffff, cd = -1;
+#pragma unroll
+        for (int r = 0; r < LUR_RPT; ++r) {
+            const double a = fabs(row[r][0]);
+            if (act[r] && luc_better(a, cur[r], v, rw)) {
+                v = a;
+                rw = cur[r];
+                cd = code[r];
+            }
+        }
+        luc_warp_best(v, rw, cd);
+        if (lane == 0) {
+            red_v[wid] = v;
+            red_r[wid] = rw;
+            red_c[wid] = cd;
+        }
+        __syncthreads();
+        if (wid == 0) {
+            v = lane < LUR_NT / 32 ? red_v[lane] : -1.0;
+            rw = lane < LUR_NT / 32 ? red_r[lane] : 0x7fffffff;
+            cd = lane < LUR_NT / 32 ? red_c[lane] : -1;
+            luc_warp_best(v, rw, cd);
+            if (lane == 0) {
+                cand[buf].v = v;
+                cand[buf].row = rw;
+                cand[buf].code = cd;
+                s_win = cd;
+            }
+        }
+        __syncthreads();
+        const int win = s_win;
+#pragma unroll
+        for (int r = 0; r < LUR_RPT; ++r)
+            if (win >= 0 && win == code[r]) {
+#pragma unroll
+                for (int j = 0; j < LUC_W; ++j)
+                    if (c + j < w) cand[buf].vals[j] = row[r][j];
+            }
+    };
+    publish(0, 0);
+    luc_cluster_sync();  // the candidates of column 0 and all shared memory initialised
+
+    int c = 0;
+#pragma unroll 1
+    for (; c < w; ++c) {
+        const int64_t k = k0 + c;
+        const int buf = c & 1;
+        if (wid == 0) {
+            // warp 0: the CL candidates with their values (one round of
+            // remote loads), the winner, the pivot row into s_u
+            double v = -1.0, vals[LUC_CL];
+            int prow = 0x7fffffff, pc = -1, q = -1;
+            if (lane < LUC_CL) {
+                const uint32_t a = luc_map(&cand[buf], (uint32_t)lane);
+                v = luc_ld_f64(a);
+                prow = luc_ld_s32(a + 8);
+                pc = luc_ld_s32(a + 12);
+                q = lane;
+            }
+#pragma unroll
+            for (int qq = 0; qq < LUC_CL; ++qq)
+                vals[qq] = c + lane < w ? luc_ld_f64(luc_map(&cand[buf].vals[lane], (uint32_t)qq))
+                                        : 0.0;
+            luc_warp_best(v, prow, q);
+            const int qb = q < 0 ? 0 : q;
+            pc = __shfl_sync(0xffffffffu, pc, qb);
+            double u = 0.0;
+#pragma unroll
+            for (int qq = 0; qq < LUC_CL; ++qq) u = qq == qb ? vals[qq] : u;
+            s_u[lane] = c + lane < w ? u : 0.0;
+            if (lane == 0) {
+                s_prow = prow;
+                s_pcode = pc;
+                s_stop = stop0 != 0 || !(v > 0.0);
+                if (rank == 0) {
+                    if (stop0 == 0 && !(v > 0.0)) *info = (int)(k + 1);
+                    if (stop0 == 0 && v > 0.0) ipiv[k] = (int64_t)prow + 1;
+                }
+            }
+        }
+        __syncthreads();
+        if (s_stop) break;  // the same decision in every CTA
+        const int prow = s_prow, pcode = s_pcode;
+        const double ivp = 1.0 / s_u[0];
+#pragma unroll
+        for (int r = 0; r < LUR_RPT; ++r) {
+            if (!has[r]) continue;
+            if (code[r] == pcode) {
+                // the pivot row: its remaining values are final (the U row)
+#pragma unroll
+                for (int j = 0; j < LUC_W; ++j)
+                    if (c + j < w) fin[(size_t)(c + j) * R + sl[r]] = row[r][j];
+                cur[r] = (int)k;
+            } else if (cur[r] == k) {
+                cur[r] = prow;  // the row the pivot row displaces
+            }
+            act[r] = cur[r] > k;  // the pivot rows so far are final
+        }
+        double l[LUR_RPT];
+#pragma unroll
+        for (int r = 0; r < LUR_RPT; ++r) {
+            l[r] = row[r][0] * ivp;
+            if (act[r]) fin[(size_t)c * R + sl[r]] = l[r];
+        }
+        // register j <- column c+1+j (rows that are no longer active compute
+        // values that are never used)
+#pragma unroll
+        for (int j = 0; j < LUC_W - 1; ++j) {
+            const double uj = s_u[j + 1];
+#pragma unroll
+            for (int r = 0; r < LUR_RPT; ++r) row[r][j] = fma(-l[r], uj, row[r][j + 1]);
+        }
+#pragma unroll
+        for (int r = 0; r < LUR_RPT; ++r) row[r][LUC_W - 1] = 0.0;
+        if (c + 1 < w) publish(c + 1, buf ^ 1);  // its barriers order this step's reads
+        else __syncthreads();
+        luc_cluster_sync();  // next candidates published; this step's remote reads done
+    }
+    // a singular column stops the panel: the active rows keep their current
+    // values from column c on
+    if (c < w) {
+#pragma unroll
+        for (int r = 0; r < LUR_RPT; ++r)
+            if (act[r]) {
+#pragma unroll
+                for (int j = 0; j < LUC_W; ++j)
+                    if (c + j < w) fin[(size_t)(c + j) * R + sl[r]] = row[r][j];
+            }
+    }
+    luc_cluster_sync();  // no CTA leaves while another may still read its shared memory
+    // write the panel back, every slot's row at its final position, and list
+    // the moved rows
+#pragma unroll
+    for (int r = 0; r < LUR_RPT; ++r) {
+        if (!has[r]) continue;
+        for (int j = 0; j < w; ++j) A.p[(k0 + j) * A.ld + cur[r]] = fin[(size_t)j * R + sl[r]];
+        const int orig = (int)(base + sl[r]);
+        if (cur[r] < k0 + w) {
+            moved[cur[r] - k0] = orig;
+        } else if (cur[r] != orig) {
+            const int e = atomicAdd(&moved[2 * LUC_W], 1);
+            moved[LUC_W + e] = cur[r];            // ext rows
+            moved[2 * LUC_W + 1 + e] = orig;      // ext sources
+        }
+    }
+}
+
 // The panel's interchanges (ipiv[k0 .. k0+w), ascending, as sequential
 // swaps) applied to every column outside the panel and, right of it, the
 // block row U12 = inv(L11) A12 (L11 the panel's unit-lower w x w block): one
@@ -673,8 +881,9 @@ __global__ void __launch_bounds__(32 * LUS_WARPS)
     }
 }
 
-// panel width nb (4..32): a panel of up to about 6000 rows lives in the
-// shared memory of an 8-CTA cluster (lu64_cluster_panel_kernel); a taller
+// panel width nb (4..32): a panel of up to 4096 rows lives in the registers
+// of an 8-CTA cluster (lu64_cluster_panel_reg_kernel), one of up to about
+// 6000 rows in its shared memory (lu64_cluster_panel_kernel); a taller
 // one streams through one CTA (lu64_panel_kernel, whose traffic grows with
 // the width); the U block row (TRSM) and the trailing update (FP64 GEMM)
 // follow each panel
@@ -700,6 +909,10 @@ static int getrf64_fast(mflab_handle *h, int64_t m, int64_t n, Mat A, int64_t *i
     rc = set_smem_once((const void *)lu64_cluster_panel_kernel, LUC_SMEM_MAX, luc_configured,
                        "lu64 cluster panel attribute");
     if (rc) return rc;
+    static std::atomic<unsigned long long> lur_configured{0};
+    rc = set_smem_once((const void *)lu64_cluster_panel_reg_kernel, LUC_SMEM_MAX, lur_configured,
+                       "lu64 register panel attribute");
+    if (rc) return rc;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -710,7 +923,10 @@ static int getrf64_fast(mflab_handle *h, int64_t m, int64_t n, Mat A, int64_t *i
         const int64_t mr = m - k0, R = (mr + LUC_CL - 1) / LUC_CL;
         const size_t smem = luc_smem(R, mr);
         const bool cluster = smem <= (size_t)LUC_SMEM_MAX && R <= 0x7fffffff;
-        if (cluster)
+        if (cluster && R <= LUR_NT * LUR_RPT && lur_smem(R) <= (size_t)LUC_SMEM_MAX)
+            lu64_cluster_panel_reg_kernel<<<LUC_CL, LUR_NT, lur_smem(R), s>>>(
+                m, A, k0, w, (int)R, ipiv, info, moved);
+        else if (cluster)
             lu64_cluster_panel_kernel<<<LUC_CL, LUC_NT, smem, s>>>(m, A, k0, w, (int)R, ipiv,
                                                                    info, moved);
         else
