@@ -60,6 +60,8 @@ extern "C" int mflab_create(mflab_handle **out, int device) {
     h->stage = nullptr;
     h->il_stream[0] = h->il_stream[1] = nullptr;
     h->il_fork = h->il_done[0] = h->il_done[1] = nullptr;
+    h->la_stream = nullptr;
+    h->la_ev[0] = h->la_ev[1] = h->la_ev[2] = nullptr;
     e = cudaMalloc((void **)&h->dev_flags, 64 * sizeof(int));
     if (e != cudaSuccess) {
         delete h;
@@ -83,6 +85,9 @@ extern "C" int mflab_destroy(mflab_handle *h) {
         if (h->il_done[i]) cudaEventDestroy(h->il_done[i]);
     }
     if (h->il_fork) cudaEventDestroy(h->il_fork);
+    if (h->la_stream) cudaStreamDestroy(h->la_stream);
+    for (int i = 0; i < 3; ++i)
+        if (h->la_ev[i]) cudaEventDestroy(h->la_ev[i]);
     if (h->dev_flags) cudaFree(h->dev_flags);
     delete h;
     return MFLAB_OK;

@@ -425,6 +425,22 @@ __device__ __forceinline__ void luc_warp_best(double &v, int &row, int &code) {
     }
 }
 
+// best of (v, row, code) over lanes 0 .. 7 (the other lanes hold no entry):
+// three exchange rounds
+__device__ __forceinline__ void luc_best8(double &v, int &row, int &code) {
+#pragma unroll
+    for (int off = 4; off > 0; off >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, v, off);
+        const int orow = __shfl_xor_sync(0xffffffffu, row, off);
+        const int ocode = __shfl_xor_sync(0xffffffffu, code, off);
+        if (luc_better(ov, orow, v, row)) {
+            v = ov;
+            row = orow;
+            code = ocode;
+        }
+    }
+}
+
 // shared memory of the cluster panel kernel for R rows per CTA and mr panel rows
 __host__ __device__ inline size_t luc_smem(int64_t R, int64_t mr) {
     return (size_t)R * LUC_W * sizeof(double) + (size_t)R * sizeof(int) +
@@ -620,8 +636,10 @@ __global__ void __cluster_dims__(LUC_CL, 1, 1) __launch_bounds__(LUR_NT, 1)
     LucCand *cand = (LucCand *)(((uintptr_t)(fin + (size_t)LUC_W * R) + 15) & ~(uintptr_t)15);
     __shared__ double red_v[LUR_NT / 32];
     __shared__ int red_r[LUR_NT / 32], red_c[LUR_NT / 32];
-    __shared__ double s_u[LUC_W];  // the pivot row, columns c .. c+31
-    __shared__ int s_prow, s_pcode, s_stop, s_win;
+    __shared__ double wstage[LUR_NT / 32][LUC_W];  // each warp's best row
+    __shared__ __align__(16) double s_u[LUC_W];    // the pivot row, columns c+1 .. c+32
+    __shared__ double s_ivp;                       // 1 / pivot
+    __shared__ int s_prow, s_pcode, s_stop;
 
     const int t = threadIdx.x, lane = t % 32, wid = t / 32;
     uint32_t rank;
@@ -649,7 +667,9 @@ __global__ void __cluster_dims__(LUC_CL, 1, 1) __launch_bounds__(LUR_NT, 1)
     }
 
     // the best active row of this CTA for column c (its value in register 0)
-    // published in cand[buf] with its values relative to column c
+    // published in cand[buf] with its values relative to column c: the best
+    // row of each warp stages its values, warp 0 picks the CTA's best and
+    // copies that warp's stage
     auto publish = [&](int c, int buf) {
         double v = -1.0;
         int rw = 0x7fffffff, cd = -1;
@@ -663,6 +683,13 @@ __global__ void __cluster_dims__(LUC_CL, 1, 1) __launch_bounds__(LUR_NT, 1)
             }
         }
         luc_warp_best(v, rw, cd);
+#pragma unroll
+        for (int r = 0; r < LUR_RPT; ++r)
+            if (cd >= 0 && cd == code[r]) {
+#pragma unroll
+                for (int j = 0; j < LUC_W; ++j)
+                    if (c + j < w) wstage[wid][j] = row[r][j];
+            }
         if (lane == 0) {
             red_v[wid] = v;
             red_r[wid] = rw;
@@ -673,23 +700,32 @@ __global__ void __cluster_dims__(LUC_CL, 1, 1) __launch_bounds__(LUR_NT, 1)
             v = lane < LUR_NT / 32 ? red_v[lane] : -1.0;
             rw = lane < LUR_NT / 32 ? red_r[lane] : 0x7fffffff;
             cd = lane < LUR_NT / 32 ? red_c[lane] : -1;
-            luc_warp_best(v, rw, cd);
+            int bw = lane;
+            static_assert(LUR_NT / 32 == 8, "three rounds reduce the warps' bests");
+#pragma unroll
+            for (int off = 4; off > 0; off >>= 1) {
+                const double ov = __shfl_xor_sync(0xffffffffu, v, off);
+                const int orow = __shfl_xor_sync(0xffffffffu, rw, off);
+                const int ocd = __shfl_xor_sync(0xffffffffu, cd, off);
+                const int obw = __shfl_xor_sync(0xffffffffu, bw, off);
+                if (luc_better(ov, orow, v, rw)) {
+                    v = ov;
+                    rw = orow;
+                    cd = ocd;
+                    bw = obw;
+                }
+            }
+            v = __shfl_sync(0xffffffffu, v, 0);
+            rw = __shfl_sync(0xffffffffu, rw, 0);
+            cd = __shfl_sync(0xffffffffu, cd, 0);
+            bw = __shfl_sync(0xffffffffu, bw, 0);
             if (lane == 0) {
                 cand[buf].v = v;
                 cand[buf].row = rw;
                 cand[buf].code = cd;
-                s_win = cd;
             }
+            if (cd >= 0 && c + lane < w) cand[buf].vals[lane] = wstage[bw][lane];
         }
-        __syncthreads();
-        const int win = s_win;
-#pragma unroll
-        for (int r = 0; r < LUR_RPT; ++r)
-            if (win >= 0 && win == code[r]) {
-#pragma unroll
-                for (int j = 0; j < LUC_W; ++j)
-                    if (c + j < w) cand[buf].vals[j] = row[r][j];
-            }
     };
     publish(0, 0);
     luc_cluster_sync();  // the candidates of column 0 and all shared memory initialised
@@ -715,14 +751,21 @@ __global__ void __cluster_dims__(LUC_CL, 1, 1) __launch_bounds__(LUR_NT, 1)
             for (int qq = 0; qq < LUC_CL; ++qq)
                 vals[qq] = c + lane < w ? luc_ld_f64(luc_map(&cand[buf].vals[lane], (uint32_t)qq))
                                         : 0.0;
-            luc_warp_best(v, prow, q);
+            static_assert(LUC_CL == 8, "three rounds reduce the CTAs' candidates");
+            luc_best8(v, prow, q);
+            v = __shfl_sync(0xffffffffu, v, 0);
+            prow = __shfl_sync(0xffffffffu, prow, 0);
+            q = __shfl_sync(0xffffffffu, q, 0);
             const int qb = q < 0 ? 0 : q;
             pc = __shfl_sync(0xffffffffu, pc, qb);
             double u = 0.0;
 #pragma unroll
             for (int qq = 0; qq < LUC_CL; ++qq) u = qq == qb ? vals[qq] : u;
-            s_u[lane] = c + lane < w ? u : 0.0;
+            // s_u[j] = column c+1+j, 16-byte pairs for the update's loads
+            if (lane > 0) s_u[lane - 1] = c + lane < w ? u : 0.0;
+            if (lane == 31) s_u[31] = 0.0;
             if (lane == 0) {
+                s_ivp = 1.0 / u;
                 s_prow = prow;
                 s_pcode = pc;
                 s_stop = stop0 != 0 || !(v > 0.0);
@@ -735,7 +778,7 @@ __global__ void __cluster_dims__(LUC_CL, 1, 1) __launch_bounds__(LUR_NT, 1)
         __syncthreads();
         if (s_stop) break;  // the same decision in every CTA
         const int prow = s_prow, pcode = s_pcode;
-        const double ivp = 1.0 / s_u[0];
+        const double ivp = s_ivp;
 #pragma unroll
         for (int r = 0; r < LUR_RPT; ++r) {
             if (!has[r]) continue;
@@ -759,14 +802,17 @@ __global__ void __cluster_dims__(LUC_CL, 1, 1) __launch_bounds__(LUR_NT, 1)
         // register j <- column c+1+j (rows that are no longer active compute
         // values that are never used)
 #pragma unroll
-        for (int j = 0; j < LUC_W - 1; ++j) {
-            const double uj = s_u[j + 1];
+        for (int j = 0; j < LUC_W - 1; j += 2) {
+            const double2 uj = *(const double2 *)&s_u[j];
 #pragma unroll
-            for (int r = 0; r < LUR_RPT; ++r) row[r][j] = fma(-l[r], uj, row[r][j + 1]);
+            for (int r = 0; r < LUR_RPT; ++r) {
+                row[r][j] = fma(-l[r], uj.x, row[r][j + 1]);
+                if (j + 2 < LUC_W) row[r][j + 1] = fma(-l[r], uj.y, row[r][j + 2]);
+            }
         }
 #pragma unroll
         for (int r = 0; r < LUR_RPT; ++r) row[r][LUC_W - 1] = 0.0;
-        if (c + 1 < w) publish(c + 1, buf ^ 1);  // its barriers order this step's reads
+        if (c + 1 < w) publish(c + 1, buf ^ 1);  // its barrier orders this step's reads
         else __syncthreads();
         luc_cluster_sync();  // next candidates published; this step's remote reads done
     }
@@ -800,7 +846,7 @@ __global__ void __cluster_dims__(LUC_CL, 1, 1) __launch_bounds__(LUR_NT, 1)
 }
 
 // The panel's interchanges (ipiv[k0 .. k0+w), ascending, as sequential
-// swaps) applied to every column outside the panel and, right of it, the
+// swaps) applied to the columns c_lo .. c_hi-1 outside the panel and, right of it, the
 // block row U12 = inv(L11) A12 (L11 the panel's unit-lower w x w block): one
 // warp per column.  The swaps permute the at most 2w rows involved (rows
 // k0 .. k0+w-1 and the pivot rows below them): `moved` lists, for each, the
@@ -812,8 +858,8 @@ __global__ void __cluster_dims__(LUC_CL, 1, 1) __launch_bounds__(LUR_NT, 1)
 constexpr int LUS_WARPS = 8;
 
 __global__ void __launch_bounds__(32 * LUS_WARPS)
-    lu64_swap_trsm_kernel(int64_t n, Mat A, int64_t k0, int w, const int64_t *ipiv,
-                          const int *moved, const int *info) {
+    lu64_swap_trsm_kernel(int64_t c_lo, int64_t c_hi, Mat A, int64_t k0, int w,
+                          const int64_t *ipiv, const int *moved, const int *info) {
     if (*info) return;
     __shared__ int rows[2 * LUC_W], src[2 * LUC_W], cnt_s;
     __shared__ double L[LUC_W][LUC_W + 1];
@@ -861,9 +907,9 @@ __global__ void __launch_bounds__(32 * LUS_WARPS)
     const int r0 = rows[lane], s0 = src[lane];
     const bool two = lane + 32 < cnt;
     const int r1 = two ? rows[lane + 32] : 0, s1 = two ? src[lane + 32] : 0;
-    for (int64_t col = (int64_t)blockIdx.x * LUS_WARPS + warp; col < n - w;
-         col += (int64_t)gridDim.x * LUS_WARPS) {
-        const int64_t c = col < k0 ? col : col + w;
+    // the columns c_lo .. c_hi-1 (a range on one side of the panel)
+    for (int64_t c = c_lo + (int64_t)blockIdx.x * LUS_WARPS + warp; c < c_hi;
+         c += (int64_t)gridDim.x * LUS_WARPS) {
         double *x = A.p + c * A.ld;
         // gather the involved rows (all reads before any write of this column)
         double v0 = lane < cnt ? x[s0] : 0.0;
@@ -881,15 +927,64 @@ __global__ void __launch_bounds__(32 * LUS_WARPS)
     }
 }
 
+// swaps (and, right of the panel, the U block row) on columns [c_lo, c_hi)
+static int lu64_swap_cols(int64_t c_lo, int64_t c_hi, Mat A, int64_t k0, int w,
+                          const int64_t *ipiv, const int *moved, const int *info, int sms,
+                          cudaStream_t s) {
+    if (c_hi <= c_lo) return MFLAB_OK;
+    const int64_t grid = std::min<int64_t>((c_hi - c_lo + LUS_WARPS - 1) / LUS_WARPS, 4 * sms);
+    lu64_swap_trsm_kernel<<<(unsigned)grid, 32 * LUS_WARPS, 0, s>>>(c_lo, c_hi, A, k0, w, ipiv,
+                                                                    moved, info);
+    return record_cuda_error(cudaGetLastError(), "getrf64 swap + trsm");
+}
+
+// A[r0:m, c_lo:c_hi] -= L21 U12 of the panel at k0 (width w; r0 = k0 + w)
+static int lu64_trailing(mflab_handle *h, int64_t m, int64_t c_lo, int64_t c_hi, Mat A,
+                         int64_t k0, int w, void *ws, size_t wsb, const int *info,
+                         cudaStream_t s) {
+    const int64_t r0 = k0 + w;
+    if (c_hi <= c_lo || r0 >= m) return MFLAB_OK;
+    const double mone[1] = {-1.0}, one[1] = {1.0};
+    // a plain binary64 GEMM (the factor has no reference order to keep); a
+    // zero pivot stops the panels, and the updates after it only touch a
+    // failed factor
+    int rc = dgemm_lt(m - r0, c_hi - c_lo, w, A.p + k0 * A.ld + r0, A.ld,
+                      A.p + c_lo * A.ld + k0, A.ld, A.p + c_lo * A.ld + r0, A.ld, -1.0, 1.0,
+                      ws, wsb, s);
+    if (rc == MFLAB_ERR_UNSUPPORTED)  // no library algorithm: the device kernel
+        rc = launch_mm(1, false, false, 0, false, m - r0, c_hi - c_lo, w, A.at(r0, k0),
+                       A.at(k0, c_lo), A.at(r0, c_lo), mone, one, s, info);
+    return rc;
+}
+
+// the high-priority stream and the events of the look-ahead factor
+static int lu64_lookahead_streams(mflab_handle *h) {
+    cudaError_t e = cudaSuccess;
+    if (!h->la_stream) {
+        int lo = 0, hi = 0;
+        e = cudaDeviceGetStreamPriorityRange(&lo, &hi);
+        if (e == cudaSuccess)
+            e = cudaStreamCreateWithPriority(&h->la_stream, cudaStreamNonBlocking, hi);
+    }
+    for (int i = 0; i < 3 && e == cudaSuccess; ++i)
+        if (!h->la_ev[i]) e = cudaEventCreateWithFlags(&h->la_ev[i], cudaEventDisableTiming);
+    return e == cudaSuccess ? MFLAB_OK : record_cuda_error(e, "getrf64 streams");
+}
+
 // panel width nb (4..32): a panel of up to 4096 rows lives in the registers
 // of an 8-CTA cluster (lu64_cluster_panel_reg_kernel), one of up to about
 // 6000 rows in its shared memory (lu64_cluster_panel_kernel); a taller
 // one streams through one CTA (lu64_panel_kernel, whose traffic grows with
-// the width); the U block row (TRSM) and the trailing update (FP64 GEMM)
-// follow each panel
+// the width).  Look-ahead over two streams: panel p, then the interchanges,
+// U block and trailing update of the next panel's columns run on a
+// high-priority stream (the panel's critical path), while the interchanges,
+// U block and trailing update of all other columns run on the caller's
+// stream, overlapping panel p+1.  Step p's next-panel work waits for step
+// p-1's other work (which updated those columns); step p's other work waits
+// for panel p.  The two moved-row lists and the two GEMM workspaces alternate
+// or belong to one stream each, so no buffer is shared by work in flight.
 static int getrf64_fast(mflab_handle *h, int64_t m, int64_t n, Mat A, int64_t *ipiv, int *info,
                         cudaStream_t s, int nb) {
-    const double mone[1] = {-1.0}, one[1] = {1.0};
     cudaError_t e = cudaMemsetAsync(info, 0, sizeof(int), s);
     if (e != cudaSuccess) return record_cuda_error(e, "getrf info");
     const int64_t kmax = m < n ? m : n;
@@ -898,12 +993,14 @@ static int getrf64_fast(mflab_handle *h, int64_t m, int64_t n, Mat A, int64_t *i
     nonfinite_kernel<1><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(m, n, A, 0, info);
     int rc = record_cuda_error(cudaGetLastError(), "getrf check");
     if (rc) return rc;
-    // workspace of the library's binary64 GEMM (the trailing updates), then
-    // the moved-row list of the cluster panel
-    const size_t wsb = (size_t)32 << 20;
-    rc = mflab_reserve_scratch(h, wsb + 4 * LUC_W * sizeof(int));
+    // two workspaces of the library's binary64 GEMM (one per stream), then
+    // two moved-row lists of the cluster panel (alternating panels)
+    const size_t wsb = (size_t)32 << 20, mvb = 4 * LUC_W * sizeof(int);
+    rc = mflab_reserve_scratch(h, 2 * wsb + 2 * mvb);
     if (rc) return rc;
-    int *moved = (int *)((char *)h->scratch + wsb);
+    void *ws[2] = {h->scratch, (char *)h->scratch + wsb};
+    int *movedb[2] = {(int *)((char *)h->scratch + 2 * wsb),
+                      (int *)((char *)h->scratch + 2 * wsb + mvb)};
     const int NB = nb < 4 ? 4 : (nb > LUC_W ? LUC_W : nb);
     static std::atomic<unsigned long long> luc_configured{0};
     rc = set_smem_once((const void *)lu64_cluster_panel_kernel, LUC_SMEM_MAX, luc_configured,
@@ -913,53 +1010,61 @@ static int getrf64_fast(mflab_handle *h, int64_t m, int64_t n, Mat A, int64_t *i
     rc = set_smem_once((const void *)lu64_cluster_panel_reg_kernel, LUC_SMEM_MAX, lur_configured,
                        "lu64 register panel attribute");
     if (rc) return rc;
+    rc = lu64_lookahead_streams(h);
+    if (rc) return rc;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    for (int64_t k0 = 0; k0 < kmax; k0 += NB) {
+    cudaStream_t sp = h->la_stream;  // the panels' stream
+    cudaEvent_t ev_fork = h->la_ev[0], ev_panel = h->la_ev[1], ev_rest = h->la_ev[2];
+    e = cudaEventRecord(ev_fork, s);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(sp, ev_fork, 0);
+    if (e != cudaSuccess) return record_cuda_error(e, "getrf64 fork");
+    int p = 0;
+    for (int64_t k0 = 0; k0 < kmax && rc == MFLAB_OK; k0 += NB, ++p) {
         const int w = (int)(kmax - k0 < NB ? kmax - k0 : NB);
-        // the panel in a cluster's shared memory when it fits, else streamed
-        // through one CTA
+        int *moved = movedb[p & 1];
+        // the panel in a cluster's registers or shared memory when it fits,
+        // else streamed through one CTA
         const int64_t mr = m - k0, R = (mr + LUC_CL - 1) / LUC_CL;
         const size_t smem = luc_smem(R, mr);
         const bool cluster = smem <= (size_t)LUC_SMEM_MAX && R <= 0x7fffffff;
         if (cluster && R <= LUR_NT * LUR_RPT && lur_smem(R) <= (size_t)LUC_SMEM_MAX)
-            lu64_cluster_panel_reg_kernel<<<LUC_CL, LUR_NT, lur_smem(R), s>>>(
+            lu64_cluster_panel_reg_kernel<<<LUC_CL, LUR_NT, lur_smem(R), sp>>>(
                 m, A, k0, w, (int)R, ipiv, info, moved);
         else if (cluster)
-            lu64_cluster_panel_kernel<<<LUC_CL, LUC_NT, smem, s>>>(m, A, k0, w, (int)R, ipiv,
-                                                                   info, moved);
+            lu64_cluster_panel_kernel<<<LUC_CL, LUC_NT, smem, sp>>>(m, A, k0, w, (int)R, ipiv,
+                                                                    info, moved);
         else
-            lu64_panel_kernel<<<1, LU64_NT, 0, s>>>(m, A, k0, w, ipiv, info);
+            lu64_panel_kernel<<<1, LU64_NT, 0, sp>>>(m, A, k0, w, ipiv, info);
         rc = record_cuda_error(cudaGetLastError(), "getrf64 panel");
-        if (rc) return rc;
-        // interchanges outside the panel and the U block row right of it
-        if (n > w) {
-            const int64_t cols = n - w;
-            const int64_t grid = std::min<int64_t>((cols + LUS_WARPS - 1) / LUS_WARPS, 4 * sms);
-            lu64_swap_trsm_kernel<<<(unsigned)grid, 32 * LUS_WARPS, 0, s>>>(
-                n, A, k0, w, ipiv, cluster ? moved : nullptr, info);
-            rc = record_cuda_error(cudaGetLastError(), "getrf64 swap + trsm");
-            if (rc) return rc;
-        }
-        const int64_t last = k0 + w - 1;
-        if (last < n - 1 && last < m - 1) {
-            // A22 -= L21 U12 (a plain binary64 GEMM; the factor has no
-            // reference order to keep).  A zero pivot stops the panels, and
-            // the updates after it only touch a failed factor.
-            rc = dgemm_lt(m - 1 - last, n - 1 - last, w, A.p + k0 * A.ld + last + 1, A.ld,
-                          A.p + (last + 1) * A.ld + k0, A.ld,
-                          A.p + (last + 1) * A.ld + last + 1, A.ld, -1.0, 1.0, h->scratch, wsb,
-                          s);
-            if (rc == MFLAB_ERR_UNSUPPORTED)  // no library algorithm: the device kernel
-                rc = launch_mm(1, false, false, 0, false, m - 1 - last, n - 1 - last, w,
-                               A.at(last + 1, k0), A.at(k0, last + 1), A.at(last + 1, last + 1),
-                               mone, one, s, info);
-            if (rc) return rc;
+        if (rc) break;
+        const int *mv = cluster ? moved : nullptr;
+        e = cudaEventRecord(ev_panel, sp);
+        // the next panel's columns, on the panels' stream, after the other
+        // work of the previous step
+        const int64_t nx0 = k0 + w, nx1 = std::min<int64_t>(n, nx0 + NB);
+        if (e == cudaSuccess && p > 0) e = cudaStreamWaitEvent(sp, ev_rest, 0);
+        if (e != cudaSuccess) return record_cuda_error(e, "getrf64 look-ahead");
+        rc = lu64_swap_cols(nx0, nx1, A, k0, w, ipiv, mv, info, sms, sp);
+        if (!rc) rc = lu64_trailing(h, m, nx0, nx1, A, k0, w, ws[0], wsb, info, sp);
+        if (rc) break;
+        // every other column, on the caller's stream, after the panel
+        e = cudaStreamWaitEvent(s, ev_panel, 0);
+        if (e != cudaSuccess) return record_cuda_error(e, "getrf64 look-ahead");
+        rc = lu64_swap_cols(0, k0, A, k0, w, ipiv, mv, info, sms, s);
+        if (!rc) rc = lu64_swap_cols(nx1, n, A, k0, w, ipiv, mv, info, sms, s);
+        if (!rc) rc = lu64_trailing(h, m, nx1, n, A, k0, w, ws[1], wsb, info, s);
+        if (!rc) {
+            e = cudaEventRecord(ev_rest, s);
+            if (e != cudaSuccess) rc = record_cuda_error(e, "getrf64 look-ahead");
         }
     }
-    (void)one;
-    return MFLAB_OK;
+    // join: the caller's stream waits for the panels' stream
+    e = cudaEventRecord(ev_fork, sp);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s, ev_fork, 0);
+    if (e != cudaSuccess && rc == MFLAB_OK) rc = record_cuda_error(e, "getrf64 join");
+    return rc;
 }
 
 template <int N>

@@ -166,6 +166,10 @@ struct mflab_handle {
     void *stage;
     cudaStream_t il_stream[2];
     cudaEvent_t il_fork, il_done[2];
+    // the high-priority panel stream of the look-ahead binary64 LU and its
+    // events (fork/join, panel done, other columns done), on first use
+    cudaStream_t la_stream;
+    cudaEvent_t la_ev[3];
 };
 
 int mflab_reserve_aux(mflab_handle *h, size_t bytes);
