@@ -425,8 +425,8 @@ __device__ __forceinline__ void luc_warp_best(double &v, int &row, int &code) {
     }
 }
 
-// best of (v, row, code) over lanes 0 .. 7 (the other lanes hold no entry):
-// three exchange rounds
+// best of (v, row, code) over lanes 0 .. 7 (the other lanes hold no entry),
+// in every lane: three exchange rounds and a broadcast
 __device__ __forceinline__ void luc_best8(double &v, int &row, int &code) {
 #pragma unroll
     for (int off = 4; off > 0; off >>= 1) {
@@ -439,6 +439,9 @@ __device__ __forceinline__ void luc_best8(double &v, int &row, int &code) {
             code = ocode;
         }
     }
+    v = __shfl_sync(0xffffffffu, v, 0);
+    row = __shfl_sync(0xffffffffu, row, 0);
+    code = __shfl_sync(0xffffffffu, code, 0);
 }
 
 // shared memory of the cluster panel kernel for R rows per CTA and mr panel rows
@@ -615,31 +618,118 @@ __global__ void __cluster_dims__(LUC_CL, 1, 1) __launch_bounds__(LUC_NT, 1)
 // on the column (the column loop stays rolled and its code small).  Every
 // final value goes to shared memory when it is formed — the multiplier of
 // an active row at its column, the whole remaining row of the pivot when it
-// is chosen — and the panel is written back from there.  Pivot rule, logical
-// interchanges (the slot holding row k recognises itself by its current row)
-// and the moved-row list are those of lu64_cluster_panel_kernel; candidates
-// and the pivot row's values are published relative to their column, the
-// CTA's winning thread writing its row after the CTA reduction.
+// is chosen — and the panel is written back from there.
+//
+// The CTAs exchange candidates by pushing, not by a cluster barrier: after
+// its CTA reduction, warp 0 of every CTA writes its best row (value, row,
+// code and the row's values from the candidate column on) into its slot of
+// every CTA's receive buffer with st.async, whose bytes complete on the
+// receiver's mbarrier.  A step waits (bounded) for the 8 x 272 bytes of its
+// buffer, and every warp then reads the 8 candidates from its own shared
+// memory.  Two buffers alternate: a CTA pushes step c+2 only after it has
+// all candidates of step c+1, which every CTA sends after its warps finished
+// reading step c.  Pivot rule (largest magnitude, ties to the smallest
+// row), logical interchanges (the slot holding row k recognises itself by
+// its current row) and the moved-row list are those of
+// lu64_cluster_panel_kernel.  A wait that runs out sets a shared abort flag
+// and records TC-style error code 5 in *err; the CTA leaves the loop after
+// its next CTA barrier, and the others, no longer receiving, time out too.
 constexpr int LUR_NT = 256, LUR_RPT = 2;
+constexpr uint32_t LUR_SLOT_TX = 16 + 8 + 32 * 8;  // bytes pushed per sender (header, u0, u)
+constexpr long long LUR_WAIT_LIMIT = 1LL << 26;
+constexpr int LUR_ERR_TIMEOUT = 5;
+
+struct LurSlot {
+    double v;       // |A[row, c]| of the candidate, -1 for none
+    int row;        // its current row
+    int code;       // owner CTA * R + slot
+    double u0;      // A[row, c]
+    double pad;
+    double u[32];   // A[row, c + 1 + j], j < 31 (u[31] is zero)
+};
+struct LurRecv {
+    LurSlot slot[LUC_CL];
+};
 
 // shared memory of the register panel kernel: the final values [w][R], two
-// candidates
+// receive buffers, two mbarriers
 __host__ __device__ inline size_t lur_smem(int64_t R) {
-    return (size_t)LUC_W * R * sizeof(double) + 2 * sizeof(LucCand) + 64;
+    return (size_t)LUC_W * R * sizeof(double) + 2 * sizeof(LurRecv) + 2 * sizeof(uint64_t) + 64;
+}
+
+// Warp-wide first-largest entry (largest v, ties to the smallest row; v < 0
+// marks a lane without an entry, whose row is 0x7fffffff and code -1), in
+// every lane, from three warp reductions of 32-bit keys: the high and low
+// words of v's bits (ordered like v for v >= 0), then the smallest row among
+// the lanes holding the maximum.
+__device__ __forceinline__ void lur_warp_best(double &v, int &row, int &code) {
+    const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+    const unsigned hi = v >= 0.0 ? (unsigned)(b >> 32) + 1u : 0u;
+    const unsigned m1 = __reduce_max_sync(0xffffffffu, hi);
+    const unsigned lo = hi == m1 ? (unsigned)b : 0u;
+    const unsigned m2 = __reduce_max_sync(0xffffffffu, lo);
+    const bool tie = hi == m1 && (unsigned)b == m2;
+    const unsigned m3 = __reduce_min_sync(0xffffffffu, tie ? (unsigned)row : 0xffffffffu);
+    const unsigned win = __ballot_sync(0xffffffffu, tie && (unsigned)row == m3);
+    code = __shfl_sync(0xffffffffu, code, __ffs(win) - 1);
+    row = (int)m3;
+    v = m1 == 0u ? -1.0
+                 : __longlong_as_double((long long)(((unsigned long long)(m1 - 1u) << 32) | m2));
+}
+
+__device__ __forceinline__ void lur_push_f64(uint32_t raddr, double v, uint32_t rbar) {
+    asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.f64 [%0], %1, [%2];" ::"r"(
+                     raddr),
+                 "d"(v), "r"(rbar)
+                 : "memory");
+}
+__device__ __forceinline__ void lur_push_v2b64(uint32_t raddr, unsigned long long a,
+                                               unsigned long long b, uint32_t rbar) {
+    asm volatile(
+        "st.async.shared::cluster.mbarrier::complete_tx::bytes.v2.b64 [%0], {%1, %2}, [%3];" ::"r"(
+            raddr),
+        "l"(a), "l"(b), "r"(rbar)
+        : "memory");
+}
+__device__ __forceinline__ void lur_mbar_init(uint64_t *bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"((uint32_t)__cvta_generic_to_shared(
+                     bar))
+                 : "memory");
+}
+__device__ __forceinline__ void lur_arm(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
+                     (uint32_t)__cvta_generic_to_shared(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool lur_wait(uint64_t *bar, uint32_t parity, const int *abort) {
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(bar);
+    for (long long i = 0; i < LUR_WAIT_LIMIT; ++i) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred P1;\n\t"
+            "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 P1, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, P1;\n\t}"
+            : "=r"(ok)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (ok) return true;
+        if (*(const volatile int *)abort) return false;
+    }
+    return false;
 }
 
 __global__ void __cluster_dims__(LUC_CL, 1, 1) __launch_bounds__(LUR_NT, 1)
     lu64_cluster_panel_reg_kernel(int64_t m, Mat A, int64_t k0, int w, int R, int64_t *ipiv,
-                                  int *info, int *moved) {
+                                  int *info, int *moved, int *err) {
     extern __shared__ __align__(16) uint8_t lur_raw[];
     double *fin = (double *)lur_raw;  // [w][R] final values
-    LucCand *cand = (LucCand *)(((uintptr_t)(fin + (size_t)LUC_W * R) + 15) & ~(uintptr_t)15);
+    LurRecv *recv = (LurRecv *)(fin + (size_t)LUC_W * R);  // [2]
+    uint64_t *rbar = (uint64_t *)(recv + 2);               // [2]
     __shared__ double red_v[LUR_NT / 32];
     __shared__ int red_r[LUR_NT / 32], red_c[LUR_NT / 32];
-    __shared__ double wstage[LUR_NT / 32][LUC_W];  // each warp's best row
-    __shared__ __align__(16) double s_u[LUC_W];    // the pivot row, columns c+1 .. c+32
-    __shared__ double s_ivp;                       // 1 / pivot
-    __shared__ int s_prow, s_pcode, s_stop;
+    __shared__ __align__(16) double wstage[LUR_NT / 32][LUC_W];  // each warp's best row
+    __shared__ int s_abort, s_stop;
 
     const int t = threadIdx.x, lane = t % 32, wid = t / 32;
     uint32_t rank;
@@ -650,6 +740,15 @@ __global__ void __cluster_dims__(LUC_CL, 1, 1) __launch_bounds__(LUR_NT, 1)
     const int nloc = (int)(left < 0 ? 0 : (left < R ? left : R));
     const int stop0 = *info;  // every CTA reads the same value
     if (rank == 0 && t == 0) moved[2 * LUC_W] = 0;  // count of the ext pairs
+    if (t == 0) {
+        s_abort = 0;
+        s_stop = 0;
+        lur_mbar_init(&rbar[0]);
+        lur_mbar_init(&rbar[1]);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        lur_arm(&rbar[0], LUC_CL * LUR_SLOT_TX);
+        lur_arm(&rbar[1], LUC_CL * LUR_SLOT_TX);
+    }
 
     double row[LUR_RPT][LUC_W];
     bool has[LUR_RPT], act[LUR_RPT];
@@ -665,12 +764,16 @@ __global__ void __cluster_dims__(LUC_CL, 1, 1) __launch_bounds__(LUR_NT, 1)
         for (int j = 0; j < LUC_W; ++j)
             row[r][j] = has[r] && j < w ? A.p[(k0 + j) * A.ld + base + sl[r]] : 0.0;
     }
+    // every CTA's mbarriers armed before anyone pushes
+    luc_cluster_sync();
 
-    // the best active row of this CTA for column c (its value in register 0)
-    // published in cand[buf] with its values relative to column c: the best
-    // row of each warp stages its values, warp 0 picks the CTA's best and
-    // copies that warp's stage
-    auto publish = [&](int c, int buf) {
+    // the best active row of this CTA for column c (its value in register 0),
+    // pushed with its values into slot `rank` of buffer buf of every CTA:
+    // the best row of each warp stages its values, warp 0 picks the CTA's
+    // best and sends that warp's stage.  Every step passes this one CTA
+    // barrier; the flags read after it (the same values in every thread)
+    // decide whether the loop ends, and nothing is pushed when it does.
+    auto publish = [&](int c, int buf) -> bool {
         double v = -1.0;
         int rw = 0x7fffffff, cd = -1;
 #pragma unroll
@@ -682,13 +785,12 @@ __global__ void __cluster_dims__(LUC_CL, 1, 1) __launch_bounds__(LUR_NT, 1)
                 cd = code[r];
             }
         }
-        luc_warp_best(v, rw, cd);
+        lur_warp_best(v, rw, cd);
 #pragma unroll
         for (int r = 0; r < LUR_RPT; ++r)
             if (cd >= 0 && cd == code[r]) {
 #pragma unroll
-                for (int j = 0; j < LUC_W; ++j)
-                    if (c + j < w) wstage[wid][j] = row[r][j];
+                for (int j = 0; j < LUC_W; ++j) wstage[wid][j] = c + j < w ? row[r][j] : 0.0;
             }
         if (lane == 0) {
             red_v[wid] = v;
@@ -696,128 +798,122 @@ __global__ void __cluster_dims__(LUC_CL, 1, 1) __launch_bounds__(LUR_NT, 1)
             red_c[wid] = cd;
         }
         __syncthreads();
-        if (wid == 0) {
+        const bool leave = *(volatile int *)&s_abort != 0 || *(volatile int *)&s_stop != 0;
+        if (wid == 0 && !leave && c < w) {
             v = lane < LUR_NT / 32 ? red_v[lane] : -1.0;
             rw = lane < LUR_NT / 32 ? red_r[lane] : 0x7fffffff;
             cd = lane < LUR_NT / 32 ? red_c[lane] : -1;
-            int bw = lane;
+            int bw = lane;  // the warp that staged it
             static_assert(LUR_NT / 32 == 8, "three rounds reduce the warps' bests");
+            luc_best8(v, rw, bw);
+            cd = __shfl_sync(0xffffffffu, cd, bw & 31);
+            // lane j sends u[j] = column c+1+j (u[31] = 0); lane 31 also
+            // the header and u0 = column c
+            const double x = cd >= 0 && lane < 31 ? wstage[bw][lane + 1] : 0.0;
+            const double x0 = cd >= 0 ? wstage[bw][0] : 0.0;
+            const unsigned long long hdr1 =
+                (unsigned long long)(unsigned)rw | ((unsigned long long)(unsigned)cd << 32);
+            const uint32_t mine = (uint32_t)__cvta_generic_to_shared(&recv[buf].slot[rank]);
+            const uint32_t bar = (uint32_t)__cvta_generic_to_shared(&rbar[buf]);
+            const uint32_t off = (uint32_t)offsetof(LurSlot, u) + 8u * lane;
 #pragma unroll
-            for (int off = 4; off > 0; off >>= 1) {
-                const double ov = __shfl_xor_sync(0xffffffffu, v, off);
-                const int orow = __shfl_xor_sync(0xffffffffu, rw, off);
-                const int ocd = __shfl_xor_sync(0xffffffffu, cd, off);
-                const int obw = __shfl_xor_sync(0xffffffffu, bw, off);
-                if (luc_better(ov, orow, v, rw)) {
-                    v = ov;
-                    rw = orow;
-                    cd = ocd;
-                    bw = obw;
+            for (int d = 0; d < LUC_CL; ++d) {
+                uint32_t ra, rb;
+                asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(ra) : "r"(mine), "r"(d));
+                asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(rb) : "r"(bar), "r"(d));
+                lur_push_f64(ra + off, x, rb);
+                if (lane == 31) {
+                    lur_push_v2b64(ra, (unsigned long long)__double_as_longlong(v), hdr1, rb);
+                    lur_push_f64(ra + (uint32_t)offsetof(LurSlot, u0), x0, rb);
                 }
             }
-            v = __shfl_sync(0xffffffffu, v, 0);
-            rw = __shfl_sync(0xffffffffu, rw, 0);
-            cd = __shfl_sync(0xffffffffu, cd, 0);
-            bw = __shfl_sync(0xffffffffu, bw, 0);
-            if (lane == 0) {
-                cand[buf].v = v;
-                cand[buf].row = rw;
-                cand[buf].code = cd;
-            }
-            if (cd >= 0 && c + lane < w) cand[buf].vals[lane] = wstage[bw][lane];
         }
+        return leave;
     };
-    publish(0, 0);
-    luc_cluster_sync();  // the candidates of column 0 and all shared memory initialised
+    bool leave = publish(0, 0);
 
     int c = 0;
 #pragma unroll 1
-    for (; c < w; ++c) {
+    for (; c < w && !leave; ++c) {
         const int64_t k = k0 + c;
         const int buf = c & 1;
-        if (wid == 0) {
-            // warp 0: the CL candidates with their values (one round of
-            // remote loads), the winner, the pivot row into s_u
-            double v = -1.0, vals[LUC_CL];
-            int prow = 0x7fffffff, pc = -1, q = -1;
+        // this step's candidates from every CTA (bounded wait)
+        // (one verdict per warp, so the warp's shuffles below stay converged)
+        const bool got =
+            __all_sync(0xffffffffu, lur_wait(&rbar[buf], (uint32_t)((c >> 1) & 1), &s_abort));
+        if (!got) {
+            if (atomicExch(&s_abort, 1) == 0) atomicExch(err, LUR_ERR_TIMEOUT);
+        }
+        double ivp = 0.0, v = -1.0;
+        int prow = 0x7fffffff, pcode = -1;
+        const LurSlot *ps = nullptr;
+        if (got) {
+            const LurRecv &rv = recv[buf];
+            int q = -1;
             if (lane < LUC_CL) {
-                const uint32_t a = luc_map(&cand[buf], (uint32_t)lane);
-                v = luc_ld_f64(a);
-                prow = luc_ld_s32(a + 8);
-                pc = luc_ld_s32(a + 12);
+                v = rv.slot[lane].v;
+                prow = rv.slot[lane].row;
                 q = lane;
             }
-#pragma unroll
-            for (int qq = 0; qq < LUC_CL; ++qq)
-                vals[qq] = c + lane < w ? luc_ld_f64(luc_map(&cand[buf].vals[lane], (uint32_t)qq))
-                                        : 0.0;
             static_assert(LUC_CL == 8, "three rounds reduce the CTAs' candidates");
             luc_best8(v, prow, q);
-            v = __shfl_sync(0xffffffffu, v, 0);
-            prow = __shfl_sync(0xffffffffu, prow, 0);
-            q = __shfl_sync(0xffffffffu, q, 0);
-            const int qb = q < 0 ? 0 : q;
-            pc = __shfl_sync(0xffffffffu, pc, qb);
-            double u = 0.0;
-#pragma unroll
-            for (int qq = 0; qq < LUC_CL; ++qq) u = qq == qb ? vals[qq] : u;
-            // s_u[j] = column c+1+j, 16-byte pairs for the update's loads
-            if (lane > 0) s_u[lane - 1] = c + lane < w ? u : 0.0;
-            if (lane == 31) s_u[31] = 0.0;
-            if (lane == 0) {
-                s_ivp = 1.0 / u;
-                s_prow = prow;
-                s_pcode = pc;
-                s_stop = stop0 != 0 || !(v > 0.0);
+            ps = &rv.slot[q < 0 ? 0 : q];
+            pcode = ps->code;
+            if (t == 0) {
                 if (rank == 0) {
                     if (stop0 == 0 && !(v > 0.0)) *info = (int)(k + 1);
                     if (stop0 == 0 && v > 0.0) ipiv[k] = (int64_t)prow + 1;
                 }
             }
         }
-        __syncthreads();
-        if (s_stop) break;  // the same decision in every CTA
-        const int prow = s_prow, pcode = s_pcode;
-        const double ivp = s_ivp;
-#pragma unroll
-        for (int r = 0; r < LUR_RPT; ++r) {
-            if (!has[r]) continue;
-            if (code[r] == pcode) {
-                // the pivot row: its remaining values are final (the U row)
-#pragma unroll
-                for (int j = 0; j < LUC_W; ++j)
-                    if (c + j < w) fin[(size_t)(c + j) * R + sl[r]] = row[r][j];
-                cur[r] = (int)k;
-            } else if (cur[r] == k) {
-                cur[r] = prow;  // the row the pivot row displaces
-            }
-            act[r] = cur[r] > k;  // the pivot rows so far are final
-        }
-        double l[LUR_RPT];
-#pragma unroll
-        for (int r = 0; r < LUR_RPT; ++r) {
-            l[r] = row[r][0] * ivp;
-            if (act[r]) fin[(size_t)c * R + sl[r]] = l[r];
-        }
-        // register j <- column c+1+j (rows that are no longer active compute
-        // values that are never used)
-#pragma unroll
-        for (int j = 0; j < LUC_W - 1; j += 2) {
-            const double2 uj = *(const double2 *)&s_u[j];
+        // the same decision in every CTA and every thread that has the data;
+        // it takes effect after the step's CTA barrier
+        const bool stop = got && (stop0 != 0 || !(v > 0.0));
+        if (stop) s_stop = 1;
+        if (got && !stop) {
+            ivp = 1.0 / ps->u0;
 #pragma unroll
             for (int r = 0; r < LUR_RPT; ++r) {
-                row[r][j] = fma(-l[r], uj.x, row[r][j + 1]);
-                if (j + 2 < LUC_W) row[r][j + 1] = fma(-l[r], uj.y, row[r][j + 2]);
-            }
-        }
+                if (!has[r]) continue;
+                if (code[r] == pcode) {
+                    // the pivot row: its remaining values are final (the U row)
 #pragma unroll
-        for (int r = 0; r < LUR_RPT; ++r) row[r][LUC_W - 1] = 0.0;
-        if (c + 1 < w) publish(c + 1, buf ^ 1);  // its barrier orders this step's reads
-        else __syncthreads();
-        luc_cluster_sync();  // next candidates published; this step's remote reads done
+                    for (int j = 0; j < LUC_W; ++j)
+                        if (c + j < w) fin[(size_t)(c + j) * R + sl[r]] = row[r][j];
+                    cur[r] = (int)k;
+                } else if (cur[r] == k) {
+                    cur[r] = prow;  // the row the pivot row displaces
+                }
+                act[r] = cur[r] > k;  // the pivot rows so far are final
+            }
+            double l[LUR_RPT];
+#pragma unroll
+            for (int r = 0; r < LUR_RPT; ++r) {
+                l[r] = row[r][0] * ivp;
+                if (act[r]) fin[(size_t)c * R + sl[r]] = l[r];
+            }
+            // register j <- column c+1+j (rows that are no longer active
+            // compute values that are never used)
+#pragma unroll
+            for (int j = 0; j < LUC_W - 1; j += 2) {
+                const double2 uj = *(const double2 *)&ps->u[j];
+#pragma unroll
+                for (int r = 0; r < LUR_RPT; ++r) {
+                    row[r][j] = fma(-l[r], uj.x, row[r][j + 1]);
+                    if (j + 2 < LUC_W) row[r][j + 1] = fma(-l[r], uj.y, row[r][j + 2]);
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < LUR_RPT; ++r) row[r][LUC_W - 1] = 0.0;
+        }
+        // re-arm this buffer for step c+2 (its step-c phase has completed)
+        if (t == 0 && got) lur_arm(&rbar[buf], LUC_CL * LUR_SLOT_TX);
+        // the candidates of column c+1 (for the last column only the barrier)
+        leave = publish(c + 1, buf ^ 1);
+        if (leave) break;
     }
     // a singular column stops the panel: the active rows keep their current
-    // values from column c on
+    // values from column c on (after a stop, the step's update did not run)
     if (c < w) {
 #pragma unroll
         for (int r = 0; r < LUR_RPT; ++r)
@@ -827,7 +923,7 @@ __global__ void __cluster_dims__(LUC_CL, 1, 1) __launch_bounds__(LUR_NT, 1)
                     if (c + j < w) fin[(size_t)(c + j) * R + sl[r]] = row[r][j];
             }
     }
-    luc_cluster_sync();  // no CTA leaves while another may still read its shared memory
+    luc_cluster_sync();  // no CTA leaves while another may still push into it
     // write the panel back, every slot's row at its final position, and list
     // the moved rows
 #pragma unroll
@@ -1031,7 +1127,7 @@ static int getrf64_fast(mflab_handle *h, int64_t m, int64_t n, Mat A, int64_t *i
         const bool cluster = smem <= (size_t)LUC_SMEM_MAX && R <= 0x7fffffff;
         if (cluster && R <= LUR_NT * LUR_RPT && lur_smem(R) <= (size_t)LUC_SMEM_MAX)
             lu64_cluster_panel_reg_kernel<<<LUC_CL, LUR_NT, lur_smem(R), sp>>>(
-                m, A, k0, w, (int)R, ipiv, info, moved);
+                m, A, k0, w, (int)R, ipiv, info, moved, h->dev_flags + 1);
         else if (cluster)
             lu64_cluster_panel_kernel<<<LUC_CL, LUC_NT, smem, sp>>>(m, A, k0, w, (int)R, ipiv,
                                                                     info, moved);
