@@ -429,11 +429,13 @@ int mflab_getrs(mflab_handle *h, void *stream, int limbs, int64_t n, int64_t nrh
 /* Repeated solves with one binary64 LU factor (the correction solves of the
    mixed-precision LU solver; no reference counterpart).  After mflab_getrf
    (limbs = 1), mflab_lu64_prepare stores in `work` (mflab_lu64_work_bytes(n)
-   bytes of device memory, owned by the caller) the row permutation of ipiv
-   and the inverses of the 128 x 128 diagonal blocks of L and U;
-   mflab_lu64_solve then overwrites B (n x nrhs binary64, column-major) with
-   inv(A) B: one gather and one kernel per block row and direction.  Results
-   differ from mflab_getrs in rounding only.  n <= 24576. */
+   bytes of device memory, owned by the caller: 2 n^2 doubles and a little
+   more) the row permutation of ipiv, the inverses of the 128 x 128 diagonal
+   blocks of L and U, and each off-diagonal block column of L and U times its
+   inverted diagonal block; mflab_lu64_solve then overwrites B (n x nrhs
+   binary64, column-major) with inv(A) B: one gather and one kernel per block
+   row and direction, reading only `work` (LU and ldl are checked, not read).
+   Results differ from mflab_getrs in rounding only.  n <= 24576. */
 int mflab_lu64_work_bytes(int64_t n, size_t *bytes);
 int mflab_lu64_prepare(mflab_handle *h, void *stream, int64_t n, const double *LU, int64_t ldl,
                        const int64_t *ipiv, void *work);

@@ -9,16 +9,21 @@
 // with a triangular solve and a GEMM per block it is launch- and
 // latency-bound (hundreds of small kernels per solve).  Here the 128 x 128
 // diagonal blocks of L (unit lower) and U are inverted once after the
-// factorization, and the row interchanges are turned into one permutation,
-// both stored in a caller-owned workspace.  A solve is then one gather and
-// one kernel per block row and direction: every CTA forms
-// y_i = inv(D_i) b_i (the 128 x 128 block product, recomputed per CTA, so no
-// CTA waits for another) and subtracts L_{r,i} y_i (U_{r,i} x_i) from its
-// own tile of the remaining rows; CTA 0 also stores y_i.
+// factorization, the row interchanges are turned into one permutation, and
+// every off-diagonal block column is premultiplied by its inverted diagonal
+// block, M_{r,i} = L_{r,i} inv(DL_i) (rows below block i) and
+// U_{r,i} inv(DU_i) (rows above it), all stored in a caller-owned workspace.
+// A solve is then one gather and one kernel per block row and direction,
+// whose CTAs share the work without redundancy and without waiting for one
+// another: with b_i the block's current right-hand side rows,
+//   the block's rows:      y_i = inv(D_i) b_i          (a few CTAs)
+//   every remaining row r: W_r -= M_{r,i} b_i          (= L_{r,i} y_i)
 //
 // Workspace: perm[n] int32 (rounded up to 256 bytes), then the inverted L
 // blocks and the inverted U blocks, nblk = ceil(n / 128) of 128 x 128
-// doubles each (column-major, ld 128; a last partial block is padded).
+// doubles each (column-major, ld 128; a last partial block is padded), then
+// ML and MU, n x n column-major (ld n) each, of which the blocks below /
+// above the diagonal are used.
 #include <algorithm>
 
 #include "mflab_internal.h"
@@ -28,9 +33,6 @@ namespace mfl {
 namespace {
 
 constexpr int IB = 128;        // diagonal block size
-constexpr int IB_RHS = 16;     // right-hand sides per pass of the solve kernel
-constexpr int SOLVE_NT = 1024;  // threads of the solve kernel
-constexpr int SOLVE_ROWS = 128;  // rows of the remaining matrix per CTA
 constexpr int64_t PIVOT_PERM_MAXN_LU64 = 24576;  // indices in shared memory (96 KB)
 
 size_t perm_bytes(int64_t n) { return ((size_t)n * 4 + 255) / 256 * 256; }
@@ -126,106 +128,111 @@ __global__ void lu64_gather_kernel(int64_t n, int64_t nrhs, const double *B, int
     W[c * ldw + i] = B[c * ldb + perm[i]];
 }
 
-// One block step of a triangular solve.  Block i spans rows [j0, j0 + jb).
-//   y = inv(D_i) * W[j0 : j0 + jb, c0 : c0 + cw]   (computed by every CTA)
-//   CTA 0 stores y into Out[j0 : j0 + jb, c0 : c0 + cw];
-//   every CTA updates its tile of the remaining rows R (below the block for
-//   the forward solve, above it for the backward one):
-//   W[r, c] -= T[r, j0 : j0 + jb] * y[:, c]   (T = L or U, column-major)
-// The remaining rows of W and the block's rows are disjoint, so CTAs that
-// still read W's block rows never see another CTA's update.
-// The 128 x 128 inverse, then the CTA's 128 x jb tile of T, are staged in
-// shared memory by all 1024 threads at once (16 independent loads each).
-// Each product is done by 512 threads: thread (row, quarter) accumulates all
-// 16 right-hand sides over a quarter of the 128 columns (one matrix load and
-// eight broadcast double2 loads per column), and the four partial sums are
-// added in shared memory.
-constexpr int SOLVE_PARTS = 4;
+// One block step of a triangular solve.  Block i spans rows [j0, j0 + jb)
+// and b = W[j0 : j0 + jb, :] holds its final right-hand side rows.
+//   CTA k < ceil(jb / 32):  Out[j0 + 32k + r, c] = (inv(D_i) b)[32k + r, c]
+//   the other CTAs, 32 rows r of [r_begin, r_end) each:
+//                           W[r, c] -= (M[r, block i] b)[r, c]
+// The rows written to W are outside the block, so no CTA reads what another
+// writes.  A CTA stages its 32 x jb slice of inv(D_i) or M (k-major) and b
+// (16 right-hand sides at a time) in shared memory; thread (row, warp)
+// accumulates two right-hand sides over the jb columns.
+constexpr int MS_ROWS = 32, MS_NT = 256, MS_RHS = 16;
 
-__device__ __forceinline__ void lu64_block_product(const double *mat, const double2 *xT,
-                                                   double *part, int t, int jmax) {
-    // part[p][c][r] = sum_{j in quarter p, j < jmax} mat[j][r] x[j][c]
-    if (t >= SOLVE_PARTS * IB) return;
-    const int r = t % IB, p = t / IB;
-    double acc[IB_RHS];
+__global__ void __launch_bounds__(MS_NT)
+    lu64_mstep_kernel(int64_t nrhs, int64_t j0, int jb, const double *__restrict__ M, int64_t ldm,
+                      const double *__restrict__ inv, double *W, int64_t ldw, double *Out,
+                      int64_t ldo, int64_t r_begin, int64_t r_end) {
+    static_assert(MS_NT / 32 * 2 == MS_RHS, "two right-hand sides per warp");
+    __shared__ double tile[IB][MS_ROWS];             // [k][row]
+    __shared__ __align__(16) double bT[IB][MS_RHS];  // [k][rhs]
+    const int t = threadIdx.x, lane = t % 32, warp = t / 32;
+    const int ndiag = (jb + MS_ROWS - 1) / MS_ROWS;
+    const bool diag = (int)blockIdx.x < ndiag;
+    // diag: the first row inside the block; else the first absolute row of R
+    const int64_t rb = diag ? (int64_t)blockIdx.x * MS_ROWS
+                            : r_begin + ((int64_t)blockIdx.x - ndiag) * MS_ROWS;
+    const int64_t left = diag ? (int64_t)jb - rb : r_end - rb;
+    const int nrows = (int)(left < MS_ROWS ? left : MS_ROWS);
+    // launched as a programmatic dependent of the previous step: the next
+    // step may start its prologue now, and this one stages its slice of M
+    // or inv(D_i) (written before the solve) before waiting for the
+    // previous step's results
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    // all loads of a thread in flight together (unrolled, then stored)
+    {
+        const double *src = diag ? inv + rb : M + j0 * ldm + rb;
+        const int64_t ld = diag ? IB : ldm;
+        double x[IB * MS_ROWS / MS_NT];
 #pragma unroll
-    for (int c = 0; c < IB_RHS; ++c) acc[c] = 0.0;
-    const int jb0 = p * (IB / SOLVE_PARTS);
-    const int jb1 = jb0 + IB / SOLVE_PARTS < jmax ? jb0 + IB / SOLVE_PARTS : jmax;
-#pragma unroll 4
-    for (int j = jb0; j < jb1; ++j) {
-        const double a = mat[j * IB + r];
+        for (int u = 0; u < IB * MS_ROWS / MS_NT; ++u) {
+            const int e = t + u * MS_NT, r = e % MS_ROWS, k = e / MS_ROWS;
+            x[u] = (r < nrows && k < jb) ? src[(int64_t)k * ld + r] : 0.0;
+        }
 #pragma unroll
-        for (int c2 = 0; c2 < IB_RHS / 2; ++c2) {
-            const double2 x = xT[j * (IB_RHS / 2) + c2];
-            acc[2 * c2] = fma(a, x.x, acc[2 * c2]);
-            acc[2 * c2 + 1] = fma(a, x.y, acc[2 * c2 + 1]);
+        for (int u = 0; u < IB * MS_ROWS / MS_NT; ++u) {
+            const int e = t + u * MS_NT;
+            tile[e / MS_ROWS][e % MS_ROWS] = x[u];
         }
     }
+    // the previous steps have completed and their writes are visible
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    for (int64_t c0 = 0; c0 < nrhs; c0 += MS_RHS) {
+        const int cw = (int)(nrhs - c0 < MS_RHS ? nrhs - c0 : MS_RHS);
+        double y[IB * MS_RHS / MS_NT];
 #pragma unroll
-    for (int c = 0; c < IB_RHS; ++c) part[(p * IB_RHS + c) * IB + r] = acc[c];
-}
-
-__global__ void __launch_bounds__(SOLVE_NT)
-    lu64_block_step_kernel(int64_t n, int64_t nrhs, int64_t j0, int jb, const double *__restrict__ T,
-                           int64_t ldt, const double *__restrict__ inv, double *W, int64_t ldw,
-                           double *Out, int64_t ldo, int64_t r_begin, int64_t r_end) {
-    static_assert(SOLVE_NT == 8 * IB && SOLVE_ROWS == IB && IB_RHS == 16, "thread layout");
-    extern __shared__ double sm[];
-    double *mat = sm;                              // [IB columns][IB rows]: inv(D), then T
-    double2 *sbT = (double2 *)(mat + IB * IB);     // [IB][IB_RHS / 2]: W's block rows
-    double2 *syT = sbT + IB * IB_RHS / 2;          // [IB][IB_RHS / 2]: y
-    double *part = (double *)(syT + IB * IB_RHS / 2);  // [PARTS][IB_RHS][IB]
-    const int t = threadIdx.x;
-    const int64_t r0 = r_begin + (int64_t)blockIdx.x * SOLVE_ROWS;
-    for (int64_t c0 = 0; c0 < nrhs; c0 += IB_RHS) {
-        const int cw = (int)(nrhs - c0 < IB_RHS ? nrhs - c0 : IB_RHS);
-#pragma unroll
-        for (int u = 0; u < IB * IB / SOLVE_NT; ++u) {
-            const int e = t + u * SOLVE_NT;
-            mat[e] = inv[e];
+        for (int u = 0; u < IB * MS_RHS / MS_NT; ++u) {
+            const int e = t + u * MS_NT, k = e % IB, c = e / IB;
+            y[u] = (k < jb && c < cw) ? W[(c0 + c) * ldw + j0 + k] : 0.0;
         }
-        for (int e = t; e < IB * IB_RHS; e += SOLVE_NT) {
-            const int r = e % IB, c = e / IB;
-            ((double *)sbT)[r * IB_RHS + c] =
-                (r < jb && c < cw) ? W[(c0 + c) * ldw + j0 + r] : 0.0;
+#pragma unroll
+        for (int u = 0; u < IB * MS_RHS / MS_NT; ++u) {
+            const int e = t + u * MS_NT;
+            bT[e % IB][e / IB] = y[u];
         }
         __syncthreads();
-        lu64_block_product(mat, sbT, part, t, IB);
-        __syncthreads();
-        for (int e = t; e < IB * IB_RHS; e += SOLVE_NT) {
-            const int r = e % IB, c = e / IB;
-            double y = 0.0;
-#pragma unroll
-            for (int p = 0; p < SOLVE_PARTS; ++p) y += part[(p * IB_RHS + c) * IB + r];
-            ((double *)syT)[r * IB_RHS + c] = y;
-            if (blockIdx.x == 0 && r < jb && c < cw) Out[(c0 + c) * ldo + j0 + r] = y;
+        double a0 = 0.0, a1 = 0.0;
+#pragma unroll 8
+        for (int k = 0; k < IB; ++k) {
+            const double m = tile[k][lane];
+            const double2 bb = *(const double2 *)&bT[k][2 * warp];
+            a0 = fma(m, bb.x, a0);
+            a1 = fma(m, bb.y, a1);
         }
-        // this CTA's tile of T: rows r0 .. r0 + 127, columns j0 .. j0 + jb - 1
-        const int r = t % IB, cq = t / IB;
-        const bool live = r0 + r < r_end;
-#pragma unroll
-        for (int u = 0; u < IB * IB / SOLVE_NT; ++u) {
-            const int j = cq + 8 * u;
-            mat[j * IB + r] = (live && j < jb) ? T[(j0 + j) * ldt + r0 + r] : 0.0;
-        }
-        __syncthreads();
-        lu64_block_product(mat, syT, part, t, jb);
-        __syncthreads();
-        for (int e = t; e < IB * IB_RHS; e += SOLVE_NT) {
-            const int rr = e % IB, c = e / IB;
-            if (r0 + rr >= r_end || c >= cw) continue;
-            double acc = 0.0;
-#pragma unroll
-            for (int p = 0; p < SOLVE_PARTS; ++p) acc += part[(p * IB_RHS + c) * IB + rr];
-            W[(c0 + c) * ldw + r0 + rr] -= acc;
+        const int c = 2 * warp;
+        if (lane < nrows) {
+            if (diag) {
+                if (c < cw) Out[(c0 + c) * ldo + j0 + rb + lane] = a0;
+                if (c + 1 < cw) Out[(c0 + c + 1) * ldo + j0 + rb + lane] = a1;
+            } else {
+                if (c < cw) W[(c0 + c) * ldw + rb + lane] -= a0;
+                if (c + 1 < cw) W[(c0 + c + 1) * ldw + rb + lane] -= a1;
+            }
         }
         __syncthreads();
     }
 }
 
-constexpr int SOLVE_SMEM =
-    (IB * IB + 2 * IB * IB_RHS + SOLVE_PARTS * IB_RHS * IB) * (int)sizeof(double);
+// one step, launched with programmatic stream serialization (its prologue
+// overlaps the previous step); grid: the block's row groups, then R's
+int mstep_launch(cudaStream_t s, int64_t nrhs, int64_t j0, int jb, const double *M, int64_t ldm,
+                 const double *inv, double *W, int64_t ldw, double *Out, int64_t ldo,
+                 int64_t r_begin, int64_t r_end) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)((jb + MS_ROWS - 1) / MS_ROWS +
+                                  (r_end - r_begin + MS_ROWS - 1) / MS_ROWS));
+    cfg.blockDim = dim3(MS_NT);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return record_cuda_error(cudaLaunchKernelEx(&cfg, lu64_mstep_kernel, nrhs, j0, jb, M, ldm,
+                                                inv, W, ldw, Out, ldo, r_begin, r_end),
+                             "lu64 solve step");
+}
 
 std::atomic<unsigned long long> g_inv_configured{0};
 
@@ -234,7 +241,8 @@ std::atomic<unsigned long long> g_inv_configured{0};
 
 extern "C" int mflab_lu64_work_bytes(int64_t n, size_t *bytes) {
     if (n < 0 || !bytes) return MFLAB_ERR_ARG;
-    *bytes = mfl::perm_bytes(n) + 2 * (size_t)mfl::nblocks(n) * mfl::IB * mfl::IB * sizeof(double);
+    *bytes = mfl::perm_bytes(n) + 2 * (size_t)mfl::nblocks(n) * mfl::IB * mfl::IB * sizeof(double) +
+             2 * (size_t)n * n * sizeof(double);
     return MFLAB_OK;
 }
 
@@ -261,7 +269,25 @@ extern "C" int mflab_lu64_prepare(mflab_handle *h, void *stream, int64_t n, cons
     mfl::lu64_perm_kernel<<<1, 256, (size_t)n * sizeof(int), s>>>(n, ipiv, perm);
     mfl::lu64_inv_diag_kernel<<<dim3((unsigned)mfl::nblocks(n), 2), mfl::IB, smem, s>>>(
         n, LU, ldl, invL, invU);
-    return mfl::record_cuda_error(cudaGetLastError(), "lu64 prepare");
+    rc = mfl::record_cuda_error(cudaGetLastError(), "lu64 prepare");
+    if (rc) return rc;
+    // ML = L_{r,i} inv(DL_i) below block i, MU = U_{r,i} inv(DU_i) above it
+    // (binary64 GEMMs of the library)
+    double *ML = invU + (size_t)mfl::nblocks(n) * mfl::IB * mfl::IB, *MU = ML + (size_t)n * n;
+    const size_t wsb = (size_t)32 << 20;
+    rc = mflab_reserve_scratch(h, wsb);
+    if (rc) return rc;
+    for (int64_t i = 0; i < mfl::nblocks(n) && rc == MFLAB_OK; ++i) {
+        const int64_t j0 = i * mfl::IB, jb = std::min<int64_t>(mfl::IB, n - j0);
+        const double *iL = invL + i * mfl::IB * mfl::IB, *iU = invU + i * mfl::IB * mfl::IB;
+        if (j0 + jb < n)
+            rc = mfl::dgemm_lt(n - j0 - jb, jb, jb, LU + j0 * ldl + j0 + jb, ldl, iL, mfl::IB,
+                               ML + j0 * n + j0 + jb, n, 1.0, 0.0, h->scratch, wsb, s);
+        if (rc == MFLAB_OK && j0 > 0)
+            rc = mfl::dgemm_lt(j0, jb, jb, LU + j0 * ldl, ldl, iU, mfl::IB, MU + j0 * n, n, 1.0,
+                               0.0, h->scratch, wsb, s);
+    }
+    return rc;
 }
 
 extern "C" int mflab_lu64_solve(mflab_handle *h, void *stream, int64_t n, int64_t nrhs,
@@ -285,30 +311,23 @@ extern "C" int mflab_lu64_solve(mflab_handle *h, void *stream, int64_t n, int64_
                                                                          n);
     rc = mfl::record_cuda_error(cudaGetLastError(), "lu64 gather");
     if (rc) return rc;
-    static std::atomic<unsigned long long> step_configured{0};
-    rc = mfl::set_smem_once((const void *)mfl::lu64_block_step_kernel, mfl::SOLVE_SMEM,
-                            step_configured, "lu64 solve attribute");
-    if (rc) return rc;
+    const double *ML = invU + (size_t)mfl::nblocks(n) * mfl::IB * mfl::IB, *MU = ML + (size_t)n * n;
     const int64_t nb = mfl::nblocks(n);
     // forward: L y = P b, y written into B, W updated below each block
-    for (int64_t i = 0; i < nb; ++i) {
+    for (int64_t i = 0; i < nb && rc == MFLAB_OK; ++i) {
         const int64_t j0 = i * mfl::IB;
         const int jb = (int)std::min<int64_t>(mfl::IB, n - j0);
-        const int64_t rb = j0 + jb, re = n;
-        const unsigned grid = (unsigned)std::max<int64_t>(1, (re - rb + mfl::SOLVE_ROWS - 1) /
-                                                                 mfl::SOLVE_ROWS);
-        mfl::lu64_block_step_kernel<<<grid, mfl::SOLVE_NT, mfl::SOLVE_SMEM, s>>>(
-            n, nrhs, j0, jb, LU, ldl, invL + i * mfl::IB * mfl::IB, W, n, B, ldb, rb, re);
+        rc = mfl::mstep_launch(s, nrhs, j0, jb, ML, n, invL + i * mfl::IB * mfl::IB, W, n, B, ldb,
+                               j0 + jb, n);
     }
     // backward: U x = y, x written into W, B (holding y) updated above each block
-    for (int64_t i = nb - 1; i >= 0; --i) {
+    for (int64_t i = nb - 1; i >= 0 && rc == MFLAB_OK; --i) {
         const int64_t j0 = i * mfl::IB;
         const int jb = (int)std::min<int64_t>(mfl::IB, n - j0);
-        const unsigned grid =
-            (unsigned)std::max<int64_t>(1, (j0 + mfl::SOLVE_ROWS - 1) / mfl::SOLVE_ROWS);
-        mfl::lu64_block_step_kernel<<<grid, mfl::SOLVE_NT, mfl::SOLVE_SMEM, s>>>(
-            n, nrhs, j0, jb, LU, ldl, invU + i * mfl::IB * mfl::IB, B, ldb, W, n, 0, j0);
+        rc = mfl::mstep_launch(s, nrhs, j0, jb, MU, n, invU + i * mfl::IB * mfl::IB, B, ldb, W, n,
+                               0, j0);
     }
+    if (rc) return rc;
     rc = mfl::record_cuda_error(cudaGetLastError(), "lu64 solve");
     if (rc) return rc;
     // the solution (in W) back into B
