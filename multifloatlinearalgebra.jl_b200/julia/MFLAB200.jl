@@ -799,10 +799,13 @@ end
     solve_mixed_lu(A, B; tol=2^(-53N), maxiter=40)
 
 A X = B for a Float64xN device matrix A: a binary64 partial-pivoting LU of
-round(A) on the device, then iterative refinement with Float64xN residuals
-through the INT8 modular GEMM (no reference counterpart; it composes lu!,
-residual! and refinement_correction!).  Returns (X, iterations, worst
-backward error)."""
+round(A) on the device, its solve workspace prepared once (mflab_lu64_prepare:
+permutation, inverted diagonal blocks, premultiplied block columns), then
+iterative refinement with Float64xN residuals through the INT8 modular GEMM;
+A's residues are prepared once (mflab_ozaki_crt_prepare) at the modulus count
+the first residual tuned.  No reference counterpart: it composes lu!,
+residual! and refinement_correction!.  Returns (X, iterations, worst backward
+error)."""
 function solve_mixed_lu(A::MFDeviceMatrix{N}, B::MFDeviceMatrix{N};
                         tol::Float64=2.0^(-53N), maxiter::Int=40,
                         handle::MFHandle=default_handle(A.device),
@@ -819,24 +822,31 @@ function solve_mixed_lu(A::MFDeviceMatrix{N}, B::MFDeviceMatrix{N};
     check(ccall((:mflab_getrf, libmflab), Cint,
                 (Ptr{Cvoid}, Ptr{Cvoid}, Cint, Int64, Int64, Ptr{Float64}, Int64, Int64,
                  Ptr{Int64}, Int64, Ptr{Cint}),
-                handle.ptr, stream, 1, n, n, LU.ptr, LU.ld, LU.ls, ipiv.ptr, 12, info.ptr))
+                handle.ptr, stream, 1, n, n, LU.ptr, LU.ld, LU.ls, ipiv.ptr, 32, info.ptr))
     st = _info(info, stream)
     st == -1 && throw(DomainError(A, "lu!: input matrix contains non-finite entries"))
     st > 0 && throw(LinearAlgebra.SingularException(st))
+    wb = Ref{Csize_t}(0)
+    check(ccall((:mflab_lu64_work_bytes, libmflab), Cint, (Int64, Ptr{Csize_t}), n, wb))
+    work = DeviceBuffer(max(Int(wb[]), 1), A.device)
+    check(ccall((:mflab_lu64_prepare, libmflab), Cint,
+                (Ptr{Cvoid}, Ptr{Cvoid}, Int64, Ptr{Float64}, Int64, Ptr{Int64}, Ptr{Cvoid}),
+                handle.ptr, stream, n, LU.ptr, LU.ld, ipiv.ptr, work.ptr))
     X = zeros(MFDeviceArray{N,2}, n, B.n; device=A.device)
     R = copy(B)
     D = MFDeviceArray{1,2}(undef, n, B.n; device=A.device)
     dc = DeviceConfig(int8=:modular)
+    one_, mone = _scalar(Val(N), one(MF{N})), _scalar(Val(N), -one(MF{N}))
+    prep, T = nothing, 0
     worst, it = Inf, 0
     for outer it in 1:maxiter
         for c in 0:B.n-1    # D = round(R): the leading limbs
             memcpy!(D.ptr + 8 * c * D.ld, R.ptr + 8 * c * R.ld, 8 * n, 2)
         end
-        check(ccall((:mflab_getrs, libmflab), Cint,
-                    (Ptr{Cvoid}, Ptr{Cvoid}, Cint, Int64, Int64, Ptr{Float64}, Int64, Int64,
-                     Ptr{Int64}, Ptr{Float64}, Int64, Int64),
-                    handle.ptr, stream, 1, n, B.n, LU.ptr, LU.ld, LU.ls, ipiv.ptr, D.ptr, D.ld,
-                    D.ls))
+        check(ccall((:mflab_lu64_solve, libmflab), Cint,
+                    (Ptr{Cvoid}, Ptr{Cvoid}, Int64, Int64, Ptr{Float64}, Int64, Ptr{Cvoid},
+                     Ptr{Float64}, Int64),
+                    handle.ptr, stream, n, B.n, LU.ptr, LU.ld, work.ptr, D.ptr, D.ld))
         check(ccall((:mflab_add_widened, libmflab), Cint,
                     (Ptr{Cvoid}, Ptr{Cvoid}, Cint, Cint, Int64, Int64, Ptr{Float64}, Int64, Int64,
                      Ptr{Float64}, Int64, Int64),
@@ -844,7 +854,28 @@ function solve_mixed_lu(A::MFDeviceMatrix{N}, B::MFDeviceMatrix{N};
         for l in 0:N-1, c in 0:B.n-1   # R = B
             memcpy!(R.ptr + 8 * (l * R.ls + c * R.ld), B.ptr + 8 * (l * B.ls + c * B.ld), 8 * n, 2)
         end
-        gemm!(R, A, X, -one(MF{N}), one(MF{N}); device_config=dc, handle=handle, stream=stream)
+        if prep === nothing
+            # the first residual tunes the modulus count; A's residues are
+            # then prepared once for the later residuals
+            gemm!(R, A, X, -one(MF{N}), one(MF{N}); device_config=dc, handle=handle,
+                  stream=stream)
+            T = Int(ccall((:mflab_ozaki_last_moduli, libmflab), Cint, (Ptr{Cvoid},), handle.ptr))
+            pb = Ref{Csize_t}(0)
+            check(ccall((:mflab_ozaki_crt_prepare_bytes, libmflab), Cint,
+                        (Cint, Cint, Int64, Int64, Ptr{Csize_t}), N, T, n, n, pb))
+            prep = DeviceBuffer(max(Int(pb[]), 1), A.device)
+            check(ccall((:mflab_ozaki_crt_prepare, libmflab), Cint,
+                        (Ptr{Cvoid}, Ptr{Cvoid}, Cint, Cint, Int64, Int64, Ptr{Float64}, Int64,
+                         Int64, Ptr{Cvoid}),
+                        handle.ptr, stream, N, T, n, n, A.ptr, A.ld, A.ls, prep.ptr))
+        else
+            check(ccall((:mflab_gemm_ozaki_crt_prepared, libmflab), Cint,
+                        (Ptr{Cvoid}, Ptr{Cvoid}, Cint, Cint, Int64, Int64, Int64, Ptr{Cvoid},
+                         Ptr{Float64}, Int64, Int64, Ptr{Float64}, Int64, Int64, Ptr{Float64},
+                         Ptr{Float64}),
+                        handle.ptr, stream, N, T, n, B.n, n, prep.ptr, X.ptr, X.ld, X.ls, R.ptr,
+                        R.ld, R.ls, mone, one_))
+        end
         worst = maximum(Float64(e) for e in normwise_backward_error(A, X, B, R; handle=handle,
                                                                     stream=stream))
         worst <= tol && break

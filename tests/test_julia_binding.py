@@ -17,7 +17,7 @@ C2JL = {
     "int": "Cint", "int64_t": "Int64", "size_t": "Csize_t",
     "double*": "Ptr{Float64}", "const double*": "Ptr{Float64}",
     "int*": "Ptr{Cint}", "const int*": "Ptr{Cint}",
-    "int64_t*": "Ptr{Int64}", "const int64_t*": "Ptr{Int64}",
+    "int64_t*": "Ptr{Int64}", "const int64_t*": "Ptr{Int64}", "size_t*": "Ptr{Csize_t}",
     "uint8_t*": "Ptr{UInt8}", "const uint8_t*": "Ptr{UInt8}",
     "void*": "Ptr{Cvoid}", "const void*": "Ptr{Cvoid}", "mflab_handle*": "Ptr{Cvoid}",
     "mflab_handle**": "Ptr{Ptr{Cvoid}}", "void**": "Ptr{Ptr{Cvoid}}",
