@@ -76,8 +76,129 @@ __global__ void potrf_panel_kernel(Mat A, int64_t f, int w, int *info) {
     }
 }
 
+// One block step of the blocked Cholesky, fused: the diagonal block's factor
+// (potrf_panel_kernel) and the solve of the rows below it (trsm_right_thread,
+// A21 <- A21 inv(L11)^T), evaluated right-looking with every entry's
+// operations in the reference's order.  Entry (r, j) of the block starts from
+// A[r, j] and receives, for k = 0 .. j-1 in ascending order,
+//     v = submul(v, x_rk, L_jk)            (submul(d, L_jk, L_jk) on the diagonal)
+// then x_rj = div(v, p_j) with p_j = sqrt(d_j) — the same operands in the same
+// order as the two kernels' left-looking loops, so the bits agree.  Each
+// thread holds one row in registers; register j holds column k + j at step k
+// (the update writes its results one register down, so no register index
+// depends on k).  Warp 0 holds the block's own rows, which every CTA factors
+// (a 16 x 16 block), warps 1-3 hold 96 rows below it per CTA.  Step k: thread k
+// forms p_k (or records the failure), every later row forms x_rk, the block's
+// rows publish L_jk, then every row updates its remaining entries.  Final
+// values collect in shared memory and are written at the end: on a failure at
+// column k, CTA 0 writes the block's columns before k and nothing else, as the
+// two kernels would (the solve never runs after a failed panel).
+constexpr int PF_W = 16, PF_NT = 128, PF_DIAG = 32;
+
 template <int N>
-static int potrf_n(int64_t n, Mat A, int64_t block, int *info, cudaStream_t s) {
+__global__ void __launch_bounds__(PF_NT)
+    potrf_step_kernel(Mat A, int64_t f, int w, int64_t t_rows, int *info) {
+    if (*info) return;
+    extern __shared__ double pf_fin[];  // [PF_W][PF_NT][N] final values of each thread's row
+    __shared__ double Ls[PF_W][PF_W][N];  // L[j][k] of the block's rows
+    __shared__ double piv[N];
+    __shared__ int fail;
+    const int tid = threadIdx.x;
+    const bool dg = tid < PF_DIAG;
+    const int64_t rb = (int64_t)blockIdx.x * (PF_NT - PF_DIAG) + (tid - PF_DIAG);
+    const bool has = dg ? tid < w : rb < t_rows;
+    const int64_t row = dg ? f + tid : f + w + rb;
+    mf<N> r[PF_W];
+#pragma unroll
+    for (int j = 0; j < PF_W; ++j)
+        r[j] = (has && j < w) ? load_mf<N>(A.p, A.ld, A.ls, row, f + j) : from_double<N>(0.0);
+    if (tid == 0) fail = 0;
+    __syncthreads();
+    int kf = w;  // the failed column, or w
+#pragma unroll 1
+    for (int k = 0; k < w; ++k) {
+        if (tid == k) {  // the block's row k: register 0 is its diagonal entry
+            const mf<N> d = r[0];
+            if (!gt(d, from_double<N>(0.0))) {
+                fail = 1;
+                if (blockIdx.x == 0) *info = (int)(f + k + 1);
+            } else {
+                const mf<N> p = sqrt_mf(d);
+#pragma unroll
+                for (int l = 0; l < N; ++l) {
+                    piv[l] = p.v[l];
+                    pf_fin[((size_t)k * PF_NT + tid) * N + l] = p.v[l];
+                }
+            }
+        }
+        __syncthreads();
+        if (fail) {
+            kf = k;
+            break;
+        }
+        mf<N> p;
+#pragma unroll
+        for (int l = 0; l < N; ++l) p.v[l] = piv[l];
+        const bool act = has && (!dg || tid > k);
+        mf<N> x = from_double<N>(0.0);
+        if (act) {
+            x = div(r[0], p);
+#pragma unroll
+            for (int l = 0; l < N; ++l) {
+                pf_fin[((size_t)k * PF_NT + tid) * N + l] = x.v[l];
+                if (dg) Ls[tid][k][l] = x.v[l];
+            }
+        }
+        __syncthreads();
+        if (act) {
+            // register j <- column k+1+j (only the lower part of the block's rows)
+#pragma unroll
+            for (int j = 0; j < PF_W - 1; ++j) {
+                const int c = k + 1 + j;
+                if (c < w && (!dg || c <= tid)) {
+                    mf<N> ljk;
+#pragma unroll
+                    for (int l = 0; l < N; ++l) ljk.v[l] = Ls[c][k][l];
+                    r[j] = submul(r[j + 1], x, ljk);
+                }
+            }
+        }
+    }
+    // final values: the block's rows from CTA 0 (lower triangle), columns
+    // before the failure; the rows below only without a failure
+    if (!has) return;
+    if (dg) {
+        if (blockIdx.x != 0) return;
+        for (int j = 0; j < kf && j <= tid; ++j) {
+            mf<N> v;
+#pragma unroll
+            for (int l = 0; l < N; ++l) v.v[l] = pf_fin[((size_t)j * PF_NT + tid) * N + l];
+            store_mf<N>(A.p, A.ld, A.ls, row, f + j, v);
+        }
+    } else if (kf == w) {
+        for (int j = 0; j < w; ++j) {
+            mf<N> v;
+#pragma unroll
+            for (int l = 0; l < N; ++l) v.v[l] = pf_fin[((size_t)j * PF_NT + tid) * N + l];
+            store_mf<N>(A.p, A.ld, A.ls, row, f + j, v);
+        }
+    }
+}
+
+static int lu64_lookahead_streams(mflab_handle *h);
+
+// Blocked Cholesky in the reference's order with look-ahead.  Per block:
+// the fused step kernel (panel + solve below it), then the trailing
+// lower(A22) -= L21 L21^T in two parts that partition its lower triangle: the
+// next block's columns (all rows) on a high-priority stream, the rest on the
+// caller's stream, where it overlaps the next block's step kernel.  Every
+// entry still receives the blocks' updates one after another in block order
+// (the next-columns part of block b waits for the rest of block b-1, which
+// updated those columns), each as the same K = block chain and epilogue, so
+// the factor is the same bit for bit.  Blocks wider than PF_W take the panel
+// kernel + TRSM path on the caller's stream.
+template <int N>
+static int potrf_n(mflab_handle *h, int64_t n, Mat A, int64_t block, int *info, cudaStream_t s) {
     const double mone[4] = {-1.0, 0.0, 0.0, 0.0}, one[4] = {1.0, 0.0, 0.0, 0.0};
     cudaError_t e = cudaMemsetAsync(info, 0, sizeof(int), s);
     if (e != cudaSuccess) return record_cuda_error(e, "potrf info");
@@ -86,23 +207,72 @@ static int potrf_n(int64_t n, Mat A, int64_t block, int *info, cudaStream_t s) {
     nonfinite_kernel<N><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(n, n, A, 1, info);
     int rc = record_cuda_error(cudaGetLastError(), "potrf check");
     if (rc) return rc;
-    for (int64_t first = 0; first < n; first += block) {
+    if (block > PF_W) {
+        for (int64_t first = 0; first < n; first += block) {
+            const int64_t last = first + block - 1 < n - 1 ? first + block - 1 : n - 1;
+            const int w = (int)(last - first + 1);
+            potrf_panel_kernel<N><<<1, 32, 0, s>>>(A, first, w, info);
+            rc = record_cuda_error(cudaGetLastError(), "potrf panel");
+            if (rc) return rc;
+            if (last < n - 1) {
+                const int64_t t = n - 1 - last;
+                rc = launch_trsm_info(N, 1, 0, 1, 0, t, w, A.at(first, first), A.at(last + 1, first),
+                                      one, s, info);
+                if (rc) return rc;
+                rc = launch_mm(N, false, true, 1, false, t, t, w, A.at(last + 1, first),
+                               A.at(last + 1, first), A.at(last + 1, last + 1), mone, one, s, info);
+                if (rc) return rc;
+            }
+        }
+        return MFLAB_OK;
+    }
+    const size_t fin_bytes = (size_t)PF_W * PF_NT * N * sizeof(double);
+    static std::atomic<unsigned long long> configured{0};
+    rc = set_smem_once((const void *)potrf_step_kernel<N>, (int)fin_bytes, configured,
+                       "potrf step attribute");
+    if (rc) return rc;
+    rc = lu64_lookahead_streams(h);
+    if (rc) return rc;
+    cudaStream_t sp = h->la_stream;
+    cudaEvent_t ev_fork = h->la_ev[0], ev_step = h->la_ev[1], ev_rest = h->la_ev[2];
+    e = cudaEventRecord(ev_fork, s);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(sp, ev_fork, 0);
+    if (e != cudaSuccess) return record_cuda_error(e, "potrf fork");
+    int b = 0;
+    for (int64_t first = 0; first < n && rc == MFLAB_OK; first += block, ++b) {
         const int64_t last = first + block - 1 < n - 1 ? first + block - 1 : n - 1;
         const int w = (int)(last - first + 1);
-        potrf_panel_kernel<N><<<1, 32, 0, s>>>(A, first, w, info);
-        rc = record_cuda_error(cudaGetLastError(), "potrf panel");
-        if (rc) return rc;
-        if (last < n - 1) {
-            const int64_t t = n - 1 - last;
-            rc = launch_trsm_info(N, 1, 0, 1, 0, t, w, A.at(first, first), A.at(last + 1, first), one,
-                                  s, info);
-            if (rc) return rc;
-            rc = launch_mm(N, false, true, 1, false, t, t, w, A.at(last + 1, first),
-                           A.at(last + 1, first), A.at(last + 1, last + 1), mone, one, s, info);
-            if (rc) return rc;
+        const int64_t t = n - 1 - last;  // rows below the block
+        const unsigned grid = (unsigned)std::max<int64_t>(1, (t + PF_NT - PF_DIAG - 1) /
+                                                                 (PF_NT - PF_DIAG));
+        potrf_step_kernel<N><<<grid, PF_NT, fin_bytes, sp>>>(A, first, w, t, info);
+        rc = record_cuda_error(cudaGetLastError(), "potrf step");
+        if (rc || t == 0) break;
+        e = cudaEventRecord(ev_step, sp);
+        // the next block's columns, after the rest of the previous block
+        const int64_t wn = std::min<int64_t>(block, t);
+        if (e == cudaSuccess && b > 0) e = cudaStreamWaitEvent(sp, ev_rest, 0);
+        if (e != cudaSuccess) return record_cuda_error(e, "potrf look-ahead");
+        rc = launch_mm(N, false, true, 1, false, t, wn, w, A.at(last + 1, first),
+                       A.at(last + 1, first), A.at(last + 1, last + 1), mone, one, sp, info);
+        if (rc) break;
+        // the rest of the lower triangle, after the step
+        if (t > wn) {
+            e = cudaStreamWaitEvent(s, ev_step, 0);
+            if (e != cudaSuccess) return record_cuda_error(e, "potrf look-ahead");
+            rc = launch_mm(N, false, true, 1, false, t - wn, t - wn, w,
+                           A.at(last + 1 + wn, first), A.at(last + 1 + wn, first),
+                           A.at(last + 1 + wn, last + 1 + wn), mone, one, s, info);
+            if (rc) break;
         }
+        e = cudaEventRecord(ev_rest, s);
+        if (e != cudaSuccess) rc = record_cuda_error(e, "potrf look-ahead");
     }
-    return MFLAB_OK;
+    // join: the caller's stream waits for the high-priority stream
+    e = cudaEventRecord(ev_fork, sp);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s, ev_fork, 0);
+    if (e != cudaSuccess && rc == MFLAB_OK) rc = record_cuda_error(e, "potrf join");
+    return rc;
 }
 
 // Cholesky with INT8 trailing updates: panels of nb columns; inside a panel
@@ -1492,9 +1662,9 @@ extern "C" int mflab_potrf(mflab_handle *h, void *stream, int limbs, int64_t n, 
     Mat a{A, lda, lsa};
     cudaStream_t s = (cudaStream_t)stream;
     switch (limbs) {
-    case 2: return mfl::potrf_n<2>(n, a, block, info, s);
-    case 3: return mfl::potrf_n<3>(n, a, block, info, s);
-    default: return mfl::potrf_n<4>(n, a, block, info, s);
+    case 2: return mfl::potrf_n<2>(h, n, a, block, info, s);
+    case 3: return mfl::potrf_n<3>(h, n, a, block, info, s);
+    default: return mfl::potrf_n<4>(h, n, a, block, info, s);
     }
 }
 
