@@ -575,6 +575,11 @@ def config_mixed_lu(R, torch, peak, reps):
     Aw = A.copy()
     t_p, ts_p, Xp = _time_median(torch, lambda: mf.solve(mf.lu_(Aw), B), lambda: Aw.copy_(A),
                                  reps)
+    # the plain x4 factor and its solve timed apart: the solve's backward
+    # substitution in the reference order (each row's chain starts at the
+    # unknown solved last) is n(n-1)/2 dependent subtractions per column
+    t_pf, ts_pf, Fp = _time_median(torch, lambda: mf.lu_(Aw), lambda: Aw.copy_(A), reps)
+    t_ps, ts_ps, _ = _time_median(torch, lambda: mf.solve(Fp, B), None, reps)
     Aw2 = A.copy()
     ocfg = mf.KernelConfig(gemm_strategy="ozaki", ozaki_scheme="modular", ozaki_block=256)
     t_o, ts_o, Xo = _time_median(torch, lambda: mf.solve(mf.lu_(Aw2, config=ocfg), B),
@@ -601,10 +606,18 @@ def config_mixed_lu(R, torch, peak, reps):
                               "and n^2 (solves) to n=4096"}
     flops64 = 2.0 * n ** 3 / 3.0
     out = {
-        "mixed_ms": t_m * 1e3, "repeats_ms": {"mixed": ts_m, "plain_x4": ts_p, "int8_x4": ts_o},
+        "mixed_ms": t_m * 1e3, "repeats_ms": {"mixed": ts_m, "plain_x4": ts_p, "int8_x4": ts_o,
+                                              "plain_x4_factor": ts_pf, "plain_x4_solve": ts_ps},
         "binary64_factor_ms": rep["factor_ms"], "refinement_ms": rep["refine_ms"],
         "iterations": rep["iterations"], "mixed_backward_error": rep["backward_error"],
         "plain_x4_ms": t_p * 1e3, "speedup_vs_plain_x4": t_p / t_m,
+        "plain_x4_factor_ms": t_pf * 1e3, "plain_x4_solve_ms": t_ps * 1e3,
+        "plain_x4_factor_md_gflops": 2.0 * n ** 3 / 3.0 / t_pf / 1e9,
+        "plain_x4_solve_chain": {"dependent_subtractions_per_column": n * (n - 1) // 2,
+                                 "ns_per_subtraction": t_ps / (n * (n - 1) / 2) * 1e9,
+                                 "note": "reference order (solve.jl / trsm.jl): row r's chain "
+                                         "starts at the unknown solved last, so the backward "
+                                         "substitution is one serial chain per column"},
         "int8_trailing_x4_ms": t_o * 1e3,
         "roofline_binary64_factor": {"bound": "fp64", "unit": "TFLOP/s",
                                      "achieved": flops64 / (rep["factor_ms"] / 1e3) / 1e12,
@@ -613,9 +626,10 @@ def config_mixed_lu(R, torch, peak, reps):
                                      "peak_source": "2 x DFMA probe instruction rate"},
         "roofline_plain_x4": _fp64_roof(n ** 3 / 3.0 * ops_per_term(4) + float(n) * n * nrhs
                                         * ops_per_term(4), t_p, peak),
+        "roofline_plain_x4_factor": _fp64_roof(n ** 3 / 3.0 * ops_per_term(4), t_pf, peak),
         "parity": parity, "cpu_baseline": cpu,
         "matrix": "U diag(sigma) V^T, sigma geometric 1 -> 1e-12, lifted to Float64x4"}
-    del A, B, X, Aw, Aw2, Xp, Xo
+    del A, B, X, Aw, Aw2, Xp, Xo, Fp
     torch.cuda.empty_cache()
     return out
 

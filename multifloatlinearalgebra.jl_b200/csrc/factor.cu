@@ -330,9 +330,13 @@ static int potrf_ozaki_n(mflab_handle *h, int64_t n, Mat A, int64_t nb, int64_t 
 // ------------------------------------------------------------------ LU ---
 // single CTA: pivot search in column k (rows k..m-1), full-row swap,
 // zero-pivot test, reciprocal and scaling of the column below the pivot
+// The interchange of step k is applied to the panel's columns [c_lo, c_hi)
+// only; lu_swap_rest_kernel applies the panel's interchanges to every other
+// column once the panel is done (no computation reads those columns in
+// between, so the factor is the same as with full-row swaps at each step).
 template <int N, int NT>
-__global__ void __launch_bounds__(NT) lu_pivot_kernel(int64_t m, int64_t n, Mat A, int64_t k,
-                                                      int64_t *ipiv, int *info) {
+__global__ void __launch_bounds__(NT) lu_pivot_kernel(int64_t m, int64_t c_lo, int64_t c_hi, Mat A,
+                                                      int64_t k, int64_t *ipiv, int *info) {
     if (*info) return;
     __shared__ double sval[NT][N];
     __shared__ int64_t sidx[NT];
@@ -383,7 +387,7 @@ __global__ void __launch_bounds__(NT) lu_pivot_kernel(int64_t m, int64_t n, Mat 
     __syncthreads();
     const int64_t p = spiv;
     if (p != k) {
-        for (int64_t c = t; c < n; c += NT) {
+        for (int64_t c = c_lo + t; c < c_hi; c += NT) {
 #pragma unroll
             for (int l = 0; l < N; ++l) {
                 double *x = A.p + l * A.ls + c * A.ld;
@@ -411,6 +415,34 @@ __global__ void __launch_bounds__(NT) lu_pivot_kernel(int64_t m, int64_t n, Mat 
     for (int l = 0; l < N; ++l) iv.v[l] = sinv[l];
     for (int64_t r = k + 1 + t; r < m; r += NT)
         store_mf<N>(A.p, A.ld, A.ls, r, k, mul(load_mf<N>(A.p, A.ld, A.ls, r, k), iv));
+}
+
+// The interchanges of panel steps first .. last (ipiv, ascending, as the
+// sequential row swaps of lu.jl) on every column outside [first, last]: one
+// thread per column.  Only the steps that ran are replayed: after a zero
+// pivot at step info-1 (no interchange there) the later steps never ran.
+template <int N>
+__global__ void lu_swap_rest_kernel(int64_t n, Mat A, int64_t first, int64_t last,
+                                    const int64_t *ipiv, const int *info) {
+    const int st = *info;
+    if (st < 0) return;
+    const int64_t upto = st == 0 ? last : (int64_t)st - 2;  // last step with an interchange
+    if (upto < first) return;
+    const int64_t w = last - first + 1;
+    const int64_t col = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= n - w) return;
+    const int64_t c = col < first ? col : col + w;
+    for (int64_t k = first; k <= upto; ++k) {
+        const int64_t p = ipiv[k] - 1;
+        if (p == k) continue;
+#pragma unroll
+        for (int l = 0; l < N; ++l) {
+            double *x = A.p + l * A.ls + c * A.ld;
+            const double tmp = x[k];
+            x[k] = x[p];
+            x[p] = tmp;
+        }
+    }
 }
 
 // rank-1 update of panel columns k+1..last for rows k+1..m-1 (lu.jl:47-82)
@@ -1348,7 +1380,7 @@ static int getrf_n(int64_t m, int64_t n, Mat A, int64_t *ipiv, int64_t block, in
     for (int64_t first = 0; first < kmax; first += block) {
         const int64_t last = first + block - 1 < kmax - 1 ? first + block - 1 : kmax - 1;
         for (int64_t k = first; k <= last; ++k) {
-            lu_pivot_kernel<N, 512><<<1, 512, 0, s>>>(m, n, A, k, ipiv, info);
+            lu_pivot_kernel<N, 512><<<1, 512, 0, s>>>(m, first, last + 1, A, k, ipiv, info);
             rc = record_cuda_error(cudaGetLastError(), "getrf pivot");
             if (rc) return rc;
             if (k < last && k + 1 < m) {
@@ -1357,6 +1389,15 @@ static int getrf_n(int64_t m, int64_t n, Mat A, int64_t *ipiv, int64_t block, in
                 rc = record_cuda_error(cudaGetLastError(), "getrf rank1");
                 if (rc) return rc;
             }
+        }
+        // the panel's interchanges on the other columns (also after a zero
+        // pivot, for the steps before it)
+        if (n > last - first + 1) {
+            const int64_t cols = n - (last - first + 1);
+            lu_swap_rest_kernel<N><<<(unsigned)((cols + 127) / 128), 128, 0, s>>>(n, A, first, last,
+                                                                                  ipiv, info);
+            rc = record_cuda_error(cudaGetLastError(), "getrf swaps");
+            if (rc) return rc;
         }
         if (last < n - 1) {
             const int64_t w = last - first + 1, rest = n - 1 - last;
@@ -1374,7 +1415,7 @@ static int getrf_n(int64_t m, int64_t n, Mat A, int64_t *ipiv, int64_t block, in
 }
 
 // LU with INT8 trailing updates: panels of nb columns factored by the blocked
-// algorithm above (pivot search and full-row interchanges, rank-1 updates,
+// algorithm above (pivot search and interchanges, rank-1 updates,
 // TRSM and GEMM restricted to the panel's columns), then U12 = L11^-1 A12 and
 // A22 -= L21 U12 through the modular INT8 route.  The device info word is read
 // after every panel (one synchronisation each) so that a zero pivot stops the
@@ -1396,7 +1437,7 @@ static int getrf_ozaki_n(mflab_handle *h, int64_t m, int64_t n, Mat A, int64_t *
         for (int64_t first = j0; first < j1; first += block) {
             const int64_t last = first + block - 1 < j1 - 1 ? first + block - 1 : j1 - 1;
             for (int64_t k = first; k <= last; ++k) {
-                lu_pivot_kernel<N, 512><<<1, 512, 0, s>>>(m, n, A, k, ipiv, info);
+                lu_pivot_kernel<N, 512><<<1, 512, 0, s>>>(m, first, last + 1, A, k, ipiv, info);
                 rc = record_cuda_error(cudaGetLastError(), "getrf pivot");
                 if (rc) return rc;
                 if (k < last && k + 1 < m) {
@@ -1406,6 +1447,13 @@ static int getrf_ozaki_n(mflab_handle *h, int64_t m, int64_t n, Mat A, int64_t *
                     rc = record_cuda_error(cudaGetLastError(), "getrf rank1");
                     if (rc) return rc;
                 }
+            }
+            if (n > last - first + 1) {
+                const int64_t cols = n - (last - first + 1);
+                lu_swap_rest_kernel<N><<<(unsigned)((cols + 127) / 128), 128, 0, s>>>(
+                    n, A, first, last, ipiv, info);
+                rc = record_cuda_error(cudaGetLastError(), "getrf swaps");
+                if (rc) return rc;
             }
             if (last < j1 - 1) {
                 const int64_t w = last - first + 1, cols = j1 - 1 - last;

@@ -102,11 +102,19 @@ __global__ void __launch_bounds__(NT) trsm_left_backward_cta(int64_t m, int64_t 
         }
         __syncthreads();
         if (t == 0) {
+            // the chain of subtractions is the row's latency; the product of
+            // the next term is read from shared memory while the current one
+            // is subtracted
             mf<N> v = load_mf<N>(B.p, B.ld, B.ls, r, col);
-            for (int64_t k = r + 1; k < m; ++k) {
-                mf<N> p;
+            mf<N> pn;
 #pragma unroll
-                for (int l = 0; l < N; ++l) p.v[l] = prod[k * N + l];
+            for (int l = 0; l < N; ++l) pn.v[l] = r + 1 < m ? prod[(r + 1) * N + l] : 0.0;
+            for (int64_t k = r + 1; k < m; ++k) {
+                const mf<N> p = pn;
+                if (k + 1 < m) {
+#pragma unroll
+                    for (int l = 0; l < N; ++l) pn.v[l] = prod[(k + 1) * N + l];
+                }
                 v = sub(v, p);
             }
             if (!unit) v = div(v, load_mf<N>(A.p, A.ld, A.ls, r, r));
