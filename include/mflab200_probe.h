@@ -70,6 +70,20 @@ int mflab_int8_gemm_tn(struct mflab_handle *h, void *stream, int engine, int64_t
    every issued copy and MMA drained, TMEM freed).  Nothing faults or hangs;
    the next launch with inject = 0 runs normally.  No reference counterpart. */
 int mflab_set_tc_debug(struct mflab_handle *h, int64_t wait_limit, int inject);
+
+/* Index checks of a debug build (libmflab200_debug.so, compiled with
+   -DMFLAB_DEBUG): out[0] = the number of failed device index checks since
+   the last reset, out[1..3] = the first one's check code and two index
+   values (codes: 1 TMA coordinate off the 16-byte rule or past K, 2 int8 GEMM
+   epilogue store outside the padded output, 3 residue split past its row,
+   4 reconstruction task outside the residue planes, 5 moved-row list of the
+   binary64 LU panel full, 6 GEMM column stride below the row count, 7 solve
+   step load outside its matrix, 8 interleaved copy strides).  A failed check
+   skips the access instead of trapping.  reset != 0 clears the records.
+   A release build always reports zeros.  mflab_debug_build() is 1 in a debug
+   build. */
+int mflab_debug_violations(long long *out, int reset);
+int mflab_debug_build(void);
 #ifdef __cplusplus
 }
 #endif

@@ -17,9 +17,12 @@ LIB_PATH = os.path.join(PKG_DIR, "libmflab200.so")
 CSRC = os.path.join(PKG_DIR, "csrc")
 INCLUDE = os.path.join(REPO_DIR, "include")
 
+# -fno-gnu-unique: the function-local statics of templates (the "attribute
+# already set" flags of the launchers) stay private to each library, so the
+# release and the debug build can be loaded into one process side by side
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
-    "--fmad=false", "-Xcompiler", "-fPIC", "-shared",
+    "--fmad=false", "-Xcompiler", "-fPIC", "-Xcompiler", "-fno-gnu-unique", "-shared",
 ]
 
 MFLAB_OK = 0
@@ -33,6 +36,10 @@ MFLAB_ERR_FLAG = -7
 
 
 OBJ_DIR = os.path.join(PKG_DIR, "_build")
+# the debug build: the same sources with -DMFLAB_DEBUG (device index checks
+# that record violations instead of trapping), loaded when MFLAB_DEBUG=1
+DEBUG_LIB_PATH = os.path.join(PKG_DIR, "libmflab200_debug.so")
+DEBUG_OBJ_DIR = os.path.join(PKG_DIR, "_build_debug")
 
 
 def sources() -> list[str]:
@@ -51,29 +58,39 @@ def _run(cmd: list[str]) -> str:
     return out.stdout + out.stderr
 
 
-def build(verbose: bool = False, jobs: int | None = None) -> str:
-    """Compile every CUDA source (sm_100a) into libmflab200.so in the package:
-    one nvcc per translation unit in parallel (objects under _build/, rebuilt
-    when the source or any header is newer), then one link."""
+def build(verbose: bool = False, jobs: int | None = None, debug: bool = True) -> str:
+    """Compile every CUDA source (sm_100a) into libmflab200.so in the package
+    and, with `debug`, into libmflab200_debug.so with -DMFLAB_DEBUG: one nvcc
+    per translation unit and variant in parallel (objects under _build/ and
+    _build_debug/, rebuilt when the source or any header is newer), then one
+    link per library.  Returns the release library's path."""
     from concurrent.futures import ThreadPoolExecutor
 
     nvcc = os.environ.get("NVCC", "nvcc")
-    os.makedirs(OBJ_DIR, exist_ok=True)
     newest_header = max((os.path.getmtime(h) for h in _headers()), default=0.0)
     compile_flags = [f for f in NVCC_FLAGS if f != "-shared"]
-    objs, todo = [], []
-    for src in sources():
-        obj = os.path.join(OBJ_DIR, os.path.basename(src)[:-3] + ".o")
-        objs.append(obj)
-        if not os.path.exists(obj) or os.path.getmtime(obj) < max(os.path.getmtime(src),
-                                                                    newest_header):
-            todo.append([nvcc, *compile_flags, "-I", INCLUDE, "-c", "-o", obj, src])
+    variants = [(OBJ_DIR, LIB_PATH, [])]
+    if debug:
+        variants.append((DEBUG_OBJ_DIR, DEBUG_LIB_PATH, ["-DMFLAB_DEBUG"]))
+    todo, links = [], []
+    for obj_dir, lib_path, extra in variants:
+        os.makedirs(obj_dir, exist_ok=True)
+        objs, stale = [], False
+        for src in sources():
+            obj = os.path.join(obj_dir, os.path.basename(src)[:-3] + ".o")
+            objs.append(obj)
+            if not os.path.exists(obj) or os.path.getmtime(obj) < max(os.path.getmtime(src),
+                                                                        newest_header):
+                todo.append([nvcc, *compile_flags, *extra, "-I", INCLUDE, "-c", "-o", obj, src])
+                stale = True
+        if stale or not os.path.exists(lib_path):
+            links.append([nvcc, *NVCC_FLAGS, "-o", lib_path, *objs, "-lcublasLt"])
     logs = []
     if todo:
         with ThreadPoolExecutor(max_workers=jobs or min(len(todo), os.cpu_count() or 4)) as ex:
             logs = list(ex.map(_run, todo))
-    if todo or not os.path.exists(LIB_PATH):
-        logs.append(_run([nvcc, *NVCC_FLAGS, "-o", LIB_PATH, *objs, "-lcublasLt"]))
+    for cmd in links:
+        logs.append(_run(cmd))
     if verbose:
         print("".join(logs))
     return LIB_PATH
@@ -185,6 +202,8 @@ SIGNATURES = {
     "mflab_d2h_interleaved": [_vp, _vp, _int, _i64, _i64, _vp, _i64, _i64, _vp, _i64],
     "mflab_interleaved_to_planes": [_vp, _vp, _int, _i64, _i64, _vp, _i64, _vp, _i64, _i64],
     "mflab_planes_to_interleaved": [_vp, _vp, _int, _i64, _i64, _vp, _i64, _i64, _vp, _i64],
+    "mflab_debug_violations": [C.POINTER(C.c_longlong), _int],
+    "mflab_debug_build": [],
 }
 _RESTYPE = {"mflab_status_string": C.c_char_p, "mflab_last_error": C.c_char_p}
 
@@ -192,11 +211,21 @@ _lib = None
 
 
 def load(path: str | None = None):
-    """Load the built library (no build, no fallback)."""
+    """Load the built library (no build, no fallback): libmflab200.so, or the
+    debug build when the environment sets MFLAB_DEBUG=1."""
     global _lib
     if _lib is not None:
         return _lib
-    path = path or LIB_PATH
+    if path is None:
+        path = DEBUG_LIB_PATH if os.environ.get("MFLAB_DEBUG") == "1" else LIB_PATH
+    lib = load_library(path)
+    _lib = lib
+    return lib
+
+
+def load_library(path: str):
+    """A separately loaded copy of a built library (its own handles and
+    device state), with the ctypes signatures set."""
     if not os.path.exists(path):
         raise RuntimeError(
             f"mflab200 CUDA library not found at {path}; build it with "
@@ -206,7 +235,6 @@ def load(path: str | None = None):
         fn = getattr(lib, name)
         fn.argtypes = args
         fn.restype = _RESTYPE.get(name, _int)
-    _lib = lib
     return lib
 
 

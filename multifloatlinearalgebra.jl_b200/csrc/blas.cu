@@ -16,6 +16,8 @@
 #include "mf_device.cuh"
 #include "mflab_internal.h"
 
+MFLAB_DEBUG_RECORD(blas)
+
 namespace mfl {
 
 __device__ __forceinline__ void cp_async8(void *smem, const void *gmem, bool pred) {
@@ -60,6 +62,8 @@ __global__ void __launch_bounds__(MMShape<N, BM, BN, BK, TM, TN>::NT)
     const int tx = tid % TX, ty = tid / TX;
     const int64_t row0 = (int64_t)blockIdx.x * BM, col0 = (int64_t)blockIdx.y * BN;
     if (TRI && row0 + BM - 1 < col0) return;  // tile strictly above the diagonal
+    // debug builds: C's column stride holds its rows
+    if (!(mode & MM_PACKED) && !MFLAB_IDX_OK(C.ld >= m, 6, C.ld, m)) return;
     if (info && *info) return;                 // an earlier factorization step failed
     // reduction range of this tile: all of K, or the triangular part TRMM needs
     int64_t kbeg = 0, kend = K;

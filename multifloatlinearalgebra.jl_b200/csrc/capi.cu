@@ -196,3 +196,35 @@ extern "C" int mflab_stream_synchronize(void *stream) {
     return mfl::record_cuda_error(cudaStreamSynchronize((cudaStream_t)stream),
                                   "mflab_stream_synchronize");
 }
+
+// index-check violations recorded by a debug build since the last reset:
+// out[0] the count, out[1..3] the first one's check code and index values
+// (all zero in a release build)
+extern "C" int mflab_debug_violations(long long *out, int reset) {
+    if (!out) return MFLAB_ERR_ARG;
+    long long tot[4] = {0, 0, 0, 0};
+#define MFLAB_DEBUG_SUM(tu)                                                  \
+    {                                                                        \
+        long long v[4];                                                      \
+        if (mfl_dbg_read_##tu(v, reset) != 0) return MFLAB_ERR_CUDA;         \
+        if (v[0] && !tot[0]) {                                               \
+            tot[1] = v[1];                                                   \
+            tot[2] = v[2];                                                   \
+            tot[3] = v[3];                                                   \
+        }                                                                    \
+        tot[0] += v[0];                                                      \
+    }
+    MFLAB_DEBUG_UNITS(MFLAB_DEBUG_SUM)
+#undef MFLAB_DEBUG_SUM
+    for (int i = 0; i < 4; ++i) out[i] = tot[i];
+    return MFLAB_OK;
+}
+
+// 1 in a debug build (-DMFLAB_DEBUG), else 0
+extern "C" int mflab_debug_build(void) {
+#ifdef MFLAB_DEBUG
+    return 1;
+#else
+    return 0;
+#endif
+}

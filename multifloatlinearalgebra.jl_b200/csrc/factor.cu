@@ -15,6 +15,8 @@
 
 #include "mflab_internal.h"
 
+MFLAB_DEBUG_RECORD(factor)
+
 namespace mfl {
 
 __global__ void iota1_kernel(int64_t *p, int64_t count) {
@@ -806,8 +808,10 @@ __global__ void __cluster_dims__(LUC_CL, 1, 1) __launch_bounds__(LUC_NT, 1)
             moved[dest - k0] = orig;
         } else if (dest != orig) {
             const int e = atomicAdd(&moved[2 * LUC_W], 1);
-            moved[LUC_W + e] = dest;              // ext rows
-            moved[2 * LUC_W + 1 + e] = orig;      // ext sources
+            if (MFLAB_IDX_OK(e < LUC_W, 5, e, dest)) {
+                moved[LUC_W + e] = dest;              // ext rows
+                moved[2 * LUC_W + 1 + e] = orig;      // ext sources
+            }
         }
     }
 }
@@ -1137,8 +1141,10 @@ __global__ void __cluster_dims__(LUC_CL, 1, 1) __launch_bounds__(LUR_NT, 1)
             moved[cur[r] - k0] = orig;
         } else if (cur[r] != orig) {
             const int e = atomicAdd(&moved[2 * LUC_W], 1);
-            moved[LUC_W + e] = cur[r];            // ext rows
-            moved[2 * LUC_W + 1 + e] = orig;      // ext sources
+            if (MFLAB_IDX_OK(e < LUC_W, 5, e, cur[r])) {
+                moved[LUC_W + e] = cur[r];            // ext rows
+                moved[2 * LUC_W + 1 + e] = orig;      // ext sources
+            }
         }
     }
 }

@@ -32,6 +32,8 @@
 
 #include "int8_tc_common.cuh"
 
+MFLAB_DEBUG_RECORD(int8_tc)
+
 namespace mfl {
 
 constexpr int TC_BM = 256, TC_MMA_M = 128, TC_BN = 256, TC_STAGES = 3;
@@ -130,8 +132,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     mbar_expect_tx(&full[s], TC_STAGE_BYTES);
                     // rows past the last plane read the map's zero fill; rows
                     // of the next plane (m % 256 == 128) feed no stored result
-                    tma_load_2d(sa, &tmA, kb * TC_BK, am0, &full[s]);
-                    tma_load_2d(sb, &tmB, b_xoff + kb * TC_BK, bn0, &full[s]);
+                    // debug builds: a copy whose inner coordinate breaks the
+                    // 16-byte rule is skipped (the stage then never fills and
+                    // the bounded waits report it)
+                    const int xa = kb * TC_BK, xb = b_xoff + kb * TC_BK;
+                    if (MFLAB_IDX_OK((xa & 15) == 0 && (xb & 15) == 0 && xa < K, 1, xa, xb)) {
+                        tma_load_2d(sa, &tmA, xa, am0, &full[s]);
+                        tma_load_2d(sb, &tmB, xb, bn0, &full[s]);
+                    }
                 }
                 if (!ok) break;
             }
@@ -222,7 +230,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 uint32_t v[16];
                 tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(half * TC_TMEM_COLS + c0),
                           v);
-                tc_store16<MODE>(Cz, ldc, row, n0 + c0, v, pz, pzinv);
+                if (MFLAB_IDX_OK(row < a_zrows && n0 + c0 + 16 <= tiles_n * TC_BN, 2, row, n0 + c0))
+                    tc_store16<MODE>(Cz, ldc, row, n0 + c0, v, pz, pzinv);
             }
             // accumulators drained: the MMA warp may overwrite them
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");

@@ -19,6 +19,8 @@
 
 #include "mflab_internal.h"
 
+MFLAB_DEBUG_RECORD(interleave)
+
 namespace mfl {
 
 namespace {
@@ -37,6 +39,9 @@ __global__ void __launch_bounds__(IL_THREADS)
                       double *__restrict__ P, int64_t ld, int64_t ls) {
     const int64_t r = (int64_t)blockIdx.x * IL_THREADS + threadIdx.x;
     if (r >= m) return;
+    // debug builds: the strides hold the rows (ldx, ld >= m) and the planes
+    if (!MFLAB_IDX_OK(ldx >= m && ld >= m && (N == 1 || ls >= ld * (n - 1) + m), 8, ld, ls))
+        return;
     for (int64_t c = blockIdx.y; c < n; c += gridDim.y) {
         double *x = X + (c * ldx + r) * N;
         double *p = P + c * ld + r;

@@ -28,6 +28,8 @@
 
 #include "mflab_internal.h"
 
+MFLAB_DEBUG_RECORD(lu64)
+
 namespace mfl {
 
 namespace {
@@ -167,7 +169,10 @@ __global__ void __launch_bounds__(MS_NT)
 #pragma unroll
         for (int u = 0; u < IB * MS_ROWS / MS_NT; ++u) {
             const int e = t + u * MS_NT, r = e % MS_ROWS, k = e / MS_ROWS;
-            x[u] = (r < nrows && k < jb) ? src[(int64_t)k * ld + r] : 0.0;
+            x[u] = (r < nrows && k < jb &&
+                    MFLAB_IDX_OK(rb + r < (diag ? (int64_t)IB : ldm), 7, rb + r, k))
+                       ? src[(int64_t)k * ld + r]
+                       : 0.0;
         }
 #pragma unroll
         for (int u = 0; u < IB * MS_ROWS / MS_NT; ++u) {

@@ -188,3 +188,49 @@ inline TcOpts tc_opts(const mflab_handle *h) {
 }
 inline bool tc_engine(const mflab_handle *h) { return h->int8_engine != MFLAB_INT8_LIBRARY; }
 }  // namespace mfl
+
+// Debug builds (-DMFLAB_DEBUG, libmflab200_debug.so): device index checks.
+// MFLAB_IDX_OK(cond, code, a, b) is true when cond holds; otherwise it
+// records the violation (the first one's code and two index values, and a
+// count) in the translation unit's debug record and is false, so the guarded
+// access is skipped — a check never traps.  MFLAB_DEBUG_RECORD(tu) defines
+// that record and its host reader mfl_dbg_read_<tu>; mflab_debug_violations
+// sums the readers.  Release builds compile the checks to `true`.
+namespace mfl {
+__device__ __forceinline__ bool dbg_note(unsigned long long *rec, int code, long long a,
+                                         long long b) {
+    if (atomicAdd(&rec[0], 1ULL) == 0ULL) {
+        rec[1] = (unsigned long long)code;
+        rec[2] = (unsigned long long)a;
+        rec[3] = (unsigned long long)b;
+    }
+    return false;
+}
+}  // namespace mfl
+#ifdef MFLAB_DEBUG
+#define MFLAB_DEBUG_RECORD(tu)                                                            \
+    static __device__ unsigned long long mfl_dbg_rec[4];                                  \
+    int mfl_dbg_read_##tu(long long *out, int reset) {                                    \
+        unsigned long long v[4] = {0, 0, 0, 0};                                           \
+        cudaError_t e = cudaMemcpyFromSymbol(v, mfl_dbg_rec, sizeof(v));                  \
+        for (int i = 0; i < 4; ++i) out[i] = (long long)v[i];                             \
+        if (e == cudaSuccess && reset) {                                                  \
+            const unsigned long long z[4] = {0, 0, 0, 0};                                 \
+            e = cudaMemcpyToSymbol(mfl_dbg_rec, z, sizeof(z));                            \
+        }                                                                                 \
+        return e == cudaSuccess ? 0 : -1;                                                 \
+    }
+#define MFLAB_IDX_OK(cond, code, a, b) \
+    ((cond) || ::mfl::dbg_note(mfl_dbg_rec, (code), (long long)(a), (long long)(b)))
+#else
+#define MFLAB_DEBUG_RECORD(tu)                                \
+    int mfl_dbg_read_##tu(long long *out, int) {              \
+        for (int i = 0; i < 4; ++i) out[i] = 0;               \
+        return 0;                                             \
+    }
+#define MFLAB_IDX_OK(cond, code, a, b) (true)
+#endif
+// the translation units with a debug record
+#define MFLAB_DEBUG_UNITS(X) X(int8_tc) X(ozaki_crt) X(lu64) X(factor) X(interleave) X(blas)
+#define MFLAB_DEBUG_DECL(tu) int mfl_dbg_read_##tu(long long *out, int reset);
+MFLAB_DEBUG_UNITS(MFLAB_DEBUG_DECL)

@@ -40,6 +40,8 @@
 #include "mflab_internal.h"
 #include "ozaki_common.cuh"
 
+MFLAB_DEBUG_RECORD(ozaki_crt)
+
 namespace mfl {
 
 constexpr int CRT_MAXT = CRT_TABLE_SIZE;
@@ -253,6 +255,7 @@ __global__ void __launch_bounds__(256)
         for (int l = N - 1; l > 0; --l) two_sum(z[u].v[l - 1], z[u].v[l], z[u].v[l - 1], z[u].v[l]);
     }
     int8_t *dst = A8 + (size_t)i * Q * kp + kg;
+    if (!MFLAB_IDX_OK(kg + U <= kp && i < mp, 3, i, kg)) return;
     for (int q = 0; q < Q; ++q) {
         uint32_t w[U][WD];
         bool ng[U];
@@ -289,6 +292,7 @@ __global__ void __launch_bounds__(128)
         for (int l = N - 1; l > 0; --l) two_sum(z[u].v[l - 1], z[u].v[l], z[u].v[l - 1], z[u].v[l]);
     }
     int8_t *dst = B8 + (size_t)j * Q * kp + kg;
+    if (!MFLAB_IDX_OK(kg + U <= kp && j < np, 3, j, kg)) return;
     for (int q = 0; q < Q; ++q) {
         uint32_t w[U][WD];
         bool ng[U];
@@ -663,6 +667,8 @@ __global__ void __launch_bounds__(CRT_TC_THREADS)
         const int64_t i0 = (task % mblk) * 128, j0 = (task / mblk) * J;
         // flags bit 2: lower triangle only (the GEMM skipped the tiles above it)
         if ((flags & 4) && i0 + 127 < j0) continue;
+        // debug builds: the task's 128 rows lie inside the padded planes
+        if (!MFLAB_IDX_OK(i0 + 128 <= ldi, 4, i0, j0)) continue;
         // 1. residue segments -> K-major rows (rows i0 .. i0+127 lie inside the
         //    padded planes; columns j >= n read nothing)
         for (int pr = warp; pr < SLOTS * kchunks; pr += CRT_TC_THREADS / 32) {

@@ -52,3 +52,17 @@ def test_capabilities(mf):
     c = mf.capabilities(2)
     assert c["supported"] and c["limb_count"] == 2 and c["syrk_authoritative_triangle"] == "lower"
     assert not mf.capabilities(7)["supported"]
+
+
+def test_debug_library_matches_release_exports(mf):
+    """the index-checking debug build (libmflab200_debug.so) exports the same
+    entry points; it reports itself as a debug build, the release as not"""
+    import os
+    nat = mf._native
+    if not os.path.exists(nat.DEBUG_LIB_PATH):
+        pytest.skip("debug library not built")
+    dbg = nat.load_library(nat.DEBUG_LIB_PATH)
+    missing = [n for n in nat.declared_symbols() if not hasattr(dbg, n)]
+    assert not missing, missing
+    assert dbg.mflab_debug_build() == 1
+    assert nat.load().mflab_debug_build() == 0
