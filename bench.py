@@ -55,6 +55,14 @@ def parse():
                    help="skip the factorization / mixed-LU / batched-SPD workloads")
     p.add_argument("--config-reps", type=int, default=3,
                    help="timed repeats (after one warm-up) of each of those workloads")
+    p.add_argument("--case", default=None,
+                   choices=["crt_gemm", "getrf64", "lu64_solve", "mixed_lu", "potrf", "getrf"],
+                   help="run one small workload (one warm-up call, then --steps calls) and "
+                        "exit: the cases the ncu summaries under profiles/ are taken on "
+                        "(crt_gemm: modular x2 GEMM at --n with --knob moduli; getrf64: "
+                        "binary64 LU at --n; lu64_solve: its 16-RHS prepared solve; "
+                        "mixed_lu: the mixed-precision solve at --n; potrf: Cholesky "
+                        "Float64x--limbs at --n; getrf: LU Float64x--limbs at --n)")
     p.add_argument("--split", default="replicas", choices=["replicas", "tiles"],
                    help="replicas: one independent problem per rank (weak scaling); tiles: "
                         "one problem held by rank 0, its 2-D output tiles computed by all "
@@ -756,8 +764,76 @@ def run_tiles(args, R, torch, dist, world, rank):
         print(json.dumps(line), flush=True)
 
 
+def run_case(args):
+    """One small workload for a profiler capture: a warm-up call, then
+    args.steps calls, timed with CUDA events (printed, not a bench value)."""
+    import ctypes as C
+    import torch
+    import __graft_entry__
+    mf = __graft_entry__.load_package()
+    from mflab200 import synthetic as syn
+    lib, n, N = mf._native.load(), args.n, args.limbs
+    h, s = mf._handle(0), torch.cuda.current_stream().cuda_stream
+    calls = []
+    if args.case == "crt_gemm":
+        A = mf.MFMatrix.zeros(N, n, n)
+        B = mf.MFMatrix.zeros(N, n, n)
+        Cm = mf.MFMatrix.zeros(N, n, n)
+        A.planes()[0].normal_()
+        B.planes()[0].normal_()
+        cfg = mf.KernelConfig(gemm_strategy="ozaki", ozaki_scheme="modular",
+                              ozaki_moduli=args.knob or 30)
+        calls.append(lambda: mf.gemm_(Cm, A, B, config=cfg))
+    elif args.case in ("getrf64", "lu64_solve", "mixed_lu"):
+        A, B = syn.mixed_lu_problem(mf, n, 16, seed=4)
+        LU = mf._leading_limb(A)
+        LU0 = LU.storage.clone()
+        ipiv = torch.arange(1, n + 1, dtype=torch.int64, device="cuda")
+        info = torch.zeros(1, dtype=torch.int32, device="cuda")
+
+        def factor():
+            LU.storage.copy_(LU0)
+            lib.mflab_getrf(h, s, 1, n, n, LU.ptr(), LU.ld, LU.ls, ipiv.data_ptr(), 32,
+                            info.data_ptr())
+        if args.case == "getrf64":
+            calls.append(factor)
+        elif args.case == "lu64_solve":
+            factor()
+            wb = C.c_size_t()
+            lib.mflab_lu64_work_bytes(n, C.byref(wb))
+            work = torch.empty(wb.value, dtype=torch.uint8, device="cuda")
+            lib.mflab_lu64_prepare(h, s, n, LU.ptr(), LU.ld, ipiv.data_ptr(), work.data_ptr())
+            D = mf._leading_limb(B)
+            calls.append(lambda: lib.mflab_lu64_solve(h, s, n, D.n, LU.ptr(), LU.ld,
+                                                      work.data_ptr(), D.ptr(), D.ld))
+        else:
+            calls.append(lambda: mf.solve_mixed_lu(A, B, tol=1e-60))
+    elif args.case == "potrf":
+        S = syn.spd_matrix_device(mf, 3, N, n)
+        Aw = S.copy()
+        calls.append(lambda: (Aw.copy_(S), mf.cholesky_(Aw)))
+    elif args.case == "getrf":
+        A, _ = syn.mixed_lu_problem(mf, n, 1, seed=4)
+        A = mf.MFMatrix(A.storage[:N].clone())
+        Aw = A.copy()
+        calls.append(lambda: (Aw.copy_(A), mf.lu_(Aw)))
+    fn = calls[0]
+    fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(max(args.steps, 1)):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    print(json.dumps({"case": args.case, "n": n, "limbs": N,
+                      "ms_per_call": e0.elapsed_time(e1) / max(args.steps, 1)}))
+
+
 def main():
     args = parse()
+    if args.case:
+        return run_case(args)
     if args.impl == "reference":
         return run_reference(args)
     import numpy as np
