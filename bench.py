@@ -905,9 +905,10 @@ def main():
     # element together): every step uploads A and B from pinned interleaved
     # host memory into limb planes (mflab_h2d_interleaved), multiplies, and
     # downloads C back to interleaved host memory (mflab_d2h_interleaved);
-    # the upload of step i+1 and the download of step i-1 run on their own
-    # streams (each with its own handle, whose staging they use) while step
-    # i multiplies (two device buffer sets)
+    # the uploads of step i+1 (A and B each on a stream and handle of its
+    # own, so that B's copy does not wait for A's permutation kernel) and the
+    # download of step i-1 run while step i multiplies (two device buffer
+    # sets); the staging of one handle takes a whole 1 GiB matrix per copy
     hA = torch.empty((n, n, N), dtype=torch.float64, pin_memory=True)
     hB = torch.empty((n, n, N), dtype=torch.float64, pin_memory=True)
     hC = torch.empty((n, n, N), dtype=torch.float64, pin_memory=True)
@@ -915,28 +916,32 @@ def main():
     B.copy_to_interleaved_(hB)
     torch.cuda.synchronize()
     bufs = [tuple(mf.MFMatrix.empty(N, n, n) for _ in range(3)) for _ in range(2)]
-    h_up, h_down = mf.create_handle(local), mf.create_handle(local)
+    h_upA, h_upB, h_down = (mf.create_handle(local) for _ in range(3))
 
     def e2e_run(steps):
         cs = torch.cuda.current_stream()
-        hs, ds = torch.cuda.Stream(), torch.cuda.Stream()
-        up = [torch.cuda.Event() for _ in range(2)]
+        hsA, hsB, ds = torch.cuda.Stream(), torch.cuda.Stream(), torch.cuda.Stream()
+        upA = [torch.cuda.Event() for _ in range(2)]
+        upB = [torch.cuda.Event() for _ in range(2)]
         done = [torch.cuda.Event() for _ in range(2)]
         down = [torch.cuda.Event() for _ in range(2)]
         R.barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(cs)
-        hs.wait_event(e0)
-        ds.wait_event(e0)
+        for st in (hsA, hsB, ds):
+            st.wait_event(e0)
         for i in range(steps):
             b = i % 2
             dA, dB, dC = bufs[b]
-            if i >= 2:
-                hs.wait_event(done[b])  # step i-2 no longer reads this set
-            dA.copy_from_interleaved_(hA, stream=hs, handle=h_up)
-            dB.copy_from_interleaved_(hB, stream=hs, handle=h_up)
-            up[b].record(hs)
-            cs.wait_event(up[b])
+            if i >= 2:  # step i-2 no longer reads this set
+                hsA.wait_event(done[b])
+                hsB.wait_event(done[b])
+            dA.copy_from_interleaved_(hA, stream=hsA, handle=h_upA)
+            upA[b].record(hsA)
+            dB.copy_from_interleaved_(hB, stream=hsB, handle=h_upB)
+            upB[b].record(hsB)
+            cs.wait_event(upA[b])
+            cs.wait_event(upB[b])
             if i >= 2:
                 cs.wait_event(down[b])  # step i-2's result has left dC
             mf.gemm_(dC, dA, dB, config=head_cfg)
@@ -944,8 +949,8 @@ def main():
             ds.wait_event(done[b])
             dC.copy_to_interleaved_(hC, stream=ds, handle=h_down)
             down[b].record(ds)
-        cs.wait_stream(hs)
-        cs.wait_stream(ds)
+        for st in (hsA, hsB, ds):
+            cs.wait_stream(st)
         e1.record(cs)
         R.barrier()
         return R.sharding.max_over_ranks(e0.elapsed_time(e1) / 1e3)
@@ -957,8 +962,8 @@ def main():
     mf.gemm_(Cm, A, B, config=head_cfg)
     e2e_ok = bool(torch.equal(torch.from_numpy(Cm.to_interleaved()), hC))
     torch.cuda.synchronize()
-    mf.destroy_handle(h_up)
-    mf.destroy_handle(h_down)
+    for hh in (h_upA, h_upB, h_down):
+        mf.destroy_handle(hh)
     del bufs, hA, hB, hC
     instr = float(n) ** 3 * ops_per_term(N)
     plain_roof = {"bound": "fp64", "achieved": instr / t_plain / 1e12, "peak": peak_fp64 / 1e12,

@@ -59,6 +59,8 @@ extern "C" int mflab_create(mflab_handle **out, int device) {
     h->tc_inject = 0;
     h->stage = nullptr;
     h->il_stream[0] = h->il_stream[1] = nullptr;
+    h->stage_half = 0;
+    h->il_next = 0;
     h->il_fork = h->il_done[0] = h->il_done[1] = nullptr;
     h->la_stream = nullptr;
     h->la_ev[0] = h->la_ev[1] = h->la_ev[2] = nullptr;

@@ -26,7 +26,9 @@ namespace mfl {
 namespace {
 
 constexpr int IL_THREADS = 256;
-constexpr size_t IL_STAGE_HALF = size_t(32) << 20;  // bytes per staging half
+// bytes per staging half: the transfer's size, between 32 MiB and 1 GiB, so
+// a matrix of up to 1 GiB moves in one copy that never waits for a kernel
+constexpr size_t IL_STAGE_MIN = size_t(32) << 20, IL_STAGE_MAX = size_t(1) << 30;
 
 // dst planes <- src interleaved (to_planes = true), or the reverse.  One
 // thread per element: the N limbs of an element are contiguous in the
@@ -120,10 +122,22 @@ int check_args(mflab_handle *h, int limbs, int64_t m, int64_t n, const void *X, 
     return MFLAB_OK;
 }
 
-// the staging buffer, two non-blocking streams of the highest priority and
-// their events, created on the first host <-> device conversion
-int reserve_stage(mflab_handle *h) {
-    if (h->stage) return MFLAB_OK;
+// the staging buffer (two halves of at least `bytes`, within the bounds
+// above), two non-blocking streams of the highest priority and their events,
+// created on the first host <-> device conversion; a larger transfer later
+// regrows the halves once the streams are idle
+int reserve_stage(mflab_handle *h, size_t bytes) {
+    size_t want = bytes < IL_STAGE_MIN ? IL_STAGE_MIN : (bytes > IL_STAGE_MAX ? IL_STAGE_MAX : bytes);
+    want = (want + IL_STAGE_MIN - 1) / IL_STAGE_MIN * IL_STAGE_MIN;
+    if (h->stage && h->stage_half >= want) return MFLAB_OK;
+    if (h->stage) {
+        cudaError_t e = cudaSuccess;
+        for (int i = 0; i < 2 && e == cudaSuccess; ++i) e = cudaStreamSynchronize(h->il_stream[i]);
+        if (e == cudaSuccess) e = cudaFree(h->stage);
+        h->stage = nullptr;
+        h->stage_half = 0;
+        if (e != cudaSuccess) return record_cuda_error(e, "staging regrow");
+    }
     int lo = 0, hi = 0;
     cudaError_t e = cudaDeviceGetStreamPriorityRange(&lo, &hi);
     for (int i = 0; i < 2 && e == cudaSuccess; ++i) {
@@ -135,12 +149,13 @@ int reserve_stage(mflab_handle *h) {
     if (e == cudaSuccess && !h->il_fork)
         e = cudaEventCreateWithFlags(&h->il_fork, cudaEventDisableTiming);
     if (e != cudaSuccess) return record_cuda_error(e, "staging streams");
-    e = cudaMalloc(&h->stage, 2 * IL_STAGE_HALF);
+    e = cudaMalloc(&h->stage, 2 * want);
     if (e != cudaSuccess) {
         record_cuda_error(e, "staging cudaMalloc");
         h->stage = nullptr;
         return MFLAB_ERR_ALLOC;
     }
+    h->stage_half = want;
     return MFLAB_OK;
 }
 
@@ -149,9 +164,9 @@ int reserve_stage(mflab_handle *h) {
 struct Chunks {
     int64_t rb, cb;
 };
-Chunks chunking(int N, int64_t m) {
+Chunks chunking(int N, int64_t m, size_t half) {
     const int64_t elem = N * (int64_t)sizeof(double);
-    const int64_t rows_per_half = (int64_t)IL_STAGE_HALF / elem;
+    const int64_t rows_per_half = (int64_t)half / elem;
     if (m <= rows_per_half) return {m, std::max<int64_t>(1, rows_per_half / m)};
     return {rows_per_half, 1};
 }
@@ -160,30 +175,34 @@ Chunks chunking(int N, int64_t m) {
 // and runs on internal stream j mod 2: its copy and its permutation kernel
 // are ordered on that stream (so chunk j + 2 reuses the half only after
 // chunk j is done with it), while the copy engine moves chunk j + 1 on the
-// other stream during chunk j's kernel.  Both streams start after the
-// caller's stream reaches this point (fork event) and the caller's stream
-// continues after both (join events), so the call is stream-ordered like
-// the others.  The high priority lets the small permutation kernels start
-// ahead of pending blocks of long kernels on other streams.
+// other stream during chunk j's kernel.  The chunk count continues across
+// calls (the handle remembers it), so two consecutive matrices of up to
+// 1 GiB go to different halves: the second one's copy does not wait for the
+// first one's permutation kernel, which may itself wait for SMs held by the
+// caller's long kernels.  Both streams start after the caller's stream
+// reaches this point (fork event) and the caller's stream continues after
+// both (join events), so the call is stream-ordered like the others.  The
+// high priority lets the permutation kernels start ahead of pending blocks of
+// long kernels on other streams.
 template <bool H2D>
 int staged(mflab_handle *h, int N, int64_t m, int64_t n, double *host, int64_t ldh, double *P,
            int64_t ld, int64_t ls, cudaStream_t s) {
-    int rc = reserve_stage(h);
+    int rc = reserve_stage(h, (size_t)m * n * N * sizeof(double));
     if (rc) return rc;
     const char *what = H2D ? "mflab_h2d_interleaved" : "mflab_d2h_interleaved";
     cudaError_t e = cudaEventRecord(h->il_fork, s);
     for (int i = 0; i < 2 && e == cudaSuccess; ++i) e = cudaStreamWaitEvent(h->il_stream[i], h->il_fork, 0);
     if (e != cudaSuccess) return record_cuda_error(e, what);
-    const Chunks ch = chunking(N, m);
+    const Chunks ch = chunking(N, m, h->stage_half);
     const size_t hpitch = (size_t)ldh * N * sizeof(double);
-    int64_t j = 0;
+    int64_t j = h->il_next;
     for (int64_t c0 = 0; c0 < n; c0 += ch.cb) {
         const int64_t w = std::min(ch.cb, n - c0);
         for (int64_t r0 = 0; r0 < m; r0 += ch.rb, ++j) {
             const int64_t hgt = std::min(ch.rb, m - r0);
             const size_t row_bytes = (size_t)hgt * N * sizeof(double);
             cudaStream_t cs = h->il_stream[j & 1];
-            double *st = (double *)((char *)h->stage + (j & 1) * IL_STAGE_HALF);
+            double *st = (double *)((char *)h->stage + (j & 1) * h->stage_half);
             double *hp = host + (c0 * ldh + r0) * N;
             double *pp = P + c0 * ld + r0;
             if (H2D) {
@@ -199,6 +218,7 @@ int staged(mflab_handle *h, int N, int64_t m, int64_t n, double *host, int64_t l
             }
         }
     }
+    h->il_next = (int)(j & 1);
     for (int i = 0; i < 2 && e == cudaSuccess; ++i) {
         e = cudaEventRecord(h->il_done[i], h->il_stream[i]);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(s, h->il_done[i], 0);

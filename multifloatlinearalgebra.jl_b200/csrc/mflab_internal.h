@@ -164,6 +164,8 @@ struct mflab_handle {
     // staging of the interleaved host <-> limb-plane copies (64 MiB, on first
     // use) and the two high-priority streams that alternate over its halves
     void *stage;
+    size_t stage_half;  // bytes per staging half (0 until the first conversion)
+    int il_next;        // staging half / internal stream of the next chunk
     cudaStream_t il_stream[2];
     cudaEvent_t il_fork, il_done[2];
     // the high-priority panel stream of the look-ahead binary64 LU and its
