@@ -168,6 +168,70 @@ __device__ __forceinline__ void crt_digit(mf<N> &z, int h, uint32_t (&w)[WD], bo
     neg = carry < 0;
 }
 
+// The same digit for h <= CRT_FAST_H and WD <= 4, with the sum formed as one
+// 128-bit two's-complement integer: the leading limb's 53-bit mantissa
+// shifted by its exponent (below 64 bits of shift for these h), each lower
+// limb converted exactly to an int64 (|d_l| <= 2^(h-54) + 1 < 2^63) and
+// added with carries.  D is the same exact integer, so the words and the
+// sign are those of crt_digit.
+constexpr int CRT_FAST_H = 116;
+
+template <int N, int WD>
+__device__ __forceinline__ void crt_digit_fast(mf<N> &z, int h, uint32_t (&w)[WD], bool &neg) {
+    static_assert(WD <= 4, "128-bit sum");
+    double d[N];
+#pragma unroll
+    for (int l = 0; l < N; ++l) {
+        z.v[l] = z.v[l] * pow2i(h);                // exact (h <= 157, |z| < 2)
+        d[l] = rint(z.v[l]);
+        z.v[l] = __dsub_rn(z.v[l], d[l]);          // exact: |z_l - rint(z_l)| <= 1/2
+    }
+#pragma unroll
+    for (int l = N - 1; l > 0; --l) two_sum(z.v[l - 1], z.v[l], z.v[l - 1], z.v[l]);
+    uint64_t lo = 0, hi = 0;
+    {
+        const uint64_t bits = (uint64_t)__double_as_longlong(d[0]);
+        const int e = (int)((bits >> 52) & 0x7ff) - 1075;
+        if (d[0] != 0.0 && e >= 0) {  // |d_0| >= 2^53: mantissa << e, e < 64
+            const uint64_t mm = (bits & ((1ULL << 52) - 1)) | (1ULL << 52);
+            lo = mm << e;
+            hi = e ? mm >> (64 - e) : 0ULL;
+            if (bits >> 63) {  // negate the 128-bit value
+                lo = ~lo + 1ULL;
+                hi = ~hi + (lo == 0ULL ? 1ULL : 0ULL);
+            }
+        } else {  // |d_0| < 2^53: an exact int64
+            const int64_t v = __double2ll_rn(d[0]);
+            lo = (uint64_t)v;
+            hi = v < 0 ? ~0ULL : 0ULL;
+        }
+    }
+#pragma unroll
+    for (int l = 1; l < N; ++l) {
+        const int64_t v = __double2ll_rn(d[l]);
+        const uint64_t a = (uint64_t)v, ah = v < 0 ? ~0ULL : 0ULL;
+        const uint64_t s0 = lo + a;
+        hi = hi + ah + (s0 < lo ? 1ULL : 0ULL);
+        lo = s0;
+    }
+    const uint32_t ws[4] = {(uint32_t)lo, (uint32_t)(lo >> 32), (uint32_t)hi, (uint32_t)(hi >> 32)};
+#pragma unroll
+    for (int j = 0; j < WD; ++j) w[j] = ws[j];
+    neg = (int64_t)hi < 0;
+}
+
+// the digit step of the split kernels: the 128-bit path where it applies
+template <int N, int WD>
+__device__ __forceinline__ void crt_digit_any(mf<N> &z, int h, uint32_t (&w)[WD], bool &neg) {
+    if constexpr (WD <= 4) {
+        if (h <= CRT_FAST_H) {
+            crt_digit_fast<N, WD>(z, h, w, neg);
+            return;
+        }
+    }
+    crt_digit<N, WD>(z, h, w, neg);
+}
+
 // (D + 128) mod p from the two's-complement words of D (off = 128 for D >= 0,
 // the modulus' negoff for D < 0); the stored byte is this value - 128, an
 // int8 congruent to D mod p
@@ -260,7 +324,7 @@ __global__ void __launch_bounds__(256)
         uint32_t w[U][WD];
         bool ng[U];
 #pragma unroll
-        for (int u = 0; u < U; ++u) crt_digit<N, WD>(z[u], h, w[u], ng[u]);
+        for (int u = 0; u < U; ++u) crt_digit_any<N, WD>(z[u], h, w[u], ng[u]);
         crt_emit<WD, U>(w, ng, T, dst + (size_t)(rev ? Q - 1 - q : q) * kp, plane8, c);
     }
 }
@@ -297,7 +361,7 @@ __global__ void __launch_bounds__(128)
         uint32_t w[U][WD];
         bool ng[U];
 #pragma unroll
-        for (int u = 0; u < U; ++u) crt_digit<N, WD>(z[u], h, w[u], ng[u]);
+        for (int u = 0; u < U; ++u) crt_digit_any<N, WD>(z[u], h, w[u], ng[u]);
         crt_emit<WD, U>(w, ng, T, dst + (size_t)(rev ? Q - 1 - q : q) * kp, plane8, c);
     }
 }
