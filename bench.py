@@ -56,13 +56,16 @@ def parse():
     p.add_argument("--config-reps", type=int, default=3,
                    help="timed repeats (after one warm-up) of each of those workloads")
     p.add_argument("--case", default=None,
-                   choices=["crt_gemm", "getrf64", "lu64_solve", "mixed_lu", "potrf", "getrf"],
+                   choices=["crt_gemm", "getrf64", "lu64_solve", "mixed_lu", "potrf", "getrf",
+                            "batched"],
                    help="run one small workload (one warm-up call, then --steps calls) and "
                         "exit: the cases the ncu summaries under profiles/ are taken on "
                         "(crt_gemm: modular x2 GEMM at --n with --knob moduli; getrf64: "
                         "binary64 LU at --n; lu64_solve: its 16-RHS prepared solve; "
                         "mixed_lu: the mixed-precision solve at --n; potrf: Cholesky "
-                        "Float64x--limbs at --n; getrf: LU Float64x--limbs at --n)")
+                        "Float64x--limbs at --n; getrf: LU Float64x--limbs at --n; batched: "
+                        "--n Float64x--limbs SPD blocks of sizes U{8..256}, factor + solve "
+                        "with --knob threads per CTA and 8 CTAs per SM)")
     p.add_argument("--split", default="replicas", choices=["replicas", "tiles"],
                    help="replicas: one independent problem per rank (weak scaling); tiles: "
                         "one problem held by rank 0, its 2-D output tiles computed by all "
@@ -812,6 +815,16 @@ def run_case(args):
         S = syn.spd_matrix_device(mf, 3, N, n)
         Aw = S.copy()
         calls.append(lambda: (Aw.copy_(S), mf.cholesky_(Aw)))
+    elif args.case == "batched":
+        import numpy as np
+        sizes = np.random.default_rng(5).integers(8, 257, n)
+        batch = mf.batched.SPDBatch(N, sizes)
+        syn.spd_batch_fill(mf, batch, seed=5)
+        S0, X0 = batch.S.clone(), batch.X.clone()
+        sms = torch.cuda.get_device_properties(0).multi_processor_count
+        shape = {"threads": args.knob or 128, "grid": sms * 8}
+        calls.append(lambda: (batch.S.copy_(S0), batch.X.copy_(X0),
+                              mf.batched.potrf_potrs_batched_(batch, tuning=shape)))
     elif args.case == "getrf":
         A, _ = syn.mixed_lu_problem(mf, n, 1, seed=4)
         A = mf.MFMatrix(A.storage[:N].clone())

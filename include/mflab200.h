@@ -477,14 +477,17 @@ int mflab_ldlt_diagnostics(mflab_handle *h, void *stream, int limbs, int64_t n, 
                            const uint8_t *blocks, const double *omax, double *out);
 
 /* ------------------------------------------------------- batched SPD --- */
-/* Factor (and with solve != 0 also solve) nblocks independent SPD blocks in
-   one persistent launch.  Block b is sizes[b] x sizes[b], column-major at
+/* Factor (and with solve != 0 also solve) nblocks independent SPD blocks:
+   one persistent launch factors every block and runs its forward
+   substitution, a second launch runs the backward substitutions (their
+   one-term-at-a-time chains, several blocks per warp).  Block b is sizes[b] x sizes[b], column-major at
    S + offsets[b] (ld = sizes[b]), its right-hand side a vector at X +
    boffsets[b]; limb planes are ls_s / ls_x apart.  CTAs take blocks in the
    order order[0..nblocks) from the device counter (reset here with one
    stream-ordered memset).  Each block follows cholesky!(S_b; block) and
    ldiv!(x_b, F_b) exactly; info[b] receives 0 or the failing column.
-   max_size <= 512.  grid <= 0 picks 4 CTAs per SM.  No allocation, no
+   max_size <= 512 bounds every sizes[b] (it sizes the per-CTA shared
+   buffer); a block larger than max_size is left untouched with info[b] = -1.  grid <= 0 picks 4 CTAs per SM.  No allocation, no
    synchronisation.  No reference counterpart (the reference factors one
    matrix per call: src/factorizations/cholesky.jl:68-107). */
 int mflab_spd_batched(mflab_handle *h, void *stream, int limbs, int64_t nblocks, int64_t max_size,
@@ -503,7 +506,7 @@ int mflab_spd_batched_adjoint(mflab_handle *h, void *stream, int limbs, int64_t 
                               const int *info, int *counter, int grid);
 
 /* mflab_spd_batched / mflab_spd_batched_adjoint with the CTA size chosen:
-   threads = 128, 256 or 512 (the plain entries use 256).  Neither the CTA
+   threads = 64, 128, 256 or 512 (the plain entries use 256).  Neither the CTA
    size nor the number of persistent CTAs (grid) changes any result: every
    block's arithmetic is per element in the reference order; they are the
    knobs of the batched autotuner.  No reference counterpart. */

@@ -111,9 +111,9 @@ def _signature(batch: SPDBatch, block: int) -> tuple:
 def autotune(batch: SPDBatch, block: int = 16, candidates: Optional[Sequence] = None,
              reps: int = 2, profile=None) -> dict:
     """Launch shape of the batched factor + solve for this batch: the CTA size
-    (128, 256 or 512 threads) and the number of persistent CTAs (1, 2, 4 or 8
-    per SM), picked by timing the real launch on the batch's own blocks
-    (restored afterwards).  Neither knob changes any result (each block's
+    (64, 128, 256 or 512 threads) and the number of persistent CTAs (1 to 32
+    per SM, at most 2048 threads per SM), picked by timing the real launch on
+    the batch's own blocks (restored afterwards).  Neither knob changes any result (each block's
     arithmetic is per element in the reference order), so the choice is free.
     Cached per (limbs, block, size signature of the batch); a tuning
     profile (tuning.TuneProfile, fingerprint checked) that holds this
@@ -132,7 +132,8 @@ def autotune(batch: SPDBatch, block: int = 16, candidates: Optional[Sequence] = 
         return {"threads": 256, "grid": 0, "ms": 0.0, "timings": {}}
     sms = torch.cuda.get_device_properties(batch.device).multi_processor_count
     cands = list(candidates) if candidates is not None else [
-        (nt, cps) for nt in (128, 256, 512) for cps in (1, 2, 4, 8) if nt * cps <= 2048]
+        (nt, cps) for nt in (64, 128, 256, 512) for cps in (1, 2, 4, 8, 16, 32)
+        if nt * cps <= 2048]
     S0, X0 = batch.S.clone(), batch.X.clone()
     timings = {}
     best = None

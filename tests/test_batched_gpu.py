@@ -186,17 +186,48 @@ def test_batched_adjoint_vs_mpmath_gradient(mf, ref, rng):
                 assert abs(mpv(got_S[:, r, c]) - want) <= 1e-28 * (1 + abs(want))
 
 
+@pytest.mark.parametrize("threads", [64, 512])
+def test_batched_block_above_max_size_is_refused(mf, ref, rng, threads):
+    """max_size sizes each CTA's shared row buffer: a block larger than the
+    declared max_size is skipped with info = -1 and left untouched, the
+    others are factored and solved as usual"""
+    N = 2
+    sizes = np.array([12, 40, 9])
+    blocks = _spd_blocks(ref, rng, N, sizes)
+    batch = mf.batched.SPDBatch(N, sizes)
+    for i, S in enumerate(blocks):
+        batch.set_block(i, S)
+        batch.set_rhs(i, np.ones((N, sizes[i])))
+    S_before = batch.block(1)
+    lib = mf._native.load()
+    rc = lib.mflab_spd_batched_ex(
+        mf._handle(batch.device), torch.cuda.current_stream().cuda_stream, N, batch.nblocks, 12,
+        batch.sizes.data_ptr(), batch.offsets.data_ptr(), batch.boffsets.data_ptr(),
+        batch.order.data_ptr(), batch.S.data_ptr(), batch.S.shape[1], batch.X.data_ptr(),
+        batch.X.shape[1], 16, 1, batch.info.data_ptr(), batch.counter.data_ptr(), 2, threads)
+    assert rc == 0
+    info = batch.info[:3].cpu().numpy()
+    assert info[0] == 0 and info[1] == -1 and info[2] == 0
+    assert_bitwise(batch.block(1), S_before, "refused block untouched")
+    for i in (0, 2):
+        L, _ = ref.potrf(blocks[i])
+        assert_bitwise(np.tril(batch.block(i)), np.tril(L), f"factor {i}")
+        assert_bitwise(batch.rhs(i), ref.potrs(L, np.ones((N, sizes[i], 1)))[:, :, 0],
+                       f"solve {i}")
+
+
 @pytest.mark.parametrize("N", [2, 4])
 def test_batched_launch_shapes_bitwise(mf, ref, rng, N):
     """every CTA size and persistent-CTA count the autotuner may pick gives the
     same factors, solutions and adjoint bit for bit (blocks up to 500, so the
-    128-thread CTA holds four rows per thread); the tuner returns one of them"""
+    64-thread CTA holds eight rows per thread); the tuner returns one of them"""
     sizes = rng.integers(1, 90, 30)
     sizes[5], sizes[11] = 500, 260
     blocks = _spd_blocks(ref, rng, N, sizes)
     rhs = [syn.randn_mf(rng, N, int(n), 1)[:, :, 0] for n in sizes]
     outs = []
-    for threads, grid in [(256, 0), (128, 7), (512, 3), (128, 0), (512, 148)]:
+    for threads, grid in [(256, 0), (128, 7), (512, 3), (128, 0), (512, 148), (64, 5),
+                          (64, 148 * 32)]:
         batch = mf.batched.SPDBatch(N, sizes)
         for i, (S, b) in enumerate(zip(blocks, rhs)):
             batch.set_block(i, S)
@@ -217,7 +248,7 @@ def test_batched_launch_shapes_bitwise(mf, ref, rng, N):
     S_before = batch.S.clone()
     t = mf.batched.autotune(batch, reps=1)
     # 30 blocks: every persistent-CTA count clamps to 30, one shape per CTA size
-    assert t["threads"] in (128, 256, 512) and t["grid"] == 30 and len(t["timings"]) == 3
+    assert t["threads"] in (64, 128, 256, 512) and t["grid"] == 30 and len(t["timings"]) == 4
     assert torch.equal(batch.S, S_before), "autotune must restore the batch"
     info = mf.batched.potrf_potrs_batched_(batch, tuning="auto")
     assert np.all(info == 0)
