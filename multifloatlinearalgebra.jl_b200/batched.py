@@ -2,17 +2,19 @@
 
 No reference counterpart: MultiFloatLinearAlgebra.jl factors one matrix per
 call.  Every block here follows cholesky!(S_i) / ldiv!(x_i, F_i) of the
-reference exactly (one persistent CTA per block at a time), so per block the
-results equal the single-matrix routines.
+reference exactly (one persistent CTA per block for the factor and the
+forward substitution, a group of four lanes per block for the backward
+substitution), so per block the results equal the single-matrix routines.
 
     batch = SPDBatch(N, sizes)              # packed device storage
     batch.set_block(i, S_i); batch.set_rhs(i, b_i)
     x, pullback = solve_spd_batched_rrule(batch)
     Sbar, bbar = pullback(xbar)             # ChainRulesCore-style pullback
 
-`BatchedSPDGraph` captures the whole launch (counter reset + persistent
-kernel) in a CUDA graph and replays it.  `autotune` picks the launch shape
-(CTA size, number of persistent CTAs) by timing the batch itself.
+`BatchedSPDGraph` captures the whole solve (counter reset, the persistent
+factor kernel, the backward-substitution kernel) in a CUDA graph and
+replays it.  `autotune` picks the launch shape (CTA size, number of
+persistent CTAs) by timing the batch itself.
 """
 from __future__ import annotations
 
