@@ -710,7 +710,8 @@ def config_batched(R, torch, peak, reps):
         "md_gflops": batch.flops() / t_b / 1e9, "adjoint_ms": t_a * 1e3,
         "failed_blocks": int(np.count_nonzero(info)),
         "roofline": _fp64_roof(instr, t_b, peak),
-        "launch": "one persistent kernel (+ counter memset) replayed from a CUDA graph",
+        "launch": "counter memset, the persistent factor + forward-substitution kernel and the "
+                  "backward-substitution kernel, replayed from a CUDA graph",
         "autotuned": {"threads": tuned["threads"], "grid": tuned["grid"],
                       "default_256x592_ms": tuned["timings"].get("256x592")},
         "parity": parity, "cpu_baseline": cpu,
