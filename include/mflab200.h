@@ -222,6 +222,19 @@ int mflab_getrf_ozaki(mflab_handle *h, void *stream, int limbs, int moduli, int6
    reference counterpart). */
 int mflab_ozaki_last_moduli(mflab_handle *h);
 
+/* The modulus count that mflab_gemm_ozaki_crt with moduli = 0 would choose
+   for A (m x k) and B (k x n): the same scale pass and sampled scale gap, one
+   stream synchronisation, no product.  A caller that prepares A once
+   (mflab_ozaki_crt_prepare) takes the count from here.  A product at a given
+   count uses digits as wide as that count allows, at least as wide as the
+   tuned call's (which are only as wide as the sampled gap requires), so its
+   error is at most the tuned call's; the low bits can differ from it.
+   MFLAB_ERR_UNSUPPORTED when the requirement exceeds the modulus table.  No
+   reference counterpart. */
+int mflab_ozaki_crt_tune(mflab_handle *h, void *stream, int limbs, int64_t m, int64_t n,
+                         int64_t k, const double *A, int64_t lda, int64_t lsa, const double *B,
+                         int64_t ldb, int64_t lsb, int *moduli);
+
 /* Host-only plan of mflab_gemm_ozaki_crt: digit count *Q, digit width *h
    (bits) and modulus count *T for `limbs`, depth k and either moduli > 0 or,
    with moduli == 0, a scale gap of gap8/8 bits (the tuner's input).  No

@@ -129,6 +129,23 @@ def create_handle(device: Optional[int] = None) -> C.c_void_p:
     return out
 
 
+_side_handles: dict = {}
+
+
+def _side_handle(device: int):
+    """a second per-thread handle (its own scratch) for work that runs on a
+    side stream concurrently with the default handle's"""
+    key = (device, threading.get_ident())
+    with _handles_lock:
+        h = _side_handles.get(key)
+        if h is None:
+            out = C.c_void_p()
+            _check(_native.load().mflab_create(C.byref(out), device), "mflab_create")
+            h = out
+            _side_handles[key] = h
+        return h
+
+
 def destroy_handle(h: C.c_void_p) -> None:
     _check(_native.load().mflab_destroy(h), "mflab_destroy")
 
@@ -536,6 +553,22 @@ def ozaki_crt_moduli() -> list:
     """The modulus table of the modular INT8 route."""
     lib = _native.load()
     return [int(lib.mflab_ozaki_crt_modulus(t)) for t in range(lib.mflab_ozaki_crt_modulus(-1))]
+
+
+def ozaki_crt_tune_moduli(A: MFMatrix, B: MFMatrix) -> int:
+    """The modulus count gemm_(C, A, B) on the modular INT8 route would pick
+    with ozaki_moduli = 0 (the sampled scale gap; one stream
+    synchronisation), without forming the product.  A product at that fixed
+    count takes digits as wide as the count allows, at least as wide as the
+    tuned call's, so its error is at most the tuned call's."""
+    N = _same_type(A, B)
+    if A.n != B.m:
+        raise DimensionMismatch("gemm! inner dimensions differ")
+    lib, h, s = _lib_h(A)
+    T = C.c_int()
+    _check(lib.mflab_ozaki_crt_tune(h, s, N, A.m, B.n, A.n, A.ptr(), A.ld, A.ls, B.ptr(), B.ld,
+                                    B.ls, C.byref(T)), "ozaki tune")
+    return int(T.value)
 
 
 def ozaki_last_moduli(device: Optional[int] = None) -> int:
@@ -1549,7 +1582,7 @@ class OpNormInf:
     """||A||_inf of one matrix on its device (the matrix term of the normwise
     backward error), for repeated backward errors against it."""
 
-    def __init__(self, A: MFMatrix, uplo: str = "general"):
+    def __init__(self, A: MFMatrix, uplo: str = "general", handle=None):
         N = _same_type(A)
         if uplo not in _UPLO_R:
             raise ArgumentError("uplo must be :general, :L or :U")
@@ -1557,6 +1590,8 @@ class OpNormInf:
         self.value = torch.zeros(N, dtype=torch.float64, device=A.storage.device)
         self.nonfinite = torch.zeros(1, dtype=torch.int32, device=A.storage.device)
         lib, h, s = _lib_h(A)
+        if handle is not None:
+            h = handle
         _check(lib.mflab_opnorm_inf(h, s, N, _UPLO_R[uplo], A.m, A.n, A.ptr(), A.ld, A.ls,
                                     self.value.data_ptr(), self.nonfinite.data_ptr()),
                "opnorm")
@@ -1645,6 +1680,16 @@ def solve_mixed_lu(A: MFMatrix, B: MFMatrix, tol: float = 0.0, maxiter: int = 40
     dev = A.storage.device
     lib, h, s = _lib_h(A)
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)] if timing else None
+    # ||A||_inf of the backward errors: one serial chain per row, independent
+    # of the factor, so it runs on a side stream (with a handle of its own)
+    # while the binary64 LU runs
+    main = torch.cuda.current_stream(dev)
+    side = torch.cuda.Stream(dev)
+    side.wait_stream(main)
+    with torch.cuda.stream(side):
+        anorm = OpNormInf(A, handle=_side_handle(A.device))
+    anorm.value.record_stream(main)
+    anorm.nonfinite.record_stream(main)
     if timing:
         ev[0].record()
     LU = _leading_limb(A)
@@ -1669,7 +1714,7 @@ def solve_mixed_lu(A: MFMatrix, B: MFMatrix, tol: float = 0.0, maxiter: int = 40
     X = MFMatrix.zeros(N, n, None if B.is_vector else B.n, device=dev)
     R = B.copy()
     D = MFMatrix.empty(1, n, None if B.is_vector else B.n, device=dev)
-    anorm = OpNormInf(A)
+    main.wait_stream(side)
     rcfg = dataclasses.replace(config, gemm_strategy="ozaki", ozaki_scheme="modular",
                                ozaki_slices=0)
     history = []
@@ -1684,12 +1729,12 @@ def solve_mixed_lu(A: MFMatrix, B: MFMatrix, tol: float = 0.0, maxiter: int = 40
         if residual == "int8":
             R.copy_(B)
             if prepared is None:
-                # the first residual tunes the modulus count; A is then
-                # prepared once for the later ones
-                gemm_(R, A, X, -1.0, 1.0, config=rcfg)
-                prepared = PreparedInt8Operand(A, ozaki_last_moduli(A.device))
-            else:
-                gemm_prepared_(R, prepared, X, -1.0, 1.0, config=rcfg)
+                # the modulus count the tuner picks for A and the first
+                # iterate; A's residues are then prepared once for every
+                # residual
+                moduli = rcfg.ozaki_moduli or ozaki_crt_tune_moduli(A, X)
+                prepared = PreparedInt8Operand(A, moduli)
+            gemm_prepared_(R, prepared, X, -1.0, 1.0, config=rcfg)
         else:
             residual_(R, A, X, B)
         be = normwise_backward_error(A, X, B, R, anorm=anorm)

@@ -162,6 +162,8 @@ SIGNATURES = {
     "mflab_gemm_ozaki_crt": [_vp, _vp, _int, _int, _i64, _i64, _i64, _vp, _i64, _i64, _vp, _i64,
                              _i64, _vp, _i64, _i64, _d, _d],
     "mflab_ozaki_last_moduli": [_vp],
+    "mflab_ozaki_crt_tune": [_vp, _vp, _int, _i64, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _i64,
+                             C.POINTER(_int)],
     "mflab_syrk_lower_ozaki": [_vp, _vp, _int, _int, _int, _i64, _i64, _vp, _i64, _i64, _vp, _i64,
                                _i64, _d, _d],
     "mflab_potrf_ozaki": [_vp, _vp, _int, _int, _i64, _vp, _i64, _i64, _i64, _i64, _vp],

@@ -1422,6 +1422,34 @@ extern "C" int mflab_gemm_ozaki_crt(mflab_handle *h, void *stream, int limbs, in
 
 extern "C" int mflab_ozaki_last_moduli(mflab_handle *h) { return h ? h->last_moduli : 0; }
 
+// The modulus count mflab_gemm_ozaki_crt(moduli = 0) would choose for these
+// operands (the same scale pass and sampled gap, one stream
+// synchronisation), without the product: a caller that prepares A once for
+// many products with it takes the count from here.  Products at that count
+// use digits as wide as the count allows (crt_h_for), at least as wide as
+// the tuned call's.
+extern "C" int mflab_ozaki_crt_tune(mflab_handle *h, void *stream, int limbs, int64_t m,
+                                    int64_t n, int64_t k, const double *A, int64_t lda,
+                                    int64_t lsa, const double *B, int64_t ldb, int64_t lsb,
+                                    int *moduli) {
+    MFLAB_RANGE("mflab_ozaki_crt_tune");
+    if (!h || !mfl::valid_limbs(limbs)) return MFLAB_ERR_UNSUPPORTED;
+    if (m < 1 || n < 1 || k < 1 || !moduli) return MFLAB_ERR_ARG;
+    if (lda < m || ldb < k) return MFLAB_ERR_ARG;
+    if ((n + 255) / 256 * 256 > 65535LL || m > 0x3fffffffLL) return MFLAB_ERR_UNSUPPORTED;
+    int *rowexp = nullptr, *colexp = nullptr;
+    int g = 0;
+    int rc = mfl::ozaki_scales(h, limbs, m, n, k, mfl::Mat{(double *)A, lda, lsa},
+                               mfl::Mat{(double *)B, ldb, lsb}, (cudaStream_t)stream, 1, &g,
+                               &rowexp, &colexp);
+    if (rc) return rc;
+    mfl::CrtPlan p;
+    rc = mfl::crt_plan(limbs, m, n, k, 0, g, p);
+    if (rc) return rc;
+    *moduli = p.T;
+    return MFLAB_OK;
+}
+
 // lower(C) = alpha * op(A) op(A)^T + beta * lower(C) through the modular
 // route: trans = 0, A n x k (the trailing-update form A A^T); trans = 1, A
 // k x n (the reference syrk! form P^T P).  moduli = 0: tuner.

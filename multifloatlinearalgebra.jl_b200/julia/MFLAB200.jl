@@ -803,7 +803,7 @@ round(A) on the device, its solve workspace prepared once (mflab_lu64_prepare:
 permutation, inverted diagonal blocks, premultiplied block columns), then
 iterative refinement with Float64xN residuals through the INT8 modular GEMM;
 A's residues are prepared once (mflab_ozaki_crt_prepare) at the modulus count
-the first residual tuned.  No reference counterpart: it composes lu!,
+the tuner picks for A and the first iterate (mflab_ozaki_crt_tune).  No reference counterpart: it composes lu!,
 residual! and refinement_correction!.  Returns (X, iterations, worst backward
 error)."""
 function solve_mixed_lu(A::MFDeviceMatrix{N}, B::MFDeviceMatrix{N};
@@ -835,7 +835,14 @@ function solve_mixed_lu(A::MFDeviceMatrix{N}, B::MFDeviceMatrix{N};
     X = zeros(MFDeviceArray{N,2}, n, B.n; device=A.device)
     R = copy(B)
     D = MFDeviceArray{1,2}(undef, n, B.n; device=A.device)
-    dc = DeviceConfig(int8=:modular)
+    # ||A||_inf once (mflab_opnorm_inf), for every iteration's backward error
+    anorm = DeviceWords{Float64}(N, A.device)
+    anf = DeviceWords{Cint}(1, A.device)
+    check(ccall((:mflab_opnorm_inf, libmflab), Cint,
+                (Ptr{Cvoid}, Ptr{Cvoid}, Cint, Cint, Int64, Int64, Ptr{Float64}, Int64, Int64,
+                 Ptr{Float64}, Ptr{Cint}),
+                handle.ptr, stream, N, 0, n, n, A.ptr, A.ld, A.ls, anorm.ptr, anf.ptr))
+    berr = DeviceWords{Float64}(max(B.n, 1) * N, A.device)
     one_, mone = _scalar(Val(N), one(MF{N})), _scalar(Val(N), -one(MF{N}))
     prep, T = nothing, 0
     worst, it = Inf, 0
@@ -855,11 +862,15 @@ function solve_mixed_lu(A::MFDeviceMatrix{N}, B::MFDeviceMatrix{N};
             memcpy!(R.ptr + 8 * (l * R.ls + c * R.ld), B.ptr + 8 * (l * B.ls + c * B.ld), 8 * n, 2)
         end
         if prep === nothing
-            # the first residual tunes the modulus count; A's residues are
-            # then prepared once for the later residuals
-            gemm!(R, A, X, -one(MF{N}), one(MF{N}); device_config=dc, handle=handle,
-                  stream=stream)
-            T = Int(ccall((:mflab_ozaki_last_moduli, libmflab), Cint, (Ptr{Cvoid},), handle.ptr))
+            # the modulus count the tuner picks for A and the first iterate;
+            # A's residues are then prepared once for every residual
+            Tr = Ref{Cint}(0)
+            check(ccall((:mflab_ozaki_crt_tune, libmflab), Cint,
+                        (Ptr{Cvoid}, Ptr{Cvoid}, Cint, Int64, Int64, Int64, Ptr{Float64}, Int64,
+                         Int64, Ptr{Float64}, Int64, Int64, Ptr{Cint}),
+                        handle.ptr, stream, N, n, B.n, n, A.ptr, A.ld, A.ls, X.ptr, X.ld, X.ls,
+                        Tr))
+            T = Int(Tr[])
             pb = Ref{Csize_t}(0)
             check(ccall((:mflab_ozaki_crt_prepare_bytes, libmflab), Cint,
                         (Cint, Cint, Int64, Int64, Ptr{Csize_t}), N, T, n, n, pb))
@@ -868,16 +879,22 @@ function solve_mixed_lu(A::MFDeviceMatrix{N}, B::MFDeviceMatrix{N};
                         (Ptr{Cvoid}, Ptr{Cvoid}, Cint, Cint, Int64, Int64, Ptr{Float64}, Int64,
                          Int64, Ptr{Cvoid}),
                         handle.ptr, stream, N, T, n, n, A.ptr, A.ld, A.ls, prep.ptr))
-        else
-            check(ccall((:mflab_gemm_ozaki_crt_prepared, libmflab), Cint,
-                        (Ptr{Cvoid}, Ptr{Cvoid}, Cint, Cint, Int64, Int64, Int64, Ptr{Cvoid},
-                         Ptr{Float64}, Int64, Int64, Ptr{Float64}, Int64, Int64, Ptr{Float64},
-                         Ptr{Float64}),
-                        handle.ptr, stream, N, T, n, B.n, n, prep.ptr, X.ptr, X.ld, X.ls, R.ptr,
-                        R.ld, R.ls, mone, one_))
         end
-        worst = maximum(Float64(e) for e in normwise_backward_error(A, X, B, R; handle=handle,
-                                                                    stream=stream))
+        check(ccall((:mflab_gemm_ozaki_crt_prepared, libmflab), Cint,
+                    (Ptr{Cvoid}, Ptr{Cvoid}, Cint, Cint, Int64, Int64, Int64, Ptr{Cvoid},
+                     Ptr{Float64}, Int64, Int64, Ptr{Float64}, Int64, Int64, Ptr{Float64},
+                     Ptr{Float64}),
+                    handle.ptr, stream, N, T, n, B.n, n, prep.ptr, X.ptr, X.ld, X.ls, R.ptr,
+                    R.ld, R.ls, mone, one_))
+        check(ccall((:mflab_backward_error_norm, libmflab), Cint,
+                    (Ptr{Cvoid}, Ptr{Cvoid}, Cint, Int64, Int64, Int64, Ptr{Float64}, Ptr{Cint},
+                     Ptr{Float64}, Int64, Int64, Ptr{Float64}, Int64, Int64, Ptr{Float64}, Int64,
+                     Int64, Ptr{Float64}),
+                    handle.ptr, stream, N, n, n, B.n, anorm.ptr, anf.ptr, X.ptr, X.ld, X.ls,
+                    B.ptr, B.ld, B.ls, R.ptr, R.ld, R.ls, berr.ptr))
+        v = host(berr, stream)
+        worst = maximum(Float64(MultiFloat{Float64,N}(ntuple(l -> v[(j - 1) * N + l], N)))
+                        for j in 1:B.n)
         worst <= tol && break
     end
     return X, it, worst

@@ -32,6 +32,39 @@ def test_prepared_equals_unprepared(mf, rng, N, shape, T):
     assert_bitwise(C2.to_numpy(), C1.to_numpy(), "prepared")
 
 
+@pytest.mark.parametrize("N", [2, 3, 4])
+@pytest.mark.parametrize("shape,spread", [((33, 70, 45), 0), ((200, 513, 130), 20),
+                                          ((300, 1100, 16), 10)], ids=str)
+def test_tune_only_matches_tuned_product(mf, ref, rng, N, shape, spread):
+    """ozaki_crt_tune_moduli picks the count the tuned product picks on the same
+    operands; the prepared product at that count equals the fixed-count
+    product bit for bit, and its error against the exact product is at most
+    the tuned product's (wider digits; the mixed solve's first residual)"""
+    m, k, n = shape
+    A, B = syn.randn_mf(rng, N, m, k, spread=spread), syn.randn_mf(rng, N, k, n, spread=spread)
+    Ad, Bd = mf.MFMatrix.from_numpy(A), mf.MFMatrix.from_numpy(B)
+    T = mf.ozaki_crt_tune_moduli(Ad, Bd)
+    C1, C2, C3 = (mf.MFMatrix.zeros(N, m, n) for _ in range(3))
+    mf.gemm_(C1, Ad, Bd, config=_cfg(mf))
+    assert mf.ozaki_last_moduli() == T
+    mf.gemm_prepared_(C2, mf.PreparedInt8Operand(Ad, T), Bd)
+    mf.gemm_(C3, Ad, Bd, config=_cfg(mf, ozaki_moduli=T))
+    assert_bitwise(C2.to_numpy(), C3.to_numpy(), "prepared at the tuned count")
+    rows, cols = (a.ravel() for a in np.meshgrid(np.arange(m), np.arange(n), indexing="ij"))
+    err1, scale, _ = ref.exact_gemm_check(A, B, C1.to_numpy(), rows, cols)
+    err2, _, _ = ref.exact_gemm_check(A, B, C2.to_numpy(), rows, cols)
+    floor = 2.0 ** (-53 * N) * scale.max()
+    assert err2.max() <= 1.01 * max(err1.max(), floor)
+
+
+def test_tune_only_argument_checks(mf, rng):
+    A = mf.MFMatrix.from_numpy(syn.randn_mf(rng, 2, 10, 12))
+    with pytest.raises(mf.DimensionMismatch):
+        mf.ozaki_crt_tune_moduli(A, mf.MFMatrix.from_numpy(syn.randn_mf(rng, 2, 11, 3)))
+    with pytest.raises(mf.ArgumentError):
+        mf.ozaki_crt_tune_moduli(A, mf.MFMatrix.from_numpy(syn.randn_mf(rng, 3, 12, 3)))
+
+
 @pytest.mark.parametrize("engine", ["tcgen05", "tcgen05_pair", "library"])
 def test_prepared_engines_and_reuse(mf, rng, engine):
     N, m, k, n, T = 2, 260, 700, 140, 20
