@@ -221,10 +221,20 @@ static int run_mm(int64_t m, int64_t n, int64_t k, Mat A, Mat B, Mat C, const do
     return record_cuda_error(cudaGetLastError(), "mm_kernel launch");
 }
 
-// tile shapes per limb count (FP64-issue bound; registers: TM*TN*N accumulators)
+// tile shapes per limb count (FP64-issue bound; registers: TM*TN*N accumulators).
+// Products at most 16 columns wide (a blocked factorization's next block
+// columns, a few right-hand sides) take 32 x 16 tiles of two outputs per
+// thread: a 64 x 64 tile would leave three quarters of its threads idle and
+// put the whole product on a few CTAs.  Every output is the same chain in
+// either shape.
 template <int N, int TA, bool TB, bool TRI, bool FUSED, bool TRMM = false>
 static int run_mm_n(int64_t m, int64_t n, int64_t k, Mat A, Mat B, Mat C, const double *alpha,
                     const double *beta, cudaStream_t s, const int *info, int mode) {
+    if constexpr (N >= 2 && !FUSED && !TRMM) {
+        if (n <= 16)
+            return run_mm<N, 32, 16, (N == 2 ? 16 : 8), 2, 1, TA, TB, TRI, FUSED, TRMM>(
+                m, n, k, A, B, C, alpha, beta, s, info, mode);
+    }
     if constexpr (N == 1)
         return run_mm<1, 64, 64, 16, 4, 4, TA, TB, TRI, FUSED, TRMM>(m, n, k, A, B, C, alpha, beta, s, info, mode);
     else if constexpr (N == 2)
