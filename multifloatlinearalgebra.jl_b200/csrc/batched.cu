@@ -367,13 +367,16 @@ static int launch_backward_n(cudaStream_t s, int64_t nblocks, int64_t maxn, cons
                              const int64_t *offsets, const int64_t *boffsets,
                              const int64_t *order, const double *L, int64_t ls_s, double *X,
                              int64_t ls_x, const int *info) {
-    static std::atomic<unsigned long long> done{0};
-    constexpr int max_smem = mfl::BW_PER_WARP * (mfl::BATCH_MAXN * N + 1) * (int)sizeof(double);
-    int rc = mfl::set_smem_once((const void *)mfl::spd_batched_backward_kernel<N>, max_smem, done,
-                                "spd batched backward smem");
-    if (rc) return rc;
     const size_t smem = (size_t)mfl::BW_PER_WARP * (size_t)((maxn > 0 ? maxn : 1) * N + 1) *
                         sizeof(double);
+    if (smem > 48 * 1024) {  // large blocks only: the opt-in above the default limit
+        static std::atomic<unsigned long long> done{0};
+        constexpr int max_smem =
+            mfl::BW_PER_WARP * (mfl::BATCH_MAXN * N + 1) * (int)sizeof(double);
+        int rc = mfl::set_smem_once((const void *)mfl::spd_batched_backward_kernel<N>, max_smem,
+                                    done, "spd batched backward smem");
+        if (rc) return rc;
+    }
     const int64_t grid = (nblocks + mfl::BW_PER_WARP - 1) / mfl::BW_PER_WARP;
     mfl::spd_batched_backward_kernel<N><<<(unsigned)grid, 32, smem, s>>>(
         nblocks, sizes, offsets, boffsets, order, L, ls_s, X, ls_x, info, maxn);

@@ -1044,7 +1044,7 @@ __global__ void __cluster_dims__(LUC_CL, 1, 1) __launch_bounds__(LUR_NT, 1)
         const int64_t k = k0 + c;
         const int buf = c & 1;
         // this step's candidates from every CTA (bounded wait)
-        // (one verdict per warp, so the warp's shuffles below stay converged)
+        // (one decision per warp, so the warp's shuffles below stay converged)
         const bool got =
             __all_sync(0xffffffffu, lur_wait(&rbar[buf], (uint32_t)((c >> 1) & 1), &s_abort));
         if (!got) {
