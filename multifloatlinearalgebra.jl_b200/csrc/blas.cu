@@ -55,6 +55,10 @@ __global__ void __launch_bounds__(MMShape<N, BM, BN, BK, TM, TN>::NT)
               int overwrite, const int *info, int mode) {
     using S = MMShape<N, BM, BN, BK, TM, TN>;
     constexpr int NT = S::NT, TX = S::TX, TY = S::TY;
+    // a kernel launched after this one as a programmatic dependent (the
+    // blocked Cholesky's next step) may be placed now; it waits for this
+    // grid's completion before reading (no effect otherwise)
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     extern __shared__ double smem[];
     double *As = smem;                   // [2][N][BK][BM]
     double *Bs = smem + 2 * N * BK * BM;  // [2][N][BK][BN]

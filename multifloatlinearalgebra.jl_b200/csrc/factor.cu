@@ -100,6 +100,9 @@ constexpr int PF_W = 16, PF_NT = 128, PF_DIAG = 32;
 template <int N>
 __global__ void __launch_bounds__(PF_NT)
     potrf_step_kernel(Mat A, int64_t f, int w, int64_t t_rows, int *info) {
+    // launched as a programmatic dependent of the previous block's update of
+    // these columns: wait for that grid's results before reading anything
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     if (*info) return;
     extern __shared__ double pf_fin[];  // [PF_W][PF_NT][N] final values of each thread's row
     __shared__ double Ls[PF_W][PF_W][N];  // L[j][k] of the block's rows
@@ -247,8 +250,23 @@ static int potrf_n(mflab_handle *h, int64_t n, Mat A, int64_t block, int *info, 
         const int64_t t = n - 1 - last;  // rows below the block
         const unsigned grid = (unsigned)std::max<int64_t>(1, (t + PF_NT - PF_DIAG - 1) /
                                                                  (PF_NT - PF_DIAG));
-        potrf_step_kernel<N><<<grid, PF_NT, fin_bytes, sp>>>(A, first, w, t, info);
-        rc = record_cuda_error(cudaGetLastError(), "potrf step");
+        {
+            // programmatic stream serialization: the step's CTAs are placed
+            // while the previous next-columns update drains
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(grid);
+            cfg.blockDim = dim3(PF_NT);
+            cfg.dynamicSmemBytes = fin_bytes;
+            cfg.stream = sp;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+            attr[0].val.programmaticStreamSerializationAllowed = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            rc = record_cuda_error(
+                cudaLaunchKernelEx(&cfg, potrf_step_kernel<N>, A, first, w, t, info),
+                "potrf step");
+        }
         if (rc || t == 0) break;
         e = cudaEventRecord(ev_step, sp);
         // the next block's columns, after the rest of the previous block
