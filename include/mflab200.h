@@ -108,8 +108,10 @@ int mflab_stream_synchronize(void *stream);
 
    Host forms: `host` is host memory (pinned for an asynchronous copy;
    pageable memory is accepted, the copy then completes before the call
-   returns).  They stage chunks through a 64 MiB buffer the handle allocates
-   on first use, so two streams converting at once need two handles.
+   returns).  They stage chunks through a buffer of two halves the handle
+   allocates on first use, each half sized to the transfer (32 MiB to
+   1 GiB, grown by a later larger transfer once the handle's copies are
+   done), so two streams converting at once need two handles.
    Device forms: X is device memory; no staging, no allocation. */
 int mflab_h2d_interleaved(mflab_handle *h, void *stream, int limbs, int64_t m, int64_t n,
                           const double *host, int64_t ldh, double *P, int64_t ld, int64_t ls);
