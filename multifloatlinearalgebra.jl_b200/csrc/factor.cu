@@ -357,6 +357,10 @@ static int potrf_ozaki_n(mflab_handle *h, int64_t n, Mat A, int64_t nb, int64_t 
 template <int N, int NT>
 __global__ void __launch_bounds__(NT) lu_pivot_kernel(int64_t m, int64_t c_lo, int64_t c_hi, Mat A,
                                                       int64_t k, int64_t *ipiv, int *info) {
+    // the panel's steps are programmatic dependent launches: wait for the
+    // previous step's grid, let the next step's CTAs be placed meanwhile
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     if (*info) return;
     __shared__ double sval[NT][N];
     __shared__ int64_t sidx[NT];
@@ -468,6 +472,8 @@ __global__ void lu_swap_rest_kernel(int64_t n, Mat A, int64_t first, int64_t las
 // rank-1 update of panel columns k+1..last for rows k+1..m-1 (lu.jl:47-82)
 template <int N>
 __global__ void lu_rank1_kernel(int64_t m, Mat A, int64_t k, int64_t last, const int *info) {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     if (*info) return;
     const int64_t r = k + 1 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= m) return;
@@ -1293,6 +1299,25 @@ static int lu64_lookahead_streams(mflab_handle *h) {
     return e == cudaSuccess ? MFLAB_OK : record_cuda_error(e, "getrf64 streams");
 }
 
+// One step of a matched LU panel (pivot or rank-1 kernel), launched with
+// programmatic stream serialization: its CTAs are placed while the previous
+// step drains and wait for it in the kernel (griddepcontrol.wait).
+template <typename... KArgs, typename... Args>
+static int launch_panel_step(void (*kern)(KArgs...), unsigned grid, unsigned block,
+                             cudaStream_t s, const char *what, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return record_cuda_error(cudaLaunchKernelEx(&cfg, kern, args...), what);
+}
+
 // panel width nb (4..32): a panel of up to 4096 rows lives in the registers
 // of an 8-CTA cluster (lu64_cluster_panel_reg_kernel), one of up to about
 // 6000 rows in its shared memory (lu64_cluster_panel_kernel); a taller
@@ -1404,13 +1429,13 @@ static int getrf_n(int64_t m, int64_t n, Mat A, int64_t *ipiv, int64_t block, in
     for (int64_t first = 0; first < kmax; first += block) {
         const int64_t last = first + block - 1 < kmax - 1 ? first + block - 1 : kmax - 1;
         for (int64_t k = first; k <= last; ++k) {
-            lu_pivot_kernel<N, 512><<<1, 512, 0, s>>>(m, first, last + 1, A, k, ipiv, info);
-            rc = record_cuda_error(cudaGetLastError(), "getrf pivot");
+            rc = launch_panel_step(lu_pivot_kernel<N, 512>, 1, 512, s, "getrf pivot", m, first,
+                                   last + 1, A, k, ipiv, info);
             if (rc) return rc;
             if (k < last && k + 1 < m) {
                 const int64_t rows = m - k - 1;
-                lu_rank1_kernel<N><<<(unsigned)((rows + 127) / 128), 128, 0, s>>>(m, A, k, last, info);
-                rc = record_cuda_error(cudaGetLastError(), "getrf rank1");
+                rc = launch_panel_step(lu_rank1_kernel<N>, (unsigned)((rows + 127) / 128), 128, s,
+                                       "getrf rank1", m, A, k, last, (const int *)info);
                 if (rc) return rc;
             }
         }

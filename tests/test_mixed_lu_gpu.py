@@ -97,6 +97,17 @@ def test_backward_error_with_cached_norm(mf, rng, N):
     a = mf.normwise_backward_error(Ad, Xd, Bd, Rd)
     b = mf.normwise_backward_error(Ad, Xd, Bd, Rd, anorm=mf.OpNormInf(Ad))
     assert np.array_equal(np.array(a).view(np.uint64), np.array(b).view(np.uint64))
+    # the norm formed on a side stream with a handle of its own (as the mixed
+    # solve does while its factor runs) is the same value
+    side, h2 = torch.cuda.Stream(), mf.create_handle()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        an2 = mf.OpNormInf(Ad, handle=h2)
+    torch.cuda.current_stream().wait_stream(side)
+    c = mf.normwise_backward_error(Ad, Xd, Bd, Rd, anorm=an2)
+    torch.cuda.synchronize()
+    mf.destroy_handle(h2)
+    assert np.array_equal(np.array(a).view(np.uint64), np.array(c).view(np.uint64))
 
 
 @pytest.mark.parametrize("m,n", [(300, 300), (257, 130), (130, 257)])
