@@ -250,23 +250,10 @@ static int potrf_n(mflab_handle *h, int64_t n, Mat A, int64_t block, int *info, 
         const int64_t t = n - 1 - last;  // rows below the block
         const unsigned grid = (unsigned)std::max<int64_t>(1, (t + PF_NT - PF_DIAG - 1) /
                                                                  (PF_NT - PF_DIAG));
-        {
-            // programmatic stream serialization: the step's CTAs are placed
-            // while the previous next-columns update drains
-            cudaLaunchConfig_t cfg = {};
-            cfg.gridDim = dim3(grid);
-            cfg.blockDim = dim3(PF_NT);
-            cfg.dynamicSmemBytes = fin_bytes;
-            cfg.stream = sp;
-            cudaLaunchAttribute attr[1];
-            attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-            attr[0].val.programmaticStreamSerializationAllowed = 1;
-            cfg.attrs = attr;
-            cfg.numAttrs = 1;
-            rc = record_cuda_error(
-                cudaLaunchKernelEx(&cfg, potrf_step_kernel<N>, A, first, w, t, info),
-                "potrf step");
-        }
+        // a programmatic dependent of the previous next-columns update: the
+        // step's CTAs are placed while that update drains
+        rc = launch_programmatic(potrf_step_kernel<N>, dim3(grid), dim3(PF_NT), fin_bytes, sp,
+                                 "potrf step", A, first, w, t, info);
         if (rc || t == 0) break;
         e = cudaEventRecord(ev_step, sp);
         // the next block's columns, after the rest of the previous block
@@ -1299,25 +1286,6 @@ static int lu64_lookahead_streams(mflab_handle *h) {
     return e == cudaSuccess ? MFLAB_OK : record_cuda_error(e, "getrf64 streams");
 }
 
-// One step of a matched LU panel (pivot or rank-1 kernel), launched with
-// programmatic stream serialization: its CTAs are placed while the previous
-// step drains and wait for it in the kernel (griddepcontrol.wait).
-template <typename... KArgs, typename... Args>
-static int launch_panel_step(void (*kern)(KArgs...), unsigned grid, unsigned block,
-                             cudaStream_t s, const char *what, Args... args) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(block);
-    cfg.dynamicSmemBytes = 0;
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    return record_cuda_error(cudaLaunchKernelEx(&cfg, kern, args...), what);
-}
-
 // panel width nb (4..32): a panel of up to 4096 rows lives in the registers
 // of an 8-CTA cluster (lu64_cluster_panel_reg_kernel), one of up to about
 // 6000 rows in its shared memory (lu64_cluster_panel_kernel); a taller
@@ -1429,13 +1397,15 @@ static int getrf_n(int64_t m, int64_t n, Mat A, int64_t *ipiv, int64_t block, in
     for (int64_t first = 0; first < kmax; first += block) {
         const int64_t last = first + block - 1 < kmax - 1 ? first + block - 1 : kmax - 1;
         for (int64_t k = first; k <= last; ++k) {
-            rc = launch_panel_step(lu_pivot_kernel<N, 512>, 1, 512, s, "getrf pivot", m, first,
-                                   last + 1, A, k, ipiv, info);
+            // the panel's steps are programmatic dependents of one another
+            rc = launch_programmatic(lu_pivot_kernel<N, 512>, dim3(1), dim3(512), 0, s,
+                                     "getrf pivot", m, first, last + 1, A, k, ipiv, info);
             if (rc) return rc;
             if (k < last && k + 1 < m) {
                 const int64_t rows = m - k - 1;
-                rc = launch_panel_step(lu_rank1_kernel<N>, (unsigned)((rows + 127) / 128), 128, s,
-                                       "getrf rank1", m, A, k, last, (const int *)info);
+                rc = launch_programmatic(lu_rank1_kernel<N>, dim3((unsigned)((rows + 127) / 128)),
+                                         dim3(128), 0, s, "getrf rank1", m, A, k, last,
+                                         (const int *)info);
                 if (rc) return rc;
             }
         }

@@ -68,6 +68,26 @@ inline int set_smem_once(const void *func, int bytes, std::atomic<unsigned long 
     return 0;
 }
 
+// A kernel launch with programmatic stream serialization: the kernel's CTAs
+// may be placed while the previous kernel on the stream drains (once its CTAs
+// have run griddepcontrol.launch_dependents); the kernel must run
+// griddepcontrol.wait before it reads anything the previous one writes.
+template <typename... KArgs, typename... Args>
+inline int launch_programmatic(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                               cudaStream_t s, const char *what, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return record_cuda_error(cudaLaunchKernelEx(&cfg, kern, args...), what);
+}
+
 inline int cuda_status(cudaError_t e) {
     if (e == cudaSuccess) return MFLAB_OK;
     return MFLAB_ERR_CUDA;

@@ -79,6 +79,10 @@ __global__ void __launch_bounds__(PSTRF_PIVOT_THREADS)
     __shared__ int go;
     __shared__ double spiv[N];
     __shared__ int64_t sp;
+    // the steps are programmatic dependents of one another: wait for the
+    // previous grid, let the next one be placed meanwhile
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     if (st->stop) return;
     const int tid = threadIdx.x;
     // largest diagonal in k..n-1, the first index among equals
@@ -198,6 +202,8 @@ constexpr int PSTRF_UPD_ROWS = 128, PSTRF_UPD_COLS = 16;
 template <int N>
 __global__ void __launch_bounds__(PSTRF_UPD_ROWS)
     pstrf_update_kernel(int64_t n, int64_t k, Mat A, const PstrfState *st) {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     if (st->stop) return;
     const int64_t r = k + 1 + (int64_t)blockIdx.x * PSTRF_UPD_ROWS + threadIdx.x;
     if (r >= n) return;
@@ -228,15 +234,20 @@ static int pstrf_n(mflab_handle *h, cudaStream_t s, int64_t n, Mat A, const doub
     pstrf_init_kernel<<<(unsigned)((n + 255) / 256 > 0 ? (n + 255) / 256 : 1), 256, 0, s>>>(st, n, perm);
     pstrf_check_kernel<N><<<grid, 256, 0, s>>>(n, A, st);
     pstrf_mirror_kernel<N><<<grid, 256, 0, s>>>(n, A, st);
-    for (int64_t k = 0; k < n; ++k) {
-        pstrf_pivot_kernel<N><<<1, PSTRF_PIVOT_THREADS, 0, s>>>(n, k, A, perm, st, t);
+    for (int64_t k = 0; k < n && rc == MFLAB_OK; ++k) {
+        // programmatic dependent launches: each step's CTAs are placed while
+        // the previous step drains
+        rc = launch_programmatic(pstrf_pivot_kernel<N>, dim3(1), dim3(PSTRF_PIVOT_THREADS), 0, s,
+                                 "pstrf pivot", n, k, A, perm, st, t);
         const int64_t tr = n - k - 1;
-        if (tr > 0) {
+        if (tr > 0 && rc == MFLAB_OK) {
             dim3 ug((unsigned)((tr + PSTRF_UPD_ROWS - 1) / PSTRF_UPD_ROWS),
                     (unsigned)((tr + PSTRF_UPD_COLS - 1) / PSTRF_UPD_COLS));
-            pstrf_update_kernel<N><<<ug, PSTRF_UPD_ROWS, 0, s>>>(n, k, A, st);
+            rc = launch_programmatic(pstrf_update_kernel<N>, ug, dim3(PSTRF_UPD_ROWS), 0, s,
+                                     "pstrf update", n, k, A, (const PstrfState *)st);
         }
     }
+    if (rc) return rc;
     pstrf_finish_kernel<<<1, 1, 0, s>>>(st, rank_info);
     return record_cuda_error(cudaGetLastError(), "pstrf launch");
 }
