@@ -218,6 +218,10 @@ template <int N>
 __global__ void __launch_bounds__(QR_CTA)
     qr_reflector_kernel(int64_t m, int64_t s, Mat A, double *tau, int64_t lt, int blocked,
                         double *diag, int64_t bs, int64_t ls, double *aux) {
+    // the steps of the unblocked loops are programmatic dependents of one
+    // another: wait for the previous grid, let the next one be placed
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     __shared__ double slead[N];
     __shared__ int go;
     __shared__ double nbuf[QR_NORM_BUF(N)];
@@ -332,6 +336,8 @@ template <int N>
 __global__ void __launch_bounds__(32 * QR_COL_WARPS)
     qr_apply_kernel(int64_t m, int64_t s, Mat V, const double *tau, int64_t lt, Mat D, int64_t c0,
                     int64_t nd) {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     __shared__ double buf[QR_COL_WARPS][32 * N];
     const int w = threadIdx.x >> 5;
     const int64_t j = (int64_t)blockIdx.x * QR_COL_WARPS + w;
@@ -413,6 +419,8 @@ template <int N>
 __global__ void __launch_bounds__(QR_COLS_PER_CTA)
     qr_update_norms_kernel(int64_t m, int64_t step, Mat A, const double *tau, int64_t lt,
                            QRNorms<N> S, scal<N> floor_) {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const int64_t c = step + 1 + (int64_t)blockIdx.x * QR_COLS_PER_CTA + threadIdx.x;
     if (c >= S.n) return;
     mf<N> t;
@@ -442,6 +450,8 @@ template <int N>
 __global__ void __launch_bounds__(QR_CTA)
     qr_hybrid_pivot_kernel(int64_t m, int64_t step, Mat A, int64_t *perm, QRNorms<N> S,
                            scal<N> one_minus_margin) {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     __shared__ int64_t sp;
     __shared__ double nbuf[QR_NORM_BUF(N)];
     if (threadIdx.x < 32) {
@@ -678,11 +688,18 @@ static int qr_n(mflab_handle *h, cudaStream_t s, int pivoted, int64_t m, int64_t
     }
     (void)hflag;
     if (!pivoted) {
+        // each step's kernels are programmatic dependent launches
         for (int64_t st = 0; st < r; ++st) {
-            qr_reflector_kernel<N><<<1, QR_CTA, 0, s>>>(m, st, A, tau, lt, 0, nullptr, 0, 0, nullptr);
-            if (st + 1 < n)
-                qr_apply_kernel<N><<<warp_col_grid(n - st - 1), 32 * QR_COL_WARPS, 0, s>>>(
-                    m, st, A, tau, lt, A, st + 1, n - st - 1);
+            int rc = launch_programmatic(qr_reflector_kernel<N>, dim3(1), dim3(QR_CTA), 0, s,
+                                         "qr reflector", m, st, A, tau, lt, 0, nullptr, 0, 0,
+                                         nullptr);
+            if (rc) return rc;
+            if (st + 1 < n) {
+                rc = launch_programmatic(qr_apply_kernel<N>, dim3(warp_col_grid(n - st - 1)),
+                                         dim3(32 * QR_COL_WARPS), 0, s, "qr apply", m, st, A,
+                                         (const double *)tau, lt, A, st + 1, n - st - 1);
+                if (rc) return rc;
+            }
         }
     } else {
         // constants of rrqr! (qr.jl:736-737): margin = sqrt(eps), floor = 16 eps,
@@ -700,14 +717,23 @@ static int qr_n(mflab_handle *h, cudaStream_t s, int pivoted, int64_t m, int64_t
         const bool blocked = r >= QR_BLOCK && m * n >= 16384;
         if (!blocked) {
             for (int64_t st = 0; st < r; ++st) {
-                qr_hybrid_pivot_kernel<N><<<1, QR_CTA, 0, s>>>(m, st, A, perm, S, om);
-                qr_reflector_kernel<N><<<1, QR_CTA, 0, s>>>(m, st, A, tau, lt, 0, nullptr, 0, 0, nullptr);
-                if (st + 1 < n) {
-                    qr_apply_kernel<N><<<warp_col_grid(n - st - 1), 32 * QR_COL_WARPS, 0, s>>>(
-                        m, st, A, tau, lt, A, st + 1, n - st - 1);
-                    qr_update_norms_kernel<N><<<col_grid(n - st - 1), QR_COLS_PER_CTA, 0, s>>>(
-                        m, st, A, tau, lt, S, fl);
+                int rc = launch_programmatic(qr_hybrid_pivot_kernel<N>, dim3(1), dim3(QR_CTA), 0,
+                                             s, "qr pivot", m, st, A, perm, S, om);
+                if (rc == MFLAB_OK)
+                    rc = launch_programmatic(qr_reflector_kernel<N>, dim3(1), dim3(QR_CTA), 0, s,
+                                             "qr reflector", m, st, A, tau, lt, 0, nullptr, 0, 0,
+                                             nullptr);
+                if (rc == MFLAB_OK && st + 1 < n) {
+                    rc = launch_programmatic(qr_apply_kernel<N>, dim3(warp_col_grid(n - st - 1)),
+                                             dim3(32 * QR_COL_WARPS), 0, s, "qr apply", m, st, A,
+                                             (const double *)tau, lt, A, st + 1, n - st - 1);
+                    if (rc == MFLAB_OK)
+                        rc = launch_programmatic(
+                            qr_update_norms_kernel<N>, dim3(col_grid(n - st - 1)),
+                            dim3(QR_COLS_PER_CTA), 0, s, "qr norms", m, st, A,
+                            (const double *)tau, lt, S, fl);
                 }
+                if (rc) return rc;
             }
         } else {
             e = cudaMallocHost(&hflag, sizeof(int));
